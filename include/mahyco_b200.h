@@ -1,0 +1,126 @@
+/*
+ * mahyco_b200.h -- C ABI of the B200 MaHyCo hydro-cycle library
+ * (libmahyco_b200.so).  Plain pointers and sizes only.
+ *
+ * Every entry point returns an int status: 0 = MHC_OK, < 0 = API error,
+ * > 0 = numerical status flags of the case (a bitwise OR of MHC_ST_*).
+ * The reference reports the same numerical conditions by exit(1) or
+ * stopComputeLoop; here they are returned so that a failing case can be
+ * retired without stopping the process.
+ *
+ * Reference interfaces replaced (file:line inside cea-hpc/MaHyCo):
+ *   module entry points      src/Mahyco.axl:244-261, src/MahycoModule.h:164-349
+ *   time loop order          src/Mahyco.config:15-36
+ *   IEquationOfState         src/eos/IEquationOfState.h:38-65
+ *   IRemap                   src/Remap/IRemap.h:44-63
+ *   EnvSummation time history src/time_history/EnvSummationService.cc:77-169
+ */
+#ifndef MAHYCO_B200_H
+#define MAHYCO_B200_H
+
+#include "mahyco_case.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* API errors */
+#define MHC_OK 0
+#define MHC_ERR_ARG (-1)          /* bad argument / unknown name */
+#define MHC_ERR_CUDA (-2)         /* CUDA runtime error (message: mhc_last_error) */
+#define MHC_ERR_UNSUPPORTED (-3)  /* option outside the implemented hot path */
+#define MHC_ERR_ORDER (-4)        /* entry point called out of time-loop order */
+#define MHC_ERR_NOMEM (-5)        /* device allocation failed / HBM budget */
+
+/* numerical status flags (returned as positive values) */
+#define MHC_ST_NEG_VOLUME 1       /* MahycoModule.cc:1164-1191 (exit(1) there) */
+#define MHC_ST_DT_UNDERFLOW 2     /* MahycoModule.cc:1816-1833 (exit(1) there) */
+#define MHC_ST_NAN 4              /* RemapADIFinal.cc:274-284 (exit(1) there) */
+#define MHC_ST_STOP 8             /* final time reached: stopComputeLoop (MahycoModule.cc:1851-1857) */
+
+typedef struct mhc_case mhc_case;
+
+/* last error message of the calling thread (static storage) */
+const char* mhc_last_error(void);
+
+/* library version string */
+const char* mhc_version(void);
+
+/* Case lifecycle.  Allocates the device state of one case on the current
+ * CUDA device, on a private stream.  Replaces the Arcane module instance. */
+int mhc_case_create(const mhc_case_params* params, mhc_case** out);
+int mhc_case_destroy(mhc_case* h);
+
+/* HBM bytes one case with these parameters needs (serving admission). */
+long long mhc_case_device_bytes(const mhc_case_params* params);
+
+/* --- init entry points (Mahyco.config:15-21) ----------------------------
+ * HydroStartInit + ComputeCellMass + ComputeNodeMass
+ * (MahycoModule.cc:21-262, MahycoAnnexe.cc:11-235). */
+int mhc_hydro_start_init(mhc_case* h);
+
+/* --- compute-loop entry points (Mahyco.config:23-36) --------------------
+ * They must be called in time-loop order.  Consecutive entry points are
+ * fused into one kernel launch; a fused stage is launched by its last
+ * entry point:
+ *   SaveValuesAtN  (no device work: values at n stay in place)
+ *   UpdateVelocity, ApplyBoundaryCondition, UpdatePosition      -> node pass
+ *   ComputeGeometricValues, UpdateDensity, ComputeArtificialViscosity,
+ *   UpdateElasticityAndPlasticity, UpdateEnergyAndPressure       -> cell pass
+ *   Remap                                                        -> ADI remap
+ *   ComputeDeltaT                                                -> dt reduction */
+int mhc_save_values_at_n(mhc_case* h);
+int mhc_update_velocity(mhc_case* h);
+int mhc_apply_boundary_condition(mhc_case* h);
+int mhc_update_position(mhc_case* h);
+int mhc_compute_geometric_values(mhc_case* h);
+int mhc_update_density(mhc_case* h);
+int mhc_compute_artificial_viscosity(mhc_case* h);
+int mhc_update_elasticity_and_plasticity(mhc_case* h);
+int mhc_update_energy_and_pressure(mhc_case* h);
+int mhc_remap(mhc_case* h);
+int mhc_compute_delta_t(mhc_case* h);
+
+/* n complete compute-loop iterations, enqueued asynchronously on the case
+ * stream (no host synchronisation inside).  Iterations after a stop or an
+ * error flag are skipped on the device. */
+int mhc_cycle(mhc_case* h, int n);
+
+/* same as mhc_cycle, but the n iterations are captured once in a CUDA
+ * graph and replayed (launch-bound small cases) */
+int mhc_cycle_graph(mhc_case* h, int n);
+
+/* wait for the case stream; returns the numerical status flags */
+int mhc_synchronize(mhc_case* h);
+
+/* time-loop scalars after the last completed iteration */
+int mhc_get_scalars(mhc_case* h, double* time, double* deltat, long long* iteration, int* status);
+
+/* Named fields (names of src/Mahyco.axl: Density, Pressure, InternalEnergy,
+ * SoundSpeed, PseudoViscosity, CellMass, CellVolume, FracVol, MassFraction,
+ * CaracteristicLength, EnvMask; nodes: Velocity (x,y,z interleaved),
+ * NodeMass, NodeCoord).  env < 0 selects the global cell value, env >= 0
+ * the environment value (0 where the cell is not in the environment).
+ * Returns the number of doubles written, or an error. */
+long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, long long capacity);
+
+/* --- IEquationOfState (IEquationOfState.h:38-65) ------------------------
+ * applyEOS(env) on the current density and internal energy of the env
+ * cells, followed (when all_envs is set) by computePressionMoyenne. */
+int mhc_eos_apply(mhc_case* h, int env);
+
+/* --- IRemap::appliRemap + remapVariables (IRemap.h:44-63) ---------------
+ * The remap stage of the current iteration, for a caller that has run the
+ * Lagrange entry points. */
+int mhc_remap_apply(mhc_case* h);
+
+/* --- EnvSummation (EnvSummationService.cc:77-169) -----------------------
+ * out[0] = time, then per environment: CellMass (plain average), Pressure
+ * (plain average), Density (volume weighted), InternalEnergy (mass
+ * weighted), present flag: 1 + 5*nb_env doubles. */
+int mhc_time_history(mhc_case* h, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

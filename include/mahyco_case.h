@@ -1,0 +1,134 @@
+/*
+ * mahyco_case.h -- plain-C description of one MaHyCo case (the subset of the
+ * .arc dataset that the hydro cycle hot path reads).
+ *
+ * Field names and defaults follow the reference option descriptors:
+ *   module options           src/Mahyco.axl:263-557
+ *   RemapADI options         src/Remap/RemapADI.axl:162-210
+ *   PerfectGas options       src/eos/perfectgas/PerfectGasEOS.axl:157-183
+ *   StiffenedGas options     src/eos/stiffenedgas/StiffenedGasEOS.axl:158-184
+ *   MieGruneisen options     src/eos/miegruneisen/MieGruneisenEOS.axl:157-219
+ *   enums (BC kinds, limiter ids, case ids)  src/TypesMahyco.h:16-105
+ *   cartesian mesh generator <meshgenerator><cartesian> block of the .arc files
+ *
+ * The struct is shared by the CUDA library (include/mahyco_b200.h) and by the
+ * CPU oracle used by the tests; it contains no pointers, so it can be filled
+ * from C, C++, Fortran or Python (ctypes) alike.  mhc_case_params_default()
+ * writes the reference defaults.
+ */
+#ifndef MAHYCO_CASE_H
+#define MAHYCO_CASE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MHC_MAX_ENV 4
+#define MHC_MAX_BC 12
+
+/* equation-of-state service kinds (<eos-model name="...">) */
+enum mhc_eos_kind {
+  MHC_EOS_PERFECT_GAS = 0,   /* PerfectGasEOSService.cc */
+  MHC_EOS_STIFFENED_GAS = 1, /* StiffenedGasEOSService.cc */
+  MHC_EOS_MIE_GRUNEISEN = 2  /* MieGruneisenEOSService.cc */
+};
+
+/* boundary-condition kinds, same numbering as TypesMahyco::eBoundaryCondition */
+enum mhc_bc_kind {
+  MHC_BC_VX = 0, MHC_BC_VY = 1, MHC_BC_VZ = 2
+};
+
+/* boundary surfaces built by MahycoModule::PrepareFaceGroup (MahycoAnnexe.cc:149-235) */
+enum mhc_surface {
+  MHC_XMIN = 0, MHC_YMIN = 1, MHC_ZMIN = 2, MHC_XMAX = 3, MHC_YMAX = 4, MHC_ZMAX = 5
+};
+
+/* limiter ids of the classical remap path (TypesMahyco.h:96-105) */
+enum mhc_limiter { MHC_MINMOD = 0, MHC_SUPERBEE = 1, MHC_VANLEER = 2 };
+
+/* case-initialisation services (<cas-model name="...">) */
+enum mhc_case_model {
+  MHC_CASE_SOD = 1,       /* casTest/SOD/SODService.cc */
+  MHC_CASE_SEDOV = 2,     /* casTest/SEDOV/SEDOVService.cc */
+  MHC_CASE_TWO_STATE = 3  /* explicit left/right states (seeded batch cases) */
+};
+
+/* cas-test ids used by SOD and SEDOV (TypesMahyco.h:44-94) */
+enum mhc_cas_test {
+  MHC_TEST_SEDOV = 1, MHC_TEST_SOD_X = 3, MHC_TEST_SOD_Y = 4, MHC_TEST_SOD_Z = 5,
+  MHC_TEST_BISEDOV = 11, MHC_TEST_BISOD_X = 13, MHC_TEST_BISOD_Y = 14, MHC_TEST_BISOD_Z = 15
+};
+
+/* longueur-caracteristique option values */
+enum mhc_char_length {
+  MHC_LENGTH_CUBE_ROOT_VOLUME = 0, /* "racine-cubique-volume" */
+  MHC_LENGTH_OPPOSITE_FACES = 1,   /* "faces-opposees" */
+  MHC_LENGTH_MONODIM_X = 2, MHC_LENGTH_MONODIM_Y = 3, MHC_LENGTH_MONODIM_Z = 4
+};
+
+/* is-euler-scheme option of RemapADI */
+enum mhc_euler_scheme { MHC_EULER_FULL = 0, MHC_EULER_NONE = 1 };
+
+typedef struct mhc_env_params {
+  int eos;                       /* mhc_eos_kind */
+  double adiabatic_cst;          /* adiabatic-cst (gamma) */
+  double limit_tension;          /* limit-tension (p_inf for StiffenedGas) */
+  double specific_heat;          /* specific-heat */
+  double tension_damage_thresold;
+  double density_damage_thresold;
+  /* Mie-Gruneisen parameters */
+  double rho0, s1, s2, s3, gamma0, a, c0, energie_ref, temperature_ref;
+  /* pseudo-viscosity coefficients */
+  double linear_pseudo_coeff, quadratic_pseudo_coeff;
+  /* initial state */
+  double densite_initiale, pression_initiale, energie_initiale, temperature_initiale;
+  double vitesse_initiale[3];
+} mhc_env_params;
+
+typedef struct mhc_bc {
+  int kind;     /* mhc_bc_kind */
+  int surface;  /* mhc_surface */
+  double value;
+  double tdebut, tfin;
+} mhc_bc;
+
+typedef struct mhc_case_params {
+  /* cartesian mesh generator */
+  int dim;                  /* 2 or 3 */
+  int nx, ny, nz;           /* cells per direction (nz ignored in 2D) */
+  double origin[3];
+  double lx, ly, lz;
+  /* environments */
+  int nb_env;
+  mhc_env_params env[MHC_MAX_ENV];
+  /* case model */
+  int cas_model;            /* mhc_case_model */
+  int cas_test;             /* mhc_cas_test */
+  double sedov_energy;      /* total energy deposited by SEDOV (reference: 0.244816) */
+  double interface_pos;     /* TWO_STATE: interface abscissa along interface_dir */
+  int interface_dir;        /* TWO_STATE: 0=x 1=y 2=z */
+  /* module options */
+  int with_projection;
+  int pseudo_centree;
+  int with_newton;
+  int pression_explicite;
+  int deltat_constant;
+  int calcul_vitson_max;
+  int longueur_caracteristique; /* mhc_char_length */
+  double cfl, deltat_init, deltat_min, deltat_max, final_time, threshold;
+  double gravity[3];
+  int nb_bc;
+  mhc_bc bc[MHC_MAX_BC];
+  /* RemapADI options */
+  int ordre_projection;
+  int projection_limiteur_id;
+  int is_euler_scheme;
+  double remap_threshold;
+  /* EnvSummation period */
+  int time_history_period;
+} mhc_case_params;
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,186 @@
+"""mahyco_b200 -- B200-native MaHyCo hydro cycle.
+
+The compute path is ``libmahyco_b200.so`` (hand-written sm_100a kernels
+behind the C ABI of ``include/mahyco_b200.h``).  This module is a thin
+ctypes binding that mirrors the reference module interface
+(``src/MahycoModule.h:164-349``): a :class:`Hydro` object exposes the
+init and compute-loop entry points under the reference names.  There is no
+CPU fallback: creating a case without the built library or without a CUDA
+device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .case import (CaseParams, EnvParams, add_bc, default_params, read_arc,  # noqa: F401
+                   symmetry_bcs, CASE_SOD, CASE_SEDOV, CASE_TWO_STATE,
+                   EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN,
+                   MINMOD, SUPERBEE, VANLEER)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmahyco_b200.so")
+
+ST_NEG_VOLUME, ST_DT_UNDERFLOW, ST_NAN, ST_STOP = 1, 2, 4, 8
+
+_lib = None
+
+# exported symbols and their (restype, argtypes)
+_SIGS = {
+    "mhc_last_error": (C.c_char_p, []),
+    "mhc_version": (C.c_char_p, []),
+    "mhc_case_create": (C.c_int, [C.POINTER(CaseParams), C.POINTER(C.c_void_p)]),
+    "mhc_case_destroy": (C.c_int, [C.c_void_p]),
+    "mhc_case_device_bytes": (C.c_longlong, [C.POINTER(CaseParams)]),
+    "mhc_hydro_start_init": (C.c_int, [C.c_void_p]),
+    "mhc_save_values_at_n": (C.c_int, [C.c_void_p]),
+    "mhc_update_velocity": (C.c_int, [C.c_void_p]),
+    "mhc_apply_boundary_condition": (C.c_int, [C.c_void_p]),
+    "mhc_update_position": (C.c_int, [C.c_void_p]),
+    "mhc_compute_geometric_values": (C.c_int, [C.c_void_p]),
+    "mhc_update_density": (C.c_int, [C.c_void_p]),
+    "mhc_compute_artificial_viscosity": (C.c_int, [C.c_void_p]),
+    "mhc_update_elasticity_and_plasticity": (C.c_int, [C.c_void_p]),
+    "mhc_update_energy_and_pressure": (C.c_int, [C.c_void_p]),
+    "mhc_remap": (C.c_int, [C.c_void_p]),
+    "mhc_compute_delta_t": (C.c_int, [C.c_void_p]),
+    "mhc_cycle": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_cycle_graph": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_synchronize": (C.c_int, [C.c_void_p]),
+    "mhc_get_scalars": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
+    "mhc_get_field": (C.c_longlong, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_longlong]),
+    "mhc_eos_apply": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_remap_apply": (C.c_int, [C.c_void_p]),
+    "mhc_time_history": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+}
+
+
+class MahycoError(RuntimeError):
+    pass
+
+
+def load(path: str | None = None) -> C.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise MahycoError(f"{p} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    lib = C.CDLL(p)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(lib, code: int, what: str) -> int:
+    if code < 0:
+        raise MahycoError(f"{what} failed ({code}): {lib.mhc_last_error().decode()}")
+    return code
+
+
+class Hydro:
+    """One MaHyCo case resident on the GPU (replaces the MahycoModule instance)."""
+
+    CELL_FIELDS = ("Density", "Pressure", "InternalEnergy", "SoundSpeed", "PseudoViscosity",
+                   "CellMass", "CellVolume", "FracVol", "MassFraction", "CaracteristicLength")
+
+    def __init__(self, params: CaseParams, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+        self.params = params
+        h = C.c_void_p()
+        _check(self.lib, self.lib.mhc_case_create(C.byref(params), C.byref(h)), "mhc_case_create")
+        self.h = h
+        self.ncell = params.ncell
+        self.nnode = params.nnode
+
+    def close(self):
+        if self.h:
+            self.lib.mhc_case_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- init entry points (Mahyco.config:15-21)
+    def hydroStartInit(self):
+        return _check(self.lib, self.lib.mhc_hydro_start_init(self.h), "HydroStartInit")
+
+    # -- compute-loop entry points (Mahyco.config:23-36)
+    def saveValuesAtN(self): return _check(self.lib, self.lib.mhc_save_values_at_n(self.h), "SaveValuesAtN")
+    def updateVelocity(self): return _check(self.lib, self.lib.mhc_update_velocity(self.h), "UpdateVelocity")
+    def applyBoundaryCondition(self): return _check(self.lib, self.lib.mhc_apply_boundary_condition(self.h), "ApplyBoundaryCondition")
+    def updatePosition(self): return _check(self.lib, self.lib.mhc_update_position(self.h), "UpdatePosition")
+    def computeGeometricValues(self): return _check(self.lib, self.lib.mhc_compute_geometric_values(self.h), "ComputeGeometricValues")
+    def updateDensity(self): return _check(self.lib, self.lib.mhc_update_density(self.h), "UpdateDensity")
+    def computeArtificialViscosity(self): return _check(self.lib, self.lib.mhc_compute_artificial_viscosity(self.h), "ComputeArtificialViscosity")
+    def updateElasticityAndPlasticity(self): return _check(self.lib, self.lib.mhc_update_elasticity_and_plasticity(self.h), "UpdateElasticityAndPlasticity")
+    def updateEnergyAndPressure(self): return _check(self.lib, self.lib.mhc_update_energy_and_pressure(self.h), "UpdateEnergyAndPressure")
+    def remap(self): return _check(self.lib, self.lib.mhc_remap(self.h), "Remap")
+    def computeDeltaT(self): return _check(self.lib, self.lib.mhc_compute_delta_t(self.h), "ComputeDeltaT")
+
+    def iterate(self):
+        """One compute-loop iteration through the individual entry points."""
+        for ep in (self.saveValuesAtN, self.updateVelocity, self.applyBoundaryCondition,
+                   self.updatePosition, self.computeGeometricValues, self.updateDensity,
+                   self.computeArtificialViscosity, self.updateElasticityAndPlasticity,
+                   self.updateEnergyAndPressure, self.remap, self.computeDeltaT):
+            ep()
+
+    def cycle(self, n: int, graph: bool = False) -> None:
+        f = self.lib.mhc_cycle_graph if graph else self.lib.mhc_cycle
+        _check(self.lib, f(self.h, int(n)), "mhc_cycle")
+
+    def synchronize(self) -> int:
+        return _check(self.lib, self.lib.mhc_synchronize(self.h), "mhc_synchronize")
+
+    def run(self, max_iter: int, chunk: int = 10) -> int:
+        """Iterate until the final time (stop flag), an error flag or max_iter."""
+        done = 0
+        while done < max_iter:
+            n = min(chunk, max_iter - done)
+            for _ in range(n):
+                self.cycle(1)
+                st = self.synchronize()
+                done += 1
+                if st:
+                    return st
+        return self.synchronize()
+
+    def scalars(self) -> dict:
+        t, dt, it, st = C.c_double(), C.c_double(), C.c_longlong(), C.c_int()
+        _check(self.lib, self.lib.mhc_get_scalars(self.h, C.byref(t), C.byref(dt), C.byref(it), C.byref(st)), "scalars")
+        return {"time": t.value, "deltat": dt.value, "iteration": it.value, "status": st.value}
+
+    def field(self, name: str, env: int = -1) -> np.ndarray:
+        n = 3 * self.nnode if name in ("Velocity", "NodeCoord") else (
+            self.nnode if name == "NodeMass" else self.ncell)
+        out = np.empty(n, dtype=np.float64)
+        got = self.lib.mhc_get_field(self.h, name.encode(), int(env),
+                                     out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        _check(self.lib, int(got), f"field {name}")
+        return out
+
+    def eos_apply(self, env: int) -> None:
+        _check(self.lib, self.lib.mhc_eos_apply(self.h, int(env)), "applyEOS")
+
+    def time_history(self) -> np.ndarray:
+        out = np.empty(1 + 5 * self.params.nb_env, dtype=np.float64)
+        _check(self.lib, self.lib.mhc_time_history(self.h, out.ctypes.data_as(C.POINTER(C.c_double))),
+               "time history")
+        return out

@@ -1,0 +1,270 @@
+"""Case description: ctypes mirror of ``include/mahyco_case.h`` and a reader
+for the subset of MaHyCo ``.arc`` datasets used by the hydro cycle.
+
+Option names and defaults follow the reference descriptors:
+``src/Mahyco.axl:263-557`` (module), ``src/Remap/RemapADI.axl:162-210``
+(remap), ``src/eos/*/*.axl`` (equations of state) and
+``src/time_history/EnvSummation.axl:27`` (time-history period).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import xml.etree.ElementTree as ET
+
+MAX_ENV = 4
+MAX_BC = 12
+
+EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN = 0, 1, 2
+EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
+               "MieGruneisen": EOS_MIE_GRUNEISEN}
+BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2}
+SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
+CASE_SOD, CASE_SEDOV, CASE_TWO_STATE = 1, 2, 3
+CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV}
+LENGTHS = {"racine-cubique-volume": 0, "faces-opposees": 1, "monodimX": 2,
+           "monodimY": 3, "monodimZ": 4}
+MINMOD, SUPERBEE, VANLEER = 0, 1, 2
+
+
+class EnvParams(C.Structure):
+    _fields_ = [
+        ("eos", C.c_int),
+        ("adiabatic_cst", C.c_double), ("limit_tension", C.c_double),
+        ("specific_heat", C.c_double), ("tension_damage_thresold", C.c_double),
+        ("density_damage_thresold", C.c_double),
+        ("rho0", C.c_double), ("s1", C.c_double), ("s2", C.c_double), ("s3", C.c_double),
+        ("gamma0", C.c_double), ("a", C.c_double), ("c0", C.c_double),
+        ("energie_ref", C.c_double), ("temperature_ref", C.c_double),
+        ("linear_pseudo_coeff", C.c_double), ("quadratic_pseudo_coeff", C.c_double),
+        ("densite_initiale", C.c_double), ("pression_initiale", C.c_double),
+        ("energie_initiale", C.c_double), ("temperature_initiale", C.c_double),
+        ("vitesse_initiale", C.c_double * 3),
+    ]
+
+
+class BC(C.Structure):
+    _fields_ = [("kind", C.c_int), ("surface", C.c_int), ("value", C.c_double),
+                ("tdebut", C.c_double), ("tfin", C.c_double)]
+
+
+class CaseParams(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("origin", C.c_double * 3), ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double),
+        ("nb_env", C.c_int), ("env", EnvParams * MAX_ENV),
+        ("cas_model", C.c_int), ("cas_test", C.c_int), ("sedov_energy", C.c_double),
+        ("interface_pos", C.c_double), ("interface_dir", C.c_int),
+        ("with_projection", C.c_int), ("pseudo_centree", C.c_int), ("with_newton", C.c_int),
+        ("pression_explicite", C.c_int), ("deltat_constant", C.c_int),
+        ("calcul_vitson_max", C.c_int), ("longueur_caracteristique", C.c_int),
+        ("cfl", C.c_double), ("deltat_init", C.c_double), ("deltat_min", C.c_double),
+        ("deltat_max", C.c_double), ("final_time", C.c_double), ("threshold", C.c_double),
+        ("gravity", C.c_double * 3),
+        ("nb_bc", C.c_int), ("bc", BC * MAX_BC),
+        ("ordre_projection", C.c_int), ("projection_limiteur_id", C.c_int),
+        ("is_euler_scheme", C.c_int), ("remap_threshold", C.c_double),
+        ("time_history_period", C.c_int),
+    ]
+
+    # -- convenience -------------------------------------------------------
+    @property
+    def ncell(self) -> int:
+        return self.nx * self.ny * (self.nz if self.dim == 3 else 1)
+
+    @property
+    def nnode(self) -> int:
+        return (self.nx + 1) * (self.ny + 1) * ((self.nz + 1) if self.dim == 3 else 1)
+
+
+def env_defaults(e: EnvParams, eos: int = EOS_PERFECT_GAS) -> None:
+    """Reference defaults of one ``<environment>`` block and its EOS service."""
+    e.eos = eos
+    e.adiabatic_cst = 1.4
+    e.limit_tension = 0.01 if eos == EOS_STIFFENED_GAS else 0.0
+    e.specific_heat = 921.0 if eos == EOS_MIE_GRUNEISEN else 0.0
+    e.tension_damage_thresold = -1.0e12
+    e.density_damage_thresold = 0.0
+    e.rho0, e.s1, e.s2, e.s3 = 0.0, 1.4, 0.0, 0.0
+    e.gamma0, e.a, e.c0 = 1.97, 0.48, 5240.0
+    e.energie_ref, e.temperature_ref = 0.0, 300.0
+    e.linear_pseudo_coeff, e.quadratic_pseudo_coeff = 0.5, 1.2
+    e.densite_initiale, e.pression_initiale = 0.0, 1.0e5
+    e.energie_initiale, e.temperature_initiale = 0.0, 0.0
+    e.vitesse_initiale[:] = (0.0, 0.0, 0.0)
+
+
+def default_params() -> CaseParams:
+    """A CaseParams filled with the reference option defaults."""
+    p = CaseParams()
+    p.dim, p.nx, p.ny, p.nz = 3, 1, 1, 1
+    p.origin[:] = (0.0, 0.0, 0.0)
+    p.lx = p.ly = p.lz = 1.0
+    p.nb_env = 1
+    for i in range(MAX_ENV):
+        env_defaults(p.env[i])
+    p.cas_model, p.cas_test = CASE_SOD, 3
+    p.sedov_energy = 0.244816
+    p.interface_pos, p.interface_dir = 0.5, 0
+    p.with_projection = 1
+    p.pseudo_centree = 0
+    p.with_newton = 0
+    p.pression_explicite = 0
+    p.deltat_constant = 0
+    p.calcul_vitson_max = 1
+    p.longueur_caracteristique = 0
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.3, 1.0e-5, 1.0e-8, 1.0e-2
+    p.final_time = 1.0e30
+    p.threshold = 1.0e-10
+    p.gravity[:] = (0.0, 0.0, 0.0)
+    p.nb_bc = 0
+    p.ordre_projection = 2
+    p.projection_limiteur_id = MINMOD
+    p.is_euler_scheme = 0
+    p.remap_threshold = 1.0e-10
+    p.time_history_period = 10
+    return p
+
+
+def add_bc(p: CaseParams, surface: str, kind: str, value: float = 0.0,
+           tdebut: float = 0.0, tfin: float = 1000.0) -> None:
+    if p.nb_bc >= MAX_BC:
+        raise ValueError("too many boundary conditions")
+    b = p.bc[p.nb_bc]
+    b.kind, b.surface, b.value, b.tdebut, b.tfin = BC_BY_NAME[kind], SURFACES[surface], value, tdebut, tfin
+    p.nb_bc += 1
+
+
+def symmetry_bcs(p: CaseParams, surfaces=("XMIN", "XMAX", "YMIN", "YMAX", "ZMIN", "ZMAX")) -> None:
+    """Zero normal velocity on the given faces, as the reference datasets set it."""
+    for s in surfaces:
+        add_bc(p, s, {"X": "Vx", "Y": "Vy", "Z": "Vz"}[s[0]], 0.0)
+
+
+# ---------------------------------------------------------------------------
+# .arc reader
+# ---------------------------------------------------------------------------
+def _txt(node, tag, default=None, conv=float):
+    el = node.find(tag)
+    if el is None or el.text is None or not el.text.strip():
+        return default
+    return conv(el.text.strip())
+
+
+def _bool(s: str) -> bool:
+    return s.strip().lower() in ("1", "true", "yes")
+
+
+def read_arc(path: str) -> tuple[CaseParams, dict]:
+    """Parse a MaHyCo ``Donnees.arc`` into CaseParams.
+
+    Returns ``(params, info)`` where ``info`` holds environment names, the
+    time loop and anything the hot path ignores.  Unsupported options that
+    change the cycle (CSTS scheme, pente-borne remap, elasto models, energy
+    deposits, non-velocity boundary conditions) raise ``NotImplementedError``.
+    """
+    root = ET.parse(path).getroot()
+    p = default_params()
+    info: dict = {"env_names": [], "timeloop": None}
+    tl = root.find("arcane/timeloop")
+    info["timeloop"] = tl.text.strip() if tl is not None else "MahycoLoop"
+    cart = root.find("mesh/meshgenerator/cartesian")
+    if cart is None:
+        raise NotImplementedError("only the cartesian mesh generator is supported")
+    org = [float(v) for v in cart.find("origine").text.split()]
+    p.origin[:] = (org + [0.0, 0.0, 0.0])[:3]
+    lx, ly, lz = cart.find("lx"), cart.find("ly"), cart.find("lz")
+    p.lx, p.nx = float(lx.text), int(lx.get("nx"))
+    p.ly, p.ny = float(ly.text), int(ly.get("ny"))
+    if lz is not None:
+        p.dim, p.lz, p.nz = 3, float(lz.text), int(lz.get("nz"))
+    else:
+        p.dim, p.lz, p.nz = 2, 0.0, 1
+    for el, n in ((lx, "prx"), (ly, "pry"), (lz, "prz")):
+        if el is not None and float(el.get(n, "1.0")) != 1.0:
+            raise NotImplementedError("non-uniform cartesian progression")
+    m = root.find("mahyco")
+    envs = m.findall("environment")
+    if not 1 <= len(envs) <= MAX_ENV:
+        raise NotImplementedError("1..4 environments supported")
+    p.nb_env = len(envs)
+    for i, ev in enumerate(envs):
+        info["env_names"].append(ev.find("name").text.strip())
+        eosel = ev.find("eos-model")
+        kind = EOS_BY_NAME[eosel.get("name")]
+        e = p.env[i]
+        env_defaults(e, kind)
+        e.densite_initiale = _txt(ev, "densite-initiale", 0.0)
+        e.pression_initiale = _txt(ev, "pression-initiale", 1.0e5)
+        e.energie_initiale = _txt(ev, "energie-initiale", 0.0)
+        e.temperature_initiale = _txt(ev, "temperature-initiale", 0.0)
+        vi = ev.find("vitesse-initiale")
+        if vi is not None:
+            e.vitesse_initiale[:] = [float(v) for v in vi.text.split()]
+        e.linear_pseudo_coeff = _txt(ev, "linear-pseudo-coeff", 0.5)
+        e.quadratic_pseudo_coeff = _txt(ev, "quadratic-pseudo-coeff", 1.2)
+        for tag, attr in (("adiabatic-cst", "adiabatic_cst"), ("limit-tension", "limit_tension"),
+                          ("specific-heat", "specific_heat"), ("rho0", "rho0"), ("s1", "s1"),
+                          ("s2", "s2"), ("s3", "s3"), ("gamma0", "gamma0"), ("a", "a"), ("c0", "c0"),
+                          ("energie-ref", "energie_ref"), ("temperature-ref", "temperature_ref"),
+                          ("tension-damage-thresold", "tension_damage_thresold"),
+                          ("density-damage-thresold", "density_damage_thresold")):
+            v = _txt(eosel, tag, None)
+            if v is not None:
+                setattr(e, attr, v)
+        el = ev.find("elasto-model")
+        if el is not None and el.get("name") not in (None, "NoModel"):
+            raise NotImplementedError("elasto-plastic models")
+        if ev.find("energy-depot") is not None:
+            raise NotImplementedError("energy deposit")
+    cm = m.find("cas-model")
+    p.cas_model = CASE_BY_NAME[cm.get("name")]
+    p.cas_test = _txt(cm, "cas-test", 0, int)
+    rm = m.find("remap")
+    if rm is not None:
+        if rm.get("name", "RemapADI") != "RemapADI":
+            raise NotImplementedError("only the RemapADI service")
+        p.ordre_projection = _txt(rm, "ordre-projection", 2, int)
+        p.projection_limiteur_id = _txt(rm, "projection-limiteur-id", 0, int)
+        p.remap_threshold = _txt(rm, "threshold", 1.0e-10)
+        eul = _txt(rm, "is-euler-scheme", "Full", str)
+        if eul != "Full":
+            raise NotImplementedError("is-euler-scheme other than Full")
+        for flag in ("projection-pente-borne", "projection-simple-pente", "conservation-energie-totale"):
+            if _txt(rm, flag, False, _bool):
+                raise NotImplementedError(flag)
+        if p.ordre_projection not in (1, 2) or p.projection_limiteur_id not in (0, 1, 2):
+            raise NotImplementedError("remap order 3 / generalised limiters")
+    if _txt(m, "schema-csts", False, _bool):
+        raise NotImplementedError("schema-csts")
+    if _txt(m, "sans-lagrange", False, _bool):
+        raise NotImplementedError("sans-lagrange")
+    p.pseudo_centree = int(_txt(m, "pseudo-centree", False, _bool))
+    p.with_projection = int(_txt(m, "with-projection", True, _bool))
+    if info["timeloop"] == "MahycoLagrangeLoop":
+        p.with_projection = 0
+    p.with_newton = int(_txt(m, "with-newton", False, _bool))
+    p.pression_explicite = int(_txt(m, "pression-explicite", False, _bool))
+    p.deltat_constant = int(_txt(m, "deltat-constant", False, _bool))
+    p.calcul_vitson_max = int(_txt(m, "calcul-vitson-max", True, _bool))
+    p.longueur_caracteristique = LENGTHS[_txt(m, "longueur-caracteristique", "racine-cubique-volume", str)]
+    p.cfl = _txt(m, "cfl", 0.3)
+    p.deltat_init = _txt(m, "deltat-init", 1.0e-5)
+    p.deltat_min = _txt(m, "deltat-min", 1.0e-8)
+    p.deltat_max = _txt(m, "deltat-max", 1.0e-2)
+    p.final_time = _txt(m, "final-time", 1.0)
+    p.threshold = _txt(m, "threshold", 1.0e-10)
+    g = m.find("gravity")
+    if g is not None:
+        p.gravity[:] = [float(v) for v in g.text.split()]
+    if _txt(m, "coef-antiderive", 0.0) != 0.0:
+        raise NotImplementedError("coef-antiderive")
+    for b in m.findall("boundary-condition"):
+        kind = b.find("type").text.strip()
+        if kind not in BC_BY_NAME:
+            raise NotImplementedError(f"boundary condition {kind}")
+        add_bc(p, b.find("surface").text.strip(), kind, _txt(b, "value", 0.0),
+               _txt(b, "Tdebut", 0.0), _txt(b, "Tfin", 1000.0))
+    th = root.find("time-history/bilan")
+    if th is not None:
+        p.time_history_period = _txt(th, "periode", 10, int)
+    return p, info

@@ -1,0 +1,185 @@
+"""Case builders for the workloads the library is measured and tested on.
+
+Each builder returns a :class:`CaseParams` for the cartesian meshes of the
+reference datasets (``NONREGRESSION/CAS_*``) at any size:
+
+* ``sod``        -- SOD service, mono (cas-test 3/4/5) or bi-material (13/14/15)
+* ``sedov``      -- SEDOV service (cas-test 1), energy deposited in the origin cell
+* ``two_state``  -- seeded generalisation of BiSod with explicit left/right
+  states and interface position (the batched workload)
+* ``water_air``  -- stiffened-gas / perfect-gas two-material shock tube
+* ``mie_gruneisen_plate`` -- two Mie-Gruneisen states, explicit pressure
+"""
+from __future__ import annotations
+
+import math
+import random
+
+from .case import (CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, EOS_MIE_GRUNEISEN, EOS_PERFECT_GAS,
+                   EOS_STIFFENED_GAS, MINMOD, SUPERBEE, VANLEER, CaseParams, default_params,
+                   env_defaults, symmetry_bcs)
+
+
+def _mesh(p: CaseParams, dim: int, n, L) -> None:
+    p.dim = dim
+    p.nx, p.ny = n[0], n[1]
+    p.lx, p.ly = L[0], L[1]
+    if dim == 3:
+        p.nz, p.lz = n[2], L[2]
+    else:
+        p.nz, p.lz = 1, 0.0
+
+
+def sod(dim=3, n=(100, 5, 5), L=(1.0, 0.1, 0.1), bi=True, axis=0, remap=True,
+        limiter=MINMOD, order=2, cfl=0.3, deltat_max=0.01, final_time=1e30,
+        deltat_init=1e-5) -> CaseParams:
+    """CAS_(2D_)(Lag_)(Bi)SodCase{X,Y,Z}: (rho,p) = (1,1) | (0.125,0.1), gamma 1.4."""
+    p = default_params()
+    _mesh(p, dim, n, L)
+    p.nb_env = 2
+    for e in range(2):
+        env_defaults(p.env[e], EOS_PERFECT_GAS)
+        p.env[e].specific_heat = 2.4
+    p.env[0].densite_initiale, p.env[0].pression_initiale = 1.0, 1.0
+    p.env[1].densite_initiale, p.env[1].pression_initiale = 0.125, 0.1
+    p.cas_model = CASE_SOD
+    p.cas_test = (13 if bi else 3) + axis
+    p.with_projection = 1 if remap else 0
+    p.projection_limiteur_id, p.ordre_projection = limiter, order
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = cfl, deltat_init, 1e-8, deltat_max
+    p.final_time = final_time
+    symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
+    return p
+
+
+def sedov(dim=3, n=(60, 60, 60), L=1.2, limiter=MINMOD, energy=0.244816, p0=0.0979264e-5,
+          final_time=1e30, deltat_init=1e-5) -> CaseParams:
+    """CAS_Sedov / CAS_2D_Sedov: rho = 1, symmetry planes at 0, energy in the origin cell."""
+    p = default_params()
+    nn = (n[0], n[1], n[2] if dim == 3 else 1)
+    _mesh(p, dim, nn, (L, L, L))
+    p.nb_env = 2
+    env_defaults(p.env[0], EOS_PERFECT_GAS)
+    env_defaults(p.env[1], EOS_PERFECT_GAS)
+    p.env[0].specific_heat = p.env[1].specific_heat = 2.4
+    p.env[0].densite_initiale, p.env[0].pression_initiale = 1.0, p0
+    p.env[1].densite_initiale, p.env[1].pression_initiale = 1.0, 1.0
+    p.cas_model, p.cas_test = CASE_SEDOV, 1
+    p.sedov_energy = energy
+    p.projection_limiteur_id = limiter
+    p.deltat_init, p.deltat_min, p.deltat_max = deltat_init, 1e-8, 1e-2
+    p.final_time = final_time
+    symmetry_bcs(p, ("XMIN", "YMIN") + (("ZMIN",) if dim == 3 else ()))
+    return p
+
+
+def two_state(dim=2, n=(64, 64), L=(1.0, 1.0), left=(1.0, 1.0), right=(0.125, 0.1),
+              gamma=1.4, interface=0.5, axis=0, nb_env=2, limiter=VANLEER, final_time=1e30,
+              deltat_init=1e-5) -> CaseParams:
+    """Seeded Sod / BiSod family: explicit (rho, p) on each side of an interface."""
+    p = default_params()
+    _mesh(p, dim, n, L)
+    p.nb_env = nb_env
+    for e in range(2):
+        env_defaults(p.env[e], EOS_PERFECT_GAS)
+        p.env[e].adiabatic_cst = gamma
+    p.env[0].densite_initiale, p.env[0].pression_initiale = left
+    p.env[1].densite_initiale, p.env[1].pression_initiale = right
+    p.cas_model = CASE_TWO_STATE
+    p.interface_pos, p.interface_dir = interface, axis
+    p.projection_limiteur_id = limiter
+    p.deltat_init, p.deltat_min, p.deltat_max = deltat_init, 1e-12, 1e-2
+    p.final_time = final_time
+    symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
+    return p
+
+
+def seeded_two_state(seed: int, n: int, dim: int = 2) -> CaseParams:
+    """One case of the batched workload: left rho,p ~ U[0.5,2], right rho,p ~
+    U[0.05,0.3], gamma in {1.4, 5/3}, interface ~ U[0.3,0.7], vanleer."""
+    rng = random.Random(seed)
+    left = (rng.uniform(0.5, 2.0), rng.uniform(0.5, 2.0))
+    right = (rng.uniform(0.05, 0.3), rng.uniform(0.05, 0.3))
+    gamma = rng.choice((1.4, 5.0 / 3.0))
+    x = rng.uniform(0.3, 0.7)
+    bi = rng.random() < 0.5
+    return two_state(dim=dim, n=(n, n) if dim == 2 else (n, n, n), L=(1.0, 1.0, 1.0)[:dim] if dim == 3 else (1.0, 1.0),
+                     left=left, right=right, gamma=gamma, interface=x, nb_env=2 if bi else 1,
+                     limiter=VANLEER)
+
+
+def log_uniform_sides(count: int, lo: int = 32, hi: int = 512, seed: int = 0) -> list[int]:
+    rng = random.Random(seed)
+    return [int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))))) for _ in range(count)]
+
+
+def water_air(dim=2, n=(80, 8), L=(1.0, 0.1), limiter=SUPERBEE, remap=True, deltat_init=1e-8) -> CaseParams:
+    """Stiffened-gas water (gamma 4.4, p_inf 6e8, rho 1000) against perfect-gas air
+    (gamma 1.4, rho 1): density ratio 1000:1, pressure ratio 1e4:1."""
+    p = default_params()
+    _mesh(p, dim, n, L)
+    p.nb_env = 2
+    env_defaults(p.env[0], EOS_STIFFENED_GAS)
+    env_defaults(p.env[1], EOS_PERFECT_GAS)
+    p.env[0].adiabatic_cst, p.env[0].limit_tension = 4.4, 6.0e8
+    p.env[0].densite_initiale, p.env[0].pression_initiale = 1000.0, 1.0e9
+    p.env[1].adiabatic_cst = 1.4
+    p.env[1].densite_initiale, p.env[1].pression_initiale = 1.0, 1.0e5
+    p.cas_model = CASE_TWO_STATE
+    p.interface_pos, p.interface_dir = 0.5, 0
+    p.with_projection = 1 if remap else 0
+    p.projection_limiteur_id = limiter
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.3, deltat_init, 1e-14, 1e-4
+    symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
+    return p
+
+
+def mie_gruneisen_plate(dim=2, n=(80, 8), L=(0.01, 0.001), remap=False, deltat_init=1e-10) -> CaseParams:
+    """Aluminium-like Mie-Gruneisen material (rho0 2710, c0 5328, s1 1.338,
+    Gamma0 2.0) compressed on one side; explicit pressure update as in
+    CAS_2D_Lag_Taylor_elasto."""
+    p = default_params()
+    _mesh(p, dim, n, L)
+    p.nb_env = 2
+    for e in range(2):
+        env_defaults(p.env[e], EOS_MIE_GRUNEISEN)
+        o = p.env[e]
+        o.rho0, o.c0, o.s1, o.gamma0 = 2710.0, 5328.0, 1.338, 2.0
+    p.env[0].densite_initiale, p.env[0].pression_initiale = 2800.0, 2.0e9
+    p.env[1].densite_initiale, p.env[1].pression_initiale = 2710.0, 1.0e5
+    p.cas_model = CASE_TWO_STATE
+    p.interface_pos, p.interface_dir = 0.5 * L[0], 0
+    p.pression_explicite = 1
+    p.with_projection = 1 if remap else 0
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.3, deltat_init, 1e-16, 1e-6
+    symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
+    return p
+
+
+# small parity cases: name -> (builder, cycles).  Initial time steps are
+# large enough that the CFL bound, shocks and mixed cells are exercised.
+PARITY_CASES = {
+    "lag2d_sod_mono": (lambda: sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=False, remap=False,
+                                   deltat_max=1e-3, deltat_init=1e-4), 150),
+    "lag3d_bisod": (lambda: sod(dim=3, n=(30, 4, 4), L=(1.0, 0.1, 0.1), bi=True, remap=False,
+                                deltat_max=1e-3, deltat_init=1e-4), 120),
+    "adi3d_bisod_superbee": (lambda: sod(dim=3, n=(32, 6, 6), L=(1.0, 0.25, 0.25), bi=True,
+                                         limiter=SUPERBEE, deltat_init=1e-3), 80),
+    "adi3d_sod_mono_y": (lambda: sod(dim=3, n=(5, 30, 5), L=(0.1, 1.0, 0.1), bi=False, axis=1,
+                                     deltat_init=1e-3), 60),
+    "adi3d_bisod_z_vanleer": (lambda: sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
+                                          limiter=VANLEER, deltat_init=1e-3), 60),
+    "adi2d_sedov": (lambda: sedov(dim=2, n=(24, 24), deltat_init=1e-4), 120),
+    "adi3d_sedov": (lambda: sedov(dim=3, n=(12, 12, 12), deltat_init=1e-4), 40),
+    "adi2d_two_state_vanleer": (lambda: two_state(dim=2, n=(40, 30), left=(1.7, 1.3), right=(0.2, 0.07),
+                                                  gamma=5.0 / 3.0, interface=0.37, deltat_init=1e-3), 100),
+    "adi2d_bisod_order1": (lambda: _order1(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True,
+                                               deltat_init=1e-3)), 80),
+    "adi2d_water_air": (lambda: water_air(deltat_init=1e-6), 80),
+    "lag2d_mie_gruneisen": (lambda: mie_gruneisen_plate(deltat_init=1e-8), 100),
+}
+
+
+def _order1(p: CaseParams) -> CaseParams:
+    p.ordre_projection = 1
+    return p

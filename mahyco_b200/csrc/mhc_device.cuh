@@ -1,0 +1,198 @@
+// mhc_device.cuh -- device-side arithmetic shared by every MaHyCo kernel.
+//
+// All kernels are compiled with --fmad=false: every expression below rounds
+// exactly like the reference's x86-64 build (no contraction), so results can
+// be compared with the CPU oracle operation by operation.  Vector operations
+// follow Arcane's Real3 helpers (component-wise, left-to-right sums).
+#pragma once
+#include <cstdint>
+#include <cmath>
+
+namespace mhc {
+
+struct R3 {
+  double x, y, z;
+};
+__device__ __forceinline__ R3 operator+(R3 a, R3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ R3 operator-(R3 a, R3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ R3 operator*(double s, R3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ R3 operator*(R3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ R3 operator/(R3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ double dot(R3 a, R3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// math::vecMul
+__device__ __forceinline__ R3 vecmul(R3 u, R3 v) {
+  return {u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
+}
+__device__ __forceinline__ double norm(R3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ double comp(R3 a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
+// MahycoModule::produit
+__device__ __forceinline__ double produit(double A, double B, double C, double D) { return A * B - C * D; }
+// Arcane math::min / math::max
+__device__ __forceinline__ double amin(double a, double b) { return (a < b) ? a : b; }
+__device__ __forceinline__ double amax(double a, double b) { return (a < b) ? b : a; }
+// std::min / std::max
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+// ---------------------------------------------------------------------------
+// correctly rounded powers
+// ---------------------------------------------------------------------------
+// Error-free product a*b = p + e (Dekker/Ogita-Rump-Oishi TwoProduct, using
+// the fused multiply-add as the exact remainder).
+__device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
+  p = a * b;
+  e = fma(a, b, -p);
+}
+
+// x^3 rounded once: the exact cube is the sum of four doubles.
+__device__ __forceinline__ double cube_rn(double x) {
+  double s, sl, t, tl, u, ul;
+  two_prod(x, x, s, sl);
+  two_prod(s, x, t, tl);
+  two_prod(sl, x, u, ul);
+  return t + (tl + (u + ul));
+}
+
+// x^y for y = the double nearest to 1/3 (the reference writes pow(V, 1./3.)).
+// With y = 1/3 - d, d = 2^-54/3 exactly, x^y = cbrt(x) * exp(-d ln x).
+// cbrt(x) is refined to double-double by one Newton step on r^3 = x with an
+// exact residual, the tiny factor exp(-d ln x) ~ 1 - d ln x is applied to
+// first order (the second-order term is below 2^-100), and the double-double
+// is rounded once.  The result is the correctly rounded x^y except when x^y
+// lies within ~2^-90 relative of a rounding boundary.
+__device__ __forceinline__ double pow_one_third(double x) {
+  if (!(x > 0.0) || isinf(x)) return pow(x, 1. / 3.);
+  double r = cbrt(x);
+  double s, sl, t, tl;
+  two_prod(r, r, s, sl);
+  two_prod(s, r, t, tl);
+  double res = ((x - t) - tl) - sl * r;   // x - r^3, exact to ~2^-106 relative
+  double c_lo = res / (3.0 * s);         // cbrt(x) = r + c_lo
+  const double d = (1.0 / 3.0) * 0x1p-54; // 1/3 - double(1/3)
+  double corr = c_lo - r * (d * log(x));
+  return r + corr;
+}
+
+// ---------------------------------------------------------------------------
+// structured mesh indexing (Arcane cartesian generator numbering)
+// ---------------------------------------------------------------------------
+struct Mesh {
+  int dim;
+  int ncx, ncy, ncz;   // cells per direction (ncz = 1 in 2D)
+  int nnx, nny, nnz;   // nodes per direction (nnz = 1 in 2D)
+  long long ncell, nnode;
+  double o[3];         // origin
+  double h[3];         // L/n per direction
+};
+
+__device__ __forceinline__ long long cell_id(const Mesh& M, int i, int j, int k) {
+  return i + (long long)M.ncx * (j + (long long)M.ncy * k);
+}
+__device__ __forceinline__ long long node_id(const Mesh& M, int i, int j, int k) {
+  return i + (long long)M.nnx * (j + (long long)M.nny * k);
+}
+__device__ __forceinline__ void cell_ijk(const Mesh& M, long long c, int& i, int& j, int& k) {
+  i = (int)(c % M.ncx);
+  long long r = c / M.ncx;
+  j = (int)(r % M.ncy);
+  k = (int)(r / M.ncy);
+}
+__device__ __forceinline__ void node_ijk(const Mesh& M, long long n, int& i, int& j, int& k) {
+  i = (int)(n % M.nnx);
+  long long r = n / M.nnx;
+  j = (int)(r % M.nny);
+  k = (int)(r / M.nny);
+}
+// initial (Euler) node position: origin + i*(L/n)
+__device__ __forceinline__ R3 node_x0(const Mesh& M, int i, int j, int k) {
+  return {M.o[0] + i * M.h[0], M.o[1] + j * M.h[1], M.dim == 3 ? M.o[2] + k * M.h[2] : 0.};
+}
+
+// Hexa8 / Quad4 local node offsets
+__device__ __forceinline__ void local_node_offset(int l, int& di, int& dj, int& dk) {
+  di = (l == 1 || l == 2 || l == 5 || l == 6) ? 1 : 0;
+  dj = (l == 2 || l == 3 || l == 6 || l == 7) ? 1 : 0;
+  dk = (l >= 4) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// corner normals
+// ---------------------------------------------------------------------------
+// face centres of a hexahedron (MahycoModule.cc:1117-1122)
+__device__ __forceinline__ void hex_face_centres(const R3* coord, R3* fc) {
+  fc[0] = 0.25 * (coord[0] + coord[3] + coord[2] + coord[1]);
+  fc[1] = 0.25 * (coord[0] + coord[4] + coord[7] + coord[3]);
+  fc[2] = 0.25 * (coord[0] + coord[1] + coord[5] + coord[4]);
+  fc[3] = 0.25 * (coord[4] + coord[5] + coord[6] + coord[7]);
+  fc[4] = 0.25 * (coord[1] + coord[2] + coord[6] + coord[5]);
+  fc[5] = 0.25 * (coord[2] + coord[3] + coord[7] + coord[6]);
+}
+
+// MahycoModule::computeCQs (MahycoModule.cc:1869-1932)
+__device__ __forceinline__ void cqs3(const R3* nc, const R3* fc, R3* out) {
+  const R3 c0 = fc[0], c1 = fc[1], c2 = fc[2], c3 = fc[3], c4 = fc[4], c5 = fc[5];
+  const R3 n1a04 = 0.5 * vecmul(nc[0] - c0, nc[3] - c0);
+  const R3 n1a03 = 0.5 * vecmul(nc[3] - c0, nc[2] - c0);
+  const R3 n1a02 = 0.5 * vecmul(nc[2] - c0, nc[1] - c0);
+  const R3 n1a01 = 0.5 * vecmul(nc[1] - c0, nc[0] - c0);
+  const R3 n2a05 = 0.5 * vecmul(nc[0] - c1, nc[4] - c1);
+  const R3 n2a12 = 0.5 * vecmul(nc[4] - c1, nc[7] - c1);
+  const R3 n2a08 = 0.5 * vecmul(nc[7] - c1, nc[3] - c1);
+  const R3 n2a04 = 0.5 * vecmul(nc[3] - c1, nc[0] - c1);
+  const R3 n3a01 = 0.5 * vecmul(nc[0] - c2, nc[1] - c2);
+  const R3 n3a06 = 0.5 * vecmul(nc[1] - c2, nc[5] - c2);
+  const R3 n3a09 = 0.5 * vecmul(nc[5] - c2, nc[4] - c2);
+  const R3 n3a05 = 0.5 * vecmul(nc[4] - c2, nc[0] - c2);
+  const R3 n4a09 = 0.5 * vecmul(nc[4] - c3, nc[5] - c3);
+  const R3 n4a10 = 0.5 * vecmul(nc[5] - c3, nc[6] - c3);
+  const R3 n4a11 = 0.5 * vecmul(nc[6] - c3, nc[7] - c3);
+  const R3 n4a12 = 0.5 * vecmul(nc[7] - c3, nc[4] - c3);
+  const R3 n5a02 = 0.5 * vecmul(nc[1] - c4, nc[2] - c4);
+  const R3 n5a07 = 0.5 * vecmul(nc[2] - c4, nc[6] - c4);
+  const R3 n5a10 = 0.5 * vecmul(nc[6] - c4, nc[5] - c4);
+  const R3 n5a06 = 0.5 * vecmul(nc[5] - c4, nc[1] - c4);
+  const R3 n6a03 = 0.5 * vecmul(nc[2] - c5, nc[3] - c5);
+  const R3 n6a08 = 0.5 * vecmul(nc[3] - c5, nc[7] - c5);
+  const R3 n6a11 = 0.5 * vecmul(nc[7] - c5, nc[6] - c5);
+  const R3 n6a07 = 0.5 * vecmul(nc[6] - c5, nc[2] - c5);
+  const double t = 1. / 12.;
+  out[0] = (5. * (n1a01 + n1a04 + n2a04 + n2a05 + n3a05 + n3a01) + (n1a02 + n1a03 + n2a08 + n2a12 + n3a06 + n3a09)) * t;
+  out[1] = (5. * (n1a01 + n1a02 + n3a01 + n3a06 + n5a06 + n5a02) + (n1a04 + n1a03 + n3a09 + n3a05 + n5a10 + n5a07)) * t;
+  out[2] = (5. * (n1a02 + n1a03 + n5a07 + n5a02 + n6a07 + n6a03) + (n1a01 + n1a04 + n5a06 + n5a10 + n6a11 + n6a08)) * t;
+  out[3] = (5. * (n1a03 + n1a04 + n2a08 + n2a04 + n6a08 + n6a03) + (n1a01 + n1a02 + n2a05 + n2a12 + n6a07 + n6a11)) * t;
+  out[4] = (5. * (n2a05 + n2a12 + n3a05 + n3a09 + n4a09 + n4a12) + (n2a08 + n2a04 + n3a01 + n3a06 + n4a10 + n4a11)) * t;
+  out[5] = (5. * (n3a06 + n3a09 + n4a09 + n4a10 + n5a10 + n5a06) + (n3a01 + n3a05 + n4a12 + n4a11 + n5a07 + n5a02)) * t;
+  out[6] = (5. * (n4a11 + n4a10 + n5a10 + n5a07 + n6a07 + n6a11) + (n4a12 + n4a09 + n5a06 + n5a02 + n6a03 + n6a08)) * t;
+  out[7] = (5. * (n2a08 + n2a12 + n4a12 + n4a11 + n6a11 + n6a08) + (n2a04 + n2a05 + n4a09 + n4a10 + n6a07 + n6a03)) * t;
+}
+
+// 2D corner normals (MahycoModule.cc:1128-1146)
+__device__ __forceinline__ void cqs2(const R3* c4, R3* out) {
+  R3 coord[5] = {c4[0], c4[1], c4[2], c4[3], c4[0]};
+  R3 npc[5];
+  for (int n = 0; n < 5; ++n) npc[n] = {0., 0., 0.};
+  for (int n = 0; n < 4; ++n) {
+    npc[n + 1].x = 0.5 * (coord[n + 1].y - coord[n].y);
+    npc[n + 1].y = 0.5 * (coord[n].x - coord[n + 1].x);
+  }
+  npc[0] = npc[4];
+  for (int ii = 0; ii < 4; ++ii) out[ii] = npc[ii + 1] + npc[ii];
+}
+
+// ---------------------------------------------------------------------------
+// remap limiters (UtilesRemap.cc:108-120, 329-345)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double flux_limiter(int id, double r) {
+  if (id == 0) return smax(0.0, smin(1.0, r));
+  if (id == 1) return smax(0.0, smax(smin(2.0 * r, 1.0), smin(r, 2.0)));
+  if (id == 2) return (r <= 0.0) ? 0.0 : 2.0 * r / (1.0 + r);
+  return 0.0;
+}
+__device__ __forceinline__ double limited_gradient(int id, double gb, double gf) {
+  double g = 0.;
+  if (gb != 0.) g += 0.5 * (flux_limiter(id, gf / gb) * gb);
+  if (gf != 0.) g += 0.5 * (flux_limiter(id, gb / gf) * gf);
+  return g;
+}
+
+}  // namespace mhc

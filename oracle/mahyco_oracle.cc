@@ -1,0 +1,1503 @@
+/*
+ * mahyco_oracle.cc -- CPU ORACLE for the MaHyCo hydro cycle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file restates, in plain sequential C++, the
+ * reference algorithm of the cycle hot path so that the CUDA library can be
+ * checked against it.  Only tests/, __graft_entry__.smoke() and the CPU
+ * baseline leg of bench.py load it; the product library never links it.
+ *
+ * Parity pinning: the oracle is checked against the reference's own
+ * non-regression time histories (the NONREGRESSION case folders, output/courbes/gnuplot,
+ * copied as fixtures under tests/golden/ by tests/golden/make_golden.py).
+ *
+ * The reference (cea-hpc/MaHyCo) builds only on top of the Arcane framework,
+ * which is not vendored, so the reference itself cannot be compiled here.
+ * Arcane semantics that the reference relies on are restated as follows:
+ *   - cartesian generator: node (i,j,k) at origin + i*(L/n), uid x-fastest;
+ *     cells x-fastest; Hexa8 local nodes (0,0,0),(1,0,0),(1,1,0),(0,1,0),
+ *     then the same at k+1; Quad4 likewise without k.
+ *   - Hexa8 local faces (0,3,2,1),(0,4,7,3),(0,1,5,4),(4,5,6,7),(1,2,6,5),
+ *     (2,3,7,6); Quad4 local faces (k,k+1).  Face nodes are re-ordered to
+ *     start at the smallest uid and continue towards the smaller neighbour.
+ *   - faces and nodes are numbered in creation order (cell by cell), so every
+ *     scatter of the reference sums in ascending cell / face local id.
+ *   - material variables: a cell holding exactly one environment stores the
+ *     environment value in the global slot (EV() below models that aliasing).
+ *   - time loop: global_time += deltat before the compute-loop entry points;
+ *     old deltat of the first iteration is 0.
+ *
+ * Quantities the reference projects but never feeds back into the hydro
+ * state without an elasto-plastic model (phase fractions, stress deviator,
+ * plastic strain, previous energy, temperature) are not carried: the remap
+ * keeps volume, mass and energy per environment plus the pseudo-viscosity.
+ */
+#include "../include/mahyco_case.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace ora {
+
+struct R3 {
+  double x, y, z;
+};
+static inline R3 operator+(R3 a, R3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline R3 operator-(R3 a, R3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline R3 operator*(double s, R3 a) { return {s * a.x, s * a.y, s * a.z}; }
+static inline R3 operator*(R3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline R3 operator/(R3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+static inline R3& operator+=(R3& a, R3 b) { a = a + b; return a; }
+static inline double dot(R3 a, R3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* math::vecMul */
+static inline R3 vecmul(R3 u, R3 v) {
+  return {u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
+}
+static inline double norm(R3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+static inline double comp(R3 a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
+/* Arcane math::min / math::max */
+static inline double amin(double a, double b) { return (a < b) ? a : b; }
+static inline double amax(double a, double b) { return (a < b) ? b : a; }
+/* ---------------------------------------------------------------------------
+ * correctly rounded powers (test switch "cr_pow")
+ *
+ * The reference calls std::pow, and glibc's pow is not correctly rounded
+ * (pow(x, 0.5) != sqrt(x) for about 1 input in 1200 with glibc 2.39).  With
+ * cr_pow set, the oracle evaluates the same powers correctly rounded, which
+ * is what the CUDA library does; the default keeps the literal std::pow.
+ * ------------------------------------------------------------------------- */
+static inline void two_prod(double a, double b, double& p, double& e) {
+  p = a * b;
+  e = std::fma(a, b, -p);
+}
+static inline double cube_cr(double x) {
+  double s, sl, t, tl, u, ul;
+  two_prod(x, x, s, sl);
+  two_prod(s, x, t, tl);
+  two_prod(sl, x, u, ul);
+  return t + (tl + (u + ul));
+}
+/* x^(1./3.): cbrt refined to double-double, times exp(-d ln x) with
+ * d = 1/3 - double(1/3) = 2^-54/3, rounded once */
+static inline double pow_third_cr(double x) {
+  if (!(x > 0.0) || std::isinf(x)) return std::pow(x, 1. / 3.);
+  double r = std::cbrt(x);
+  double s, sl, t, tl;
+  two_prod(r, r, s, sl);
+  two_prod(s, r, t, tl);
+  double res = ((x - t) - tl) - sl * r;
+  double c_lo = res / (3.0 * s);
+  const double d = (1.0 / 3.0) * 0x1p-54;
+  double corr = c_lo - r * (d * std::log(x));
+  return r + corr;
+}
+
+/* MahycoModule::produit (MahycoModule.cc:1935) */
+static inline double produit(double A, double B, double C, double D) { return A * B - C * D; }
+
+struct MatField {
+  std::vector<double> g;
+  std::vector<double> e[MHC_MAX_ENV];
+  void init(long n, int nenv, double v = 0.0) {
+    g.assign(n, v);
+    for (int k = 0; k < nenv; ++k) e[k].assign(n, v);
+  }
+  void fill(double v) {
+    std::fill(g.begin(), g.end(), v);
+    for (auto& a : e) std::fill(a.begin(), a.end(), v);
+  }
+};
+
+enum { ST_OK = 0, ST_NEG_VOLUME = 1, ST_DT_UNDERFLOW = 2, ST_NAN = 3 };
+
+struct THLine {
+  double time;
+  double v[MHC_MAX_ENV][4];  /* CellMass, Pressure, Density, InternalEnergy */
+  int present[MHC_MAX_ENV];
+};
+
+struct Case {
+  mhc_case_params P;
+  int dim = 3, nenv = 1;
+  int ncx = 1, ncy = 1, ncz = 1, nnx = 2, nny = 2, nnz = 1;
+  long ncell = 0, nnode = 0;
+  int nbn = 8;  /* nodes per cell */
+  /* nodes */
+  std::vector<R3> coord, coord0, vel, vel_n, force;
+  std::vector<double> node_mass;
+  /* cells (non material) */
+  std::vector<R3> cell_coord;
+  std::vector<double> char_len, div_u, euler_volume, materiau;
+  std::vector<R3> cqs, cqs_n;         /* ncell * nbn */
+  std::vector<R3> outer_normal;       /* ncell * 2*dim */
+  /* faces, per direction */
+  long nface[3] = {0, 0, 0};
+  std::vector<R3> face_normal[3], face_coord[3];
+  std::vector<double> face_len[3];     /* face_length_lagrange component d */
+  std::vector<double> face_un[3];      /* face_normal_velocity */
+  std::vector<double> deltax[3];
+  /* material fields */
+  MatField density, density_n, density_0, pressure, pressure_n, pseudo, pseudo_n, pseudo_nm1,
+      mass_fraction, cell_mass, internal_energy, internal_energy_n, dpde, fracvol,
+      cell_volume, cell_volume_n, tau_density, sound_speed;
+  std::vector<uint8_t> envmask, nenvc;
+  /* remap */
+  int nvars = 4;
+  std::vector<double> u_lag, phi_lag, grad_phi, grad_phi_face, phi_face, dual_phi_flux;
+  std::vector<double> u_dual, phi_dual, dual_grad;
+  std::vector<double> back_flux, front_flux;
+  int sens_projection = 0;
+  /* emulation of a protection/reprise restart (test pinning only): after
+   * iteration restart_at the reference projects only 3*nb_env+5 variables
+   * (MahycoModule.cc:288), which leaves the pseudo-viscosity unprojected */
+  long restart_at = 0;
+  int nproj() const { return (restart_at > 0 && iteration > restart_at) ? 3 * nenv : nvars; }
+  /* time */
+  double t = 0.0, dt = 0.0, old_dt = 0.0, m_old_deltat = 0.0;
+  long iteration = 0;
+  int status = ST_OK;
+  bool stop = false;
+  std::vector<THLine> th;
+
+  long cid(int i, int j, int k) const { return i + (long)ncx * (j + (long)ncy * k); }
+  long nid(int i, int j, int k) const { return i + (long)nnx * (j + (long)nny * k); }
+  void cijk(long c, int& i, int& j, int& k) const {
+    i = (int)(c % ncx); long r = c / ncx; j = (int)(r % ncy); k = (int)(r / ncy);
+  }
+  void nijk(long n, int& i, int& j, int& k) const {
+    i = (int)(n % nnx); long r = n / nnx; j = (int)(r % nny); k = (int)(r / nny);
+  }
+  bool pure(long c) const { return nenvc[c] == 1; }
+  bool has(long c, int e) const { return (envmask[c] >> e) & 1; }
+  double& EV(MatField& f, int e, long c) { return pure(c) ? f.g[c] : f.e[e][c]; }
+
+  /* local node l of cell c */
+  long cnode(long c, int l) const {
+    int i, j, k;
+    cijk(c, i, j, k);
+    static const int off[8][3] = {{0,0,0},{1,0,0},{1,1,0},{0,1,0},{0,0,1},{1,0,1},{1,1,1},{0,1,1}};
+    return nid(i + off[l][0], j + off[l][1], k + off[l][2]);
+  }
+  /* face index inside direction d */
+  long fid(int d, int i, int j, int k) const {
+    if (d == 0) return i + (long)(ncx + 1) * (j + (long)ncy * k);
+    if (d == 1) return i + (long)ncx * (j + (long)(ncy + 1) * k);
+    return i + (long)ncx * (j + (long)ncy * k);
+  }
+  void fijk(int d, long f, int& i, int& j, int& k) const {
+    int ex = ncx + (d == 0), ey = ncy + (d == 1);
+    i = (int)(f % ex); long r = f / ex; j = (int)(r % ey); k = (int)(r / ey);
+  }
+  /* re-ordered face nodes (smallest uid first, then the smaller neighbour) */
+  int face_nodes(int d, int i, int j, int k, long* n) const {
+    if (dim == 2) {
+      if (d == 0) { n[0] = nid(i, j, 0); n[1] = nid(i, j + 1, 0); }
+      else { n[0] = nid(i, j, 0); n[1] = nid(i + 1, j, 0); }
+      return 2;
+    }
+    if (d == 0) { n[0] = nid(i,j,k); n[1] = nid(i,j+1,k); n[2] = nid(i,j+1,k+1); n[3] = nid(i,j,k+1); }
+    else if (d == 1) { n[0] = nid(i,j,k); n[1] = nid(i+1,j,k); n[2] = nid(i+1,j,k+1); n[3] = nid(i,j,k+1); }
+    else { n[0] = nid(i,j,k); n[1] = nid(i+1,j,k); n[2] = nid(i+1,j+1,k); n[3] = nid(i,j+1,k); }
+    return 4;
+  }
+  /* local face l of cell (i,j,k): direction and face index (Hexa8 / Quad4 order) */
+  void cell_face(int i, int j, int k, int l, int& d, long& f) const {
+    if (dim == 3) {
+      switch (l) {
+        case 0: d = 2; f = fid(2, i, j, k); break;
+        case 1: d = 0; f = fid(0, i, j, k); break;
+        case 2: d = 1; f = fid(1, i, j, k); break;
+        case 3: d = 2; f = fid(2, i, j, k + 1); break;
+        case 4: d = 0; f = fid(0, i + 1, j, k); break;
+        default: d = 1; f = fid(1, i, j + 1, k); break;
+      }
+    } else {
+      switch (l) {
+        case 0: d = 1; f = fid(1, i, j, 0); break;
+        case 1: d = 0; f = fid(0, i + 1, j, 0); break;
+        case 2: d = 1; f = fid(1, i, j + 1, 0); break;
+        default: d = 0; f = fid(0, i, j, 0); break;
+      }
+    }
+  }
+  int ncd(int d) const { return d == 0 ? ncx : (d == 1 ? ncy : ncz); }
+};
+
+/* ---------------------------------------------------------------------------
+ * geometry helpers
+ * ------------------------------------------------------------------------- */
+
+/* MahycoModule::computeCQs (MahycoModule.cc:1869-1932) */
+static void compute_cqs3(const R3* node_coord, const R3* face_coord, R3* out) {
+  const R3 c0 = face_coord[0], c1 = face_coord[1], c2 = face_coord[2];
+  const R3 c3 = face_coord[3], c4 = face_coord[4], c5 = face_coord[5];
+  const R3 n1a04 = 0.5 * vecmul(node_coord[0] - c0, node_coord[3] - c0);
+  const R3 n1a03 = 0.5 * vecmul(node_coord[3] - c0, node_coord[2] - c0);
+  const R3 n1a02 = 0.5 * vecmul(node_coord[2] - c0, node_coord[1] - c0);
+  const R3 n1a01 = 0.5 * vecmul(node_coord[1] - c0, node_coord[0] - c0);
+  const R3 n2a05 = 0.5 * vecmul(node_coord[0] - c1, node_coord[4] - c1);
+  const R3 n2a12 = 0.5 * vecmul(node_coord[4] - c1, node_coord[7] - c1);
+  const R3 n2a08 = 0.5 * vecmul(node_coord[7] - c1, node_coord[3] - c1);
+  const R3 n2a04 = 0.5 * vecmul(node_coord[3] - c1, node_coord[0] - c1);
+  const R3 n3a01 = 0.5 * vecmul(node_coord[0] - c2, node_coord[1] - c2);
+  const R3 n3a06 = 0.5 * vecmul(node_coord[1] - c2, node_coord[5] - c2);
+  const R3 n3a09 = 0.5 * vecmul(node_coord[5] - c2, node_coord[4] - c2);
+  const R3 n3a05 = 0.5 * vecmul(node_coord[4] - c2, node_coord[0] - c2);
+  const R3 n4a09 = 0.5 * vecmul(node_coord[4] - c3, node_coord[5] - c3);
+  const R3 n4a10 = 0.5 * vecmul(node_coord[5] - c3, node_coord[6] - c3);
+  const R3 n4a11 = 0.5 * vecmul(node_coord[6] - c3, node_coord[7] - c3);
+  const R3 n4a12 = 0.5 * vecmul(node_coord[7] - c3, node_coord[4] - c3);
+  const R3 n5a02 = 0.5 * vecmul(node_coord[1] - c4, node_coord[2] - c4);
+  const R3 n5a07 = 0.5 * vecmul(node_coord[2] - c4, node_coord[6] - c4);
+  const R3 n5a10 = 0.5 * vecmul(node_coord[6] - c4, node_coord[5] - c4);
+  const R3 n5a06 = 0.5 * vecmul(node_coord[5] - c4, node_coord[1] - c4);
+  const R3 n6a03 = 0.5 * vecmul(node_coord[2] - c5, node_coord[3] - c5);
+  const R3 n6a08 = 0.5 * vecmul(node_coord[3] - c5, node_coord[7] - c5);
+  const R3 n6a11 = 0.5 * vecmul(node_coord[7] - c5, node_coord[6] - c5);
+  const R3 n6a07 = 0.5 * vecmul(node_coord[6] - c5, node_coord[2] - c5);
+  const double t = 1. / 12.;
+  out[0] = (5. * (n1a01 + n1a04 + n2a04 + n2a05 + n3a05 + n3a01) + (n1a02 + n1a03 + n2a08 + n2a12 + n3a06 + n3a09)) * t;
+  out[1] = (5. * (n1a01 + n1a02 + n3a01 + n3a06 + n5a06 + n5a02) + (n1a04 + n1a03 + n3a09 + n3a05 + n5a10 + n5a07)) * t;
+  out[2] = (5. * (n1a02 + n1a03 + n5a07 + n5a02 + n6a07 + n6a03) + (n1a01 + n1a04 + n5a06 + n5a10 + n6a11 + n6a08)) * t;
+  out[3] = (5. * (n1a03 + n1a04 + n2a08 + n2a04 + n6a08 + n6a03) + (n1a01 + n1a02 + n2a05 + n2a12 + n6a07 + n6a11)) * t;
+  out[4] = (5. * (n2a05 + n2a12 + n3a05 + n3a09 + n4a09 + n4a12) + (n2a08 + n2a04 + n3a01 + n3a06 + n4a10 + n4a11)) * t;
+  out[5] = (5. * (n3a06 + n3a09 + n4a09 + n4a10 + n5a10 + n5a06) + (n3a01 + n3a05 + n4a12 + n4a11 + n5a07 + n5a02)) * t;
+  out[6] = (5. * (n4a11 + n4a10 + n5a10 + n5a07 + n6a07 + n6a11) + (n4a12 + n4a09 + n5a06 + n5a02 + n6a03 + n6a08)) * t;
+  out[7] = (5. * (n2a08 + n2a12 + n4a12 + n4a11 + n6a11 + n6a08) + (n2a04 + n2a05 + n4a09 + n4a10 + n6a07 + n6a03)) * t;
+}
+
+/* face centres of a hexahedron (MahycoModule.cc:1117-1122) */
+static void hex_face_centres(const R3* coord, R3* fc) {
+  fc[0] = 0.25 * (coord[0] + coord[3] + coord[2] + coord[1]);
+  fc[1] = 0.25 * (coord[0] + coord[4] + coord[7] + coord[3]);
+  fc[2] = 0.25 * (coord[0] + coord[1] + coord[5] + coord[4]);
+  fc[3] = 0.25 * (coord[4] + coord[5] + coord[6] + coord[7]);
+  fc[4] = 0.25 * (coord[1] + coord[2] + coord[6] + coord[5]);
+  fc[5] = 0.25 * (coord[2] + coord[3] + coord[7] + coord[6]);
+}
+
+/* 2D corner normals (MahycoModule.cc:1128-1146) */
+static void compute_cqs2(const R3* c4, R3* out) {
+  R3 coord[5] = {c4[0], c4[1], c4[2], c4[3], c4[0]};
+  R3 npc[5] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int n = 0; n < 4; ++n) {
+    npc[n + 1].x = 0.5 * (coord[n + 1].y - coord[n].y);
+    npc[n + 1].y = 0.5 * (coord[n].x - coord[n + 1].x);
+  }
+  npc[0] = npc[4];
+  for (int ii = 0; ii < 4; ++ii) out[ii] = npc[ii + 1] + npc[ii];
+}
+
+/* ---------------------------------------------------------------------------
+ * equation-of-state services
+ * ------------------------------------------------------------------------- */
+
+/* pressure of the Mie-Gruneisen law for a given density
+ * (MieGruneisenEOSService.cc:55-64 and the two finite-difference copies) */
+static bool g_cr_pow = false;
+static inline double ipow2(double x) { return g_cr_pow ? x * x : std::pow(x, 2); }
+static inline double ipow3(double x) { return g_cr_pow ? cube_cr(x) : std::pow(x, 3); }
+
+static double mg_pressure(const mhc_env_params& o, double density, double e) {
+  double J = o.rho0 / density;
+  double mu = 1. / J - 1.;
+  if (g_cr_pow) {
+    if (mu > 0.) {
+      double num = o.rho0 * ipow2(o.c0) * mu * (1 + (1. - o.gamma0 / 2.) * mu - o.a * ipow2(mu) / 2.);
+      double den = ipow2((1. - (o.s1 - 1.) * mu - o.s2 * ipow2(mu) / (1 + mu) - o.s2 * ipow3(mu) / ipow2(1. + mu)));
+      return num / den + (o.gamma0 + o.a * mu) * e;
+    }
+    return o.rho0 * ipow2(o.c0) * mu + (o.gamma0 + o.a * mu) * e;
+  }
+  if (mu > 0.) {
+    double num = o.rho0 * std::pow(o.c0, 2) * mu * (1 + (1. - o.gamma0 / 2.) * mu - o.a * std::pow(mu, 2) / 2.);
+    double den = std::pow((1. - (o.s1 - 1.) * mu - o.s2 * std::pow(mu, 2) / (1 + mu) - o.s2 * std::pow(mu, 3) / std::pow(1. + mu, 2)), 2);
+    return num / den + (o.gamma0 + o.a * mu) * e;
+  }
+  return o.rho0 * std::pow(o.c0, 2) * mu + (o.gamma0 + o.a * mu) * e;
+}
+
+/* IEquationOfState::initEOS for one environment */
+static void eos_init(Case& C, int env) {
+  const mhc_env_params& o = C.P.env[env];
+  for (long c = 0; c < C.ncell; ++c) {
+    if (!C.has(c, env)) continue;
+    double p = C.EV(C.pressure, env, c), rho = C.EV(C.density, env, c);
+    if (o.eos == MHC_EOS_PERFECT_GAS) {
+      /* PerfectGasEOSService.cc:12-35 */
+      double g = o.adiabatic_cst;
+      C.EV(C.internal_energy, env, c) = p / ((g - 1.) * rho);
+      C.EV(C.sound_speed, env, c) = std::sqrt(g * p / rho);
+    } else if (o.eos == MHC_EOS_STIFFENED_GAS) {
+      /* StiffenedGasEOSService.cc:14-33 */
+      double g = o.adiabatic_cst, pinf = o.limit_tension;
+      C.EV(C.internal_energy, env, c) = (p + (g * pinf)) / ((g - 1.) * rho);
+      C.EV(C.sound_speed, env, c) = std::sqrt((g / rho) * (p + pinf));
+    } else {
+      /* MieGruneisenEOSService.cc:12-34 */
+      C.EV(C.internal_energy, env, c) = C.EV(C.pressure, env, c) / o.gamma0;
+      C.EV(C.sound_speed, env, c) = o.c0;
+    }
+    C.EV(C.density_0, env, c) = C.EV(C.density, env, c);
+  }
+}
+
+/* IEquationOfState::applyEOS for one environment (PG 45-67, SG 43-63, MG 44-97).
+ * Damage (m_maille_endo) never triggers with the threshold defaults, and the
+ * temperature update has no hydro feedback; neither is carried. */
+static void eos_apply(Case& C, int env) {
+  const mhc_env_params& o = C.P.env[env];
+  for (long c = 0; c < C.ncell; ++c) {
+    if (!C.has(c, env)) continue;
+    double e = C.EV(C.internal_energy, env, c);
+    double rho = C.EV(C.density, env, c);
+    if (o.eos == MHC_EOS_PERFECT_GAS) {
+      double g = o.adiabatic_cst;
+      double p = (g - 1.) * rho * e;
+      C.EV(C.pressure, env, c) = p;
+      C.EV(C.sound_speed, env, c) = std::sqrt(g * p / rho);
+      C.EV(C.dpde, env, c) = (g - 1.) * rho;
+    } else if (o.eos == MHC_EOS_STIFFENED_GAS) {
+      double g = o.adiabatic_cst, pinf = o.limit_tension;
+      double p = ((g - 1.) * rho * e) - (g * pinf);
+      C.EV(C.pressure, env, c) = p;
+      C.EV(C.sound_speed, env, c) = std::sqrt((g / rho) * (p + pinf));
+      C.EV(C.dpde, env, c) = (g - 1.) * rho;
+    } else {
+      double J = o.rho0 / rho;
+      double mu = 1. / J - 1.;
+      C.EV(C.pressure, env, c) = mg_pressure(o, rho, e);
+      C.EV(C.dpde, env, c) = (o.gamma0 + o.a * mu);
+      double e_now = C.EV(C.internal_energy, env, c);
+      double p1 = mg_pressure(o, rho - 1.e-7, e_now);
+      double p2 = mg_pressure(o, rho + 1.e-7, e_now);
+      if ((p2 - p1) > 0.) C.EV(C.sound_speed, env, c) = std::sqrt((p2 - p1) / 2.e-7);
+      else C.EV(C.sound_speed, env, c) = 1.e4;
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * init entry points
+ * ------------------------------------------------------------------------- */
+
+static void gather_cell_coords(Case& C, long c, R3* out) {
+  for (int l = 0; l < C.nbn; ++l) out[l] = C.coord[C.cnode(c, l)];
+}
+
+/* MahycoModule::computeGeometricValues (MahycoModule.cc:1097-1253) */
+static int compute_geometric_values(Case& C) {
+  const double racine = C.dim == 2 ? .5 : 1. / 3.;
+  for (long c = 0; c < C.ncell; ++c) {
+    R3 coord[8];
+    gather_cell_coords(C, c, coord);
+    if (C.dim == 3) {
+      R3 fc[6];
+      hex_face_centres(coord, fc);
+      compute_cqs3(coord, fc, &C.cqs[c * 8]);
+    } else {
+      compute_cqs2(coord, &C.cqs[c * 4]);
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) {
+    double volume = 0.;
+    for (int n = 0; n < C.nbn; ++n) volume += dot(C.coord[C.cnode(c, n)], C.cqs[c * C.nbn + n]);
+    volume /= C.dim;
+    C.cell_volume.g[c] = volume;
+    if (volume < 0.) { C.status = ST_NEG_VOLUME; return C.status; }
+    int lc = C.P.longueur_caracteristique;
+    if (lc == MHC_LENGTH_CUBE_ROOT_VOLUME) {
+      if (g_cr_pow) C.char_len[c] = C.dim == 2 ? std::sqrt(C.cell_volume.g[c]) : pow_third_cr(C.cell_volume.g[c]);
+      else C.char_len[c] = std::pow(C.cell_volume.g[c], racine);
+    } else if (lc == MHC_LENGTH_OPPOSITE_FACES) {
+      R3 coord[8], fc[6];
+      gather_cell_coords(C, c, coord);
+      hex_face_centres(coord, fc);
+      double d1 = norm(fc[0] - fc[3]), d2 = norm(fc[2] - fc[5]), d3 = norm(fc[1] - fc[4]);
+      C.char_len[c] = (d1 * d2 * d3) / (d1 * d2 + d1 * d3 + d2 * d3);
+    } else {
+      int d = lc - MHC_LENGTH_MONODIM_X;
+      double a = comp(C.coord[C.cnode(c, 0)], d), b = comp(C.coord[C.cnode(c, 2)], d);
+      C.char_len[c] = std::fabs(b - a);
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) {
+    if (C.pure(c)) continue;
+    for (int e = 0; e < C.nenv; ++e)
+      if (C.has(c, e)) C.EV(C.cell_volume, e, c) = C.EV(C.fracvol, e, c) * C.cell_volume.g[c];
+  }
+  return ST_OK;
+}
+
+static void cell_centres(Case& C) {
+  const double w = C.dim == 2 ? .25 : .125;
+  for (long c = 0; c < C.ncell; ++c) {
+    R3 s = {0., 0., 0.};
+    for (int l = 0; l < C.nbn; ++l) s += C.coord[C.cnode(c, l)];
+    C.cell_coord[c] = w * s;
+  }
+}
+
+/* SODService::initMat / SEDOVService::initMat and the environment sort of
+ * MahycoModule::hydroStartInitEnvAndMat (MahycoAnnexe.cc:86-139) */
+static void init_materials(Case& C) {
+  const mhc_case_params& P = C.P;
+  for (long c = 0; c < C.ncell; ++c) {
+    double m = 0.;
+    if (P.cas_model == MHC_CASE_SOD) {
+      if (P.cas_test == MHC_TEST_BISOD_X || P.cas_test == MHC_TEST_BISOD_Y || P.cas_test == MHC_TEST_BISOD_Z) {
+        double r = comp(C.cell_coord[c], P.cas_test - MHC_TEST_BISOD_X);
+        m = (r < 0.5) ? 0. : 1.;
+      }
+    } else if (P.cas_model == MHC_CASE_TWO_STATE) {
+      if (C.nenv > 1) {
+        double r = comp(C.cell_coord[c], P.interface_dir);
+        m = (r < P.interface_pos) ? 0. : 1.;
+      }
+    } else if (P.cas_model == MHC_CASE_SEDOV && P.cas_test != MHC_TEST_SEDOV) {
+      bool center = false;
+      for (int l = 0; l < C.nbn; ++l) {
+        R3 x = C.coord[C.cnode(c, l)];
+        if (std::sqrt(x.x * x.x + x.y * x.y + x.z * x.z) < 1.e-10) center = true;
+      }
+      m = center ? 1. : 0.;
+    }
+    C.materiau[c] = m;
+    uint8_t mask = 0;
+    if (m == 0.) mask = 1;
+    else if (m > 0. && m < 1.) mask = 3;
+    else if (m == 1.) mask = 2;
+    else if (m > 1. && m < 2.) mask = 6;
+    else if (m == 2.) mask = 4;
+    else if (m > 2. && m < 3.) mask = 12;
+    else if (m == 3.) mask = 8;
+    else mask = 15;
+    mask &= (uint8_t)((1 << C.nenv) - 1);
+    C.envmask[c] = mask;
+    C.nenvc[c] = (uint8_t)__builtin_popcount(mask);
+  }
+}
+
+/* SODService::initVar(Mono), SEDOVService::initVar(Mono) and the seeded
+ * two-state variant (same structure as BiSod with explicit states) */
+static void init_variables(Case& C) {
+  const mhc_case_params& P = C.P;
+  if (P.cas_model == MHC_CASE_SOD) {
+    bool mono = P.cas_test == MHC_TEST_SOD_X || P.cas_test == MHC_TEST_SOD_Y || P.cas_test == MHC_TEST_SOD_Z;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (mono) {
+        double r = comp(C.cell_coord[c], P.cas_test - MHC_TEST_SOD_X);
+        double p, rho;
+        if (r < 0.5) { p = P.env[0].pression_initiale; rho = P.env[0].densite_initiale; }
+        else { p = P.env[0].pression_initiale / 10.; rho = P.env[0].densite_initiale / 8.; }
+        C.density.g[c] = rho;
+        C.pressure.g[c] = p;
+      } else {
+        int s = (C.materiau[c] == 0) ? 0 : 1;
+        C.density.g[c] = P.env[s].densite_initiale;
+        C.pressure.g[c] = P.env[s].pression_initiale;
+        if (!C.pure(c))
+          for (int e = 0; e < C.nenv; ++e)
+            if (C.has(c, e)) { C.EV(C.density, e, c) = P.env[s].densite_initiale; C.EV(C.pressure, e, c) = P.env[s].pression_initiale; }
+      }
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
+  } else if (P.cas_model == MHC_CASE_TWO_STATE) {
+    for (long c = 0; c < C.ncell; ++c) {
+      double r = comp(C.cell_coord[c], P.interface_dir);
+      int s = (r < P.interface_pos) ? 0 : 1;
+      C.density.g[c] = P.env[s].densite_initiale;
+      C.pressure.g[c] = P.env[s].pression_initiale;
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {0., 0., 0.};
+  } else if (P.cas_model == MHC_CASE_SEDOV) {
+    double rhoInit = P.env[0].densite_initiale, pInit = P.env[0].pression_initiale;
+    bool mono = P.cas_test == MHC_TEST_SEDOV;
+    const double e1 = 0.244816e-5;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (mono) C.internal_energy.g[c] = e1;
+      C.density.g[c] = rhoInit;
+      C.pressure.g[c] = pInit;
+      double vol = C.cell_volume.g[c];
+      bool center = false;
+      for (int l = 0; l < C.nbn; ++l) {
+        R3 x = C.coord[C.cnode(c, l)];
+        double rn = C.dim == 3 ? std::sqrt(x.x * x.x + x.y * x.y + x.z * x.z) : std::sqrt(x.x * x.x + x.y * x.y);
+        if (rn < 1.e-10) center = true;
+      }
+      if (center) {
+        C.internal_energy.g[c] += P.sedov_energy / vol;
+        C.pressure.g[c] = 0.4 * rhoInit * C.internal_energy.g[c];
+      }
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {0., 0., 0.};
+  }
+}
+
+/* MahycoModule::InitGeometricValues (MahycoModule.cc:1041-1093) */
+static void init_geometric_values(Case& C) {
+  C.coord0 = C.coord;
+  const double w = C.dim == 2 ? .5 : .25;
+  for (int d = 0; d < C.dim; ++d) {
+    for (long f = 0; f < C.nface[d]; ++f) {
+      int i, j, k;
+      C.fijk(d, f, i, j, k);
+      long n[4];
+      int nb = C.face_nodes(d, i, j, k, n);
+      R3 nrm;
+      if (C.dim == 3) {
+        R3 v1 = C.coord[n[2]] - C.coord[n[0]], v2 = C.coord[n[3]] - C.coord[n[1]];
+        nrm.x = produit(v1.y, v2.z, v1.z, v2.y);
+        nrm.y = -produit(v2.x, v1.z, v2.z, v1.x);
+        nrm.z = produit(v1.x, v2.y, v1.y, v2.x);
+      } else {
+        nrm.x = (C.coord[n[1]].y - C.coord[n[0]].y);
+        nrm.y = (C.coord[n[1]].x - C.coord[n[0]].x);
+        nrm.z = 0.;
+      }
+      C.face_normal[d][f] = nrm / norm(nrm);
+      R3 fc = {0., 0., 0.};
+      for (int q = 0; q < nb; ++q) fc += w * C.coord[n[q]];
+      C.face_coord[d][f] = fc;
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) {
+    int i, j, k;
+    C.cijk(c, i, j, k);
+    for (int l = 0; l < 2 * C.dim; ++l) {
+      int d; long f;
+      C.cell_face(i, j, k, l, d, f);
+      R3 diff = C.face_coord[d][f] - C.cell_coord[c];
+      C.outer_normal[c * 2 * C.dim + l] = diff / norm(diff);
+    }
+  }
+}
+
+static void setup(Case& C, const mhc_case_params* p) {
+  C.P = *p;
+  C.dim = p->dim;
+  C.nenv = p->nb_env;
+  C.ncx = p->nx; C.ncy = p->ny; C.ncz = (C.dim == 3) ? p->nz : 1;
+  C.nnx = C.ncx + 1; C.nny = C.ncy + 1; C.nnz = (C.dim == 3) ? C.ncz + 1 : 1;
+  C.ncell = (long)C.ncx * C.ncy * C.ncz;
+  C.nnode = (long)C.nnx * C.nny * C.nnz;
+  C.nbn = C.dim == 3 ? 8 : 4;
+  C.coord.resize(C.nnode);
+  double dx = p->lx / p->nx, dy = p->ly / p->ny, dz = (C.dim == 3) ? p->lz / p->nz : 0.;
+  for (long n = 0; n < C.nnode; ++n) {
+    int i, j, k;
+    C.nijk(n, i, j, k);
+    C.coord[n] = {p->origin[0] + i * dx, p->origin[1] + j * dy, (C.dim == 3) ? p->origin[2] + k * dz : 0.};
+  }
+  C.vel.assign(C.nnode, {0, 0, 0});
+  C.vel_n = C.vel;
+  C.force = C.vel;
+  C.node_mass.assign(C.nnode, 0.);
+  C.cell_coord.assign(C.ncell, {0, 0, 0});
+  C.char_len.assign(C.ncell, 0.);
+  C.div_u.assign(C.ncell, 0.);
+  C.euler_volume.assign(C.ncell, 0.);
+  C.materiau.assign(C.ncell, 0.);
+  C.cqs.assign(C.ncell * C.nbn, {0, 0, 0});
+  C.cqs_n = C.cqs;
+  C.outer_normal.assign(C.ncell * 2 * C.dim, {0, 0, 0});
+  for (int d = 0; d < C.dim; ++d) {
+    long ex = C.ncx + (d == 0), ey = C.ncy + (d == 1), ez = C.ncz + (d == 2);
+    if (C.dim == 2) ez = 1;
+    C.nface[d] = ex * ey * ez;
+    C.face_normal[d].assign(C.nface[d], {0, 0, 0});
+    C.face_coord[d].assign(C.nface[d], {0, 0, 0});
+    C.face_len[d].assign(C.nface[d], 0.);
+    C.face_un[d].assign(C.nface[d], 0.);
+    C.deltax[d].assign(C.nface[d], 0.);
+  }
+  MatField* mf[] = {&C.density, &C.density_n, &C.density_0, &C.pressure, &C.pressure_n, &C.pseudo,
+                    &C.pseudo_n, &C.pseudo_nm1, &C.mass_fraction, &C.cell_mass, &C.internal_energy,
+                    &C.internal_energy_n, &C.dpde, &C.fracvol, &C.cell_volume, &C.cell_volume_n,
+                    &C.tau_density, &C.sound_speed};
+  for (MatField* f : mf) f->init(C.ncell, C.nenv, 0.);
+  C.envmask.assign(C.ncell, 1);
+  C.nenvc.assign(C.ncell, 1);
+  C.nvars = 3 * C.nenv + 1;
+  C.u_lag.assign(C.ncell * C.nvars, 0.);
+  C.phi_lag = C.u_lag;
+  C.grad_phi = C.u_lag;
+  C.dual_phi_flux = C.u_lag;
+  C.u_dual.assign(C.nnode * 5, 0.);
+  C.phi_dual = C.u_dual;
+  C.dual_grad = C.u_dual;
+  C.back_flux.assign(C.nnode, 0.);
+  C.front_flux.assign(C.nnode, 0.);
+}
+
+/* MahycoModule::hydroStartInit (MahycoModule.cc:21-210) followed by
+ * computeCellMass (221-237) and computeNodeMass (247-262) */
+static int hydro_start_init(Case& C) {
+  C.dt = C.P.deltat_init;
+  C.sens_projection = 0;
+  cell_centres(C);                         /* MahycoAnnexe.cc:75-82 */
+  init_materials(C);
+  if (compute_geometric_values(C) != ST_OK) return C.status;
+  C.fracvol.fill(1.0);
+  C.mass_fraction.fill(1.0);
+  C.pseudo.fill(0.0);
+  C.internal_energy_n.fill(0.0);
+  init_variables(C);
+  for (int e = 0; e < C.nenv; ++e) eos_init(C, e);
+  for (long c = 0; c < C.ncell; ++c) {
+    if (C.pure(c)) continue;
+    C.internal_energy.g[c] = 0.;
+    for (int e = 0; e < C.nenv; ++e) {
+      if (!C.has(c, e)) continue;
+      C.internal_energy.g[c] += C.EV(C.internal_energy, e, c) * C.EV(C.mass_fraction, e, c);
+      C.sound_speed.g[c] = std::max(C.EV(C.sound_speed, e, c), C.sound_speed.g[c]);
+      C.density.g[c] += C.EV(C.density, e, c) * C.EV(C.fracvol, e, c);
+      C.pressure.g[c] += C.EV(C.pressure, e, c) * C.EV(C.fracvol, e, c);
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) C.euler_volume[c] = C.cell_volume.g[c];
+  init_geometric_values(C);
+  for (long c = 0; c < C.ncell; ++c) {
+    double volume = 0.;
+    for (int n = 0; n < C.nbn; ++n) volume += dot(C.coord[C.cnode(c, n)], C.cqs[c * C.nbn + n]);
+    volume /= C.dim;
+    C.cell_volume.g[c] = volume;
+  }
+  /* computeCellMass */
+  for (long c = 0; c < C.ncell; ++c) C.cell_mass.g[c] = C.density.g[c] * C.cell_volume.g[c];
+  for (int e = 0; e < C.nenv; ++e)
+    for (long c = 0; c < C.ncell; ++c)
+      if (C.has(c, e)) C.EV(C.cell_mass, e, c) = C.EV(C.mass_fraction, e, c) * C.cell_mass.g[c];
+  /* computeNodeMass */
+  std::fill(C.node_mass.begin(), C.node_mass.end(), 0.);
+  const double w = C.dim == 2 ? .25 : .125;
+  for (long c = 0; c < C.ncell; ++c) {
+    double contrib = w * C.cell_mass.g[c];
+    for (int l = 0; l < C.nbn; ++l) C.node_mass[C.cnode(c, l)] += contrib;
+  }
+  return ST_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * compute-loop entry points
+ * ------------------------------------------------------------------------- */
+
+/* MahycoModule::saveValuesAtN (MahycoModule.cc:311-382) */
+static void save_values_at_n(Case& C) {
+  C.old_dt = C.m_old_deltat;
+  auto cp = [&](MatField& dst, MatField& src) {
+    for (long c = 0; c < C.ncell; ++c) dst.g[c] = src.g[c];
+    for (int e = 0; e < C.nenv; ++e)
+      for (long c = 0; c < C.ncell; ++c)
+        if (C.has(c, e) && !C.pure(c)) dst.e[e][c] = src.e[e][c];
+  };
+  for (long c = 0; c < C.ncell; ++c) C.pseudo_nm1.g[c] = C.pseudo_n.g[c];
+  for (int e = 0; e < C.nenv; ++e)
+    for (long c = 0; c < C.ncell; ++c)
+      if (C.has(c, e) && !C.pure(c)) C.pseudo_nm1.e[e][c] = C.pseudo_n.e[e][c];
+  cp(C.pseudo_n, C.pseudo);
+  cp(C.pressure_n, C.pressure);
+  cp(C.cell_volume_n, C.cell_volume);
+  cp(C.density_n, C.density);
+  cp(C.internal_energy_n, C.internal_energy);
+  C.cqs_n = C.cqs;
+  C.vel_n = C.vel;
+}
+
+/* MahycoModule::updateVelocity (MahycoModule.cc:438-562); no stress
+ * deviator without an elasto model, so the elasto-plastic force term adds
+ * exact zeros and is omitted. */
+static void update_velocity(Case& C) {
+  for (auto& f : C.force) f = {0., 0., 0.};
+  for (long c = 0; c < C.ncell; ++c) {
+    double pressure = C.pressure_n.g[c] + C.pseudo_n.g[c];
+    for (int l = 0; l < C.nbn; ++l) C.force[C.cnode(c, l)] += pressure * C.cqs_n[c * C.nbn + l];
+  }
+  const double dt = 0.5 * (C.old_dt + C.dt);
+  for (long n = 0; n < C.nnode; ++n) C.vel[n] += (dt / C.node_mass[n]) * C.force[n];
+  R3 g = {C.P.gravity[0], C.P.gravity[1], C.P.gravity[2]};
+  for (long n = 0; n < C.nnode; ++n) C.vel[n] += dt * g;
+}
+
+static bool node_on_surface(const Case& C, long n, int surf) {
+  int i, j, k;
+  C.nijk(n, i, j, k);
+  switch (surf) {
+    case MHC_XMIN: return i == 0;
+    case MHC_XMAX: return i == C.nnx - 1;
+    case MHC_YMIN: return j == 0;
+    case MHC_YMAX: return j == C.nny - 1;
+    case MHC_ZMIN: return C.dim == 3 && k == 0;
+    default: return C.dim == 3 && k == C.nnz - 1;
+  }
+}
+
+/* MahycoModule::applyBoundaryCondition (MahycoModule.cc:756-807), velocity
+ * kinds on the PrepareFaceGroup surfaces.  A node lies on a surface exactly
+ * when it belongs to one of the surface's faces. */
+static void apply_boundary_condition(Case& C) {
+  const double eps = 1.e-8;
+  for (int b = 0; b < C.P.nb_bc; ++b) {
+    const mhc_bc& bc = C.P.bc[b];
+    bool novalue = false;
+    if ((C.t - C.dt * (1 - eps)) < bc.tdebut) novalue = true;
+    if ((C.t - C.dt * (1 - eps)) > bc.tfin) novalue = true;
+    if (novalue) continue;
+    for (long n = 0; n < C.nnode; ++n) {
+      if (!node_on_surface(C, n, bc.surface)) continue;
+      if (bc.kind == MHC_BC_VX) C.vel[n].x = bc.value;
+      else if (bc.kind == MHC_BC_VY) C.vel[n].y = bc.value;
+      else if (bc.kind == MHC_BC_VZ) C.vel[n].z = bc.value;
+    }
+  }
+}
+
+/* MahycoModule::updatePosition (MahycoModule.cc:730-751) */
+static void update_position(Case& C) {
+  for (long n = 0; n < C.nnode; ++n) C.coord[n] += C.dt * C.vel[n];
+  cell_centres(C);
+}
+
+/* MahycoModule::updateDensity (MahycoModule.cc:1267-1316) */
+static void update_density(Case& C) {
+  for (int e = 0; e < C.nenv; ++e) {
+    double thr = C.P.env[e].density_damage_thresold;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (!C.has(c, e)) continue;
+      double nd = C.EV(C.cell_mass, e, c) / C.EV(C.cell_volume, e, c);
+      C.EV(C.density, e, c) = nd;
+      if (C.EV(C.density, e, c) / C.density_0.g[c] < thr) C.EV(C.density, e, c) = thr * C.density_0.g[c];
+      C.EV(C.tau_density, e, c) = 0.5 * (1.0 / C.EV(C.density_n, e, c) + 1.0 / C.EV(C.density, e, c));
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) {
+    double nd = C.cell_mass.g[c] / C.cell_volume.g[c];
+    C.density.g[c] = nd;
+    C.tau_density.g[c] = 0.5 * (1.0 / C.density_n.g[c] + 1.0 / C.density.g[c]);
+    C.div_u[c] = 1.0 / C.dt * (1.0 / C.density.g[c] - 1.0 / C.density_n.g[c]) / C.tau_density.g[c];
+  }
+}
+
+/* MahycoModule::computeArtificialViscosity (MahycoModule.cc:386-426) */
+static void compute_artificial_viscosity(Case& C) {
+  for (int e = 0; e < C.nenv; ++e) {
+    double a1 = C.P.env[e].linear_pseudo_coeff, a2 = C.P.env[e].quadratic_pseudo_coeff;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (!C.has(c, e)) continue;
+      C.EV(C.pseudo, e, c) = 0.;
+      if (C.div_u[c] < 0.0) {
+        C.EV(C.pseudo, e, c) = 1. / C.EV(C.tau_density, e, c) *
+            (-a1 * C.char_len[c] * C.sound_speed.g[c] * C.div_u[c] +
+             a2 * C.char_len[c] * C.char_len[c] * C.div_u[c] * C.div_u[c]);
+      }
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) {
+    if (C.pure(c)) continue;
+    C.pseudo.g[c] = 0.;
+    for (int e = 0; e < C.nenv; ++e)
+      if (C.has(c, e)) C.pseudo.g[c] += C.EV(C.pseudo, e, c) * C.EV(C.fracvol, e, c);
+  }
+}
+
+/* MahycoModule::computePressionMoyenne (MahycoModule.cc:1708-1735) */
+static void compute_pression_moyenne(Case& C) {
+  double option = C.P.calcul_vitson_max ? 1. : 0.;
+  for (long c = 0; c < C.ncell; ++c) {
+    if (C.pure(c)) continue;
+    C.pressure.g[c] = 0.;
+    C.sound_speed.g[c] = 0.;
+    for (int e = 0; e < C.nenv; ++e) {
+      if (!C.has(c, e)) continue;
+      C.pressure.g[c] += C.EV(C.fracvol, e, c) * C.EV(C.pressure, e, c);
+      C.sound_speed.g[c] = option * std::max(C.EV(C.sound_speed, e, c), C.sound_speed.g[c]);
+      C.sound_speed.g[c] += (1. - option) * C.EV(C.fracvol, e, c) * C.EV(C.sound_speed, e, c);
+    }
+  }
+}
+
+/* MahycoModule::updateEnergyAndPressure (MahycoModule.cc:1430-1480) with
+ * updateEnergyAndPressureforGP (1623-1698, non-CSTS branch) or
+ * updateEnergyAndPressureExplicite (1484-1502) */
+static void update_energy_and_pressure(Case& C) {
+  if (C.P.pression_explicite) {
+    for (int e = 0; e < C.nenv; ++e) {
+      for (long c = 0; c < C.ncell; ++c) {
+        if (!C.has(c, e)) continue;
+        C.EV(C.internal_energy, e, c) -= (C.EV(C.pressure_n, e, c) + C.EV(C.pseudo, e, c)) *
+                                          (1.0 / C.EV(C.density, e, c) - 1.0 / C.EV(C.density_n, e, c));
+      }
+      eos_apply(C, e);
+    }
+  } else {
+    bool pc = C.P.pseudo_centree;
+    for (int e = 0; e < C.nenv; ++e) {
+      double g = C.P.env[e].adiabatic_cst;
+      for (long c = 0; c < C.ncell; ++c) {
+        if (!C.has(c, e)) continue;
+        double q = C.EV(C.pseudo, e, c), qn = C.EV(C.pseudo_n, e, c);
+        double rho = C.EV(C.density, e, c), rhon = C.EV(C.density_n, e, c);
+        double pseudo = 0.;
+        if (pc && ((qn + q) * (1.0 / rho - 1.0 / rhon) < 0.)) pseudo = 0.5 * (q + qn);
+        if (!pc && (q * (1.0 / rho - 1.0 / rhon) < 0.)) pseudo = q;
+        double den = 1 + 0.5 * (g - 1.0) * rho * (1.0 / rho - 1.0 / rhon);
+        double num = C.EV(C.internal_energy_n, e, c) - (0.5 * C.EV(C.pressure, e, c) + pseudo) * (1.0 / rho - 1.0 / rhon);
+        C.EV(C.internal_energy, e, c) = num / den;
+      }
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) {
+    if (C.pure(c)) continue;
+    C.internal_energy.g[c] = 0.;
+    for (int e = 0; e < C.nenv; ++e)
+      if (C.has(c, e)) C.internal_energy.g[c] += C.EV(C.mass_fraction, e, c) * C.EV(C.internal_energy, e, c);
+  }
+  if (!C.P.with_projection) {
+    if (!C.P.pression_explicite)
+      for (int e = 0; e < C.nenv; ++e) eos_apply(C, e);
+    compute_pression_moyenne(C);
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * remap (PrepareRemap.cc, RemapADIService.cc, UtilesRemap.cc,
+ * DualPhaseRemap.cc, RemapADIFinal.cc)
+ * ------------------------------------------------------------------------- */
+
+/* RemapADIService::fluxLimiter (UtilesRemap.cc:108-120) */
+static double flux_limiter(int id, double r) {
+  if (id == MHC_MINMOD) return std::max(0.0, std::min(1.0, r));
+  if (id == MHC_SUPERBEE) return std::max(0.0, std::max(std::min(2.0 * r, 1.0), std::min(r, 2.0)));
+  if (id == MHC_VANLEER) return (r <= 0.0) ? 0.0 : 2.0 * r / (1.0 + r);
+  return 0.0;
+}
+
+/* classical branch of computeAndLimitGradPhi (UtilesRemap.cc:329-345) */
+static double limited_gradient(int id, double gb, double gf) {
+  double g = 0.;
+  if (gb != 0.) g += 0.5 * (flux_limiter(id, gf / gb) * gb);
+  if (gf != 0.) g += 0.5 * (flux_limiter(id, gb / gf) * gf);
+  return g;
+}
+
+/* MahycoModule::computeVariablesForRemap (PrepareRemap.cc:94-193) */
+static void compute_variables_for_remap(Case& C) {
+  const int ne = C.nenv, nv = C.nvars;
+  std::fill(C.u_lag.begin(), C.u_lag.end(), 0.);
+  for (int e = 0; e < ne; ++e) {
+    for (long c = 0; c < C.ncell; ++c) {
+      if (!C.has(c, e)) continue;
+      double* u = &C.u_lag[c * nv];
+      double V = C.EV(C.cell_volume, e, c), rho = C.EV(C.density, e, c);
+      u[e] = V;
+      u[ne + e] = V * rho;
+      u[2 * ne + e] = V * rho * C.EV(C.internal_energy, e, c);
+      u[3 * ne] = C.cell_volume.g[c] * C.pseudo.g[c];
+      for (int iv = 0; iv < C.nproj(); ++iv) C.phi_lag[c * nv + iv] = u[iv] / C.cell_volume.g[c];
+    }
+  }
+  for (long n = 0; n < C.nnode; ++n) {
+    double m = C.node_mass[n];
+    R3 v = C.vel[n];
+    double* ud = &C.u_dual[n * 5];
+    double* pd = &C.phi_dual[n * 5];
+    ud[0] = m * v.x; ud[1] = m * v.y; ud[2] = m * v.z; ud[3] = m;
+    ud[4] = 0.5 * m * (v.x * v.x + v.y * v.y + v.z * v.z);
+    pd[0] = v.x; pd[1] = v.y; pd[2] = v.z; pd[3] = m;
+    pd[4] = 0.5 * (v.x * v.x + v.y * v.y + v.z * v.z);
+  }
+}
+
+/* MahycoModule::computeFaceQuantitesForRemap (PrepareRemap.cc:18-59) */
+static void compute_face_quantities_for_remap(Case& C) {
+  const double w = C.dim == 2 ? .5 : .25;
+  for (int d = 0; d < C.dim; ++d) {
+    for (long f = 0; f < C.nface[d]; ++f) {
+      int i, j, k;
+      C.fijk(d, f, i, j, k);
+      long n[4];
+      int nb = C.face_nodes(d, i, j, k, n);
+      if (C.dim == 3) {
+        R3 v1 = C.coord[n[2]] - C.coord[n[0]], v2 = C.coord[n[3]] - C.coord[n[1]];
+        double L[3];
+        L[0] = 0.5 * std::fabs(produit(v1.y, v2.z, v1.z, v2.y));
+        L[1] = 0.5 * std::fabs(produit(v2.x, v1.z, v2.z, v1.x));
+        L[2] = 0.5 * std::fabs(produit(v1.x, v2.y, v1.y, v2.x));
+        C.face_len[d][f] = L[d];
+      } else {
+        R3 t = C.coord[n[1]] - C.coord[n[0]];
+        C.face_len[d][f] = (d == 0) ? std::fabs(t.y) : std::fabs(t.x);
+      }
+      R3 vm = {0., 0., 0.}, fc = {0., 0., 0.};
+      for (int q = 0; q < nb; ++q) {
+        fc += w * C.coord[n[q]];
+        vm += C.vel[n[q]];
+      }
+      C.face_coord[d][f] = fc;
+      C.face_un[d][f] = dot((w * vm), C.face_normal[d][f]);
+    }
+  }
+}
+
+/* previous / next cell of an inner face of direction d */
+static void face_cells(const Case& C, int d, long f, long& cb, long& cf) {
+  int i, j, k;
+  C.fijk(d, f, i, j, k);
+  int id = d == 0 ? i : (d == 1 ? j : k);
+  cb = cf = -1;
+  if (id > 0) cb = (d == 0) ? C.cid(i - 1, j, k) : (d == 1 ? C.cid(i, j - 1, k) : C.cid(i, j, k - 1));
+  if (id < C.ncd(d)) cf = C.cid(i, j, k);
+}
+
+/* RemapADIService::computeGradPhiFace (RemapADIService.cc:119-149) */
+static void compute_grad_phi_face(Case& C, int d) {
+  const int nv = C.nvars;
+  C.grad_phi_face.assign(C.nface[d] * nv, 0.);
+  for (long f = 0; f < C.nface[d]; ++f) {
+    long cb, cf;
+    face_cells(C, d, f, cb, cf);
+    if (cb < 0 || cf < 0) continue;
+    C.deltax[d][f] = dot((C.cell_coord[cf] - C.cell_coord[cb]), C.face_normal[d][f]);
+    for (int iv = 0; iv < C.nproj(); ++iv)
+      C.grad_phi_face[f * nv + iv] = (C.phi_lag[cf * nv + iv] - C.phi_lag[cb * nv + iv]) / C.deltax[d][f];
+  }
+}
+
+/* back / front face of cell c in direction d */
+static void cell_dir_faces(const Case& C, long c, int d, long& fb, long& ff) {
+  int i, j, k;
+  C.cijk(c, i, j, k);
+  fb = C.fid(d, i, j, k);
+  ff = (d == 0) ? C.fid(0, i + 1, j, k) : (d == 1 ? C.fid(1, i, j + 1, k) : C.fid(2, i, j, k + 1));
+}
+
+/* RemapADIService::computeGradPhiCell (RemapADIService.cc:161-267), classical limiter */
+static void compute_grad_phi_cell(Case& C, int d) {
+  const int nv = C.nvars;
+  std::fill(C.grad_phi.begin(), C.grad_phi.end(), 0.);
+  if (C.P.ordre_projection <= 1) return;
+  for (long c = 0; c < C.ncell; ++c) {
+    long fb, ff;
+    cell_dir_faces(C, c, d, fb, ff);
+    for (int iv = 0; iv < C.nproj(); ++iv)
+      C.grad_phi[c * nv + iv] = limited_gradient(C.P.projection_limiteur_id, C.grad_phi_face[fb * nv + iv], C.grad_phi_face[ff * nv + iv]);
+  }
+}
+
+/* RemapADIService::computeUpwindFaceQuantitiesForProjection (279-383), order <= 2 */
+static void compute_upwind_face_quantities(Case& C, int d) {
+  const int nv = C.nvars;
+  C.phi_face.assign(C.nface[d] * nv, 0.);
+  int order2 = C.P.ordre_projection - 1;
+  for (long f = 0; f < C.nface[d]; ++f) {
+    long cb, cf;
+    face_cells(C, d, f, cb, cf);
+    if (cb < 0 || cf < 0) continue;
+    long cu = (C.face_un[d][f] * C.deltax[d][f] > 0.0) ? cb : cf;
+    for (int iv = 0; iv < C.nproj(); ++iv)
+      C.phi_face[f * nv + iv] = C.phi_lag[cu * nv + iv] +
+          order2 * dot((C.face_coord[d][f] - C.cell_coord[cu]), C.face_normal[d][f]) * C.grad_phi[cu * nv + iv];
+  }
+}
+
+/* RemapADIService::computeUremap (RemapADIService.cc:395-575), classical path */
+static void compute_uremap(Case& C, int d) {
+  const int nv = C.nvars, ne = C.nenv;
+  const double dt = C.dt;
+  std::fill(C.dual_phi_flux.begin(), C.dual_phi_flux.end(), 0.);
+  std::vector<double> flux_face(nv);
+  for (long c = 0; c < C.ncell; ++c) {
+    int i, j, k;
+    C.cijk(c, i, j, k);
+    std::fill(flux_face.begin(), flux_face.end(), 0.);
+    for (int l = 0; l < 2 * C.dim; ++l) {
+      int fd; long f;
+      C.cell_face(i, j, k, l, fd, f);
+      if (fd != d) continue;
+      double un = C.face_un[d][f], L = C.face_len[d][f];
+      R3 on = C.outer_normal[c * 2 * C.dim + l];
+      double ond = comp(on, d);
+      for (int iv = 0; iv < C.nproj(); ++iv) {
+        double flux = ond * un * L * dt * C.phi_face[f * nv + iv];
+        flux_face[iv] += flux;
+        C.dual_phi_flux[c * nv + iv] += 0.5 * flux * comp(on, d);
+      }
+    }
+    double* u = &C.u_lag[c * nv];
+    for (int iv = 0; iv < C.nproj(); ++iv) u[iv] -= flux_face[iv];
+    for (int e = 0; e < ne; ++e) {
+      if (u[ne + e] < 0.) u[ne + e] = 0.;
+      if (u[2 * ne + e] < 0.) u[2 * ne + e] = 0.;
+    }
+    double sv = 0.;
+    for (int e = 0; e < ne; ++e) sv += u[e];
+    for (int iv = 0; iv < C.nproj(); ++iv) C.phi_lag[c * nv + iv] = u[iv] / sv;
+  }
+}
+
+/* RemapADIService::computeDualUremap (DualPhaseRemap.cc:38-258), classical limiter */
+static void compute_dual_uremap(Case& C, int d) {
+  const int ne = C.nenv, nv = C.nvars;
+  const double dt = C.dt;
+  const int nnd = d == 0 ? C.nnx : (d == 1 ? C.nny : C.nnz);
+  auto ncoord = [&](long n) { return comp(C.coord[n], d); };
+  auto step = [&](long n, int s) -> long {
+    int i, j, k;
+    C.nijk(n, i, j, k);
+    if (d == 0) i += s; else if (d == 1) j += s; else k += s;
+    int id = d == 0 ? i : (d == 1 ? j : k);
+    if (id < 0 || id >= nnd) return -1;
+    return C.nid(i, j, k);
+  };
+  auto inner = [&](long n) {
+    int i, j, k;
+    C.nijk(n, i, j, k);
+    int id = d == 0 ? i : (d == 1 ? j : k);
+    return id > 0 && id < nnd - 1;
+  };
+  std::fill(C.dual_grad.begin(), C.dual_grad.end(), 0.);
+  if (C.P.ordre_projection > 1) {
+    for (long n = 0; n < C.nnode; ++n) {
+      if (!inner(n)) continue;
+      long nb = step(n, -1), nf = step(n, +1);
+      for (int iv = 0; iv < 3; ++iv) {
+        double gf = (C.phi_dual[nf * 5 + iv] - C.phi_dual[n * 5 + iv]) / (ncoord(nf) - ncoord(n));
+        double gb = (C.phi_dual[n * 5 + iv] - C.phi_dual[nb * 5 + iv]) / (ncoord(n) - ncoord(nb));
+        C.dual_grad[n * 5 + iv] = limited_gradient(C.P.projection_limiteur_id, gb, gf);
+      }
+    }
+  }
+  /* node mass fluxes: faces of direction d in face id order, then envs */
+  std::fill(C.back_flux.begin(), C.back_flux.end(), 0.);
+  std::fill(C.front_flux.begin(), C.front_flux.end(), 0.);
+  const double w = C.dim == 2 ? .5 : .25;
+  for (long f = 0; f < C.nface[d]; ++f) {
+    long cb, cf;
+    face_cells(C, d, f, cb, cf);
+    int i, j, k;
+    C.fijk(d, f, i, j, k);
+    long fn[4];
+    int nb = C.face_nodes(d, i, j, k, fn);
+    if (cb >= 0)
+      for (int q = 0; q < nb; ++q)
+        for (int e = 0; e < ne; ++e) C.back_flux[fn[q]] += w * C.dual_phi_flux[cb * nv + ne + e];
+    if (cf >= 0)
+      for (int q = 0; q < nb; ++q)
+        for (int e = 0; e < ne; ++e) C.front_flux[fn[q]] += w * C.dual_phi_flux[cf * nv + ne + e];
+  }
+  const int order2 = C.P.ordre_projection - 1;
+  for (long n = 0; n < C.nnode; ++n) {
+    if (!inner(n)) continue;
+    long nb = step(n, -1), nf = step(n, +1);
+    double* U = &C.u_dual[n * 5];
+    const double* P = C.phi_dual.data();
+    const double* G = C.dual_grad.data();
+    double bfm = C.back_flux[n], ffm = C.front_flux[n];
+    U[3] += bfm - ffm;
+    double FV[3], BV[3], FE, BE;
+    double ufront = 0.5 * (P[n * 5 + d] + P[nf * 5 + d]);
+    int signfront = (ufront > 0) ? 1 : -1;
+    long src = (ffm < 0.) ? nf : n;
+    double geo = (signfront * (ncoord(nf) - ncoord(n)) - dt * ufront);
+    for (int iv = 0; iv < 3; ++iv) FV[iv] = P[src * 5 + iv] + order2 * (0.5 * G[src * 5 + iv] * geo);
+    FE = P[src * 5 + 4] + order2 * (0.5 * G[src * 5 + 4] * geo);
+    double uback = 0.5 * (P[nb * 5 + d] + P[n * 5 + d]);
+    int signback = (uback > 0) ? 1 : -1;
+    src = (bfm > 0.) ? nb : n;
+    geo = (signback * (ncoord(n) - ncoord(nb)) - dt * uback);
+    for (int iv = 0; iv < 3; ++iv) BV[iv] = P[src * 5 + iv] + order2 * (0.5 * G[src * 5 + iv] * geo);
+    BE = P[src * 5 + 4] + order2 * (0.5 * G[src * 5 + 4] * geo);
+    for (int iv = 0; iv < 3; ++iv) U[iv] += bfm * BV[iv] - ffm * FV[iv];
+    U[4] += bfm * BE - ffm * FE;
+  }
+  for (long n = 0; n < C.nnode; ++n) {
+    if (!inner(n)) continue;
+    double* U = &C.u_dual[n * 5];
+    double* P = &C.phi_dual[n * 5];
+    for (int iv = 0; iv < 3; ++iv)
+      if (std::fabs(U[iv]) < 1.e-300) U[iv] = 0.;
+    P[0] = U[0] / U[3];
+    P[1] = U[1] / U[3];
+    P[2] = U[2] / U[3];
+    P[3] = U[3];
+    P[4] = U[4] / U[3];
+  }
+}
+
+/* RemapADIService::remapVariables (RemapADIFinal.cc:21-346) */
+static int remap_variables(Case& C) {
+  const int ne = C.nenv, nv = C.nvars;
+  const double thr = C.P.remap_threshold;
+  const bool with_dual = true;
+  /* environment membership update: the add / remove criteria of one
+   * environment only read that environment's membership, so the new masks
+   * are computed first and the storage transfer is applied once per cell */
+  std::vector<uint8_t> newmask(C.envmask);
+  for (int e = 0; e < ne; ++e) {
+    for (long c = 0; c < C.ncell; ++c) {
+      const double* u = &C.u_lag[c * nv];
+      bool in = C.has(c, e);
+      if (((u[e] / C.euler_volume[c]) < thr || (u[ne + e] == 0. && with_dual)) && in) {
+        newmask[c] &= (uint8_t)~(1 << e);
+      } else if ((u[e] / C.euler_volume[c]) > thr && !in) {
+        double volt = 0.;
+        for (int q = 0; q < ne; ++q) volt += u[q];
+        double vn = u[e] * C.euler_volume[c] / volt;
+        if ((vn / C.euler_volume[c]) > thr && u[ne + e] != 0.) newmask[c] |= (uint8_t)(1 << e);
+      }
+    }
+  }
+  {
+    MatField* mf[] = {&C.density, &C.density_n, &C.density_0, &C.pressure, &C.pressure_n, &C.pseudo,
+                      &C.pseudo_n, &C.pseudo_nm1, &C.mass_fraction, &C.cell_mass, &C.internal_energy,
+                      &C.internal_energy_n, &C.dpde, &C.fracvol, &C.cell_volume, &C.cell_volume_n,
+                      &C.tau_density, &C.sound_speed};
+    for (long c = 0; c < C.ncell; ++c) {
+      uint8_t old = C.envmask[c], nm = newmask[c];
+      if (old == nm) continue;
+      int oldn = __builtin_popcount(old), newn = __builtin_popcount(nm);
+      /* values of environments that stay keep their value; a new
+       * environment starts from zero */
+      for (int e = 0; e < ne; ++e) {
+        bool was = (old >> e) & 1, is = (nm >> e) & 1;
+        if (!is) continue;
+        for (MatField* f : mf) {
+          double v = was ? (oldn == 1 ? f->g[c] : f->e[e][c]) : 0.;
+          if (newn == 1) { if (was) f->g[c] = v; }
+          else f->e[e][c] = v;
+        }
+      }
+      C.envmask[c] = nm;
+      C.nenvc[c] = (uint8_t)newn;
+    }
+  }
+  std::vector<double> vol(ne), dens(ne), ener(ne);
+  std::fill(C.cell_mass.g.begin(), C.cell_mass.g.end(), 0.);
+  for (long c = 0; c < C.ncell; ++c) {
+    const double* u = &C.u_lag[c * nv];
+    double V = C.euler_volume[c];
+    C.cell_volume.g[c] = C.euler_volume[c];
+    double volt = 0., masset = 0.;
+    for (int e = 0; e < ne; ++e) { vol[e] = u[e]; volt += vol[e]; masset += u[ne + e]; }
+    double unsurvolt = 1. / volt;
+    for (int e = 0; e < ne; ++e) vol[e] *= V * unsurvolt;
+    double somme_frac = 0.;
+    double unsurvol = 1. / V;
+    for (int e = 0; e < ne; ++e) {
+      if (!C.has(c, e)) continue;
+      double& f = C.EV(C.fracvol, e, c);
+      f = vol[e] * unsurvol;
+      if (f < thr) f = 0.;
+      somme_frac += f;
+    }
+    double unsursf = 0.;
+    if (somme_frac != 0.) unsursf = 1. / somme_frac;
+    for (int e = 0; e < ne; ++e)
+      if (C.has(c, e)) C.EV(C.fracvol, e, c) *= unsursf;
+    if (masset > thr * thr) {
+      double unsurm = 1. / masset, fm = 0.;
+      for (int e = 0; e < ne; ++e) {
+        if (!C.has(c, e)) continue;
+        C.EV(C.mass_fraction, e, c) = u[ne + e] * unsurm;
+        if (C.EV(C.fracvol, e, c) < thr) C.EV(C.mass_fraction, e, c) = 0.;
+        fm += C.EV(C.mass_fraction, e, c);
+      }
+      if (fm != 0.) {
+        double unsurfm = 1. / fm;
+        for (int e = 0; e < ne; ++e)
+          if (C.has(c, e)) C.EV(C.mass_fraction, e, c) *= unsurfm;
+      }
+    }
+    double dn = 0.;
+    for (int e = 0; e < ne; ++e) {
+      if (!C.has(c, e)) continue;
+      dens[e] = 0.;
+      if (C.EV(C.fracvol, e, c) > thr && vol[e] != 0.) dens[e] = u[ne + e] / vol[e];
+      dn += C.EV(C.fracvol, e, c) * dens[e];
+    }
+    for (int e = 0; e < ne; ++e) {
+      if (!C.has(c, e)) continue;
+      ener[e] = 0.;
+      if (C.EV(C.fracvol, e, c) > thr && u[ne + e] != 0.) ener[e] = u[2 * ne + e] / u[ne + e];
+    }
+    C.density.g[c] = dn;
+    C.cell_mass.g[c] = C.euler_volume[c] * dn;
+    double en = 0., ps = 0.;
+    for (int e = 0; e < ne; ++e) {
+      if (!C.has(c, e)) continue;
+      C.EV(C.cell_mass, e, c) = C.EV(C.mass_fraction, e, c) * C.cell_mass.g[c];
+      C.EV(C.pseudo, e, c) = u[3 * ne] * unsurvol;
+      C.EV(C.density, e, c) = dens[e];
+      C.EV(C.internal_energy, e, c) = ener[e];
+      en += C.EV(C.mass_fraction, e, c) * C.EV(C.internal_energy, e, c);
+      ps += C.EV(C.fracvol, e, c) * C.EV(C.pseudo, e, c);
+    }
+    C.internal_energy.g[c] = en;
+    C.pseudo.g[c] = ps;
+    for (int e = 0; e < ne; ++e) {
+      if (!C.has(c, e)) continue;
+      if (C.EV(C.density, e, c) < 0. || C.EV(C.internal_energy, e, c) < 0.) {
+        C.EV(C.internal_energy, e, c) = 0.;
+        C.EV(C.density, e, c) = 0.;
+        C.EV(C.fracvol, e, c) = 0.;
+        C.EV(C.mass_fraction, e, c) = 0.;
+      }
+      double r = C.EV(C.density, e, c), ie = C.EV(C.internal_energy, e, c);
+      if (r != r || ie != ie) { C.status = ST_NAN; return C.status; }
+    }
+  }
+  for (long n = 0; n < C.nnode; ++n) {
+    const double* U = &C.u_dual[n * 5];
+    double m = U[3];
+    if (m != 0.) C.vel[n] = {U[0] / m, U[1] / m, U[2] / m};
+  }
+  std::fill(C.node_mass.begin(), C.node_mass.end(), 0.);
+  const double w = C.dim == 2 ? .25 : .125;
+  for (long c = 0; c < C.ncell; ++c) {
+    double contrib = w * C.cell_mass.g[c];
+    for (int l = 0; l < C.nbn; ++l) C.node_mass[C.cnode(c, l)] += contrib;
+    if (!C.pure(c))
+      for (int e = 0; e < ne; ++e)
+        if (C.has(c, e)) C.EV(C.cell_volume, e, c) = C.EV(C.fracvol, e, c) * C.cell_volume.g[c];
+  }
+  return ST_OK;
+}
+
+/* RemapADIService::appliRemap (RemapADIService.cc:15-90) */
+static int appli_remap(Case& C) {
+  for (int i = 0; i < C.dim; ++i) {
+    int d = (i + C.sens_projection) % C.dim;
+    if (C.ncd(d) == 1) continue;
+    compute_grad_phi_face(C, d);
+    compute_grad_phi_cell(C, d);
+    compute_upwind_face_quantities(C, d);
+    compute_uremap(C, d);
+    compute_dual_uremap(C, d);
+  }
+  C.sens_projection = (C.sens_projection + 1) % C.dim;
+  if (C.P.is_euler_scheme == MHC_EULER_FULL) C.coord = C.coord0;
+  return remap_variables(C);
+}
+
+/* MahycoModule::remap (PrepareRemap.cc:203-251) */
+static int remap(Case& C) {
+  if (!C.P.with_projection) return ST_OK;
+  compute_variables_for_remap(C);
+  compute_face_quantities_for_remap(C);
+  if (appli_remap(C) != ST_OK) return C.status;
+  for (int e = 0; e < C.nenv; ++e) eos_apply(C, e);
+  compute_pression_moyenne(C);
+  return ST_OK;
+}
+
+/* MahycoModule::computeDeltaT (MahycoModule.cc:1739-1864) */
+static int compute_delta_t(Case& C) {
+  C.old_dt = C.dt;
+  C.m_old_deltat = C.old_dt;
+  double new_dt;
+  if (C.P.deltat_constant) {
+    new_dt = C.P.deltat_init;
+  } else {
+    double minimum_aux = 1.7976931348623157e308;
+    for (long c = 0; c < C.ncell; ++c) {
+      double vmax = 0.;
+      if (C.P.is_euler_scheme == MHC_EULER_FULL)
+        for (int l = 0; l < C.nbn; ++l) vmax = amax(norm(C.vel[C.cnode(c, l)]), vmax);
+      double dx_sound = C.char_len[c] / (C.sound_speed.g[c] + vmax);
+      minimum_aux = amin(minimum_aux, dx_sound);
+    }
+    new_dt = C.P.cfl * minimum_aux;
+    new_dt = amin(new_dt, 1.05 * C.old_dt);
+    new_dt = amin(new_dt, C.P.deltat_max);
+    if (new_dt < C.P.deltat_min) { C.status = ST_DT_UNDERFLOW; return C.status; }
+  }
+  C.dt = new_dt;
+  double stop = C.P.final_time;
+  bool not_yet = C.t < stop, finish = C.t > stop, too_much = (C.t + new_dt) > stop;
+  if ((not_yet && too_much) || finish) C.stop = true;
+  return ST_OK;
+}
+
+/* EnvSummationService::write (EnvSummationService.cc:77-169) */
+static void time_history_write(Case& C) {
+  int period = C.P.time_history_period > 0 ? C.P.time_history_period : 10;
+  if (C.iteration % period != 0) return;
+  THLine L;
+  L.time = C.t;
+  for (int e = 0; e < C.nenv; ++e) {
+    long cnt = 0;
+    double m = 0., p = 0., rv = 0., vv = 0., em = 0., mm = 0.;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (!C.has(c, e)) continue;
+      ++cnt;
+      m += C.EV(C.cell_mass, e, c);
+      p += C.EV(C.pressure, e, c);
+    }
+    for (long c = 0; c < C.ncell; ++c) {
+      if (!C.has(c, e)) continue;
+      em += C.EV(C.internal_energy, e, c) * C.EV(C.cell_mass, e, c);
+      mm += C.EV(C.cell_mass, e, c);
+    }
+    for (long c = 0; c < C.ncell; ++c) {
+      if (!C.has(c, e)) continue;
+      rv += C.EV(C.density, e, c) * C.EV(C.cell_volume, e, c);
+      vv += C.EV(C.cell_volume, e, c);
+    }
+    L.present[e] = cnt > 0;
+    L.v[e][0] = m / cnt;
+    L.v[e][1] = p / cnt;
+    L.v[e][2] = rv / vv;
+    L.v[e][3] = em / mm;
+  }
+  C.th.push_back(L);
+}
+
+/* one iteration of the MahycoLoop / MahycoLagrangeLoop compute loop
+ * (Mahyco.config:23-36) */
+static int iterate(Case& C) {
+  C.iteration += 1;
+  C.t = C.t + C.dt;
+  save_values_at_n(C);
+  update_velocity(C);
+  apply_boundary_condition(C);
+  update_position(C);
+  if (compute_geometric_values(C) != ST_OK) return C.status;
+  update_density(C);
+  compute_artificial_viscosity(C);
+  update_energy_and_pressure(C);
+  if (remap(C) != ST_OK) return C.status;
+  if (compute_delta_t(C) != ST_OK) return C.status;
+  time_history_write(C);
+  return ST_OK;
+}
+
+}  // namespace ora
+
+/* ===========================================================================
+ * C interface used by the tests (ctypes)
+ * ========================================================================= */
+extern "C" {
+
+void* oracle_create(const mhc_case_params* p) {
+  ora::Case* C = new ora::Case();
+  ora::setup(*C, p);
+  return C;
+}
+
+void oracle_destroy(void* h) { delete (ora::Case*)h; }
+
+int oracle_init(void* h) { return ora::hydro_start_init(*(ora::Case*)h); }
+
+/* run up to n iterations; stops early on error or when the final time is reached */
+int oracle_iterate(void* h, int n) {
+  ora::Case& C = *(ora::Case*)h;
+  for (int it = 0; it < n; ++it) {
+    if (C.status != ora::ST_OK) return C.status;
+    if (C.stop) break;
+    if (ora::iterate(C) != ora::ST_OK) return C.status;
+  }
+  return C.status;
+}
+
+/* run until the reference time loop would stop (final time) or max_iter */
+int oracle_run(void* h, long max_iter) {
+  ora::Case& C = *(ora::Case*)h;
+  while (!C.stop && C.iteration < max_iter) {
+    if (ora::iterate(C) != ora::ST_OK) return C.status;
+  }
+  return C.status;
+}
+
+/* test-only switches: "restart_at" = iteration after which a
+ * protection/reprise restart is emulated; "cr_pow" = correctly rounded
+ * powers instead of std::pow (process-wide) */
+int oracle_set_option(void* h, const char* name, double value) {
+  ora::Case& C = *(ora::Case*)h;
+  if (!strcmp(name, "restart_at")) { C.restart_at = (long)value; return 0; }
+  if (!strcmp(name, "cr_pow")) { ora::g_cr_pow = value != 0.; return 0; }
+  return -1;
+}
+
+double oracle_scalar(void* h, const char* name) {
+  ora::Case& C = *(ora::Case*)h;
+  if (!strcmp(name, "time")) return C.t;
+  if (!strcmp(name, "deltat")) return C.dt;
+  if (!strcmp(name, "old_deltat")) return C.old_dt;
+  if (!strcmp(name, "iteration")) return (double)C.iteration;
+  if (!strcmp(name, "stop")) return C.stop ? 1. : 0.;
+  if (!strcmp(name, "status")) return C.status;
+  if (!strcmp(name, "ncell")) return (double)C.ncell;
+  if (!strcmp(name, "nnode")) return (double)C.nnode;
+  return NAN;
+}
+
+static ora::MatField* mat_field(ora::Case& C, const char* name) {
+  struct { const char* n; ora::MatField* f; } tab[] = {
+      {"Density", &C.density}, {"Pressure", &C.pressure}, {"InternalEnergy", &C.internal_energy},
+      {"SoundSpeed", &C.sound_speed}, {"PseudoViscosity", &C.pseudo}, {"CellMass", &C.cell_mass},
+      {"CellVolume", &C.cell_volume}, {"FracVol", &C.fracvol}, {"MassFraction", &C.mass_fraction},
+      {"DpDe", &C.dpde}, {"TauxDensity", &C.tau_density}};
+  for (auto& t : tab)
+    if (!strcmp(name, t.n)) return t.f;
+  return nullptr;
+}
+
+/* env < 0: global cell value; env >= 0: environment value (0 where the cell
+ * is not in the environment).  Node Real3 fields are returned interleaved. */
+long oracle_get_field(void* h, const char* name, int env, double* out, long cap) {
+  ora::Case& C = *(ora::Case*)h;
+  if (ora::MatField* f = mat_field(C, name)) {
+    if (cap < C.ncell) return -1;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (env < 0) out[c] = f->g[c];
+      else out[c] = C.has(c, env) ? C.EV(*f, env, c) : 0.;
+    }
+    return C.ncell;
+  }
+  if (!strcmp(name, "CaracteristicLength") || !strcmp(name, "EulerVolume") || !strcmp(name, "EnvMask")) {
+    if (cap < C.ncell) return -1;
+    for (long c = 0; c < C.ncell; ++c)
+      out[c] = name[0] == 'C' ? C.char_len[c] : (name[0] == 'E' && name[1] == 'u' ? C.euler_volume[c] : (double)C.envmask[c]);
+    return C.ncell;
+  }
+  if (!strcmp(name, "NodeMass")) {
+    if (cap < C.nnode) return -1;
+    for (long n = 0; n < C.nnode; ++n) out[n] = C.node_mass[n];
+    return C.nnode;
+  }
+  if (!strcmp(name, "Velocity") || !strcmp(name, "NodeCoord") || !strcmp(name, "CellCoord")) {
+    bool cc = !strcmp(name, "CellCoord");
+    long n_ = cc ? C.ncell : C.nnode;
+    if (cap < 3 * n_) return -1;
+    const std::vector<ora::R3>& v = cc ? C.cell_coord : (name[0] == 'V' ? C.vel : C.coord);
+    for (long n = 0; n < n_; ++n) { out[3 * n] = v[n].x; out[3 * n + 1] = v[n].y; out[3 * n + 2] = v[n].z; }
+    return 3 * n_;
+  }
+  return -2;
+}
+
+/* the oracle's correctly rounded x^(1./3.), for its own unit test */
+double oracle_pow_third_cr(double x) { return ora::pow_third_cr(x); }
+double oracle_cube_cr(double x) { return ora::cube_cr(x); }
+
+/* number of time-history lines recorded so far */
+long oracle_th_count(void* h) { return (long)((ora::Case*)h)->th.size(); }
+
+/* line i: out[0]=time, then per env 4 values (CellMass, Pressure, Density,
+ * InternalEnergy) and a presence flag: 1 + 5*nb_env doubles */
+int oracle_th_line(void* h, long i, double* out) {
+  ora::Case& C = *(ora::Case*)h;
+  if (i < 0 || i >= (long)C.th.size()) return -1;
+  const ora::THLine& L = C.th[i];
+  out[0] = L.time;
+  for (int e = 0; e < C.nenv; ++e) {
+    for (int q = 0; q < 4; ++q) out[1 + 5 * e + q] = L.v[e][q];
+    out[1 + 5 * e + 4] = L.present[e];
+  }
+  return 0;
+}
+
+}  /* extern "C" */

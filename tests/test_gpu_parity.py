@@ -1,0 +1,87 @@
+"""GPU parity: the CUDA library against the CPU oracle on the same inputs.
+
+Two bars, on every case of mahyco_b200.cases.PARITY_CASES:
+
+* exact: against the oracle with correctly rounded powers (the arithmetic
+  the CUDA library implements) every cell, environment and node field and
+  the time-loop scalars must be bit-identical after N iterations;
+* reference libm: against the oracle that calls glibc's std::pow like the
+  reference (glibc's pow is not correctly rounded), every field must agree
+  to a relative L-infinity |gpu - oracle|_inf / |oracle|_inf <= 1e-12 after
+  min(N, 40) iterations.
+"""
+import numpy as np
+import pytest
+
+from mahyco_b200.cases import PARITY_CASES
+
+TOL = 1e-12
+LIBM_CYCLES = 40
+CELL_FIELDS = ["Density", "Pressure", "InternalEnergy", "SoundSpeed", "PseudoViscosity",
+               "CellMass", "CellVolume", "CaracteristicLength"]
+ENV_FIELDS = ["Density", "Pressure", "InternalEnergy", "FracVol", "CellMass"]
+
+
+def rel_inf(a, b):
+    d = np.max(np.abs(a - b)) if a.size else 0.0
+    s = np.max(np.abs(b)) if b.size else 0.0
+    return d / s if s > 0 else d
+
+
+def compare(gpu, ora, nenv):
+    errs = {}
+    for f in CELL_FIELDS:
+        errs[f] = rel_inf(gpu.field(f), ora.field(f))
+    for f in ("Velocity", "NodeMass"):
+        errs[f] = rel_inf(gpu.field(f), ora.field(f))
+    if nenv > 1:
+        errs["EnvMask"] = float(np.any(gpu.field("EnvMask") != ora.field("EnvMask")))
+        for e in range(nenv):
+            for f in ENV_FIELDS:
+                errs[f"{f}[{e}]"] = rel_inf(gpu.field(f, e), ora.field(f, e))
+    return errs
+
+
+def run_pair(name, cr_pow, ncycles=None):
+    from mahyco_b200 import Hydro
+    from tests.oracle import Oracle
+    build, n = PARITY_CASES[name]
+    n = n if ncycles is None else min(n, ncycles)
+    p = build()
+    ora = Oracle(p, cr_pow=cr_pow)
+    assert ora.init() == 0
+    gpu = Hydro(p)
+    gpu.hydroStartInit()
+    init_errs = compare(gpu, ora, p.nb_env)
+    # first iteration through the individual entry points, the rest fused
+    gpu.iterate()
+    assert ora.iterate(1) == 0
+    gpu.cycle(n - 1)
+    st = gpu.synchronize()
+    assert st == 0, st
+    assert ora.iterate(n - 1) == 0
+    s = gpu.scalars()
+    assert s["iteration"] == n
+    errs = compare(gpu, ora, p.nb_env)
+    errs["time"] = abs(s["time"] - ora.scalar("time")) / abs(ora.scalar("time"))
+    errs["deltat"] = abs(s["deltat"] - ora.scalar("deltat")) / abs(ora.scalar("deltat"))
+    gpu.close()
+    return init_errs, errs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(PARITY_CASES))
+def test_parity_exact(name):
+    init_errs, errs = run_pair(name, cr_pow=True)
+    assert max(init_errs.values()) == 0.0, init_errs
+    bad = {k: v for k, v in errs.items() if v != 0.0}
+    assert not bad, (name, bad)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(PARITY_CASES))
+def test_parity_reference_libm(name):
+    init_errs, errs = run_pair(name, cr_pow=False, ncycles=LIBM_CYCLES)
+    assert max(init_errs.values()) <= TOL, init_errs
+    bad = {k: v for k, v in errs.items() if v > TOL}
+    assert not bad, (name, bad, errs)
