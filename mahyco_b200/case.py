@@ -268,3 +268,41 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     if th is not None:
         p.time_history_period = _txt(th, "periode", 10, int)
     return p, info
+
+
+# ---------------------------------------------------------------------------
+# (de)serialisation
+# ---------------------------------------------------------------------------
+def _to_py(v):
+    if isinstance(v, C.Array):
+        return [_to_py(x) for x in v]
+    if isinstance(v, C.Structure):
+        return {n: _to_py(getattr(v, n)) for n, _ in v._fields_}
+    return v
+
+
+def _from_py(obj, v):
+    for n, _ in obj._fields_:
+        if n not in v:
+            continue
+        cur = getattr(obj, n)
+        if isinstance(cur, C.Array):
+            for i, x in enumerate(v[n]):
+                if isinstance(cur[i], C.Structure):
+                    _from_py(cur[i], x)
+                else:
+                    cur[i] = x
+        elif isinstance(cur, C.Structure):
+            _from_py(cur, v[n])
+        else:
+            setattr(obj, n, v[n])
+
+
+def params_to_dict(p: CaseParams) -> dict:
+    return _to_py(p)
+
+
+def params_from_dict(d: dict) -> CaseParams:
+    p = default_params()
+    _from_py(p, d)
+    return p

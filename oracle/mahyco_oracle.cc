@@ -1479,6 +1479,22 @@ long oracle_get_field(void* h, const char* name, int env, double* out, long cap)
   return -2;
 }
 
+/* known-answer hooks for the oracle's own unit tests */
+double oracle_flux_limiter(int id, double r) { return ora::flux_limiter(id, r); }
+double oracle_limited_gradient(int id, double gb, double gf) { return ora::limited_gradient(id, gb, gf); }
+void oracle_eos_point(const mhc_env_params* o, double rho, double e, double* p, double* c) {
+  mhc_case_params P;
+  memset(&P, 0, sizeof(P));
+  P.dim = 2; P.nx = 1; P.ny = 1; P.lx = P.ly = 1.; P.nb_env = 1; P.env[0] = *o;
+  ora::Case C;
+  ora::setup(C, &P);
+  C.density.g[0] = rho;
+  C.internal_energy.g[0] = e;
+  ora::eos_apply(C, 0);
+  *p = C.pressure.g[0];
+  *c = C.sound_speed.g[0];
+}
+
 /* the oracle's correctly rounded x^(1./3.), for its own unit test */
 double oracle_pow_third_cr(double x) { return ora::pow_third_cr(x); }
 double oracle_cube_cr(double x) { return ora::cube_cr(x); }

@@ -1,0 +1,57 @@
+"""Extract golden fixtures from the reference's non-regression data.
+
+Run in a checkout that has the reference tree (default: /root/reference):
+
+    python tests/golden/make_golden.py [REFERENCE_ROOT]
+
+For each case below it parses NONREGRESSION/<case>/Donnees.arc with
+mahyco_b200.case.read_arc and stores the resulting parameters plus the
+reference's EnvSummation time histories (output/courbes/gnuplot/<Var>_<Env>,
+17 significant digits) in tests/golden/<case>.json.  The tests never read
+the reference tree; they only read these JSON files.
+"""
+import ctypes
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from mahyco_b200.case import read_arc, params_to_dict  # noqa: E402
+
+# case -> extra oracle switches needed to reproduce how the reference ran it
+CASES = {
+    "CAS_2D_Lag_SodCaseX": {},
+    "CAS_2D_Lag_BiSodCaseX": {},
+    "CAS_Lag_BiSodCaseX": {},
+    "CAS_BiSodCaseX": {},
+    # seq_pr test: 10 iterations, then a restart (launch_test.sh:25-38)
+    "CAS_SodCaseX": {"restart_at": 10},
+    "CAS_2D_Sedov": {},
+    # run on 8 MPI ranks by the reference (src/CMakeLists.txt:193-208)
+    "CAS_Sedov": {"mpi_ranks": 8},
+}
+VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
+
+
+def main(ref_root="/root/reference"):
+    for case, extra in CASES.items():
+        d = os.path.join(ref_root, "NONREGRESSION", case)
+        p, info = read_arc(os.path.join(d, "Donnees.arc"))
+        hist = {}
+        for env in info["env_names"]:
+            for v in VARS:
+                fn = os.path.join(d, "output", "courbes", "gnuplot", f"{v}_{env}")
+                if not os.path.exists(fn):
+                    continue
+                rows = [[float(x) for x in line.split()] for line in open(fn) if line.strip()]
+                hist[f"{v}_{env}"] = rows
+        out = {"case": case, "params": params_to_dict(p), "env_names": info["env_names"],
+               "timeloop": info["timeloop"], "extra": extra, "time_history": hist}
+        with open(os.path.join(HERE, case + ".json"), "w") as f:
+            json.dump(out, f, indent=0)
+        print(case, {k: len(v) for k, v in hist.items()})
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

@@ -98,3 +98,21 @@ class Oracle:
             self.L.oracle_th_line(self.h, i, buf)
             rows.append(list(buf))
         return np.array(rows).reshape(-1, w)
+
+
+def setup_kat(L):
+    L.oracle_flux_limiter.restype = C.c_double
+    L.oracle_flux_limiter.argtypes = [C.c_int, C.c_double]
+    L.oracle_limited_gradient.restype = C.c_double
+    L.oracle_limited_gradient.argtypes = [C.c_int, C.c_double, C.c_double]
+    from mahyco_b200.case import EnvParams
+    L.oracle_eos_point.argtypes = [C.POINTER(EnvParams), C.c_double, C.c_double,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    return L
+
+
+def eos_point(env, rho, e):
+    L = setup_kat(lib())
+    p, c = C.c_double(), C.c_double()
+    L.oracle_eos_point(C.byref(env), rho, e, C.byref(p), C.byref(c))
+    return p.value, c.value

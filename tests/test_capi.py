@@ -1,0 +1,62 @@
+"""The C ABI library loads without a GPU, exports every symbol that
+include/*.h declares, and fails loudly (an error code, no CPU fallback) when
+no CUDA device is available."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import mahyco_b200 as mb
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(INCLUDE):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(INCLUDE, h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(mhc_\w+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = mb.load()
+    names = declared_symbols()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol():
+    assert declared_symbols() <= set(mb._SIGS)
+
+
+def test_version_and_budget_query():
+    lib = mb.load()
+    assert b"sm_100a" in lib.mhc_version()
+    p = mb.default_params()
+    p.dim, p.nx, p.ny, p.nz, p.nb_env = 3, 64, 64, 64, 2
+    assert lib.mhc_case_device_bytes(ctypes.byref(p)) > 64 ** 3 * 8 * 20
+
+
+def test_rejects_options_outside_the_hot_path():
+    lib = mb.load()
+    p = mb.default_params()
+    p.with_newton = 1
+    h = ctypes.c_void_p()
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+
+
+@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", "x") != "" and os.path.exists("/dev/nvidia0"),
+                    reason="a GPU is present")
+def test_no_gpu_fails_loudly():
+    p = mb.default_params()
+    p.nx = p.ny = p.nz = 4
+    with pytest.raises(mb.MahycoError):
+        mb.Hydro(p)

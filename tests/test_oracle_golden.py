@@ -1,0 +1,52 @@
+"""The CPU oracle against the reference's own non-regression time histories.
+
+tests/golden/<case>.json holds the parameters parsed from the case's
+Donnees.arc and the EnvSummation curves the reference wrote
+(NONREGRESSION/<case>/output/courbes/gnuplot), made by make_golden.py.
+Sequential runs agree to ~1e-14 (the residue is the summation order of the
+per-environment averages); the 8-rank CAS_Sedov reference run sums its
+averages per rank, hence the looser bound.
+"""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from mahyco_b200.case import params_from_dict
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "CAS_*.json")))
+VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
+
+
+def run_oracle(g, cr_pow=False):
+    from tests.oracle import Oracle
+    p = params_from_dict(g["params"])
+    o = Oracle(p, cr_pow=cr_pow)
+    if "restart_at" in g["extra"]:
+        o.set_option("restart_at", g["extra"]["restart_at"])
+    assert o.init() == 0
+    nlines = max(len(v) for v in g["time_history"].values())
+    assert o.run(max_iter=10 * nlines) == 0
+    return p, o.time_history()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-5] for p in GOLDEN])
+@pytest.mark.parametrize("cr_pow", [False, True], ids=["glibc_pow", "cr_pow"])
+def test_oracle_matches_reference_goldens(path, cr_pow):
+    g = json.load(open(path))
+    tol = 5e-12 if g["extra"].get("mpi_ranks", 1) > 1 else 1e-13
+    p, th = run_oracle(g, cr_pow)
+    for e, env in enumerate(g["env_names"]):
+        for q, var in enumerate(VARS):
+            key = f"{var}_{env}"
+            if key not in g["time_history"]:
+                continue
+            ref = np.array(g["time_history"][key])
+            assert len(th) >= len(ref), (key, len(th), len(ref))
+            ours = th[: len(ref)]
+            np.testing.assert_allclose(ours[:, 0], ref[:, 0], rtol=1e-14, atol=0)
+            rel = np.abs(ours[:, 1 + 5 * e + q] - ref[:, 1]) / np.abs(ref[:, 1])
+            assert rel.max() <= tol, (key, rel.max(), int(rel.argmax()))
