@@ -51,6 +51,10 @@ const char* mhc_version(void);
 int mhc_case_create(const mhc_case_params* params, mhc_case** out);
 int mhc_case_destroy(mhc_case* h);
 
+/* the CUDA stream (cudaStream_t) every kernel of the case is launched on,
+ * so that callers can record events or order their own work after it */
+void* mhc_case_stream(mhc_case* h);
+
 /* HBM bytes one case with these parameters needs (serving admission). */
 long long mhc_case_device_bytes(const mhc_case_params* params);
 
@@ -90,6 +94,24 @@ int mhc_cycle(mhc_case* h, int n);
  * graph and replayed (launch-bound small cases) */
 int mhc_cycle_graph(mhc_case* h, int n);
 
+/* kernel groups of one iteration, for mhc_cycle_timed */
+enum mhc_stage {
+  MHC_STAGE_LAGRANGE_NODES = 0,  /* velocity, BC, position */
+  MHC_STAGE_LAGRANGE_CELLS = 1,  /* geometry, density, pseudo, energy */
+  MHC_STAGE_SWEEP_CELLS = 2,     /* one remap direction, cells */
+  MHC_STAGE_SWEEP_NODES = 3,     /* one remap direction, dual (nodes) */
+  MHC_STAGE_FINALIZE_CELLS = 4,  /* remapVariables + EOS */
+  MHC_STAGE_FINALIZE_NODES = 5,  /* node velocity and mass */
+  MHC_STAGE_DELTA_T = 6,         /* CFL reduction */
+  MHC_NUM_STAGES = 7
+};
+
+/* mhc_cycle with CUDA events recorded on the case stream around every
+ * kernel group; stage_ms[s] receives the summed device time of stage s,
+ * stage_launches[s] (optional) its number of launches.  Synchronises after
+ * each group, so use it for measurement, not production. */
+int mhc_cycle_timed(mhc_case* h, int n, double* stage_ms, long long* stage_launches);
+
 /* wait for the case stream; returns the numerical status flags */
 int mhc_synchronize(mhc_case* h);
 
@@ -106,7 +128,7 @@ long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, lo
 
 /* --- IEquationOfState (IEquationOfState.h:38-65) ------------------------
  * applyEOS(env) on the current density and internal energy of the env
- * cells, followed (when all_envs is set) by computePressionMoyenne. */
+ * cells; mixed cells holding env then get computePressionMoyenne. */
 int mhc_eos_apply(mhc_case* h, int env);
 
 /* --- IRemap::appliRemap + remapVariables (IRemap.h:44-63) ---------------

@@ -33,6 +33,7 @@ _SIGS = {
     "mhc_version": (C.c_char_p, []),
     "mhc_case_create": (C.c_int, [C.POINTER(CaseParams), C.POINTER(C.c_void_p)]),
     "mhc_case_destroy": (C.c_int, [C.c_void_p]),
+    "mhc_case_stream": (C.c_void_p, [C.c_void_p]),
     "mhc_case_device_bytes": (C.c_longlong, [C.POINTER(CaseParams)]),
     "mhc_hydro_start_init": (C.c_int, [C.c_void_p]),
     "mhc_save_values_at_n": (C.c_int, [C.c_void_p]),
@@ -48,6 +49,7 @@ _SIGS = {
     "mhc_compute_delta_t": (C.c_int, [C.c_void_p]),
     "mhc_cycle": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_cycle_graph": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_cycle_timed": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "mhc_synchronize": (C.c_int, [C.c_void_p]),
     "mhc_get_scalars": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                   C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
@@ -100,6 +102,11 @@ class Hydro:
         self.ncell = params.ncell
         self.nnode = params.nnode
 
+    @property
+    def stream_handle(self) -> int:
+        """cudaStream_t of the case (for torch.cuda.ExternalStream / events)"""
+        return int(self.lib.mhc_case_stream(self.h))
+
     def close(self):
         if self.h:
             self.lib.mhc_case_destroy(self.h)
@@ -145,6 +152,17 @@ class Hydro:
     def cycle(self, n: int, graph: bool = False) -> None:
         f = self.lib.mhc_cycle_graph if graph else self.lib.mhc_cycle
         _check(self.lib, f(self.h, int(n)), "mhc_cycle")
+
+    STAGES = ("lagrange_nodes", "lagrange_cells", "sweep_cells", "sweep_nodes",
+              "finalize_cells", "finalize_nodes", "delta_t")
+
+    def cycle_timed(self, n: int) -> dict:
+        """n iterations with CUDA events around every kernel group (on the
+        case stream); returns {stage: (total_ms, launches)}."""
+        ms = (C.c_double * len(self.STAGES))()
+        ln = (C.c_longlong * len(self.STAGES))()
+        _check(self.lib, self.lib.mhc_cycle_timed(self.h, int(n), ms, ln), "mhc_cycle_timed")
+        return {s: (ms[i], ln[i]) for i, s in enumerate(self.STAGES)}
 
     def synchronize(self) -> int:
         return _check(self.lib, self.lib.mhc_synchronize(self.h), "mhc_synchronize")

@@ -9,6 +9,7 @@
 
 #include "../../include/mahyco_b200.h"
 #include "mhc_kernels.cuh"
+#include "mhc_sweep.cuh"
 
 using namespace mhc;
 
@@ -45,6 +46,30 @@ struct mhc_case {
   cudaGraphExec_t graph = nullptr;
   int graph_n = 0;
   size_t lagrange_smem = 0;
+  // optional per-stage timing: events recorded around every kernel group
+  bool timing = false;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double stage_ms[MHC_NUM_STAGES] = {0};
+  long long stage_launches[MHC_NUM_STAGES] = {0};
+};
+
+// brackets one kernel group with events on the case stream and accumulates
+// its device time (only when timing is enabled)
+struct StageTimer {
+  mhc_case* h;
+  int stage;
+  StageTimer(mhc_case* h_, int s) : h(h_), stage(s) {
+    if (h->timing) cudaEventRecord(h->ev[0], h->stream);
+  }
+  ~StageTimer() {
+    if (!h->timing) return;
+    cudaEventRecord(h->ev[1], h->stream);
+    cudaEventSynchronize(h->ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+    h->stage_ms[stage] += ms;
+    h->stage_launches[stage] += 1;
+  }
 };
 
 static long long count_doubles(const mhc_case_params* p, long long& ncell, long long& nnode) {
@@ -161,10 +186,14 @@ int mhc_case_create(const mhc_case_params* params, mhc_case** out) {
   return MHC_OK;
 }
 
+void* mhc_case_stream(mhc_case* h) { return h ? (void*)h->stream : nullptr; }
+
 int mhc_case_destroy(mhc_case* h) {
   if (!h) return MHC_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (int i = 0; i < 2; ++i)
+    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
   for (void* p : h->allocs) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -187,6 +216,7 @@ static int launch_init(mhc_case* h) {
 
 template <int DIM>
 static int launch_lagrange_nodes(mhc_case* h) {
+  StageTimer tm(h, MHC_STAGE_LAGRANGE_NODES);
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(k_lagrange_nodes<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->lagrange_smem));
@@ -201,6 +231,7 @@ static int launch_lagrange_nodes(mhc_case* h) {
 
 template <int DIM, int NE>
 static int launch_lagrange_cells(mhc_case* h) {
+  StageTimer tm(h, MHC_STAGE_LAGRANGE_CELLS);
   const int T = 256;
   if (h->P.with_projection)
     k_lagrange_cells<DIM, NE, true><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F);
@@ -210,11 +241,28 @@ static int launch_lagrange_cells(mhc_case* h) {
   return MHC_OK;
 }
 
+// grid of the sweep tiles (SweepTile<D>): lanes along x, tile along D
+template <int D>
+static dim3 sweep_grid(int nx, int ny, int nz) {
+  using T = SweepTile<D>;
+  if (D == 0) return dim3((nx + T::TD - 1) / T::TD, ny, nz);
+  if (D == 1) return dim3((nx + T::TW - 1) / T::TW, (ny + T::TD - 1) / T::TD, nz);
+  return dim3((nx + T::TW - 1) / T::TW, (nz + T::TD - 1) / T::TD, ny);
+}
+
 template <int DIM, int NE, int D>
 static void launch_sweep_dir(mhc_case* h, SweepArgs sa, DualArgs da) {
-  const int T = 256;
-  k_sweep_cells<DIM, NE, D><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F, sa);
-  k_sweep_nodes<DIM, NE, D><<<blocks_for(h->M.nnode, T), T, 0, h->stream>>>(h->M, h->P, h->F, da);
+  const Mesh& M = h->M;
+  {
+    StageTimer tm(h, MHC_STAGE_SWEEP_CELLS);
+    k_sweep_cells<DIM, NE, D><<<sweep_grid<D>(M.ncx, M.ncy, M.ncz), SweepTile<D>::THREADS, 0, h->stream>>>(
+        h->M, h->P, h->F, sa);
+  }
+  {
+    StageTimer tm(h, MHC_STAGE_SWEEP_NODES);
+    k_sweep_nodes<DIM, NE, D><<<sweep_grid<D>(M.nnx, M.nny, M.nnz), SweepTile<D>::THREADS, 0, h->stream>>>(
+        h->M, h->P, h->F, da);
+  }
 }
 
 template <int DIM, int NE>
@@ -251,14 +299,21 @@ static int launch_remap(mhc_case* h) {
   const double* Ufin = h->F.U[ub];
   const double* Udfin = first ? nullptr : h->F.Ud[udb];
   const int T = 256;
-  k_remap_finalize_cells<DIM, NE><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F, Ufin);
-  if (Udfin) k_remap_finalize_nodes<DIM><<<blocks_for(h->M.nnode, T), T, 0, h->stream>>>(h->M, h->F, Udfin);
+  {
+    StageTimer tm(h, MHC_STAGE_FINALIZE_CELLS);
+    k_remap_finalize_cells<DIM, NE><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F, Ufin);
+  }
+  if (Udfin) {
+    StageTimer tm(h, MHC_STAGE_FINALIZE_NODES);
+    k_remap_finalize_nodes<DIM><<<blocks_for(h->M.nnode, T), T, 0, h->stream>>>(h->M, h->F, Udfin);
+  }
   CK(cudaGetLastError());
   return MHC_OK;
 }
 
 template <int DIM>
 static int launch_dt(mhc_case* h) {
+  StageTimer tm(h, MHC_STAGE_DELTA_T);
   const int T = 256;
   k_delta_t<DIM><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F);
   k_delta_t_finalize<<<1, 1, 0, h->stream>>>(h->P, h->F);
@@ -392,6 +447,23 @@ int mhc_cycle_graph(mhc_case* h, int n) {
   h->sens_projection = (h->sens_projection + n) % h->DIM;
   if ((n & 1) != 0) swap_positions(h);
   return MHC_OK;
+}
+
+int mhc_cycle_timed(mhc_case* h, int n, double* stage_ms, long long* stage_launches) {
+  if (!h || !stage_ms) return set_err(MHC_ERR_ARG, "null argument");
+  if (!h->ev[0]) {
+    CK(cudaEventCreate(&h->ev[0]));
+    CK(cudaEventCreate(&h->ev[1]));
+  }
+  for (int s = 0; s < MHC_NUM_STAGES; ++s) { h->stage_ms[s] = 0.; h->stage_launches[s] = 0; }
+  h->timing = true;
+  int r = mhc_cycle(h, n);
+  h->timing = false;
+  for (int s = 0; s < MHC_NUM_STAGES; ++s) {
+    stage_ms[s] = h->stage_ms[s];
+    if (stage_launches) stage_launches[s] = h->stage_launches[s];
+  }
+  return r;
 }
 
 int mhc_synchronize(mhc_case* h) {

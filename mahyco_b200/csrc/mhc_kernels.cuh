@@ -561,312 +561,7 @@ __global__ void __launch_bounds__(256) k_lagrange_cells(Mesh M, mhc_case_params 
   }
 }
 
-// ---------------------------------------------------------------------------
-// remap sweep, cell part: computeGradPhiFace + computeGradPhiCell +
-// computeUpwindFaceQuantitiesForProjection + computeUremap for direction D
-// (RemapADIService.cc:119-575, UtilesRemap.cc:108-120, 325-357, classical
-// limiters, order <= 2).  Face quantities of the Lagrangian mesh
-// (PrepareRemap.cc:18-59) are rebuilt from the node positions: initial face
-// normals are the unit axis vectors of the cartesian grid, so every
-// dot(., n) reduces to the D component.
-// ---------------------------------------------------------------------------
-struct SweepArgs {
-  const double* Uin;
-  double* Uout;
-  int first;
-  int order;
-  int limiter;
-};
-
-template <int DIM, int D>
-__device__ __forceinline__ void face_node_ijk(int i, int j, int k, int q, int& a, int& b, int& cz) {
-  // re-ordered face nodes: smallest uid first, then the smaller neighbour
-  a = i; b = j; cz = k;
-  if (DIM == 2) {
-    if (D == 0) b += q; else a += q;
-    return;
-  }
-  int s1 = (q == 1 || q == 2), s2 = (q == 2 || q == 3);
-  if (D == 0) { b += s1; cz += s2; }
-  else if (D == 1) { a += s1; cz += s2; }
-  else { a += s1; b += s2; }
-}
-
-template <int DIM, int NE, int D>
-__global__ void __launch_bounds__(256) k_sweep_cells(Mesh M, mhc_case_params P, Fields F, SweepArgs A) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= M.ncell) return;
-  const long long N = M.ncell;
-  constexpr int NV = 3 * NE + 1;
-  int i, j, k;
-  cell_ijk(M, c, i, j, k);
-  const int id = D == 0 ? i : (D == 1 ? j : k);
-  const int nd = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
-  const long long stride = D == 0 ? 1 : (D == 1 ? (long long)M.ncx : (long long)M.ncx * M.ncy);
-  const double dt = F.s->dt;
-  const int NBN = DIM == 3 ? 8 : 4;
-  const double wc = DIM == 2 ? .25 : .125;
-  const double wf = DIM == 2 ? .5 : .25;
-  const double* Xd = F.Xn[D];
-  double phi[5][NV];
-  double xc[5];
-  bool ex[5];
-  for (int s = 0; s < 5; ++s) {
-    int is = id + s - 2;
-    ex[s] = is >= 0 && is < nd;
-    if (!ex[s]) continue;
-    long long cs = c + (s - 2) * stride;
-    double u[NV];
-    for (int v = 0; v < NV; ++v) u[v] = A.Uin[v * N + cs];
-    double den;
-    if (A.first) den = F.V[cs];
-    else { den = 0.; for (int q = 0; q < NE; ++q) den += u[q]; }
-    for (int v = 0; v < NV; ++v) phi[s][v] = u[v] / den;
-    int ci = i, cj = j, ck = k;
-    if (D == 0) ci += s - 2; else if (D == 1) cj += s - 2; else ck += s - 2;
-    double sum = 0.;
-    for (int l = 0; l < NBN; ++l) {
-      int a, b, d;
-      local_node_offset(l, a, b, d);
-      sum += Xd[node_id(M, ci + a, cj + b, ck + d)];
-    }
-    xc[s] = wc * sum;
-  }
-  // faces: back (between s=1,2) and front (between s=2,3)
-  double fcd[2], un[2], L[2], ond[2];
-  for (int f = 0; f < 2; ++f) {
-    int fi = i, fj = j, fk = k;
-    if (D == 0) fi += f; else if (D == 1) fj += f; else fk += f;
-    long long fn[4];
-    int nfn = DIM == 3 ? 4 : 2;
-    double fc = 0., vm = 0.;
-    const double* vD = D == 0 ? F.vx : (D == 1 ? F.vy : F.vz);
-    for (int q = 0; q < nfn; ++q) {
-      int a, b, cz;
-      face_node_ijk<DIM, D>(fi, fj, fk, q, a, b, cz);
-      fn[q] = node_id(M, a, b, cz);
-      fc = fc + wf * Xd[fn[q]];
-      vm = vm + vD[fn[q]];
-    }
-    fcd[f] = fc;
-    un[f] = wf * vm;
-    if (DIM == 3) {
-      R3 x0 = {F.Xn[0][fn[0]], F.Xn[1][fn[0]], F.Xn[2][fn[0]]};
-      R3 x1 = {F.Xn[0][fn[1]], F.Xn[1][fn[1]], F.Xn[2][fn[1]]};
-      R3 x2 = {F.Xn[0][fn[2]], F.Xn[1][fn[2]], F.Xn[2][fn[2]]};
-      R3 x3 = {F.Xn[0][fn[3]], F.Xn[1][fn[3]], F.Xn[2][fn[3]]};
-      R3 v1 = x2 - x0, v2 = x3 - x1;
-      if (D == 0) L[f] = 0.5 * fabs(produit(v1.y, v2.z, v1.z, v2.y));
-      else if (D == 1) L[f] = 0.5 * fabs(produit(v2.x, v1.z, v2.z, v1.x));
-      else L[f] = 0.5 * fabs(produit(v1.x, v2.y, v1.y, v2.x));
-    } else {
-      const double* Xt = F.Xn[1 - D];
-      L[f] = fabs(Xt[fn[1]] - Xt[fn[0]]);
-    }
-    // outer normal of this cell at the face, from the initial grid
-    // (MahycoModule.cc:1070-1091)
-    R3 sc = {0., 0., 0.};
-    for (int l = 0; l < NBN; ++l) {
-      int a, b, d;
-      local_node_offset(l, a, b, d);
-      sc = sc + node_x0(M, i + a, j + b, k + d);
-    }
-    R3 cc0 = wc * sc;
-    R3 fc0 = {0., 0., 0.};
-    for (int q = 0; q < nfn; ++q) {
-      int a, b, cz;
-      face_node_ijk<DIM, D>(fi, fj, fk, q, a, b, cz);
-      fc0 = fc0 + wf * node_x0(M, a, b, cz);
-    }
-    R3 diff = fc0 - cc0;
-    ond[f] = comp(diff / norm(diff), D);
-  }
-  const int order2 = A.order - 1;
-  double* Uo = A.Uout;
-  double mf_out[NE];
-  for (int q = 0; q < NE; ++q) mf_out[q] = 0.;
-  double uo[NV];
-  for (int v = 0; v < NV; ++v) {
-    // face gradients (faces between s and s+1, s = 0..3)
-    double gface[4];
-    for (int s = 0; s < 4; ++s)
-      gface[s] = (ex[s] && ex[s + 1]) ? (phi[s + 1][v] - phi[s][v]) / (xc[s + 1] - xc[s]) : 0.;
-    double grad[5] = {0., 0., 0., 0., 0.};
-    if (A.order > 1)
-      for (int s = 1; s <= 3; ++s)
-        if (ex[s]) grad[s] = limited_gradient(A.limiter, gface[s - 1], gface[s]);
-    double flux[2] = {0., 0.};
-    bool fex[2] = {ex[1], ex[3]};
-    for (int f = 0; f < 2; ++f) {
-      if (!fex[f]) continue;
-      int sb = 1 + f, sf = 2 + f;
-      double dx = xc[sf] - xc[sb];
-      int su = (un[f] * dx > 0.0) ? sb : sf;
-      double pf = phi[su][v] + order2 * (fcd[f] - xc[su]) * grad[su];
-      flux[f] = ond[f] * un[f] * L[f] * dt * pf;
-    }
-    double ff = 0.;
-    double dual = 0.;
-    // cell local face order: 3D back then front; 2D x: front then back
-    int fa = (DIM == 2 && D == 0) ? 1 : 0, fb = 1 - fa;
-    if (fex[fa]) { ff += flux[fa]; dual += 0.5 * flux[fa] * ond[fa]; }
-    if (fex[fb]) { ff += flux[fb]; dual += 0.5 * flux[fb] * ond[fb]; }
-    uo[v] = A.Uin[v * N + c] - ff;
-    if (v >= NE && v < 2 * NE) mf_out[v - NE] = dual;
-  }
-  for (int q = 0; q < NE; ++q) {
-    if (uo[NE + q] < 0.) uo[NE + q] = 0.;
-    if (uo[2 * NE + q] < 0.) uo[2 * NE + q] = 0.;
-  }
-  for (int v = 0; v < NV; ++v) Uo[v * N + c] = uo[v];
-  for (int q = 0; q < NE; ++q) F.mflux[q * N + c] = mf_out[q];
-}
-
-// ---------------------------------------------------------------------------
-// remap sweep, node part: RemapADIService::computeDualUremap
-// (DualPhaseRemap.cc:38-258, classical limiter)
-// ---------------------------------------------------------------------------
-struct DualArgs {
-  const double* Uin;   // null on the first sweep (U built from m and v)
-  double* Uout;
-  int order;
-  int limiter;
-  int done_dirs;       // bit d: direction d already swept this cycle
-};
-
-template <int DIM>
-__device__ __forceinline__ bool node_inner(const Mesh& M, int i, int j, int k, int d) {
-  int id = d == 0 ? i : (d == 1 ? j : k);
-  int nn = d == 0 ? M.nnx : (d == 1 ? M.nny : M.nnz);
-  return id > 0 && id < nn - 1;
-}
-
-template <int DIM, int NE, int D>
-__global__ void __launch_bounds__(256) k_sweep_nodes(Mesh M, mhc_case_params P, Fields F, DualArgs A) {
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (n >= M.nnode) return;
-  const long long NN = M.nnode, N = M.ncell;
-  int i, j, k;
-  node_ijk(M, n, i, j, k);
-  const long long stride = D == 0 ? 1 : (D == 1 ? (long long)M.nnx : (long long)M.nnx * M.nny);
-  auto loadU = [&](long long m, double* U) {
-    if (A.Uin) {
-      for (int q = 0; q < 5; ++q) U[q] = A.Uin[q * NN + m];
-    } else {
-      double mn = F.mn[m], vx = F.vx[m], vy = F.vy[m], vz = F.vz[m];
-      U[0] = mn * vx; U[1] = mn * vy; U[2] = mn * vz; U[3] = mn;
-      U[4] = 0.5 * mn * (vx * vx + vy * vy + vz * vz);
-    }
-  };
-  double U[5];
-  loadU(n, U);
-  const bool inner = node_inner<DIM>(M, i, j, k, D);
-  if (!inner) {
-    for (int q = 0; q < 5; ++q) A.Uout[q * NN + n] = U[q];
-    return;
-  }
-  const int id = D == 0 ? i : (D == 1 ? j : k);
-  // Phi of nodes id-2..id+2 and their Lagrangian coordinate along D
-  double Ph[5][5], xd[5];
-  bool exn[5];
-  const int nn = D == 0 ? M.nnx : (D == 1 ? M.nny : M.nnz);
-  for (int s = 0; s < 5; ++s) {
-    int is = id + s - 2;
-    exn[s] = is >= 0 && is < nn;
-    if (!exn[s]) continue;
-    long long m = n + (s - 2) * stride;
-    xd[s] = F.Xn[D][m];
-    int mi = i, mj = j, mk = k;
-    if (D == 0) mi += s - 2; else if (D == 1) mj += s - 2; else mk += s - 2;
-    bool was_inner = false;
-    for (int d = 0; d < DIM; ++d)
-      if (((A.done_dirs >> d) & 1) && node_inner<DIM>(M, mi, mj, mk, d)) was_inner = true;
-    double Um[5];
-    loadU(m, Um);
-    if (was_inner) {
-      Ph[s][0] = Um[0] / Um[3]; Ph[s][1] = Um[1] / Um[3]; Ph[s][2] = Um[2] / Um[3];
-      Ph[s][3] = Um[3]; Ph[s][4] = Um[4] / Um[3];
-    } else {
-      double vx = F.vx[m], vy = F.vy[m], vz = F.vz[m];
-      Ph[s][0] = vx; Ph[s][1] = vy; Ph[s][2] = vz; Ph[s][3] = F.mn[m];
-      Ph[s][4] = 0.5 * (vx * vx + vy * vy + vz * vz);
-    }
-  }
-  // limited node gradients at id-1, id, id+1 (velocity components only)
-  double G[5][5];
-  for (int s = 0; s < 5; ++s)
-    for (int q = 0; q < 5; ++q) G[s][q] = 0.;
-  if (A.order > 1) {
-    for (int s = 1; s <= 3; ++s) {
-      int is = id + s - 2;
-      if (!(is > 0 && is < nn - 1)) continue;
-      for (int q = 0; q < 3; ++q) {
-        double gf = (Ph[s + 1][q] - Ph[s][q]) / (xd[s + 1] - xd[s]);
-        double gb = (Ph[s][q] - Ph[s - 1][q]) / (xd[s] - xd[s - 1]);
-        G[s][q] = limited_gradient(A.limiter, gb, gf);
-      }
-    }
-  }
-  // node mass fluxes: faces of the node plane in face id order, then envs
-  const double w = DIM == 2 ? .5 : .25;
-  double bfm = 0., ffm = 0.;
-  {
-    int nt1 = DIM == 3 ? 2 : 1;
-    for (int b2 = 0; b2 < nt1; ++b2) {
-      for (int b1 = 0; b1 < 2; ++b1) {
-        // transverse cell indices (t1 minor, t2 major)
-        int ci = i, cj = j, ck = k;
-        int t1 = b1 - 1, t2 = b2 - 1;
-        if (D == 0) { cj += t1; ck += (DIM == 3 ? t2 : 0); }
-        else if (D == 1) { ci += t1; ck += (DIM == 3 ? t2 : 0); }
-        else { ci += t1; cj += t2; }
-        if (ci < 0 || cj < 0 || ck < 0) continue;
-        if (D != 0 && ci >= M.ncx) continue;
-        if (D != 1 && cj >= M.ncy) continue;
-        if (DIM == 3 && D != 2 && ck >= M.ncz) continue;
-        // behind the plane: index along D = id-1; ahead: id
-        int bi = ci, bj = cj, bk = ck;
-        if (D == 0) bi = id - 1; else if (D == 1) bj = id - 1; else bk = id - 1;
-        int fi = ci, fj = cj, fk = ck;
-        if (D == 0) fi = id; else if (D == 1) fj = id; else fk = id;
-        int ndc = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
-        if (id - 1 >= 0) {
-          long long cb = cell_id(M, bi, bj, DIM == 3 ? bk : 0);
-          for (int q = 0; q < NE; ++q) bfm += w * F.mflux[q * N + cb];
-        }
-        if (id < ndc) {
-          long long cf = cell_id(M, fi, fj, DIM == 3 ? fk : 0);
-          for (int q = 0; q < NE; ++q) ffm += w * F.mflux[q * N + cf];
-        }
-      }
-    }
-  }
-  const double dt = F.s->dt;
-  const int order2 = A.order - 1;
-  U[3] += bfm - ffm;
-  double FV[3], BV[3], FE, BE;
-  {
-    double ufront = 0.5 * (Ph[2][D] + Ph[3][D]);
-    int signfront = (ufront > 0) ? 1 : -1;
-    int src = (ffm < 0.) ? 3 : 2;
-    double geo = (signfront * (xd[3] - xd[2]) - dt * ufront);
-    for (int q = 0; q < 3; ++q) FV[q] = Ph[src][q] + order2 * (0.5 * G[src][q] * geo);
-    FE = Ph[src][4] + order2 * (0.5 * G[src][4] * geo);
-  }
-  {
-    double uback = 0.5 * (Ph[1][D] + Ph[2][D]);
-    int signback = (uback > 0) ? 1 : -1;
-    int src = (bfm > 0.) ? 1 : 2;
-    double geo = (signback * (xd[2] - xd[1]) - dt * uback);
-    for (int q = 0; q < 3; ++q) BV[q] = Ph[src][q] + order2 * (0.5 * G[src][q] * geo);
-    BE = Ph[src][4] + order2 * (0.5 * G[src][4] * geo);
-  }
-  for (int q = 0; q < 3; ++q) U[q] += bfm * BV[q] - ffm * FV[q];
-  U[4] += bfm * BE - ffm * FE;
-  for (int q = 0; q < 3; ++q)
-    if (fabs(U[q]) < 1.e-300) U[q] = 0.;
-  for (int q = 0; q < 5; ++q) A.Uout[q * NN + n] = U[q];
-}
+// The remap sweeps (one direction, cells and nodes) live in mhc_sweep.cuh.
 
 // ---------------------------------------------------------------------------
 // remap finalize, cells: RemapADIService::remapVariables (RemapADIFinal.cc:21-319)
