@@ -142,6 +142,35 @@ int mhc_remap_apply(mhc_case* h);
  * weighted), present flag: 1 + 5*nb_env doubles. */
 int mhc_time_history(mhc_case* h, double* out);
 
+/* --- allocation-free CFL time step --------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory -- host codes that own all of their device
+ * memory through their own pool (as mesh frameworks do), or that run where
+ * allocation is not allowed -- and therefore cannot create a case.  It
+ * computes the deltat of computeDeltaT (MahycoModule.cc:1739-1833) from the
+ * caller's device buffers: cell char_length and sound_speed [ncell], node
+ * velocity components vx, vy, vz [nnode] (cartesian numbering, x fastest),
+ * and writes the new deltat to deltat_out[0] (device memory): cfl * min
+ * l/(c + vmax), bounded by 1.05*old_deltat and deltat_max; -2 when below
+ * deltat_min, -1 when a cell gives NaN.  Work is enqueued on `stream`
+ * (a cudaStream_t, or NULL).
+ *
+ * It calls no allocator: the per-block minima live in a fixed array inside
+ * the library (MHC_NOALLOC_SCRATCH_BYTES on every GPU that loads it, until
+ * the process exits), so meshes above MHC_NOALLOC_MAX_CELLS cells are
+ * rejected with MHC_ERR_ARG.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress); make that first call outside any
+ * stream capture.  All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.
+ * Errors: mhc_noalloc_last_error(). */
+#define MHC_NOALLOC_MAX_CELLS (1 << 22)
+#define MHC_NOALLOC_SCRATCH_BYTES (MHC_NOALLOC_MAX_CELLS / 256 * 8)
+int mhc_cfl_delta_t_noalloc(int dim, int nx, int ny, int nz, const double* char_length,
+                            const double* sound_speed, const double* vx, const double* vy,
+                            const double* vz, double cfl, double old_deltat, double deltat_max,
+                            double deltat_min, double* deltat_out, void* stream);
+const char* mhc_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,10 @@ _SIGS = {
     "mhc_eos_apply": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_remap_apply": (C.c_int, [C.c_void_p]),
     "mhc_time_history": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "mhc_cfl_delta_t_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
+    "mhc_noalloc_last_error": (C.c_char_p, []),
 }
 
 
