@@ -142,6 +142,36 @@ int mhc_remap_apply(mhc_case* h);
  * weighted), present flag: 1 + 5*nb_env doubles. */
 int mhc_time_history(mhc_case* h, double* out);
 
+/* --- batches: many independent cases, one launch per phase ---------------
+ * No counterpart in the reference (which runs one case per process).  All
+ * cases of a batch live on the device at once; mhc_batch_cycle advances
+ * every active case by n iterations with one persistent launch per kernel
+ * phase over a work list that covers all their blocks, whatever their mesh
+ * sizes.  A case stops advancing once it reaches its iteration limit, its
+ * final time or an error flag; its neighbours are unaffected.  Results are
+ * bit-identical to the same case run alone. */
+typedef struct mhc_batch mhc_batch;
+int mhc_batch_create(mhc_batch** out);
+int mhc_batch_destroy(mhc_batch* b);
+void* mhc_batch_stream(mhc_batch* b);
+/* add a case (device state allocated, not yet initialised); iteration_limit
+ * <= 0 means unlimited; *index identifies the case in this batch */
+int mhc_batch_add(mhc_batch* b, const mhc_case_params* params, long long iteration_limit, int* index);
+/* HydroStartInit of every case added since the last call */
+int mhc_batch_init(mhc_batch* b);
+/* retire a case and release its device memory */
+int mhc_batch_remove(mhc_batch* b, int index);
+int mhc_batch_cycle(mhc_batch* b, int n);
+/* same, replaying a CUDA graph of 6 iterations (one sweep-rotation period) */
+int mhc_batch_cycle_graph(mhc_batch* b, int n);
+int mhc_batch_cycle_timed(mhc_batch* b, int n, double* stage_ms, long long* stage_launches);
+int mhc_batch_synchronize(mhc_batch* b);
+/* launch grid of the phases: 0 (default) = one block per work item,
+ * k > 0 = k x the blocks the device can hold at once, striding the list */
+int mhc_batch_set_grid_scale(mhc_batch* b, int scale);
+int mhc_batch_get_scalars(mhc_batch* b, int index, double* time, double* deltat, long long* iteration, int* status);
+long long mhc_batch_get_field(mhc_batch* b, int index, const char* name, int env, double* host, long long capacity);
+
 /* --- allocation-free CFL time step --------------------------------------
  * No counterpart in the reference: an extra entry point for callers that
  * cannot allocate device memory -- host codes that own all of their device

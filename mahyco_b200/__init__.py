@@ -57,6 +57,21 @@ _SIGS = {
     "mhc_eos_apply": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_remap_apply": (C.c_int, [C.c_void_p]),
     "mhc_time_history": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "mhc_batch_create": (C.c_int, [C.POINTER(C.c_void_p)]),
+    "mhc_batch_destroy": (C.c_int, [C.c_void_p]),
+    "mhc_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "mhc_batch_add": (C.c_int, [C.c_void_p, C.POINTER(CaseParams), C.c_longlong, C.POINTER(C.c_int)]),
+    "mhc_batch_init": (C.c_int, [C.c_void_p]),
+    "mhc_batch_remove": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_batch_cycle": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_batch_cycle_graph": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_batch_cycle_timed": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    "mhc_batch_synchronize": (C.c_int, [C.c_void_p]),
+    "mhc_batch_set_grid_scale": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_batch_get_scalars": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
+    "mhc_batch_get_field": (C.c_longlong, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double),
+                                           C.c_longlong]),
     "mhc_cfl_delta_t_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
@@ -205,4 +220,82 @@ class Hydro:
         out = np.empty(1 + 5 * self.params.nb_env, dtype=np.float64)
         _check(self.lib, self.lib.mhc_time_history(self.h, out.ctypes.data_as(C.POINTER(C.c_double))),
                "time history")
+        return out
+
+
+class Batch:
+    """Many independent cases resident on the GPU, advanced together by one
+    persistent launch per kernel phase (``mhc_batch_*`` of the C ABI)."""
+
+    def __init__(self, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+        b = C.c_void_p()
+        _check(self.lib, self.lib.mhc_batch_create(C.byref(b)), "mhc_batch_create")
+        self.b = b
+        self.params = {}
+
+    def close(self):
+        if self.b:
+            self.lib.mhc_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self.lib.mhc_batch_stream(self.b))
+
+    def add(self, params: CaseParams, iteration_limit: int = 0) -> int:
+        idx = C.c_int()
+        _check(self.lib, self.lib.mhc_batch_add(self.b, C.byref(params), int(iteration_limit), C.byref(idx)),
+               "mhc_batch_add")
+        self.params[idx.value] = params
+        return idx.value
+
+    def init(self):
+        _check(self.lib, self.lib.mhc_batch_init(self.b), "mhc_batch_init")
+
+    def remove(self, idx: int):
+        _check(self.lib, self.lib.mhc_batch_remove(self.b, int(idx)), "mhc_batch_remove")
+        self.params.pop(idx, None)
+
+    def cycle(self, n: int, graph: bool = False):
+        f = self.lib.mhc_batch_cycle_graph if graph else self.lib.mhc_batch_cycle
+        _check(self.lib, f(self.b, int(n)), "mhc_batch_cycle")
+
+    def cycle_timed(self, n: int) -> dict:
+        ms = (C.c_double * len(Hydro.STAGES))()
+        ln = (C.c_longlong * len(Hydro.STAGES))()
+        _check(self.lib, self.lib.mhc_batch_cycle_timed(self.b, int(n), ms, ln), "mhc_batch_cycle_timed")
+        return {s: (ms[i], ln[i]) for i, s in enumerate(Hydro.STAGES)}
+
+    def synchronize(self):
+        _check(self.lib, self.lib.mhc_batch_synchronize(self.b), "mhc_batch_synchronize")
+
+    def set_grid_scale(self, scale: int):
+        _check(self.lib, self.lib.mhc_batch_set_grid_scale(self.b, int(scale)), "grid scale")
+
+    def scalars(self, idx: int) -> dict:
+        t, dt, it, st = C.c_double(), C.c_double(), C.c_longlong(), C.c_int()
+        _check(self.lib, self.lib.mhc_batch_get_scalars(self.b, int(idx), C.byref(t), C.byref(dt), C.byref(it),
+                                                        C.byref(st)), "batch scalars")
+        return {"time": t.value, "deltat": dt.value, "iteration": it.value, "status": st.value}
+
+    def field(self, idx: int, name: str, env: int = -1) -> np.ndarray:
+        p = self.params[idx]
+        n = 3 * p.nnode if name in ("Velocity", "NodeCoord") else (p.nnode if name == "NodeMass" else p.ncell)
+        out = np.empty(n, dtype=np.float64)
+        got = self.lib.mhc_batch_get_field(self.b, int(idx), name.encode(), int(env),
+                                           out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        _check(self.lib, int(got), f"batch field {name}")
         return out

@@ -1,15 +1,25 @@
-// mhc_capi.cu -- C ABI of the MaHyCo B200 library: case lifecycle, module
-// entry points (fused into kernel stages), fused cycles and field access.
+// mhc_capi.cu -- C ABI of the MaHyCo B200 library.
+//
+// Every launch goes through an Engine: a set of cases, their device
+// descriptors and one work list per (group, phase).  A case created with
+// mhc_case_create runs on a private engine holding only itself; a batch
+// (mhc_batch_*) runs many cases of uneven sizes through one persistent
+// launch per phase.  Cases are grouped by everything that selects a kernel
+// template: dimension, number of environments, remap on/off, the set of
+// one-cell-thick axes and the current sweep rotation.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/mahyco_b200.h"
-#include "mhc_kernels.cuh"
-#include "mhc_sweep.cuh"
+#include "mhc_launch.cuh"
 
 using namespace mhc;
 
@@ -19,18 +29,18 @@ int set_err(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
-#define CK(x)                                                                 \
-  do {                                                                        \
-    cudaError_t e_ = (x);                                                     \
-    if (e_ != cudaSuccess)                                                    \
-      return set_err(MHC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+#define CK(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess) return set_err(MHC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-enum Stage {
-  S_IDLE = 0, S_SAVED, S_VELOCITY, S_BC, S_POSITION, S_GEOM, S_DENSITY, S_VISCO,
-  S_ELASTO, S_ENERGY, S_REMAP
-};
+enum Stage { S_IDLE = 0, S_SAVED, S_VELOCITY, S_BC, S_POSITION, S_GEOM, S_DENSITY, S_VISCO, S_ELASTO, S_ENERGY, S_REMAP };
+
+inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
 }  // namespace
+
+struct Engine;
 
 struct mhc_case {
   mhc_case_params P;
@@ -38,41 +48,475 @@ struct mhc_case {
   int DIM = 3, NE = 1, NV = 4;
   Fields F;
   Scalars* d_scal = nullptr;
-  cudaStream_t stream = nullptr;
-  int sens_projection = 0;
+  mhc_case_params* d_params = nullptr;
+  cudaStream_t stream = nullptr;   // allocation stream (and launches when standalone)
+  bool own_stream = false;
+  std::vector<void*> allocs;
+  long long it_host = 1;           // iteration the next launched cycle runs
   int stage = S_IDLE;
   bool initialised = false;
-  std::vector<void*> allocs;
-  cudaGraphExec_t graph = nullptr;
-  int graph_n = 0;
-  size_t lagrange_smem = 0;
-  // optional per-stage timing: events recorded around every kernel group
+  Engine* solo = nullptr;          // private engine of a standalone case
+  int slot = -1;                   // index inside its engine
+};
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+struct DevList {
+  size_t off = 0;  // offset (in items) inside the engine list arena
+  int n = 0;
+};
+
+struct Group {
+  int DIM, NE, EULER, skip;
+  long long it0;               // iteration of the members when the lists were built
+  std::vector<int> members;
+  DevList init_cells, init_nodes, lag_nodes, lag_cells, fin_cells, fin_nodes, dt;
+  DevList sw_cells[3], sw_nodes[3];
+  DevList cases;               // offset into the case-index arena
+};
+
+struct Engine {
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<mhc_case*> cases;
+  CaseDesc* d_desc = nullptr;
+  int desc_cap = 0;
+  WorkItem* d_items = nullptr;
+  size_t items_cap = 0;
+  int* d_caseidx = nullptr;
+  size_t caseidx_cap = 0;
+  std::vector<Group> groups;
+  bool dirty = true;
+  long long cycles_since_build = 0;
+  int nsm = 0;
+  // timing
   bool timing = false;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   double stage_ms[MHC_NUM_STAGES] = {0};
   long long stage_launches[MHC_NUM_STAGES] = {0};
+  // graph of one rotation period
+  cudaGraphExec_t graph = nullptr;
+  // grid of the work-list launches: 0 = one block per work item (the block
+  // scheduler balances), k > 0 = k x the blocks the device holds at once
+  // (persistent blocks striding over the list)
+  int grid_scale = 0;
 };
 
-// brackets one kernel group with events on the case stream and accumulates
-// its device time (only when timing is enabled)
+namespace {
+
 struct StageTimer {
-  mhc_case* h;
+  Engine* e;
   int stage;
-  StageTimer(mhc_case* h_, int s) : h(h_), stage(s) {
-    if (h->timing) cudaEventRecord(h->ev[0], h->stream);
+  StageTimer(Engine* e_, int s) : e(e_), stage(s) {
+    if (e->timing) cudaEventRecord(e->ev[0], e->stream);
   }
   ~StageTimer() {
-    if (!h->timing) return;
-    cudaEventRecord(h->ev[1], h->stream);
-    cudaEventSynchronize(h->ev[1]);
+    if (!e->timing) return;
+    cudaEventRecord(e->ev[1], e->stream);
+    cudaEventSynchronize(e->ev[1]);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
-    h->stage_ms[stage] += ms;
-    h->stage_launches[stage] += 1;
+    cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+    e->stage_ms[stage] += ms;
+    e->stage_launches[stage] += 1;
   }
 };
 
-static long long count_doubles(const mhc_case_params* p, long long& ncell, long long& nnode) {
+template <int D>
+dim3 sweep_grid(int nx, int ny, int nz) {
+  using T = SweepTile<D>;
+  if (D == 0) return dim3(cdiv(nx, T::TD), ny, nz);
+  if (D == 1) return dim3(cdiv(nx, T::TW), cdiv(ny, T::TD), nz);
+  return dim3(cdiv(nx, T::TW), cdiv(nz, T::TD), ny);
+}
+
+dim3 sweep_grid_d(int D, int nx, int ny, int nz) {
+  return D == 0 ? sweep_grid<0>(nx, ny, nz) : (D == 1 ? sweep_grid<1>(nx, ny, nz) : sweep_grid<2>(nx, ny, nz));
+}
+
+// virtual blocks of the cell sweep (mhc_sweep2.cuh): x = XOUT-cell windows
+// along D, y = groups of SW_ROWS transverse rows
+dim3 cell_sweep_grid(int D, int nx, int ny, int nz) {
+  const int nd = D == 0 ? nx : (D == 1 ? ny : nz);
+  const long long rows = (long long)nx * ny * nz / nd;
+  return dim3(cdiv(nd, XOUT), (unsigned)cdiv(rows, SW_ROWS), 1);
+}
+
+int skip_mask(const mhc_case* h) {
+  int m = 0;
+  if (h->M.ncx == 1) m |= 1;
+  if (h->M.ncy == 1) m |= 2;
+  if (h->DIM == 3 && h->M.ncz == 1) m |= 4;
+  return m;
+}
+
+// persistent grid for a kernel: resident blocks on the device (cached)
+template <class K>
+int resident_blocks(Engine* e, K kernel, int threads, size_t smem) {
+  static std::map<const void*, int> cache;
+  auto it = cache.find((const void*)kernel);
+  if (it != cache.end()) return it->second * e->nsm;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  cache[(const void*)kernel] = per_sm;
+  return per_sm * e->nsm;
+}
+
+template <class K, class... Args>
+void plaunch(Engine* e, K kernel, int threads, size_t smem, const DevList& L, Args... args) {
+  if (L.n <= 0) return;
+  int grid = e->grid_scale == 0 ? L.n : std::min(L.n, resident_blocks(e, kernel, threads, smem) * e->grid_scale);
+  kernel<<<grid, threads, smem, e->stream>>>(e->d_desc, e->d_items + L.off, L.n, args...);
+}
+
+size_t lagrange_smem(int dim) {
+  return (size_t)(LTX + 1) * (LTY + 1) * ((dim == 3 ? 8 : 4) * 3 * sizeof(double) + 1);
+}
+
+// -- list building -----------------------------------------------------------
+int engine_rebuild(Engine* e) {
+  if (!e->dirty) return MHC_OK;
+  if (e->nsm == 0) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const int nc = (int)e->cases.size();
+  // descriptors
+  if (nc > e->desc_cap) {
+    if (e->d_desc) CK(cudaFreeAsync(e->d_desc, e->stream));
+    e->desc_cap = std::max(nc, 2 * e->desc_cap);
+    CK(cudaMallocAsync((void**)&e->d_desc, e->desc_cap * sizeof(CaseDesc), e->stream));
+  }
+  std::vector<CaseDesc> desc(nc);
+  for (int i = 0; i < nc; ++i) {
+    mhc_case* h = e->cases[i];
+    h->slot = i;
+    desc[i].M = h->M;
+    desc[i].F = h->F;
+    desc[i].P = h->d_params;
+  }
+  if (nc) CK(cudaMemcpyAsync(e->d_desc, desc.data(), nc * sizeof(CaseDesc), cudaMemcpyHostToDevice, e->stream));
+  // groups
+  std::map<std::tuple<int, int, int, int, int>, int> gidx;
+  e->groups.clear();
+  for (int i = 0; i < nc; ++i) {
+    mhc_case* h = e->cases[i];
+    int euler = h->P.with_projection ? 1 : 0;
+    int sens = (int)((h->it_host - 1) % h->DIM);
+    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens);
+    auto it = gidx.find(key);
+    if (it == gidx.end()) {
+      Group g;
+      g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
+      gidx[key] = (int)e->groups.size();
+      e->groups.push_back(g);
+      it = gidx.find(key);
+    }
+    e->groups[it->second].members.push_back(i);
+  }
+  // work items
+  std::vector<WorkItem> items;
+  std::vector<int> caseidx;
+  auto open = [&](DevList& L) { L.off = items.size(); L.n = 0; };
+  auto close_ = [&](DevList& L) { L.n = (int)(items.size() - L.off); };
+  auto cells1d = [&](const Group& g, DevList& L, bool nodes) {
+    open(L);
+    for (int c : g.members) {
+      const Mesh& M = e->cases[c]->M;
+      int nb = cdiv(nodes ? M.nnode : M.ncell, CT);
+      for (int b = 0; b < nb; ++b) items.push_back(WorkItem{c, b, 0, 0});
+    }
+    close_(L);
+  };
+  for (Group& g : e->groups) {
+    cells1d(g, g.init_cells, false);
+    cells1d(g, g.init_nodes, true);
+    cells1d(g, g.lag_cells, false);
+    cells1d(g, g.fin_cells, false);
+    cells1d(g, g.fin_nodes, true);
+    cells1d(g, g.dt, false);
+    open(g.lag_nodes);
+    for (int c : g.members) {
+      const Mesh& M = e->cases[c]->M;
+      int gz = g.DIM == 3 ? cdiv(M.nnz, LZCHUNK) : 1;
+      for (int z = 0; z < gz; ++z)
+        for (int y = 0; y < cdiv(M.nny, LTY); ++y)
+          for (int x = 0; x < cdiv(M.nnx, LTX); ++x) items.push_back(WorkItem{c, x, y, z});
+    }
+    close_(g.lag_nodes);
+    for (int D = 0; D < g.DIM; ++D) {
+      for (int pass = 0; pass < 2; ++pass) {
+        DevList& L = pass == 0 ? g.sw_cells[D] : g.sw_nodes[D];
+        open(L);
+        for (int c : g.members) {
+          const Mesh& M = e->cases[c]->M;
+          dim3 gr = pass == 0 ? cell_sweep_grid(D, M.ncx, M.ncy, M.ncz) : sweep_grid_d(D, M.nnx, M.nny, M.nnz);
+          for (unsigned z = 0; z < gr.z; ++z)
+            for (unsigned y = 0; y < gr.y; ++y)
+              for (unsigned x = 0; x < gr.x; ++x) items.push_back(WorkItem{c, (int)x, (int)y, (int)z});
+        }
+        close_(L);
+      }
+    }
+    g.cases.off = caseidx.size();
+    for (int c : g.members) caseidx.push_back(c);
+    g.cases.n = (int)g.members.size();
+  }
+  if (items.size() > e->items_cap) {
+    if (e->d_items) CK(cudaFreeAsync(e->d_items, e->stream));
+    e->items_cap = std::max(items.size(), 2 * e->items_cap);
+    CK(cudaMallocAsync((void**)&e->d_items, e->items_cap * sizeof(WorkItem), e->stream));
+  }
+  if (caseidx.size() > e->caseidx_cap) {
+    if (e->d_caseidx) CK(cudaFreeAsync(e->d_caseidx, e->stream));
+    e->caseidx_cap = std::max(caseidx.size(), 2 * e->caseidx_cap);
+    CK(cudaMallocAsync((void**)&e->d_caseidx, e->caseidx_cap * sizeof(int), e->stream));
+  }
+  if (!items.empty())
+    CK(cudaMemcpyAsync(e->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, e->stream));
+  if (!caseidx.empty())
+    CK(cudaMemcpyAsync(e->d_caseidx, caseidx.data(), caseidx.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  // the host vectors must outlive the async copies
+  CK(cudaStreamSynchronize(e->stream));
+  e->dirty = false;
+  e->cycles_since_build = 0;
+  if (e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  return MHC_OK;
+}
+
+// -- phase launches -------------------------------------------------------------
+#define DISPATCH_GROUP(g, CALL)                                   \
+  do {                                                            \
+    if ((g).DIM == 2) {                                           \
+      constexpr int DIM_ = 2;                                     \
+      switch ((g).NE) {                                           \
+        case 1: { constexpr int NE_ = 1; CALL; } break;           \
+        case 2: { constexpr int NE_ = 2; CALL; } break;           \
+        case 3: { constexpr int NE_ = 3; CALL; } break;           \
+        default: { constexpr int NE_ = 4; CALL; } break;          \
+      }                                                           \
+    } else {                                                      \
+      constexpr int DIM_ = 3;                                     \
+      switch ((g).NE) {                                           \
+        case 1: { constexpr int NE_ = 1; CALL; } break;           \
+        case 2: { constexpr int NE_ = 2; CALL; } break;           \
+        case 3: { constexpr int NE_ = 3; CALL; } break;           \
+        default: { constexpr int NE_ = 4; CALL; } break;          \
+      }                                                           \
+    }                                                             \
+  } while (0)
+
+void launch_init(Engine* e) {
+  for (Group& g : e->groups) {
+    DISPATCH_GROUP(g, (plaunch(e, kb_init_cells<DIM_, NE_>, CT, 0, g.init_cells)));
+    DISPATCH_GROUP(g, (plaunch(e, kb_init_nodes<DIM_>, CT, 0, g.init_nodes)));
+  }
+}
+
+template <int DIM>
+void lag_nodes_attr() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(kb_lagrange_nodes<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lagrange_smem(DIM));
+  done = true;
+}
+
+void launch_lagrange_nodes(Engine* e) {
+  StageTimer tm(e, MHC_STAGE_LAGRANGE_NODES);
+  for (Group& g : e->groups) {
+    if (g.DIM == 2) { lag_nodes_attr<2>(); plaunch(e, kb_lagrange_nodes<2>, LTX * LTY, lagrange_smem(2), g.lag_nodes); }
+    else { lag_nodes_attr<3>(); plaunch(e, kb_lagrange_nodes<3>, LTX * LTY, lagrange_smem(3), g.lag_nodes); }
+  }
+}
+
+void launch_lagrange_cells(Engine* e) {
+  StageTimer tm(e, MHC_STAGE_LAGRANGE_CELLS);
+  for (Group& g : e->groups) {
+    if (g.EULER) DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true>, CT, 0, g.lag_cells)));
+    else DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, false>, CT, 0, g.lag_cells)));
+  }
+}
+
+// directions swept this cycle by the members of a group (host mirror of
+// sweep_dirs in mhc_launch.cuh)
+int group_dirs(Engine* e, const Group& g, int* dirs) {
+  const int dim = g.DIM;
+  const long long it = g.it0 + e->cycles_since_build;
+  const int sens = (int)((it - 1) % dim);
+  int n = 0;
+  for (int i = 0; i < dim; ++i) {
+    int d = (i + sens) % dim;
+    if ((g.skip >> d) & 1) continue;
+    dirs[n++] = d;
+  }
+  return n;
+}
+
+template <int DIM, int NE>
+void sweep_step(Engine* e, Group& g, int D, int k) {
+  {
+    StageTimer tm(e, MHC_STAGE_SWEEP_CELLS);
+    if (D == 0) plaunch(e, kb_sweep_cells<DIM, NE, 0>, SW_THREADS, 0, g.sw_cells[0], k);
+    else if (D == 1) plaunch(e, kb_sweep_cells<DIM, NE, 1>, SW_THREADS, 0, g.sw_cells[1], k);
+    else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells<DIM, NE, 2>, SW_THREADS, 0, g.sw_cells[2], k);
+  }
+  {
+    StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
+    if (D == 0) plaunch(e, kb_sweep_nodes<DIM, NE, 0>, SweepTile<0>::THREADS, 0, g.sw_nodes[0], k);
+    else if (D == 1) plaunch(e, kb_sweep_nodes<DIM, NE, 1>, SweepTile<1>::THREADS, 0, g.sw_nodes[1], k);
+    else if constexpr (DIM == 3) plaunch(e, kb_sweep_nodes<DIM, NE, 2>, SweepTile<2>::THREADS, 0, g.sw_nodes[2], k);
+  }
+}
+
+// RemapADIService::appliRemap (RemapADIService.cc:15-90) for every group
+void launch_remap(Engine* e) {
+  for (int k = 0; k < 3; ++k) {
+    for (Group& g : e->groups) {
+      if (!g.EULER) continue;
+      int dirs[3];
+      int nd = group_dirs(e, g, dirs);
+      if (k >= nd) continue;
+      DISPATCH_GROUP(g, (sweep_step<DIM_, NE_>(e, g, dirs[k], k)));
+    }
+  }
+  for (Group& g : e->groups) {
+    if (!g.EULER) continue;
+    int dirs[3];
+    int K = group_dirs(e, g, dirs);
+    {
+      StageTimer tm(e, MHC_STAGE_FINALIZE_CELLS);
+      DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_cells<DIM_, NE_>, CT, 0, g.fin_cells, K)));
+    }
+    if (K > 0) {
+      StageTimer tm(e, MHC_STAGE_FINALIZE_NODES);
+      DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_nodes<DIM_>, CT, 0, g.fin_nodes, K)));
+    }
+  }
+}
+
+void launch_dt(Engine* e) {
+  StageTimer tm(e, MHC_STAGE_DELTA_T);
+  for (Group& g : e->groups) {
+    DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_>, CT, 0, g.dt)));
+    if (g.cases.n > 0)
+      kb_delta_t_finalize<<<cdiv(g.cases.n, 128), 128, 0, e->stream>>>(e->d_desc, e->d_caseidx + g.cases.off, g.cases.n);
+  }
+}
+
+void end_cycle(Engine* e) {
+  e->cycles_since_build += 1;
+  for (mhc_case* h : e->cases) h->it_host += 1;
+}
+
+void launch_cycle(Engine* e) {
+  launch_lagrange_nodes(e);
+  launch_lagrange_cells(e);
+  launch_remap(e);
+  launch_dt(e);
+  end_cycle(e);
+}
+
+int engine_cycle(Engine* e, int n) {
+  int r = engine_rebuild(e);
+  if (r) return r;
+  for (int it = 0; it < n; ++it) launch_cycle(e);
+  CK(cudaGetLastError());
+  return MHC_OK;
+}
+
+// CUDA graph of one rotation period: 6 iterations bring every 2D and 3D
+// group back to the same sweep order, so the same graph replays
+int engine_cycle_graph(Engine* e, int n) {
+  int r = engine_rebuild(e);
+  if (r) return r;
+  const int period = 6;
+  while (n > 0 && e->cycles_since_build % period != 0) {
+    launch_cycle(e);
+    --n;
+  }
+  if (n >= period && !e->graph) {
+    long long saved = e->cycles_since_build;
+    std::vector<long long> its;
+    for (mhc_case* h : e->cases) its.push_back(h->it_host);
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < period; ++it) launch_cycle(e);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (ce != cudaSuccess) return set_err(MHC_ERR_CUDA, cudaGetErrorString(ce));
+    CK(cudaGraphInstantiate(&e->graph, g, 0));
+    cudaGraphDestroy(g);
+    e->cycles_since_build = saved;
+    for (size_t i = 0; i < e->cases.size(); ++i) e->cases[i]->it_host = its[i];
+  }
+  while (n >= period && e->graph) {
+    CK(cudaGraphLaunch(e->graph, e->stream));
+    for (int it = 0; it < period; ++it) end_cycle(e);
+    n -= period;
+  }
+  for (; n > 0; --n) launch_cycle(e);
+  CK(cudaGetLastError());
+  return MHC_OK;
+}
+
+int engine_create(cudaStream_t stream, Engine** out) {
+  Engine* e = new Engine();
+  if (stream) {
+    e->stream = stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete e;
+      cudaGetLastError();
+      return set_err(MHC_ERR_CUDA, "stream creation failed (no CUDA device?)");
+    }
+    e->own_stream = true;
+  }
+  *out = e;
+  return MHC_OK;
+}
+
+void engine_release(Engine* e) {
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->d_desc) cudaFreeAsync(e->d_desc, e->stream);
+  if (e->d_items) cudaFreeAsync(e->d_items, e->stream);
+  if (e->d_caseidx) cudaFreeAsync(e->d_caseidx, e->stream);
+  for (int i = 0; i < 2; ++i)
+    if (e->ev[i]) cudaEventDestroy(e->ev[i]);
+  e->graph = nullptr; e->d_desc = nullptr; e->d_items = nullptr; e->d_caseidx = nullptr;
+  e->ev[0] = e->ev[1] = nullptr;
+}
+
+void engine_destroy(Engine* e) {
+  if (!e) return;
+  cudaStreamSynchronize(e->stream);
+  engine_release(e);
+  cudaStreamSynchronize(e->stream);
+  if (e->own_stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+int engine_timed(Engine* e, int n, double* stage_ms, long long* launches) {
+  if (!e->ev[0]) {
+    CK(cudaEventCreate(&e->ev[0]));
+    CK(cudaEventCreate(&e->ev[1]));
+  }
+  for (int s = 0; s < MHC_NUM_STAGES; ++s) { e->stage_ms[s] = 0.; e->stage_launches[s] = 0; }
+  e->timing = true;
+  int r = engine_cycle(e, n);
+  e->timing = false;
+  for (int s = 0; s < MHC_NUM_STAGES; ++s) {
+    stage_ms[s] = e->stage_ms[s];
+    if (launches) launches[s] = e->stage_launches[s];
+  }
+  return r;
+}
+
+// -- cases ------------------------------------------------------------------------
+long long count_doubles(const mhc_case_params* p, long long& ncell, long long& nnode) {
   int dim = p->dim;
   ncell = (long long)p->nx * p->ny * (dim == 3 ? p->nz : 1);
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
@@ -82,19 +526,7 @@ static long long count_doubles(const mhc_case_params* p, long long& ncell, long 
   return cells * ncell + nodes * nnode;
 }
 
-// the API functions take their C linkage from the declarations in mahyco_b200.h
-
-const char* mhc_last_error(void) { return g_err.c_str(); }
-const char* mhc_version(void) { return "mahyco_b200 0.1 (sm_100a, fp64)"; }
-
-long long mhc_case_device_bytes(const mhc_case_params* p) {
-  if (!p) return -1;
-  long long nc, nn;
-  long long d = count_doubles(p, nc, nn);
-  return d * 8 + nc + (long long)sizeof(Scalars);
-}
-
-static int validate(const mhc_case_params* p) {
+int validate(const mhc_case_params* p) {
   if (p->dim != 2 && p->dim != 3) return set_err(MHC_ERR_ARG, "dim must be 2 or 3");
   if (p->nx < 1 || p->ny < 1 || (p->dim == 3 && p->nz < 1)) return set_err(MHC_ERR_ARG, "mesh size");
   if (p->nb_env < 1 || p->nb_env > MHC_MAX_ENV) return set_err(MHC_ERR_ARG, "nb_env must be 1..4");
@@ -115,8 +547,20 @@ static int validate(const mhc_case_params* p) {
   return MHC_OK;
 }
 
-int mhc_case_create(const mhc_case_params* params, mhc_case** out) {
-  if (!params || !out) return set_err(MHC_ERR_ARG, "null argument");
+void case_free(mhc_case* h) {
+  if (!h) return;
+  if (h->solo) { engine_destroy(h->solo); h->solo = nullptr; }
+  if (h->stream) {
+    for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
+    cudaStreamSynchronize(h->stream);
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+  }
+  delete h;
+}
+
+// allocates the device state of one case on `stream` (stream-ordered pool);
+// a null stream gives the case a private stream
+int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** out) {
   *out = nullptr;
   int v = validate(params);
   if (v != MHC_OK) return v;
@@ -135,201 +579,71 @@ int mhc_case_create(const mhc_case_params* params, mhc_case** out) {
   M.h[0] = params->lx / params->nx;
   M.h[1] = params->ly / params->ny;
   M.h[2] = h->DIM == 3 ? params->lz / params->nz : 0.;
-  auto fail = [&](int code) { mhc_case_destroy(h); return code; };
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
-    return fail(set_err(MHC_ERR_CUDA, "stream creation failed"));
+  if (stream) {
+    h->stream = stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      delete h;
+      return set_err(MHC_ERR_CUDA, "stream creation failed (no CUDA device?)");
+    }
+    h->own_stream = true;
+  }
   const long long N = M.ncell, NN = M.nnode;
+  bool ok = true;
   auto alloc = [&](size_t bytes) -> void* {
     void* p = nullptr;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    if (!ok || cudaMallocAsync(&p, bytes, h->stream) != cudaSuccess) { ok = false; return nullptr; }
     h->allocs.push_back(p);
     return p;
   };
-  bool ok = true;
-  auto dcell = [&]() { double* p = (double*)alloc(N * sizeof(double)); ok = ok && p; return p; };
-  auto dnode = [&]() { double* p = (double*)alloc(NN * sizeof(double)); ok = ok && p; return p; };
+  auto dcell = [&]() { return (double*)alloc(N * sizeof(double)); };
+  auto dnode = [&]() { return (double*)alloc(NN * sizeof(double)); };
   Fields& F = h->F;
   memset(&F, 0, sizeof(F));
   F.rho = dcell(); F.e = dcell(); F.p = dcell(); F.c = dcell(); F.q = dcell();
   F.m = dcell(); F.V = dcell(); F.l = dcell(); F.Veul = dcell();
   if (h->NE > 1) {
-    auto denv = [&]() { double* p = (double*)alloc(h->NE * N * sizeof(double)); ok = ok && p; return p; };
+    auto denv = [&]() { return (double*)alloc(h->NE * N * sizeof(double)); };
     F.ef = denv(); F.emf = denv(); F.em = denv(); F.erho = denv();
     F.ee = denv(); F.ep = denv(); F.ec = denv(); F.eq = denv();
   }
   F.mask = (uint8_t*)alloc(N);
-  ok = ok && F.mask;
   F.vx = dnode(); F.vy = dnode(); F.vz = dnode(); F.mn = dnode();
-  for (int d = 0; d < 3; ++d) { F.Xp[d] = dnode(); F.Xn[d] = dnode(); }
+  for (int b = 0; b < 2; ++b)
+    for (int d = 0; d < 3; ++d) F.X[b][d] = dnode();
   for (int b = 0; b < 2; ++b) {
     F.U[b] = (double*)alloc(h->NV * N * sizeof(double));
     F.Ud[b] = (double*)alloc(5 * NN * sizeof(double));
-    ok = ok && F.U[b] && F.Ud[b];
   }
   F.mflux = (double*)alloc(h->NE * N * sizeof(double));
   h->d_scal = (Scalars*)alloc(sizeof(Scalars));
-  ok = ok && F.mflux && h->d_scal;
+  h->d_params = (mhc_case_params*)alloc(sizeof(mhc_case_params));
   F.s = h->d_scal;
   if (!ok) {
     cudaGetLastError();
-    return fail(set_err(MHC_ERR_NOMEM, "device allocation failed"));
+    case_free(h);
+    return set_err(MHC_ERR_NOMEM, "device allocation failed");
   }
   if (h->NE > 1) {
-    // env slots of cells that never hold the env must read as zero
+    // env slots of cells that never hold the env read as zero
     double* arr[] = {F.ef, F.emf, F.em, F.erho, F.ee, F.ep, F.ec, F.eq};
     for (double* a : arr)
-      if (cudaMemsetAsync(a, 0, h->NE * N * sizeof(double), h->stream) != cudaSuccess)
-        return fail(set_err(MHC_ERR_CUDA, "memset"));
+      if (cudaMemsetAsync(a, 0, h->NE * N * sizeof(double), h->stream) != cudaSuccess) {
+        case_free(h);
+        return set_err(MHC_ERR_CUDA, "memset");
+      }
   }
-  h->lagrange_smem = (size_t)(LTX + 1) * (LTY + 1) * ((h->DIM == 3 ? 8 : 4) * 3 * sizeof(double) + 1);
+  if (cudaMemcpyAsync(h->d_params, &h->P, sizeof(mhc_case_params), cudaMemcpyHostToDevice, h->stream) != cudaSuccess) {
+    case_free(h);
+    return set_err(MHC_ERR_CUDA, "params upload");
+  }
   *out = h;
   return MHC_OK;
 }
 
-void* mhc_case_stream(mhc_case* h) { return h ? (void*)h->stream : nullptr; }
-
-int mhc_case_destroy(mhc_case* h) {
-  if (!h) return MHC_OK;
-  if (h->stream) cudaStreamSynchronize(h->stream);
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  for (int i = 0; i < 2; ++i)
-    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
-  for (void* p : h->allocs) cudaFree(p);
-  if (h->stream) cudaStreamDestroy(h->stream);
-  delete h;
-  return MHC_OK;
-}
-
-// ---------------------------------------------------------------------------
-// template dispatch
-// ---------------------------------------------------------------------------
-static inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
-
-template <int DIM, int NE>
-static int launch_init(mhc_case* h) {
-  const int T = 256;
-  k_init_cells<DIM, NE><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F);
-  k_init_nodes<DIM><<<blocks_for(h->M.nnode, T), T, 0, h->stream>>>(h->M, h->P, h->F);
-  CK(cudaGetLastError());
-  return MHC_OK;
-}
-
-template <int DIM>
-static int launch_lagrange_nodes(mhc_case* h) {
-  StageTimer tm(h, MHC_STAGE_LAGRANGE_NODES);
-  static bool attr_set = false;
-  if (!attr_set) {
-    CK(cudaFuncSetAttribute(k_lagrange_nodes<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->lagrange_smem));
-    attr_set = true;
-  }
-  dim3 grid((h->M.nnx + LTX - 1) / LTX, (h->M.nny + LTY - 1) / LTY,
-            DIM == 3 ? (h->M.nnz + LZCHUNK - 1) / LZCHUNK : 1);
-  k_lagrange_nodes<DIM><<<grid, LTX * LTY, h->lagrange_smem, h->stream>>>(h->M, h->P, h->F, h->P.with_projection ? 1 : 0);
-  CK(cudaGetLastError());
-  return MHC_OK;
-}
-
-template <int DIM, int NE>
-static int launch_lagrange_cells(mhc_case* h) {
-  StageTimer tm(h, MHC_STAGE_LAGRANGE_CELLS);
-  const int T = 256;
-  if (h->P.with_projection)
-    k_lagrange_cells<DIM, NE, true><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F);
-  else
-    k_lagrange_cells<DIM, NE, false><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F);
-  CK(cudaGetLastError());
-  return MHC_OK;
-}
-
-// grid of the sweep tiles (SweepTile<D>): lanes along x, tile along D
-template <int D>
-static dim3 sweep_grid(int nx, int ny, int nz) {
-  using T = SweepTile<D>;
-  if (D == 0) return dim3((nx + T::TD - 1) / T::TD, ny, nz);
-  if (D == 1) return dim3((nx + T::TW - 1) / T::TW, (ny + T::TD - 1) / T::TD, nz);
-  return dim3((nx + T::TW - 1) / T::TW, (nz + T::TD - 1) / T::TD, ny);
-}
-
-template <int DIM, int NE, int D>
-static void launch_sweep_dir(mhc_case* h, SweepArgs sa, DualArgs da) {
-  const Mesh& M = h->M;
-  {
-    StageTimer tm(h, MHC_STAGE_SWEEP_CELLS);
-    k_sweep_cells<DIM, NE, D><<<sweep_grid<D>(M.ncx, M.ncy, M.ncz), SweepTile<D>::THREADS, 0, h->stream>>>(
-        h->M, h->P, h->F, sa);
-  }
-  {
-    StageTimer tm(h, MHC_STAGE_SWEEP_NODES);
-    k_sweep_nodes<DIM, NE, D><<<sweep_grid<D>(M.nnx, M.nny, M.nnz), SweepTile<D>::THREADS, 0, h->stream>>>(
-        h->M, h->P, h->F, da);
-  }
-}
-
-template <int DIM, int NE>
-static int launch_remap(mhc_case* h) {
-  // RemapADIService::appliRemap (RemapADIService.cc:15-90)
-  int ub = 0, udb = 0;
-  bool first = true;
-  int done = 0;
-  for (int i = 0; i < DIM; ++i) {
-    int d = (i + h->sens_projection) % DIM;
-    int ncd = d == 0 ? h->M.ncx : (d == 1 ? h->M.ncy : h->M.ncz);
-    if (ncd == 1) continue;
-    SweepArgs sa;
-    sa.Uin = h->F.U[ub];
-    sa.Uout = h->F.U[1 - ub];
-    sa.first = first ? 1 : 0;
-    sa.order = h->P.ordre_projection;
-    sa.limiter = h->P.projection_limiteur_id;
-    DualArgs da;
-    da.Uin = first ? nullptr : h->F.Ud[udb];
-    da.Uout = h->F.Ud[first ? 0 : 1 - udb];
-    da.order = h->P.ordre_projection;
-    da.limiter = h->P.projection_limiteur_id;
-    da.done_dirs = done;
-    if (d == 0) launch_sweep_dir<DIM, NE, 0>(h, sa, da);
-    else if (d == 1) launch_sweep_dir<DIM, NE, 1>(h, sa, da);
-    else if (DIM == 3) launch_sweep_dir<DIM, NE, (DIM == 3 ? 2 : 1)>(h, sa, da);
-    ub = 1 - ub;
-    udb = first ? 0 : 1 - udb;
-    first = false;
-    done |= 1 << d;
-  }
-  h->sens_projection = (h->sens_projection + 1) % DIM;
-  const double* Ufin = h->F.U[ub];
-  const double* Udfin = first ? nullptr : h->F.Ud[udb];
-  const int T = 256;
-  {
-    StageTimer tm(h, MHC_STAGE_FINALIZE_CELLS);
-    k_remap_finalize_cells<DIM, NE><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F, Ufin);
-  }
-  if (Udfin) {
-    StageTimer tm(h, MHC_STAGE_FINALIZE_NODES);
-    k_remap_finalize_nodes<DIM><<<blocks_for(h->M.nnode, T), T, 0, h->stream>>>(h->M, h->F, Udfin);
-  }
-  CK(cudaGetLastError());
-  return MHC_OK;
-}
-
-template <int DIM>
-static int launch_dt(mhc_case* h) {
-  StageTimer tm(h, MHC_STAGE_DELTA_T);
-  const int T = 256;
-  k_delta_t<DIM><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F);
-  k_delta_t_finalize<<<1, 1, 0, h->stream>>>(h->P, h->F);
-  CK(cudaGetLastError());
-  return MHC_OK;
-}
-
-#define DISPATCH_DN(fn, h)                                          \
-  ((h)->DIM == 2 ? ((h)->NE == 1 ? fn<2, 1>(h) : (h)->NE == 2 ? fn<2, 2>(h) \
-                    : (h)->NE == 3 ? fn<2, 3>(h) : fn<2, 4>(h))      \
-                 : ((h)->NE == 1 ? fn<3, 1>(h) : (h)->NE == 2 ? fn<3, 2>(h) \
-                    : (h)->NE == 3 ? fn<3, 3>(h) : fn<3, 4>(h)))
-#define DISPATCH_D(fn, h) ((h)->DIM == 2 ? fn<2>(h) : fn<3>(h))
-
-int mhc_hydro_start_init(mhc_case* h) {
-  if (!h) return set_err(MHC_ERR_ARG, "null case");
+// scalars of a case at start-init (iteration 1 about to run)
+int case_reset_scalars(mhc_case* h, long long iteration_limit) {
   Scalars s;
   memset(&s, 0, sizeof(s));
   s.t = h->P.deltat_init;  // global time of iteration 1
@@ -337,163 +651,36 @@ int mhc_hydro_start_init(mhc_case* h) {
   s.old_dt = 0.;
   s.iteration = 1;
   s.dt_min_bits = 0x7fefffffffffffffull;
+  s.iteration_limit = iteration_limit;
   CK(cudaMemcpyAsync(h->d_scal, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
-  int r = DISPATCH_DN(launch_init, h);
-  if (r != MHC_OK) return r;
-  h->sens_projection = 0;
-  h->stage = S_IDLE;
-  h->initialised = true;
-  return MHC_OK;
-}
-
-static void swap_positions(mhc_case* h) {
-  for (int d = 0; d < 3; ++d) std::swap(h->F.Xp[d], h->F.Xn[d]);
-}
-
-static int expect(mhc_case* h, int from, int to) {
-  if (!h) return set_err(MHC_ERR_ARG, "null case");
-  if (!h->initialised) return set_err(MHC_ERR_ORDER, "HydroStartInit has not run");
-  if (h->stage != from) return set_err(MHC_ERR_ORDER, "entry point called out of time-loop order");
-  h->stage = to;
-  return MHC_OK;
-}
-
-int mhc_save_values_at_n(mhc_case* h) { return expect(h, S_IDLE, S_SAVED); }
-int mhc_update_velocity(mhc_case* h) { return expect(h, S_SAVED, S_VELOCITY); }
-int mhc_apply_boundary_condition(mhc_case* h) { return expect(h, S_VELOCITY, S_BC); }
-int mhc_update_position(mhc_case* h) {
-  int r = expect(h, S_BC, S_POSITION);
-  if (r) return r;
-  return DISPATCH_D(launch_lagrange_nodes, h);
-}
-int mhc_compute_geometric_values(mhc_case* h) { return expect(h, S_POSITION, S_GEOM); }
-int mhc_update_density(mhc_case* h) { return expect(h, S_GEOM, S_DENSITY); }
-int mhc_compute_artificial_viscosity(mhc_case* h) { return expect(h, S_DENSITY, S_VISCO); }
-int mhc_update_elasticity_and_plasticity(mhc_case* h) { return expect(h, S_VISCO, S_ELASTO); }
-int mhc_update_energy_and_pressure(mhc_case* h) {
-  int r = expect(h, S_ELASTO, S_ENERGY);
-  if (r) return r;
-  return DISPATCH_DN(launch_lagrange_cells, h);
-}
-int mhc_remap(mhc_case* h) {
-  int r = expect(h, S_ENERGY, S_REMAP);
-  if (r) return r;
-  if (!h->P.with_projection) return MHC_OK;
-  return DISPATCH_DN(launch_remap, h);
-}
-int mhc_remap_apply(mhc_case* h) { return mhc_remap(h); }
-int mhc_compute_delta_t(mhc_case* h) {
-  int r = expect(h, S_REMAP, S_IDLE);
-  if (r) return r;
-  r = DISPATCH_D(launch_dt, h);
-  swap_positions(h);
-  return r;
-}
-
-static int one_iteration(mhc_case* h) {
-  int r;
-  if ((r = mhc_save_values_at_n(h))) return r;
-  if ((r = mhc_update_velocity(h))) return r;
-  if ((r = mhc_apply_boundary_condition(h))) return r;
-  if ((r = mhc_update_position(h))) return r;
-  if ((r = mhc_compute_geometric_values(h))) return r;
-  if ((r = mhc_update_density(h))) return r;
-  if ((r = mhc_compute_artificial_viscosity(h))) return r;
-  if ((r = mhc_update_elasticity_and_plasticity(h))) return r;
-  if ((r = mhc_update_energy_and_pressure(h))) return r;
-  if ((r = mhc_remap(h))) return r;
-  return mhc_compute_delta_t(h);
-}
-
-int mhc_cycle(mhc_case* h, int n) {
-  if (!h) return set_err(MHC_ERR_ARG, "null case");
-  for (int it = 0; it < n; ++it) {
-    int r = one_iteration(h);
-    if (r) return r;
-  }
-  return MHC_OK;
-}
-
-int mhc_cycle_graph(mhc_case* h, int n) {
-  if (!h) return set_err(MHC_ERR_ARG, "null case");
-  if (n <= 0) return MHC_OK;
-  // the captured sequence depends on the direction rotation and on the
-  // position buffer parity; a graph of dim*2 iterations returns both to
-  // their starting state, so only multiples of that period are replayed
-  const int period = 2 * h->DIM;
-  if (n % period != 0 || h->stage != S_IDLE) return mhc_cycle(h, n);
-  if (!h->graph || h->graph_n != period) {
-    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
-    int sp = h->sens_projection;
-    double* xp[3] = {h->F.Xp[0], h->F.Xp[1], h->F.Xp[2]};
-    double* xn[3] = {h->F.Xn[0], h->F.Xn[1], h->F.Xn[2]};
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int r = mhc_cycle(h, period);
-    cudaGraph_t gg;
-    cudaError_t e = cudaStreamEndCapture(h->stream, &gg);
-    if (r) return r;
-    if (e != cudaSuccess) return set_err(MHC_ERR_CUDA, cudaGetErrorString(e));
-    g = gg;
-    CK(cudaGraphInstantiate(&h->graph, g, 0));
-    cudaGraphDestroy(g);
-    h->graph_n = period;
-    // capture did not execute anything: restore the host-side state
-    h->sens_projection = sp;
-    for (int d = 0; d < 3; ++d) { h->F.Xp[d] = xp[d]; h->F.Xn[d] = xn[d]; }
-  }
-  for (int r = 0; r < n / period; ++r) CK(cudaGraphLaunch(h->graph, h->stream));
-  // host mirror of the state advanced by the replayed iterations
-  h->sens_projection = (h->sens_projection + n) % h->DIM;
-  if ((n & 1) != 0) swap_positions(h);
-  return MHC_OK;
-}
-
-int mhc_cycle_timed(mhc_case* h, int n, double* stage_ms, long long* stage_launches) {
-  if (!h || !stage_ms) return set_err(MHC_ERR_ARG, "null argument");
-  if (!h->ev[0]) {
-    CK(cudaEventCreate(&h->ev[0]));
-    CK(cudaEventCreate(&h->ev[1]));
-  }
-  for (int s = 0; s < MHC_NUM_STAGES; ++s) { h->stage_ms[s] = 0.; h->stage_launches[s] = 0; }
-  h->timing = true;
-  int r = mhc_cycle(h, n);
-  h->timing = false;
-  for (int s = 0; s < MHC_NUM_STAGES; ++s) {
-    stage_ms[s] = h->stage_ms[s];
-    if (stage_launches) stage_launches[s] = h->stage_launches[s];
-  }
-  return r;
-}
-
-int mhc_synchronize(mhc_case* h) {
-  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  // the host copies (scalars, params) must stay valid until the copies ran
   CK(cudaStreamSynchronize(h->stream));
-  Scalars s;
-  CK(cudaMemcpy(&s, h->d_scal, sizeof(s), cudaMemcpyDeviceToHost));
-  return s.status;
-}
-
-int mhc_get_scalars(mhc_case* h, double* time, double* deltat, long long* iteration, int* status) {
-  if (!h) return set_err(MHC_ERR_ARG, "null case");
-  CK(cudaStreamSynchronize(h->stream));
-  Scalars s;
-  CK(cudaMemcpy(&s, h->d_scal, sizeof(s), cudaMemcpyDeviceToHost));
-  if (time) *time = s.t_done;
-  if (deltat) *deltat = s.dt;
-  if (iteration) *iteration = s.iteration_done;
-  if (status) *status = s.status;
+  h->it_host = 1;
   return MHC_OK;
 }
 
-static int fetch(mhc_case* h, const void* dev, void* host, size_t bytes) {
-  CK(cudaStreamSynchronize(h->stream));
+int solo_engine(mhc_case* h) {
+  if (h->solo) return MHC_OK;
+  int r = engine_create(h->stream, &h->solo);
+  if (r) return r;
+  h->solo->cases.push_back(h);
+  h->solo->dirty = true;
+  return MHC_OK;
+}
+
+int fetch(cudaStream_t s, const void* dev, void* host, size_t bytes) {
+  CK(cudaStreamSynchronize(s));
   CK(cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost));
   return MHC_OK;
 }
 
-long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, long long cap) {
-  if (!h || !name || !host) return set_err(MHC_ERR_ARG, "null argument");
+int read_scalars(mhc_case* h, cudaStream_t s, Scalars* out) {
+  CK(cudaStreamSynchronize(s));
+  CK(cudaMemcpy(out, h->d_scal, sizeof(Scalars), cudaMemcpyDeviceToHost));
+  return MHC_OK;
+}
+
+long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env, double* host, long long cap) {
   const long long N = h->M.ncell, NN = h->M.nnode;
   Fields& F = h->F;
   struct { const char* n; double* g; double* e; } cells[] = {
@@ -508,25 +695,22 @@ long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, lo
     std::vector<double> g(N, 0.), e;
     std::vector<uint8_t> mask(N);
     int r;
-    if ((r = fetch(h, F.mask, mask.data(), N))) return r;
-    if (c.g) { if ((r = fetch(h, c.g, g.data(), N * 8))) return r; }
+    if ((r = fetch(st, F.mask, mask.data(), N))) return r;
+    if (c.g) { if ((r = fetch(st, c.g, g.data(), N * 8))) return r; }
     if (env < 0) {
-      if (!c.g) {  // global fraction of a cell: 1 for pure cells, not defined for mixed ones
-        for (long long i = 0; i < N; ++i) host[i] = 1.;
-      } else {
-        memcpy(host, g.data(), N * 8);
-      }
+      if (!c.g) for (long long i = 0; i < N; ++i) host[i] = 1.;
+      else memcpy(host, g.data(), N * 8);
       return N;
     }
     if (h->NE > 1 && c.e) {
       e.resize(N);
-      if ((r = fetch(h, c.e + env * N, e.data(), N * 8))) return r;
+      if ((r = fetch(st, c.e + env * N, e.data(), N * 8))) return r;
     }
     const bool volume = !strcmp(name, "CellVolume");
     std::vector<double> fr;
     if (volume && h->NE > 1) {
       fr.resize(N);
-      if ((r = fetch(h, F.ef + env * N, fr.data(), N * 8))) return r;
+      if ((r = fetch(st, F.ef + env * N, fr.data(), N * 8))) return r;
     }
     for (long long i = 0; i < N; ++i) {
       bool in = (mask[i] >> env) & 1;
@@ -541,14 +725,14 @@ long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, lo
   if (!strcmp(name, "EnvMask")) {
     if (cap < N) return set_err(MHC_ERR_ARG, "capacity too small");
     std::vector<uint8_t> mask(N);
-    int r = fetch(h, F.mask, mask.data(), N);
+    int r = fetch(st, F.mask, mask.data(), N);
     if (r) return r;
     for (long long i = 0; i < N; ++i) host[i] = mask[i];
     return N;
   }
   if (!strcmp(name, "NodeMass")) {
     if (cap < NN) return set_err(MHC_ERR_ARG, "capacity too small");
-    int r = fetch(h, F.mn, host, NN * 8);
+    int r = fetch(st, F.mn, host, NN * 8);
     return r ? r : NN;
   }
   if (!strcmp(name, "Velocity") || !strcmp(name, "NodeCoord")) {
@@ -556,10 +740,16 @@ long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, lo
     std::vector<double> a(NN), b(NN), c(NN);
     const double *pa, *pb, *pc;
     if (name[0] == 'V') { pa = F.vx; pb = F.vy; pc = F.vz; }
-    else { pa = F.Xp[0]; pb = F.Xp[1]; pc = F.Xp[2]; }  // last Lagrangian positions
+    else {
+      // last Lagrangian positions: X of the last completed iteration
+      Scalars s;
+      int r = read_scalars(h, st, &s);
+      if (r) return r;
+      int par = (int)(s.iteration_done & 1);
+      pa = F.X[par][0]; pb = F.X[par][1]; pc = F.X[par][2];
+    }
     int r;
-    if ((r = fetch(h, pa, a.data(), NN * 8)) || (r = fetch(h, pb, b.data(), NN * 8)) ||
-        (r = fetch(h, pc, c.data(), NN * 8)))
+    if ((r = fetch(st, pa, a.data(), NN * 8)) || (r = fetch(st, pb, b.data(), NN * 8)) || (r = fetch(st, pc, c.data(), NN * 8)))
       return r;
     for (long long i = 0; i < NN; ++i) { host[3 * i] = a[i]; host[3 * i + 1] = b[i]; host[3 * i + 2] = c[i]; }
     return 3 * NN;
@@ -567,41 +757,20 @@ long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, lo
   return set_err(MHC_ERR_ARG, std::string("unknown field ") + name);
 }
 
-template <int NE>
-static int launch_eos(mhc_case* h, int env) {
-  const int T = 256;
-  k_eos_apply<NE><<<blocks_for(h->M.ncell, T), T, 0, h->stream>>>(h->M, h->P, h->F, env);
-  CK(cudaGetLastError());
-  return MHC_OK;
-}
-
-int mhc_eos_apply(mhc_case* h, int env) {
-  if (!h) return set_err(MHC_ERR_ARG, "null case");
-  if (env < 0 || env >= h->NE) return set_err(MHC_ERR_ARG, "env out of range");
-  switch (h->NE) {
-    case 1: return launch_eos<1>(h, env);
-    case 2: return launch_eos<2>(h, env);
-    case 3: return launch_eos<3>(h, env);
-    default: return launch_eos<4>(h, env);
-  }
-}
-
-int mhc_time_history(mhc_case* h, double* out) {
-  if (!h || !out) return set_err(MHC_ERR_ARG, "null argument");
+int case_time_history(mhc_case* h, cudaStream_t st, double* out) {
   const long long N = h->M.ncell;
-  const int NE = h->NE;
-  double t;
-  int r = mhc_get_scalars(h, &t, nullptr, nullptr, nullptr);
+  Scalars s;
+  int r = read_scalars(h, st, &s);
   if (r) return r;
-  out[0] = t;
+  out[0] = s.t_done;
   std::vector<double> m(N), p(N), rho(N), e(N), V(N), env(N);
-  for (int q = 0; q < NE; ++q) {
-    if (mhc_get_field(h, "CellMass", q, m.data(), N) < 0) return MHC_ERR_CUDA;
-    if (mhc_get_field(h, "Pressure", q, p.data(), N) < 0) return MHC_ERR_CUDA;
-    if (mhc_get_field(h, "Density", q, rho.data(), N) < 0) return MHC_ERR_CUDA;
-    if (mhc_get_field(h, "InternalEnergy", q, e.data(), N) < 0) return MHC_ERR_CUDA;
-    if (mhc_get_field(h, "CellVolume", q, V.data(), N) < 0) return MHC_ERR_CUDA;
-    if (mhc_get_field(h, "EnvMask", -1, env.data(), N) < 0) return MHC_ERR_CUDA;
+  if (case_get_field(h, st, "EnvMask", -1, env.data(), N) < 0) return MHC_ERR_CUDA;
+  for (int q = 0; q < h->NE; ++q) {
+    if (case_get_field(h, st, "CellMass", q, m.data(), N) < 0 || case_get_field(h, st, "Pressure", q, p.data(), N) < 0 ||
+        case_get_field(h, st, "Density", q, rho.data(), N) < 0 ||
+        case_get_field(h, st, "InternalEnergy", q, e.data(), N) < 0 ||
+        case_get_field(h, st, "CellVolume", q, V.data(), N) < 0)
+      return MHC_ERR_CUDA;
     long long cnt = 0;
     double sm = 0., sp = 0., rv = 0., vv = 0., em = 0., mm = 0.;
     for (long long c = 0; c < N; ++c) {
@@ -625,3 +794,277 @@ int mhc_time_history(mhc_case* h, double* out) {
   return MHC_OK;
 }
 
+}  // namespace
+
+// ===========================================================================
+// C ABI (linkage from the declarations in mahyco_b200.h)
+// ===========================================================================
+const char* mhc_last_error(void) { return g_err.c_str(); }
+const char* mhc_version(void) { return "mahyco_b200 0.2 (sm_100a, fp64, batched engine)"; }
+
+long long mhc_case_device_bytes(const mhc_case_params* p) {
+  if (!p) return -1;
+  long long nc, nn;
+  long long d = count_doubles(p, nc, nn);
+  return d * 8 + nc + (long long)sizeof(Scalars) + (long long)sizeof(mhc_case_params);
+}
+
+int mhc_case_create(const mhc_case_params* params, mhc_case** out) {
+  if (!params || !out) return set_err(MHC_ERR_ARG, "null argument");
+  return case_alloc(params, nullptr, out);
+}
+
+void* mhc_case_stream(mhc_case* h) { return h ? (void*)h->stream : nullptr; }
+
+int mhc_case_destroy(mhc_case* h) {
+  case_free(h);
+  return MHC_OK;
+}
+
+int mhc_hydro_start_init(mhc_case* h) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  int r = case_reset_scalars(h, LLONG_MAX);
+  if (r) return r;
+  if ((r = solo_engine(h))) return r;
+  h->solo->dirty = true;
+  if ((r = engine_rebuild(h->solo))) return r;
+  launch_init(h->solo);
+  CK(cudaGetLastError());
+  h->stage = S_IDLE;
+  h->initialised = true;
+  return MHC_OK;
+}
+
+static int expect(mhc_case* h, int from, int to) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  if (!h->initialised) return set_err(MHC_ERR_ORDER, "HydroStartInit has not run");
+  if (h->stage != from) return set_err(MHC_ERR_ORDER, "entry point called out of time-loop order");
+  h->stage = to;
+  return MHC_OK;
+}
+
+int mhc_save_values_at_n(mhc_case* h) { return expect(h, S_IDLE, S_SAVED); }
+int mhc_update_velocity(mhc_case* h) { return expect(h, S_SAVED, S_VELOCITY); }
+int mhc_apply_boundary_condition(mhc_case* h) { return expect(h, S_VELOCITY, S_BC); }
+int mhc_update_position(mhc_case* h) {
+  int r = expect(h, S_BC, S_POSITION);
+  if (r) return r;
+  if ((r = engine_rebuild(h->solo))) return r;
+  launch_lagrange_nodes(h->solo);
+  CK(cudaGetLastError());
+  return MHC_OK;
+}
+int mhc_compute_geometric_values(mhc_case* h) { return expect(h, S_POSITION, S_GEOM); }
+int mhc_update_density(mhc_case* h) { return expect(h, S_GEOM, S_DENSITY); }
+int mhc_compute_artificial_viscosity(mhc_case* h) { return expect(h, S_DENSITY, S_VISCO); }
+int mhc_update_elasticity_and_plasticity(mhc_case* h) { return expect(h, S_VISCO, S_ELASTO); }
+int mhc_update_energy_and_pressure(mhc_case* h) {
+  int r = expect(h, S_ELASTO, S_ENERGY);
+  if (r) return r;
+  launch_lagrange_cells(h->solo);
+  CK(cudaGetLastError());
+  return MHC_OK;
+}
+int mhc_remap(mhc_case* h) {
+  int r = expect(h, S_ENERGY, S_REMAP);
+  if (r) return r;
+  launch_remap(h->solo);
+  CK(cudaGetLastError());
+  return MHC_OK;
+}
+int mhc_remap_apply(mhc_case* h) { return mhc_remap(h); }
+int mhc_compute_delta_t(mhc_case* h) {
+  int r = expect(h, S_REMAP, S_IDLE);
+  if (r) return r;
+  launch_dt(h->solo);
+  end_cycle(h->solo);
+  CK(cudaGetLastError());
+  return MHC_OK;
+}
+
+int mhc_cycle(mhc_case* h, int n) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  if (!h->initialised) return set_err(MHC_ERR_ORDER, "HydroStartInit has not run");
+  if (h->stage != S_IDLE) return set_err(MHC_ERR_ORDER, "an iteration is in progress");
+  return engine_cycle(h->solo, n);
+}
+
+int mhc_cycle_graph(mhc_case* h, int n) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  if (!h->initialised) return set_err(MHC_ERR_ORDER, "HydroStartInit has not run");
+  if (h->stage != S_IDLE) return set_err(MHC_ERR_ORDER, "an iteration is in progress");
+  return engine_cycle_graph(h->solo, n);
+}
+
+int mhc_cycle_timed(mhc_case* h, int n, double* stage_ms, long long* stage_launches) {
+  if (!h || !stage_ms) return set_err(MHC_ERR_ARG, "null argument");
+  if (!h->initialised) return set_err(MHC_ERR_ORDER, "HydroStartInit has not run");
+  return engine_timed(h->solo, n, stage_ms, stage_launches);
+}
+
+int mhc_synchronize(mhc_case* h) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  Scalars s;
+  int r = read_scalars(h, h->stream, &s);
+  return r ? r : s.status;
+}
+
+int mhc_get_scalars(mhc_case* h, double* time, double* deltat, long long* iteration, int* status) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  Scalars s;
+  int r = read_scalars(h, h->stream, &s);
+  if (r) return r;
+  if (time) *time = s.t_done;
+  if (deltat) *deltat = s.dt;
+  if (iteration) *iteration = s.iteration_done;
+  if (status) *status = s.status;
+  return MHC_OK;
+}
+
+long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, long long cap) {
+  if (!h || !name || !host) return set_err(MHC_ERR_ARG, "null argument");
+  return case_get_field(h, h->stream, name, env, host, cap);
+}
+
+int mhc_eos_apply(mhc_case* h, int env) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  if (env < 0 || env >= h->NE) return set_err(MHC_ERR_ARG, "env out of range");
+  int r = solo_engine(h);
+  if (r || (r = engine_rebuild(h->solo))) return r;
+  Engine* e = h->solo;
+  for (Group& g : e->groups) {
+    switch (g.NE) {
+      case 1: plaunch(e, kb_eos_apply<1>, CT, 0, g.init_cells, env); break;
+      case 2: plaunch(e, kb_eos_apply<2>, CT, 0, g.init_cells, env); break;
+      case 3: plaunch(e, kb_eos_apply<3>, CT, 0, g.init_cells, env); break;
+      default: plaunch(e, kb_eos_apply<4>, CT, 0, g.init_cells, env); break;
+    }
+  }
+  CK(cudaGetLastError());
+  return MHC_OK;
+}
+
+int mhc_time_history(mhc_case* h, double* out) {
+  if (!h || !out) return set_err(MHC_ERR_ARG, "null argument");
+  return case_time_history(h, h->stream, out);
+}
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+struct mhc_batch {
+  Engine* e = nullptr;
+  std::vector<mhc_case*> slots;   // case index -> case (nullptr once removed)
+};
+
+int mhc_batch_create(mhc_batch** out) {
+  if (!out) return set_err(MHC_ERR_ARG, "null argument");
+  mhc_batch* b = new mhc_batch();
+  int r = engine_create(nullptr, &b->e);
+  if (r) { delete b; return r; }
+  *out = b;
+  return MHC_OK;
+}
+
+int mhc_batch_destroy(mhc_batch* b) {
+  if (!b) return MHC_OK;
+  cudaStreamSynchronize(b->e->stream);
+  for (mhc_case* h : b->slots) case_free(h);
+  engine_destroy(b->e);
+  delete b;
+  return MHC_OK;
+}
+
+void* mhc_batch_stream(mhc_batch* b) { return b ? (void*)b->e->stream : nullptr; }
+
+int mhc_batch_add(mhc_batch* b, const mhc_case_params* params, long long iteration_limit, int* index) {
+  if (!b || !params || !index) return set_err(MHC_ERR_ARG, "null argument");
+  mhc_case* h = nullptr;
+  int r = case_alloc(params, b->e->stream, &h);
+  if (r) return r;
+  if ((r = case_reset_scalars(h, iteration_limit > 0 ? iteration_limit : LLONG_MAX))) { case_free(h); return r; }
+  h->initialised = false;
+  *index = (int)b->slots.size();
+  b->slots.push_back(h);
+  b->e->cases.push_back(h);
+  b->e->dirty = true;
+  return MHC_OK;
+}
+
+int mhc_batch_init(mhc_batch* b) {
+  if (!b) return set_err(MHC_ERR_ARG, "null batch");
+  // start-init of the cases that have not run yet, through a temporary engine
+  Engine* tmp = nullptr;
+  int r = engine_create(b->e->stream, &tmp);
+  if (r) return r;
+  for (mhc_case* h : b->e->cases)
+    if (!h->initialised) tmp->cases.push_back(h);
+  if (!tmp->cases.empty()) {
+    if ((r = engine_rebuild(tmp))) { engine_destroy(tmp); return r; }
+    launch_init(tmp);
+    for (mhc_case* h : tmp->cases) h->initialised = true;
+  }
+  cudaError_t ce = cudaGetLastError();
+  engine_destroy(tmp);
+  if (ce != cudaSuccess) return set_err(MHC_ERR_CUDA, cudaGetErrorString(ce));
+  b->e->dirty = true;
+  return MHC_OK;
+}
+
+int mhc_batch_remove(mhc_batch* b, int index) {
+  if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
+  mhc_case* h = b->slots[index];
+  cudaStreamSynchronize(b->e->stream);
+  auto& v = b->e->cases;
+  v.erase(std::remove(v.begin(), v.end(), h), v.end());
+  b->e->dirty = true;
+  case_free(h);
+  b->slots[index] = nullptr;
+  return MHC_OK;
+}
+
+int mhc_batch_cycle(mhc_batch* b, int n) {
+  if (!b) return set_err(MHC_ERR_ARG, "null batch");
+  return engine_cycle(b->e, n);
+}
+
+int mhc_batch_cycle_graph(mhc_batch* b, int n) {
+  if (!b) return set_err(MHC_ERR_ARG, "null batch");
+  return engine_cycle_graph(b->e, n);
+}
+
+int mhc_batch_cycle_timed(mhc_batch* b, int n, double* stage_ms, long long* stage_launches) {
+  if (!b || !stage_ms) return set_err(MHC_ERR_ARG, "null argument");
+  return engine_timed(b->e, n, stage_ms, stage_launches);
+}
+
+int mhc_batch_synchronize(mhc_batch* b) {
+  if (!b) return set_err(MHC_ERR_ARG, "null batch");
+  CK(cudaStreamSynchronize(b->e->stream));
+  return MHC_OK;
+}
+
+int mhc_batch_set_grid_scale(mhc_batch* b, int scale) {
+  if (!b || scale < 0 || scale > 64) return set_err(MHC_ERR_ARG, "grid scale must be 0..64");
+  b->e->grid_scale = scale;
+  if (b->e->graph) { cudaGraphExecDestroy(b->e->graph); b->e->graph = nullptr; }
+  return MHC_OK;
+}
+
+int mhc_batch_get_scalars(mhc_batch* b, int index, double* time, double* deltat, long long* iteration, int* status) {
+  if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
+  Scalars s;
+  int r = read_scalars(b->slots[index], b->e->stream, &s);
+  if (r) return r;
+  if (time) *time = s.t_done;
+  if (deltat) *deltat = s.dt;
+  if (iteration) *iteration = s.iteration_done;
+  if (status) *status = s.status;
+  return MHC_OK;
+}
+
+long long mhc_batch_get_field(mhc_batch* b, int index, const char* name, int env, double* host, long long cap) {
+  if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index] || !name || !host)
+    return set_err(MHC_ERR_ARG, "bad argument");
+  return case_get_field(b->slots[index], b->e->stream, name, env, host, cap);
+}

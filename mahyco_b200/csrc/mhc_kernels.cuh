@@ -34,6 +34,7 @@ struct Scalars {
   long long iteration;       // iteration in progress (1-based)
   long long iteration_done;  // last completed iteration
   unsigned long long dt_min_bits;  // running min of l/(c+vmax) as ordered bits
+  long long iteration_limit;  // last iteration this case may run
   int status;        // ST_* flags
   int pad;
 };
@@ -43,12 +44,33 @@ struct Fields {
   double *ef, *emf, *em, *erho, *ee, *ep, *ec, *eq;
   uint8_t* mask;
   double *vx, *vy, *vz, *mn;
-  double *Xp[3], *Xn[3];
+  double* X[2][3];         // Lagrangian positions, alternating by iteration
+  double *Xp[3], *Xn[3];   // X of the previous / current iteration (resolved per launch)
   double* U[2];
   double* mflux;
   double* Ud[2];
   Scalars* s;
 };
+
+// the previous cycle's Lagrangian positions are X[(iteration-1)&1], this
+// cycle's are X[iteration&1]
+// (selects rather than a runtime index, so the struct stays in registers)
+__device__ __forceinline__ void resolve_positions(Fields& F) {
+  const bool odd = ((F.s->iteration - 1) & 1) != 0;
+  F.Xp[0] = odd ? F.X[1][0] : F.X[0][0];
+  F.Xp[1] = odd ? F.X[1][1] : F.X[0][1];
+  F.Xp[2] = odd ? F.X[1][2] : F.X[0][2];
+  F.Xn[0] = odd ? F.X[0][0] : F.X[1][0];
+  F.Xn[1] = odd ? F.X[0][1] : F.X[1][1];
+  F.Xn[2] = odd ? F.X[0][2] : F.X[1][2];
+}
+
+// a case takes part in a launch only while it is below its iteration limit
+// and has no error flag (a stop or an error retires it on the device)
+__device__ __forceinline__ bool case_active(const Fields& F) {
+  const Scalars* s = F.s;
+  return s->status == 0 && s->iteration <= s->iteration_limit;
+}
 
 // ---------------------------------------------------------------------------
 // equations of state
@@ -146,9 +168,11 @@ __device__ __forceinline__ bool node_on_surface(const Mesh& M, int i, int j, int
 // ---------------------------------------------------------------------------
 // init: MahycoModule::hydroStartInit + computeCellMass (MahycoModule.cc:21-237)
 // ---------------------------------------------------------------------------
+constexpr int CT = 256;  // threads of the one-dimensional cell / node kernels
+
 template <int DIM, int NE>
-__global__ void k_init_cells(Mesh M, mhc_case_params P, Fields F) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  long long c = bx * (long long)CT + threadIdx.x;
   if (c >= M.ncell) return;
   const long long N = M.ncell;
   int i, j, k;
@@ -289,8 +313,8 @@ __device__ __forceinline__ double node_mass_gather(const Mesh& M, const double* 
 }
 
 template <int DIM>
-__global__ void k_init_nodes(Mesh M, mhc_case_params P, Fields F) {
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  long long n = bx * (long long)CT + threadIdx.x;
   if (n >= M.nnode) return;
   int i, j, k;
   node_ijk(M, n, i, j, k);
@@ -320,13 +344,15 @@ constexpr int LTX = 16, LTY = 16;
 constexpr int LZCHUNK = 16;
 
 template <int DIM>
-__global__ void __launch_bounds__(LTX * LTY) k_lagrange_nodes(Mesh M, mhc_case_params P, Fields F, int euler) {
+__device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F,
+                                                    int bx, int by, int bz) {
+  const int euler = P.with_projection ? 1 : 0;
   constexpr int CW = LTX + 1, CH = LTY + 1, NCL = CW * CH;
   extern __shared__ double smem_dyn[];
   double* corner = smem_dyn;  // [NCL][NBN][3] corner forces of one cell layer
   unsigned char* cvalid = reinterpret_cast<unsigned char*>(smem_dyn + NCL * (DIM == 3 ? 8 : 4) * 3);
   const int tx = threadIdx.x % LTX, ty = threadIdx.x / LTX;
-  const int i0 = blockIdx.x * LTX, j0 = blockIdx.y * LTY;
+  const int i0 = bx * LTX, j0 = by * LTY;
   const int ni = i0 + tx, nj = j0 + ty;
   const bool node_ok = ni < M.nnx && nj < M.nny;
   const int NBN = DIM == 3 ? 8 : 4;
@@ -335,7 +361,7 @@ __global__ void __launch_bounds__(LTX * LTY) k_lagrange_nodes(Mesh M, mhc_case_p
   const double t = F.s->t;
   int kz0 = 0, kz1 = 1;
   if (DIM == 3) {
-    kz0 = blockIdx.z * LZCHUNK;
+    kz0 = bz * LZCHUNK;
     kz1 = min(kz0 + LZCHUNK, M.nnz);
   }
   R3 S = {0., 0., 0.};
@@ -424,8 +450,8 @@ __global__ void __launch_bounds__(LTX * LTY) k_lagrange_nodes(Mesh M, mhc_case_p
 // (Lagrange-only time loop).
 // ---------------------------------------------------------------------------
 template <int DIM, int NE, bool EULER>
-__global__ void __launch_bounds__(256) k_lagrange_cells(Mesh M, mhc_case_params P, Fields F) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  long long c = bx * (long long)CT + threadIdx.x;
   if (c >= M.ncell) return;
   const long long N = M.ncell;
   constexpr int NV = 3 * NE + 1;
@@ -569,8 +595,9 @@ __global__ void __launch_bounds__(256) k_lagrange_cells(Mesh M, mhc_case_params 
 // (PrepareRemap.cc:242-249, MahycoModule.cc:1708-1735)
 // ---------------------------------------------------------------------------
 template <int DIM, int NE>
-__global__ void __launch_bounds__(256) k_remap_finalize_cells(Mesh M, mhc_case_params P, Fields F, const double* Ufin) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const mhc_case_params& P, const Fields& F,
+                                                          const double* Ufin, int bx) {
+  long long c = bx * (long long)CT + threadIdx.x;
   if (c >= M.ncell) return;
   const long long N = M.ncell;
   constexpr int NV = 3 * NE + 1;
@@ -726,8 +753,8 @@ __global__ void __launch_bounds__(256) k_remap_finalize_cells(Mesh M, mhc_case_p
 // remap finalize, nodes: velocity from projected momentum and node mass
 // rebuilt from the new cell masses (RemapADIFinal.cc:287-319)
 template <int DIM>
-__global__ void __launch_bounds__(256) k_remap_finalize_nodes(Mesh M, Fields F, const double* Ud) {
-  long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void body_remap_finalize_nodes(const Mesh& M, const Fields& F, const double* Ud, int bx) {
+  long long n = bx * (long long)CT + threadIdx.x;
   if (n >= M.nnode) return;
   const long long NN = M.nnode;
   double m = Ud[3 * NN + n];
@@ -747,8 +774,8 @@ __global__ void __launch_bounds__(256) k_remap_finalize_nodes(Mesh M, Fields F, 
 // non-NaN values does not depend on the reduction order.
 // ---------------------------------------------------------------------------
 template <int DIM>
-__global__ void __launch_bounds__(256) k_delta_t(Mesh M, mhc_case_params P, Fields F) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void body_delta_t(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  long long c = bx * (long long)CT + threadIdx.x;
   double dx = 1.7976931348623157e308;
   if (c < M.ncell) {
     int i, j, k;
@@ -772,7 +799,7 @@ __global__ void __launch_bounds__(256) k_delta_t(Mesh M, mhc_case_params P, Fiel
   if (lane == 0) red[wid] = dx;
   __syncthreads();
   if (wid == 0) {
-    dx = (lane < (blockDim.x + 31) / 32) ? red[lane] : 1.7976931348623157e308;
+    dx = (lane < CT / 32) ? red[lane] : 1.7976931348623157e308;
     for (int o = 16; o > 0; o >>= 1) dx = fmin(dx, __shfl_xor_sync(0xffffffffu, dx, o));
     if (lane == 0) atomicMin(&F.s->dt_min_bits, (unsigned long long)__double_as_longlong(dx));
   }
@@ -781,8 +808,8 @@ __global__ void __launch_bounds__(256) k_delta_t(Mesh M, mhc_case_params P, Fiel
 // standalone IEquationOfState::applyEOS(env) on the current state of the
 // environment cells, followed by computePressionMoyenne for mixed cells
 template <int NE>
-__global__ void __launch_bounds__(256) k_eos_apply(Mesh M, mhc_case_params P, Fields F, int env) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void body_eos_apply(const Mesh& M, const mhc_case_params& P, const Fields& F, int env, int bx) {
+  long long c = bx * (long long)CT + threadIdx.x;
   if (c >= M.ncell) return;
   const long long N = M.ncell;
   const uint8_t mask = F.mask[c];
@@ -810,7 +837,7 @@ __global__ void __launch_bounds__(256) k_eos_apply(Mesh M, mhc_case_params P, Fi
 }
 
 // end of iteration: new deltat, stop test, advance to the next iteration
-__global__ void k_delta_t_finalize(mhc_case_params P, Fields F) {
+__device__ __forceinline__ void body_delta_t_finalize(const mhc_case_params& P, const Fields& F) {
   Scalars* s = F.s;
   double old = s->dt;
   double new_dt;

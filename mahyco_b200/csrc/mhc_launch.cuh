@@ -1,0 +1,190 @@
+// mhc_launch.cuh -- persistent kernels that run one phase of the cycle over
+// a work list of (case, virtual block) items.
+//
+// A single case is a work list over its own blocks; a batch of uneven cases
+// is one list per phase covering every block of every case, so one launch
+// per phase advances all of them.  Blocks stride over the list; the case
+// descriptor of each item gives its mesh, fields and parameters.  Items of a
+// case that is stopped, failed or past its iteration limit are skipped (the
+// test is uniform per block).
+#pragma once
+#include "mhc_kernels.cuh"
+#include "mhc_sweep.cuh"
+#include "mhc_sweep2.cuh"
+
+namespace mhc {
+
+struct CaseDesc {
+  Mesh M;
+  Fields F;
+  const mhc_case_params* P;  // device copy of the case parameters
+};
+
+struct WorkItem {
+  int c;        // case index in the descriptor table
+  int x, y, z;  // virtual block index inside the case
+};
+
+#define MHC_FOR_ITEMS(W, n)                                      \
+  for (int w_ = blockIdx.x; w_ < (n); w_ += gridDim.x)
+
+template <int DIM, int NE>
+__global__ void __launch_bounds__(CT) kb_init_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_init_cells<DIM, NE>(M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_init_nodes<DIM>(M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(LTX * LTY) kb_lagrange_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_lagrange_nodes<DIM>(M, *C[wi.c].P, F, wi.x, wi.y, wi.z);
+    __syncthreads();
+  }
+}
+
+template <int DIM, int NE, bool EULER>
+__global__ void __launch_bounds__(CT) kb_lagrange_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_lagrange_cells<DIM, NE, EULER>(M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+// k-th performed sweep of the cycle in direction D: U[k&1] -> U[(k+1)&1]
+template <int DIM, int NE, int D>
+__global__ void __launch_bounds__(SW_THREADS)
+kb_sweep_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int k) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const mhc_case_params& P = *C[wi.c].P;
+    SweepArgs A;
+    A.Uin = (k & 1) ? F.U[1] : F.U[0];
+    A.Uout = (k & 1) ? F.U[0] : F.U[1];
+    A.first = k == 0;
+    A.order = P.ordre_projection;
+    A.limiter = P.projection_limiteur_id;
+    const Mesh M = C[wi.c].M;
+    body_sweep_cells_lanes<DIM, NE, D>(M, F, A, wi.x, wi.y);
+  }
+}
+
+template <int DIM, int NE, int D>
+__global__ void __launch_bounds__(SweepTile<D>::THREADS)
+kb_sweep_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int k) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    const mhc_case_params& P = *C[wi.c].P;
+    // directions swept before step k this cycle (RemapADIService.cc:23-33)
+    int done = 0;
+    {
+      const int sens = (int)((F.s->iteration - 1) % M.dim);
+      int cnt = 0;
+      for (int i = 0; i < M.dim; ++i) {
+        const int d = (i + sens) % M.dim;
+        const int ncd = d == 0 ? M.ncx : (d == 1 ? M.ncy : M.ncz);
+        if (ncd == 1) continue;
+        if (cnt < k) done |= 1 << d;
+        ++cnt;
+      }
+    }
+    DualArgs A;
+    A.Uin = k == 0 ? nullptr : (((k - 1) & 1) ? F.Ud[1] : F.Ud[0]);
+    A.Uout = (k & 1) ? F.Ud[1] : F.Ud[0];
+    A.order = P.ordre_projection;
+    A.limiter = P.projection_limiteur_id;
+    A.done_dirs = done;
+    body_sweep_nodes<DIM, NE, D>(M, P, F, A, VB{wi.x, wi.y, wi.z});
+    __syncthreads();
+  }
+}
+
+// remap finalize after K performed sweeps: cells read U[K&1], nodes Ud[(K-1)&1]
+template <int DIM, int NE>
+__global__ void __launch_bounds__(CT) kb_remap_finalize_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int K) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_remap_finalize_cells<DIM, NE>(M, *C[wi.c].P, F, (K & 1) ? F.U[1] : F.U[0], wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int K) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_remap_finalize_nodes<DIM>(M, F, ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_delta_t(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_delta_t<DIM>(M, *C[wi.c].P, F, wi.x);
+    __syncthreads();
+  }
+}
+
+// one thread per case
+__global__ void kb_delta_t_finalize(const CaseDesc* __restrict__ C, const int* __restrict__ cases, int n) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const CaseDesc& cd = C[cases[t]];
+    if (!case_active(cd.F)) continue;
+    body_delta_t_finalize(*cd.P, cd.F);
+  }
+}
+
+template <int NE>
+__global__ void __launch_bounds__(CT) kb_eos_apply(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int env) {
+  MHC_FOR_ITEMS(W, n) {
+    const WorkItem wi = W[w_];
+    Fields F = C[wi.c].F;
+    const Mesh M = C[wi.c].M;
+    body_eos_apply<NE>(M, *C[wi.c].P, F, env, wi.x);
+  }
+}
+
+}  // namespace mhc

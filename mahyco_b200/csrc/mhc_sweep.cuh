@@ -1,13 +1,12 @@
-// mhc_sweep.cuh -- one direction of the ADI remap, tiled along the sweep.
+// mhc_sweep.cuh -- node part of one direction of the ADI remap, tiled along
+// the sweep.
 //
-// Blocks own a tile of TD cells (nodes) along the sweep direction D times TW
-// lanes along x (TW = 1 for the x sweep, whose tile then runs along x).  Each
-// tile reads its cells once plus two halo cells on each side into shared
-// memory, and every intermediate of the reference -- phi, face gradient,
-// limited cell gradient, upwind face value -- is computed once per cell or
-// face and shared by the neighbours, with the operation order of the
-// reference function it replaces.  Variables are processed one at a time so
-// the shared footprint does not grow with the number of environments.
+// Blocks own a tile of TD nodes along the sweep direction D times TW lanes
+// along x (TW = 1 for the x sweep, whose tile then runs along x).  Each tile
+// reads its nodes once plus two halo nodes on each side into shared memory,
+// and every intermediate of the reference -- phi, limited gradient -- is
+// computed once per node and shared by the neighbours, with the operation
+// order of the reference function it replaces.
 #pragma once
 #include "mhc_kernels.cuh"
 
@@ -21,12 +20,14 @@ template <int D> struct SweepTile {
 };
 
 // cell (or node) coordinates of tile slot s (along D) and lane tw
+struct VB { int x, y, z; };  // virtual block index of a tile
+
 template <int D>
-__device__ __forceinline__ void tile_coord(int s, int tw, int& i, int& j, int& k) {
+__device__ __forceinline__ void tile_coord(const VB& b, int s, int tw, int& i, int& j, int& k) {
   constexpr int TW = SweepTile<D>::TW, TD = SweepTile<D>::TD;
-  if (D == 0) { i = blockIdx.x * TD + s; j = blockIdx.y; k = blockIdx.z; }
-  else if (D == 1) { i = blockIdx.x * TW + tw; j = blockIdx.y * TD + s; k = blockIdx.z; }
-  else { i = blockIdx.x * TW + tw; j = blockIdx.z; k = blockIdx.y * TD + s; }
+  if (D == 0) { i = b.x * TD + s; j = b.y; k = b.z; }
+  else if (D == 1) { i = b.x * TW + tw; j = b.y * TD + s; k = b.z; }
+  else { i = b.x * TW + tw; j = b.z; k = b.y * TD + s; }
 }
 
 template <int D>
@@ -40,15 +41,8 @@ struct SweepArgs {
   int limiter;
 };
 
-// ---------------------------------------------------------------------------
-// cell part: computeGradPhiFace + computeGradPhiCell +
-// computeUpwindFaceQuantitiesForProjection + computeUremap
-// (RemapADIService.cc:119-575, UtilesRemap.cc:108-120, 325-357; classical
-// limiters, order <= 2).  Face quantities of the Lagrangian mesh
-// (PrepareRemap.cc:18-59) are rebuilt from the node positions; the initial
-// face normals are the unit axis vectors of the cartesian grid, so every
-// dot(., n) of the reference reduces to the D component.
-// ---------------------------------------------------------------------------
+// face node q (in the order of the reference face, smallest node id first)
+// of the face normal to D whose lowest node is (i, j, k)
 template <int DIM, int D>
 __device__ __forceinline__ void face_node_ijk2(int i, int j, int k, int q, int& a, int& b, int& cz) {
   a = i; b = j; cz = k;
@@ -60,182 +54,6 @@ __device__ __forceinline__ void face_node_ijk2(int i, int j, int k, int q, int& 
   if (D == 0) { b += s1; cz += s2; }
   else if (D == 1) { a += s1; cz += s2; }
   else { a += s1; b += s2; }
-}
-
-template <int DIM, int NE, int D>
-__global__ void __launch_bounds__(SweepTile<D>::THREADS)
-k_sweep_cells(Mesh M, mhc_case_params P, Fields F, SweepArgs A) {
-  using T = SweepTile<D>;
-  constexpr int TW = T::TW, TD = T::TD, NS = T::NS;
-  constexpr int NV = 3 * NE + 1;
-  __shared__ double s_den[NS * TW];     // phi denominator per slot
-  __shared__ double s_xc[NS * TW];      // Lagrangian cell centre along D
-  __shared__ double s_phi[NS * TW];     // phi of the current variable
-  __shared__ double s_gf[(NS - 1) * TW];  // face gradient, then upwind face value
-  __shared__ double s_gr[(NS - 2) * TW];  // limited cell gradient (slots -1 .. TD)
-  __shared__ double s_un[(TD + 1) * TW], s_L[(TD + 1) * TW], s_fc[(TD + 1) * TW];
-  __shared__ unsigned char s_ok[NS * TW];
-  const long long N = M.ncell;
-  const int nd = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
-  const double dt = F.s->dt;
-  const int NBN = DIM == 3 ? 8 : 4;
-  const double wc = DIM == 2 ? .25 : .125;
-  const double wf = DIM == 2 ? .5 : .25;
-  const double* Xd = F.Xn[D];
-  const double* vD = D == 0 ? F.vx : (D == 1 ? F.vy : F.vz);
-  const int tid = threadIdx.x;
-
-  // stage 0: slots (cells) -- validity, phi denominator, centre along D;
-  // faces 0..TD (back face of slots 0..TD) -- Lagrangian geometry
-  for (int it = tid; it < NS * TW; it += T::THREADS) {
-    const int tw = it % TW, s = it / TW - 2;
-    int i, j, k;
-    tile_coord<D>(s, tw, i, j, k);
-    const int a = along<D>(i, j, k);
-    bool ok = a >= 0 && a < nd && i < M.ncx && j < M.ncy && (DIM == 2 || k < M.ncz);
-    s_ok[it] = ok;
-    if (!ok) continue;
-    const long long c = cell_id(M, i, j, k);
-    double den;
-    if (A.first) den = F.V[c];
-    else { den = 0.; for (int q = 0; q < NE; ++q) den += A.Uin[q * N + c]; }
-    s_den[it] = den;
-    double sum = 0.;
-    for (int l = 0; l < NBN; ++l) {
-      int da, db, dc;
-      local_node_offset(l, da, db, dc);
-      sum += Xd[node_id(M, i + da, j + db, k + dc)];
-    }
-    s_xc[it] = wc * sum;
-    if (s >= 0 && s <= TD) {
-      // back face of this cell
-      long long fn[4];
-      const int nfn = DIM == 3 ? 4 : 2;
-      double fc = 0., vm = 0.;
-      for (int q = 0; q < nfn; ++q) {
-        int fa, fb, fz;
-        face_node_ijk2<DIM, D>(i, j, k, q, fa, fb, fz);
-        fn[q] = node_id(M, fa, fb, fz);
-        fc = fc + wf * Xd[fn[q]];
-        vm = vm + vD[fn[q]];
-      }
-      double L;
-      if (DIM == 3) {
-        R3 x0 = {F.Xn[0][fn[0]], F.Xn[1][fn[0]], F.Xn[2][fn[0]]};
-        R3 x1 = {F.Xn[0][fn[1]], F.Xn[1][fn[1]], F.Xn[2][fn[1]]};
-        R3 x2 = {F.Xn[0][fn[2]], F.Xn[1][fn[2]], F.Xn[2][fn[2]]};
-        R3 x3 = {F.Xn[0][fn[3]], F.Xn[1][fn[3]], F.Xn[2][fn[3]]};
-        R3 v1 = x2 - x0, v2 = x3 - x1;
-        if (D == 0) L = 0.5 * fabs(produit(v1.y, v2.z, v1.z, v2.y));
-        else if (D == 1) L = 0.5 * fabs(produit(v2.x, v1.z, v2.z, v1.x));
-        else L = 0.5 * fabs(produit(v1.x, v2.y, v1.y, v2.x));
-      } else {
-        const double* Xt = F.Xn[1 - D];
-        L = fabs(Xt[fn[1]] - Xt[fn[0]]);
-      }
-      const int f = s * TW + tw;
-      s_fc[f] = fc;
-      s_un[f] = wf * vm;
-      s_L[f] = L;
-    }
-  }
-  // own cell: outer normals (initial grid, MahycoModule.cc:1070-1091)
-  const int tw0 = tid % TW, s0 = tid / TW;
-  int i0, j0, k0;
-  tile_coord<D>(s0, tw0, i0, j0, k0);
-  const int me = (s0 + 2) * TW + tw0;
-  __syncthreads();
-  const bool mine = s_ok[me];
-  double ond[2] = {0., 0.};
-  long long c0 = 0;
-  if (mine) {
-    c0 = cell_id(M, i0, j0, k0);
-    R3 sc = {0., 0., 0.};
-    for (int l = 0; l < NBN; ++l) {
-      int da, db, dc;
-      local_node_offset(l, da, db, dc);
-      sc = sc + node_x0(M, i0 + da, j0 + db, k0 + dc);
-    }
-    const R3 cc0 = wc * sc;
-    for (int f = 0; f < 2; ++f) {
-      int fi = i0, fj = j0, fk = k0;
-      if (D == 0) fi += f; else if (D == 1) fj += f; else fk += f;
-      R3 fc0 = {0., 0., 0.};
-      for (int q = 0; q < (DIM == 3 ? 4 : 2); ++q) {
-        int a, b, cz;
-        face_node_ijk2<DIM, D>(fi, fj, fk, q, a, b, cz);
-        fc0 = fc0 + wf * node_x0(M, a, b, cz);
-      }
-      R3 diff = fc0 - cc0;
-      ond[f] = comp(diff / norm(diff), D);
-    }
-  }
-  const int order2 = A.order - 1;
-  double uo[NV], dualm[NE];
-  for (int q = 0; q < NE; ++q) dualm[q] = 0.;
-  // cell local face order: 3D back then front; 2D x sweep: front then back
-  constexpr int FA = (DIM == 2 && D == 0) ? 1 : 0;
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    // a: phi of every slot
-    for (int it = tid; it < NS * TW; it += T::THREADS) {
-      if (!s_ok[it]) continue;
-      const int tw = it % TW, s = it / TW - 2;
-      int i, j, k;
-      tile_coord<D>(s, tw, i, j, k);
-      s_phi[it] = A.Uin[v * N + cell_id(M, i, j, k)] / s_den[it];
-    }
-    __syncthreads();
-    // b: face gradients, faces between slots s-1 and s for s = -1 .. TD+1
-    for (int it = tid; it < (NS - 1) * TW; it += T::THREADS) {
-      const int hi = it + TW, lo = it;  // slot indices (offset by 2) of the two cells
-      s_gf[it] = (s_ok[lo] && s_ok[hi]) ? (s_phi[hi] - s_phi[lo]) / (s_xc[hi] - s_xc[lo]) : 0.;
-    }
-    __syncthreads();
-    // c: limited gradients of slots -1 .. TD
-    for (int it = tid; it < (NS - 2) * TW; it += T::THREADS) {
-      const int slot = it + TW;  // offset-2 index of slot s = it/TW - 1
-      double g = 0.;
-      if (A.order > 1 && s_ok[slot]) g = limited_gradient(A.limiter, s_gf[it], s_gf[it + TW]);
-      s_gr[it] = g;
-    }
-    __syncthreads();
-    // d: upwind face values of faces 0 .. TD (between slots f-1 and f)
-    for (int it = tid; it < (TD + 1) * TW; it += T::THREADS) {
-      const int lo = it + TW, hi = it + 2 * TW;  // offset-2 slot indices of f-1, f
-      double pf = 0.;
-      if (s_ok[lo] && s_ok[hi]) {
-        const double dx = s_xc[hi] - s_xc[lo];
-        const bool back = s_un[it] * dx > 0.0;
-        const int su = back ? lo : hi;
-        pf = s_phi[su] + order2 * (s_fc[it] - s_xc[su]) * s_gr[su - TW];
-      }
-      s_gf[it] = pf;  // reuse: upwind value of face it
-    }
-    __syncthreads();
-    // e: conservative update of the own cell
-    if (mine) {
-      const int fb = s0 * TW + tw0, ff = fb + TW;  // back and front faces
-      const bool exb = s_ok[me - TW], exf = s_ok[me + TW];
-      double flux[2];
-      flux[0] = exb ? ond[0] * s_un[fb] * s_L[fb] * dt * s_gf[fb] : 0.;
-      flux[1] = exf ? ond[1] * s_un[ff] * s_L[ff] * dt * s_gf[ff] : 0.;
-      const bool ex[2] = {exb, exf};
-      double sumf = 0., dual = 0.;
-      if (ex[FA]) { sumf += flux[FA]; dual += 0.5 * flux[FA] * ond[FA]; }
-      if (ex[1 - FA]) { sumf += flux[1 - FA]; dual += 0.5 * flux[1 - FA] * ond[1 - FA]; }
-      uo[v] = A.Uin[v * N + c0] - sumf;
-      if (v >= NE && v < 2 * NE) dualm[v - NE] = dual;
-    }
-    __syncthreads();
-  }
-  if (!mine) return;
-  for (int q = 0; q < NE; ++q) {
-    if (uo[NE + q] < 0.) uo[NE + q] = 0.;
-    if (uo[2 * NE + q] < 0.) uo[2 * NE + q] = 0.;
-  }
-  for (int v = 0; v < NV; ++v) A.Uout[v * N + c0] = uo[v];
-  for (int q = 0; q < NE; ++q) F.mflux[q * N + c0] = dualm[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -257,8 +75,8 @@ __device__ __forceinline__ bool node_inner_dir(const Mesh& M, int i, int j, int 
 }
 
 template <int DIM, int NE, int D>
-__global__ void __launch_bounds__(SweepTile<D>::THREADS)
-k_sweep_nodes(Mesh M, mhc_case_params P, Fields F, DualArgs A) {
+__device__ __forceinline__ void body_sweep_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F,
+                                                 const DualArgs& A, VB vb) {
   using T = SweepTile<D>;
   constexpr int TW = T::TW, TD = T::TD, NS = T::NS;
   __shared__ double s_ph[4][NS * TW];  // phi components 0,1,2 and 4
@@ -281,7 +99,7 @@ k_sweep_nodes(Mesh M, mhc_case_params P, Fields F, DualArgs A) {
   for (int it = tid; it < NS * TW; it += T::THREADS) {
     const int tw = it % TW, s = it / TW - 2;
     int i, j, k;
-    tile_coord<D>(s, tw, i, j, k);
+    tile_coord<D>(vb, s, tw, i, j, k);
     const int a = along<D>(i, j, k);
     bool ok = a >= 0 && a < nn && i < M.nnx && j < M.nny && (DIM == 2 || k < M.nnz);
     s_ok[it] = ok;
@@ -322,7 +140,7 @@ k_sweep_nodes(Mesh M, mhc_case_params P, Fields F, DualArgs A) {
   const int me = (s0 + 2) * TW + tw0;
   if (!s_ok[me]) return;
   int i, j, k;
-  tile_coord<D>(s0, tw0, i, j, k);
+  tile_coord<D>(vb, s0, tw0, i, j, k);
   const long long n = node_id(M, i, j, k);
   double U[5];
   loadU(n, U);

@@ -1,0 +1,271 @@
+// mhc_sweep2.cuh -- cell part of one ADI remap direction without shared
+// memory or barriers.
+//
+// A warp holds 32 consecutive cells along the sweep direction, one per
+// lane; every intermediate of the reference -- phi, face gradient, limited
+// cell gradient, upwind face value, face flux -- is computed once per cell
+// or face and handed to the neighbour lane by a shuffle.  The 4 warps of a
+// block hold neighbouring transverse columns, so for the y and z sweeps the
+// block reads whole 32-byte sectors of every row it touches.
+//
+// Arithmetic and operation order are those of computeGradPhiFace,
+// computeGradPhiCell, computeUpwindFaceQuantitiesForProjection and
+// computeUremap (RemapADIService.cc:119-575, UtilesRemap.cc:108-120,
+// 325-357); face quantities of the Lagrangian mesh (PrepareRemap.cc:18-59)
+// are rebuilt from the node positions.  The initial face normals of the
+// cartesian grid are unit axis vectors, so dot(., n) is the D component.
+#pragma once
+#include "mhc_sweep.cuh"
+
+namespace mhc {
+
+constexpr int SW_LANES = 32; // cells along D per warp
+constexpr int SW_ROWS = 4;   // warps (transverse rows) per block
+constexpr int SW_THREADS = SW_LANES * SW_ROWS;
+constexpr int XOUT = 27;     // cells written per warp (lanes 2 .. 28)
+
+// ---------------------------------------------------------------------------
+// Initial-grid quantities of the outer normals, one coordinate at a time.
+// Node coordinate A of the initial grid depends on the node index along A
+// only, so the sums of the reference (cell centre over the local nodes,
+// face centre over the face nodes, in their orders) are rebuilt from the
+// two coordinate values c0 (offset 0) and c1 (offset 1).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ double grid_coord(const Mesh& M, int A, int idx) {
+  return (DIM == 2 && A == 2) ? 0. : M.o[A] + idx * M.h[A];
+}
+
+// component A of the initial cell centre (wc * sum over local nodes)
+template <int DIM, int A>
+__device__ __forceinline__ double cc0_comp(const Mesh& M, int idx) {
+  if (DIM == 2 && A == 2) return 0.;
+  const double c0 = grid_coord<DIM>(M, A, idx), c1 = grid_coord<DIM>(M, A, idx + 1);
+  double s = 0.;
+#pragma unroll
+  for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+    int da, db, dc;
+    local_node_offset(l, da, db, dc);
+    s += (A == 0 ? da : (A == 1 ? db : dc)) ? c1 : c0;
+  }
+  return (DIM == 2 ? .25 : .125) * s;
+}
+
+// component A of the initial centre of a face normal to D (sum over the
+// face nodes of wf * coordinate)
+template <int DIM, int D, int A>
+__device__ __forceinline__ double fc0_comp(const Mesh& M, int idx) {
+  if (DIM == 2 && A == 2) return 0.;
+  const double wf = DIM == 2 ? .5 : .25;
+  const double c0 = grid_coord<DIM>(M, A, idx), c1 = grid_coord<DIM>(M, A, idx + 1);
+  double s = 0.;
+#pragma unroll
+  for (int q = 0; q < (DIM == 3 ? 4 : 2); ++q) {
+    int a, b, cz;
+    face_node_ijk2<DIM, D>(0, 0, 0, q, a, b, cz);
+    const int off = A == 0 ? a : (A == 1 ? b : cz);
+    s = s + wf * ((A == D) ? c0 : (off ? c1 : c0));
+  }
+  return s;
+}
+
+// D component of the unit outer normal: diff_D / |diff| with the sum of
+// squares in x, y, z order
+template <int D>
+__device__ __forceinline__ double unit_comp(double dD, double t0, double t1) {
+  // t0, t1: transverse differences in increasing axis order
+  double ss;
+  if (D == 0) ss = dD * dD + t0 * t0 + t1 * t1;
+  else if (D == 1) ss = t0 * t0 + dD * dD + t1 * t1;
+  else ss = t0 * t0 + t1 * t1 + dD * dD;
+  return dD / sqrt(ss);
+}
+
+// face-node slot q (face_node_ijk2 order) of local node l of a cell, and
+// whether l sits on the front plane along D
+template <int DIM, int D>
+__device__ __forceinline__ void local_to_plane(int l, int& q, int& front) {
+  int da, db, dc;
+  local_node_offset(l, da, db, dc);
+  int s1, s2;
+  if (D == 0) { front = da; s1 = db; s2 = dc; }
+  else if (D == 1) { front = db; s1 = da; s2 = dc; }
+  else { front = dc; s1 = da; s2 = db; }
+  if (DIM == 2) s2 = 0;
+  q = s2 ? (s1 ? 2 : 3) : (s1 ? 1 : 0);
+}
+
+// Lagrangian plane data: the D coordinates of the face nodes, and the face
+// centre, normal velocity and length of the face (PrepareRemap.cc:18-59)
+template <int DIM> struct Plane {
+  double xd[DIM == 3 ? 4 : 2];
+  double fc, un, L;
+};
+
+template <int DIM, int D>
+__device__ __forceinline__ void load_plane(const Mesh& M, const Fields& F, int i, int j, int k, Plane<DIM>& P) {
+  constexpr int NQ = DIM == 3 ? 4 : 2;
+  const double wf = DIM == 2 ? .5 : .25;
+  const double* vD = D == 0 ? F.vx : (D == 1 ? F.vy : F.vz);
+  long long fn[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    int a, b, cz;
+    face_node_ijk2<DIM, D>(i, j, k, q, a, b, cz);
+    fn[q] = node_id(M, a, b, cz);
+  }
+  double vm = 0.;
+  P.fc = 0.;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    P.xd[q] = __ldg(F.Xn[D] + fn[q]);
+    P.fc = P.fc + wf * P.xd[q];
+    vm = vm + __ldg(vD + fn[q]);
+  }
+  P.un = wf * vm;
+  if (DIM == 3) {
+    R3 x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      x[q].x = D == 0 ? P.xd[q] : __ldg(F.Xn[0] + fn[q]);
+      x[q].y = D == 1 ? P.xd[q] : __ldg(F.Xn[1] + fn[q]);
+      x[q].z = D == 2 ? P.xd[q] : __ldg(F.Xn[2] + fn[q]);
+    }
+    const R3 v1 = x[2] - x[0], v2 = x[3] - x[1];
+    if (D == 0) P.L = 0.5 * fabs(produit(v1.y, v2.z, v1.z, v2.y));
+    else if (D == 1) P.L = 0.5 * fabs(produit(v2.x, v1.z, v2.z, v1.x));
+    else P.L = 0.5 * fabs(produit(v1.x, v2.y, v1.y, v2.x));
+  } else {
+    const double* Xt = F.Xn[1 - D];
+    P.L = fabs(__ldg(Xt + fn[1]) - __ldg(Xt + fn[0]));
+  }
+}
+
+// Lagrangian cell centre along D from its back (B) and front (Fr) planes,
+// summed in local node order
+template <int DIM, int D>
+__device__ __forceinline__ double centre_from_planes(const Plane<DIM>& B, const Plane<DIM>& Fr) {
+  double s = 0.;
+#pragma unroll
+  for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+    int q, front;
+    local_to_plane<DIM, D>(l, q, front);
+    s += front ? Fr.xd[q] : B.xd[q];
+  }
+  return (DIM == 2 ? .25 : .125) * s;
+}
+
+// ---------------------------------------------------------------------------
+// Cell sweep along D with warp shuffles.  A warp holds 32 consecutive cells
+// along D (lane l: cell x0 - 2 + l), loads the back node plane of each and
+// takes the front plane from lane l+1; stencil neighbours come from lanes
+// l-1 / l+1.  Lanes 2 .. XOUT+1 write.  Virtual block: x = window index
+// along D, y = group of SW_ROWS rows.  Rows are the transverse cells with
+// the lowest transverse axis fastest, so the warps of a block read
+// neighbouring columns and share L1 sectors.
+// ---------------------------------------------------------------------------
+template <int DIM, int NE, int D>
+__device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fields& F, const SweepArgs& A,
+                                                       int vbx, int vby) {
+  constexpr int NV = 3 * NE + 1;
+  constexpr int NQ = DIM == 3 ? 4 : 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  const long long N = M.ncell;
+  const int lane = threadIdx.x % SW_LANES, row = threadIdx.x / SW_LANES;
+  const int r = vby * SW_ROWS + row;
+  // transverse extents: (na, nb) = the two other axes in increasing order
+  const int na = D == 0 ? M.ncy : M.ncx;
+  const int nb = D == 2 ? M.ncy : M.ncz;
+  const int nd = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
+  if (r >= na * nb) return;  // whole warp leaves together
+  const int ta = r % na, tb = r / na;
+  const int p = vbx * XOUT - 2 + lane;  // index along D
+  int i, j, k;
+  if (D == 0) { i = p; j = ta; k = tb; }
+  else if (D == 1) { i = ta; j = p; k = tb; }
+  else { i = ta; j = tb; k = p; }
+  const bool ok = p >= 0 && p < nd;
+  const bool out = ok && lane >= 2 && lane < 2 + XOUT;
+  const double dt = F.s->dt;
+  const int order2 = A.order - 1;
+  const double* __restrict__ Uin = A.Uin;
+  // back node plane of the own cell (planes exist for p in [0, nd])
+  Plane<DIM> back;
+  if (p >= 0 && p <= nd) load_plane<DIM, D>(M, F, i, j, k, back);
+  else {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) back.xd[q] = 0.;
+    back.fc = back.un = back.L = 0.;
+  }
+  Plane<DIM> front;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) front.xd[q] = __shfl_down_sync(FULL, back.xd[q], 1);
+  long long c = 0;
+  double u[NV], den = 1., xc = 0., ondB = 0., ondF = 0.;
+  if (ok) {
+    c = cell_id(M, i, j, k);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = __ldg(Uin + v * N + c);
+    if (A.first) {
+      den = __ldg(F.V + c);
+    } else {
+      den = 0.;
+#pragma unroll
+      for (int q = 0; q < NE; ++q) den += u[q];
+    }
+    xc = centre_from_planes<DIM, D>(back, front);
+    if (out) {
+      // outer normals of the back and front faces (initial grid)
+      constexpr int A0 = D == 0 ? 1 : 0, A1 = D == 2 ? 1 : 2;
+      const double t0 = fc0_comp<DIM, D, A0>(M, ta) - cc0_comp<DIM, A0>(M, ta);
+      const double t1 = fc0_comp<DIM, D, A1>(M, tb) - cc0_comp<DIM, A1>(M, tb);
+      const double cc0 = cc0_comp<DIM, D>(M, p);
+      ondB = unit_comp<D>(fc0_comp<DIM, D, D>(M, p) - cc0, t0, t1);
+      ondF = unit_comp<D>(fc0_comp<DIM, D, D>(M, p + 1) - cc0, t0, t1);
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = 0.;
+  }
+  const double fc = back.fc, un = back.un, L = back.L;  // back face of the cell
+  const bool ok_l = __shfl_up_sync(FULL, ok, 1) && lane > 0;
+  const double xc_l = __shfl_up_sync(FULL, xc, 1);
+  const bool face_b = ok && ok_l;                       // face between p-1 and p
+  const bool face_f = __shfl_down_sync(FULL, face_b, 1) && lane < 31;
+  const double un_r = __shfl_down_sync(FULL, un, 1), L_r = __shfl_down_sync(FULL, L, 1);
+  const double dxb = xc - xc_l;
+  const bool up_left = un * dxb > 0.0;
+  // cell local face order: along x in 2D front then back, otherwise back
+  // then front
+  constexpr bool FRONT_FIRST = DIM == 2 && D == 0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double phi = ok ? u[v] / den : 0.;
+    const double phi_l = __shfl_up_sync(FULL, phi, 1);
+    const double gf = face_b ? (phi - phi_l) / dxb : 0.;
+    const double gf_r = __shfl_down_sync(FULL, gf, 1);
+    const double gr = (A.order > 1 && ok) ? limited_gradient(A.limiter, gf, gf_r) : 0.;
+    const double gr_l = __shfl_up_sync(FULL, gr, 1);
+    double pf = 0.;
+    if (face_b) pf = up_left ? phi_l + order2 * (fc - xc_l) * gr_l : phi + order2 * (fc - xc) * gr;
+    const double pf_r = __shfl_down_sync(FULL, pf, 1);
+    if (out) {
+      const double fB = face_b ? ondB * un * L * dt * pf : 0.;
+      const double fF = face_f ? ondF * un_r * L_r * dt * pf_r : 0.;
+      double sumf = 0., dual = 0.;
+      if (FRONT_FIRST) {
+        if (face_f) { sumf += fF; dual += 0.5 * fF * ondF; }
+        if (face_b) { sumf += fB; dual += 0.5 * fB * ondB; }
+      } else {
+        if (face_b) { sumf += fB; dual += 0.5 * fB * ondB; }
+        if (face_f) { sumf += fF; dual += 0.5 * fF * ondF; }
+      }
+      double uo = u[v] - sumf;
+      if (v >= NE && v < 3 * NE && uo < 0.) uo = 0.;  // masses and energies stay >= 0
+      A.Uout[v * N + c] = uo;
+      if (v >= NE && v < 2 * NE) F.mflux[(v - NE) * N + c] = dual;
+    }
+  }
+}
+
+}  // namespace mhc
