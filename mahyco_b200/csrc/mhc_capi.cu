@@ -122,24 +122,12 @@ struct StageTimer {
   }
 };
 
-template <int D>
-dim3 sweep_grid(int nx, int ny, int nz) {
-  using T = SweepTile<D>;
-  if (D == 0) return dim3(cdiv(nx, T::TD), ny, nz);
-  if (D == 1) return dim3(cdiv(nx, T::TW), cdiv(ny, T::TD), nz);
-  return dim3(cdiv(nx, T::TW), cdiv(nz, T::TD), ny);
-}
-
-dim3 sweep_grid_d(int D, int nx, int ny, int nz) {
-  return D == 0 ? sweep_grid<0>(nx, ny, nz) : (D == 1 ? sweep_grid<1>(nx, ny, nz) : sweep_grid<2>(nx, ny, nz));
-}
-
-// virtual blocks of the cell sweep (mhc_sweep2.cuh): x = XOUT-cell windows
-// along D, y = groups of SW_ROWS transverse rows
-dim3 cell_sweep_grid(int D, int nx, int ny, int nz) {
+// virtual blocks of a sweep (mhc_sweep.cuh): x = windows of `out` cells or
+// nodes along D, y = groups of SW_ROWS transverse rows
+dim3 lane_sweep_grid(int D, int nx, int ny, int nz, int out) {
   const int nd = D == 0 ? nx : (D == 1 ? ny : nz);
   const long long rows = (long long)nx * ny * nz / nd;
-  return dim3(cdiv(nd, XOUT), (unsigned)cdiv(rows, SW_ROWS), 1);
+  return dim3(cdiv(nd, out), (unsigned)cdiv(rows, SW_ROWS), 1);
 }
 
 int skip_mask(const mhc_case* h) {
@@ -252,7 +240,7 @@ int engine_rebuild(Engine* e) {
         open(L);
         for (int c : g.members) {
           const Mesh& M = e->cases[c]->M;
-          dim3 gr = pass == 0 ? cell_sweep_grid(D, M.ncx, M.ncy, M.ncz) : sweep_grid_d(D, M.nnx, M.nny, M.nnz);
+          dim3 gr = pass == 0 ? lane_sweep_grid(D, M.ncx, M.ncy, M.ncz, XOUT) : lane_sweep_grid(D, M.nnx, M.nny, M.nnz, NOUT);
           for (unsigned z = 0; z < gr.z; ++z)
             for (unsigned y = 0; y < gr.y; ++y)
               for (unsigned x = 0; x < gr.x; ++x) items.push_back(WorkItem{c, (int)x, (int)y, (int)z});
@@ -367,9 +355,9 @@ void sweep_step(Engine* e, Group& g, int D, int k) {
   }
   {
     StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
-    if (D == 0) plaunch(e, kb_sweep_nodes<DIM, NE, 0>, SweepTile<0>::THREADS, 0, g.sw_nodes[0], k);
-    else if (D == 1) plaunch(e, kb_sweep_nodes<DIM, NE, 1>, SweepTile<1>::THREADS, 0, g.sw_nodes[1], k);
-    else if constexpr (DIM == 3) plaunch(e, kb_sweep_nodes<DIM, NE, 2>, SweepTile<2>::THREADS, 0, g.sw_nodes[2], k);
+    if (D == 0) plaunch(e, kb_sweep_nodes<DIM, NE, 0>, SW_THREADS, 0, g.sw_nodes[0], k);
+    else if (D == 1) plaunch(e, kb_sweep_nodes<DIM, NE, 1>, SW_THREADS, 0, g.sw_nodes[1], k);
+    else if constexpr (DIM == 3) plaunch(e, kb_sweep_nodes<DIM, NE, 2>, SW_THREADS, 0, g.sw_nodes[2], k);
   }
 }
 

@@ -10,7 +10,6 @@
 #pragma once
 #include "mhc_kernels.cuh"
 #include "mhc_sweep.cuh"
-#include "mhc_sweep2.cuh"
 
 namespace mhc {
 
@@ -97,7 +96,7 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, i
 }
 
 template <int DIM, int NE, int D>
-__global__ void __launch_bounds__(SweepTile<D>::THREADS)
+__global__ void __launch_bounds__(SW_THREADS)
 kb_sweep_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int k) {
   MHC_FOR_ITEMS(W, n) {
     const WorkItem wi = W[w_];
@@ -125,8 +124,7 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, i
     A.order = P.ordre_projection;
     A.limiter = P.projection_limiteur_id;
     A.done_dirs = done;
-    body_sweep_nodes<DIM, NE, D>(M, P, F, A, VB{wi.x, wi.y, wi.z});
-    __syncthreads();
+    body_sweep_nodes_lanes<DIM, NE, D>(M, F, A, wi.x, wi.y);
   }
 }
 
