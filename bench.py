@@ -48,6 +48,11 @@ WORKLOADS = {
     "bisod3d": ("plain 3D BiSod 256x64x64, 2 materials, ADI remap, superbee, FP64", 2),
     "sedov3d": ("plain 3D Sedov 384^3, 1 material, ADI remap, minmod, FP64", 1),
     "sod2d_lagrange": ("plain 2D Lagrange Sod 200x10, FP64", 1),
+    "batch2d": ("batched: 4096 independent 2D Sod/BiSod cases, sides log-uniform 32..512, seeded states, "
+                "ADI remap, vanleer, FP64", 2),
+    "serve": ("served: Poisson arrivals of mixed 2D/3D Sedov, 3D BiSod, stiffened-gas water/air and "
+              "Mie-Gruneisen bar impact requests of 1e3..1e7 cells, HBM-budget admission, continuous "
+              "batching, FP64", 2),
 }
 
 
@@ -59,15 +64,16 @@ def build_params(name: str, scale: float = 1.0):
                    limiter=SUPERBEE, deltat_init=1e-5)
     if name == "sedov3d":
         n = max(2, int(round(384 * scale)))
-        p = sedov(dim=3, n=(n, n, n), L=1.2 * n / 384, limiter=MINMOD, energy=0.2468, p0=1e-6)
+        p = sedov(dim=3, n=(n, n, n), L=1.2 * n / 384, limiter=MINMOD, energy=0.2468, p0=1e-6,
+                  deltat_init=None)
         return p
     if name == "sod2d_lagrange":
         return sod(dim=2, n=(200, 10), L=(1.0, 0.05), bi=False, remap=False, deltat_max=1e-4)
     raise ValueError(name)
 
 
-# algorithmic bytes per launch of each kernel group (compulsory traffic of
-# the live fields, FP64): see DESIGN.md "Roofline model"
+# algorithmic bytes per launch of each kernel group: compulsory traffic of
+# the live fields (one read and/or write of each per pass, FP64)
 def stage_bytes(stage: str, dim: int, ne: int, ncell: int, nnode: int) -> float:
     nv = 3 * ne + 1
     per = {
@@ -229,12 +235,14 @@ def run_ours(args):
             torch.cuda.synchronize()
 
     barrier()
+    l0 = h.launches
     with ClockSampler(local) as clocks:
         e0.record(stream)
         h.cycle(args.steps)
         e1.record(stream)
         e1.synchronize()
     barrier()
+    launches = h.launches - l0
     ms = e0.elapsed_time(e1)
     st |= h.synchronize()
     if world > 1:
@@ -286,7 +294,7 @@ def run_ours(args):
                    "materials": p.nb_env, "remap": bool(p.with_projection),
                    "l2": "working set > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
         "status": st,
-        "gpu_launches": launches_per_cycle(p) * args.steps,
+        "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk.get("hbm_gbs"),
                      "unit": "GB/s", "frac": achieved / pk.get("hbm_gbs"),
                      "peak_source": "measured" if "how" in pk else "fallback",
@@ -307,6 +315,245 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def batch_cases(count: int, seed: int = 2024):
+    from mahyco_b200.cases import seeded_two_state, log_uniform_sides
+    sides = log_uniform_sides(count, seed=seed)
+    return [seeded_two_state(seed * 100003 + i, n) for i, n in enumerate(sides)]
+
+
+def run_batch(args):
+    """Batched form: every case resident, one launch per phase for all of
+    them, cycles replayed from a CUDA graph, launch shapes autotuned during
+    the warm-up; against the plain form (one case at a time through its own
+    handle) on a seeded sample of the same cases."""
+    import ctypes
+    import torch
+    import mahyco_b200 as mb
+    from mahyco_b200.autotune import tune, CANDIDATES
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = mb.load()
+    cases = batch_cases(args.cases)
+    tune_cycles = 2 * len(CANDIDATES)
+    warm = max(args.warmup, tune_cycles + 2)
+    limit = warm + args.steps
+    cells = sum(p.ncell for p in cases)
+    # -- batched arm
+    t_wall0 = time.perf_counter()
+    b = mb.Batch(lib)
+    idx = [b.add(p, iteration_limit=limit) for p in cases]
+    b.init()
+    tuned = tune(b, cycles_per_trial=2)
+    b.cycle(warm - tune_cycles, graph=True)
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.stream_handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    l0 = b.launches
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        b.cycle(args.steps, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = b.launches - l0
+    done = [b.scalars(i) for i in idx]
+    t_wall = time.perf_counter() - t_wall0
+    bad = sum(1 for d in done if d["iteration"] != limit)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    batched = world * cells * args.steps / (ms * 1e-3)
+    # -- plain arm on a seeded sample (every k-th case), device time of the
+    # same K cycles per case, plus its per-solve wall latency
+    k = max(1, len(cases) // args.plain_sample) if args.plain_sample > 0 else 1
+    sample = list(range(0, len(cases), k))
+    plain_ms, plain_cells, lat, same, plain_launches = 0.0, 0, [], True, 0
+    check = set(sample[:: max(1, len(sample) // 8)])
+    for i in sample:
+        p = cases[i]
+        w0 = time.perf_counter()
+        h = mb.Hydro(p, lib)
+        h.hydroStartInit()
+        h.cycle(warm)
+        st = torch.cuda.ExternalStream(h.stream_handle)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(st)
+        pl0 = h.launches
+        h.cycle(args.steps)
+        plain_launches += h.launches - pl0
+        a1.record(st)
+        a1.synchronize()
+        rho = h.field("Density")
+        lat.append(time.perf_counter() - w0)
+        plain_ms += a0.elapsed_time(a1)
+        plain_cells += p.ncell
+        if i in check:
+            import numpy as np
+            same &= bool(np.array_equal(rho, b.field(idx[i], "Density")))
+        h.close()
+    b.close()
+    plain = plain_cells * args.steps / (plain_ms * 1e-3)
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    lat.sort()
+    out = {
+        "metric": METRIC, "value": batched, "unit": "cell-cycles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": warm, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS["batch2d"][0], "cases": len(cases), "cells": cells,
+                   "step": "one cycle of every case", "graph": "CUDA graph of 6 cycles",
+                   "l2": "working set > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
+        "batched_vs_plain": batched / plain,
+        "plain": {"value": plain, "unit": "cell-cycles/s", "sample_cases": len(sample),
+                  "sample_cells": plain_cells, "same_results": same, "gpu_launches": plain_launches,
+                  "latency_s": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+                  "how": "each sampled case alone through its own handle: create, init, warm-up, K timed cycles"},
+        "autotune": tuned["best"],
+        "cases_not_at_limit": bad,
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "e2e": {"value": world * cells * args.steps / t_wall, "unit": "cell-cycles/s",
+                "h2d_bytes_per_step": len(cases) * ctypes.sizeof(cases[0]) / args.steps,
+                "d2h_bytes_per_step": len(cases) * 40 / args.steps,
+                "timer": "host wall clock of the whole batched run: case creation, init, tuning, warm-up, K cycles, status read-back"},
+    }
+    print(json.dumps(out), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def serve_requests(count: int, seed: int = 7):
+    """(kind, params, iterations) of the served mix: kinds uniform, cells
+    log-uniform in [1e3, 1e7] (the bar impact is always 80x400)."""
+    import math
+    import random
+    from mahyco_b200.cases import serving_request, SERVING_KINDS
+    rng = random.Random(seed)
+    out = []
+    for _ in range(count):
+        kind = rng.choice(SERVING_KINDS)
+        cells = int(math.exp(rng.uniform(math.log(1e3), math.log(1e7))))
+        out.append((kind, serving_request(kind, cells)))
+    return out
+
+
+def run_serve(args):
+    """Served form: a request loop (mhc_server_*) fed by Poisson arrivals,
+    against sequential plain solves of the same requests on the same GPU."""
+    import random
+    import torch
+    import mahyco_b200 as mb
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return  # the served form runs on one GPU; other ranks have nothing to do
+    lib = mb.load()
+    its = args.steps
+    reqs = serve_requests(args.requests)
+    rng = random.Random(11)
+    arrivals, t = [], 0.0
+    for _ in reqs:
+        t += rng.expovariate(args.rate)
+        arrivals.append(t)
+    work = sum(p.ncell for _, p in reqs) * its
+    # warm-up: one small solve of every kind through the server (module load,
+    # pools, first launches)
+    srv = mb.Server()
+    for kind, p in serve_requests(len(reqs))[:10]:
+        if p.ncell < 50000:
+            srv.submit(p, 3)
+    while srv.stats()["queued"] or srv.stats()["running"]:
+        srv.step(3)
+    srv.close()
+    srv = mb.Server()
+    t0 = time.perf_counter()
+    nxt, tickets, done_at = 0, {}, {}
+    l0 = srv.launches
+    with ClockSampler(local) as clocks:
+        while len(done_at) < len(reqs):
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and arrivals[nxt] <= now:
+                tickets[srv.submit(reqs[nxt][1], its)] = nxt
+                nxt += 1
+            if not tickets or len(done_at) == len(tickets):
+                if nxt < len(reqs):
+                    time.sleep(max(0.0, min(0.002, arrivals[nxt] - now)))
+                continue
+            srv.step(args.cycles_per_step)
+            now = time.perf_counter() - t0
+            for tk, i in list(tickets.items()):
+                if i in done_at:
+                    continue
+                st = srv.poll(tk)
+                if st["state"] in (mb.REQ_DONE, mb.REQ_FAILED):
+                    done_at[i] = (now, st["state"], st["status"])
+                    srv.release(tk)
+    launches = srv.launches - l0
+    srv.close()
+    makespan = max(d[0] for d in done_at.values()) - arrivals[0]
+    lat = sorted(done_at[i][0] - arrivals[i] for i in range(len(reqs)))
+    failed = [{"kind": reqs[i][0], "cells": reqs[i][1].ncell, "status": d[2]}
+              for i, d in sorted(done_at.items()) if d[1] != mb.REQ_DONE]
+    served = work / makespan
+    # sequential plain solves, each alone: create, init, cycles, read-back
+    service = []
+    for kind, p in reqs:
+        w0 = time.perf_counter()
+        h = mb.Hydro(p, lib)
+        h.hydroStartInit()
+        h.cycle(its)
+        h.scalars()
+        h.close()
+        service.append(time.perf_counter() - w0)
+    plain = work / sum(service)
+    fin, plat = 0.0, []
+    for a, sv in zip(arrivals, service):  # FIFO queue under the same arrivals
+        fin = max(fin, a) + sv
+        plat.append(fin - a)
+    plat.sort()
+
+    def pct(v, q):
+        return v[min(len(v) - 1, int(q * len(v)))]
+    out = {
+        "metric": METRIC, "value": served, "unit": "cell-cycles/s", "n_gpus": 1,
+        "steps": its, "warmup": 3, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS["serve"][0], "requests": len(reqs), "rate_per_s": args.rate,
+                   "iterations_per_request": its, "cells": sum(p.ncell for _, p in reqs),
+                   "cycles_per_step": args.cycles_per_step,
+                   "offered_cell_cycles_per_s": work / (arrivals[-1] - arrivals[0]),
+                   "l2": "mixed sizes; large requests exceed L2"},
+        "latency_s": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99), "max": lat[-1]},
+        "failed": failed,
+        "served_vs_plain": served / plain,
+        "plain": {"value": plain, "unit": "cell-cycles/s",
+                  "latency_s": {"p50": pct(plat, 0.5), "p99": pct(plat, 0.99), "max": plat[-1]},
+                  "how": "the same requests solved one after another through their own handles; latency "
+                         "from a FIFO queue of the measured service times under the same arrivals"},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "e2e": {"value": served, "unit": "cell-cycles/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "timer": "host wall clock from the first arrival to the last completion"},
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -315,9 +562,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="bisod3d", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cases", type=int, default=4096, help="batch2d: number of cases")
+    ap.add_argument("--plain-sample", type=int, default=0,
+                    help="batch2d: cases timed one at a time (0 = all of them)")
+    ap.add_argument("--requests", type=int, default=120, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=8.0, help="serve: Poisson arrival rate (1/s)")
+    ap.add_argument("--cycles-per-step", type=int, default=4, help="serve: cycles between admissions")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch2d":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -37,6 +37,8 @@ extern "C" {
 #define MHC_ST_DT_UNDERFLOW 2     /* MahycoModule.cc:1816-1833 (exit(1) there) */
 #define MHC_ST_NAN 4              /* RemapADIFinal.cc:274-284 (exit(1) there) */
 #define MHC_ST_STOP 8             /* final time reached: stopComputeLoop (MahycoModule.cc:1851-1857) */
+#define MHC_ST_OOM_ADMISSION 16   /* serving: the case does not fit the HBM budget */
+#define MHC_ST_TIMEOUT 32         /* serving: the request outlived its deadline */
 
 typedef struct mhc_case mhc_case;
 
@@ -169,8 +171,50 @@ int mhc_batch_synchronize(mhc_batch* b);
 /* launch grid of the phases: 0 (default) = one block per work item,
  * k > 0 = k x the blocks the device can hold at once, striding the list */
 int mhc_batch_set_grid_scale(mhc_batch* b, int scale);
+/* per-phase override of the grid scale (stage = enum mhc_stage, scale -1 =
+ * back to the batch-wide value); the autotuner sets these */
+int mhc_batch_set_stage_grid_scale(mhc_batch* b, int stage, int scale);
+/* number of kernels the batch (or a single case) has put on the GPU so far;
+ * a CUDA graph replay counts every kernel node it runs */
+long long mhc_batch_launches(mhc_batch* b);
+long long mhc_case_launches(mhc_case* h);
 int mhc_batch_get_scalars(mhc_batch* b, int index, double* time, double* deltat, long long* iteration, int* status);
 long long mhc_batch_get_field(mhc_batch* b, int index, const char* name, int env, double* host, long long capacity);
+/* stop advancing a case but keep its state resident (fields stay readable
+ * until mhc_batch_remove) */
+int mhc_batch_detach(mhc_batch* b, int index);
+/* iteration done, status flags and time of every case index (removed: -1),
+ * read with one gather kernel and one copy; returns the number of indices */
+int mhc_batch_poll(mhc_batch* b, int capacity, long long* iteration, int* status, double* time);
+
+/* --- serving: continuous batching under an HBM budget --------------------
+ * No counterpart in the reference (one case per process there).  Requests
+ * (a case and an iteration count) are queued by submit; every step admits
+ * queued requests whose device footprint (mhc_case_device_bytes) fits the
+ * budget, in arrival order with bounded backfilling, advances every
+ * resident case `cycles` iterations with one launch per phase, and retires
+ * the cases that reached their iteration count, stopped or failed.  Results
+ * stay resident, and charged to the budget, until released.  Per-request
+ * status: the MHC_ST_* flags, including MHC_ST_OOM_ADMISSION (larger than
+ * the whole budget) and MHC_ST_TIMEOUT (deadline exceeded). */
+typedef struct mhc_server mhc_server;
+enum { MHC_REQ_QUEUED = 0, MHC_REQ_RUNNING = 1, MHC_REQ_DONE = 2, MHC_REQ_FAILED = 3 };
+/* budget <= 0: 90% of the device memory free at creation */
+int mhc_server_create(long long hbm_budget_bytes, mhc_server** out);
+int mhc_server_destroy(mhc_server* s);
+void* mhc_server_stream(mhc_server* s);
+mhc_batch* mhc_server_batch(mhc_server* s);
+/* timeout_s <= 0: no deadline */
+int mhc_server_submit(mhc_server* s, const mhc_case_params* p, long long iterations, double timeout_s, long long* ticket);
+/* returns the number of requests that completed (done or failed) in this step */
+int mhc_server_step(mhc_server* s, int cycles);
+int mhc_server_poll(mhc_server* s, long long ticket, int* state, int* status, long long* iteration, double* time);
+/* host clock (seconds since server creation) of submission, admission, completion (-1: not yet) */
+int mhc_server_times(mhc_server* s, long long ticket, double* submit, double* admit, double* done);
+long long mhc_server_fetch(mhc_server* s, long long ticket, const char* name, int env, double* host, long long capacity);
+/* frees a finished request's device state (MHC_ERR_ORDER while queued or running) */
+int mhc_server_release(mhc_server* s, long long ticket);
+int mhc_server_stats(mhc_server* s, long long* queued, long long* running, long long* bytes_in_use, long long* budget);
 
 /* --- allocation-free CFL time step --------------------------------------
  * No counterpart in the reference: an extra entry point for callers that

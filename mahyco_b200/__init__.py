@@ -24,6 +24,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmahyco_b200.so")
 
 ST_NEG_VOLUME, ST_DT_UNDERFLOW, ST_NAN, ST_STOP = 1, 2, 4, 8
+ST_OOM_ADMISSION, ST_TIMEOUT = 16, 32
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 _lib = None
 
@@ -68,6 +70,9 @@ _SIGS = {
     "mhc_batch_cycle_timed": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "mhc_batch_synchronize": (C.c_int, [C.c_void_p]),
     "mhc_batch_set_grid_scale": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_batch_set_stage_grid_scale": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "mhc_batch_launches": (C.c_longlong, [C.c_void_p]),
+    "mhc_case_launches": (C.c_longlong, [C.c_void_p]),
     "mhc_batch_get_scalars": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                         C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "mhc_batch_get_field": (C.c_longlong, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double),
@@ -76,6 +81,24 @@ _SIGS = {
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "mhc_noalloc_last_error": (C.c_char_p, []),
+    "mhc_batch_detach": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_batch_poll": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_double)]),
+    "mhc_server_create": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
+    "mhc_server_destroy": (C.c_int, [C.c_void_p]),
+    "mhc_server_stream": (C.c_void_p, [C.c_void_p]),
+    "mhc_server_batch": (C.c_void_p, [C.c_void_p]),
+    "mhc_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.POINTER(C.c_longlong)]),
+    "mhc_server_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_server_poll": (C.c_int, [C.c_void_p, C.c_longlong, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
+    "mhc_server_times": (C.c_int, [C.c_void_p, C.c_longlong, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double)]),
+    "mhc_server_fetch": (C.c_longlong, [C.c_void_p, C.c_longlong, C.c_char_p, C.c_int, C.POINTER(C.c_double),
+                                        C.c_longlong]),
+    "mhc_server_release": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "mhc_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                   C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
 }
 
 
@@ -125,6 +148,11 @@ class Hydro:
     def stream_handle(self) -> int:
         """cudaStream_t of the case (for torch.cuda.ExternalStream / events)"""
         return int(self.lib.mhc_case_stream(self.h))
+
+    @property
+    def launches(self) -> int:
+        """Kernels this case has put on the GPU so far."""
+        return int(self.lib.mhc_case_launches(self.h))
 
     def close(self):
         if self.h:
@@ -285,6 +313,27 @@ class Batch:
     def set_grid_scale(self, scale: int):
         _check(self.lib, self.lib.mhc_batch_set_grid_scale(self.b, int(scale)), "grid scale")
 
+    @property
+    def launches(self) -> int:
+        """Kernels this batch has put on the GPU so far."""
+        return int(self.lib.mhc_batch_launches(self.b))
+
+    def set_stage_grid_scale(self, stage: int | str, scale: int):
+        st = Hydro.STAGES.index(stage) if isinstance(stage, str) else int(stage)
+        _check(self.lib, self.lib.mhc_batch_set_stage_grid_scale(self.b, st, int(scale)), "stage grid scale")
+
+    def detach(self, idx: int):
+        _check(self.lib, self.lib.mhc_batch_detach(self.b, int(idx)), "mhc_batch_detach")
+
+    def poll(self) -> list[tuple[int, int, float]]:
+        """(iteration, status, time) of every case index, from one read-back."""
+        n = max(self.params) + 1 if self.params else 0
+        it = (C.c_longlong * max(n, 1))()
+        st = (C.c_int * max(n, 1))()
+        tm = (C.c_double * max(n, 1))()
+        _check(self.lib, self.lib.mhc_batch_poll(self.b, n, it, st, tm), "mhc_batch_poll")
+        return [(it[i], st[i], tm[i]) for i in range(n)]
+
     def scalars(self, idx: int) -> dict:
         t, dt, it, st = C.c_double(), C.c_double(), C.c_longlong(), C.c_int()
         _check(self.lib, self.lib.mhc_batch_get_scalars(self.b, int(idx), C.byref(t), C.byref(dt), C.byref(it),
@@ -299,3 +348,82 @@ class Batch:
                                            out.ctypes.data_as(C.POINTER(C.c_double)), n)
         _check(self.lib, int(got), f"batch field {name}")
         return out
+
+
+class Server:
+    """Request loop with continuous batching under an HBM budget
+    (``mhc_server_*`` of the C ABI).  submit() queues a solve; step() admits
+    what fits, advances every resident case and retires finished ones."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+        s = C.c_void_p()
+        _check(self.lib, self.lib.mhc_server_create(int(hbm_budget_bytes), C.byref(s)), "mhc_server_create")
+        self.s = s
+        self.params = {}
+
+    def close(self):
+        if self.s:
+            self.lib.mhc_server_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self.lib.mhc_server_stream(self.s) or 0)
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.mhc_batch_launches(self.lib.mhc_server_batch(self.s)))
+
+    def submit(self, params: CaseParams, iterations: int, timeout_s: float = 0.0) -> int:
+        t = C.c_longlong()
+        _check(self.lib, self.lib.mhc_server_submit(self.s, C.byref(params), int(iterations), float(timeout_s),
+                                                    C.byref(t)), "mhc_server_submit")
+        self.params[t.value] = params
+        return t.value
+
+    def step(self, cycles: int = 1) -> int:
+        return _check(self.lib, self.lib.mhc_server_step(self.s, int(cycles)), "mhc_server_step")
+
+    def poll(self, ticket: int) -> dict:
+        state, status, it, tm = C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
+        _check(self.lib, self.lib.mhc_server_poll(self.s, int(ticket), C.byref(state), C.byref(status), C.byref(it),
+                                                  C.byref(tm)), "mhc_server_poll")
+        return {"state": state.value, "status": status.value, "iteration": it.value, "time": tm.value}
+
+    def times(self, ticket: int) -> dict:
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _check(self.lib, self.lib.mhc_server_times(self.s, int(ticket), C.byref(a), C.byref(b), C.byref(c)),
+               "mhc_server_times")
+        return {"submit": a.value, "admit": b.value, "done": c.value}
+
+    def fetch(self, ticket: int, name: str, env: int = -1) -> np.ndarray:
+        p = self.params[ticket]
+        n = 3 * p.nnode if name in ("Velocity", "NodeCoord") else (p.nnode if name == "NodeMass" else p.ncell)
+        out = np.empty(n, dtype=np.float64)
+        got = self.lib.mhc_server_fetch(self.s, int(ticket), name.encode(), int(env),
+                                        out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        _check(self.lib, int(got), f"server fetch {name}")
+        return out
+
+    def release(self, ticket: int):
+        _check(self.lib, self.lib.mhc_server_release(self.s, int(ticket)), "mhc_server_release")
+        self.params.pop(ticket, None)
+
+    def stats(self) -> dict:
+        q, r, b, g = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(self.lib, self.lib.mhc_server_stats(self.s, C.byref(q), C.byref(r), C.byref(b), C.byref(g)),
+               "mhc_server_stats")
+        return {"queued": q.value, "running": r.value, "bytes_in_use": b.value, "budget": g.value}

@@ -52,9 +52,23 @@ def sod(dim=3, n=(100, 5, 5), L=(1.0, 0.1, 0.1), bi=True, axis=0, remap=True,
     return p
 
 
+def sedov_safe_dt(dim: int, n: int, L: float, energy: float, gamma: float = 1.4) -> float:
+    """A first time step inside the CFL bound of the energised origin cell:
+    0.1 h / c with c the sound speed of `energy` spread over that cell
+    (rho = 1).  The reference datasets start at 1e-5 on coarse meshes; on
+    fine meshes that step crushes the origin cell in the first cycle."""
+    h = L / n
+    e0 = energy / h ** dim
+    c = math.sqrt(gamma * (gamma - 1.0) * e0)
+    return 0.1 * h / c
+
+
 def sedov(dim=3, n=(60, 60, 60), L=1.2, limiter=MINMOD, energy=0.244816, p0=0.0979264e-5,
           final_time=1e30, deltat_init=1e-5) -> CaseParams:
-    """CAS_Sedov / CAS_2D_Sedov: rho = 1, symmetry planes at 0, energy in the origin cell."""
+    """CAS_Sedov / CAS_2D_Sedov: rho = 1, symmetry planes at 0, energy in the
+    origin cell.  deltat_init=None picks min(1e-5, sedov_safe_dt)."""
+    if deltat_init is None:
+        deltat_init = min(1e-5, sedov_safe_dt(dim, max(n[:dim]), L, energy))
     p = default_params()
     nn = (n[0], n[1], n[2] if dim == 3 else 1)
     _mesh(p, dim, nn, (L, L, L))
@@ -156,6 +170,49 @@ def mie_gruneisen_plate(dim=2, n=(80, 8), L=(0.01, 0.001), remap=False, deltat_i
     return p
 
 
+def bar_impact(n=(80, 400), L=(0.01, 0.05), velocity=200.0, deltat_init=1e-9) -> CaseParams:
+    """Aluminium bar (Mie-Gruneisen rho0 2710, c0 5328, s1 1.338, Gamma0 2.0)
+    hitting the rigid wall y = 0 at `velocity`: Lagrangian, explicit
+    pressure as in CAS_2D_Lag_Taylor_elasto."""
+    p = default_params()
+    _mesh(p, 2, n, L)
+    p.nb_env = 1
+    env_defaults(p.env[0], EOS_MIE_GRUNEISEN)
+    o = p.env[0]
+    o.rho0, o.c0, o.s1, o.gamma0 = 2710.0, 5328.0, 1.338, 2.0
+    o.densite_initiale, o.pression_initiale = 2710.0, 1.0e5
+    o.vitesse_initiale[:] = (0.0, -velocity, 0.0)
+    p.cas_model = CASE_TWO_STATE
+    p.interface_pos, p.interface_dir = 1e30, 0
+    p.pression_explicite = 1
+    p.with_projection = 0
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.3, deltat_init, 1e-16, 1e-6
+    symmetry_bcs(p, ("XMIN", "YMIN"))
+    return p
+
+
+def serving_request(kind: str, cells: int) -> CaseParams:
+    """One request of the served mix, scaled to about `cells` cells."""
+    if kind == "sedov2d":
+        m = max(4, int(round(cells ** 0.5)))
+        return sedov(dim=2, n=(m, m, 1), L=1.2, limiter=MINMOD, energy=0.2468, p0=1e-6, deltat_init=None)
+    if kind == "sedov3d":
+        m = max(4, int(round(cells ** (1 / 3))))
+        return sedov(dim=3, n=(m, m, m), L=1.2, limiter=MINMOD, energy=0.2468, p0=1e-6, deltat_init=None)
+    if kind == "bisod3d":
+        m = max(2, int(round((cells / 4) ** (1 / 3))))
+        return sod(dim=3, n=(4 * m, m, m), L=(1.0, 0.25, 0.25), bi=True, limiter=SUPERBEE)
+    if kind == "water_air":
+        m = max(2, int(round((cells / 10) ** 0.5)))
+        return water_air(dim=2, n=(10 * m, m), L=(1.0, 0.1))
+    if kind == "bar":
+        return bar_impact()
+    raise ValueError(kind)
+
+
+SERVING_KINDS = ("sedov2d", "sedov3d", "bisod3d", "water_air", "bar")
+
+
 # small parity cases: name -> (builder, cycles).  Initial time steps are
 # large enough that the CFL bound, shocks and mixed cells are exercised.
 PARITY_CASES = {
@@ -177,6 +234,7 @@ PARITY_CASES = {
                                                deltat_init=1e-3)), 80),
     "adi2d_water_air": (lambda: water_air(deltat_init=1e-6), 80),
     "lag2d_mie_gruneisen": (lambda: mie_gruneisen_plate(deltat_init=1e-8), 100),
+    "lag2d_bar_impact": (lambda: bar_impact(n=(8, 40), L=(0.01, 0.05)), 80),
 }
 
 

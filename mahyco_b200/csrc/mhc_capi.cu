@@ -63,8 +63,10 @@ struct mhc_case {
 // engine
 // ---------------------------------------------------------------------------
 struct DevList {
-  size_t off = 0;  // offset (in items) inside the engine list arena
-  int n = 0;
+  size_t off_cases = 0;  // offsets inside the engine's int arena
+  size_t off_start = 0;
+  int n = 0;             // member cases
+  int total = 0;         // virtual blocks of all members
 };
 
 struct Group {
@@ -82,10 +84,8 @@ struct Engine {
   std::vector<mhc_case*> cases;
   CaseDesc* d_desc = nullptr;
   int desc_cap = 0;
-  WorkItem* d_items = nullptr;
-  size_t items_cap = 0;
-  int* d_caseidx = nullptr;
-  size_t caseidx_cap = 0;
+  int* d_ints = nullptr;   // case indices and block prefix sums of every list
+  size_t ints_cap = 0;
   std::vector<Group> groups;
   bool dirty = true;
   long long cycles_since_build = 0;
@@ -101,6 +101,16 @@ struct Engine {
   // scheduler balances), k > 0 = k x the blocks the device holds at once
   // (persistent blocks striding over the list)
   int grid_scale = 0;
+  // per-phase override of grid_scale (-1 = use grid_scale), set by a tuner
+  int stage_scale[MHC_NUM_STAGES] = {-1, -1, -1, -1, -1, -1, -1};
+  int cur_stage = -1;  // phase being launched (StageTimer scope)
+  // kernels this engine put on the GPU (graph replays count their nodes)
+  long long launches = 0;
+  long long graph_launches = 0;  // kernel nodes of the captured graph
+  // status gather of every case (one kernel + one copy)
+  Scalars* d_gather = nullptr;
+  Scalars* h_gather = nullptr;   // pinned
+  int gather_cap = 0;
 };
 
 namespace {
@@ -109,9 +119,11 @@ struct StageTimer {
   Engine* e;
   int stage;
   StageTimer(Engine* e_, int s) : e(e_), stage(s) {
+    e->cur_stage = s;
     if (e->timing) cudaEventRecord(e->ev[0], e->stream);
   }
   ~StageTimer() {
+    e->cur_stage = -1;
     if (!e->timing) return;
     cudaEventRecord(e->ev[1], e->stream);
     cudaEventSynchronize(e->ev[1]);
@@ -121,14 +133,6 @@ struct StageTimer {
     e->stage_launches[stage] += 1;
   }
 };
-
-// virtual blocks of a sweep (mhc_sweep.cuh): x = windows of `out` cells or
-// nodes along D, y = groups of SW_ROWS transverse rows
-dim3 lane_sweep_grid(int D, int nx, int ny, int nz, int out) {
-  const int nd = D == 0 ? nx : (D == 1 ? ny : nz);
-  const long long rows = (long long)nx * ny * nz / nd;
-  return dim3(cdiv(nd, out), (unsigned)cdiv(rows, SW_ROWS), 1);
-}
 
 int skip_mask(const mhc_case* h) {
   int m = 0;
@@ -153,9 +157,12 @@ int resident_blocks(Engine* e, K kernel, int threads, size_t smem) {
 
 template <class K, class... Args>
 void plaunch(Engine* e, K kernel, int threads, size_t smem, const DevList& L, Args... args) {
-  if (L.n <= 0) return;
-  int grid = e->grid_scale == 0 ? L.n : std::min(L.n, resident_blocks(e, kernel, threads, smem) * e->grid_scale);
-  kernel<<<grid, threads, smem, e->stream>>>(e->d_desc, e->d_items + L.off, L.n, args...);
+  if (L.total <= 0) return;
+  const int sc = (e->cur_stage >= 0 && e->stage_scale[e->cur_stage] >= 0) ? e->stage_scale[e->cur_stage] : e->grid_scale;
+  int grid = sc == 0 ? L.total : std::min(L.total, resident_blocks(e, kernel, threads, smem) * sc);
+  const PhaseList pl{e->d_ints + L.off_cases, e->d_ints + L.off_start, L.n, L.total};
+  kernel<<<grid, threads, smem, e->stream>>>(e->d_desc, pl, args...);
+  ++e->launches;
 }
 
 size_t lagrange_smem(int dim) {
@@ -204,68 +211,41 @@ int engine_rebuild(Engine* e) {
     }
     e->groups[it->second].members.push_back(i);
   }
-  // work items
-  std::vector<WorkItem> items;
-  std::vector<int> caseidx;
-  auto open = [&](DevList& L) { L.off = items.size(); L.n = 0; };
-  auto close_ = [&](DevList& L) { L.n = (int)(items.size() - L.off); };
-  auto cells1d = [&](const Group& g, DevList& L, bool nodes) {
-    open(L);
-    for (int c : g.members) {
-      const Mesh& M = e->cases[c]->M;
-      int nb = cdiv(nodes ? M.nnode : M.ncell, CT);
-      for (int b = 0; b < nb; ++b) items.push_back(WorkItem{c, b, 0, 0});
-    }
-    close_(L);
-  };
+  // per group: member case indices, then for every phase the prefix sums
+  // of the members' virtual blocks
+  std::vector<int> ints;
   for (Group& g : e->groups) {
-    cells1d(g, g.init_cells, false);
-    cells1d(g, g.init_nodes, true);
-    cells1d(g, g.lag_cells, false);
-    cells1d(g, g.fin_cells, false);
-    cells1d(g, g.fin_nodes, true);
-    cells1d(g, g.dt, false);
-    open(g.lag_nodes);
-    for (int c : g.members) {
-      const Mesh& M = e->cases[c]->M;
-      int gz = g.DIM == 3 ? cdiv(M.nnz, LZCHUNK) : 1;
-      for (int z = 0; z < gz; ++z)
-        for (int y = 0; y < cdiv(M.nny, LTY); ++y)
-          for (int x = 0; x < cdiv(M.nnx, LTX); ++x) items.push_back(WorkItem{c, x, y, z});
-    }
-    close_(g.lag_nodes);
-    for (int D = 0; D < g.DIM; ++D) {
-      for (int pass = 0; pass < 2; ++pass) {
-        DevList& L = pass == 0 ? g.sw_cells[D] : g.sw_nodes[D];
-        open(L);
-        for (int c : g.members) {
-          const Mesh& M = e->cases[c]->M;
-          dim3 gr = pass == 0 ? lane_sweep_grid(D, M.ncx, M.ncy, M.ncz, XOUT) : lane_sweep_grid(D, M.nnx, M.nny, M.nnz, NOUT);
-          for (unsigned z = 0; z < gr.z; ++z)
-            for (unsigned y = 0; y < gr.y; ++y)
-              for (unsigned x = 0; x < gr.x; ++x) items.push_back(WorkItem{c, (int)x, (int)y, (int)z});
-        }
-        close_(L);
-      }
-    }
-    g.cases.off = caseidx.size();
-    for (int c : g.members) caseidx.push_back(c);
+    const size_t oc = ints.size();
+    for (int c : g.members) ints.push_back(c);
+    g.cases.off_cases = oc;
     g.cases.n = (int)g.members.size();
+    auto phase = [&](DevList& L, int ph) -> bool {
+      L.off_cases = oc;
+      L.n = (int)g.members.size();
+      L.off_start = ints.size();
+      long long tot = 0;
+      for (int c : g.members) {
+        ints.push_back((int)tot);
+        int gx, gy, gz;
+        phase_grid(ph, e->cases[c]->M, gx, gy, gz);
+        tot += (long long)gx * gy * gz;
+      }
+      L.total = (int)tot;
+      return tot <= INT_MAX;
+    };
+    bool ok = phase(g.init_cells, PH_CELLS) && phase(g.init_nodes, PH_NODES) && phase(g.lag_cells, PH_CELLS) &&
+              phase(g.fin_cells, PH_CELLS) && phase(g.fin_nodes, PH_NODES) && phase(g.dt, PH_CELLS) &&
+              phase(g.lag_nodes, PH_LAG_NODES);
+    for (int D = 0; D < g.DIM; ++D) ok = ok && phase(g.sw_cells[D], PH_SWC0 + D) && phase(g.sw_nodes[D], PH_SWN0 + D);
+    if (!ok) return set_err(MHC_ERR_ARG, "more than 2^31 blocks in one phase of a batch");
   }
-  if (items.size() > e->items_cap) {
-    if (e->d_items) CK(cudaFreeAsync(e->d_items, e->stream));
-    e->items_cap = std::max(items.size(), 2 * e->items_cap);
-    CK(cudaMallocAsync((void**)&e->d_items, e->items_cap * sizeof(WorkItem), e->stream));
+  if (ints.size() > e->ints_cap) {
+    if (e->d_ints) CK(cudaFreeAsync(e->d_ints, e->stream));
+    e->ints_cap = std::max(ints.size(), 2 * e->ints_cap);
+    CK(cudaMallocAsync((void**)&e->d_ints, e->ints_cap * sizeof(int), e->stream));
   }
-  if (caseidx.size() > e->caseidx_cap) {
-    if (e->d_caseidx) CK(cudaFreeAsync(e->d_caseidx, e->stream));
-    e->caseidx_cap = std::max(caseidx.size(), 2 * e->caseidx_cap);
-    CK(cudaMallocAsync((void**)&e->d_caseidx, e->caseidx_cap * sizeof(int), e->stream));
-  }
-  if (!items.empty())
-    CK(cudaMemcpyAsync(e->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, e->stream));
-  if (!caseidx.empty())
-    CK(cudaMemcpyAsync(e->d_caseidx, caseidx.data(), caseidx.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  if (!ints.empty())
+    CK(cudaMemcpyAsync(e->d_ints, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
   // the host vectors must outlive the async copies
   CK(cudaStreamSynchronize(e->stream));
   e->dirty = false;
@@ -392,7 +372,8 @@ void launch_dt(Engine* e) {
   for (Group& g : e->groups) {
     DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_>, CT, 0, g.dt)));
     if (g.cases.n > 0)
-      kb_delta_t_finalize<<<cdiv(g.cases.n, 128), 128, 0, e->stream>>>(e->d_desc, e->d_caseidx + g.cases.off, g.cases.n);
+      kb_delta_t_finalize<<<cdiv(g.cases.n, 128), 128, 0, e->stream>>>(e->d_desc, e->d_ints + g.cases.off_cases, g.cases.n);
+      ++e->launches;
   }
 }
 
@@ -432,8 +413,11 @@ int engine_cycle_graph(Engine* e, int n) {
     std::vector<long long> its;
     for (mhc_case* h : e->cases) its.push_back(h->it_host);
     cudaGraph_t g;
+    const long long before = e->launches;
     CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < period; ++it) launch_cycle(e);
+    e->graph_launches = e->launches - before;
+    e->launches = before;
     cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
     if (ce != cudaSuccess) return set_err(MHC_ERR_CUDA, cudaGetErrorString(ce));
     CK(cudaGraphInstantiate(&e->graph, g, 0));
@@ -443,6 +427,7 @@ int engine_cycle_graph(Engine* e, int n) {
   }
   while (n >= period && e->graph) {
     CK(cudaGraphLaunch(e->graph, e->stream));
+    e->launches += e->graph_launches;
     for (int it = 0; it < period; ++it) end_cycle(e);
     n -= period;
   }
@@ -470,11 +455,13 @@ int engine_create(cudaStream_t stream, Engine** out) {
 void engine_release(Engine* e) {
   if (e->graph) cudaGraphExecDestroy(e->graph);
   if (e->d_desc) cudaFreeAsync(e->d_desc, e->stream);
-  if (e->d_items) cudaFreeAsync(e->d_items, e->stream);
-  if (e->d_caseidx) cudaFreeAsync(e->d_caseidx, e->stream);
+  if (e->d_ints) cudaFreeAsync(e->d_ints, e->stream);
   for (int i = 0; i < 2; ++i)
     if (e->ev[i]) cudaEventDestroy(e->ev[i]);
-  e->graph = nullptr; e->d_desc = nullptr; e->d_items = nullptr; e->d_caseidx = nullptr;
+  if (e->d_gather) cudaFreeAsync(e->d_gather, e->stream);
+  if (e->h_gather) { cudaStreamSynchronize(e->stream); cudaFreeHost(e->h_gather); }
+  e->d_gather = nullptr; e->h_gather = nullptr; e->gather_cap = 0;
+  e->graph = nullptr; e->d_desc = nullptr; e->desc_cap = 0; e->d_ints = nullptr; e->ints_cap = 0;
   e->ev[0] = e->ev[1] = nullptr;
 }
 
@@ -943,6 +930,8 @@ int mhc_time_history(mhc_case* h, double* out) {
 struct mhc_batch {
   Engine* e = nullptr;
   std::vector<mhc_case*> slots;   // case index -> case (nullptr once removed)
+  std::vector<char> detached;     // slot kept resident but no longer advanced
+  std::vector<Scalars> last;      // scalars read when the slot was detached
 };
 
 int mhc_batch_create(mhc_batch** out) {
@@ -974,6 +963,8 @@ int mhc_batch_add(mhc_batch* b, const mhc_case_params* params, long long iterati
   h->initialised = false;
   *index = (int)b->slots.size();
   b->slots.push_back(h);
+  b->detached.push_back(0);
+  b->last.push_back(Scalars{});
   b->e->cases.push_back(h);
   b->e->dirty = true;
   return MHC_OK;
@@ -1008,7 +999,53 @@ int mhc_batch_remove(mhc_batch* b, int index) {
   b->e->dirty = true;
   case_free(h);
   b->slots[index] = nullptr;
+  b->detached[index] = 0;
   return MHC_OK;
+}
+
+int mhc_batch_detach(mhc_batch* b, int index) {
+  if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
+  if (b->detached[index]) return MHC_OK;
+  mhc_case* h = b->slots[index];
+  int r = read_scalars(h, b->e->stream, &b->last[index]);
+  if (r) return r;
+  auto& v = b->e->cases;
+  v.erase(std::remove(v.begin(), v.end(), h), v.end());
+  b->e->dirty = true;
+  b->detached[index] = 1;
+  return MHC_OK;
+}
+
+int mhc_batch_poll(mhc_batch* b, int capacity, long long* iteration, int* status, double* time) {
+  if (!b || capacity < 0) return set_err(MHC_ERR_ARG, "bad argument");
+  Engine* e = b->e;
+  int r = engine_rebuild(e);
+  if (r) return r;
+  const int n = (int)e->cases.size();
+  if (n > e->gather_cap) {
+    if (e->d_gather) CK(cudaFreeAsync(e->d_gather, e->stream));
+    if (e->h_gather) { CK(cudaStreamSynchronize(e->stream)); CK(cudaFreeHost(e->h_gather)); }
+    e->gather_cap = std::max(n, 2 * e->gather_cap);
+    CK(cudaMallocAsync((void**)&e->d_gather, e->gather_cap * sizeof(Scalars), e->stream));
+    CK(cudaMallocHost((void**)&e->h_gather, e->gather_cap * sizeof(Scalars)));
+  }
+  if (n > 0) {
+    kb_gather_scalars<<<cdiv(n, 128), 128, 0, e->stream>>>(e->d_desc, n, e->d_gather);
+    ++e->launches;
+    CK(cudaMemcpyAsync(e->h_gather, e->d_gather, n * sizeof(Scalars), cudaMemcpyDeviceToHost, e->stream));
+  }
+  CK(cudaStreamSynchronize(e->stream));
+  const int ns = (int)b->slots.size();
+  for (int i = 0; i < ns && i < capacity; ++i) {
+    mhc_case* h = b->slots[i];
+    const Scalars* sc = nullptr;
+    if (!h) { if (iteration) iteration[i] = -1; if (status) status[i] = -1; if (time) time[i] = 0.; continue; }
+    sc = b->detached[i] ? &b->last[i] : &e->h_gather[h->slot];
+    if (iteration) iteration[i] = sc->iteration_done;
+    if (status) status[i] = sc->status;
+    if (time) time[i] = sc->t_done;
+  }
+  return ns;
 }
 
 int mhc_batch_cycle(mhc_batch* b, int n) {
@@ -1035,6 +1072,18 @@ int mhc_batch_synchronize(mhc_batch* b) {
 int mhc_batch_set_grid_scale(mhc_batch* b, int scale) {
   if (!b || scale < 0 || scale > 64) return set_err(MHC_ERR_ARG, "grid scale must be 0..64");
   b->e->grid_scale = scale;
+  if (b->e->graph) { cudaGraphExecDestroy(b->e->graph); b->e->graph = nullptr; }
+  return MHC_OK;
+}
+
+long long mhc_batch_launches(mhc_batch* b) { return b ? b->e->launches : -1; }
+
+long long mhc_case_launches(mhc_case* h) { return (h && h->solo) ? h->solo->launches : (h ? 0 : -1); }
+
+int mhc_batch_set_stage_grid_scale(mhc_batch* b, int stage, int scale) {
+  if (!b || stage < 0 || stage >= MHC_NUM_STAGES || scale < -1 || scale > 64)
+    return set_err(MHC_ERR_ARG, "stage must be 0..MHC_NUM_STAGES-1 and scale -1..64");
+  b->e->stage_scale[stage] = scale;
   if (b->e->graph) { cudaGraphExecDestroy(b->e->graph); b->e->graph = nullptr; }
   return MHC_OK;
 }

@@ -321,7 +321,7 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
   R3 x = node_x0(M, i, j, k);
   F.Xp[0][n] = x.x; F.Xp[1][n] = x.y; F.Xp[2][n] = x.z;
   double vx = 0., vy = 0., vz = 0.;
-  if (P.cas_model == MHC_CASE_SOD) {
+  if (P.cas_model == MHC_CASE_SOD || P.cas_model == MHC_CASE_TWO_STATE) {
     vx = P.env[0].vitesse_initiale[0]; vy = P.env[0].vitesse_initiale[1]; vz = P.env[0].vitesse_initiale[2];
   }
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;

@@ -24,13 +24,69 @@ struct WorkItem {
   int x, y, z;  // virtual block index inside the case
 };
 
-#define MHC_FOR_ITEMS(W, n)                                      \
-  for (int w_ = blockIdx.x; w_ < (n); w_ += gridDim.x)
+// work decomposition of the phases: virtual blocks of one case
+enum PhaseKind {
+  PH_CELLS = 0,      // one block per CT cells
+  PH_NODES = 1,      // one block per CT nodes
+  PH_LAG_NODES = 2,  // LTX x LTY x LZCHUNK node tiles
+  PH_SWC0 = 3,       // cell sweep along D = PH - PH_SWC0
+  PH_SWN0 = 6        // node sweep along D = PH - PH_SWN0
+};
+
+__host__ __device__ inline int cdiv_i(long long a, int b) { return (int)((a + b - 1) / b); }
+
+// virtual-block grid (gx, gy, gz) of one case in a phase; blocks are
+// numbered with x fastest
+__host__ __device__ inline void phase_grid(int ph, const Mesh& M, int& gx, int& gy, int& gz) {
+  gy = gz = 1;
+  if (ph == PH_CELLS) { gx = cdiv_i(M.ncell, CT); return; }
+  if (ph == PH_NODES) { gx = cdiv_i(M.nnode, CT); return; }
+  if (ph == PH_LAG_NODES) {
+    gx = cdiv_i(M.nnx, LTX);
+    gy = cdiv_i(M.nny, LTY);
+    gz = M.dim == 3 ? cdiv_i(M.nnz, LZCHUNK) : 1;
+    return;
+  }
+  const bool nodes = ph >= PH_SWN0;
+  const int D = nodes ? ph - PH_SWN0 : ph - PH_SWC0;
+  const int nx = nodes ? M.nnx : M.ncx, ny = nodes ? M.nny : M.ncy, nz = nodes ? M.nnz : M.ncz;
+  const int nd = D == 0 ? nx : (D == 1 ? ny : nz);
+  const long long rows = (long long)nx * ny * nz / nd;
+  gx = cdiv_i(nd, nodes ? NOUT : XOUT);
+  gy = cdiv_i(rows, SW_ROWS);
+}
+
+// the cases of one group and the first virtual block of each (ascending
+// prefix sums); a launch covers `total` virtual blocks
+struct PhaseList {
+  const int* cases;
+  const int* start;
+  int n;
+  int total;
+};
+
+// case and virtual block of global block w: binary search of the prefix sums
+template <int PH>
+__device__ __forceinline__ WorkItem item_at(const CaseDesc* __restrict__ C, const PhaseList& L, int w) {
+  int lo = 0, hi = L.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(L.start + mid) <= w) lo = mid;
+    else hi = mid - 1;
+  }
+  const int c = __ldg(L.cases + lo);
+  const int b = w - __ldg(L.start + lo);
+  int gx, gy, gz;
+  phase_grid(PH, C[c].M, gx, gy, gz);
+  return WorkItem{c, b % gx, (b / gx) % gy, b / (gx * gy)};
+}
+
+#define MHC_FOR_ITEMS(L) for (int w_ = blockIdx.x; w_ < (L).total; w_ += gridDim.x)
 
 template <int DIM, int NE>
-__global__ void __launch_bounds__(CT) kb_init_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(CT) kb_init_cells(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
     Fields F = C[wi.c].F;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
@@ -39,9 +95,9 @@ __global__ void __launch_bounds__(CT) kb_init_cells(const CaseDesc* __restrict__
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
     Fields F = C[wi.c].F;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
@@ -50,9 +106,9 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(LTX * LTY) kb_lagrange_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(LTX * LTY) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_LAG_NODES>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -63,9 +119,9 @@ __global__ void __launch_bounds__(LTX * LTY) kb_lagrange_nodes(const CaseDesc* _
 }
 
 template <int DIM, int NE, bool EULER>
-__global__ void __launch_bounds__(CT) kb_lagrange_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(CT) kb_lagrange_cells(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -77,9 +133,9 @@ __global__ void __launch_bounds__(CT) kb_lagrange_cells(const CaseDesc* __restri
 // k-th performed sweep of the cycle in direction D: U[k&1] -> U[(k+1)&1]
 template <int DIM, int NE, int D>
 __global__ void __launch_bounds__(SW_THREADS)
-kb_sweep_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int k) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_SWC0 + D>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -97,9 +153,9 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, i
 
 template <int DIM, int NE, int D>
 __global__ void __launch_bounds__(SW_THREADS)
-kb_sweep_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int k) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_SWN0 + D>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -130,9 +186,9 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, i
 
 // remap finalize after K performed sweeps: cells read U[K&1], nodes Ud[(K-1)&1]
 template <int DIM, int NE>
-__global__ void __launch_bounds__(CT) kb_remap_finalize_cells(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int K) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(CT) kb_remap_finalize_cells(const CaseDesc* __restrict__ C, PhaseList L, int K) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -142,9 +198,9 @@ __global__ void __launch_bounds__(CT) kb_remap_finalize_cells(const CaseDesc* __
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int K) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __restrict__ C, PhaseList L, int K) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -154,9 +210,9 @@ __global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(CT) kb_delta_t(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(CT) kb_delta_t(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -175,10 +231,15 @@ __global__ void kb_delta_t_finalize(const CaseDesc* __restrict__ C, const int* _
   }
 }
 
+// copy of every case's scalars into one array (one read-back per poll)
+__global__ void kb_gather_scalars(const CaseDesc* __restrict__ C, int n, Scalars* __restrict__ out) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) out[t] = *C[t].F.s;
+}
+
 template <int NE>
-__global__ void __launch_bounds__(CT) kb_eos_apply(const CaseDesc* __restrict__ C, const WorkItem* __restrict__ W, int n, int env) {
-  MHC_FOR_ITEMS(W, n) {
-    const WorkItem wi = W[w_];
+__global__ void __launch_bounds__(CT) kb_eos_apply(const CaseDesc* __restrict__ C, PhaseList L, int env) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
     Fields F = C[wi.c].F;
     const Mesh M = C[wi.c].M;
     body_eos_apply<NE>(M, *C[wi.c].P, F, env, wi.x);

@@ -1,0 +1,279 @@
+// mhc_serve.cc -- request loop over the batch engine: continuous batching
+// of independent solves admitted by HBM budget.
+//
+// A request is one case (parameters) to be advanced a number of iterations.
+// submit() queues it; every step() admits queued requests while their
+// device footprint fits the budget (in arrival order, with bounded
+// backfilling of smaller requests behind a blocked one), starts them, runs
+// the requested number of cycles of everything resident in one launch per
+// phase, then reads every case's status in one copy and retires the cases
+// that finished.  A retired case stays resident until the caller fetches its
+// results and releases it, and its memory stays charged to the budget until
+// then.  Requests never block each other's arithmetic: each case's results
+// are the same alone and in any mix.
+//
+// Host-only C++ over the public batch API; no counterpart in the reference,
+// whose time loop runs one case per process.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/mahyco_b200.h"
+
+namespace {
+
+struct Request {
+  long long ticket = 0;
+  mhc_case_params P;
+  long long iterations = 0;
+  double timeout_s = 0.;      // 0 = none
+  long long bytes = 0;
+  int state = MHC_REQ_QUEUED;
+  int status = 0;
+  int slot = -1;
+  long long iteration = 0;
+  double time = 0.;
+  double t_submit = 0., t_admit = -1., t_done = -1.;
+};
+
+double now_s(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct mhc_server {
+  mhc_batch* batch = nullptr;
+  long long budget = 0;
+  long long in_use = 0;
+  int max_bypass = 64;        // admissions allowed past a blocked queue head
+  int bypassed = 0;
+  long long next_ticket = 1;
+  std::chrono::steady_clock::time_point t0;
+  std::deque<long long> queue;                     // tickets, arrival order
+  std::vector<long long> running;                  // tickets on the GPU
+  std::unordered_map<long long, Request> reqs;
+  std::unordered_map<int, long long> by_slot;
+  std::vector<long long> poll_it;
+  std::vector<int> poll_st;
+  std::vector<double> poll_t;
+  long long completed = 0;
+};
+
+int mhc_server_create(long long hbm_budget_bytes, mhc_server** out) {
+  if (!out) return MHC_ERR_ARG;
+  mhc_server* s = new mhc_server();
+  int r = mhc_batch_create(&s->batch);
+  if (r) { delete s; return r; }
+  if (hbm_budget_bytes <= 0) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { mhc_batch_destroy(s->batch); delete s; return MHC_ERR_CUDA; }
+    hbm_budget_bytes = (long long)(0.9 * (double)fr);
+  }
+  s->budget = hbm_budget_bytes;
+  s->t0 = std::chrono::steady_clock::now();
+  *out = s;
+  return MHC_OK;
+}
+
+int mhc_server_destroy(mhc_server* s) {
+  if (!s) return MHC_OK;
+  mhc_batch_destroy(s->batch);
+  delete s;
+  return MHC_OK;
+}
+
+void* mhc_server_stream(mhc_server* s) { return s ? mhc_batch_stream(s->batch) : nullptr; }
+
+mhc_batch* mhc_server_batch(mhc_server* s) { return s ? s->batch : nullptr; }
+
+int mhc_server_submit(mhc_server* s, const mhc_case_params* p, long long iterations, double timeout_s,
+                      long long* ticket) {
+  if (!s || !p || !ticket || iterations < 1) return MHC_ERR_ARG;
+  Request q;
+  q.ticket = s->next_ticket++;
+  q.P = *p;
+  q.iterations = iterations;
+  q.timeout_s = timeout_s;
+  q.bytes = mhc_case_device_bytes(p);
+  if (q.bytes < 0) return MHC_ERR_ARG;
+  q.t_submit = now_s(s->t0);
+  if (q.bytes > s->budget) {
+    // can never fit: refused at once
+    q.state = MHC_REQ_FAILED;
+    q.status = MHC_ST_OOM_ADMISSION;
+    q.t_done = q.t_submit;
+    s->reqs[q.ticket] = q;
+    *ticket = q.ticket;
+    return MHC_OK;
+  }
+  s->reqs[q.ticket] = q;
+  s->queue.push_back(q.ticket);
+  *ticket = q.ticket;
+  return MHC_OK;
+}
+
+namespace {
+
+void finish(mhc_server* s, Request& q, int state, int status, double t) {
+  q.state = state;
+  q.status = status;
+  q.t_done = t;
+  ++s->completed;
+}
+
+int admit(mhc_server* s) {
+  int added = 0;
+  bool head_blocked = false;
+  for (auto it = s->queue.begin(); it != s->queue.end();) {
+    Request& q = s->reqs[*it];
+    const double t = now_s(s->t0);
+    if (q.timeout_s > 0. && t - q.t_submit > q.timeout_s) {
+      finish(s, q, MHC_REQ_FAILED, MHC_ST_TIMEOUT, t);
+      it = s->queue.erase(it);
+      continue;
+    }
+    if (s->in_use + q.bytes > s->budget) {
+      if (it == s->queue.begin()) head_blocked = true;
+      ++it;
+      continue;
+    }
+    if (head_blocked && it != s->queue.begin()) {
+      if (s->bypassed >= s->max_bypass) break;  // let the head through first
+      ++s->bypassed;
+    }
+    int slot = -1;
+    int r = mhc_batch_add(s->batch, &q.P, q.iterations, &slot);
+    if (r == MHC_ERR_NOMEM || r == MHC_ERR_CUDA) {
+      // the device refused the memory the budget allowed: wait for frees
+      if (s->running.empty()) {
+        finish(s, q, MHC_REQ_FAILED, MHC_ST_OOM_ADMISSION, t);
+        it = s->queue.erase(it);
+        continue;
+      }
+      break;
+    }
+    if (r) {
+      finish(s, q, MHC_REQ_FAILED, MHC_ST_NAN, t);
+      it = s->queue.erase(it);
+      continue;
+    }
+    if (it == s->queue.begin()) s->bypassed = 0;
+    q.slot = slot;
+    q.state = MHC_REQ_RUNNING;
+    q.t_admit = t;
+    s->in_use += q.bytes;
+    s->by_slot[slot] = q.ticket;
+    s->running.push_back(q.ticket);
+    it = s->queue.erase(it);
+    ++added;
+  }
+  if (added) {
+    int r = mhc_batch_init(s->batch);
+    if (r) return r;
+  }
+  return added;
+}
+
+}  // namespace
+
+int mhc_server_step(mhc_server* s, int cycles) {
+  if (!s || cycles < 0) return MHC_ERR_ARG;
+  const long long done0 = s->completed;
+  int r = admit(s);
+  if (r < 0) return r;
+  if (s->running.empty()) return (int)(s->completed - done0);
+  if (cycles > 0 && (r = mhc_batch_cycle(s->batch, cycles))) return r;
+  int ns = 0;
+  for (long long tk : s->running) ns = std::max(ns, s->reqs[tk].slot + 1);
+  s->poll_it.resize(ns);
+  s->poll_st.resize(ns);
+  s->poll_t.resize(ns);
+  r = mhc_batch_poll(s->batch, ns, s->poll_it.data(), s->poll_st.data(), s->poll_t.data());
+  if (r < 0) return r;
+  const double t = now_s(s->t0);
+  std::vector<long long> still;
+  for (long long tk : s->running) {
+    Request& q = s->reqs[tk];
+    q.iteration = s->poll_it[q.slot];
+    q.time = s->poll_t[q.slot];
+    const int st = s->poll_st[q.slot];
+    const int err = st & ~MHC_ST_STOP;
+    bool end = false;
+    if (err) { finish(s, q, MHC_REQ_FAILED, st, t); end = true; }
+    else if ((st & MHC_ST_STOP) || q.iteration >= q.iterations) { finish(s, q, MHC_REQ_DONE, st, t); end = true; }
+    else if (q.timeout_s > 0. && t - q.t_submit > q.timeout_s) {
+      finish(s, q, MHC_REQ_FAILED, st | MHC_ST_TIMEOUT, t);
+      end = true;
+    }
+    if (end) {
+      if ((r = mhc_batch_detach(s->batch, q.slot))) return r;
+    } else {
+      still.push_back(tk);
+    }
+  }
+  s->running.swap(still);
+  return (int)(s->completed - done0);
+}
+
+int mhc_server_poll(mhc_server* s, long long ticket, int* state, int* status, long long* iteration,
+                    double* time) {
+  if (!s) return MHC_ERR_ARG;
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return MHC_ERR_ARG;
+  const Request& q = it->second;
+  if (state) *state = q.state;
+  if (status) *status = q.status;
+  if (iteration) *iteration = q.iteration;
+  if (time) *time = q.time;
+  return MHC_OK;
+}
+
+int mhc_server_times(mhc_server* s, long long ticket, double* submit, double* admit_t, double* done) {
+  if (!s) return MHC_ERR_ARG;
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return MHC_ERR_ARG;
+  if (submit) *submit = it->second.t_submit;
+  if (admit_t) *admit_t = it->second.t_admit;
+  if (done) *done = it->second.t_done;
+  return MHC_OK;
+}
+
+long long mhc_server_fetch(mhc_server* s, long long ticket, const char* name, int env, double* host,
+                           long long capacity) {
+  if (!s) return MHC_ERR_ARG;
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end() || it->second.slot < 0) return MHC_ERR_ARG;
+  return mhc_batch_get_field(s->batch, it->second.slot, name, env, host, capacity);
+}
+
+int mhc_server_release(mhc_server* s, long long ticket) {
+  if (!s) return MHC_ERR_ARG;
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return MHC_ERR_ARG;
+  Request& q = it->second;
+  if (q.state == MHC_REQ_QUEUED || q.state == MHC_REQ_RUNNING) return MHC_ERR_ORDER;
+  if (q.slot >= 0) {
+    int r = mhc_batch_remove(s->batch, q.slot);
+    if (r) return r;
+    s->by_slot.erase(q.slot);
+    s->in_use -= q.bytes;
+  }
+  s->reqs.erase(it);
+  return MHC_OK;
+}
+
+int mhc_server_stats(mhc_server* s, long long* queued, long long* running, long long* bytes_in_use,
+                     long long* budget) {
+  if (!s) return MHC_ERR_ARG;
+  if (queued) *queued = (long long)s->queue.size();
+  if (running) *running = (long long)s->running.size();
+  if (bytes_in_use) *bytes_in_use = s->in_use;
+  if (budget) *budget = s->budget;
+  return MHC_OK;
+}

@@ -512,7 +512,9 @@ static void init_variables(Case& C) {
       C.density.g[c] = P.env[s].densite_initiale;
       C.pressure.g[c] = P.env[s].pression_initiale;
     }
-    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {0., 0., 0.};
+    // every node starts at the velocity of the first environment (zero in
+    // the shock tubes, the impact velocity of a projectile)
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
   } else if (P.cas_model == MHC_CASE_SEDOV) {
     double rhoInit = P.env[0].densite_initiale, pInit = P.env[0].pression_initiale;
     bool mono = P.cas_test == MHC_TEST_SEDOV;
