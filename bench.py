@@ -66,6 +66,7 @@ def build_params(name: str, scale: float = 1.0):
         n = max(2, int(round(384 * scale)))
         p = sedov(dim=3, n=(n, n, n), L=1.2 * n / 384, limiter=MINMOD, energy=0.2468, p0=1e-6,
                   deltat_init=None)
+        p.nb_env = 1  # a single perfect gas (the reference dataset's second environment stays empty)
         return p
     if name == "sod2d_lagrange":
         return sod(dim=2, n=(200, 10), L=(1.0, 0.05), bi=False, remap=False, deltat_max=1e-4)
@@ -341,7 +342,7 @@ def run_batch(args):
     lib = mb.load()
     cases = batch_cases(args.cases)
     tune_cycles = 2 * len(CANDIDATES)
-    warm = max(args.warmup, tune_cycles + 2)
+    warm = max(args.warmup, tune_cycles + 4)
     limit = warm + args.steps
     cells = sum(p.ncell for p in cases)
     # -- batched arm
@@ -350,7 +351,9 @@ def run_batch(args):
     idx = [b.add(p, iteration_limit=limit) for p in cases]
     b.init()
     tuned = tune(b, cycles_per_trial=2)
-    b.cycle(warm - tune_cycles, graph=True)
+    st = b.cycle_timed(2)  # per-phase device time with the tuned shapes
+    stages = {k: v[0] / 2 for k, v in st.items()}
+    b.cycle(warm - tune_cycles - 2, graph=True)
     b.synchronize()
     stream = torch.cuda.ExternalStream(b.stream_handle)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -422,6 +425,7 @@ def run_batch(args):
                   "latency_s": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
                   "how": "each sampled case alone through its own handle: create, init, warm-up, K timed cycles"},
         "autotune": tuned["best"],
+        "stages_ms_per_cycle": stages,
         "cases_not_at_limit": bad,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
@@ -562,6 +566,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="bisod3d", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="run init, W and K cycles of one case and exit (for ncu launch lists)")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="with --kernels-only: linear scale of the mesh (same cell size)")
     ap.add_argument("--cases", type=int, default=4096, help="batch2d: number of cases")
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="batch2d: cases timed one at a time (0 = all of them)")
@@ -569,7 +577,15 @@ def main():
     ap.add_argument("--rate", type=float, default=8.0, help="serve: Poisson arrival rate (1/s)")
     ap.add_argument("--cycles-per-step", type=int, default=4, help="serve: cycles between admissions")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernels_only:
+        import mahyco_b200 as mb
+        h = mb.Hydro(build_params(args.workload, args.scale))
+        h.hydroStartInit()
+        h.cycle(args.warmup + args.steps)
+        print(json.dumps({"kernels_only": args.workload, "scale": args.scale, "cells": h.ncell,
+                          "launches": h.launches, "scalars": h.scalars()}))
+        h.close()
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch2d":
         run_batch(args)

@@ -297,8 +297,8 @@ void lag_nodes_attr() {
 void launch_lagrange_nodes(Engine* e) {
   StageTimer tm(e, MHC_STAGE_LAGRANGE_NODES);
   for (Group& g : e->groups) {
-    if (g.DIM == 2) { lag_nodes_attr<2>(); plaunch(e, kb_lagrange_nodes<2>, LTX * LTY, lagrange_smem(2), g.lag_nodes); }
-    else { lag_nodes_attr<3>(); plaunch(e, kb_lagrange_nodes<3>, LTX * LTY, lagrange_smem(3), g.lag_nodes); }
+    if (g.DIM == 2) { lag_nodes_attr<2>(); plaunch(e, kb_lagrange_nodes<2>, LAG_THREADS, lagrange_smem(2), g.lag_nodes); }
+    else { lag_nodes_attr<3>(); plaunch(e, kb_lagrange_nodes<3>, LAG_THREADS, lagrange_smem(3), g.lag_nodes); }
   }
 }
 

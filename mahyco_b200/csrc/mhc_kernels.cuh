@@ -340,7 +340,8 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
 // so every corner normal is computed once per (tile, layer) and no atomics
 // are used.
 // ---------------------------------------------------------------------------
-constexpr int LTX = 16, LTY = 16;
+constexpr int LTX = 15, LTY = 15;                    // node columns of a tile
+constexpr int LAG_THREADS = (LTX + 1) * (LTY + 1);   // one thread per cell of a layer
 constexpr int LZCHUNK = 16;
 
 template <int DIM>
@@ -354,7 +355,7 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
   const int tx = threadIdx.x % LTX, ty = threadIdx.x / LTX;
   const int i0 = bx * LTX, j0 = by * LTY;
   const int ni = i0 + tx, nj = j0 + ty;
-  const bool node_ok = ni < M.nnx && nj < M.nny;
+  const bool node_ok = threadIdx.x < LTX * LTY && ni < M.nnx && nj < M.nny;
   const int NBN = DIM == 3 ? 8 : 4;
   const double dt = F.s->dt;
   const double dth = 0.5 * (F.s->old_dt + dt);
@@ -367,7 +368,7 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
   R3 S = {0., 0., 0.};
   for (int L = (DIM == 3 ? kz0 - 1 : 0); L < (DIM == 3 ? kz1 : 1); ++L) {
     // corner forces of cell layer L
-    for (int cl = threadIdx.x; cl < NCL; cl += LTX * LTY) {
+    for (int cl = threadIdx.x; cl < NCL; cl += LAG_THREADS) {
       int a = cl % CW, b = cl / CW;
       int ci = i0 - 1 + a, cj = j0 - 1 + b;
       bool ok = ci >= 0 && ci < M.ncx && cj >= 0 && cj < M.ncy && (DIM == 2 || (L >= 0 && L < M.ncz));

@@ -47,13 +47,17 @@ __host__ __device__ inline void phase_grid(int ph, const Mesh& M, int& gx, int& 
     gz = M.dim == 3 ? cdiv_i(M.nnz, LZCHUNK) : 1;
     return;
   }
+  // lane layout of mhc_sweep.cuh (sweep_lane)
   const bool nodes = ph >= PH_SWN0;
   const int D = nodes ? ph - PH_SWN0 : ph - PH_SWC0;
   const int nx = nodes ? M.nnx : M.ncx, ny = nodes ? M.nny : M.ncy, nz = nodes ? M.nnz : M.ncz;
-  const int nd = D == 0 ? nx : (D == 1 ? ny : nz);
-  const long long rows = (long long)nx * ny * nz / nd;
-  gx = cdiv_i(nd, nodes ? NOUT : XOUT);
-  gy = cdiv_i(rows, SW_ROWS);
+  const int out = nodes ? NOUT : XOUT;
+  if (D == 0) {
+    gx = cdiv_i(cdiv_i((long long)nx * ny * nz, out), SW_ROWS);
+  } else {
+    gx = cdiv_i(nx, SW_ROWS);
+    gy = cdiv_i((long long)ny * nz, out);
+  }
 }
 
 // the cases of one group and the first virtual block of each (ascending
@@ -105,8 +109,14 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
   }
 }
 
+// resident blocks per SM asked of the compiler for the two Lagrange kernels
+// (their corner normals hold ~100 doubles live per thread)
+#ifndef MHC_LAG_MIN_BLOCKS
+#define MHC_LAG_MIN_BLOCKS 1
+#endif
+
 template <int DIM>
-__global__ void __launch_bounds__(LTX * LTY) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
+__global__ void __launch_bounds__(LAG_THREADS, MHC_LAG_MIN_BLOCKS) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_LAG_NODES>(C, L, w_);
     Fields F = C[wi.c].F;
@@ -119,7 +129,7 @@ __global__ void __launch_bounds__(LTX * LTY) kb_lagrange_nodes(const CaseDesc* _
 }
 
 template <int DIM, int NE, bool EULER>
-__global__ void __launch_bounds__(CT) kb_lagrange_cells(const CaseDesc* __restrict__ C, PhaseList L) {
+__global__ void __launch_bounds__(CT, MHC_LAG_MIN_BLOCKS) kb_lagrange_cells(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
     Fields F = C[wi.c].F;

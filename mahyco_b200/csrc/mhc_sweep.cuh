@@ -44,7 +44,10 @@ __device__ __forceinline__ void face_node_ijk2(int i, int j, int k, int q, int& 
 
 
 constexpr int SW_LANES = 32; // cells along D per warp
-constexpr int SW_ROWS = 4;   // warps (transverse rows) per block
+#ifndef MHC_SW_ROWS
+#define MHC_SW_ROWS 4
+#endif
+constexpr int SW_ROWS = MHC_SW_ROWS;  // warps (transverse rows) per block
 constexpr int SW_THREADS = SW_LANES * SW_ROWS;
 constexpr int XOUT = 27;     // cells written per warp (lanes 2 .. 28)
 
@@ -180,6 +183,69 @@ __device__ __forceinline__ double centre_from_planes(const Plane<DIM>& B, const 
 }
 
 // ---------------------------------------------------------------------------
+// Lane layout of a sweep along D over an nx x ny x nz array of cells or
+// nodes.  The array is cut into lines along D; consecutive lines are
+// concatenated so that every warp window holds `out` written elements plus
+// two halo elements on each side, whatever the line length.
+//  * D = 0: lines are consecutive in memory; window w = vbx * SW_ROWS + row
+//    covers flat positions [w*out - 2, w*out + 30).
+//  * D = 1, 2: warp `row` of the block owns x column ta = vbx * SW_ROWS +
+//    row and walks the lines of that column (slow transverse index tb, then
+//    p along D) in windows vby; the 4 warps of a block hold neighbouring x
+//    columns at the same positions, so each row of the block is one or two
+//    32-byte sectors, and consecutive blocks (vbx fastest) hold the
+//    neighbouring columns, so the SMs that run them at the same time read
+//    whole DRAM bursts together.
+// Returns false when the lane holds nothing; p is the index along D and
+// (ta, tb) the transverse indices in increasing axis order.
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ bool sweep_lane(int nx, int ny, int nz, int out, int vbx, int vby, int lane, int row,
+                                           int& i, int& j, int& k, int& p, int& ta, int& tb) {
+  i = j = k = p = ta = tb = 0;
+  if (D == 0) {
+    const long long g = ((long long)vbx * SW_ROWS + row) * out - 2 + lane;
+    if (g < 0 || g >= (long long)nx * ny * nz) return false;
+    i = (int)(g % nx);
+    const long long r = g / nx;
+    j = (int)(r % ny);
+    k = (int)(r / ny);
+    p = i; ta = j; tb = k;
+    return true;
+  }
+  const int nd = D == 1 ? ny : nz, nb = D == 1 ? nz : ny;
+  ta = vbx * SW_ROWS + row;
+  const long long g = (long long)vby * out - 2 + lane;
+  if (ta >= nx || g < 0 || g >= (long long)nb * nd) return false;
+  tb = (int)(g / nd);
+  p = (int)(g % nd);
+  i = ta;
+  if (D == 1) { j = p; k = tb; }
+  else { j = tb; k = p; }
+  return true;
+}
+
+// the whole warp holds nothing (warp-uniform test, before any shuffle)
+template <int D>
+__device__ __forceinline__ bool sweep_warp_empty(int nx, int ny, int nz, int out, int vbx, int vby, int row) {
+  if (D == 0) return ((long long)vbx * SW_ROWS + row) * out - 2 >= (long long)nx * ny * nz;
+  const int nd = D == 1 ? ny : nz, nb = D == 1 ? nz : ny;
+  return vbx * SW_ROWS + row >= nx || (long long)vby * out - 2 >= (long long)nb * nd;
+}
+
+// D coordinates of the face nodes of the node plane whose lowest node is
+// (i, j, k)
+template <int DIM, int D>
+__device__ __forceinline__ void load_plane_xd(const Mesh& M, const Fields& F, int i, int j, int k, Plane<DIM>& P) {
+#pragma unroll
+  for (int q = 0; q < (DIM == 3 ? 4 : 2); ++q) {
+    int a, b, cz;
+    face_node_ijk2<DIM, D>(i, j, k, q, a, b, cz);
+    P.xd[q] = __ldg(F.Xn[D] + node_id(M, a, b, cz));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Cell sweep along D with warp shuffles.  A warp holds 32 consecutive cells
 // along D (lane l: cell x0 - 2 + l), loads the back node plane of each and
 // takes the front plane from lane l+1; stencil neighbours come from lanes
@@ -196,26 +262,18 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
   constexpr unsigned FULL = 0xffffffffu;
   const long long N = M.ncell;
   const int lane = threadIdx.x % SW_LANES, row = threadIdx.x / SW_LANES;
-  const int r = vby * SW_ROWS + row;
-  // transverse extents: (na, nb) = the two other axes in increasing order
-  const int na = D == 0 ? M.ncy : M.ncx;
-  const int nb = D == 2 ? M.ncy : M.ncz;
   const int nd = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
-  if (r >= na * nb) return;  // whole warp leaves together
-  const int ta = r % na, tb = r / na;
-  const int p = vbx * XOUT - 2 + lane;  // index along D
-  int i, j, k;
-  if (D == 0) { i = p; j = ta; k = tb; }
-  else if (D == 1) { i = ta; j = p; k = tb; }
-  else { i = ta; j = tb; k = p; }
-  const bool ok = p >= 0 && p < nd;
+  if (sweep_warp_empty<D>(M.ncx, M.ncy, M.ncz, XOUT, vbx, vby, row)) return;  // whole warp leaves together
+  int i, j, k, p, ta, tb;
+  const bool ok = sweep_lane<D>(M.ncx, M.ncy, M.ncz, XOUT, vbx, vby, lane, row, i, j, k, p, ta, tb);
   const bool out = ok && lane >= 2 && lane < 2 + XOUT;
   const double dt = F.s->dt;
   const int order2 = A.order - 1;
   const double* __restrict__ Uin = A.Uin;
-  // back node plane of the own cell (planes exist for p in [0, nd])
+  // back node plane of the own cell; the front plane is the back plane of
+  // the next lane, except at the end of a line
   Plane<DIM> back;
-  if (p >= 0 && p <= nd) load_plane<DIM, D>(M, F, i, j, k, back);
+  if (ok) load_plane<DIM, D>(M, F, i, j, k, back);
   else {
 #pragma unroll
     for (int q = 0; q < NQ; ++q) back.xd[q] = 0.;
@@ -224,6 +282,8 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
   Plane<DIM> front;
 #pragma unroll
   for (int q = 0; q < NQ; ++q) front.xd[q] = __shfl_down_sync(FULL, back.xd[q], 1);
+  if (ok && p == nd - 1)
+    load_plane_xd<DIM, D>(M, F, D == 0 ? i + 1 : i, D == 1 ? j + 1 : j, D == 2 ? k + 1 : k, front);
   long long c = 0;
   double u[NV], den = 1., xc = 0., ondB = 0., ondF = 0.;
   if (ok) {
@@ -252,7 +312,7 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
     for (int v = 0; v < NV; ++v) u[v] = 0.;
   }
   const double fc = back.fc, un = back.un, L = back.L;  // back face of the cell
-  const bool ok_l = __shfl_up_sync(FULL, ok, 1) && lane > 0;
+  const bool ok_l = __shfl_up_sync(FULL, ok, 1) && lane > 0 && p > 0;  // same line
   const double xc_l = __shfl_up_sync(FULL, xc, 1);
   const bool face_b = ok && ok_l;                       // face between p-1 and p
   const bool face_f = __shfl_down_sync(FULL, face_b, 1) && lane < 31;
@@ -322,18 +382,10 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
   constexpr unsigned FULL = 0xffffffffu;
   const long long NN = M.nnode, N = M.ncell;
   const int lane = threadIdx.x % SW_LANES, row = threadIdx.x / SW_LANES;
-  const int r = vby * SW_ROWS + row;
-  const int na = D == 0 ? M.nny : M.nnx;
-  const int nb = D == 2 ? M.nny : M.nnz;
   const int nn = D == 0 ? M.nnx : (D == 1 ? M.nny : M.nnz);
-  if (r >= na * nb) return;  // whole warp leaves together
-  const int ta = r % na, tb = r / na;
-  const int id = vbx * NOUT - 2 + lane;  // node index along D
-  int i, j, k;
-  if (D == 0) { i = id; j = ta; k = tb; }
-  else if (D == 1) { i = ta; j = id; k = tb; }
-  else { i = ta; j = tb; k = id; }
-  const bool ok = id >= 0 && id < nn;
+  if (sweep_warp_empty<D>(M.nnx, M.nny, M.nnz, NOUT, vbx, vby, row)) return;  // whole warp leaves together
+  int i, j, k, id, ta, tb;
+  const bool ok = sweep_lane<D>(M.nnx, M.nny, M.nnz, NOUT, vbx, vby, lane, row, i, j, k, id, ta, tb);
   const bool inner = ok && id > 0 && id < nn - 1;
   const bool out = ok && lane >= 2 && lane < 2 + NOUT;
   long long n = 0;
