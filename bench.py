@@ -89,11 +89,22 @@ def stage_bytes(stage: str, dim: int, ne: int, ncell: int, nnode: int) -> float:
     return 8.0 * per
 
 
-def launches_per_cycle(p) -> int:
-    dirs = sum(1 for n in ((p.nx, p.ny, p.nz) if p.dim == 3 else (p.nx, p.ny)) if n > 1)
-    if p.with_projection:
-        return 2 + 2 * dirs + 2 + 2
-    return 2 + 2
+def max_over_ranks(ms: float, device: str = "cuda") -> float:
+    """Slowest rank's time (all ranks take this collective in the same
+    order); the identity without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank: float, world: int, ms_max: float) -> float:
+    """Whole-job throughput of `world` replicas: all ranks' units over the
+    slowest rank's time."""
+    return world * units_per_rank / (ms_max * 1e-3)
 
 
 class ClockSampler:
@@ -159,49 +170,82 @@ def profile_traffic(workload: str) -> dict:
         return {}
 
 
-def cpu_baseline(workload: str, cycles: int = 20) -> dict:
-    """The CPU oracle on a bounded slab of the workload (same per-cell work),
-    about 10 s of single-core work."""
+def _oracle_slab(workload: str, cells_target: float):
+    """A slab of the workload with the same cell size and about
+    `cells_target` cells (the CPU sample of the reference arm)."""
+    full = build_params(workload)
+    return build_params(workload, min(1.0, (cells_target / full.ncell) ** (1.0 / full.dim)))
+
+
+def _oracle_worker(task):
+    """One host core: the CPU oracle on its own slab, timed after warm-up
+    (spawned process; returns cell-cycles and seconds)."""
+    workload, cells_target, warmup, steps, seed = task
+    sys.path.insert(0, ROOT)
     from tests.oracle import Oracle
-    scale = {"bisod3d": 0.5, "sedov3d": 0.125, "sod2d_lagrange": 1.0}[workload]
-    if workload == "sod2d_lagrange":
-        cycles = 2000
-    p = build_params(workload, scale)
-    o = Oracle(p, cr_pow=False)
-    o.init()
-    o.iterate(1)
+    if workload == "batch2d":
+        import random
+        from mahyco_b200.cases import seeded_two_state
+        rng = random.Random(seed)
+        cases = []
+        while sum(c.ncell for c in cases) < cells_target:
+            cases.append(seeded_two_state(seed * 7919 + len(cases), rng.randint(32, 96)))
+    else:
+        cases = [_oracle_slab(workload, cells_target)]
+    work, sec = 0, 0.0
+    for p in cases:
+        o = Oracle(p, cr_pow=False)
+        o.init()
+        o.iterate(warmup)
+        t0 = time.perf_counter()
+        o.iterate(steps)
+        sec += time.perf_counter() - t0
+        work += p.ncell * steps
+    return work, sec, sum(c.ncell for c in cases)
+
+
+def oracle_throughput(workload: str, steps: int, warmup: int, cores: int | None = None,
+                      cell_cycles_per_core: float = 8e6) -> dict:
+    """The CPU oracle (sequential restatement of the reference path) on
+    every host core at once, one independent slab per core; aggregate
+    cell-cycles/s over the parallel phase."""
+    import multiprocessing as mp
+    cores = cores or len(os.sched_getaffinity(0))
+    wl = "bisod3d" if workload == "serve" else workload
+    cells_target = max(2000.0, cell_cycles_per_core / max(1, steps))
+    tasks = [(wl, cells_target, warmup, steps, 1000 + r) for r in range(cores)]
     t0 = time.perf_counter()
-    o.iterate(cycles)
-    dt = time.perf_counter() - t0
-    return {"value": p.ncell * cycles / dt, "unit": "cell-cycles/s", "cores": 1, "kind": "port",
-            "sample": f"{cycles} iterations of a {p.nx}x{p.ny}x{p.nz if p.dim == 3 else 1} slab of the same "
-                      f"workload ({p.ncell} cells), single-threaded sequential oracle"}
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_oracle_worker, tasks)
+    wall = time.perf_counter() - t0
+    work = sum(r[0] for r in res)
+    slowest = max(r[1] for r in res)
+    return {"value": work / slowest, "unit": "cell-cycles/s", "cores": cores, "kind": "port",
+            "sample": f"{cores} independent {'sets of seeded 2D cases' if wl == 'batch2d' else 'slabs'} of "
+                      f"about {int(res[0][2])} cells of the {wl} workload (same cell size and states), "
+                      f"{steps} timed iterations each after {warmup} warm-up, one spawned process per host "
+                      f"core running the sequential oracle; value = all cores' cell-cycles / slowest core's "
+                      f"time (wall {wall:.1f} s including start-up)"}
+
+
+def cpu_baseline(workload: str, steps: int = 20) -> dict:
+    """Bounded CPU sample reported beside the GPU number (about 10 s)."""
+    return oracle_throughput(workload, steps=steps, warmup=1)
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    base = cpu_baseline(args.workload, cycles=max(1, min(args.steps, 8)))
-    from tests.oracle import Oracle
-    scale = {"bisod3d": 0.25, "sedov3d": 0.125, "sod2d_lagrange": 1.0}[args.workload]
-    p = build_params(args.workload, scale)
-    o = Oracle(p, cr_pow=False)
-    o.init()
-    o.iterate(args.warmup)
-    t0 = time.perf_counter()
-    o.iterate(args.steps)
-    dt = time.perf_counter() - t0
-    v = p.ncell * args.steps / dt
-    base["value"] = v
-    base["sample"] = (f"{args.steps} iterations of a {p.nx}x{p.ny}x{p.nz if p.dim == 3 else 1} slab "
-                      f"({p.ncell} cells) of the workload; the reference itself needs the Arcane "
-                      f"framework and cannot be built here, so its sequential restatement runs")
+    base = oracle_throughput(args.workload, steps=args.steps, warmup=max(1, args.warmup))
+    base["sample"] += ("; the reference itself needs the Arcane framework and cannot be built here, so "
+                       "its sequential CPU restatement (oracle/) runs")
+    v = base["value"]
     out = {"metric": METRIC, "value": v, "unit": "cell-cycles/s", "impl": "reference",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+           "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOADS[args.workload][0], "cells": p.ncell},
+           "config": {"workload": WORKLOADS[args.workload][0]},
            "cpu_baseline": base,
            "e2e": {"value": v, "unit": "cell-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -246,11 +290,8 @@ def run_ours(args):
     launches = h.launches - l0
     ms = e0.elapsed_time(e1)
     st |= h.synchronize()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * ncell * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(ms)
+    value = replica_value(ncell * args.steps, world, ms)
     # -- per-kernel device times (events on the case stream around each group)
     nprof = max(2 * p.dim, min(args.steps, 4 * p.dim))
     stages = h.cycle_timed(nprof)
@@ -309,6 +350,23 @@ def run_ours(args):
                 "h2d_bytes_per_step": ctypes.sizeof(p) / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "timer": "host wall clock; includes case allocation, device init, per-iteration status read-back and final field download"},
     }
+    if world == 1 and not args.no_extras:
+        # the batched and served forms against the plain form, on bounded
+        # samples of their workloads (full runs: --workload batch2d / serve)
+        sub = argparse.Namespace(**vars(args))
+        sub.workload, sub.cases, sub.steps, sub.warmup, sub.plain_sample = "bisod3d", 1024, 12, 0, 128
+        bo = run_batch(sub)
+        out["batched"] = {"value": bo["value"], "plain_value": bo["plain"]["value"],
+                          "batched_vs_plain": bo["batched_vs_plain"], "same_results": bo["plain"]["same_results"],
+                          "config": f"{sub.cases} cases of the batch2d workload, {sub.steps} timed cycles, plain form "
+                                    f"on {bo['plain']['sample_cases']} of them", "gpu_launches": bo["gpu_launches"]}
+        sub = argparse.Namespace(**vars(args))
+        sub.workload, sub.requests, sub.rate, sub.steps, sub.cycles_per_step = "bisod3d", 60, 40.0, 30, 4
+        so = run_serve(sub)
+        out["served"] = {"value": so["value"], "plain_value": so["plain"]["value"],
+                         "served_vs_plain": so["served_vs_plain"], "latency_s": so["latency_s"],
+                         "plain_latency_s": so["plain"]["latency_s"], "failed": len(so["failed"]),
+                         "config": f"{sub.requests} requests of the serve mix at {sub.rate}/s, {sub.steps} iterations each"}
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.workload)
     print(json.dumps(out), flush=True)
@@ -371,11 +429,8 @@ def run_batch(args):
     done = [b.scalars(i) for i in idx]
     t_wall = time.perf_counter() - t_wall0
     bad = sum(1 for d in done if d["iteration"] != limit)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    batched = world * cells * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(ms)
+    batched = replica_value(cells * args.steps, world, ms)
     # -- plain arm on a seeded sample (every k-th case), device time of the
     # same K cycles per case, plus its per-solve wall latency
     k = max(1, len(cases) // args.plain_sample) if args.plain_sample > 0 else 1
@@ -434,9 +489,11 @@ def run_batch(args):
                 "d2h_bytes_per_step": len(cases) * 40 / args.steps,
                 "timer": "host wall clock of the whole batched run: case creation, init, tuning, warm-up, K cycles, status read-back"},
     }
-    print(json.dumps(out), flush=True)
+    if args.workload == "batch2d":
+        print(json.dumps(out), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+    return out
 
 
 def serve_requests(count: int, seed: int = 7):
@@ -523,12 +580,13 @@ def run_serve(args):
         h.scalars()
         h.close()
         service.append(time.perf_counter() - w0)
-    plain = work / sum(service)
     fin, plat = 0.0, []
     for a, sv in zip(arrivals, service):  # FIFO queue under the same arrivals
         fin = max(fin, a) + sv
         plat.append(fin - a)
     plat.sort()
+    # both forms over the same arrivals: work / (last completion - first arrival)
+    plain = work / (fin - arrivals[0])
 
     def pct(v, q):
         return v[min(len(v) - 1, int(q * len(v)))]
@@ -547,15 +605,19 @@ def run_serve(args):
         "served_vs_plain": served / plain,
         "plain": {"value": plain, "unit": "cell-cycles/s",
                   "latency_s": {"p50": pct(plat, 0.5), "p99": pct(plat, 0.99), "max": plat[-1]},
-                  "how": "the same requests solved one after another through their own handles; latency "
-                         "from a FIFO queue of the measured service times under the same arrivals"},
+                  "busy_value": work / sum(service),
+                  "how": "the same requests solved one after another through their own handles (create, init, "
+                         "iterations, status read-back); value and latency from a FIFO queue of the measured "
+                         "service times under the same arrivals; busy_value = work / sum of service times"},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "e2e": {"value": served, "unit": "cell-cycles/s",
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "timer": "host wall clock from the first arrival to the last completion"},
     }
-    print(json.dumps(out), flush=True)
+    if args.workload == "serve":
+        print(json.dumps(out), flush=True)
+    return out
 
 
 def main():
@@ -566,6 +628,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="bisod3d", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain workloads: skip the batched and served samples")
     ap.add_argument("--kernels-only", action="store_true",
                     help="run init, W and K cycles of one case and exit (for ncu launch lists)")
     ap.add_argument("--scale", type=float, default=1.0,

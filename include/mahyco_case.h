@@ -83,6 +83,13 @@ typedef struct mhc_env_params {
   /* initial state */
   double densite_initiale, pression_initiale, energie_initiale, temperature_initiale;
   double vitesse_initiale[3];
+  /* elasto-model: 0 NoModel, 1 DefaultModel (src/elasto/DefaultModelService.cc)
+   * with the EPP shear modulus (elasto-mu-model elastic-cst) and the YEPP
+   * yield strength (elasto-y-model limit-elastic); ordre-rotation 1 or 2 */
+  int elasto_model;
+  int rotation_order;
+  double shear_modulus;
+  double yield_strength;
 } mhc_env_params;
 
 typedef struct mhc_bc {
@@ -126,6 +133,7 @@ typedef struct mhc_case_params {
   double remap_threshold;
   /* EnvSummation period */
   int time_history_period;
+  double coef_antiderive;   /* coef-antiderive: anti-hourglass velocity correction (Lagrange only) */
 } mhc_case_params;
 
 #ifdef __cplusplus

@@ -39,6 +39,8 @@ class EnvParams(C.Structure):
         ("densite_initiale", C.c_double), ("pression_initiale", C.c_double),
         ("energie_initiale", C.c_double), ("temperature_initiale", C.c_double),
         ("vitesse_initiale", C.c_double * 3),
+        ("elasto_model", C.c_int), ("rotation_order", C.c_int),
+        ("shear_modulus", C.c_double), ("yield_strength", C.c_double),
     ]
 
 
@@ -64,6 +66,7 @@ class CaseParams(C.Structure):
         ("ordre_projection", C.c_int), ("projection_limiteur_id", C.c_int),
         ("is_euler_scheme", C.c_int), ("remap_threshold", C.c_double),
         ("time_history_period", C.c_int),
+        ("coef_antiderive", C.c_double),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -91,6 +94,8 @@ def env_defaults(e: EnvParams, eos: int = EOS_PERFECT_GAS) -> None:
     e.densite_initiale, e.pression_initiale = 0.0, 1.0e5
     e.energie_initiale, e.temperature_initiale = 0.0, 0.0
     e.vitesse_initiale[:] = (0.0, 0.0, 0.0)
+    e.elasto_model, e.rotation_order = 0, 1
+    e.shear_modulus, e.yield_strength = 2.94e10, 3.0e8
 
 
 def default_params() -> CaseParams:
@@ -122,6 +127,7 @@ def default_params() -> CaseParams:
     p.is_euler_scheme = 0
     p.remap_threshold = 1.0e-10
     p.time_history_period = 10
+    p.coef_antiderive = 0.0
     return p
 
 
@@ -213,7 +219,18 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
                 setattr(e, attr, v)
         el = ev.find("elasto-model")
         if el is not None and el.get("name") not in (None, "NoModel"):
-            raise NotImplementedError("elasto-plastic models")
+            if el.get("name") != "DefaultModel":
+                raise NotImplementedError(f"elasto-model {el.get('name')}")
+            mu_el, y_el = el.find("elasto-mu-model"), el.find("elasto-y-model")
+            if (mu_el is not None and mu_el.get("name", "EPP") != "EPP") or \
+                    (y_el is not None and y_el.get("name", "YEPP") != "YEPP"):
+                raise NotImplementedError("elasto mu/y models other than EPP/YEPP")
+            e.elasto_model = 1
+            e.rotation_order = _txt(el, "ordre-rotation", 1, int)
+            if mu_el is not None:
+                e.shear_modulus = _txt(mu_el, "elastic-cst", 2.94e10)
+            if y_el is not None:
+                e.yield_strength = _txt(y_el, "limit-elastic", 3.0e8)
         if ev.find("energy-depot") is not None:
             raise NotImplementedError("energy deposit")
     cm = m.find("cas-model")
@@ -256,8 +273,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     g = m.find("gravity")
     if g is not None:
         p.gravity[:] = [float(v) for v in g.text.split()]
-    if _txt(m, "coef-antiderive", 0.0) != 0.0:
-        raise NotImplementedError("coef-antiderive")
+    p.coef_antiderive = _txt(m, "coef-antiderive", 0.0)
     for b in m.findall("boundary-condition"):
         kind = b.find("type").text.strip()
         if kind not in BC_BY_NAME:

@@ -170,10 +170,12 @@ def mie_gruneisen_plate(dim=2, n=(80, 8), L=(0.01, 0.001), remap=False, deltat_i
     return p
 
 
-def bar_impact(n=(80, 400), L=(0.01, 0.05), velocity=200.0, deltat_init=1e-9) -> CaseParams:
+def bar_impact(n=(80, 400), L=(0.01, 0.05), velocity=200.0, deltat_init=1e-9, elasto=True,
+               shear_modulus=26.0e9, yield_strength=0.3e9, coef_antiderive=0.01) -> CaseParams:
     """Aluminium bar (Mie-Gruneisen rho0 2710, c0 5328, s1 1.338, Gamma0 2.0)
     hitting the rigid wall y = 0 at `velocity`: Lagrangian, explicit
-    pressure as in CAS_2D_Lag_Taylor_elasto."""
+    pressure, elasto-plastic DefaultModel (EPP shear modulus, YEPP yield)
+    and anti-hourglass correction as in CAS_2D_Lag_Taylor_elasto."""
     p = default_params()
     _mesh(p, 2, n, L)
     p.nb_env = 1
@@ -182,6 +184,10 @@ def bar_impact(n=(80, 400), L=(0.01, 0.05), velocity=200.0, deltat_init=1e-9) ->
     o.rho0, o.c0, o.s1, o.gamma0 = 2710.0, 5328.0, 1.338, 2.0
     o.densite_initiale, o.pression_initiale = 2710.0, 1.0e5
     o.vitesse_initiale[:] = (0.0, -velocity, 0.0)
+    if elasto:
+        o.elasto_model, o.rotation_order = 1, 1
+        o.shear_modulus, o.yield_strength = shear_modulus, yield_strength
+        p.coef_antiderive = coef_antiderive
     p.cas_model = CASE_TWO_STATE
     p.interface_pos, p.interface_dir = 1e30, 0
     p.pression_explicite = 1
@@ -235,7 +241,34 @@ PARITY_CASES = {
     "adi2d_water_air": (lambda: water_air(deltat_init=1e-6), 80),
     "lag2d_mie_gruneisen": (lambda: mie_gruneisen_plate(deltat_init=1e-8), 100),
     "lag2d_bar_impact": (lambda: bar_impact(n=(8, 40), L=(0.01, 0.05)), 80),
+    "lag2d_bar_impact_rot2": (lambda: _rot2(bar_impact(n=(10, 30), L=(0.01, 0.03), velocity=400.0)), 80),
+    "lag3d_bar_impact": (lambda: _bar3d(), 40),
+    "lag2d_bar_no_elasto": (lambda: bar_impact(n=(8, 40), L=(0.01, 0.05), elasto=False, coef_antiderive=0.0), 80),
+    "lag2d_sod_newton": (lambda: _newton(sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=True, remap=False,
+                                             deltat_max=1e-3, deltat_init=1e-4)), 120),
+    "adi3d_bisod_newton": (lambda: _newton(sod(dim=3, n=(24, 4, 4), L=(1.0, 0.2, 0.2), bi=True,
+                                               limiter=SUPERBEE, deltat_init=1e-3)), 50),
 }
+
+
+def _rot2(p: CaseParams) -> CaseParams:
+    p.env[0].rotation_order = 2
+    return p
+
+
+def _bar3d() -> CaseParams:
+    """3D square bar on the wall z = 0 (elasto, anti-hourglass)."""
+    p = bar_impact(n=(6, 6, 1), L=(0.006, 0.006, 1.0))
+    _mesh(p, 3, (6, 6, 24), (0.006, 0.006, 0.024))
+    p.env[0].vitesse_initiale[:] = (0.0, 0.0, -300.0)
+    p.nb_bc = 0
+    symmetry_bcs(p, ("XMIN", "YMIN", "ZMIN"))
+    return p
+
+
+def _newton(p: CaseParams) -> CaseParams:
+    p.with_newton = 1
+    return p
 
 
 def _order1(p: CaseParams) -> CaseParams:

@@ -19,155 +19,25 @@
 #include <vector>
 
 #include "../../include/mahyco_b200.h"
-#include "mhc_launch.cuh"
-
-using namespace mhc;
+#include "mhc_engine.cuh"
 
 namespace {
 thread_local std::string g_err;
-int set_err(int code, const std::string& msg) {
+}  // namespace
+
+int mhc::set_err(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
-#define CK(x)                                                                              \
-  do {                                                                                     \
-    cudaError_t e_ = (x);                                                                  \
-    if (e_ != cudaSuccess) return set_err(MHC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-enum Stage { S_IDLE = 0, S_SAVED, S_VELOCITY, S_BC, S_POSITION, S_GEOM, S_DENSITY, S_VISCO, S_ELASTO, S_ENERGY, S_REMAP };
-
-inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
-}  // namespace
-
-struct Engine;
-
-struct mhc_case {
-  mhc_case_params P;
-  Mesh M;
-  int DIM = 3, NE = 1, NV = 4;
-  Fields F;
-  Scalars* d_scal = nullptr;
-  mhc_case_params* d_params = nullptr;
-  cudaStream_t stream = nullptr;   // allocation stream (and launches when standalone)
-  bool own_stream = false;
-  std::vector<void*> allocs;
-  long long it_host = 1;           // iteration the next launched cycle runs
-  int stage = S_IDLE;
-  bool initialised = false;
-  Engine* solo = nullptr;          // private engine of a standalone case
-  int slot = -1;                   // index inside its engine
-};
-
-// ---------------------------------------------------------------------------
-// engine
-// ---------------------------------------------------------------------------
-struct DevList {
-  size_t off_cases = 0;  // offsets inside the engine's int arena
-  size_t off_start = 0;
-  int n = 0;             // member cases
-  int total = 0;         // virtual blocks of all members
-};
-
-struct Group {
-  int DIM, NE, EULER, skip;
-  long long it0;               // iteration of the members when the lists were built
-  std::vector<int> members;
-  DevList init_cells, init_nodes, lag_nodes, lag_cells, fin_cells, fin_nodes, dt;
-  DevList sw_cells[3], sw_nodes[3];
-  DevList cases;               // offset into the case-index arena
-};
-
-struct Engine {
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  std::vector<mhc_case*> cases;
-  CaseDesc* d_desc = nullptr;
-  int desc_cap = 0;
-  int* d_ints = nullptr;   // case indices and block prefix sums of every list
-  size_t ints_cap = 0;
-  std::vector<Group> groups;
-  bool dirty = true;
-  long long cycles_since_build = 0;
-  int nsm = 0;
-  // timing
-  bool timing = false;
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  double stage_ms[MHC_NUM_STAGES] = {0};
-  long long stage_launches[MHC_NUM_STAGES] = {0};
-  // graph of one rotation period
-  cudaGraphExec_t graph = nullptr;
-  // grid of the work-list launches: 0 = one block per work item (the block
-  // scheduler balances), k > 0 = k x the blocks the device holds at once
-  // (persistent blocks striding over the list)
-  int grid_scale = 0;
-  // per-phase override of grid_scale (-1 = use grid_scale), set by a tuner
-  int stage_scale[MHC_NUM_STAGES] = {-1, -1, -1, -1, -1, -1, -1};
-  int cur_stage = -1;  // phase being launched (StageTimer scope)
-  // kernels this engine put on the GPU (graph replays count their nodes)
-  long long launches = 0;
-  long long graph_launches = 0;  // kernel nodes of the captured graph
-  // status gather of every case (one kernel + one copy)
-  Scalars* d_gather = nullptr;
-  Scalars* h_gather = nullptr;   // pinned
-  int gather_cap = 0;
-};
 
 namespace {
 
-struct StageTimer {
-  Engine* e;
-  int stage;
-  StageTimer(Engine* e_, int s) : e(e_), stage(s) {
-    e->cur_stage = s;
-    if (e->timing) cudaEventRecord(e->ev[0], e->stream);
-  }
-  ~StageTimer() {
-    e->cur_stage = -1;
-    if (!e->timing) return;
-    cudaEventRecord(e->ev[1], e->stream);
-    cudaEventSynchronize(e->ev[1]);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
-    e->stage_ms[stage] += ms;
-    e->stage_launches[stage] += 1;
-  }
-};
-
-int skip_mask(const mhc_case* h) {
-  int m = 0;
-  if (h->M.ncx == 1) m |= 1;
-  if (h->M.ncy == 1) m |= 2;
-  if (h->DIM == 3 && h->M.ncz == 1) m |= 4;
-  return m;
+size_t lagrange_smem(int dim, bool elasto = false) {
+  return (size_t)(LTX + 1) * (LTY + 1) * ((dim == 3 ? 8 : 4) * 3 * sizeof(double) * (elasto ? 2 : 1) + 1);
 }
 
-// persistent grid for a kernel: resident blocks on the device (cached)
-template <class K>
-int resident_blocks(Engine* e, K kernel, int threads, size_t smem) {
-  static std::map<const void*, int> cache;
-  auto it = cache.find((const void*)kernel);
-  if (it != cache.end()) return it->second * e->nsm;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  cache[(const void*)kernel] = per_sm;
-  return per_sm * e->nsm;
-}
-
-template <class K, class... Args>
-void plaunch(Engine* e, K kernel, int threads, size_t smem, const DevList& L, Args... args) {
-  if (L.total <= 0) return;
-  const int sc = (e->cur_stage >= 0 && e->stage_scale[e->cur_stage] >= 0) ? e->stage_scale[e->cur_stage] : e->grid_scale;
-  int grid = sc == 0 ? L.total : std::min(L.total, resident_blocks(e, kernel, threads, smem) * sc);
-  const PhaseList pl{e->d_ints + L.off_cases, e->d_ints + L.off_start, L.n, L.total};
-  kernel<<<grid, threads, smem, e->stream>>>(e->d_desc, pl, args...);
-  ++e->launches;
-}
-
-size_t lagrange_smem(int dim) {
-  return (size_t)(LTX + 1) * (LTY + 1) * ((dim == 3 ? 8 : 4) * 3 * sizeof(double) + 1);
-}
+bool case_elasto(const mhc_case* h) { return h->P.env[0].elasto_model != 0; }
+bool case_hourglass(const mhc_case* h) { return !h->P.with_projection && h->P.coef_antiderive != 0.; }
 
 // -- list building -----------------------------------------------------------
 int engine_rebuild(Engine* e) {
@@ -194,17 +64,20 @@ int engine_rebuild(Engine* e) {
   }
   if (nc) CK(cudaMemcpyAsync(e->d_desc, desc.data(), nc * sizeof(CaseDesc), cudaMemcpyHostToDevice, e->stream));
   // groups
-  std::map<std::tuple<int, int, int, int, int>, int> gidx;
+  std::map<std::tuple<int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
     int euler = h->P.with_projection ? 1 : 0;
     int sens = (int)((h->it_host - 1) % h->DIM);
-    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens);
+    const int el = case_elasto(h) ? 1 : 0, hg = case_hourglass(h) ? 1 : 0;
+    const int lim = h->P.ordre_projection == 1 ? LIM_ORDER1 : h->P.projection_limiteur_id;
+    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim);
     auto it = gidx.find(key);
     if (it == gidx.end()) {
       Group g;
       g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
+      g.EL = el; g.HG = hg; g.LIM = lim;
       gidx[key] = (int)e->groups.size();
       e->groups.push_back(g);
       it = gidx.find(key);
@@ -258,27 +131,6 @@ int engine_rebuild(Engine* e) {
 }
 
 // -- phase launches -------------------------------------------------------------
-#define DISPATCH_GROUP(g, CALL)                                   \
-  do {                                                            \
-    if ((g).DIM == 2) {                                           \
-      constexpr int DIM_ = 2;                                     \
-      switch ((g).NE) {                                           \
-        case 1: { constexpr int NE_ = 1; CALL; } break;           \
-        case 2: { constexpr int NE_ = 2; CALL; } break;           \
-        case 3: { constexpr int NE_ = 3; CALL; } break;           \
-        default: { constexpr int NE_ = 4; CALL; } break;          \
-      }                                                           \
-    } else {                                                      \
-      constexpr int DIM_ = 3;                                     \
-      switch ((g).NE) {                                           \
-        case 1: { constexpr int NE_ = 1; CALL; } break;           \
-        case 2: { constexpr int NE_ = 2; CALL; } break;           \
-        case 3: { constexpr int NE_ = 3; CALL; } break;           \
-        default: { constexpr int NE_ = 4; CALL; } break;          \
-      }                                                           \
-    }                                                             \
-  } while (0)
-
 void launch_init(Engine* e) {
   for (Group& g : e->groups) {
     DISPATCH_GROUP(g, (plaunch(e, kb_init_cells<DIM_, NE_>, CT, 0, g.init_cells)));
@@ -286,27 +138,49 @@ void launch_init(Engine* e) {
   }
 }
 
+template <int DIM, bool EL, bool HG>
+void lag_nodes_launch(Engine* e, Group& g) {
+  static bool attr = false;
+  const size_t smem = lagrange_smem(DIM, EL);
+  if (!attr) {
+    cudaFuncSetAttribute(kb_lagrange_nodes<DIM, EL, HG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  plaunch(e, kb_lagrange_nodes<DIM, EL, HG>, LAG_THREADS, smem, g.lag_nodes);
+  if (HG) plaunch(e, kb_hourglass<DIM>, CT, 0, g.fin_nodes);
+}
+
 template <int DIM>
-void lag_nodes_attr() {
-  static bool done = false;
-  if (done) return;
-  cudaFuncSetAttribute(kb_lagrange_nodes<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lagrange_smem(DIM));
-  done = true;
+void lag_nodes_dispatch(Engine* e, Group& g) {
+  if (g.EL) {
+    if (g.HG) lag_nodes_launch<DIM, true, true>(e, g);
+    else lag_nodes_launch<DIM, true, false>(e, g);
+  } else {
+    if (g.HG) lag_nodes_launch<DIM, false, true>(e, g);
+    else lag_nodes_launch<DIM, false, false>(e, g);
+  }
 }
 
 void launch_lagrange_nodes(Engine* e) {
   StageTimer tm(e, MHC_STAGE_LAGRANGE_NODES);
   for (Group& g : e->groups) {
-    if (g.DIM == 2) { lag_nodes_attr<2>(); plaunch(e, kb_lagrange_nodes<2>, LAG_THREADS, lagrange_smem(2), g.lag_nodes); }
-    else { lag_nodes_attr<3>(); plaunch(e, kb_lagrange_nodes<3>, LAG_THREADS, lagrange_smem(3), g.lag_nodes); }
+    if (g.DIM == 2) lag_nodes_dispatch<2>(e, g);
+    else lag_nodes_dispatch<3>(e, g);
   }
 }
 
 void launch_lagrange_cells(Engine* e) {
   StageTimer tm(e, MHC_STAGE_LAGRANGE_CELLS);
   for (Group& g : e->groups) {
-    if (g.EULER) DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true>, CT, 0, g.lag_cells)));
-    else DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, false>, CT, 0, g.lag_cells)));
+    if (g.EL) {
+      // elasto cases: one environment, Lagrangian (validated at creation)
+      if (g.DIM == 2) plaunch(e, kb_lagrange_cells<2, 1, false, true>, CT, 0, g.lag_cells);
+      else plaunch(e, kb_lagrange_cells<3, 1, false, true>, CT, 0, g.lag_cells);
+    } else if (g.EULER) {
+      DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true, false>, CT, 0, g.lag_cells)));
+    } else {
+      DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, false, false>, CT, 0, g.lag_cells)));
+    }
   }
 }
 
@@ -325,22 +199,6 @@ int group_dirs(Engine* e, const Group& g, int* dirs) {
   return n;
 }
 
-template <int DIM, int NE>
-void sweep_step(Engine* e, Group& g, int D, int k) {
-  {
-    StageTimer tm(e, MHC_STAGE_SWEEP_CELLS);
-    if (D == 0) plaunch(e, kb_sweep_cells<DIM, NE, 0>, SW_THREADS, 0, g.sw_cells[0], k);
-    else if (D == 1) plaunch(e, kb_sweep_cells<DIM, NE, 1>, SW_THREADS, 0, g.sw_cells[1], k);
-    else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells<DIM, NE, 2>, SW_THREADS, 0, g.sw_cells[2], k);
-  }
-  {
-    StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
-    if (D == 0) plaunch(e, kb_sweep_nodes<DIM, NE, 0>, SW_THREADS, 0, g.sw_nodes[0], k);
-    else if (D == 1) plaunch(e, kb_sweep_nodes<DIM, NE, 1>, SW_THREADS, 0, g.sw_nodes[1], k);
-    else if constexpr (DIM == 3) plaunch(e, kb_sweep_nodes<DIM, NE, 2>, SW_THREADS, 0, g.sw_nodes[2], k);
-  }
-}
-
 // RemapADIService::appliRemap (RemapADIService.cc:15-90) for every group
 void launch_remap(Engine* e) {
   for (int k = 0; k < 3; ++k) {
@@ -349,7 +207,7 @@ void launch_remap(Engine* e) {
       int dirs[3];
       int nd = group_dirs(e, g, dirs);
       if (k >= nd) continue;
-      DISPATCH_GROUP(g, (sweep_step<DIM_, NE_>(e, g, dirs[k], k)));
+      sweep_step_any(e, g, dirs[k], k);
     }
   }
   for (Group& g : e->groups) {
@@ -496,7 +354,7 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   ncell = (long long)p->nx * p->ny * (dim == 3 ? p->nz : 1);
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
   int ne = p->nb_env, nv = 3 * ne + 1;
-  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne;
+  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0);
   long long nodes = 4 + 6 + 10;
   return cells * ncell + nodes * nnode;
 }
@@ -505,13 +363,23 @@ int validate(const mhc_case_params* p) {
   if (p->dim != 2 && p->dim != 3) return set_err(MHC_ERR_ARG, "dim must be 2 or 3");
   if (p->nx < 1 || p->ny < 1 || (p->dim == 3 && p->nz < 1)) return set_err(MHC_ERR_ARG, "mesh size");
   if (p->nb_env < 1 || p->nb_env > MHC_MAX_ENV) return set_err(MHC_ERR_ARG, "nb_env must be 1..4");
+  if ((long long)(p->nx + 1) * (p->ny + 1) * (p->dim == 3 ? p->nz + 1 : 1) > INT_MAX)
+    return set_err(MHC_ERR_ARG, "a case holds at most 2^31 - 1 nodes");
   if (p->nb_bc < 0 || p->nb_bc > MHC_MAX_BC) return set_err(MHC_ERR_ARG, "nb_bc");
-  if (p->with_newton) return set_err(MHC_ERR_UNSUPPORTED, "with-newton energy update is not implemented");
   if (p->ordre_projection < 1 || p->ordre_projection > 2)
     return set_err(MHC_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");
   if (p->projection_limiteur_id < 0 || p->projection_limiteur_id > 2)
     return set_err(MHC_ERR_UNSUPPORTED, "only the classical limiters (0 minmod, 1 superbee, 2 vanleer)");
   if (p->is_euler_scheme != MHC_EULER_FULL) return set_err(MHC_ERR_UNSUPPORTED, "is-euler-scheme must be Full");
+  for (int e = 0; e < p->nb_env; ++e) {
+    const mhc_env_params& o = p->env[e];
+    if (o.elasto_model < 0 || o.elasto_model > 1) return set_err(MHC_ERR_UNSUPPORTED, "elasto-model must be NoModel or DefaultModel");
+    if (o.elasto_model == 0) continue;
+    if (p->nb_env != 1 || p->with_projection)
+      return set_err(MHC_ERR_UNSUPPORTED, "elasto-plasticity needs one environment and a Lagrangian loop");
+    if (o.rotation_order != 1 && o.rotation_order != 2) return set_err(MHC_ERR_UNSUPPORTED, "ordre-rotation must be 1 or 2");
+    if (!(o.shear_modulus > 0.) || !(o.yield_strength > 0.)) return set_err(MHC_ERR_ARG, "shear modulus and yield strength must be > 0");
+  }
   for (int e = 0; e < p->nb_env; ++e) {
     if (p->env[e].density_damage_thresold != 0.0 || p->env[e].tension_damage_thresold > -1.e12)
       return set_err(MHC_ERR_UNSUPPORTED, "damage thresholds other than the defaults");
@@ -592,6 +460,7 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
     F.Ud[b] = (double*)alloc(5 * NN * sizeof(double));
   }
   F.mflux = (double*)alloc(h->NE * N * sizeof(double));
+  if (h->P.env[0].elasto_model) F.S = (double*)alloc(6 * N * sizeof(double));
   h->d_scal = (Scalars*)alloc(sizeof(Scalars));
   h->d_params = (mhc_case_params*)alloc(sizeof(mhc_case_params));
   F.s = h->d_scal;
@@ -599,6 +468,10 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
     cudaGetLastError();
     case_free(h);
     return set_err(MHC_ERR_NOMEM, "device allocation failed");
+  }
+  if (F.S && cudaMemsetAsync(F.S, 0, 6 * N * sizeof(double), h->stream) != cudaSuccess) {
+    case_free(h);
+    return set_err(MHC_ERR_CUDA, "memset");
   }
   if (h->NE > 1) {
     // env slots of cells that never hold the env read as zero

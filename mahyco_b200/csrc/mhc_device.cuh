@@ -18,6 +18,7 @@ __device__ __forceinline__ R3 operator-(R3 a, R3 b) { return {a.x - b.x, a.y - b
 __device__ __forceinline__ R3 operator*(double s, R3 a) { return {s * a.x, s * a.y, s * a.z}; }
 __device__ __forceinline__ R3 operator*(R3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
 __device__ __forceinline__ R3 operator/(R3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ R3 operator-(R3 a) { return {-a.x, -a.y, -a.z}; }
 __device__ __forceinline__ double dot(R3 a, R3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 // math::vecMul
 __device__ __forceinline__ R3 vecmul(R3 u, R3 v) {
@@ -85,11 +86,13 @@ struct Mesh {
   double h[3];         // L/n per direction
 };
 
+// linear ids in 32-bit arithmetic: a case has fewer than 2^31 nodes
+// (checked at creation), and every offset into a field array stays 64-bit
 __device__ __forceinline__ long long cell_id(const Mesh& M, int i, int j, int k) {
-  return i + (long long)M.ncx * (j + (long long)M.ncy * k);
+  return (long long)(unsigned)(i + M.ncx * (j + M.ncy * k));
 }
 __device__ __forceinline__ long long node_id(const Mesh& M, int i, int j, int k) {
-  return i + (long long)M.nnx * (j + (long long)M.nny * k);
+  return (long long)(unsigned)(i + M.nnx * (j + M.nny * k));
 }
 __device__ __forceinline__ void cell_ijk(const Mesh& M, long long c, int& i, int& j, int& k) {
   i = (int)(c % M.ncx);
@@ -187,6 +190,22 @@ __device__ __forceinline__ double flux_limiter(int id, double r) {
   if (id == 1) return smax(0.0, smax(smin(2.0 * r, 1.0), smin(r, 2.0)));
   if (id == 2) return (r <= 0.0) ? 0.0 : 2.0 * r / (1.0 + r);
   return 0.0;
+}
+// limiter id as a template argument (LIM_ORDER1: first-order remap, no slope)
+constexpr int LIM_ORDER1 = 3;
+template <int LIM>
+__device__ __forceinline__ double flux_limiter_t(double r) {
+  if (LIM == 0) return smax(0.0, smin(1.0, r));
+  if (LIM == 1) return smax(0.0, smax(smin(2.0 * r, 1.0), smin(r, 2.0)));
+  if (LIM == 2) return (r <= 0.0) ? 0.0 : 2.0 * r / (1.0 + r);
+  return 0.0;
+}
+template <int LIM>
+__device__ __forceinline__ double limited_gradient_t(double gb, double gf) {
+  double g = 0.;
+  if (gb != 0.) g += 0.5 * (flux_limiter_t<LIM>(gf / gb) * gb);
+  if (gf != 0.) g += 0.5 * (flux_limiter_t<LIM>(gb / gf) * gf);
+  return g;
 }
 __device__ __forceinline__ double limited_gradient(int id, double gb, double gf) {
   double g = 0.;

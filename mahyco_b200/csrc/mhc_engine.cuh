@@ -1,0 +1,185 @@
+// mhc_engine.cuh -- host-side engine shared by the C ABI translation units:
+// cases, groups of cases that share kernel templates, per-phase work lists,
+// and the persistent launch helper.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/mahyco_b200.h"
+#include "mhc_launch.cuh"
+
+namespace mhc {
+
+// records the calling thread's error message (mhc_last_error) and returns code
+int set_err(int code, const std::string& msg);
+
+#define CK(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess) return ::mhc::set_err(MHC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+enum Stage { S_IDLE = 0, S_SAVED, S_VELOCITY, S_BC, S_POSITION, S_GEOM, S_DENSITY, S_VISCO, S_ELASTO, S_ENERGY, S_REMAP };
+
+inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
+
+}  // namespace mhc
+
+struct Engine;
+
+using namespace mhc;
+
+struct mhc_case {
+  mhc_case_params P;
+  Mesh M;
+  int DIM = 3, NE = 1, NV = 4;
+  Fields F;
+  Scalars* d_scal = nullptr;
+  mhc_case_params* d_params = nullptr;
+  cudaStream_t stream = nullptr;   // allocation stream (and launches when standalone)
+  bool own_stream = false;
+  std::vector<void*> allocs;
+  long long it_host = 1;           // iteration the next launched cycle runs
+  int stage = S_IDLE;
+  bool initialised = false;
+  Engine* solo = nullptr;          // private engine of a standalone case
+  int slot = -1;                   // index inside its engine
+};
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+struct DevList {
+  size_t off_cases = 0;  // offsets inside the engine's int arena
+  size_t off_start = 0;
+  int n = 0;             // member cases
+  int total = 0;         // virtual blocks of all members
+};
+
+struct Group {
+  int DIM, NE, EULER, skip;
+  int EL = 0, HG = 0;          // elasto-plastic model; anti-hourglass correction
+  int LIM = 0;                 // remap slope limiter id, or LIM_ORDER1 for a first-order remap
+  long long it0;               // iteration of the members when the lists were built
+  std::vector<int> members;
+  DevList init_cells, init_nodes, lag_nodes, lag_cells, fin_cells, fin_nodes, dt;
+  DevList sw_cells[3], sw_nodes[3];
+  DevList cases;               // offset into the case-index arena
+};
+
+struct Engine {
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<mhc_case*> cases;
+  CaseDesc* d_desc = nullptr;
+  int desc_cap = 0;
+  int* d_ints = nullptr;   // case indices and block prefix sums of every list
+  size_t ints_cap = 0;
+  std::vector<Group> groups;
+  bool dirty = true;
+  long long cycles_since_build = 0;
+  int nsm = 0;
+  // timing
+  bool timing = false;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double stage_ms[MHC_NUM_STAGES] = {0};
+  long long stage_launches[MHC_NUM_STAGES] = {0};
+  // graph of one rotation period
+  cudaGraphExec_t graph = nullptr;
+  // grid of the work-list launches: 0 = one block per work item (the block
+  // scheduler balances), k > 0 = k x the blocks the device holds at once
+  // (persistent blocks striding over the list)
+  int grid_scale = 0;
+  // per-phase override of grid_scale (-1 = use grid_scale), set by a tuner
+  int stage_scale[MHC_NUM_STAGES] = {-1, -1, -1, -1, -1, -1, -1};
+  int cur_stage = -1;  // phase being launched (StageTimer scope)
+  // kernels this engine put on the GPU (graph replays count their nodes)
+  long long launches = 0;
+  long long graph_launches = 0;  // kernel nodes of the captured graph
+  // status gather of every case (one kernel + one copy)
+  Scalars* d_gather = nullptr;
+  Scalars* h_gather = nullptr;   // pinned
+  int gather_cap = 0;
+};
+
+
+struct StageTimer {
+  Engine* e;
+  int stage;
+  StageTimer(Engine* e_, int s) : e(e_), stage(s) {
+    e->cur_stage = s;
+    if (e->timing) cudaEventRecord(e->ev[0], e->stream);
+  }
+  ~StageTimer() {
+    e->cur_stage = -1;
+    if (!e->timing) return;
+    cudaEventRecord(e->ev[1], e->stream);
+    cudaEventSynchronize(e->ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+    e->stage_ms[stage] += ms;
+    e->stage_launches[stage] += 1;
+  }
+};
+
+inline int skip_mask(const mhc_case* h) {
+  int m = 0;
+  if (h->M.ncx == 1) m |= 1;
+  if (h->M.ncy == 1) m |= 2;
+  if (h->DIM == 3 && h->M.ncz == 1) m |= 4;
+  return m;
+}
+
+// persistent grid for a kernel: resident blocks on the device (cached)
+template <class K>
+inline int resident_blocks(Engine* e, K kernel, int threads, size_t smem) {
+  static std::map<const void*, int> cache;
+  auto it = cache.find((const void*)kernel);
+  if (it != cache.end()) return it->second * e->nsm;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  cache[(const void*)kernel] = per_sm;
+  return per_sm * e->nsm;
+}
+
+template <class K, class... Args>
+inline void plaunch(Engine* e, K kernel, int threads, size_t smem, const DevList& L, Args... args) {
+  if (L.total <= 0) return;
+  const int sc = (e->cur_stage >= 0 && e->stage_scale[e->cur_stage] >= 0) ? e->stage_scale[e->cur_stage] : e->grid_scale;
+  int grid = sc == 0 ? L.total : std::min(L.total, resident_blocks(e, kernel, threads, smem) * sc);
+  const PhaseList pl{e->d_ints + L.off_cases, e->d_ints + L.off_start, L.n, L.total};
+  kernel<<<grid, threads, smem, e->stream>>>(e->d_desc, pl, args...);
+  ++e->launches;
+}
+
+
+#define DISPATCH_GROUP(g, CALL)                                   \
+  do {                                                            \
+    if ((g).DIM == 2) {                                           \
+      constexpr int DIM_ = 2;                                     \
+      switch ((g).NE) {                                           \
+        case 1: { constexpr int NE_ = 1; CALL; } break;           \
+        case 2: { constexpr int NE_ = 2; CALL; } break;           \
+        case 3: { constexpr int NE_ = 3; CALL; } break;           \
+        default: { constexpr int NE_ = 4; CALL; } break;          \
+      }                                                           \
+    } else {                                                      \
+      constexpr int DIM_ = 3;                                     \
+      switch ((g).NE) {                                           \
+        case 1: { constexpr int NE_ = 1; CALL; } break;           \
+        case 2: { constexpr int NE_ = 2; CALL; } break;           \
+        case 3: { constexpr int NE_ = 3; CALL; } break;           \
+        default: { constexpr int NE_ = 4; CALL; } break;          \
+      }                                                           \
+    }                                                             \
+  } while (0)
+
+
+// one performed sweep (cells, then nodes) of direction D as the k-th of the
+// cycle, for the members of a group (mhc_sweeps.cu)
+void sweep_step_any(Engine* e, Group& g, int D, int k);

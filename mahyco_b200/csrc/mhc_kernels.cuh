@@ -49,6 +49,7 @@ struct Fields {
   double* U[2];
   double* mflux;
   double* Ud[2];
+  double* S;               // elasto: stress deviator [6][ncell] (xx yy zz xy yz zx)
   Scalars* s;
 };
 
@@ -107,6 +108,34 @@ __device__ __forceinline__ void eos_apply(const mhc_env_params& o, double rho, d
     double p2 = mg_pressure(o, rho + 1.e-7, e);
     c = ((p2 - p1) > 0.) ? sqrt((p2 - p1) / 2.e-7) : 1.e4;
   }
+}
+
+// applyOneCellEOS (PerfectGas 71-88, StiffenedGas 67-83, MieGruneisen
+// 101-146): pressure and dp/de of one environment cell
+__device__ __forceinline__ void eos_one_cell(const mhc_env_params& o, double rho, double e, double& p, double& dpde) {
+  if (o.eos == MHC_EOS_PERFECT_GAS) {
+    double g = o.adiabatic_cst;
+    p = (g - 1.) * rho * e;
+    dpde = (g - 1.) * rho;
+  } else if (o.eos == MHC_EOS_STIFFENED_GAS) {
+    double g = o.adiabatic_cst, pinf = o.limit_tension;
+    p = ((g - 1.) * rho * e) - (g * pinf);
+    dpde = (g - 1.) * rho;
+  } else {
+    double J = o.rho0 / rho;
+    double mu = 1. / J - 1.;
+    p = mg_pressure(o, rho, e);
+    dpde = (o.gamma0 + o.a * mu);
+  }
+}
+
+// residual of the energy equation and its derivative (fvnr, fvnrderiv:
+// MahycoModule.h:378-386)
+__device__ __forceinline__ double fvnr(double e, double p, double en, double qnn1, double pn, double rn1, double rn) {
+  return e - en + 0.5 * (p + pn + 2. * qnn1) * (1. / rn1 - 1. / rn);
+}
+__device__ __forceinline__ double fvnrderiv(double dpde, double rn1, double rn) {
+  return 1. + 0.5 * dpde * (1. / rn1 - 1. / rn);
 }
 
 // IEquationOfState::initEOS for one environment cell: (p, rho) -> (e, c)
@@ -344,28 +373,36 @@ constexpr int LTX = 15, LTY = 15;                    // node columns of a tile
 constexpr int LAG_THREADS = (LTX + 1) * (LTY + 1);   // one thread per cell of a layer
 constexpr int LZCHUNK = 16;
 
-template <int DIM>
+// EL: elasto-plastic forces -S_n.C_n added after the pressure forces
+// (MahycoModule.cc:467-474).  HG: the anti-hourglass correction follows
+// (kb_hourglass), so this pass only writes the uncorrected velocity into
+// the dual-remap scratch Ud[0] (unused by a Lagrangian run).
+template <int DIM, bool EL, bool HG>
 __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F,
                                                     int bx, int by, int bz) {
   const int euler = P.with_projection ? 1 : 0;
   constexpr int CW = LTX + 1, CH = LTY + 1, NCL = CW * CH;
+  constexpr int NBN = DIM == 3 ? 8 : 4;
   extern __shared__ double smem_dyn[];
-  double* corner = smem_dyn;  // [NCL][NBN][3] corner forces of one cell layer
-  unsigned char* cvalid = reinterpret_cast<unsigned char*>(smem_dyn + NCL * (DIM == 3 ? 8 : 4) * 3);
+  double* corner = smem_dyn;                      // [NCL][NBN][3] pressure corner forces of one layer
+  double* ecorner = smem_dyn + NCL * NBN * 3;     // [NCL][NBN][3] elasto corner forces (EL)
+  unsigned char* cvalid = reinterpret_cast<unsigned char*>(smem_dyn + NCL * NBN * 3 * (EL ? 2 : 1));
   const int tx = threadIdx.x % LTX, ty = threadIdx.x / LTX;
   const int i0 = bx * LTX, j0 = by * LTY;
   const int ni = i0 + tx, nj = j0 + ty;
   const bool node_ok = threadIdx.x < LTX * LTY && ni < M.nnx && nj < M.nny;
-  const int NBN = DIM == 3 ? 8 : 4;
   const double dt = F.s->dt;
   const double dth = 0.5 * (F.s->old_dt + dt);
   const double t = F.s->t;
+  const long long N = M.ncell, NN = M.nnode;
   int kz0 = 0, kz1 = 1;
   if (DIM == 3) {
     kz0 = bz * LZCHUNK;
     kz1 = min(kz0 + LZCHUNK, M.nnz);
   }
   R3 S = {0., 0., 0.};
+  R3 eprev[4];  // EL, 3D: elasto terms of the layer below, kept until the pressure sum is complete
+  bool eok[4] = {false, false, false, false};
   for (int L = (DIM == 3 ? kz0 - 1 : 0); L < (DIM == 3 ? kz1 : 1); ++L) {
     // corner forces of cell layer L
     for (int cl = threadIdx.x; cl < NCL; cl += LAG_THREADS) {
@@ -397,49 +434,158 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
         R3 fv = pr * cq[l];
         dst[3 * l] = fv.x; dst[3 * l + 1] = fv.y; dst[3 * l + 2] = fv.z;
       }
+      if (EL) {
+        // force_tensor = -S_n; prodTensVec(t, v) = (t.x.v, t.y.v, t.z.v)
+        const double sxx = F.S[cc], syy = F.S[N + cc], szz = F.S[2 * N + cc];
+        const double sxy = F.S[3 * N + cc], syz = F.S[4 * N + cc], szx = F.S[5 * N + cc];
+        const R3 rx = {-sxx, -sxy, -szx}, ry = {-sxy, -syy, -syz}, rz = {-szx, -syz, -szz};
+        double* edst = &ecorner[cl * NBN * 3];
+        for (int l = 0; l < NBN; ++l) {
+          edst[3 * l] = dot(rx, cq[l]); edst[3 * l + 1] = dot(ry, cq[l]); edst[3 * l + 2] = dot(rz, cq[l]);
+        }
+      }
     }
     __syncthreads();
     if (node_ok) {
       // cells around node (ni,nj): local index (a,b) = (tx + di, ty + dj), di,dj in {0,1}
       const int c00 = ty * CW + tx, c10 = ty * CW + tx + 1, c01 = (ty + 1) * CW + tx, c11 = (ty + 1) * CW + tx + 1;
-      auto add = [&](R3& acc, int cl, int l) {
+      auto add = [&](R3& acc, const double* arr, int cl, int l) {
         if (!cvalid[cl]) return;
-        const double* src = &corner[cl * NBN * 3 + 3 * l];
+        const double* src = &arr[cl * NBN * 3 + 3 * l];
         acc.x = acc.x + src[0]; acc.y = acc.y + src[1]; acc.z = acc.z + src[2];
+      };
+      auto get = [&](const double* arr, int cl, int l, R3& out) {
+        if (!cvalid[cl]) { out = {0., 0., 0.}; return false; }
+        const double* src = &arr[cl * NBN * 3 + 3 * l];
+        out = {src[0], src[1], src[2]};
+        return true;
       };
       int kplane = DIM == 3 ? L : 0;
       if (DIM == 2 || L >= kz0) {
-        // bottoms of layer L complete node plane L
-        if (DIM == 3) { add(S, c00, 2); add(S, c10, 3); add(S, c01, 1); add(S, c11, 0); }
-        else { add(S, c00, 2); add(S, c10, 3); add(S, c01, 1); add(S, c11, 0); }
+        // bottoms of layer L complete node plane L (cells in ascending id)
+        add(S, corner, c00, 2); add(S, corner, c10, 3); add(S, corner, c01, 1); add(S, corner, c11, 0);
+        if (EL) {
+          // elasto terms after the complete pressure sum, cells in ascending id
+          if (DIM == 3) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (eok[q]) S = S + eprev[q];
+          }
+          add(S, ecorner, c00, 2); add(S, ecorner, c10, 3); add(S, ecorner, c01, 1); add(S, ecorner, c11, 0);
+        }
         long long n = node_id(M, ni, nj, kplane);
         double mnode = F.mn[n];
         double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
         double f = dth / mnode;
         vx = vx + f * S.x; vy = vy + f * S.y; vz = vz + f * S.z;
         vx = vx + dth * P.gravity[0]; vy = vy + dth * P.gravity[1]; vz = vz + dth * P.gravity[2];
-        const double eps = 1.e-8;
-        for (int b = 0; b < P.nb_bc; ++b) {
-          const mhc_bc& bc = P.bc[b];
-          if ((t - dt * (1 - eps)) < bc.tdebut) continue;
-          if ((t - dt * (1 - eps)) > bc.tfin) continue;
-          if (!node_on_surface(M, ni, nj, kplane, bc.surface)) continue;
-          if (bc.kind == MHC_BC_VX) vx = bc.value;
-          else if (bc.kind == MHC_BC_VY) vy = bc.value;
-          else if (bc.kind == MHC_BC_VZ) vz = bc.value;
+        if (HG) {
+          F.Ud[0][n] = vx; F.Ud[0][NN + n] = vy; F.Ud[0][2 * NN + n] = vz;
+        } else {
+          const double eps = 1.e-8;
+          for (int b = 0; b < P.nb_bc; ++b) {
+            const mhc_bc& bc = P.bc[b];
+            if ((t - dt * (1 - eps)) < bc.tdebut) continue;
+            if ((t - dt * (1 - eps)) > bc.tfin) continue;
+            if (!node_on_surface(M, ni, nj, kplane, bc.surface)) continue;
+            if (bc.kind == MHC_BC_VX) vx = bc.value;
+            else if (bc.kind == MHC_BC_VY) vy = bc.value;
+            else if (bc.kind == MHC_BC_VZ) vz = bc.value;
+          }
+          R3 x = euler ? node_x0(M, ni, nj, kplane) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+          F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
+          F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
         }
-        R3 x = euler ? node_x0(M, ni, nj, kplane) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
-        F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
-        F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
       }
       if (DIM == 3 && L + 1 < kz1) {
         // tops of layer L start node plane L+1
         S = {0., 0., 0.};
-        add(S, c00, 6); add(S, c10, 7); add(S, c01, 5); add(S, c11, 4);
+        add(S, corner, c00, 6); add(S, corner, c10, 7); add(S, corner, c01, 5); add(S, corner, c11, 4);
+        if (EL) {
+          eok[0] = get(ecorner, c00, 6, eprev[0]);
+          eok[1] = get(ecorner, c10, 7, eprev[1]);
+          eok[2] = get(ecorner, c01, 5, eprev[2]);
+          eok[3] = get(ecorner, c11, 4, eprev[3]);
+        }
       }
     }
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Anti-hourglass correction of a Lagrangian run (MahycoModule.cc:497-555),
+// then applyBoundaryCondition and updatePosition.  Reads the uncorrected
+// velocities the node pass left in Ud[0]; each node gathers the corrections
+// of its cells in ascending cell id.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long n = bx * (long long)CT + threadIdx.x;
+  if (n >= M.nnode) return;
+  const long long NN = M.nnode;
+  int i, j, k;
+  node_ijk(M, n, i, j, k);
+  const double coeff = P.coef_antiderive;
+  const double* ux = F.Ud[0];
+  const double* uy = ux + NN;
+  const double* uz = ux + 2 * NN;
+  const double nb = (double)(((i > 0 && i < M.nnx - 1) ? 2 : 1) * ((j > 0 && j < M.nny - 1) ? 2 : 1) *
+                             (DIM == 3 ? ((k > 0 && k < M.nnz - 1) ? 2 : 1) : 1));
+  R3 h = {0., 0., 0.};
+  for (int dk = (DIM == 3 ? -1 : 0); dk <= 0; ++dk)
+    for (int dj = -1; dj <= 0; ++dj)
+      for (int di = -1; di <= 0; ++di) {
+        const int ci = i + di, cj = j + dj, ck = k + dk;
+        if (ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy) continue;
+        if (DIM == 3 && (ck < 0 || ck >= M.ncz)) continue;
+        const int oa = -di, ob = -dj, oc = -dk;  // offset of the node in the cell
+        const int l = oc * 4 + (ob ? (oa ? 2 : 3) : (oa ? 1 : 0));
+        R3 v[8];
+#pragma unroll
+        for (int q = 0; q < (DIM == 3 ? 8 : 4); ++q) {
+          int a, b, c;
+          local_node_offset(q, a, b, c);
+          const long long m = node_id(M, ci + a, cj + b, ck + c);
+          v[q] = {ux[m], uy[m], uz[m]};
+        }
+        if (DIM == 2) {
+          const R3 psi = coeff * (v[0] + v[2] - v[1] - v[3]);
+          if (l == 0 || l == 2) h = h + 1. / nb * psi;
+          else h = h - 1. / nb * psi;
+        } else {
+          const R3 p1 = coeff * (v[0] + v[1] - v[2] - v[3] - v[4] - v[5] + v[6] + v[7]);
+          const R3 p2 = coeff * (v[0] - v[1] - v[2] + v[3] - v[4] + v[5] + v[6] - v[7]);
+          const R3 p3 = coeff * (v[0] - v[1] + v[2] - v[3] + v[4] - v[5] + v[6] - v[7]);
+          const R3 p4 = coeff * (-v[0] + v[1] - v[2] + v[3] + v[4] - v[5] + v[6] - v[7]);
+          R3 w;
+          switch (l) {
+            case 0: w = p1 + p2 + p3 - p4; break;
+            case 1: w = p1 - p2 - p3 + p4; break;
+            case 2: w = -p1 - p2 + p3 - p4; break;
+            case 3: w = -p1 + p2 - p3 + p4; break;
+            case 4: w = -p1 - p2 + p3 + p4; break;
+            case 5: w = -p1 + p2 - p3 - p4; break;
+            case 6: w = p1 + p2 + p3 + p4; break;
+            default: w = p1 - p2 - p3 - p4; break;
+          }
+          h = h + 1. / nb * w;
+        }
+      }
+  double vx = ux[n] - h.x, vy = uy[n] - h.y, vz = uz[n] - h.z;
+  const double dt = F.s->dt, t = F.s->t;
+  const double eps = 1.e-8;
+  for (int b = 0; b < P.nb_bc; ++b) {
+    const mhc_bc& bc = P.bc[b];
+    if ((t - dt * (1 - eps)) < bc.tdebut) continue;
+    if ((t - dt * (1 - eps)) > bc.tfin) continue;
+    if (!node_on_surface(M, i, j, k, bc.surface)) continue;
+    if (bc.kind == MHC_BC_VX) vx = bc.value;
+    else if (bc.kind == MHC_BC_VY) vy = bc.value;
+    else if (bc.kind == MHC_BC_VZ) vz = bc.value;
+  }
+  F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
+  F.Xn[0][n] = F.Xp[0][n] + dt * vx; F.Xn[1][n] = F.Xp[1][n] + dt * vy; F.Xn[2][n] = F.Xp[2][n] + dt * vz;
 }
 
 // ---------------------------------------------------------------------------
@@ -450,7 +596,128 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
 // (PrepareRemap.cc:94-193).  Otherwise the EOS is applied here
 // (Lagrange-only time loop).
 // ---------------------------------------------------------------------------
-template <int DIM, int NE, bool EULER>
+// ---------------------------------------------------------------------------
+// updateElasticityAndPlasticity (MahycoModule.cc:1327-1353) with
+// DefaultModelService (src/elasto/DefaultModelService.cc:27-242) and the
+// constant EPP shear modulus / YEPP yield strength, for one environment:
+// velocity gradient from the mean corner normals, deformation rate and
+// spin, work with S_n, deviator update with rotation, radial return, work
+// with S_n+1.  Returns the two work increments in order.  Where the
+// reference relies on undefined or framework behaviour: the deviator
+// increment takes trace = tr(D) (an uninitialised `trace` there,
+// DefaultModelService.cc:82,96), doubleContraction sums row by row, each
+// row left to right, pow(x, 2.) is x*x, Real3x3 / Real divides each
+// component.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh& M, const Fields& F, long long c,
+                                            int i, int j, int k, const R3* cqs, double V, double Vn, double mass,
+                                            double dt, double& w1, double& w2) {
+  constexpr int NBN = DIM == 3 ? 8 : 4;
+  const long long N = M.ncell;
+  R3 coordn[8], cqn[8];
+  R3 vel[8];
+  for (int l = 0; l < NBN; ++l) {
+    int a, b, d;
+    local_node_offset(l, a, b, d);
+    const long long nn = node_id(M, i + a, j + b, k + d);
+    coordn[l] = {F.Xp[0][nn], F.Xp[1][nn], F.Xp[2][nn]};
+    vel[l] = {F.vx[nn], F.vy[nn], F.vz[nn]};
+  }
+  if (DIM == 3) {
+    R3 fc[6];
+    hex_face_centres(coordn, fc);
+    cqs3(coordn, fc, cqn);
+  } else {
+    cqs2(coordn, cqn);
+  }
+  double G[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+  for (int l = 0; l < NBN; ++l) {
+    const R3 cq = .5 * (cqn[l] + cqs[l]);
+    const double va[3] = {vel[l].x, vel[l].y, vel[l].z}, cb[3] = {cq.x, cq.y, cq.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) G[a][b] = G[a][b] + va[a] * cb[b];
+  }
+  const double volume = .5 * (Vn + V);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) G[a][b] = G[a][b] / volume;
+  double D[3][3];
+  D[0][0] = G[0][0]; D[1][1] = G[1][1]; D[2][2] = G[2][2];
+  D[0][1] = 0.5 * (G[0][1] + G[1][0]);
+  D[0][2] = 0.5 * (G[0][2] + G[2][0]);
+  D[1][2] = 0.5 * (G[1][2] + G[2][1]);
+  D[1][0] = D[0][1]; D[2][0] = D[0][2]; D[2][1] = D[1][2];
+  const double wx = 0.5 * (G[1][2] - G[2][1]), wy = 0.5 * (G[2][0] - G[0][2]), wz = 0.5 * (G[0][1] - G[1][0]);
+  double Sv[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) Sv[q] = F.S[q * N + c];
+  auto work = [&]() {
+    const double r0 = Sv[0] * D[0][0] + Sv[3] * D[0][1] + Sv[5] * D[0][2];
+    const double r1 = Sv[3] * D[1][0] + Sv[1] * D[1][1] + Sv[4] * D[1][2];
+    const double r2 = Sv[5] * D[2][0] + Sv[4] * D[2][1] + Sv[2] * D[2][2];
+    const double dc = r0 + r1 + r2;
+    return 0.25 * dt * (V + Vn) * dc / mass;
+  };
+  w1 = work();
+  const double sxx = Sv[0], syy = Sv[1], szz = Sv[2], sxy = Sv[3], syz = Sv[4], szx = Sv[5];
+  const double mu = o.shear_modulus, Y = o.yield_strength;
+  const double trace = D[0][0] + D[1][1] + D[2][2];
+  double Pt[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) Pt[a][b] = 2 * mu * (D[a][b] - (1. / 3.) * trace * (a == b ? 1.0 : 0.0)) * dt;
+  if (DIM == 2) {
+    if (o.rotation_order == 1) {
+      Pt[0][0] += 2 * dt * sxy * wz;
+      Pt[1][1] -= 2 * dt * sxy * wz;
+      Pt[0][1] -= dt * (sxx - syy) * wz;
+      Pt[1][0] = Pt[0][1];
+    } else {
+      const double syx = sxy;
+      const double a = -0.5 * dt * wz;
+      const double qxx = (1. - a * a) / (1. + a * a), qyy = qxx;
+      const double qxy = -2. * a / (1. + a * a), qyx = -qxy;
+      const double blxx = sxx * qxx + sxy * qxy, blxy = sxx * qyx + sxy * qyy;
+      const double blyx = syx * qxx + syy * qxy, blyy = syx * qyx + syy * qyy;
+      Pt[0][0] = qxx * blxx + qxy * blyx;
+      Pt[1][1] = qyx * blxy + qyy * blyy;
+      Pt[0][1] = qxx * blxy + qxy * blyy;
+      Pt[1][0] = Pt[0][1];
+    }
+  } else {
+    Pt[0][0] -= 2 * dt * (szx * wy - sxy * wz);
+    Pt[1][1] -= 2 * dt * (sxy * wz - syz * wx);
+    Pt[2][2] -= 2 * dt * (syz * wx - szx * wy);
+    Pt[0][1] -= dt * (sxx - syy) * wz - dt * syz * wy - dt * szx * wx;
+    Pt[1][2] -= dt * (syy - szz) * wx - dt * szx * wz - dt * sxy * wy;
+    Pt[2][0] -= dt * (szz - sxx) * wy - dt * sxy * wx - dt * syz * wz;
+  }
+  Sv[0] = sxx + Pt[0][0]; Sv[1] = syy + Pt[1][1]; Sv[2] = szz + Pt[2][2];
+  Sv[3] = sxy + Pt[0][1]; Sv[4] = syz + Pt[1][2]; Sv[5] = szx + Pt[2][0];
+  double j2 = Sv[0] * Sv[0];
+  j2 += Sv[1] * Sv[1];
+  j2 += Sv[0] * Sv[1];
+  j2 += Sv[3] * Sv[3];
+  if (DIM == 3) {
+    j2 += Sv[4] * Sv[4];
+    j2 += Sv[5] * Sv[5];
+  }
+  if (j2 > (Y * Y) / 3.) {
+    const double coeff = Y / sqrt(3. * j2);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) Sv[q] *= coeff;
+  }
+  w2 = work();
+#pragma unroll
+  for (int q = 0; q < 6; ++q) F.S[q * N + c] = Sv[q];
+}
+
+template <int DIM, int NE, bool EULER, bool EL = false>
 __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   long long c = bx * (long long)CT + threadIdx.x;
   if (c >= M.ncell) return;
@@ -515,6 +782,16 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   } else {
     for (int q = 0; q < NE; ++q) if ((mask >> q) & 1) qg += qe[q] * fe[q];
   }
+  // updateElasticityAndPlasticity: the work is added to the energy the
+  // explicit and Newton updates start from (the GP update restarts from e_n)
+  double ecur[NE];
+  for (int q = 0; q < NE; ++q) ecur[q] = ene[q];
+  if (EL) {
+    double w1, w2;
+    elasto_cell<DIM>(P.env[0], M, F, c, i, j, k, cqs, V, F.V[c], me[0], dt, w1, w2);
+    ecur[0] = ecur[0] + w1;
+    ecur[0] = ecur[0] + w2;
+  }
   // updateEnergyAndPressure
   double ee_[NE], pe[NE], ce[NE];
   for (int q = 0; q < NE; ++q) {
@@ -524,8 +801,26 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
     double qn = qne[q];
     double r = rhoe[q], rn = rhone[q];
     if (P.pression_explicite) {
-      ee_[q] = ene[q] - (pne[q] + qq) * (1.0 / r - 1.0 / rn);
+      ee_[q] = ecur[q] - (pne[q] + qq) * (1.0 / r - 1.0 / rn);
       eos_apply(P.env[q], r, ee_[q], pe[q], ce[q]);
+    } else if (P.with_newton) {
+      // updateEnergyAndPressurebyNewton, non-CSTS branch (MahycoModule.cc:1506-1571):
+      // at most 50 Newton steps from the energy at n; the pressure and sound
+      // speed of the last step are recomputed from the final energy (EOS of
+      // the Lagrange-only loop below, or after the remap) before any use
+      double pseudo = 0.;
+      if (P.pseudo_centree && ((qn + qq) * (1.0 / r - 1.0 / rn) < 0.)) pseudo = 0.5 * (qq + qn);
+      if (!P.pseudo_centree && (qq * (1.0 / r - 1.0 / rn) < 0.)) pseudo = qq;
+      const double en = ene[q], pn = pne[q];
+      double en1 = ecur[q], pp = pn, dpde = 0.;
+      int it = 0;
+      while (it < 50 && fabs(fvnr(en1, pp, en, pseudo, pn, r, rn)) >= P.threshold) {
+        eos_one_cell(P.env[q], r, en1, pp, dpde);
+        const double enew = en1 - fvnr(en1, pp, en, pseudo, pn, r, rn) / fvnrderiv(dpde, r, rn);
+        en1 = enew;
+        ++it;
+      }
+      ee_[q] = en1;
     } else {
       double pseudo = 0.;
       if (P.pseudo_centree && ((qn + qq) * (1.0 / r - 1.0 / rn) < 0.)) pseudo = 0.5 * (qq + qn);

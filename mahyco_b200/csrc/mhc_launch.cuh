@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
 #define MHC_LAG_MIN_BLOCKS 1
 #endif
 
-template <int DIM>
+template <int DIM, bool EL, bool HG>
 __global__ void __launch_bounds__(LAG_THREADS, MHC_LAG_MIN_BLOCKS) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_LAG_NODES>(C, L, w_);
@@ -123,12 +123,12 @@ __global__ void __launch_bounds__(LAG_THREADS, MHC_LAG_MIN_BLOCKS) kb_lagrange_n
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_lagrange_nodes<DIM>(M, *C[wi.c].P, F, wi.x, wi.y, wi.z);
+    body_lagrange_nodes<DIM, EL, HG>(M, *C[wi.c].P, F, wi.x, wi.y, wi.z);
     __syncthreads();
   }
 }
 
-template <int DIM, int NE, bool EULER>
+template <int DIM, int NE, bool EULER, bool EL>
 __global__ void __launch_bounds__(CT, MHC_LAG_MIN_BLOCKS) kb_lagrange_cells(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
@@ -136,12 +136,24 @@ __global__ void __launch_bounds__(CT, MHC_LAG_MIN_BLOCKS) kb_lagrange_cells(cons
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_lagrange_cells<DIM, NE, EULER>(M, *C[wi.c].P, F, wi.x);
+    body_lagrange_cells<DIM, NE, EULER, EL>(M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_hourglass(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_hourglass<DIM>(M, *C[wi.c].P, F, wi.x);
   }
 }
 
 // k-th performed sweep of the cycle in direction D: U[k&1] -> U[(k+1)&1]
-template <int DIM, int NE, int D>
+template <int DIM, int NE, int D, int LIM>
 __global__ void __launch_bounds__(SW_THREADS)
 kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
@@ -157,11 +169,11 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     A.order = P.ordre_projection;
     A.limiter = P.projection_limiteur_id;
     const Mesh M = C[wi.c].M;
-    body_sweep_cells_lanes<DIM, NE, D>(M, F, A, wi.x, wi.y);
+    body_sweep_cells_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
   }
 }
 
-template <int DIM, int NE, int D>
+template <int DIM, int NE, int D, int LIM>
 __global__ void __launch_bounds__(SW_THREADS)
 kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
@@ -190,7 +202,7 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     A.order = P.ordre_projection;
     A.limiter = P.projection_limiteur_id;
     A.done_dirs = done;
-    body_sweep_nodes_lanes<DIM, NE, D>(M, F, A, wi.x, wi.y);
+    body_sweep_nodes_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
   }
 }
 
@@ -233,7 +245,7 @@ __global__ void __launch_bounds__(CT) kb_delta_t(const CaseDesc* __restrict__ C,
 }
 
 // one thread per case
-__global__ void kb_delta_t_finalize(const CaseDesc* __restrict__ C, const int* __restrict__ cases, int n) {
+static __global__ void kb_delta_t_finalize(const CaseDesc* __restrict__ C, const int* __restrict__ cases, int n) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const CaseDesc& cd = C[cases[t]];
     if (!case_active(cd.F)) continue;
@@ -242,7 +254,7 @@ __global__ void kb_delta_t_finalize(const CaseDesc* __restrict__ C, const int* _
 }
 
 // copy of every case's scalars into one array (one read-back per poll)
-__global__ void kb_gather_scalars(const CaseDesc* __restrict__ C, int n, Scalars* __restrict__ out) {
+static __global__ void kb_gather_scalars(const CaseDesc* __restrict__ C, int n, Scalars* __restrict__ out) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) out[t] = *C[t].F.s;
 }
 

@@ -254,7 +254,7 @@ __device__ __forceinline__ void load_plane_xd(const Mesh& M, const Fields& F, in
 // the lowest transverse axis fastest, so the warps of a block read
 // neighbouring columns and share L1 sectors.
 // ---------------------------------------------------------------------------
-template <int DIM, int NE, int D>
+template <int DIM, int NE, int D, int LIM>
 __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fields& F, const SweepArgs& A,
                                                        int vbx, int vby) {
   constexpr int NV = 3 * NE + 1;
@@ -268,7 +268,7 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
   const bool ok = sweep_lane<D>(M.ncx, M.ncy, M.ncz, XOUT, vbx, vby, lane, row, i, j, k, p, ta, tb);
   const bool out = ok && lane >= 2 && lane < 2 + XOUT;
   const double dt = F.s->dt;
-  const int order2 = A.order - 1;
+  const int order2 = LIM == LIM_ORDER1 ? 0 : 1;  // ordre-projection - 1
   const double* __restrict__ Uin = A.Uin;
   // back node plane of the own cell; the front plane is the back plane of
   // the next lane, except at the end of a line
@@ -328,7 +328,7 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
     const double phi_l = __shfl_up_sync(FULL, phi, 1);
     const double gf = face_b ? (phi - phi_l) / dxb : 0.;
     const double gf_r = __shfl_down_sync(FULL, gf, 1);
-    const double gr = (A.order > 1 && ok) ? limited_gradient(A.limiter, gf, gf_r) : 0.;
+    const double gr = (LIM != LIM_ORDER1 && ok) ? limited_gradient_t<LIM>(gf, gf_r) : 0.;
     const double gr_l = __shfl_up_sync(FULL, gr, 1);
     double pf = 0.;
     if (face_b) pf = up_left ? phi_l + order2 * (fc - xc_l) * gr_l : phi + order2 * (fc - xc) * gr;
@@ -376,7 +376,7 @@ __device__ __forceinline__ bool node_inner_dir(const Mesh& M, int i, int j, int 
   return id > 0 && id < nn - 1;
 }
 
-template <int DIM, int NE, int D>
+template <int DIM, int NE, int D, int LIM>
 __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fields& F, const DualArgs& A,
                                                        int vbx, int vby) {
   constexpr unsigned FULL = 0xffffffffu;
@@ -456,10 +456,10 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     g[q] = 0.;
-    if (A.order > 1 && inner) {
+    if (LIM != LIM_ORDER1 && inner) {
       const double gfw = (ph_r[q] - ph[q]) / (x_r - x);
       const double gbw = (ph[q] - ph_l[q]) / (x - x_l);
-      g[q] = limited_gradient(A.limiter, gbw, gfw);
+      g[q] = limited_gradient_t<LIM>(gbw, gfw);
     }
     g_l[q] = __shfl_up_sync(FULL, g[q], 1);
     g_r[q] = __shfl_down_sync(FULL, g[q], 1);
@@ -471,7 +471,7 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
     return;
   }
   const double dt = F.s->dt;
-  const int order2 = A.order - 1;
+  const int order2 = LIM == LIM_ORDER1 ? 0 : 1;  // ordre-projection - 1
   U[3] += bfm - ffm;
   double FV[3], BV[3], FE, BE;
   {

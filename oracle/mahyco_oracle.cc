@@ -51,6 +51,8 @@ static inline R3 operator*(double s, R3 a) { return {s * a.x, s * a.y, s * a.z};
 static inline R3 operator*(R3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
 static inline R3 operator/(R3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
 static inline R3& operator+=(R3& a, R3 b) { a = a + b; return a; }
+static inline R3& operator-=(R3& a, R3 b) { a = a - b; return a; }
+static inline R3 operator-(R3 a) { return {-a.x, -a.y, -a.z}; }
 static inline double dot(R3 a, R3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 /* math::vecMul */
 static inline R3 vecmul(R3 u, R3 v) {
@@ -132,6 +134,11 @@ struct Case {
   std::vector<R3> cell_coord;
   std::vector<double> char_len, div_u, euler_volume, materiau;
   std::vector<R3> cqs, cqs_n;         /* ncell * nbn */
+  /* elasto-plasticity (single environment): stress deviator at n+1 and n,
+   * symmetric, components xx yy zz xy yz zx per cell */
+  bool elasto = false;
+  std::vector<double> sdev, sdev_n;
+  std::vector<R3> hourglass;          /* anti-hourglass velocity correction */
   std::vector<R3> outer_normal;       /* ncell * 2*dim */
   /* faces, per direction */
   long nface[3] = {0, 0, 0};
@@ -380,6 +387,33 @@ static void eos_apply(Case& C, int env) {
   }
 }
 
+/* applyOneCellEOS (PerfectGas 71-88, StiffenedGas 67-83, MieGruneisen
+ * 101-146): pressure and dp/de of one environment cell; the sound speed and
+ * temperature it also writes are not read by the Newton loop */
+static void eos_one_cell(const mhc_env_params& o, double rho, double e, double& p, double& dpde) {
+  if (o.eos == MHC_EOS_PERFECT_GAS) {
+    double g = o.adiabatic_cst;
+    p = (g - 1.) * rho * e;
+    dpde = (g - 1.) * rho;
+  } else if (o.eos == MHC_EOS_STIFFENED_GAS) {
+    double g = o.adiabatic_cst, pinf = o.limit_tension;
+    p = ((g - 1.) * rho * e) - (g * pinf);
+    dpde = (g - 1.) * rho;
+  } else {
+    double J = o.rho0 / rho;
+    double mu = 1. / J - 1.;
+    p = mg_pressure(o, rho, e);
+    dpde = (o.gamma0 + o.a * mu);
+  }
+}
+
+/* fvnr / fvnrderiv (MahycoModule.h:378-386): residual of the energy
+ * equation and its derivative */
+static inline double fvnr(double e, double p, double en, double qnn1, double pn, double rn1, double rn) {
+  return e - en + 0.5 * (p + pn + 2. * qnn1) * (1. / rn1 - 1. / rn);
+}
+static inline double fvnrderiv(double dpde, double rn1, double rn) { return 1. + 0.5 * dpde * (1. / rn1 - 1. / rn); }
+
 /* ---------------------------------------------------------------------------
  * init entry points
  * ------------------------------------------------------------------------- */
@@ -605,6 +639,10 @@ static void setup(Case& C, const mhc_case_params* p) {
   C.materiau.assign(C.ncell, 0.);
   C.cqs.assign(C.ncell * C.nbn, {0, 0, 0});
   C.cqs_n = C.cqs;
+  C.elasto = p->env[0].elasto_model != 0;
+  C.sdev.assign(C.elasto ? C.ncell * 6 : 0, 0.);
+  C.sdev_n = C.sdev;
+  C.hourglass.assign(C.nnode, {0, 0, 0});
   C.outer_normal.assign(C.ncell * 2 * C.dim, {0, 0, 0});
   for (int d = 0; d < C.dim; ++d) {
     long ex = C.ncx + (d == 0), ey = C.ncy + (d == 1), ez = C.ncz + (d == 2);
@@ -707,21 +745,72 @@ static void save_values_at_n(Case& C) {
   cp(C.internal_energy_n, C.internal_energy);
   C.cqs_n = C.cqs;
   C.vel_n = C.vel;
+  C.sdev_n = C.sdev;
 }
 
-/* MahycoModule::updateVelocity (MahycoModule.cc:438-562); no stress
- * deviator without an elasto model, so the elasto-plastic force term adds
- * exact zeros and is omitted. */
+/* MahycoModule::updateVelocity (MahycoModule.cc:438-562): pressure forces
+ * summed over all cells, then the elasto-plastic forces -S_n.C_n (only
+ * with an elasto model: without one they add exact zeros), gravity, and
+ * the anti-hourglass correction of a Lagrangian run */
 static void update_velocity(Case& C) {
   for (auto& f : C.force) f = {0., 0., 0.};
   for (long c = 0; c < C.ncell; ++c) {
     double pressure = C.pressure_n.g[c] + C.pseudo_n.g[c];
     for (int l = 0; l < C.nbn; ++l) C.force[C.cnode(c, l)] += pressure * C.cqs_n[c * C.nbn + l];
   }
+  if (C.elasto) {
+    for (long c = 0; c < C.ncell; ++c) {
+      const double* S = &C.sdev_n[c * 6];
+      /* force_tensor = -S_n; prodTensVec(t, v) = (t.x.v, t.y.v, t.z.v) */
+      const R3 tx = {-S[0], -S[3], -S[5]}, ty = {-S[3], -S[1], -S[4]}, tz = {-S[5], -S[4], -S[2]};
+      for (int l = 0; l < C.nbn; ++l) {
+        const R3 v = C.cqs_n[c * C.nbn + l];
+        C.force[C.cnode(c, l)] += R3{dot(tx, v), dot(ty, v), dot(tz, v)};
+      }
+    }
+  }
   const double dt = 0.5 * (C.old_dt + C.dt);
   for (long n = 0; n < C.nnode; ++n) C.vel[n] += (dt / C.node_mass[n]) * C.force[n];
   R3 g = {C.P.gravity[0], C.P.gravity[1], C.P.gravity[2]};
   for (long n = 0; n < C.nnode; ++n) C.vel[n] += dt * g;
+  if (!C.P.with_projection && C.P.coef_antiderive != 0.) {
+    /* MahycoModule.cc:497-555 */
+    const double coeff = C.P.coef_antiderive;
+    for (auto& h : C.hourglass) h = {0., 0., 0.};
+    auto nbcell = [&](long n) {
+      int i, j, k;
+      C.nijk(n, i, j, k);
+      int m = ((i > 0 && i < C.nnx - 1) ? 2 : 1) * ((j > 0 && j < C.nny - 1) ? 2 : 1);
+      if (C.dim == 3) m *= (k > 0 && k < C.nnz - 1) ? 2 : 1;
+      return (double)m;
+    };
+    for (long c = 0; c < C.ncell; ++c) {
+      long nd[8];
+      R3 v[8];
+      for (int l = 0; l < C.nbn; ++l) { nd[l] = C.cnode(c, l); v[l] = C.vel[nd[l]]; }
+      if (C.dim == 2) {
+        R3 psi = coeff * (v[0] + v[2] - v[1] - v[3]);
+        C.hourglass[nd[0]] += 1. / nbcell(nd[0]) * psi;
+        C.hourglass[nd[1]] -= 1. / nbcell(nd[1]) * psi;
+        C.hourglass[nd[2]] += 1. / nbcell(nd[2]) * psi;
+        C.hourglass[nd[3]] -= 1. / nbcell(nd[3]) * psi;
+      } else {
+        R3 p1 = coeff * (v[0] + v[1] - v[2] - v[3] - v[4] - v[5] + v[6] + v[7]);
+        R3 p2 = coeff * (v[0] - v[1] - v[2] + v[3] - v[4] + v[5] + v[6] - v[7]);
+        R3 p3 = coeff * (v[0] - v[1] + v[2] - v[3] + v[4] - v[5] + v[6] - v[7]);
+        R3 p4 = coeff * (-v[0] + v[1] - v[2] + v[3] + v[4] - v[5] + v[6] - v[7]);
+        C.hourglass[nd[0]] += 1. / nbcell(nd[0]) * (p1 + p2 + p3 - p4);
+        C.hourglass[nd[1]] += 1. / nbcell(nd[1]) * (p1 - p2 - p3 + p4);
+        C.hourglass[nd[2]] += 1. / nbcell(nd[2]) * (-p1 - p2 + p3 - p4);
+        C.hourglass[nd[3]] += 1. / nbcell(nd[3]) * (-p1 + p2 - p3 + p4);
+        C.hourglass[nd[4]] += 1. / nbcell(nd[4]) * (-p1 - p2 + p3 + p4);
+        C.hourglass[nd[5]] += 1. / nbcell(nd[5]) * (-p1 + p2 - p3 - p4);
+        C.hourglass[nd[6]] += 1. / nbcell(nd[6]) * (p1 + p2 + p3 + p4);
+        C.hourglass[nd[7]] += 1. / nbcell(nd[7]) * (p1 - p2 - p3 - p4);
+      }
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] -= C.hourglass[n];
+  }
 }
 
 static bool node_on_surface(const Case& C, long n, int surf) {
@@ -805,6 +894,108 @@ static void compute_artificial_viscosity(Case& C) {
   }
 }
 
+/* MahycoModule::updateElasticityAndPlasticity (MahycoModule.cc:1327-1353)
+ * with DefaultModelService (src/elasto/DefaultModelService.cc:27-242) and
+ * the constant EPP shear modulus / YEPP yield strength, one environment:
+ * velocity gradient from the mean corner normals, deformation rate and
+ * spin, elasto-plastic work with S_n, deviator update with rotation, radial
+ * return, work with S_n+1.  Restated where the reference is undefined or
+ * relies on Arcane: the deviator increment takes trace = tr(D) (the
+ * reference reads an uninitialised `trace`, DefaultModelService.cc:82,96);
+ * doubleContraction sums row by row, each row left to right; pow(x, 2.) is
+ * x*x; Real3x3 / Real divides every component. */
+static void update_elasticity_and_plasticity(Case& C) {
+  if (!C.elasto) return;
+  const double dt = C.dt;
+  const mhc_env_params& o = C.P.env[0];
+  const double mu = o.shear_modulus, Y = o.yield_strength;
+  for (long c = 0; c < C.ncell; ++c) {
+    double G[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+    for (int l = 0; l < C.nbn; ++l) {
+      const R3 vi = C.vel[C.cnode(c, l)];
+      const R3 cq = .5 * (C.cqs_n[c * C.nbn + l] + C.cqs[c * C.nbn + l]);
+      const double va[3] = {vi.x, vi.y, vi.z}, cb[3] = {cq.x, cq.y, cq.z};
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) G[a][b] += va[a] * cb[b];
+    }
+    const double volume = .5 * (C.cell_volume_n.g[c] + C.cell_volume.g[c]);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) G[a][b] = G[a][b] / volume;
+    double D[3][3];
+    D[0][0] = G[0][0]; D[1][1] = G[1][1]; D[2][2] = G[2][2];
+    D[0][1] = 0.5 * (G[0][1] + G[1][0]);
+    D[0][2] = 0.5 * (G[0][2] + G[2][0]);
+    D[1][2] = 0.5 * (G[1][2] + G[2][1]);
+    D[1][0] = D[0][1]; D[2][0] = D[0][2]; D[2][1] = D[1][2];
+    const double wx = 0.5 * (G[1][2] - G[2][1]), wy = 0.5 * (G[2][0] - G[0][2]), wz = 0.5 * (G[0][1] - G[1][0]);
+    double* S = &C.sdev[c * 6];  /* xx yy zz xy yz zx */
+    auto full = [&](double M[3][3]) {
+      M[0][0] = S[0]; M[1][1] = S[1]; M[2][2] = S[2];
+      M[0][1] = M[1][0] = S[3]; M[1][2] = M[2][1] = S[4]; M[2][0] = M[0][2] = S[5];
+    };
+    auto work = [&]() {
+      double M[3][3];
+      full(M);
+      double r0 = M[0][0] * D[0][0] + M[0][1] * D[0][1] + M[0][2] * D[0][2];
+      double r1 = M[1][0] * D[1][0] + M[1][1] * D[1][1] + M[1][2] * D[1][2];
+      double r2 = M[2][0] * D[2][0] + M[2][1] * D[2][1] + M[2][2] * D[2][2];
+      double dc = r0 + r1 + r2;
+      C.EV(C.internal_energy, 0, c) += 0.25 * dt * (C.cell_volume.g[c] + C.cell_volume_n.g[c]) * dc /
+                                       C.EV(C.cell_mass, 0, c);
+    };
+    work();
+    /* ComputeElasticity (78-169) */
+    const double sxx = S[0], syy = S[1], szz = S[2], sxy = S[3], syz = S[4], szx = S[5];
+    const double trace = D[0][0] + D[1][1] + D[2][2];
+    double P[3][3];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) P[a][b] = 2 * mu * (D[a][b] - (1. / 3.) * trace * (a == b ? 1.0 : 0.0)) * dt;
+    if (C.dim == 2) {
+      if (o.rotation_order == 1) {
+        P[0][0] += 2 * dt * sxy * wz;
+        P[1][1] -= 2 * dt * sxy * wz;
+        P[0][1] -= dt * (sxx - syy) * wz;
+        P[1][0] = P[0][1];
+      } else {
+        const double syx = sxy;
+        double a = -0.5 * dt * wz;
+        double qxx = (1. - a * a) / (1. + a * a), qyy = qxx;
+        double qxy = -2. * a / (1. + a * a), qyx = -qxy;
+        double blxx = sxx * qxx + sxy * qxy, blxy = sxx * qyx + sxy * qyy;
+        double blyx = syx * qxx + syy * qxy, blyy = syx * qyx + syy * qyy;
+        P[0][0] = qxx * blxx + qxy * blyx;
+        P[1][1] = qyx * blxy + qyy * blyy;
+        P[0][1] = qxx * blxy + qxy * blyy;
+        P[1][0] = P[0][1];
+      }
+    } else {
+      P[0][0] -= 2 * dt * (szx * wy - sxy * wz);
+      P[1][1] -= 2 * dt * (sxy * wz - syz * wx);
+      P[2][2] -= 2 * dt * (syz * wx - szx * wy);
+      P[0][1] -= dt * (sxx - syy) * wz - dt * syz * wy - dt * szx * wx;
+      P[1][2] -= dt * (syy - szz) * wx - dt * szx * wz - dt * sxy * wy;
+      P[2][0] -= dt * (szz - sxx) * wy - dt * sxy * wx - dt * syz * wz;
+      P[1][0] = P[0][1]; P[2][1] = P[1][2]; P[0][2] = P[2][0];
+    }
+    S[0] = sxx + P[0][0]; S[1] = syy + P[1][1]; S[2] = szz + P[2][2];
+    S[3] = sxy + P[0][1]; S[4] = syz + P[1][2]; S[5] = szx + P[2][0];
+    /* ComputePlasticity (173-226): radial return onto the yield surface */
+    double j2 = S[0] * S[0];
+    j2 += S[1] * S[1];
+    j2 += S[0] * S[1];
+    j2 += S[3] * S[3];
+    if (C.dim == 3) {
+      j2 += S[4] * S[4];
+      j2 += S[5] * S[5];
+    }
+    if (j2 > (Y * Y) / 3.) {
+      const double coeff = Y / std::sqrt(3. * j2);
+      for (int q = 0; q < 6; ++q) S[q] *= coeff;
+    }
+    work();
+  }
+}
+
 /* MahycoModule::computePressionMoyenne (MahycoModule.cc:1708-1735) */
 static void compute_pression_moyenne(Case& C) {
   double option = C.P.calcul_vitson_max ? 1. : 0.;
@@ -822,7 +1013,8 @@ static void compute_pression_moyenne(Case& C) {
 }
 
 /* MahycoModule::updateEnergyAndPressure (MahycoModule.cc:1430-1480) with
- * updateEnergyAndPressureforGP (1623-1698, non-CSTS branch) or
+ * updateEnergyAndPressureforGP (1623-1698, non-CSTS branch),
+ * updateEnergyAndPressurebyNewton (1506-1571) or
  * updateEnergyAndPressureExplicite (1484-1502) */
 static void update_energy_and_pressure(Case& C) {
   if (C.P.pression_explicite) {
@@ -833,6 +1025,35 @@ static void update_energy_and_pressure(Case& C) {
                                           (1.0 / C.EV(C.density, e, c) - 1.0 / C.EV(C.density_n, e, c));
       }
       eos_apply(C, e);
+    }
+  } else if (C.P.with_newton) {
+    /* updateEnergyAndPressurebyNewton, non-CSTS branch (MahycoModule.cc:1506-1571):
+     * at most 50 Newton steps on fvnr, starting from the energy at n; the
+     * pressure and sound speed left by the last applyOneCellEOS are
+     * recomputed from the final energy (final applyEOS of a Lagrange-only
+     * loop, or the EOS after the remap) before anything reads them */
+    bool pc = C.P.pseudo_centree;
+    for (int e = 0; e < C.nenv; ++e) {
+      const mhc_env_params& o = C.P.env[e];
+      for (long c = 0; c < C.ncell; ++c) {
+        if (!C.has(c, e)) continue;
+        double q = C.EV(C.pseudo, e, c), qn = C.EV(C.pseudo_n, e, c);
+        double rn1 = C.EV(C.density, e, c), rn = C.EV(C.density_n, e, c);
+        double pseudo = 0.;
+        if (pc && ((qn + q) * (1.0 / rn1 - 1.0 / rn) < 0.)) pseudo = 0.5 * (q + qn);
+        if (!pc && (q * (1.0 / rn1 - 1.0 / rn) < 0.)) pseudo = q;
+        const double pn = C.EV(C.pressure_n, e, c), en = C.EV(C.internal_energy_n, e, c);
+        const double eps = C.P.threshold;
+        double en1 = C.EV(C.internal_energy, e, c), p = pn, dpde = 0.;
+        int i = 0;
+        while (i < 50 && std::fabs(fvnr(en1, p, en, pseudo, pn, rn1, rn)) >= eps) {
+          eos_one_cell(o, rn1, en1, p, dpde);
+          double enew = en1 - fvnr(en1, p, en, pseudo, pn, rn1, rn) / fvnrderiv(dpde, rn1, rn);
+          en1 = enew;
+          i++;
+        }
+        C.EV(C.internal_energy, e, c) = en1;
+      }
     }
   } else {
     bool pc = C.P.pseudo_centree;
@@ -1369,6 +1590,7 @@ static int iterate(Case& C) {
   if (compute_geometric_values(C) != ST_OK) return C.status;
   update_density(C);
   compute_artificial_viscosity(C);
+  update_elasticity_and_plasticity(C);
   update_energy_and_pressure(C);
   if (remap(C) != ST_OK) return C.status;
   if (compute_delta_t(C) != ST_OK) return C.status;

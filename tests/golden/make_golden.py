@@ -22,6 +22,7 @@ from mahyco_b200.case import read_arc, params_to_dict  # noqa: E402
 # case -> extra oracle switches needed to reproduce how the reference ran it
 CASES = {
     "CAS_2D_Lag_SodCaseX": {},
+    "CAS_2D_Lag_SodCaseX_newton": {},
     "CAS_2D_Lag_BiSodCaseX": {},
     "CAS_Lag_BiSodCaseX": {},
     "CAS_BiSodCaseX": {},

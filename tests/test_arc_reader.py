@@ -35,7 +35,7 @@ def test_lagrange_loop_disables_remap(tmp_path):
 
 
 @pytest.mark.parametrize("snippet", ["<schema-csts>1</schema-csts>",
-                                     "<coef-antiderive>0.1</coef-antiderive>"])
+                                     "<sans-lagrange>true</sans-lagrange>"])
 def test_unsupported_options_raise(tmp_path, snippet):
     text = open(ARC).read().replace("<pseudo-centree>0</pseudo-centree>", "<pseudo-centree>0</pseudo-centree>" + snippet)
     f = tmp_path / "u.arc"
@@ -48,3 +48,28 @@ def test_params_roundtrip():
     p, _ = read_arc(ARC)
     q = params_from_dict(params_to_dict(p))
     assert bytes(p) == bytes(q)
+
+
+def test_anti_hourglass_and_elasto_options(tmp_path):
+    """coef-antiderive and the DefaultModel/EPP/YEPP elasto block are read
+    (CAS_2D_Lag_Taylor_elasto style); other elasto models are refused."""
+    text = open(ARC).read().replace("<pseudo-centree>0</pseudo-centree>",
+                                    "<pseudo-centree>0</pseudo-centree><coef-antiderive>0.01</coef-antiderive>")
+    f = tmp_path / "h.arc"
+    f.write_text(text)
+    p, _ = read_arc(str(f))
+    assert p.coef_antiderive == 0.01
+    el = ('<elasto-model name="DefaultModel"><ordre-rotation>2</ordre-rotation>'
+          '<elasto-mu-model name="EPP"><elastic-cst>2.6e10</elastic-cst></elasto-mu-model>'
+          '<elasto-y-model name="YEPP"><limit-elastic>3.e8</limit-elastic></elasto-y-model></elasto-model>')
+    src = open(ARC).read()
+    i = src.index("</environment>")
+    f2 = tmp_path / "e.arc"
+    f2.write_text(src[:i] + el + src[i:])
+    p2, _ = read_arc(str(f2))
+    assert (p2.env[0].elasto_model, p2.env[0].rotation_order) == (1, 2)
+    assert (p2.env[0].shear_modulus, p2.env[0].yield_strength) == (2.6e10, 3.e8)
+    f3 = tmp_path / "n.arc"
+    f3.write_text(src[:i] + el.replace("DefaultModel", "NewHypoModel") + src[i:])
+    with pytest.raises(NotImplementedError):
+        read_arc(str(f3))

@@ -46,10 +46,20 @@ def test_version_and_budget_query():
 
 
 def test_rejects_options_outside_the_hot_path():
+    """Options outside the implemented path are refused before any device
+    work (MHC_ERR_UNSUPPORTED), so this runs without a GPU."""
     lib = mb.load()
-    p = mb.default_params()
-    p.with_newton = 1
     h = ctypes.c_void_p()
+    p = mb.default_params()
+    p.ordre_projection = 3                      # order-3 remap
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p = mb.default_params()
+    p.projection_limiteur_id = 5                # generalised limiters
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p = mb.default_params()
+    p.env[0].elasto_model = 1                   # elasto with the Euler remap
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.with_projection, p.nb_env = 0, 2          # elasto with two environments
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
 
 
