@@ -153,8 +153,18 @@ __global__ void __launch_bounds__(CT) kb_hourglass(const CaseDesc* __restrict__ 
 }
 
 // k-th performed sweep of the cycle in direction D: U[k&1] -> U[(k+1)&1]
+// resident blocks per SM asked of the compiler for the sweeps (caps their
+// registers at 65536 / (SW_THREADS * value)); measured best on B200: 6 for
+// the cell sweeps (80 registers), 8 for the node sweeps (64 registers)
+#ifndef MHC_SW_MIN_BLOCKS_CELLS
+#define MHC_SW_MIN_BLOCKS_CELLS 6
+#endif
+#ifndef MHC_SW_MIN_BLOCKS_NODES
+#define MHC_SW_MIN_BLOCKS_NODES 8
+#endif
+
 template <int DIM, int NE, int D, int LIM>
-__global__ void __launch_bounds__(SW_THREADS)
+__global__ void __launch_bounds__(SW_THREADS, MHC_SW_MIN_BLOCKS_CELLS)
 kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_SWC0 + D>(C, L, w_);
@@ -174,7 +184,7 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
 }
 
 template <int DIM, int NE, int D, int LIM>
-__global__ void __launch_bounds__(SW_THREADS)
+__global__ void __launch_bounds__(SW_THREADS, MHC_SW_MIN_BLOCKS_NODES)
 kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_SWN0 + D>(C, L, w_);
