@@ -32,10 +32,6 @@ int mhc::set_err(int code, const std::string& msg) {
 
 namespace {
 
-size_t lagrange_smem(int dim, bool elasto = false) {
-  return (size_t)(LTX + 1) * (LTY + 1) * ((dim == 3 ? 8 : 4) * 3 * sizeof(double) * (elasto ? 2 : 1) + 1);
-}
-
 bool case_elasto(const mhc_case* h) { return h->P.env[0].elasto_model != 0; }
 bool case_hourglass(const mhc_case* h) { return !h->P.with_projection && h->P.coef_antiderive != 0.; }
 
@@ -108,7 +104,7 @@ int engine_rebuild(Engine* e) {
     };
     bool ok = phase(g.init_cells, PH_CELLS) && phase(g.init_nodes, PH_NODES) && phase(g.lag_cells, PH_CELLS) &&
               phase(g.fin_cells, PH_CELLS) && phase(g.fin_nodes, PH_NODES) && phase(g.dt, PH_CELLS) &&
-              phase(g.lag_nodes, PH_LAG_NODES);
+              phase(g.lag_nodes, PH_NODES);
     for (int D = 0; D < g.DIM; ++D) ok = ok && phase(g.sw_cells[D], PH_SWC0 + D) && phase(g.sw_nodes[D], PH_SWN0 + D);
     if (!ok) return set_err(MHC_ERR_ARG, "more than 2^31 blocks in one phase of a batch");
   }
@@ -140,14 +136,8 @@ void launch_init(Engine* e) {
 
 template <int DIM, bool EL, bool HG>
 void lag_nodes_launch(Engine* e, Group& g) {
-  static bool attr = false;
-  const size_t smem = lagrange_smem(DIM, EL);
-  if (!attr) {
-    cudaFuncSetAttribute(kb_lagrange_nodes<DIM, EL, HG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
-  plaunch(e, kb_lagrange_nodes<DIM, EL, HG>, LAG_THREADS, smem, g.lag_nodes);
-  if (HG) plaunch(e, kb_hourglass<DIM>, CT, 0, g.fin_nodes);
+  plaunch(e, kb_lagrange_nodes<DIM, EL, HG>, CT, 0, g.lag_nodes);
+  if (HG) plaunch(e, kb_hourglass<DIM>, CT, 0, g.lag_nodes);
 }
 
 template <int DIM>
@@ -354,7 +344,7 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   ncell = (long long)p->nx * p->ny * (dim == 3 ? p->nz : 1);
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
   int ne = p->nb_env, nv = 3 * ne + 1;
-  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0);
+  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8);
   long long nodes = 4 + 6 + 10;
   return cells * ncell + nodes * nnode;
 }
@@ -461,6 +451,7 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   }
   F.mflux = (double*)alloc(h->NE * N * sizeof(double));
   if (h->P.env[0].elasto_model) F.S = (double*)alloc(6 * N * sizeof(double));
+  F.cqs = (double*)alloc((h->DIM == 3 ? 24 : 8) * N * sizeof(double));
   h->d_scal = (Scalars*)alloc(sizeof(Scalars));
   h->d_params = (mhc_case_params*)alloc(sizeof(mhc_case_params));
   F.s = h->d_scal;

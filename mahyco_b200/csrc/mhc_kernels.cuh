@@ -50,6 +50,7 @@ struct Fields {
   double* mflux;
   double* Ud[2];
   double* S;               // elasto: stress deviator [6][ncell] (xx yy zz xy yz zx)
+  double* cqs;             // corner normals of the last Lagrangian mesh [NBN][3][ncell]
   Scalars* s;
 };
 
@@ -182,6 +183,35 @@ __device__ __forceinline__ double cell_volume(const R3* coord, R3* cqs) {
   return volume / DIM;
 }
 
+// corner normals kept for the next node pass (CQS at n of the next cycle:
+// the reference does not recompute them after the remap).  Layout
+// [corner][component][cell]; in 2D the z components are always +0 (the 2D
+// corner normals have none) and only x, y are kept.
+template <int DIM>
+__device__ __forceinline__ void store_cqs(const Fields& F, long long N, long long c, const R3* cqs) {
+  constexpr int NC = DIM == 3 ? 3 : 2;
+#pragma unroll
+  for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+    F.cqs[(NC * l) * N + c] = cqs[l].x;
+    F.cqs[(NC * l + 1) * N + c] = cqs[l].y;
+    if (DIM == 3) F.cqs[(NC * l + 2) * N + c] = cqs[l].z;
+  }
+}
+
+// read-only path: only for kernels that do not also write the corner normals
+template <int DIM>
+__device__ __forceinline__ R3 load_cqs(const Fields& F, long long N, long long c, int l) {
+  constexpr int NC = DIM == 3 ? 3 : 2;
+  return {__ldg(F.cqs + (NC * l) * N + c), __ldg(F.cqs + (NC * l + 1) * N + c),
+          DIM == 3 ? __ldg(F.cqs + (NC * l + 2) * N + c) : 0.0};
+}
+// coherent load, ordered before the same thread's store_cqs
+template <int DIM>
+__device__ __forceinline__ R3 load_cqs_rw(const Fields& F, long long N, long long c, int l) {
+  constexpr int NC = DIM == 3 ? 3 : 2;
+  return {F.cqs[(NC * l) * N + c], F.cqs[(NC * l + 1) * N + c], DIM == 3 ? F.cqs[(NC * l + 2) * N + c] : 0.0};
+}
+
 __device__ __forceinline__ bool node_on_surface(const Mesh& M, int i, int j, int k, int surf) {
   switch (surf) {
     case MHC_XMIN: return i == 0;
@@ -246,6 +276,7 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   R3 cqs[8];
   double V = cell_volume<DIM>(coord, cqs);
   if (V < 0.) atomicOr(&F.s->status, ST_NEG_VOLUME);
+  store_cqs<DIM>(F, N, c, cqs);
   double l = char_length(P, DIM, V, coord);
   // state: globals g*, env slots *e[]
   double rho = 0., p = 0., e = 0., cs = 0.;
@@ -361,156 +392,76 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
 // Lagrange, node pass: updateVelocity + applyBoundaryCondition + updatePosition
 // (MahycoModule.cc:438-501, 756-807, 730-741).
 //
-// The force on a node is the sum over its <= 8 cells, in ascending cell id,
-// of (p_n + q_n) * CQS_n where CQS_n are the corner normals of the previous
-// Lagrangian mesh.  Blocks own a TX x TY tile of node columns and march along
-// z: each step computes the corner forces of one cell layer into shared
-// memory once, finishes the node plane below it and starts the one above,
-// so every corner normal is computed once per (tile, layer) and no atomics
-// are used.
-// ---------------------------------------------------------------------------
-constexpr int LTX = 15, LTY = 15;                    // node columns of a tile
-constexpr int LAG_THREADS = (LTX + 1) * (LTY + 1);   // one thread per cell of a layer
-constexpr int LZCHUNK = 16;
-
-// EL: elasto-plastic forces -S_n.C_n added after the pressure forces
-// (MahycoModule.cc:467-474).  HG: the anti-hourglass correction follows
+// One thread per node gathers (p_n + q_n) * CQS_n over its <= 8 cells in
+// ascending cell id, then (EL) the elasto-plastic forces -S_n.CQS_n in the
+// same order: the reference's cell loops add into the node forces in that
+// order, and no atomics are used.  CQS_n are the corner normals the
+// previous cell pass stored.  HG: the anti-hourglass correction follows
 // (kb_hourglass), so this pass only writes the uncorrected velocity into
 // the dual-remap scratch Ud[0] (unused by a Lagrangian run).
+// ---------------------------------------------------------------------------
 template <int DIM, bool EL, bool HG>
-__device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F,
-                                                    int bx, int by, int bz) {
-  const int euler = P.with_projection ? 1 : 0;
-  constexpr int CW = LTX + 1, CH = LTY + 1, NCL = CW * CH;
-  constexpr int NBN = DIM == 3 ? 8 : 4;
-  extern __shared__ double smem_dyn[];
-  double* corner = smem_dyn;                      // [NCL][NBN][3] pressure corner forces of one layer
-  double* ecorner = smem_dyn + NCL * NBN * 3;     // [NCL][NBN][3] elasto corner forces (EL)
-  unsigned char* cvalid = reinterpret_cast<unsigned char*>(smem_dyn + NCL * NBN * 3 * (EL ? 2 : 1));
-  const int tx = threadIdx.x % LTX, ty = threadIdx.x / LTX;
-  const int i0 = bx * LTX, j0 = by * LTY;
-  const int ni = i0 + tx, nj = j0 + ty;
-  const bool node_ok = threadIdx.x < LTX * LTY && ni < M.nnx && nj < M.nny;
+__device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long n = bx * (long long)CT + threadIdx.x;
+  if (n >= M.nnode) return;
+  const long long N = M.ncell, NN = M.nnode;
+  int i, j, k;
+  node_ijk(M, n, i, j, k);
+  // the <= 8 cells around the node in ascending id: slot s = (dk, dj, di)
+  // bits, the node's local index in the cell is the complement
+  constexpr int NS = DIM == 3 ? 8 : 4;
+  R3 S = {0., 0., 0.};
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int di = (s & 1) - 1, dj = ((s >> 1) & 1) - 1, dk = DIM == 3 ? ((s >> 2) & 1) - 1 : 0;
+    const int ci = i + di, cj = j + dj, ck = k + dk;
+    if (ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy || (DIM == 3 && (ck < 0 || ck >= M.ncz))) continue;
+    const int l = (-dk) * 4 + ((-dj) ? ((-di) ? 2 : 3) : ((-di) ? 1 : 0));
+    const long long c = cell_id(M, ci, cj, ck);
+    const double pr = __ldg(F.p + c) + __ldg(F.q + c);
+    const R3 fv = pr * load_cqs<DIM>(F, N, c, l);
+    S.x = S.x + fv.x; S.y = S.y + fv.y; S.z = S.z + fv.z;
+  }
+  if (EL) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const int di = (s & 1) - 1, dj = ((s >> 1) & 1) - 1, dk = DIM == 3 ? ((s >> 2) & 1) - 1 : 0;
+      const int ci = i + di, cj = j + dj, ck = k + dk;
+      if (ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy || (DIM == 3 && (ck < 0 || ck >= M.ncz))) continue;
+      const int l = (-dk) * 4 + ((-dj) ? ((-di) ? 2 : 3) : ((-di) ? 1 : 0));
+      const long long c = cell_id(M, ci, cj, ck);
+      // force_tensor = -S_n; prodTensVec(t, v) = (t.x.v, t.y.v, t.z.v)
+      const double sxx = F.S[c], syy = F.S[N + c], szz = F.S[2 * N + c];
+      const double sxy = F.S[3 * N + c], syz = F.S[4 * N + c], szx = F.S[5 * N + c];
+      const R3 rx = {-sxx, -sxy, -szx}, ry = {-sxy, -syy, -syz}, rz = {-szx, -syz, -szz};
+      const R3 cq = load_cqs<DIM>(F, N, c, l);
+      S.x = S.x + dot(rx, cq); S.y = S.y + dot(ry, cq); S.z = S.z + dot(rz, cq);
+    }
+  }
   const double dt = F.s->dt;
   const double dth = 0.5 * (F.s->old_dt + dt);
   const double t = F.s->t;
-  const long long N = M.ncell, NN = M.nnode;
-  int kz0 = 0, kz1 = 1;
-  if (DIM == 3) {
-    kz0 = bz * LZCHUNK;
-    kz1 = min(kz0 + LZCHUNK, M.nnz);
+  double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
+  const double f = dth / F.mn[n];
+  vx = vx + f * S.x; vy = vy + f * S.y; vz = vz + f * S.z;
+  vx = vx + dth * P.gravity[0]; vy = vy + dth * P.gravity[1]; vz = vz + dth * P.gravity[2];
+  if (HG) {
+    F.Ud[0][n] = vx; F.Ud[0][NN + n] = vy; F.Ud[0][2 * NN + n] = vz;
+    return;
   }
-  R3 S = {0., 0., 0.};
-  R3 eprev[4];  // EL, 3D: elasto terms of the layer below, kept until the pressure sum is complete
-  bool eok[4] = {false, false, false, false};
-  for (int L = (DIM == 3 ? kz0 - 1 : 0); L < (DIM == 3 ? kz1 : 1); ++L) {
-    // corner forces of cell layer L
-    for (int cl = threadIdx.x; cl < NCL; cl += LAG_THREADS) {
-      int a = cl % CW, b = cl / CW;
-      int ci = i0 - 1 + a, cj = j0 - 1 + b;
-      bool ok = ci >= 0 && ci < M.ncx && cj >= 0 && cj < M.ncy && (DIM == 2 || (L >= 0 && L < M.ncz));
-      cvalid[cl] = ok;
-      if (!ok) continue;
-      int ck = DIM == 3 ? L : 0;
-      R3 coord[8];
-      for (int l = 0; l < NBN; ++l) {
-        int da, db, dc;
-        local_node_offset(l, da, db, dc);
-        long long nn = node_id(M, ci + da, cj + db, ck + dc);
-        coord[l] = {F.Xp[0][nn], F.Xp[1][nn], F.Xp[2][nn]};
-      }
-      R3 cq[8];
-      if (DIM == 3) {
-        R3 fc[6];
-        hex_face_centres(coord, fc);
-        cqs3(coord, fc, cq);
-      } else {
-        cqs2(coord, cq);
-      }
-      long long cc = cell_id(M, ci, cj, ck);
-      double pr = F.p[cc] + F.q[cc];
-      double* dst = &corner[cl * NBN * 3];
-      for (int l = 0; l < NBN; ++l) {
-        R3 fv = pr * cq[l];
-        dst[3 * l] = fv.x; dst[3 * l + 1] = fv.y; dst[3 * l + 2] = fv.z;
-      }
-      if (EL) {
-        // force_tensor = -S_n; prodTensVec(t, v) = (t.x.v, t.y.v, t.z.v)
-        const double sxx = F.S[cc], syy = F.S[N + cc], szz = F.S[2 * N + cc];
-        const double sxy = F.S[3 * N + cc], syz = F.S[4 * N + cc], szx = F.S[5 * N + cc];
-        const R3 rx = {-sxx, -sxy, -szx}, ry = {-sxy, -syy, -syz}, rz = {-szx, -syz, -szz};
-        double* edst = &ecorner[cl * NBN * 3];
-        for (int l = 0; l < NBN; ++l) {
-          edst[3 * l] = dot(rx, cq[l]); edst[3 * l + 1] = dot(ry, cq[l]); edst[3 * l + 2] = dot(rz, cq[l]);
-        }
-      }
-    }
-    __syncthreads();
-    if (node_ok) {
-      // cells around node (ni,nj): local index (a,b) = (tx + di, ty + dj), di,dj in {0,1}
-      const int c00 = ty * CW + tx, c10 = ty * CW + tx + 1, c01 = (ty + 1) * CW + tx, c11 = (ty + 1) * CW + tx + 1;
-      auto add = [&](R3& acc, const double* arr, int cl, int l) {
-        if (!cvalid[cl]) return;
-        const double* src = &arr[cl * NBN * 3 + 3 * l];
-        acc.x = acc.x + src[0]; acc.y = acc.y + src[1]; acc.z = acc.z + src[2];
-      };
-      auto get = [&](const double* arr, int cl, int l, R3& out) {
-        if (!cvalid[cl]) { out = {0., 0., 0.}; return false; }
-        const double* src = &arr[cl * NBN * 3 + 3 * l];
-        out = {src[0], src[1], src[2]};
-        return true;
-      };
-      int kplane = DIM == 3 ? L : 0;
-      if (DIM == 2 || L >= kz0) {
-        // bottoms of layer L complete node plane L (cells in ascending id)
-        add(S, corner, c00, 2); add(S, corner, c10, 3); add(S, corner, c01, 1); add(S, corner, c11, 0);
-        if (EL) {
-          // elasto terms after the complete pressure sum, cells in ascending id
-          if (DIM == 3) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-              if (eok[q]) S = S + eprev[q];
-          }
-          add(S, ecorner, c00, 2); add(S, ecorner, c10, 3); add(S, ecorner, c01, 1); add(S, ecorner, c11, 0);
-        }
-        long long n = node_id(M, ni, nj, kplane);
-        double mnode = F.mn[n];
-        double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
-        double f = dth / mnode;
-        vx = vx + f * S.x; vy = vy + f * S.y; vz = vz + f * S.z;
-        vx = vx + dth * P.gravity[0]; vy = vy + dth * P.gravity[1]; vz = vz + dth * P.gravity[2];
-        if (HG) {
-          F.Ud[0][n] = vx; F.Ud[0][NN + n] = vy; F.Ud[0][2 * NN + n] = vz;
-        } else {
-          const double eps = 1.e-8;
-          for (int b = 0; b < P.nb_bc; ++b) {
-            const mhc_bc& bc = P.bc[b];
-            if ((t - dt * (1 - eps)) < bc.tdebut) continue;
-            if ((t - dt * (1 - eps)) > bc.tfin) continue;
-            if (!node_on_surface(M, ni, nj, kplane, bc.surface)) continue;
-            if (bc.kind == MHC_BC_VX) vx = bc.value;
-            else if (bc.kind == MHC_BC_VY) vy = bc.value;
-            else if (bc.kind == MHC_BC_VZ) vz = bc.value;
-          }
-          R3 x = euler ? node_x0(M, ni, nj, kplane) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
-          F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
-          F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
-        }
-      }
-      if (DIM == 3 && L + 1 < kz1) {
-        // tops of layer L start node plane L+1
-        S = {0., 0., 0.};
-        add(S, corner, c00, 6); add(S, corner, c10, 7); add(S, corner, c01, 5); add(S, corner, c11, 4);
-        if (EL) {
-          eok[0] = get(ecorner, c00, 6, eprev[0]);
-          eok[1] = get(ecorner, c10, 7, eprev[1]);
-          eok[2] = get(ecorner, c01, 5, eprev[2]);
-          eok[3] = get(ecorner, c11, 4, eprev[3]);
-        }
-      }
-    }
-    __syncthreads();
+  const double eps = 1.e-8;
+  for (int b = 0; b < P.nb_bc; ++b) {
+    const mhc_bc& bc = P.bc[b];
+    if ((t - dt * (1 - eps)) < bc.tdebut) continue;
+    if ((t - dt * (1 - eps)) > bc.tfin) continue;
+    if (!node_on_surface(M, i, j, k, bc.surface)) continue;
+    if (bc.kind == MHC_BC_VX) vx = bc.value;
+    else if (bc.kind == MHC_BC_VY) vy = bc.value;
+    else if (bc.kind == MHC_BC_VZ) vz = bc.value;
   }
+  const R3 x = P.with_projection ? node_x0(M, i, j, k) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+  F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
+  F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
 }
 
 // ---------------------------------------------------------------------------
@@ -611,25 +562,16 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
 // ---------------------------------------------------------------------------
 template <int DIM>
 __device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh& M, const Fields& F, long long c,
-                                            int i, int j, int k, const R3* cqs, double V, double Vn, double mass,
-                                            double dt, double& w1, double& w2) {
+                                            int i, int j, int k, const R3* cqn, const R3* cqs, double V, double Vn,
+                                            double mass, double dt, double& w1, double& w2) {
   constexpr int NBN = DIM == 3 ? 8 : 4;
   const long long N = M.ncell;
-  R3 coordn[8], cqn[8];
   R3 vel[8];
   for (int l = 0; l < NBN; ++l) {
     int a, b, d;
     local_node_offset(l, a, b, d);
     const long long nn = node_id(M, i + a, j + b, k + d);
-    coordn[l] = {F.Xp[0][nn], F.Xp[1][nn], F.Xp[2][nn]};
     vel[l] = {F.vx[nn], F.vy[nn], F.vz[nn]};
-  }
-  if (DIM == 3) {
-    R3 fc[6];
-    hex_face_centres(coordn, fc);
-    cqs3(coordn, fc, cqn);
-  } else {
-    cqs2(coordn, cqn);
   }
   double G[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
   for (int l = 0; l < NBN; ++l) {
@@ -736,6 +678,10 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   R3 cqs[8];
   const double V = cell_volume<DIM>(coord, cqs);
   if (V < 0.) atomicOr(&F.s->status, ST_NEG_VOLUME);
+  R3 cqn[EL ? 8 : 1];  // EL: corner normals at n, read before they are replaced
+  if (EL)
+    for (int q = 0; q < NBN; ++q) cqn[q] = load_cqs_rw<DIM>(F, N, c, q);
+  store_cqs<DIM>(F, N, c, cqs);
   const double l = char_length(P, DIM, V, coord);
   const uint8_t mask = F.mask[c];
   const bool pure = __popc(mask) == 1;
@@ -788,7 +734,7 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   for (int q = 0; q < NE; ++q) ecur[q] = ene[q];
   if (EL) {
     double w1, w2;
-    elasto_cell<DIM>(P.env[0], M, F, c, i, j, k, cqs, V, F.V[c], me[0], dt, w1, w2);
+    elasto_cell<DIM>(P.env[0], M, F, c, i, j, k, cqn, cqs, V, F.V[c], me[0], dt, w1, w2);
     ecur[0] = ecur[0] + w1;
     ecur[0] = ecur[0] + w2;
   }

@@ -28,7 +28,7 @@ struct WorkItem {
 enum PhaseKind {
   PH_CELLS = 0,      // one block per CT cells
   PH_NODES = 1,      // one block per CT nodes
-  PH_LAG_NODES = 2,  // LTX x LTY x LZCHUNK node tiles
+  PH_UNUSED = 2,
   PH_SWC0 = 3,       // cell sweep along D = PH - PH_SWC0
   PH_SWN0 = 6        // node sweep along D = PH - PH_SWN0
 };
@@ -41,12 +41,6 @@ __host__ __device__ inline void phase_grid(int ph, const Mesh& M, int& gx, int& 
   gy = gz = 1;
   if (ph == PH_CELLS) { gx = cdiv_i(M.ncell, CT); return; }
   if (ph == PH_NODES) { gx = cdiv_i(M.nnode, CT); return; }
-  if (ph == PH_LAG_NODES) {
-    gx = cdiv_i(M.nnx, LTX);
-    gy = cdiv_i(M.nny, LTY);
-    gz = M.dim == 3 ? cdiv_i(M.nnz, LZCHUNK) : 1;
-    return;
-  }
   // lane layout of mhc_sweep.cuh (sweep_lane)
   const bool nodes = ph >= PH_SWN0;
   const int D = nodes ? ph - PH_SWN0 : ph - PH_SWC0;
@@ -116,15 +110,14 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
 #endif
 
 template <int DIM, bool EL, bool HG>
-__global__ void __launch_bounds__(LAG_THREADS, MHC_LAG_MIN_BLOCKS) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
+__global__ void __launch_bounds__(CT) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
-    const WorkItem wi = item_at<PH_LAG_NODES>(C, L, w_);
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_lagrange_nodes<DIM, EL, HG>(M, *C[wi.c].P, F, wi.x, wi.y, wi.z);
-    __syncthreads();
+    body_lagrange_nodes<DIM, EL, HG>(M, *C[wi.c].P, F, wi.x);
   }
 }
 
