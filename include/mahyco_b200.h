@@ -191,8 +191,10 @@ int mhc_batch_poll(mhc_batch* b, int capacity, long long* iteration, int* status
  * No counterpart in the reference (one case per process there).  Requests
  * (a case and an iteration count) are queued by submit; every step admits
  * queued requests whose device footprint (mhc_case_device_bytes) fits the
- * budget, in arrival order with bounded backfilling, advances every
- * resident case `cycles` iterations with one launch per phase, and retires
+ * budget, in arrival order with bounded backfilling, advances the resident
+ * cases with one launch per phase and size class (the slowest class
+ * `cycles` iterations, smaller classes as many as take about as long,
+ * at most 64 x cycles), and retires
  * the cases that reached their iteration count, stopped or failed.  Results
  * stay resident, and charged to the budget, until released.  Per-request
  * status: the MHC_ST_* flags, including MHC_ST_OOM_ADMISSION (larger than
@@ -202,8 +204,11 @@ enum { MHC_REQ_QUEUED = 0, MHC_REQ_RUNNING = 1, MHC_REQ_DONE = 2, MHC_REQ_FAILED
 /* budget <= 0: 90% of the device memory free at creation */
 int mhc_server_create(long long hbm_budget_bytes, mhc_server** out);
 int mhc_server_destroy(mhc_server* s);
-void* mhc_server_stream(mhc_server* s);
-mhc_batch* mhc_server_batch(mhc_server* s);
+/* requests are served by size class (cells < 3e4, < 1e6, larger), each a
+ * batch on its own stream; stream of class cls (0..2) */
+void* mhc_server_stream(mhc_server* s, int cls);
+/* kernels the server has put on the GPU so far */
+long long mhc_server_launches(mhc_server* s);
 /* timeout_s <= 0: no deadline */
 int mhc_server_submit(mhc_server* s, const mhc_case_params* p, long long iterations, double timeout_s, long long* ticket);
 /* returns the number of requests that completed (done or failed) in this step */

@@ -86,8 +86,8 @@ _SIGS = {
                                  C.POINTER(C.c_double)]),
     "mhc_server_create": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
     "mhc_server_destroy": (C.c_int, [C.c_void_p]),
-    "mhc_server_stream": (C.c_void_p, [C.c_void_p]),
-    "mhc_server_batch": (C.c_void_p, [C.c_void_p]),
+    "mhc_server_stream": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "mhc_server_launches": (C.c_longlong, [C.c_void_p]),
     "mhc_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.POINTER(C.c_longlong)]),
     "mhc_server_step": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_server_poll": (C.c_int, [C.c_void_p, C.c_longlong, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -379,13 +379,12 @@ class Server:
     def __exit__(self, *a):
         self.close()
 
-    @property
-    def stream_handle(self) -> int:
-        return int(self.lib.mhc_server_stream(self.s) or 0)
+    def stream_handle(self, size_class: int = 0) -> int:
+        return int(self.lib.mhc_server_stream(self.s, int(size_class)) or 0)
 
     @property
     def launches(self) -> int:
-        return int(self.lib.mhc_batch_launches(self.lib.mhc_server_batch(self.s)))
+        return int(self.lib.mhc_server_launches(self.s))
 
     def submit(self, params: CaseParams, iterations: int, timeout_s: float = 0.0) -> int:
         t = C.c_longlong()

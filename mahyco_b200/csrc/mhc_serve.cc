@@ -5,11 +5,18 @@
 // submit() queues it; every step() admits queued requests while their
 // device footprint fits the budget (in arrival order, with bounded
 // backfilling of smaller requests behind a blocked one), starts them, runs
-// the requested number of cycles of everything resident in one launch per
-// phase, then reads every case's status in one copy and retires the cases
-// that finished.  A retired case stays resident until the caller fetches its
-// results and releases it, and its memory stays charged to the budget until
-// then.  Requests never block each other's arithmetic: each case's results
+// cycles of everything resident, then reads every case's status in one copy
+// per batch and retires the cases that finished.  A retired case stays
+// resident until the caller fetches its results and releases it, and its
+// memory stays charged to the budget until then.
+//
+// Resident cases are split into size classes, each a batch on its own
+// stream: all cases of a batch advance in lockstep (one launch per phase),
+// so a small request sharing a batch with a large one would move at the
+// large one's pace.  Each step gives every class the number of cycles that
+// takes about as long as the slowest class's `cycles` (estimated from the
+// launches and cells per cycle), and the classes' streams overlap on the
+// GPU.  Requests never change each other's arithmetic: each case's results
 // are the same alone and in any mix.
 //
 // Host-only C++ over the public batch API; no counterpart in the reference,
@@ -27,8 +34,14 @@
 
 namespace {
 
+constexpr int kClasses = 3;
+// class of a request by its cells: [0, 3e4), [3e4, 1e6), [1e6, inf)
+int size_class(long long cells) { return cells < 30000 ? 0 : (cells < 1000000 ? 1 : 2); }
+
 struct Request {
   long long ticket = 0;
+  int cls = 0;
+  long long cells = 0;
   mhc_case_params P;
   long long iterations = 0;
   double timeout_s = 0.;      // 0 = none
@@ -48,7 +61,7 @@ double now_s(std::chrono::steady_clock::time_point t0) {
 }  // namespace
 
 struct mhc_server {
-  mhc_batch* batch = nullptr;
+  mhc_batch* batch[kClasses] = {nullptr, nullptr, nullptr};
   long long budget = 0;
   long long in_use = 0;
   int max_bypass = 64;        // admissions allowed past a blocked queue head
@@ -58,7 +71,7 @@ struct mhc_server {
   std::deque<long long> queue;                     // tickets, arrival order
   std::vector<long long> running;                  // tickets on the GPU
   std::unordered_map<long long, Request> reqs;
-  std::unordered_map<int, long long> by_slot;
+
   std::vector<long long> poll_it;
   std::vector<int> poll_st;
   std::vector<double> poll_t;
@@ -68,11 +81,13 @@ struct mhc_server {
 int mhc_server_create(long long hbm_budget_bytes, mhc_server** out) {
   if (!out) return MHC_ERR_ARG;
   mhc_server* s = new mhc_server();
-  int r = mhc_batch_create(&s->batch);
-  if (r) { delete s; return r; }
+  for (int c = 0; c < kClasses; ++c) {
+    int r = mhc_batch_create(&s->batch[c]);
+    if (r) { mhc_server_destroy(s); return r; }
+  }
   if (hbm_budget_bytes <= 0) {
     size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { mhc_batch_destroy(s->batch); delete s; return MHC_ERR_CUDA; }
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { mhc_server_destroy(s); return MHC_ERR_CUDA; }
     hbm_budget_bytes = (long long)(0.9 * (double)fr);
   }
   s->budget = hbm_budget_bytes;
@@ -83,14 +98,21 @@ int mhc_server_create(long long hbm_budget_bytes, mhc_server** out) {
 
 int mhc_server_destroy(mhc_server* s) {
   if (!s) return MHC_OK;
-  mhc_batch_destroy(s->batch);
+  for (int c = 0; c < kClasses; ++c) mhc_batch_destroy(s->batch[c]);
   delete s;
   return MHC_OK;
 }
 
-void* mhc_server_stream(mhc_server* s) { return s ? mhc_batch_stream(s->batch) : nullptr; }
+void* mhc_server_stream(mhc_server* s, int cls) {
+  return (s && cls >= 0 && cls < kClasses) ? mhc_batch_stream(s->batch[cls]) : nullptr;
+}
 
-mhc_batch* mhc_server_batch(mhc_server* s) { return s ? s->batch : nullptr; }
+long long mhc_server_launches(mhc_server* s) {
+  if (!s) return MHC_ERR_ARG;
+  long long n = 0;
+  for (int c = 0; c < kClasses; ++c) n += mhc_batch_launches(s->batch[c]);
+  return n;
+}
 
 int mhc_server_submit(mhc_server* s, const mhc_case_params* p, long long iterations, double timeout_s,
                       long long* ticket) {
@@ -102,6 +124,8 @@ int mhc_server_submit(mhc_server* s, const mhc_case_params* p, long long iterati
   q.timeout_s = timeout_s;
   q.bytes = mhc_case_device_bytes(p);
   if (q.bytes < 0) return MHC_ERR_ARG;
+  q.cells = (long long)p->nx * p->ny * (p->dim == 3 ? p->nz : 1);
+  q.cls = size_class(q.cells);
   q.t_submit = now_s(s->t0);
   if (q.bytes > s->budget) {
     // can never fit: refused at once
@@ -129,6 +153,7 @@ void finish(mhc_server* s, Request& q, int state, int status, double t) {
 
 int admit(mhc_server* s) {
   int added = 0;
+  bool touched[kClasses] = {false, false, false};
   bool head_blocked = false;
   for (auto it = s->queue.begin(); it != s->queue.end();) {
     Request& q = s->reqs[*it];
@@ -148,7 +173,7 @@ int admit(mhc_server* s) {
       ++s->bypassed;
     }
     int slot = -1;
-    int r = mhc_batch_add(s->batch, &q.P, q.iterations, &slot);
+    int r = mhc_batch_add(s->batch[q.cls], &q.P, q.iterations, &slot);
     if (r == MHC_ERR_NOMEM || r == MHC_ERR_CUDA) {
       // the device refused the memory the budget allowed: wait for frees
       if (s->running.empty()) {
@@ -168,15 +193,16 @@ int admit(mhc_server* s) {
     q.state = MHC_REQ_RUNNING;
     q.t_admit = t;
     s->in_use += q.bytes;
-    s->by_slot[slot] = q.ticket;
     s->running.push_back(q.ticket);
+    touched[q.cls] = true;
     it = s->queue.erase(it);
     ++added;
   }
-  if (added) {
-    int r = mhc_batch_init(s->batch);
-    if (r) return r;
-  }
+  for (int c = 0; c < kClasses; ++c)
+    if (touched[c]) {
+      int r = mhc_batch_init(s->batch[c]);
+      if (r) return r;
+    }
   return added;
 }
 
@@ -188,21 +214,45 @@ int mhc_server_step(mhc_server* s, int cycles) {
   int r = admit(s);
   if (r < 0) return r;
   if (s->running.empty()) return (int)(s->completed - done0);
-  if (cycles > 0 && (r = mhc_batch_cycle(s->batch, cycles))) return r;
-  int ns = 0;
-  for (long long tk : s->running) ns = std::max(ns, s->reqs[tk].slot + 1);
-  s->poll_it.resize(ns);
-  s->poll_st.resize(ns);
-  s->poll_t.resize(ns);
-  r = mhc_batch_poll(s->batch, ns, s->poll_it.data(), s->poll_st.data(), s->poll_t.data());
-  if (r < 0) return r;
+  // estimated seconds per cycle of each class: launches + streamed cells
+  long long cells[kClasses] = {0, 0, 0};
+  int cases[kClasses] = {0, 0, 0}, nslot[kClasses] = {0, 0, 0};
+  for (long long tk : s->running) {
+    const Request& q = s->reqs[tk];
+    cells[q.cls] += q.cells;
+    cases[q.cls] += 1;
+    nslot[q.cls] = std::max(nslot[q.cls], q.slot + 1);
+  }
+  double cost[kClasses], tmax = 0.;
+  for (int c = 0; c < kClasses; ++c) {
+    cost[c] = cases[c] ? 60e-6 + 1.0e-9 * (double)cells[c] : 0.;
+    tmax = std::max(tmax, cost[c]);
+  }
+  if (cycles > 0)
+    for (int c = 0; c < kClasses; ++c) {
+      if (!cases[c]) continue;
+      const double k = (double)cycles * tmax / cost[c];
+      const int kc = (int)std::min((double)(64 * cycles), std::max((double)cycles, k + 0.5));
+      if ((r = mhc_batch_cycle(s->batch[c], kc))) return r;
+    }
+  std::vector<long long> pit[kClasses];
+  std::vector<int> pst[kClasses];
+  std::vector<double> ptm[kClasses];
+  for (int c = 0; c < kClasses; ++c) {
+    if (!cases[c]) continue;
+    pit[c].resize(nslot[c]);
+    pst[c].resize(nslot[c]);
+    ptm[c].resize(nslot[c]);
+    r = mhc_batch_poll(s->batch[c], nslot[c], pit[c].data(), pst[c].data(), ptm[c].data());
+    if (r < 0) return r;
+  }
   const double t = now_s(s->t0);
   std::vector<long long> still;
   for (long long tk : s->running) {
     Request& q = s->reqs[tk];
-    q.iteration = s->poll_it[q.slot];
-    q.time = s->poll_t[q.slot];
-    const int st = s->poll_st[q.slot];
+    q.iteration = pit[q.cls][q.slot];
+    q.time = ptm[q.cls][q.slot];
+    const int st = pst[q.cls][q.slot];
     const int err = st & ~MHC_ST_STOP;
     bool end = false;
     if (err) { finish(s, q, MHC_REQ_FAILED, st, t); end = true; }
@@ -212,7 +262,7 @@ int mhc_server_step(mhc_server* s, int cycles) {
       end = true;
     }
     if (end) {
-      if ((r = mhc_batch_detach(s->batch, q.slot))) return r;
+      if ((r = mhc_batch_detach(s->batch[q.cls], q.slot))) return r;
     } else {
       still.push_back(tk);
     }
@@ -249,7 +299,7 @@ long long mhc_server_fetch(mhc_server* s, long long ticket, const char* name, in
   if (!s) return MHC_ERR_ARG;
   auto it = s->reqs.find(ticket);
   if (it == s->reqs.end() || it->second.slot < 0) return MHC_ERR_ARG;
-  return mhc_batch_get_field(s->batch, it->second.slot, name, env, host, capacity);
+  return mhc_batch_get_field(s->batch[it->second.cls], it->second.slot, name, env, host, capacity);
 }
 
 int mhc_server_release(mhc_server* s, long long ticket) {
@@ -259,9 +309,8 @@ int mhc_server_release(mhc_server* s, long long ticket) {
   Request& q = it->second;
   if (q.state == MHC_REQ_QUEUED || q.state == MHC_REQ_RUNNING) return MHC_ERR_ORDER;
   if (q.slot >= 0) {
-    int r = mhc_batch_remove(s->batch, q.slot);
+    int r = mhc_batch_remove(s->batch[q.cls], q.slot);
     if (r) return r;
-    s->by_slot.erase(q.slot);
     s->in_use -= q.bytes;
   }
   s->reqs.erase(it);
