@@ -166,10 +166,11 @@ void launch_lagrange_cells(Engine* e) {
       // elasto cases: one environment, Lagrangian (validated at creation)
       if (g.DIM == 2) plaunch(e, kb_lagrange_cells<2, 1, false, true>, CT, 0, g.lag_cells);
       else plaunch(e, kb_lagrange_cells<3, 1, false, true>, CT, 0, g.lag_cells);
-    } else if (g.EULER) {
-      DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true, false>, CT, 0, g.lag_cells)));
     } else {
-      DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, false, false>, CT, 0, g.lag_cells)));
+      if (g.DIM == 2) plaunch(e, kb_lagrange_geom<2>, CT, 0, g.lag_cells);
+      else plaunch(e, kb_lagrange_geom<3>, CT, 0, g.lag_cells);
+      if (g.EULER) DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true, false>, CT, 0, g.lag_cells)));
+      else DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, false, false>, CT, 0, g.lag_cells)));
     }
   }
 }

@@ -212,6 +212,185 @@ __device__ __forceinline__ R3 load_cqs_rw(const Fields& F, long long N, long lon
   return {F.cqs[(NC * l) * N + c], F.cqs[(NC * l + 1) * N + c], DIM == 3 ? F.cqs[(NC * l + 2) * N + c] : 0.0};
 }
 
+// computeCQs (MahycoModule.cc:1869-1932) and the volume of
+// computeGeometricValues, face by face: each corner keeps its two partial
+// sums (weight 5 and weight 1) and receives the half-face normals of each
+// face in the order of the reference sums, so the results are bit-identical
+// to computing all 24 half-face normals first; only the corners whose faces
+// are not all done stay live.  Stores the corner normals (store_cqs layout)
+// and returns the volume.
+__device__ __forceinline__ double cell_volume_store3(const R3* nc, const Fields& F, long long N, long long c) {
+  const double t = 1. / 12.;
+  R3 a0, a1, a2, a3, a4, a5, a6, a7, b0, b1, b2, b3, b4, b5, b6, b7;
+  double d[8];
+  {  // face 1
+    const R3 fc0 = 0.25 * (nc[0] + nc[3] + nc[2] + nc[1]);
+    const R3 n1a04 = 0.5 * vecmul(nc[0] - fc0, nc[3] - fc0);
+    const R3 n1a03 = 0.5 * vecmul(nc[3] - fc0, nc[2] - fc0);
+    const R3 n1a02 = 0.5 * vecmul(nc[2] - fc0, nc[1] - fc0);
+    const R3 n1a01 = 0.5 * vecmul(nc[1] - fc0, nc[0] - fc0);
+    a0 = n1a01 + n1a04;
+    b0 = n1a02 + n1a03;
+    a1 = n1a01 + n1a02;
+    b1 = n1a04 + n1a03;
+    a2 = n1a02 + n1a03;
+    b2 = n1a01 + n1a04;
+    a3 = n1a03 + n1a04;
+    b3 = n1a01 + n1a02;
+  }
+  {  // face 2
+    const R3 fc1 = 0.25 * (nc[0] + nc[4] + nc[7] + nc[3]);
+    const R3 n2a05 = 0.5 * vecmul(nc[0] - fc1, nc[4] - fc1);
+    const R3 n2a12 = 0.5 * vecmul(nc[4] - fc1, nc[7] - fc1);
+    const R3 n2a08 = 0.5 * vecmul(nc[7] - fc1, nc[3] - fc1);
+    const R3 n2a04 = 0.5 * vecmul(nc[3] - fc1, nc[0] - fc1);
+    a0 = a0 + n2a04;
+    a0 = a0 + n2a05;
+    b0 = b0 + n2a08;
+    b0 = b0 + n2a12;
+    a3 = a3 + n2a08;
+    a3 = a3 + n2a04;
+    b3 = b3 + n2a05;
+    b3 = b3 + n2a12;
+    a4 = n2a05 + n2a12;
+    b4 = n2a08 + n2a04;
+    a7 = n2a08 + n2a12;
+    b7 = n2a04 + n2a05;
+  }
+  {  // face 3
+    const R3 fc2 = 0.25 * (nc[0] + nc[1] + nc[5] + nc[4]);
+    const R3 n3a01 = 0.5 * vecmul(nc[0] - fc2, nc[1] - fc2);
+    const R3 n3a06 = 0.5 * vecmul(nc[1] - fc2, nc[5] - fc2);
+    const R3 n3a09 = 0.5 * vecmul(nc[5] - fc2, nc[4] - fc2);
+    const R3 n3a05 = 0.5 * vecmul(nc[4] - fc2, nc[0] - fc2);
+    a0 = a0 + n3a05;
+    a0 = a0 + n3a01;
+    b0 = b0 + n3a06;
+    b0 = b0 + n3a09;
+    a1 = a1 + n3a01;
+    a1 = a1 + n3a06;
+    b1 = b1 + n3a09;
+    b1 = b1 + n3a05;
+    a4 = a4 + n3a05;
+    a4 = a4 + n3a09;
+    b4 = b4 + n3a01;
+    b4 = b4 + n3a06;
+    a5 = n3a06 + n3a09;
+    b5 = n3a01 + n3a05;
+  }
+  {  // corner 0 complete
+    const R3 o = (5. * a0 + b0) * t;
+    F.cqs[0 * N + c] = o.x; F.cqs[1 * N + c] = o.y; F.cqs[2 * N + c] = o.z;
+    d[0] = dot(nc[0], o);
+  }
+  {  // face 4
+    const R3 fc3 = 0.25 * (nc[4] + nc[5] + nc[6] + nc[7]);
+    const R3 n4a09 = 0.5 * vecmul(nc[4] - fc3, nc[5] - fc3);
+    const R3 n4a10 = 0.5 * vecmul(nc[5] - fc3, nc[6] - fc3);
+    const R3 n4a11 = 0.5 * vecmul(nc[6] - fc3, nc[7] - fc3);
+    const R3 n4a12 = 0.5 * vecmul(nc[7] - fc3, nc[4] - fc3);
+    a4 = a4 + n4a09;
+    a4 = a4 + n4a12;
+    b4 = b4 + n4a10;
+    b4 = b4 + n4a11;
+    a5 = a5 + n4a09;
+    a5 = a5 + n4a10;
+    b5 = b5 + n4a12;
+    b5 = b5 + n4a11;
+    a6 = n4a11 + n4a10;
+    b6 = n4a12 + n4a09;
+    a7 = a7 + n4a12;
+    a7 = a7 + n4a11;
+    b7 = b7 + n4a09;
+    b7 = b7 + n4a10;
+  }
+  {  // corner 4 complete
+    const R3 o = (5. * a4 + b4) * t;
+    F.cqs[12 * N + c] = o.x; F.cqs[13 * N + c] = o.y; F.cqs[14 * N + c] = o.z;
+    d[4] = dot(nc[4], o);
+  }
+  {  // face 5
+    const R3 fc4 = 0.25 * (nc[1] + nc[2] + nc[6] + nc[5]);
+    const R3 n5a02 = 0.5 * vecmul(nc[1] - fc4, nc[2] - fc4);
+    const R3 n5a07 = 0.5 * vecmul(nc[2] - fc4, nc[6] - fc4);
+    const R3 n5a10 = 0.5 * vecmul(nc[6] - fc4, nc[5] - fc4);
+    const R3 n5a06 = 0.5 * vecmul(nc[5] - fc4, nc[1] - fc4);
+    a1 = a1 + n5a06;
+    a1 = a1 + n5a02;
+    b1 = b1 + n5a10;
+    b1 = b1 + n5a07;
+    a2 = a2 + n5a07;
+    a2 = a2 + n5a02;
+    b2 = b2 + n5a06;
+    b2 = b2 + n5a10;
+    a5 = a5 + n5a10;
+    a5 = a5 + n5a06;
+    b5 = b5 + n5a07;
+    b5 = b5 + n5a02;
+    a6 = a6 + n5a10;
+    a6 = a6 + n5a07;
+    b6 = b6 + n5a06;
+    b6 = b6 + n5a02;
+  }
+  {  // corner 1 complete
+    const R3 o = (5. * a1 + b1) * t;
+    F.cqs[3 * N + c] = o.x; F.cqs[4 * N + c] = o.y; F.cqs[5 * N + c] = o.z;
+    d[1] = dot(nc[1], o);
+  }
+  {  // corner 5 complete
+    const R3 o = (5. * a5 + b5) * t;
+    F.cqs[15 * N + c] = o.x; F.cqs[16 * N + c] = o.y; F.cqs[17 * N + c] = o.z;
+    d[5] = dot(nc[5], o);
+  }
+  {  // face 6
+    const R3 fc5 = 0.25 * (nc[2] + nc[3] + nc[7] + nc[6]);
+    const R3 n6a03 = 0.5 * vecmul(nc[2] - fc5, nc[3] - fc5);
+    const R3 n6a08 = 0.5 * vecmul(nc[3] - fc5, nc[7] - fc5);
+    const R3 n6a11 = 0.5 * vecmul(nc[7] - fc5, nc[6] - fc5);
+    const R3 n6a07 = 0.5 * vecmul(nc[6] - fc5, nc[2] - fc5);
+    a2 = a2 + n6a07;
+    a2 = a2 + n6a03;
+    b2 = b2 + n6a11;
+    b2 = b2 + n6a08;
+    a3 = a3 + n6a08;
+    a3 = a3 + n6a03;
+    b3 = b3 + n6a07;
+    b3 = b3 + n6a11;
+    a6 = a6 + n6a07;
+    a6 = a6 + n6a11;
+    b6 = b6 + n6a03;
+    b6 = b6 + n6a08;
+    a7 = a7 + n6a11;
+    a7 = a7 + n6a08;
+    b7 = b7 + n6a07;
+    b7 = b7 + n6a03;
+  }
+  {  // corner 2 complete
+    const R3 o = (5. * a2 + b2) * t;
+    F.cqs[6 * N + c] = o.x; F.cqs[7 * N + c] = o.y; F.cqs[8 * N + c] = o.z;
+    d[2] = dot(nc[2], o);
+  }
+  {  // corner 3 complete
+    const R3 o = (5. * a3 + b3) * t;
+    F.cqs[9 * N + c] = o.x; F.cqs[10 * N + c] = o.y; F.cqs[11 * N + c] = o.z;
+    d[3] = dot(nc[3], o);
+  }
+  {  // corner 6 complete
+    const R3 o = (5. * a6 + b6) * t;
+    F.cqs[18 * N + c] = o.x; F.cqs[19 * N + c] = o.y; F.cqs[20 * N + c] = o.z;
+    d[6] = dot(nc[6], o);
+  }
+  {  // corner 7 complete
+    const R3 o = (5. * a7 + b7) * t;
+    F.cqs[21 * N + c] = o.x; F.cqs[22 * N + c] = o.y; F.cqs[23 * N + c] = o.z;
+    d[7] = dot(nc[7], o);
+  }
+  double volume = 0.;
+#pragma unroll
+  for (int l = 0; l < 8; ++l) volume += d[l];
+  return volume / 3;
+}
+
 __device__ __forceinline__ bool node_on_surface(const Mesh& M, int i, int j, int k, int surf) {
   switch (surf) {
     case MHC_XMIN: return i == 0;
@@ -659,6 +838,41 @@ __device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh&
   for (int q = 0; q < 6; ++q) F.S[q * N + c] = Sv[q];
 }
 
+// computeGeometricValues of one cell: corner normals (kept for the next
+// node pass), volume and characteristic length.  The cell pass reads V and
+// l back, so neither kernel holds the corner normals and the
+// thermodynamics live at the same time.
+template <int DIM>
+__device__ __forceinline__ void body_lagrange_geom(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long c = bx * (long long)CT + threadIdx.x;
+  if (c >= M.ncell) return;
+  const long long N = M.ncell;
+  int i, j, k;
+  cell_ijk(M, c, i, j, k);
+  R3 coord[8];
+#pragma unroll
+  for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+    int a, b, d;
+    local_node_offset(l, a, b, d);
+    const long long nn = node_id(M, i + a, j + b, k + d);
+    coord[l] = {F.Xn[0][nn], F.Xn[1][nn], F.Xn[2][nn]};
+  }
+  double V;
+  if (DIM == 3) {
+    V = cell_volume_store3(coord, F, N, c);
+  } else {
+    R3 cqs[4];
+    V = cell_volume<DIM>(coord, cqs);
+    store_cqs<DIM>(F, N, c, cqs);
+  }
+  if (V < 0.) atomicOr(&F.s->status, ST_NEG_VOLUME);
+  F.V[c] = V;
+  F.l[c] = char_length(P, DIM, V, coord);
+}
+
+// EL: the elasto-plastic model needs the corner normals at n and n+1, so
+// this pass computes the geometry itself; otherwise body_lagrange_geom ran
+// first and V, l are read back.
 template <int DIM, int NE, bool EULER, bool EL = false>
 __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   long long c = bx * (long long)CT + threadIdx.x;
@@ -668,21 +882,26 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   int i, j, k;
   cell_ijk(M, c, i, j, k);
   const int NBN = DIM == 3 ? 8 : 4;
-  R3 coord[8];
-  for (int l = 0; l < NBN; ++l) {
-    int a, b, d;
-    local_node_offset(l, a, b, d);
-    long long nn = node_id(M, i + a, j + b, k + d);
-    coord[l] = {F.Xn[0][nn], F.Xn[1][nn], F.Xn[2][nn]};
-  }
-  R3 cqs[8];
-  const double V = cell_volume<DIM>(coord, cqs);
-  if (V < 0.) atomicOr(&F.s->status, ST_NEG_VOLUME);
+  R3 cqs[EL ? 8 : 1];
   R3 cqn[EL ? 8 : 1];  // EL: corner normals at n, read before they are replaced
-  if (EL)
+  double V, l;
+  if (EL) {
+    R3 coord[8];
+    for (int q = 0; q < NBN; ++q) {
+      int a, b, d;
+      local_node_offset(q, a, b, d);
+      long long nn = node_id(M, i + a, j + b, k + d);
+      coord[q] = {F.Xn[0][nn], F.Xn[1][nn], F.Xn[2][nn]};
+    }
+    V = cell_volume<DIM>(coord, cqs);
     for (int q = 0; q < NBN; ++q) cqn[q] = load_cqs_rw<DIM>(F, N, c, q);
-  store_cqs<DIM>(F, N, c, cqs);
-  const double l = char_length(P, DIM, V, coord);
+    store_cqs<DIM>(F, N, c, cqs);
+    if (V < 0.) atomicOr(&F.s->status, ST_NEG_VOLUME);
+    l = char_length(P, DIM, V, coord);
+  } else {
+    V = F.V[c];
+    l = F.l[c];
+  }
   const uint8_t mask = F.mask[c];
   const bool pure = __popc(mask) == 1;
   const double dt = F.s->dt;

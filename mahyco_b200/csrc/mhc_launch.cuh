@@ -121,6 +121,23 @@ __global__ void __launch_bounds__(CT) kb_lagrange_nodes(const CaseDesc* __restri
   }
 }
 
+// resident blocks per SM asked of the compiler for the geometry pass
+#ifndef MHC_GEOM_MIN_BLOCKS
+#define MHC_GEOM_MIN_BLOCKS 1
+#endif
+
+template <int DIM>
+__global__ void __launch_bounds__(CT, MHC_GEOM_MIN_BLOCKS) kb_lagrange_geom(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_lagrange_geom<DIM>(M, *C[wi.c].P, F, wi.x);
+  }
+}
+
 template <int DIM, int NE, bool EULER, bool EL>
 __global__ void __launch_bounds__(CT, MHC_LAG_MIN_BLOCKS) kb_lagrange_cells(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
