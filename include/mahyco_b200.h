@@ -57,6 +57,17 @@ int mhc_case_destroy(mhc_case* h);
  * so that callers can record events or order their own work after it */
 void* mhc_case_stream(mhc_case* h);
 
+/* Checkpoint / restart of the device-resident state (protection-reprise,
+ * MahycoModule.cc:273-308): every device field, the time-loop scalars and
+ * the host-side loop state of a case, copied to a host buffer of
+ * mhc_case_checkpoint_bytes(h) bytes between iterations; a restore into a
+ * case created with identical parameters continues bit-identically.
+ * MHC_ERR_ORDER in the middle of an iteration, MHC_ERR_ARG for a buffer
+ * of another case or layout. */
+long long mhc_case_checkpoint_bytes(mhc_case* h);
+int mhc_case_checkpoint(mhc_case* h, void* host, long long capacity);
+int mhc_case_restore(mhc_case* h, const void* host, long long size);
+
 /* HBM bytes one case with these parameters needs (serving admission). */
 long long mhc_case_device_bytes(const mhc_case_params* params);
 
@@ -183,6 +194,10 @@ long long mhc_batch_get_field(mhc_batch* b, int index, const char* name, int env
 /* stop advancing a case but keep its state resident (fields stay readable
  * until mhc_batch_remove) */
 int mhc_batch_detach(mhc_batch* b, int index);
+/* checkpoint / restart of one case of a batch (see mhc_case_checkpoint) */
+long long mhc_batch_checkpoint_bytes(mhc_batch* b, int index);
+int mhc_batch_checkpoint(mhc_batch* b, int index, void* host, long long capacity);
+int mhc_batch_restore(mhc_batch* b, int index, const void* host, long long size);
 /* iteration done, status flags and time of every case index (removed: -1),
  * read with one gather kernel and one copy; returns the number of indices */
 int mhc_batch_poll(mhc_batch* b, int capacity, long long* iteration, int* status, double* time);

@@ -82,6 +82,12 @@ _SIGS = {
                                           C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "mhc_noalloc_last_error": (C.c_char_p, []),
     "mhc_batch_detach": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_case_checkpoint_bytes": (C.c_longlong, [C.c_void_p]),
+    "mhc_case_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    "mhc_case_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    "mhc_batch_checkpoint_bytes": (C.c_longlong, [C.c_void_p, C.c_int]),
+    "mhc_batch_checkpoint": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong]),
+    "mhc_batch_restore": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong]),
     "mhc_batch_poll": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                                  C.POINTER(C.c_double)]),
     "mhc_server_create": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
@@ -153,6 +159,18 @@ class Hydro:
     def launches(self) -> int:
         """Kernels this case has put on the GPU so far."""
         return int(self.lib.mhc_case_launches(self.h))
+
+    def checkpoint(self) -> bytes:
+        """Whole device state between iterations (protection)."""
+        n = _check(self.lib, int(self.lib.mhc_case_checkpoint_bytes(self.h)), "checkpoint size")
+        buf = C.create_string_buffer(n)
+        _check(self.lib, self.lib.mhc_case_checkpoint(self.h, buf, n), "mhc_case_checkpoint")
+        return buf.raw
+
+    def restore(self, data: bytes) -> None:
+        """Continue from a checkpoint of a case with identical parameters (reprise)."""
+        buf = C.create_string_buffer(data, len(data))
+        _check(self.lib, self.lib.mhc_case_restore(self.h, buf, len(data)), "mhc_case_restore")
 
     def close(self):
         if self.h:

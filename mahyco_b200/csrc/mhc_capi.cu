@@ -429,6 +429,7 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
     void* p = nullptr;
     if (!ok || cudaMallocAsync(&p, bytes, h->stream) != cudaSuccess) { ok = false; return nullptr; }
     h->allocs.push_back(p);
+    h->alloc_bytes.push_back(bytes);
     return p;
   };
   auto dcell = [&]() { return (double*)alloc(N * sizeof(double)); };
@@ -568,6 +569,22 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
     int r = fetch(st, F.mask, mask.data(), N);
     if (r) return r;
     for (long long i = 0; i < N; ++i) host[i] = mask[i];
+    return N;
+  }
+  // elasto output variables: minus the deviator components
+  // (DefaultModelService.cc:217-221)
+  static const char* kStrain[] = {"StrainTensorXX", "StrainTensorYY", "StrainTensorZZ", "StrainTensorXY",
+                                  "StrainTensorYZ", "StrainTensorXZ"};
+  for (int q = 0; q < 6; ++q) {
+    if (strcmp(name, kStrain[q])) continue;
+    if (cap < N) return set_err(MHC_ERR_ARG, "capacity too small");
+    if (!F.S) {
+      for (long long i = 0; i < N; ++i) host[i] = 0.;
+      return N;
+    }
+    int r = fetch(st, F.S + q * N, host, N * 8);
+    if (r) return r;
+    for (long long i = 0; i < N; ++i) host[i] = -host[i];
     return N;
   }
   if (!strcmp(name, "NodeMass")) {
@@ -742,6 +759,104 @@ int mhc_cycle_timed(mhc_case* h, int n, double* stage_ms, long long* stage_launc
   return engine_timed(h->solo, n, stage_ms, stage_launches);
 }
 
+// -- checkpoint / restart (protection-reprise) --------------------------------
+// A checkpoint is a header (magic, the case parameters, the host-side loop
+// state, the size of every device allocation) followed by the bytes of
+// every device allocation in creation order: the whole device state of the
+// case, scalars included.
+namespace {
+struct CkptHeader {
+  char magic[8];
+  long long version;
+  mhc_case_params params;
+  long long it_host;
+  int stage;
+  int initialised;
+  long long nalloc;
+};
+constexpr char kCkptMagic[8] = {'M', 'H', 'C', 'C', 'K', 'P', 'T', '1'};
+
+long long ckpt_bytes(const mhc_case* h) {
+  long long b = (long long)sizeof(CkptHeader) + (long long)(h->alloc_bytes.size() * sizeof(long long));
+  for (size_t a : h->alloc_bytes) b += (long long)a;
+  return b;
+}
+
+int ckpt_save(mhc_case* h, cudaStream_t st, void* host, long long capacity) {
+  const long long need = ckpt_bytes(h);
+  if (!host || capacity < need) return set_err(MHC_ERR_ARG, "checkpoint buffer smaller than mhc_case_checkpoint_bytes");
+  CkptHeader hd;
+  memset(&hd, 0, sizeof(hd));
+  memcpy(hd.magic, kCkptMagic, 8);
+  hd.version = 1;
+  hd.params = h->P;
+  hd.it_host = h->it_host;
+  hd.stage = h->stage;
+  hd.initialised = h->initialised ? 1 : 0;
+  hd.nalloc = (long long)h->allocs.size();
+  char* out = static_cast<char*>(host);
+  memcpy(out, &hd, sizeof(hd));
+  out += sizeof(hd);
+  for (size_t a : h->alloc_bytes) {
+    const long long b = (long long)a;
+    memcpy(out, &b, sizeof(b));
+    out += sizeof(b);
+  }
+  CK(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < h->allocs.size(); ++i) {
+    CK(cudaMemcpyAsync(out, h->allocs[i], h->alloc_bytes[i], cudaMemcpyDeviceToHost, st));
+    out += h->alloc_bytes[i];
+  }
+  CK(cudaStreamSynchronize(st));
+  return MHC_OK;
+}
+
+int ckpt_restore(mhc_case* h, cudaStream_t st, const void* host, long long size) {
+  if (!host || size < (long long)sizeof(CkptHeader)) return set_err(MHC_ERR_ARG, "checkpoint too small");
+  CkptHeader hd;
+  memcpy(&hd, host, sizeof(hd));
+  if (memcmp(hd.magic, kCkptMagic, 8) || hd.version != 1) return set_err(MHC_ERR_ARG, "not a checkpoint of this library");
+  if (memcmp(&hd.params, &h->P, sizeof(mhc_case_params)))
+    return set_err(MHC_ERR_ARG, "checkpoint of a case with other parameters");
+  if (hd.nalloc != (long long)h->allocs.size() || size != ckpt_bytes(h))
+    return set_err(MHC_ERR_ARG, "checkpoint layout does not match the case");
+  const char* in = static_cast<const char*>(host) + sizeof(hd);
+  for (size_t i = 0; i < h->alloc_bytes.size(); ++i) {
+    long long b;
+    memcpy(&b, in, sizeof(b));
+    in += sizeof(b);
+    if (b != (long long)h->alloc_bytes[i]) return set_err(MHC_ERR_ARG, "checkpoint layout does not match the case");
+  }
+  CK(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < h->allocs.size(); ++i) {
+    CK(cudaMemcpyAsync(h->allocs[i], in, h->alloc_bytes[i], cudaMemcpyHostToDevice, st));
+    in += h->alloc_bytes[i];
+  }
+  CK(cudaStreamSynchronize(st));
+  h->it_host = hd.it_host;
+  h->stage = hd.stage;
+  h->initialised = hd.initialised != 0;
+  return MHC_OK;
+}
+}  // namespace
+
+long long mhc_case_checkpoint_bytes(mhc_case* h) { return h ? ckpt_bytes(h) : set_err(MHC_ERR_ARG, "null case"); }
+
+int mhc_case_checkpoint(mhc_case* h, void* host, long long capacity) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  if (h->stage != S_IDLE) return set_err(MHC_ERR_ORDER, "checkpoint between iterations only");
+  return ckpt_save(h, h->stream, host, capacity);
+}
+
+int mhc_case_restore(mhc_case* h, const void* host, long long size) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  if (h->stage != S_IDLE) return set_err(MHC_ERR_ORDER, "restore between iterations only");
+  int r = ckpt_restore(h, h->stream, host, size);
+  if (r) return r;
+  if (h->solo) h->solo->dirty = true;  // iteration-dependent work lists are rebuilt
+  return MHC_OK;
+}
+
 int mhc_synchronize(mhc_case* h) {
   if (!h) return set_err(MHC_ERR_ARG, "null case");
   Scalars s;
@@ -865,6 +980,24 @@ int mhc_batch_remove(mhc_batch* b, int index) {
   case_free(h);
   b->slots[index] = nullptr;
   b->detached[index] = 0;
+  return MHC_OK;
+}
+
+long long mhc_batch_checkpoint_bytes(mhc_batch* b, int index) {
+  if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
+  return ckpt_bytes(b->slots[index]);
+}
+
+int mhc_batch_checkpoint(mhc_batch* b, int index, void* host, long long capacity) {
+  if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
+  return ckpt_save(b->slots[index], b->e->stream, host, capacity);
+}
+
+int mhc_batch_restore(mhc_batch* b, int index, const void* host, long long size) {
+  if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
+  int r = ckpt_restore(b->slots[index], b->e->stream, host, size);
+  if (r) return r;
+  b->e->dirty = true;
   return MHC_OK;
 }
 

@@ -43,6 +43,7 @@ struct mhc_case {
   cudaStream_t stream = nullptr;   // allocation stream (and launches when standalone)
   bool own_stream = false;
   std::vector<void*> allocs;
+  std::vector<size_t> alloc_bytes;  // size of each allocation (checkpoints)
   long long it_host = 1;           // iteration the next launched cycle runs
   int stage = S_IDLE;
   bool initialised = false;

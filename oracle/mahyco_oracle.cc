@@ -1687,6 +1687,14 @@ long oracle_get_field(void* h, const char* name, int env, double* out, long cap)
       out[c] = name[0] == 'C' ? C.char_len[c] : (name[0] == 'E' && name[1] == 'u' ? C.euler_volume[c] : (double)C.envmask[c]);
     return C.ncell;
   }
+  static const char* kStrain[] = {"StrainTensorXX", "StrainTensorYY", "StrainTensorZZ", "StrainTensorXY",
+                                  "StrainTensorYZ", "StrainTensorXZ"};
+  for (int q = 0; q < 6; ++q) {
+    if (strcmp(name, kStrain[q])) continue;
+    if (cap < C.ncell) return -1;
+    for (long c = 0; c < C.ncell; ++c) out[c] = C.elasto ? -C.sdev[c * 6 + q] : 0.;
+    return C.ncell;
+  }
   if (!strcmp(name, "NodeMass")) {
     if (cap < C.nnode) return -1;
     for (long n = 0; n < C.nnode; ++n) out[n] = C.node_mass[n];

@@ -34,6 +34,8 @@ def compare(gpu, ora, nenv):
         errs[f] = rel_inf(gpu.field(f), ora.field(f))
     for f in ("Velocity", "NodeMass"):
         errs[f] = rel_inf(gpu.field(f), ora.field(f))
+    for f in ("StrainTensorXX", "StrainTensorYY", "StrainTensorXY"):
+        errs[f] = rel_inf(gpu.field(f), ora.field(f))
     if nenv > 1:
         errs["EnvMask"] = float(np.any(gpu.field("EnvMask") != ora.field("EnvMask")))
         for e in range(nenv):
