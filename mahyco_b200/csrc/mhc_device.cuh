@@ -191,6 +191,16 @@ __device__ __forceinline__ double flux_limiter(int id, double r) {
   if (id == 2) return (r <= 0.0) ? 0.0 : 2.0 * r / (1.0 + r);
   return 0.0;
 }
+// x / y with IEEE round-to-nearest, taking the zero-numerator case out of
+// the division: 0 / y is exactly +-0 (sign of x xor sign of y) for every y
+// other than 0 and NaN, and such quotients (absent materials, flat fields)
+// would otherwise leave the division's fast path.
+__device__ __forceinline__ double div_rn(double x, double y) {
+  if (x == 0.0 && y == y && y != 0.0)
+    return ((__double_as_longlong(x) ^ __double_as_longlong(y)) < 0) ? -0.0 : 0.0;
+  return x / y;
+}
+
 // limiter id as a template argument (LIM_ORDER1: first-order remap, no slope)
 constexpr int LIM_ORDER1 = 3;
 template <int LIM>
@@ -203,8 +213,8 @@ __device__ __forceinline__ double flux_limiter_t(double r) {
 template <int LIM>
 __device__ __forceinline__ double limited_gradient_t(double gb, double gf) {
   double g = 0.;
-  if (gb != 0.) g += 0.5 * (flux_limiter_t<LIM>(gf / gb) * gb);
-  if (gf != 0.) g += 0.5 * (flux_limiter_t<LIM>(gb / gf) * gf);
+  if (gb != 0.) g += 0.5 * (flux_limiter_t<LIM>(div_rn(gf, gb)) * gb);
+  if (gf != 0.) g += 0.5 * (flux_limiter_t<LIM>(div_rn(gb, gf)) * gf);
   return g;
 }
 __device__ __forceinline__ double limited_gradient(int id, double gb, double gf) {

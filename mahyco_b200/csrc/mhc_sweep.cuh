@@ -324,9 +324,9 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
   constexpr bool FRONT_FIRST = DIM == 2 && D == 0;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    const double phi = ok ? u[v] / den : 0.;
+    const double phi = ok ? div_rn(u[v], den) : 0.;
     const double phi_l = __shfl_up_sync(FULL, phi, 1);
-    const double gf = face_b ? (phi - phi_l) / dxb : 0.;
+    const double gf = face_b ? div_rn(phi - phi_l, dxb) : 0.;
     const double gf_r = __shfl_down_sync(FULL, gf, 1);
     const double gr = (LIM != LIM_ORDER1 && ok) ? limited_gradient_t<LIM>(gf, gf_r) : 0.;
     const double gr_l = __shfl_up_sync(FULL, gr, 1);
@@ -410,8 +410,8 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
       U[4] = 0.5 * mn * (vx * vx + vy * vy + vz * vz);
     }
     if (was_inner) {
-      ph[0] = U[0] / U[3]; ph[1] = U[1] / U[3]; ph[2] = U[2] / U[3];
-      ph[3] = U[4] / U[3];
+      ph[0] = div_rn(U[0], U[3]); ph[1] = div_rn(U[1], U[3]); ph[2] = div_rn(U[2], U[3]);
+      ph[3] = div_rn(U[4], U[3]);
     } else {
       const double vx = __ldg(F.vx + n), vy = __ldg(F.vy + n), vz = __ldg(F.vz + n);
       ph[0] = vx; ph[1] = vy; ph[2] = vz;
@@ -457,8 +457,8 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
   for (int q = 0; q < 3; ++q) {
     g[q] = 0.;
     if (LIM != LIM_ORDER1 && inner) {
-      const double gfw = (ph_r[q] - ph[q]) / (x_r - x);
-      const double gbw = (ph[q] - ph_l[q]) / (x - x_l);
+      const double gfw = div_rn(ph_r[q] - ph[q], x_r - x);
+      const double gbw = div_rn(ph[q] - ph_l[q], x - x_l);
       g[q] = limited_gradient_t<LIM>(gbw, gfw);
     }
     g_l[q] = __shfl_up_sync(FULL, g[q], 1);
