@@ -1070,13 +1070,13 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   uint8_t nm = old;
   for (int q = 0; q < NE; ++q) {
     bool in = (old >> q) & 1;
-    if (((u[q] / Veul) < thr || (u[NE + q] == 0.)) && in) {
+    if ((div_rn(u[q], Veul) < thr || (u[NE + q] == 0.)) && in) {
       nm &= (uint8_t)~(1 << q);
-    } else if ((u[q] / Veul) > thr && !in) {
+    } else if (div_rn(u[q], Veul) > thr && !in) {
       double volt = 0.;
       for (int r = 0; r < NE; ++r) volt += u[r];
-      double vn = u[q] * Veul / volt;
-      if ((vn / Veul) > thr && u[NE + q] != 0.) nm |= (uint8_t)(1 << q);
+      double vn = div_rn(u[q] * Veul, volt);
+      if (div_rn(vn, Veul) > thr && u[NE + q] != 0.) nm |= (uint8_t)(1 << q);
     }
   }
   const bool oldpure = __popc(old) == 1;
@@ -1133,13 +1133,13 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   for (int q = 0; q < NE; ++q) {
     dens[q] = 0.;
     if (!((nm >> q) & 1)) continue;
-    if (EVF(q) > thr && vol[q] != 0.) dens[q] = u[NE + q] / vol[q];
+    if (EVF(q) > thr && vol[q] != 0.) dens[q] = div_rn(u[NE + q], vol[q]);
     dn += EVF(q) * dens[q];
   }
   for (int q = 0; q < NE; ++q) {
     ener[q] = 0.;
     if (!((nm >> q) & 1)) continue;
-    if (EVF(q) > thr && u[NE + q] != 0.) ener[q] = u[2 * NE + q] / u[NE + q];
+    if (EVF(q) > thr && u[NE + q] != 0.) ener[q] = div_rn(u[2 * NE + q], u[NE + q]);
   }
   // aliased stores: g* are the global slots, e*[] the env slots
   double rhog = dn;
@@ -1220,9 +1220,9 @@ __device__ __forceinline__ void body_remap_finalize_nodes(const Mesh& M, const F
   const long long NN = M.nnode;
   double m = Ud[3 * NN + n];
   if (m != 0.) {
-    F.vx[n] = Ud[n] / m;
-    F.vy[n] = Ud[NN + n] / m;
-    F.vz[n] = Ud[2 * NN + n] / m;
+    F.vx[n] = div_rn(Ud[n], m);
+    F.vy[n] = div_rn(Ud[NN + n], m);
+    F.vz[n] = div_rn(Ud[2 * NN + n], m);
   }
   int i, j, k;
   node_ijk(M, n, i, j, k);
