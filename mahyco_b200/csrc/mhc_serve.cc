@@ -16,7 +16,9 @@
 // large one's pace.  Each step gives every class the number of cycles that
 // takes about as long as the slowest class's `cycles` (estimated from the
 // launches and cells per cycle), and the classes' streams overlap on the
-// GPU.  Requests never change each other's arithmetic: each case's results
+// GPU.  A class advances a bounded number of cells at once (one large case,
+// about two large cases' worth of medium ones, any number of small ones):
+// cases that already fill the GPU gain nothing from sharing it.  Requests never change each other's arithmetic: each case's results
 // are the same alone and in any mix.
 //
 // Host-only C++ over the public batch API; no counterpart in the reference,
@@ -24,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <deque>
 #include <string>
@@ -37,6 +40,11 @@ namespace {
 constexpr int kClasses = 3;
 // class of a request by its cells: [0, 3e4), [3e4, 1e6), [1e6, inf)
 int size_class(long long cells) { return cells < 30000 ? 0 : (cells < 1000000 ? 1 : 2); }
+// cells a class may advance at once: one large case already fills the GPU,
+// so large cases run one after the other (sharing the GPU between them would
+// only delay each), medium ones share up to about two large ones' worth;
+// small cases are launch-bound and all run together
+const long long kClassCells[kClasses] = {LLONG_MAX, 2000000, 1};
 
 struct Request {
   long long ticket = 0;
@@ -154,6 +162,12 @@ void finish(mhc_server* s, Request& q, int state, int status, double t) {
 int admit(mhc_server* s) {
   int added = 0;
   bool touched[kClasses] = {false, false, false};
+  long long run_cells[kClasses] = {0, 0, 0};
+  int run_cases[kClasses] = {0, 0, 0};
+  for (long long tk : s->running) {
+    run_cells[s->reqs[tk].cls] += s->reqs[tk].cells;
+    run_cases[s->reqs[tk].cls] += 1;
+  }
   bool head_blocked = false;
   for (auto it = s->queue.begin(); it != s->queue.end();) {
     Request& q = s->reqs[*it];
@@ -161,6 +175,10 @@ int admit(mhc_server* s) {
     if (q.timeout_s > 0. && t - q.t_submit > q.timeout_s) {
       finish(s, q, MHC_REQ_FAILED, MHC_ST_TIMEOUT, t);
       it = s->queue.erase(it);
+      continue;
+    }
+    if (run_cases[q.cls] > 0 && run_cells[q.cls] + q.cells > kClassCells[q.cls]) {
+      ++it;  // its class is busy: wait, others may go ahead
       continue;
     }
     if (s->in_use + q.bytes > s->budget) {
@@ -195,6 +213,8 @@ int admit(mhc_server* s) {
     s->in_use += q.bytes;
     s->running.push_back(q.ticket);
     touched[q.cls] = true;
+    run_cells[q.cls] += q.cells;
+    run_cases[q.cls] += 1;
     it = s->queue.erase(it);
     ++added;
   }
