@@ -109,8 +109,14 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
 #define MHC_LAG_MIN_BLOCKS 1
 #endif
 
+// resident blocks per SM asked of the compiler for the node pass (a latency
+// bound gather: more warps in flight hide more of it)
+#ifndef MHC_NODES_MIN_BLOCKS
+#define MHC_NODES_MIN_BLOCKS 4
+#endif
+
 template <int DIM, bool EL, bool HG>
-__global__ void __launch_bounds__(CT) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
+__global__ void __launch_bounds__(CT, MHC_NODES_MIN_BLOCKS) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_NODES>(C, L, w_);
     Fields F = C[wi.c].F;
