@@ -233,8 +233,12 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
 }
 
 // remap finalize after K performed sweeps: cells read U[K&1], nodes Ud[(K-1)&1]
+#ifndef MHC_FIN_MIN_BLOCKS
+#define MHC_FIN_MIN_BLOCKS 3
+#endif
+
 template <int DIM, int NE>
-__global__ void __launch_bounds__(CT) kb_remap_finalize_cells(const CaseDesc* __restrict__ C, PhaseList L, int K) {
+__global__ void __launch_bounds__(CT, MHC_FIN_MIN_BLOCKS) kb_remap_finalize_cells(const CaseDesc* __restrict__ C, PhaseList L, int K) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
     Fields F = C[wi.c].F;
