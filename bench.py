@@ -304,12 +304,18 @@ def run_ours(args):
     g = mb.Hydro(p, lib)
     g.hydroStartInit()
     g.cycle(args.warmup)
+    # every step's status (time, deltat, iteration, flags) comes back to the
+    # host; the read of step k overlaps step k+1 on the GPU
+    prev = None
     for _ in range(args.steps):
         g.cycle(1)
-        sc = g.scalars()   # time, deltat, status flags: 40 bytes
-        d2h += 40
-        if sc["status"] & ~mb.ST_STOP:
+        slot = g.scalars_request()
+        d2h += 88
+        if prev is not None and g.scalars_wait(prev)["status"] & ~mb.ST_STOP:
             break
+        prev = slot
+    if prev is not None:
+        g.scalars_wait(prev)
     for f in ("Density", "Pressure", "InternalEnergy", "SoundSpeed"):
         d2h += g.field(f).nbytes
     d2h += g.field("Velocity").nbytes
@@ -348,7 +354,7 @@ def run_ours(args):
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": "cell-cycles/s",
                 "h2d_bytes_per_step": ctypes.sizeof(p) / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-                "timer": "host wall clock; includes case allocation, device init, per-iteration status read-back and final field download"},
+                "timer": "host wall clock; includes case allocation, device init, every iteration's status read-back (overlapping the next iteration) and the final field download"},
     }
     if world == 1 and not args.no_extras:
         # the batched and served forms against the plain form, on bounded

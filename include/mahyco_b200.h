@@ -130,6 +130,15 @@ int mhc_synchronize(mhc_case* h);
 
 /* time-loop scalars after the last completed iteration */
 int mhc_get_scalars(mhc_case* h, double* time, double* deltat, long long* iteration, int* status);
+/* asynchronous status read-back: mhc_scalars_request enqueues, after the
+ * work already on the case stream, a copy of the scalars into one of two
+ * pinned host slots and returns the slot (0 or 1, alternating);
+ * mhc_scalars_wait blocks until that copy has landed and returns its values
+ * (same meaning as mhc_get_scalars).  A time loop can enqueue iteration k+1,
+ * then wait for the scalars of iteration k, so the GPU never idles on the
+ * read-back. */
+int mhc_scalars_request(mhc_case* h);
+int mhc_scalars_wait(mhc_case* h, int slot, double* time, double* deltat, long long* iteration, int* status);
 
 /* Named fields (names of src/Mahyco.axl: Density, Pressure, InternalEnergy,
  * SoundSpeed, PseudoViscosity, CellMass, CellVolume, FracVol, MassFraction,

@@ -82,6 +82,9 @@ _SIGS = {
                                           C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "mhc_noalloc_last_error": (C.c_char_p, []),
     "mhc_batch_detach": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_scalars_request": (C.c_int, [C.c_void_p]),
+    "mhc_scalars_wait": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "mhc_case_checkpoint_bytes": (C.c_longlong, [C.c_void_p]),
     "mhc_case_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     "mhc_case_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
@@ -159,6 +162,17 @@ class Hydro:
     def launches(self) -> int:
         """Kernels this case has put on the GPU so far."""
         return int(self.lib.mhc_case_launches(self.h))
+
+    def scalars_request(self) -> int:
+        """Enqueue an asynchronous read-back of the scalars; returns its slot."""
+        return _check(self.lib, self.lib.mhc_scalars_request(self.h), "mhc_scalars_request")
+
+    def scalars_wait(self, slot: int) -> dict:
+        """Scalars of an earlier scalars_request, once the copy has landed."""
+        t, dt, it, st = C.c_double(), C.c_double(), C.c_longlong(), C.c_int()
+        _check(self.lib, self.lib.mhc_scalars_wait(self.h, int(slot), C.byref(t), C.byref(dt), C.byref(it),
+                                                   C.byref(st)), "mhc_scalars_wait")
+        return {"time": t.value, "deltat": dt.value, "iteration": it.value, "status": st.value}
 
     def checkpoint(self) -> bytes:
         """Whole device state between iterations (protection)."""

@@ -383,6 +383,9 @@ int validate(const mhc_case_params* p) {
 
 void case_free(mhc_case* h) {
   if (!h) return;
+  if (h->h_scal) { cudaStreamSynchronize(h->stream); cudaFreeHost(h->h_scal); h->h_scal = nullptr; }
+  for (int i = 0; i < 2; ++i)
+    if (h->scal_ev[i]) { cudaEventDestroy(h->scal_ev[i]); h->scal_ev[i] = nullptr; }
   if (h->solo) { engine_destroy(h->solo); h->solo = nullptr; }
   if (h->stream) {
     for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
@@ -394,10 +397,27 @@ void case_free(mhc_case* h) {
 
 // allocates the device state of one case on `stream` (stream-ordered pool);
 // a null stream gives the case a private stream
+// keep freed device memory in the stream-ordered pool of the current device
+// instead of returning it at every synchronisation: cases come and go
+// (serving, batches), and re-mapping their memory costs milliseconds
+void keep_pool_memory() {
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done[dev] = true;
+}
+
 int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** out) {
   *out = nullptr;
   int v = validate(params);
   if (v != MHC_OK) return v;
+  keep_pool_memory();
   mhc_case* h = new mhc_case();
   h->P = *params;
   h->DIM = params->dim;
@@ -854,6 +874,31 @@ int mhc_case_restore(mhc_case* h, const void* host, long long size) {
   int r = ckpt_restore(h, h->stream, host, size);
   if (r) return r;
   if (h->solo) h->solo->dirty = true;  // iteration-dependent work lists are rebuilt
+  return MHC_OK;
+}
+
+int mhc_scalars_request(mhc_case* h) {
+  if (!h) return set_err(MHC_ERR_ARG, "null case");
+  if (!h->h_scal) {
+    CK(cudaMallocHost((void**)&h->h_scal, 2 * sizeof(Scalars)));
+    for (int i = 0; i < 2; ++i) CK(cudaEventCreateWithFlags(&h->scal_ev[i], cudaEventDisableTiming));
+  }
+  const int slot = h->scal_next;
+  h->scal_next ^= 1;
+  CK(cudaEventSynchronize(h->scal_ev[slot]));  // the slot's previous copy has landed
+  CK(cudaMemcpyAsync(&h->h_scal[slot], h->d_scal, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaEventRecord(h->scal_ev[slot], h->stream));
+  return slot;
+}
+
+int mhc_scalars_wait(mhc_case* h, int slot, double* time, double* deltat, long long* iteration, int* status) {
+  if (!h || slot < 0 || slot > 1 || !h->h_scal) return set_err(MHC_ERR_ARG, "bad case or slot");
+  CK(cudaEventSynchronize(h->scal_ev[slot]));
+  const Scalars& s = h->h_scal[slot];
+  if (time) *time = s.t_done;
+  if (deltat) *deltat = s.dt;
+  if (iteration) *iteration = s.iteration_done;
+  if (status) *status = s.status;
   return MHC_OK;
 }
 

@@ -44,6 +44,10 @@ struct mhc_case {
   bool own_stream = false;
   std::vector<void*> allocs;
   std::vector<size_t> alloc_bytes;  // size of each allocation (checkpoints)
+  // asynchronous status read-back: two pinned slots and their events
+  Scalars* h_scal = nullptr;
+  cudaEvent_t scal_ev[2] = {nullptr, nullptr};
+  int scal_next = 0;
   long long it_host = 1;           // iteration the next launched cycle runs
   int stage = S_IDLE;
   bool initialised = false;

@@ -55,3 +55,21 @@ def test_restore_refuses_other_cases():
         a.restore(ck[:-8])
     a.close()
     c.close()
+
+
+def test_async_scalars_match_synchronous():
+    build, _ = PARITY_CASES["adi2d_sedov"]
+    h = mb.Hydro(build())
+    h.hydroStartInit()
+    seen = []
+    prev = None
+    for _ in range(6):
+        h.cycle(1)
+        slot = h.scalars_request()
+        if prev is not None:
+            seen.append(h.scalars_wait(prev))
+        prev = slot
+    seen.append(h.scalars_wait(prev))
+    assert [s["iteration"] for s in seen] == [1, 2, 3, 4, 5, 6]
+    assert seen[-1] == h.scalars()
+    h.close()
