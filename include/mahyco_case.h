@@ -43,8 +43,12 @@ enum mhc_surface {
   MHC_XMIN = 0, MHC_YMIN = 1, MHC_ZMIN = 2, MHC_XMAX = 3, MHC_YMAX = 4, MHC_ZMAX = 5
 };
 
-/* limiter ids of the classical remap path (TypesMahyco.h:96-105) */
-enum mhc_limiter { MHC_MINMOD = 0, MHC_SUPERBEE = 1, MHC_VANLEER = 2 };
+/* remap limiter ids (TypesMahyco.h:96-105): classical (0-2) and the
+ * generalised limiters of fluxLimiterG that use the cell widths (3-7) */
+enum mhc_limiter {
+  MHC_MINMOD = 0, MHC_SUPERBEE = 1, MHC_VANLEER = 2,
+  MHC_MINMOD_G = 3, MHC_SUPERBEE_G = 4, MHC_VANLEER_G = 5, MHC_ARITHMETIC_G = 6, MHC_ULTRABEE_G = 7
+};
 
 /* case-initialisation services (<cas-model name="...">) */
 enum mhc_case_model {
@@ -134,6 +138,7 @@ typedef struct mhc_case_params {
   /* EnvSummation period */
   int time_history_period;
   double coef_antiderive;   /* coef-antiderive: anti-hourglass velocity correction (Lagrange only) */
+  int projection_simple_pente; /* projection-simple-pente: single-slope bound of the generalised limiters */
 } mhc_case_params;
 
 #ifdef __cplusplus

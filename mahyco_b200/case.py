@@ -24,6 +24,7 @@ CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV}
 LENGTHS = {"racine-cubique-volume": 0, "faces-opposees": 1, "monodimX": 2,
            "monodimY": 3, "monodimZ": 4}
 MINMOD, SUPERBEE, VANLEER = 0, 1, 2
+MINMOD_G, SUPERBEE_G, VANLEER_G, ARITHMETIC_G, ULTRABEE_G = 3, 4, 5, 6, 7
 
 
 class EnvParams(C.Structure):
@@ -67,6 +68,7 @@ class CaseParams(C.Structure):
         ("is_euler_scheme", C.c_int), ("remap_threshold", C.c_double),
         ("time_history_period", C.c_int),
         ("coef_antiderive", C.c_double),
+        ("projection_simple_pente", C.c_int),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -246,11 +248,12 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         eul = _txt(rm, "is-euler-scheme", "Full", str)
         if eul != "Full":
             raise NotImplementedError("is-euler-scheme other than Full")
-        for flag in ("projection-pente-borne", "projection-simple-pente", "conservation-energie-totale"):
+        for flag in ("projection-pente-borne", "conservation-energie-totale"):
             if _txt(rm, flag, False, _bool):
                 raise NotImplementedError(flag)
-        if p.ordre_projection not in (1, 2) or p.projection_limiteur_id not in (0, 1, 2):
-            raise NotImplementedError("remap order 3 / generalised limiters")
+        p.projection_simple_pente = int(_txt(rm, "projection-simple-pente", False, _bool))
+        if p.ordre_projection not in (1, 2, 3) or not 0 <= p.projection_limiteur_id <= 7:
+            raise NotImplementedError("ordre-projection / projection-limiteur-id out of range")
     if _txt(m, "schema-csts", False, _bool):
         raise NotImplementedError("schema-csts")
     if _txt(m, "sans-lagrange", False, _bool):

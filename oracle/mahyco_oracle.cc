@@ -156,6 +156,8 @@ struct Case {
   std::vector<double> u_lag, phi_lag, grad_phi, grad_phi_face, phi_face, dual_phi_flux;
   std::vector<double> u_dual, phi_dual, dual_grad;
   std::vector<double> back_flux, front_flux;
+  std::vector<double> h_cell;          /* m_h_cell_lagrange of the current direction */
+  std::vector<int> est_mixte, est_pure; /* EstMixte / EstPure (Arcane default 0) */
   int sens_projection = 0;
   /* emulation of a protection/reprise restart (test pinning only): after
    * iteration restart_at the reference projects only 3*nb_env+5 variables
@@ -671,6 +673,9 @@ static void setup(Case& C, const mhc_case_params* p) {
   C.dual_grad = C.u_dual;
   C.back_flux.assign(C.nnode, 0.);
   C.front_flux.assign(C.nnode, 0.);
+  C.h_cell.assign(C.ncell, 0.);
+  C.est_mixte.assign(C.ncell, 0);
+  C.est_pure.assign(C.ncell, 0);
 }
 
 /* MahycoModule::hydroStartInit (MahycoModule.cc:21-210) followed by
@@ -1106,6 +1111,94 @@ static double limited_gradient(int id, double gb, double gf) {
   return g;
 }
 
+/* RemapADIService::fluxLimiterG (UtilesRemap.cc:130-190): slope limited
+ * with the widths of the three cells (ids 3..7), optionally clipped to the
+ * single-slope bound (projection-simple-pente) */
+static double generalized_gradient(int id, double gp, double gm, double y0, double yp, double ym,
+                                   double h0, double hp, double hm, bool simple_pente) {
+  (void)y0;
+  if (gp * gm < 0.0) return 0.;
+  double g = 0.;
+  const double dy = yp - ym;
+  if (id == MHC_MINMOD_G) {
+    const double a = std::min(std::fabs(gp), std::fabs(gm));
+    g = dy > 0. ? a : -a;
+  } else if (id == MHC_SUPERBEE_G) {
+    const double a = std::max(std::fabs(gp), std::fabs(gm));
+    g = dy > 0. ? a : -a;
+  } else if (id == MHC_VANLEER_G) {
+    const double lp = (h0 / 2. + hp) / (h0 + hp + hm);
+    const double lm = (h0 / 2. + hm) / (h0 + hp + hm);
+    const double den = lp * gp + lm * gm;
+    g = den != 0. ? gp * gm / den : 0.;
+  } else if (id == MHC_ULTRABEE_G) {
+    g = dy / h0;
+  } else if (id == MHC_ARITHMETIC_G) {
+    const double lp = (h0 / 2. + hp) / (h0 + hp + hm);
+    const double lm = (h0 / 2. + hm) / (h0 + hp + hm);
+    g = lm * gp + lp * gm;
+  }
+  if (simple_pente) {
+    const double mp = gp * (h0 + hp) / h0;
+    const double mm = gm * (h0 + hm) / h0;
+    const double M = std::min(std::fabs(mp), std::fabs(mm));
+    const double a = std::min(std::fabs(M), std::fabs(g));
+    g = dy > 0. ? a : -a;
+  }
+  return g;
+}
+
+/* third-order face value of the ADI remap (Remap-ordre-3.cc):
+ * evaluate_grad (16-27), evaluate_ystar (35-48), evaluate_fm / evaluate_fp
+ * (56-78), define_interval / intersection (86-112) and ComputeFluxOrdre3
+ * (127-188).  y[0..5] / h[0..5]: values and widths of the cells
+ * b-2, b-1, b, f, f+1, f+2 around the face (clamped at the line ends). */
+static double o3_grad(double hm, double h0, double hp, double ym, double y0, double yp) {
+  return h0 / (hm + h0 + hp) * ((2. * hm + h0) / (h0 + hp) * (yp - y0) + (h0 + 2. * hp) / (hm + h0) * (y0 - ym));
+}
+static double o3_ystar(double hmm, double hm, double hp, double hpp, double ymm, double ym, double yp, double ypp,
+                       double gm, double gp) {
+  const double a = (2. * hp * hm) / (hm + hp) * ((hmm + hm) / (2. * hm + hp) - (hpp + hp) / (2. * hp + hm)) * (yp - ym);
+  const double b = -hm * (hmm + hm) / (2. * hm + hp) * gp + hp * (hp + hpp) / (hm + 2. * hp) * gm;
+  return ym + hm / (hm + hp) * (yp - ym) + 1. / (hmm + hm + hp + hpp) * (a + b);
+}
+static double order3_face_value(const double* y, const double* h, double vdt) {
+  const double g0 = o3_grad(h[0], h[1], h[2], y[0], y[1], y[2]);
+  const double g1 = o3_grad(h[1], h[2], h[3], y[1], y[2], y[3]);
+  const double g2 = o3_grad(h[2], h[3], h[4], y[2], y[3], y[4]);
+  const double g3 = o3_grad(h[3], h[4], h[5], y[3], y[4], y[5]);
+  const double sm = o3_ystar(h[0], h[1], h[2], h[3], y[0], y[1], y[2], y[3], g0, g1);
+  const double s0 = o3_ystar(h[1], h[2], h[3], h[4], y[1], y[2], y[3], y[4], g1, g2);
+  const double sp = o3_ystar(h[2], h[3], h[4], h[5], y[2], y[3], y[4], y[5], g2, g3);
+  double v;
+  if (vdt > 0.) {
+    const double du = s0 - sm, u6 = 6. * (y[2] - 0.5 * (sm + s0));
+    v = s0 - 0.5 * vdt / h[2] * (du - (1. - 2. / 3. * vdt / h[2]) * u6);
+  } else if (vdt < 0.) {
+    const double du = sp - s0, u6 = 6. * (y[3] - 0.5 * (s0 + sp)), x = -vdt;
+    v = s0 + 0.5 * x / h[3] * (du - (1. - 2. / 3. * x / h[3]) * u6);
+  } else {
+    return 0.;
+  }
+  /* TVD bound: intersection of [y_b, y_f] with the upwind extrapolation */
+  const double num = vdt / h[2], nup = vdt / h[3];
+  const double ext_b = y[2] + (1. - num) / num * (y[2] - y[1]);
+  const double ext_f = y[3] - (1. + nup) / nup * (y[3] - y[4]);
+  const double i1a = amin(y[2], y[3]), i1b = amax(y[2], y[3]);
+  const double o = vdt >= 0. ? y[2] : y[3], x = vdt >= 0. ? ext_b : ext_f;
+  const double i2a = amin(o, x), i2b = amax(o, x);
+  double lo, hi;
+  if (i1b < i2a || i2b < i1a) {
+    lo = hi = 0.;
+  } else {
+    lo = amax(i1a, i2a);
+    hi = amin(i1b, i2b);
+  }
+  if (v < lo) v = lo;
+  if (v > hi) v = hi;
+  return v;
+}
+
 /* MahycoModule::computeVariablesForRemap (PrepareRemap.cc:94-193) */
 static void compute_variables_for_remap(Case& C) {
   const int ne = C.nenv, nv = C.nvars;
@@ -1175,10 +1268,13 @@ static void face_cells(const Case& C, int d, long f, long& cb, long& cf) {
   if (id < C.ncd(d)) cf = C.cid(i, j, k);
 }
 
-/* RemapADIService::computeGradPhiFace (RemapADIService.cc:119-149) */
+/* RemapADIService::computeGradPhiFace (RemapADIService.cc:119-149): face
+ * gradients and the cell widths along d (distances from the cell centre to
+ * the centres of its inner faces of direction d) */
 static void compute_grad_phi_face(Case& C, int d) {
   const int nv = C.nvars;
   C.grad_phi_face.assign(C.nface[d] * nv, 0.);
+  std::fill(C.h_cell.begin(), C.h_cell.end(), 0.);
   for (long f = 0; f < C.nface[d]; ++f) {
     long cb, cf;
     face_cells(C, d, f, cb, cf);
@@ -1186,7 +1282,19 @@ static void compute_grad_phi_face(Case& C, int d) {
     C.deltax[d][f] = dot((C.cell_coord[cf] - C.cell_coord[cb]), C.face_normal[d][f]);
     for (int iv = 0; iv < C.nproj(); ++iv)
       C.grad_phi_face[f * nv + iv] = (C.phi_lag[cf * nv + iv] - C.phi_lag[cb * nv + iv]) / C.deltax[d][f];
+    C.h_cell[cb] += norm(C.face_coord[d][f] - C.cell_coord[cb]);
+    C.h_cell[cf] += norm(C.face_coord[d][f] - C.cell_coord[cf]);
   }
+}
+
+/* neighbour of cell c at offset s (+-1) along d, or -1 outside the mesh */
+static long cell_step(const Case& C, long c, int d, int s) {
+  int i, j, k;
+  C.cijk(c, i, j, k);
+  int& id = d == 0 ? i : (d == 1 ? j : k);
+  id += s;
+  if (id < 0 || id >= C.ncd(d)) return -1;
+  return C.cid(i, j, k);
 }
 
 /* back / front face of cell c in direction d */
@@ -1197,33 +1305,90 @@ static void cell_dir_faces(const Case& C, long c, int d, long& fb, long& ff) {
   ff = (d == 0) ? C.fid(0, i + 1, j, k) : (d == 1 ? C.fid(1, i, j + 1, k) : C.fid(2, i, j, k + 1));
 }
 
-/* RemapADIService::computeGradPhiCell (RemapADIService.cc:161-267), classical limiter */
+/* RemapADIService::computeGradPhiCell (RemapADIService.cc:161-267) with
+ * computeAndLimitGradPhi (UtilesRemap.cc:325-357), without pente-borne */
 static void compute_grad_phi_cell(Case& C, int d) {
   const int nv = C.nvars;
+  const int lim = C.P.projection_limiteur_id;
   std::fill(C.grad_phi.begin(), C.grad_phi.end(), 0.);
   if (C.P.ordre_projection <= 1) return;
   for (long c = 0; c < C.ncell; ++c) {
     long fb, ff;
     cell_dir_faces(C, c, d, fb, ff);
-    for (int iv = 0; iv < C.nproj(); ++iv)
-      C.grad_phi[c * nv + iv] = limited_gradient(C.P.projection_limiteur_id, C.grad_phi_face[fb * nv + iv], C.grad_phi_face[ff * nv + iv]);
+    long cb = cell_step(C, c, d, -1), cf = cell_step(C, c, d, +1);
+    if (cb < 0) cb = c;
+    if (cf < 0) cf = c;
+    for (int iv = 0; iv < C.nproj(); ++iv) {
+      const double gb = C.grad_phi_face[fb * nv + iv], gf = C.grad_phi_face[ff * nv + iv];
+      C.grad_phi[c * nv + iv] = lim < MHC_MINMOD_G
+          ? limited_gradient(lim, gb, gf)
+          : generalized_gradient(lim, gf, gb, C.phi_lag[c * nv + iv], C.phi_lag[cf * nv + iv], C.phi_lag[cb * nv + iv],
+                                 C.h_cell[c], C.h_cell[cf], C.h_cell[cb], C.P.projection_simple_pente != 0);
+    }
   }
 }
 
-/* RemapADIService::computeUpwindFaceQuantitiesForProjection (279-383), order <= 2 */
+/* RemapADIService::computeUpwindFaceQuantitiesForProjection (279-383),
+ * without pente-borne: upwind value plus slope (order 1, 2) or the
+ * third-order face value with the mixed-neighbourhood correction */
 static void compute_upwind_face_quantities(Case& C, int d) {
-  const int nv = C.nvars;
+  const int nv = C.nvars, ne = C.nenv;
   C.phi_face.assign(C.nface[d] * nv, 0.);
   int order2 = C.P.ordre_projection - 1;
   for (long f = 0; f < C.nface[d]; ++f) {
     long cb, cf;
     face_cells(C, d, f, cb, cf);
     if (cb < 0 || cf < 0) continue;
-    long cu = (C.face_un[d][f] * C.deltax[d][f] > 0.0) ? cb : cf;
-    for (int iv = 0; iv < C.nproj(); ++iv)
-      C.phi_face[f * nv + iv] = C.phi_lag[cu * nv + iv] +
-          order2 * dot((C.face_coord[d][f] - C.cell_coord[cu]), C.face_normal[d][f]) * C.grad_phi[cu * nv + iv];
+    if (C.P.ordre_projection <= 2) {
+      long cu = (C.face_un[d][f] * C.deltax[d][f] > 0.0) ? cb : cf;
+      for (int iv = 0; iv < C.nproj(); ++iv)
+        C.phi_face[f * nv + iv] = C.phi_lag[cu * nv + iv] +
+            order2 * dot((C.face_coord[d][f] - C.cell_coord[cu]), C.face_normal[d][f]) * C.grad_phi[cu * nv + iv];
+      continue;
+    }
+    /* stencil b-2 .. f+2, repeated at the line ends */
+    long s[6];
+    s[2] = cb; s[3] = cf;
+    s[1] = cell_step(C, cb, d, -1);
+    if (s[1] < 0) { s[1] = s[0] = cb; }
+    else { s[0] = cell_step(C, s[1], d, -1); if (s[0] < 0) s[0] = s[1]; }
+    s[4] = cell_step(C, cf, d, +1);
+    if (s[4] < 0) { s[4] = s[5] = cf; }
+    else { s[5] = cell_step(C, s[4], d, +1); if (s[5] < 0) s[5] = s[4]; }
+    const double vdt = C.face_un[d][f] * C.dt;
+    double h[6], y[6];
+    for (int q = 0; q < 6; ++q) h[q] = C.h_cell[s[q]];
+    for (int iv = 0; iv < C.nproj(); ++iv) {
+      for (int q = 0; q < 6; ++q) y[q] = C.phi_lag[s[q] * nv + iv];
+      C.phi_face[f * nv + iv] = order3_face_value(y, h, vdt);
+    }
+    const bool pure_nb = C.est_mixte[cb] == 0 && C.est_mixte[cf] == 0 && C.est_pure[cb] == C.est_pure[cf];
+    if (pure_nb) continue;
+    /* masses from the volume flux and energies from the mass flux with the
+     * upwind cell's density and specific energy */
+    double* pf = &C.phi_face[f * nv];
+    for (int e = 0; e < ne; ++e) {
+      const double* pb = &C.phi_lag[cb * nv];
+      const double* pfr = &C.phi_lag[cf * nv];
+      if (vdt > 0. && pb[e] != 0. && pb[ne + e] != 0.) {
+        pf[ne + e] = (pb[ne + e] / pb[e]) * pf[e];
+        pf[2 * ne + e] = (pb[2 * ne + e] / pb[ne + e]) * pf[ne + e];
+      } else if (vdt < 0. && pfr[e] != 0. && pfr[ne + e] != 0.) {
+        pf[ne + e] = (pfr[ne + e] / pfr[e]) * pf[e];
+        pf[2 * ne + e] = (pfr[2 * ne + e] / pfr[ne + e]) * pf[ne + e];
+      }
+    }
   }
+}
+
+/* mixed / pure indicator of a cell from its volume fractions
+ * (RemapADIService.cc:558-573, RemapADIFinal.cc:131-145) */
+static void set_cell_purity(Case& C, long c, const double* frac, const bool* present) {
+  int count = 0, last = -1;
+  for (int e = 0; e < C.nenv; ++e)
+    if (present[e] && frac[e] > 0.) { ++count; last = e; }
+  if (count > 1) { C.est_mixte[c] = 1; C.est_pure[c] = -1; }
+  else { C.est_mixte[c] = 0; C.est_pure[c] = last; }
 }
 
 /* RemapADIService::computeUremap (RemapADIService.cc:395-575), classical path */
@@ -1258,6 +1423,9 @@ static void compute_uremap(Case& C, int d) {
     double sv = 0.;
     for (int e = 0; e < ne; ++e) sv += u[e];
     for (int iv = 0; iv < C.nproj(); ++iv) C.phi_lag[c * nv + iv] = u[iv] / sv;
+    bool all[MHC_MAX_ENV];
+    for (int e = 0; e < ne; ++e) all[e] = true;
+    set_cell_purity(C, c, &C.phi_lag[c * nv], all);
   }
 }
 
@@ -1286,10 +1454,27 @@ static void compute_dual_uremap(Case& C, int d) {
     for (long n = 0; n < C.nnode; ++n) {
       if (!inner(n)) continue;
       long nb = step(n, -1), nf = step(n, +1);
+      /* dual cell widths (UtilesRemap.cc:51-63); a missing second
+       * neighbour gives a zero width */
+      const long nbb = step(nb, -1), nff = step(nf, +1);
+      const double h0 = 0.5 * (ncoord(nf) - ncoord(nb));
+      double hm = 0., hp = 0.;
+      if (nbb < 0) {
+        if (nff >= 0) hp = 0.5 * (ncoord(nff) - ncoord(n));
+      } else if (nff < 0) {
+        hm = 0.5 * (ncoord(n) - ncoord(nbb));
+      } else {
+        hm = 0.5 * (ncoord(n) - ncoord(nbb));
+        hp = 0.5 * (ncoord(nff) - ncoord(n));
+      }
+      const int lim = C.P.projection_limiteur_id;
       for (int iv = 0; iv < 3; ++iv) {
         double gf = (C.phi_dual[nf * 5 + iv] - C.phi_dual[n * 5 + iv]) / (ncoord(nf) - ncoord(n));
         double gb = (C.phi_dual[n * 5 + iv] - C.phi_dual[nb * 5 + iv]) / (ncoord(n) - ncoord(nb));
-        C.dual_grad[n * 5 + iv] = limited_gradient(C.P.projection_limiteur_id, gb, gf);
+        C.dual_grad[n * 5 + iv] = lim < MHC_MINMOD_G
+            ? limited_gradient(lim, gb, gf)
+            : generalized_gradient(lim, gf, gb, C.phi_dual[n * 5 + iv], C.phi_dual[nf * 5 + iv],
+                                   C.phi_dual[nb * 5 + iv], h0, hp, hm, C.P.projection_simple_pente != 0);
       }
     }
   }
@@ -1420,6 +1605,15 @@ static int remap_variables(Case& C) {
     if (somme_frac != 0.) unsursf = 1. / somme_frac;
     for (int e = 0; e < ne; ++e)
       if (C.has(c, e)) C.EV(C.fracvol, e, c) *= unsursf;
+    {
+      double fr[MHC_MAX_ENV];
+      bool pres[MHC_MAX_ENV];
+      for (int e = 0; e < ne; ++e) {
+        pres[e] = C.has(c, e);
+        fr[e] = pres[e] ? C.EV(C.fracvol, e, c) : 0.;
+      }
+      set_cell_purity(C, c, fr, pres);
+    }
     if (masset > thr * thr) {
       double unsurm = 1. / masset, fm = 0.;
       for (int e = 0; e < ne; ++e) {

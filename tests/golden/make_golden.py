@@ -31,6 +31,14 @@ CASES = {
     "CAS_2D_Sedov": {},
     # run on 8 MPI ranks by the reference (src/CMakeLists.txt:193-208)
     "CAS_Sedov": {"mpi_ranks": 8},
+    # third-order remap, run on 4 MPI ranks with 3 ghost layers
+    # (src/CMakeLists.txt:164-189)
+    "CAS_SodCaseX_ordre_3": {"mpi_ranks": 4},
+    "CAS_SodCaseY_ordre_3": {"mpi_ranks": 4},
+    "CAS_SodCaseZ_ordre_3": {"mpi_ranks": 4},
+    "CAS_BiSodCaseX_ordre_3": {"mpi_ranks": 4},
+    "CAS_BiSodCaseY_ordre_3": {"mpi_ranks": 4},
+    "CAS_BiSodCaseZ_ordre_3": {"mpi_ranks": 4},
 }
 VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
 

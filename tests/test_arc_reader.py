@@ -73,3 +73,23 @@ def test_anti_hourglass_and_elasto_options(tmp_path):
     f3.write_text(src[:i] + el.replace("DefaultModel", "NewHypoModel") + src[i:])
     with pytest.raises(NotImplementedError):
         read_arc(str(f3))
+
+
+def test_remap_order_and_generalised_limiter_options(tmp_path):
+    """ordre-projection 3, the generalised limiters (ids 3-7) and
+    projection-simple-pente are read; pente-borne is refused."""
+    text = open(ARC).read().replace("<ordre-projection>2</ordre-projection>",
+                                    "<ordre-projection>3</ordre-projection>").replace(
+        "<projection-limiteur-id>1</projection-limiteur-id>",
+        "<projection-limiteur-id>5</projection-limiteur-id>"
+        "<projection-simple-pente>true</projection-simple-pente>")
+    assert text != open(ARC).read()
+    f = tmp_path / "o3.arc"
+    f.write_text(text)
+    p, _ = read_arc(str(f))
+    assert (p.ordre_projection, p.projection_limiteur_id, p.projection_simple_pente) == (3, 5, 1)
+    g = tmp_path / "pb.arc"
+    g.write_text(text.replace("<ordre-projection>3</ordre-projection>",
+                              "<projection-pente-borne>true</projection-pente-borne>"))
+    with pytest.raises(NotImplementedError):
+        read_arc(str(g))

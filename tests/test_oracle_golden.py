@@ -4,8 +4,9 @@ tests/golden/<case>.json holds the parameters parsed from the case's
 Donnees.arc and the EnvSummation curves the reference wrote
 (NONREGRESSION/<case>/output/courbes/gnuplot), made by make_golden.py.
 Sequential runs agree to ~1e-14 (the residue is the summation order of the
-per-environment averages); the 8-rank CAS_Sedov reference run sums its
-averages per rank, hence the looser bound.
+per-environment averages); the multi-rank reference runs (CAS_Sedov on 8
+ranks, the third-order cases on 4) sum their averages per rank and their
+node sums in per-rank order, hence the looser bounds.
 """
 import glob
 import json
@@ -37,7 +38,9 @@ def run_oracle(g, cr_pow=False):
 @pytest.mark.parametrize("cr_pow", [False, True], ids=["glibc_pow", "cr_pow"])
 def test_oracle_matches_reference_goldens(path, cr_pow):
     g = json.load(open(path))
-    tol = 5e-12 if g["extra"].get("mpi_ranks", 1) > 1 else 1e-13
+    multi = g["extra"].get("mpi_ranks", 1) > 1
+    tol = 5e-12 if multi else 1e-13
+    ttol = 1e-13 if multi else 1e-14  # the time: a sum of deltat, per-rank orders move it by ulps
     p, th = run_oracle(g, cr_pow)
     for e, env in enumerate(g["env_names"]):
         for q, var in enumerate(VARS):
@@ -47,6 +50,6 @@ def test_oracle_matches_reference_goldens(path, cr_pow):
             ref = np.array(g["time_history"][key])
             assert len(th) >= len(ref), (key, len(th), len(ref))
             ours = th[: len(ref)]
-            np.testing.assert_allclose(ours[:, 0], ref[:, 0], rtol=1e-14, atol=0)
+            np.testing.assert_allclose(ours[:, 0], ref[:, 0], rtol=ttol, atol=0)
             rel = np.abs(ours[:, 1 + 5 * e + q] - ref[:, 1]) / np.abs(ref[:, 1])
             assert rel.max() <= tol, (key, rel.max(), int(rel.argmax()))
