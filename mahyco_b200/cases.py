@@ -15,9 +15,10 @@ from __future__ import annotations
 import math
 import random
 
-from .case import (CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, EOS_MIE_GRUNEISEN, EOS_PERFECT_GAS,
-                   EOS_STIFFENED_GAS, MINMOD, SUPERBEE, VANLEER, CaseParams, default_params,
-                   env_defaults, symmetry_bcs)
+from .case import (ARITHMETIC_G, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, EOS_MIE_GRUNEISEN,
+                   EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
+                   ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, default_params, env_defaults,
+                   symmetry_bcs)
 
 
 def _mesh(p: CaseParams, dim: int, n, L) -> None:
@@ -248,7 +249,36 @@ PARITY_CASES = {
                                              deltat_max=1e-3, deltat_init=1e-4)), 120),
     "adi3d_bisod_newton": (lambda: _newton(sod(dim=3, n=(24, 4, 4), L=(1.0, 0.2, 0.2), bi=True,
                                                limiter=SUPERBEE, deltat_init=1e-3)), 50),
+    # third-order remap (Remap-ordre-3.cc) and the generalised limiters
+    # (fluxLimiterG) on the cell and node sweeps
+    "adi3d_bisod_order3": (lambda: sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True, order=3,
+                                       deltat_init=1e-3), 60),
+    "adi2d_bisod_y_order3_superbee": (lambda: sod(dim=2, n=(5, 40), L=(0.1, 1.0), bi=True, axis=1, order=3,
+                                                  limiter=SUPERBEE, deltat_init=1e-3), 60),
+    "adi2d_sedov_order3": (lambda: _order3(sedov(dim=2, n=(24, 24), deltat_init=1e-4)), 100),
+    "adi3d_sedov_order3_vanleerG": (lambda: _order3(sedov(dim=3, n=(12, 12, 12), limiter=VANLEER_G,
+                                                          deltat_init=1e-4)), 30),
+    "adi2d_two_state_minmodG": (lambda: two_state(dim=2, n=(40, 30), left=(1.7, 1.3), right=(0.2, 0.07),
+                                                  interface=0.41, limiter=MINMOD_G, deltat_init=1e-3), 80),
+    "adi3d_bisod_superbeeG": (lambda: sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True,
+                                          limiter=SUPERBEE_G, deltat_init=1e-3), 60),
+    "adi2d_sedov_vanleerG_simple_pente": (lambda: _simple_pente(sedov(dim=2, n=(24, 24), limiter=VANLEER_G,
+                                                                      deltat_init=1e-4)), 100),
+    "adi2d_bisod_arithmeticG": (lambda: sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True, limiter=ARITHMETIC_G,
+                                            deltat_init=1e-3), 80),
+    "adi3d_bisod_z_ultrabeeG": (lambda: sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
+                                            limiter=ULTRABEE_G, deltat_init=1e-3), 60),
 }
+
+
+def _order3(p: CaseParams) -> CaseParams:
+    p.ordre_projection = 3
+    return p
+
+
+def _simple_pente(p: CaseParams) -> CaseParams:
+    p.projection_simple_pente = 1
+    return p
 
 
 def _rot2(p: CaseParams) -> CaseParams:

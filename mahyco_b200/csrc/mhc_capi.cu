@@ -60,20 +60,20 @@ int engine_rebuild(Engine* e) {
   }
   if (nc) CK(cudaMemcpyAsync(e->d_desc, desc.data(), nc * sizeof(CaseDesc), cudaMemcpyHostToDevice, e->stream));
   // groups
-  std::map<std::tuple<int, int, int, int, int, int, int, int>, int> gidx;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
     int euler = h->P.with_projection ? 1 : 0;
     int sens = (int)((h->it_host - 1) % h->DIM);
     const int el = case_elasto(h) ? 1 : 0, hg = case_hourglass(h) ? 1 : 0;
-    const int lim = h->P.ordre_projection == 1 ? LIM_ORDER1 : h->P.projection_limiteur_id;
-    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim);
+    const int lim = node_sweep_mode(h->P), clim = cell_sweep_mode(h->P);
+    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim);
     auto it = gidx.find(key);
     if (it == gidx.end()) {
       Group g;
       g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
-      g.EL = el; g.HG = hg; g.LIM = lim;
+      g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim;
       gidx[key] = (int)e->groups.size();
       e->groups.push_back(g);
       it = gidx.find(key);
@@ -105,7 +105,8 @@ int engine_rebuild(Engine* e) {
     bool ok = phase(g.init_cells, PH_CELLS) && phase(g.init_nodes, PH_NODES) && phase(g.lag_cells, PH_CELLS) &&
               phase(g.fin_cells, PH_CELLS) && phase(g.fin_nodes, PH_NODES) && phase(g.dt, PH_CELLS) &&
               phase(g.lag_nodes, PH_NODES);
-    for (int D = 0; D < g.DIM; ++D) ok = ok && phase(g.sw_cells[D], PH_SWC0 + D) && phase(g.sw_nodes[D], PH_SWN0 + D);
+    const int phc = g.CLIM == LIM_O3 ? PH_SWCW0 : PH_SWC0, phn = g.LIM == LIM_GEN ? PH_SWNW0 : PH_SWN0;
+    for (int D = 0; D < g.DIM; ++D) ok = ok && phase(g.sw_cells[D], phc + D) && phase(g.sw_nodes[D], phn + D);
     if (!ok) return set_err(MHC_ERR_ARG, "more than 2^31 blocks in one phase of a batch");
   }
   if (ints.size() > e->ints_cap) {
@@ -357,10 +358,10 @@ int validate(const mhc_case_params* p) {
   if ((long long)(p->nx + 1) * (p->ny + 1) * (p->dim == 3 ? p->nz + 1 : 1) > INT_MAX)
     return set_err(MHC_ERR_ARG, "a case holds at most 2^31 - 1 nodes");
   if (p->nb_bc < 0 || p->nb_bc > MHC_MAX_BC) return set_err(MHC_ERR_ARG, "nb_bc");
-  if (p->ordre_projection < 1 || p->ordre_projection > 2)
-    return set_err(MHC_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");
-  if (p->projection_limiteur_id < 0 || p->projection_limiteur_id > 2)
-    return set_err(MHC_ERR_UNSUPPORTED, "only the classical limiters (0 minmod, 1 superbee, 2 vanleer)");
+  if (p->ordre_projection < 1 || p->ordre_projection > 3)
+    return set_err(MHC_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
+  if (p->projection_limiteur_id < 0 || p->projection_limiteur_id > 7)
+    return set_err(MHC_ERR_UNSUPPORTED, "projection-limiteur-id must be 0..7 (TypesMahyco.h limiteur)");
   if (p->is_euler_scheme != MHC_EULER_FULL) return set_err(MHC_ERR_UNSUPPORTED, "is-euler-scheme must be Full");
   for (int e = 0; e < p->nb_env; ++e) {
     const mhc_env_params& o = p->env[e];

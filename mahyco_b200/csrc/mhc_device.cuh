@@ -201,8 +201,48 @@ __device__ __forceinline__ double div_rn(double x, double y) {
   return x / y;
 }
 
-// limiter id as a template argument (LIM_ORDER1: first-order remap, no slope)
+// limiter id as a template argument: 0-2 the classical limiters (one
+// instance each), LIM_ORDER1 a first-order remap (no slope), LIM_GEN the
+// generalised limiters 3-7 (id read at run time), LIM_O3 the third-order
+// face values of the cell sweep
 constexpr int LIM_ORDER1 = 3;
+constexpr int LIM_GEN = 4;
+constexpr int LIM_O3 = 5;
+
+// RemapADIService::fluxLimiterG (UtilesRemap.cc:130-190): limited slope from
+// the back / front gradients gm / gp, the values ym, yp of the neighbours
+// and the widths hm, h0, hp of three consecutive cells (or dual cells)
+__device__ __forceinline__ double generalized_gradient(int id, double gp, double gm, double yp, double ym,
+                                                      double h0, double hp, double hm, int simple_pente) {
+  if (gp * gm < 0.0) return 0.;
+  const double dy = yp - ym;
+  double g = 0.;
+  if (id == 3) {
+    const double a = smin(fabs(gp), fabs(gm));
+    g = dy > 0. ? a : -a;
+  } else if (id == 4) {
+    const double a = smax(fabs(gp), fabs(gm));
+    g = dy > 0. ? a : -a;
+  } else if (id == 5) {
+    const double lp = (h0 / 2. + hp) / (h0 + hp + hm);
+    const double lm = (h0 / 2. + hm) / (h0 + hp + hm);
+    const double den = lp * gp + lm * gm;
+    g = den != 0. ? gp * gm / den : 0.;
+  } else if (id == 7) {
+    g = dy / h0;
+  } else if (id == 6) {
+    const double lp = (h0 / 2. + hp) / (h0 + hp + hm);
+    const double lm = (h0 / 2. + hm) / (h0 + hp + hm);
+    g = lm * gp + lp * gm;
+  }
+  if (simple_pente) {
+    const double mp = gp * (h0 + hp) / h0;
+    const double mm = gm * (h0 + hm) / h0;
+    const double a = smin(fabs(smin(fabs(mp), fabs(mm))), fabs(g));
+    g = dy > 0. ? a : -a;
+  }
+  return g;
+}
 template <int LIM>
 __device__ __forceinline__ double flux_limiter_t(double r) {
   if (LIM == 0) return smax(0.0, smin(1.0, r));

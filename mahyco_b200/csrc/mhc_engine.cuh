@@ -68,7 +68,8 @@ struct DevList {
 struct Group {
   int DIM, NE, EULER, skip;
   int EL = 0, HG = 0;          // elasto-plastic model; anti-hourglass correction
-  int LIM = 0;                 // remap slope limiter id, or LIM_ORDER1 for a first-order remap
+  int LIM = 0;                 // node-sweep instance: limiter 0-2, LIM_ORDER1 or LIM_GEN
+  int CLIM = 0;                // cell-sweep instance: the same, or LIM_O3 for a third-order remap
   long long it0;               // iteration of the members when the lists were built
   std::vector<int> members;
   DevList init_cells, init_nodes, lag_nodes, lag_cells, fin_cells, fin_nodes, dt;
@@ -130,6 +131,16 @@ struct StageTimer {
     e->stage_launches[stage] += 1;
   }
 };
+
+// sweep instances of a case (the template argument LIM of kb_sweep_nodes /
+// kb_sweep_cells)
+inline int node_sweep_mode(const mhc_case_params& P) {
+  if (P.ordre_projection == 1) return LIM_ORDER1;
+  return P.projection_limiteur_id >= MHC_MINMOD_G ? LIM_GEN : P.projection_limiteur_id;
+}
+inline int cell_sweep_mode(const mhc_case_params& P) {
+  return P.ordre_projection == 3 ? LIM_O3 : node_sweep_mode(P);
+}
 
 inline int skip_mask(const mhc_case* h) {
   int m = 0;

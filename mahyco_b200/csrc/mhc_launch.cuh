@@ -30,7 +30,9 @@ enum PhaseKind {
   PH_NODES = 1,      // one block per CT nodes
   PH_UNUSED = 2,
   PH_SWC0 = 3,       // cell sweep along D = PH - PH_SWC0
-  PH_SWN0 = 6        // node sweep along D = PH - PH_SWN0
+  PH_SWN0 = 6,       // node sweep along D = PH - PH_SWN0
+  PH_SWCW0 = 9,      // cell sweep with the wide (third-order) stencil
+  PH_SWNW0 = 12      // node sweep with the wide (generalised limiter) stencil
 };
 
 __host__ __device__ inline int cdiv_i(long long a, int b) { return (int)((a + b - 1) / b); }
@@ -42,10 +44,12 @@ __host__ __device__ inline void phase_grid(int ph, const Mesh& M, int& gx, int& 
   if (ph == PH_CELLS) { gx = cdiv_i(M.ncell, CT); return; }
   if (ph == PH_NODES) { gx = cdiv_i(M.nnode, CT); return; }
   // lane layout of mhc_sweep.cuh (sweep_lane)
-  const bool nodes = ph >= PH_SWN0;
-  const int D = nodes ? ph - PH_SWN0 : ph - PH_SWC0;
+  const bool wide = ph >= PH_SWCW0;
+  const int base = wide ? (ph >= PH_SWNW0 ? PH_SWNW0 : PH_SWCW0) : (ph >= PH_SWN0 ? PH_SWN0 : PH_SWC0);
+  const bool nodes = base == PH_SWN0 || base == PH_SWNW0;
+  const int D = ph - base;
   const int nx = nodes ? M.nnx : M.ncx, ny = nodes ? M.nny : M.ncy, nz = nodes ? M.nnz : M.ncz;
-  const int out = nodes ? NOUT : XOUT;
+  const int out = wide ? (nodes ? NOUT_W : XOUT_W) : (nodes ? NOUT : XOUT);
   if (D == 0) {
     gx = cdiv_i(cdiv_i((long long)nx * ny * nz, out), SW_ROWS);
   } else {
@@ -179,11 +183,13 @@ __global__ void __launch_bounds__(CT) kb_hourglass(const CaseDesc* __restrict__ 
 #define MHC_SW_MIN_BLOCKS_NODES 8
 #endif
 
+// the generalised-limiter and third-order instances hold more state per
+// lane and are asked for fewer resident blocks
 template <int DIM, int NE, int D, int LIM>
-__global__ void __launch_bounds__(SW_THREADS, MHC_SW_MIN_BLOCKS_CELLS)
+__global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_GEN ? 2 : MHC_SW_MIN_BLOCKS_CELLS)
 kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
-    const WorkItem wi = item_at<PH_SWC0 + D>(C, L, w_);
+    const WorkItem wi = item_at<(LIM == LIM_O3 ? PH_SWCW0 : PH_SWC0) + D>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -194,16 +200,20 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     A.first = k == 0;
     A.order = P.ordre_projection;
     A.limiter = P.projection_limiteur_id;
+    A.simple_pente = P.projection_simple_pente;
+    // EstMixte / EstPure are zero before the first remap of the run
+    A.first_remap = k == 0 && F.s->iteration == 1;
     const Mesh M = C[wi.c].M;
-    body_sweep_cells_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
+    if constexpr (LIM == LIM_O3) body_sweep_cells_o3<DIM, NE, D>(M, F, A, wi.x, wi.y);
+    else body_sweep_cells_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
   }
 }
 
 template <int DIM, int NE, int D, int LIM>
-__global__ void __launch_bounds__(SW_THREADS, MHC_SW_MIN_BLOCKS_NODES)
+__global__ void __launch_bounds__(SW_THREADS, LIM == LIM_GEN ? 4 : MHC_SW_MIN_BLOCKS_NODES)
 kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
-    const WorkItem wi = item_at<PH_SWN0 + D>(C, L, w_);
+    const WorkItem wi = item_at<(LIM == LIM_GEN ? PH_SWNW0 : PH_SWN0) + D>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -227,6 +237,7 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     A.Uout = (k & 1) ? F.Ud[1] : F.Ud[0];
     A.order = P.ordre_projection;
     A.limiter = P.projection_limiteur_id;
+    A.simple_pente = P.projection_simple_pente;
     A.done_dirs = done;
     body_sweep_nodes_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
   }

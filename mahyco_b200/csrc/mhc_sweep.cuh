@@ -25,6 +25,8 @@ struct SweepArgs {
   int first;
   int order;
   int limiter;
+  int simple_pente;   // projection-simple-pente (generalised limiters)
+  int first_remap;    // first remap of the run: every cell counts as pure
 };
 
 // face node q (in the order of the reference face, smallest node id first)
@@ -50,6 +52,7 @@ constexpr int SW_LANES = 32; // cells along D per warp
 constexpr int SW_ROWS = MHC_SW_ROWS;  // warps (transverse rows) per block
 constexpr int SW_THREADS = SW_LANES * SW_ROWS;
 constexpr int XOUT = 27;     // cells written per warp (lanes 2 .. 28)
+constexpr int XOUT_W = 26;   // wide stencils (3 halo lanes each side): lanes 3 .. 28
 
 // ---------------------------------------------------------------------------
 // Initial-grid quantities of the outer normals, one coordinate at a time.
@@ -186,9 +189,10 @@ __device__ __forceinline__ double centre_from_planes(const Plane<DIM>& B, const 
 // Lane layout of a sweep along D over an nx x ny x nz array of cells or
 // nodes.  The array is cut into lines along D; consecutive lines are
 // concatenated so that every warp window holds `out` written elements plus
-// two halo elements on each side, whatever the line length.
+// `hl` halo elements before them (2, or 3 for the wide stencils) and the
+// rest after them, whatever the line length.
 //  * D = 0: lines are consecutive in memory; window w = vbx * SW_ROWS + row
-//    covers flat positions [w*out - 2, w*out + 30).
+//    covers flat positions [w*out - hl, w*out - hl + 32).
 //  * D = 1, 2: warp `row` of the block owns x column ta = vbx * SW_ROWS +
 //    row and walks the lines of that column (slow transverse index tb, then
 //    p along D) in windows vby; the 4 warps of a block hold neighbouring x
@@ -200,11 +204,11 @@ __device__ __forceinline__ double centre_from_planes(const Plane<DIM>& B, const 
 // (ta, tb) the transverse indices in increasing axis order.
 // ---------------------------------------------------------------------------
 template <int D>
-__device__ __forceinline__ bool sweep_lane(int nx, int ny, int nz, int out, int vbx, int vby, int lane, int row,
-                                           int& i, int& j, int& k, int& p, int& ta, int& tb) {
+__device__ __forceinline__ bool sweep_lane(int nx, int ny, int nz, int out, int hl, int vbx, int vby, int lane,
+                                           int row, int& i, int& j, int& k, int& p, int& ta, int& tb) {
   i = j = k = p = ta = tb = 0;
   if (D == 0) {
-    const long long g = ((long long)vbx * SW_ROWS + row) * out - 2 + lane;
+    const long long g = ((long long)vbx * SW_ROWS + row) * out - hl + lane;
     if (g < 0 || g >= (long long)nx * ny * nz) return false;
     i = (int)(g % nx);
     const long long r = g / nx;
@@ -215,7 +219,7 @@ __device__ __forceinline__ bool sweep_lane(int nx, int ny, int nz, int out, int 
   }
   const int nd = D == 1 ? ny : nz, nb = D == 1 ? nz : ny;
   ta = vbx * SW_ROWS + row;
-  const long long g = (long long)vby * out - 2 + lane;
+  const long long g = (long long)vby * out - hl + lane;
   if (ta >= nx || g < 0 || g >= (long long)nb * nd) return false;
   tb = (int)(g / nd);
   p = (int)(g % nd);
@@ -227,10 +231,10 @@ __device__ __forceinline__ bool sweep_lane(int nx, int ny, int nz, int out, int 
 
 // the whole warp holds nothing (warp-uniform test, before any shuffle)
 template <int D>
-__device__ __forceinline__ bool sweep_warp_empty(int nx, int ny, int nz, int out, int vbx, int vby, int row) {
-  if (D == 0) return ((long long)vbx * SW_ROWS + row) * out - 2 >= (long long)nx * ny * nz;
+__device__ __forceinline__ bool sweep_warp_empty(int nx, int ny, int nz, int out, int hl, int vbx, int vby, int row) {
+  if (D == 0) return ((long long)vbx * SW_ROWS + row) * out - hl >= (long long)nx * ny * nz;
   const int nd = D == 1 ? ny : nz, nb = D == 1 ? nz : ny;
-  return vbx * SW_ROWS + row >= nx || (long long)vby * out - 2 >= (long long)nb * nd;
+  return vbx * SW_ROWS + row >= nx || (long long)vby * out - hl >= (long long)nb * nd;
 }
 
 // D coordinates of the face nodes of the node plane whose lowest node is
@@ -243,6 +247,73 @@ __device__ __forceinline__ void load_plane_xd(const Mesh& M, const Fields& F, in
     face_node_ijk2<DIM, D>(i, j, k, q, a, b, cz);
     P.xd[q] = __ldg(F.Xn[D] + node_id(M, a, b, cz));
   }
+}
+
+// all coordinates of the face nodes of the node plane whose lowest node is
+// (i, j, k); z = 0 in 2D
+template <int DIM, int D>
+__device__ __forceinline__ void load_plane_full(const Mesh& M, const Fields& F, int i, int j, int k,
+                                                double (&x)[DIM == 3 ? 4 : 2][3]) {
+#pragma unroll
+  for (int q = 0; q < (DIM == 3 ? 4 : 2); ++q) {
+    int a, b, cz;
+    face_node_ijk2<DIM, D>(i, j, k, q, a, b, cz);
+    const long long n = node_id(M, a, b, cz);
+    x[q][0] = __ldg(F.Xn[0] + n);
+    x[q][1] = __ldg(F.Xn[1] + n);
+    x[q][2] = DIM == 3 ? __ldg(F.Xn[2] + n) : 0.;
+  }
+}
+
+__device__ __forceinline__ double norm3(double a, double b, double c) { return sqrt(a * a + b * b + c * c); }
+
+// Width of the lane's cell along D (m_h_cell_lagrange,
+// RemapADIService.cc:141-143): distance from the Lagrangian cell centre to
+// the centres of its inner faces of direction D, back face first.  Every
+// lane of the warp calls it (the front plane comes from lane + 1).
+template <int DIM, int D>
+__device__ __forceinline__ double lane_cell_width(const Mesh& M, const Fields& F, bool ok, int i, int j, int k,
+                                                  int p, int nd) {
+  constexpr int NQ = DIM == 3 ? 4 : 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  double b[NQ][3], f[NQ][3];
+  if (ok) load_plane_full<DIM, D>(M, F, i, j, k, b);
+  else {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) b[q][0] = b[q][1] = b[q][2] = 0.;
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) f[q][a] = __shfl_down_sync(FULL, b[q][a], 1);
+  // the front plane is loaded at the end of a line, and by the last lane,
+  // whose next cell lies outside the warp
+  if (ok && (p == nd - 1 || (threadIdx.x % SW_LANES) == SW_LANES - 1))
+    load_plane_full<DIM, D>(M, F, D == 0 ? i + 1 : i, D == 1 ? j + 1 : j, D == 2 ? k + 1 : k, f);
+  if (!ok) return 0.;
+  const double wf = DIM == 2 ? .5 : .25, wc = DIM == 2 ? .25 : .125;
+  double cc[3], fb[3], ff[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double s = 0.;
+#pragma unroll
+    for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+      int q, front;
+      local_to_plane<DIM, D>(l, q, front);
+      s += front ? f[q][a] : b[q][a];
+    }
+    cc[a] = wc * s;
+    fb[a] = ff[a] = 0.;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      fb[a] = fb[a] + wf * b[q][a];
+      ff[a] = ff[a] + wf * f[q][a];
+    }
+  }
+  double h = 0.;
+  if (p > 0) h += norm3(fb[0] - cc[0], fb[1] - cc[1], fb[2] - cc[2]);
+  if (p < nd - 1) h += norm3(ff[0] - cc[0], ff[1] - cc[1], ff[2] - cc[2]);
+  return h;
 }
 
 // ---------------------------------------------------------------------------
@@ -263,9 +334,9 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
   const long long N = M.ncell;
   const int lane = threadIdx.x % SW_LANES, row = threadIdx.x / SW_LANES;
   const int nd = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
-  if (sweep_warp_empty<D>(M.ncx, M.ncy, M.ncz, XOUT, vbx, vby, row)) return;  // whole warp leaves together
+  if (sweep_warp_empty<D>(M.ncx, M.ncy, M.ncz, XOUT, 2, vbx, vby, row)) return;  // whole warp leaves together
   int i, j, k, p, ta, tb;
-  const bool ok = sweep_lane<D>(M.ncx, M.ncy, M.ncz, XOUT, vbx, vby, lane, row, i, j, k, p, ta, tb);
+  const bool ok = sweep_lane<D>(M.ncx, M.ncy, M.ncz, XOUT, 2, vbx, vby, lane, row, i, j, k, p, ta, tb);
   const bool out = ok && lane >= 2 && lane < 2 + XOUT;
   const double dt = F.s->dt;
   const int order2 = LIM == LIM_ORDER1 ? 0 : 1;  // ordre-projection - 1
@@ -311,6 +382,15 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
 #pragma unroll
     for (int v = 0; v < NV; ++v) u[v] = 0.;
   }
+  // widths of the own and neighbouring cells (generalised limiters only)
+  double hw = 0., hw_l = 0., hw_r = 0.;
+  if constexpr (LIM == LIM_GEN) {
+    hw = lane_cell_width<DIM, D>(M, F, ok, i, j, k, p, nd);
+    hw_l = __shfl_up_sync(FULL, hw, 1);
+    hw_r = __shfl_down_sync(FULL, hw, 1);
+    if (p == 0) hw_l = hw;
+    if (p == nd - 1) hw_r = hw;
+  }
   const double fc = back.fc, un = back.un, L = back.L;  // back face of the cell
   const bool ok_l = __shfl_up_sync(FULL, ok, 1) && lane > 0 && p > 0;  // same line
   const double xc_l = __shfl_up_sync(FULL, xc, 1);
@@ -328,10 +408,212 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
     const double phi_l = __shfl_up_sync(FULL, phi, 1);
     const double gf = face_b ? div_rn(phi - phi_l, dxb) : 0.;
     const double gf_r = __shfl_down_sync(FULL, gf, 1);
-    const double gr = (LIM != LIM_ORDER1 && ok) ? limited_gradient_t<LIM>(gf, gf_r) : 0.;
+    double gr;
+    if constexpr (LIM == LIM_GEN) {
+      // back / front neighbours, the cell itself at the line ends
+      const double phi_r = __shfl_down_sync(FULL, phi, 1);
+      const double ym = p > 0 ? phi_l : phi, yp = p < nd - 1 ? phi_r : phi;
+      gr = ok ? generalized_gradient(A.limiter, gf_r, gf, yp, ym, hw, hw_r, hw_l, A.simple_pente) : 0.;
+    } else {
+      gr = (LIM != LIM_ORDER1 && ok) ? limited_gradient_t<LIM>(gf, gf_r) : 0.;
+    }
     const double gr_l = __shfl_up_sync(FULL, gr, 1);
     double pf = 0.;
     if (face_b) pf = up_left ? phi_l + order2 * (fc - xc_l) * gr_l : phi + order2 * (fc - xc) * gr;
+    const double pf_r = __shfl_down_sync(FULL, pf, 1);
+    if (out) {
+      const double fB = face_b ? ondB * un * L * dt * pf : 0.;
+      const double fF = face_f ? ondF * un_r * L_r * dt * pf_r : 0.;
+      double sumf = 0., dual = 0.;
+      if (FRONT_FIRST) {
+        if (face_f) { sumf += fF; dual += 0.5 * fF * ondF; }
+        if (face_b) { sumf += fB; dual += 0.5 * fB * ondB; }
+      } else {
+        if (face_b) { sumf += fB; dual += 0.5 * fB * ondB; }
+        if (face_f) { sumf += fF; dual += 0.5 * fF * ondF; }
+      }
+      double uo = u[v] - sumf;
+      if (v >= NE && v < 3 * NE && uo < 0.) uo = 0.;  // masses and energies stay >= 0
+      A.Uout[v * N + c] = uo;
+      if (v >= NE && v < 2 * NE) F.mflux[(v - NE) * N + c] = dual;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Third-order face value (Remap-ordre-3.cc:16-188: evaluate_grad,
+// evaluate_ystar, evaluate_fm / evaluate_fp, the TVD interval bound of
+// ComputeFluxOrdre3).  y[0..5], h[0..5]: values and widths of the cells
+// b-2 .. f+2 around the face, repeated at the line ends; vdt = face normal
+// velocity x deltat.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double o3_grad(double hm, double h0, double hp, double ym, double y0, double yp) {
+  return h0 / (hm + h0 + hp) * ((2. * hm + h0) / (h0 + hp) * (yp - y0) + (h0 + 2. * hp) / (hm + h0) * (y0 - ym));
+}
+__device__ __forceinline__ double o3_ystar(double hmm, double hm, double hp, double hpp, double ymm, double ym,
+                                           double yp, double ypp, double gm, double gp) {
+  const double a =
+      (2. * hp * hm) / (hm + hp) * ((hmm + hm) / (2. * hm + hp) - (hpp + hp) / (2. * hp + hm)) * (yp - ym);
+  const double b = -hm * (hmm + hm) / (2. * hm + hp) * gp + hp * (hp + hpp) / (hm + 2. * hp) * gm;
+  return ym + hm / (hm + hp) * (yp - ym) + 1. / (hmm + hm + hp + hpp) * (a + b);
+}
+__device__ __forceinline__ double order3_face_value(const double (&y)[6], const double (&h)[6], double vdt) {
+  if (!(vdt > 0.) && !(vdt < 0.)) return 0.;
+  const double g0 = o3_grad(h[0], h[1], h[2], y[0], y[1], y[2]);
+  const double g1 = o3_grad(h[1], h[2], h[3], y[1], y[2], y[3]);
+  const double g2 = o3_grad(h[2], h[3], h[4], y[2], y[3], y[4]);
+  const double g3 = o3_grad(h[3], h[4], h[5], y[3], y[4], y[5]);
+  const double s0 = o3_ystar(h[1], h[2], h[3], h[4], y[1], y[2], y[3], y[4], g1, g2);
+  double v;
+  if (vdt > 0.) {
+    const double sm = o3_ystar(h[0], h[1], h[2], h[3], y[0], y[1], y[2], y[3], g0, g1);
+    const double du = s0 - sm, u6 = 6. * (y[2] - 0.5 * (sm + s0));
+    v = s0 - 0.5 * vdt / h[2] * (du - (1. - 2. / 3. * vdt / h[2]) * u6);
+  } else {
+    const double sp = o3_ystar(h[2], h[3], h[4], h[5], y[2], y[3], y[4], y[5], g2, g3);
+    const double du = sp - s0, u6 = 6. * (y[3] - 0.5 * (s0 + sp)), x = -vdt;
+    v = s0 + 0.5 * x / h[3] * (du - (1. - 2. / 3. * x / h[3]) * u6);
+  }
+  // TVD bound: [y_b, y_f] intersected with the upwind extrapolation
+  double o, x;
+  if (vdt > 0.) {
+    const double num = vdt / h[2];
+    o = y[2];
+    x = y[2] + (1. - num) / num * (y[2] - y[1]);
+  } else {
+    const double nup = vdt / h[3];
+    o = y[3];
+    x = y[3] - (1. + nup) / nup * (y[3] - y[4]);
+  }
+  const double i1a = amin(y[2], y[3]), i1b = amax(y[2], y[3]);
+  const double i2a = amin(o, x), i2b = amax(o, x);
+  double lo = 0., hi = 0.;
+  if (!(i1b < i2a || i2b < i1a)) {
+    lo = amax(i1a, i2a);
+    hi = amin(i1b, i2b);
+  }
+  if (v < lo) v = lo;
+  if (v > hi) v = hi;
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Cell sweep along D with the third-order face values
+// (computeUpwindFaceQuantitiesForProjection, RemapADIService.cc:319-380):
+// the same lane layout with 3 halo lanes on each side (lane l: cell
+// x0 - 3 + l, lanes 3 .. 28 write).  Faces between two cells that are not
+// both pure in the same material (EstMixte / EstPure, which equal the
+// volume-fraction signs of the cell values read here; every cell is pure in
+// material 0 before the first remap of the run) take their mass and energy
+// values from the volume value with the upwind cell's density and specific
+// energy.
+// ---------------------------------------------------------------------------
+template <int DIM, int NE, int D>
+__device__ __forceinline__ void body_sweep_cells_o3(const Mesh& M, const Fields& F, const SweepArgs& A, int vbx,
+                                                    int vby) {
+  constexpr int NV = 3 * NE + 1;
+  constexpr int NQ = DIM == 3 ? 4 : 2;
+  constexpr int HL = 3;
+  constexpr unsigned FULL = 0xffffffffu;
+  const long long N = M.ncell;
+  const int lane = threadIdx.x % SW_LANES, row = threadIdx.x / SW_LANES;
+  const int nd = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
+  if (sweep_warp_empty<D>(M.ncx, M.ncy, M.ncz, XOUT_W, HL, vbx, vby, row)) return;  // whole warp leaves together
+  int i, j, k, p, ta, tb;
+  const bool ok = sweep_lane<D>(M.ncx, M.ncy, M.ncz, XOUT_W, HL, vbx, vby, lane, row, i, j, k, p, ta, tb);
+  const bool out = ok && lane >= HL && lane < HL + XOUT_W;
+  const double dt = F.s->dt;
+  const double* __restrict__ Uin = A.Uin;
+  Plane<DIM> back;
+  if (ok) load_plane<DIM, D>(M, F, i, j, k, back);
+  else {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) back.xd[q] = 0.;
+    back.fc = back.un = back.L = 0.;
+  }
+  long long c = 0;
+  double u[NV], den = 1., ondB = 0., ondF = 0.;
+  if (ok) {
+    c = cell_id(M, i, j, k);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = __ldg(Uin + v * N + c);
+    if (A.first) {
+      den = __ldg(F.V + c);
+    } else {
+      den = 0.;
+#pragma unroll
+      for (int q = 0; q < NE; ++q) den += u[q];
+    }
+    if (out) {
+      constexpr int A0 = D == 0 ? 1 : 0, A1 = D == 2 ? 1 : 2;
+      const double t0 = fc0_comp<DIM, D, A0>(M, ta) - cc0_comp<DIM, A0>(M, ta);
+      const double t1 = fc0_comp<DIM, D, A1>(M, tb) - cc0_comp<DIM, A1>(M, tb);
+      const double cc0 = cc0_comp<DIM, D>(M, p);
+      ondB = unit_comp<D>(fc0_comp<DIM, D, D>(M, p) - cc0, t0, t1);
+      ondF = unit_comp<D>(fc0_comp<DIM, D, D>(M, p + 1) - cc0, t0, t1);
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = 0.;
+  }
+  // widths of the stencil b-2 .. f+2 of the back face (f = this cell)
+  const double hw = lane_cell_width<DIM, D>(M, F, ok, i, j, k, p, nd);
+  const bool m2 = p >= 2, m3 = p >= 3, p1 = p + 1 < nd, p2 = p + 2 < nd;
+  double h[6];
+  {
+    const double a1 = __shfl_up_sync(FULL, hw, 1), a2 = __shfl_up_sync(FULL, hw, 2),
+                 a3 = __shfl_up_sync(FULL, hw, 3), b1 = __shfl_down_sync(FULL, hw, 1),
+                 b2 = __shfl_down_sync(FULL, hw, 2);
+    h[2] = a1; h[1] = m2 ? a2 : h[2]; h[0] = m3 ? a3 : h[1];
+    h[3] = hw; h[4] = p1 ? b1 : h[3]; h[5] = p2 ? b2 : h[4];
+  }
+  // purity code: -2 mixed, else the last material with a positive volume
+  // fraction (-1: none)
+  int code = 0;
+  if (ok && !A.first_remap) {
+    int cnt = 0;
+    code = -1;
+#pragma unroll
+    for (int q = 0; q < NE; ++q)
+      if (div_rn(u[q], den) > 0.) { ++cnt; code = q; }
+    if (cnt > 1) code = -2;
+  }
+  const int code_l = __shfl_up_sync(FULL, code, 1);
+  const bool pure_nb = code_l == code && code != -2;
+  const double un = back.un, L = back.L;  // back face of the cell
+  const bool ok_l = __shfl_up_sync(FULL, ok, 1) && lane > 0 && p > 0;  // same line
+  const bool face_b = ok && ok_l;
+  const bool face_f = __shfl_down_sync(FULL, face_b, 1) && lane < 31;
+  const double un_r = __shfl_down_sync(FULL, un, 1), L_r = __shfl_down_sync(FULL, L, 1);
+  const double vdt = un * dt;
+  constexpr bool FRONT_FIRST = DIM == 2 && D == 0;
+  double pf_v[NE], yb_v[NE], yf_v[NE], pf_m[NE], yb_m[NE], yf_m[NE];
+  bool corr[NE];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double phi = ok ? div_rn(u[v], den) : 0.;
+    double y[6];
+    {
+      const double a1 = __shfl_up_sync(FULL, phi, 1), a2 = __shfl_up_sync(FULL, phi, 2),
+                   a3 = __shfl_up_sync(FULL, phi, 3), b1 = __shfl_down_sync(FULL, phi, 1),
+                   b2 = __shfl_down_sync(FULL, phi, 2);
+      y[2] = a1; y[1] = m2 ? a2 : y[2]; y[0] = m3 ? a3 : y[1];
+      y[3] = phi; y[4] = p1 ? b1 : y[3]; y[5] = p2 ? b2 : y[4];
+    }
+    double pf = face_b ? order3_face_value(y, h, vdt) : 0.;
+    if (v < NE) {
+      pf_v[v] = pf; yb_v[v] = y[2]; yf_v[v] = y[3];
+    } else if (v < 2 * NE) {
+      const int e = v - NE;
+      const bool cb = vdt > 0. && yb_v[e] != 0. && y[2] != 0.;
+      const bool cf = vdt < 0. && yf_v[e] != 0. && y[3] != 0.;
+      corr[e] = !pure_nb && (cb || cf);
+      if (corr[e]) pf = (cb ? (y[2] / yb_v[e]) : (y[3] / yf_v[e])) * pf_v[e];
+      pf_m[e] = pf; yb_m[e] = y[2]; yf_m[e] = y[3];
+    } else if (v < 3 * NE) {
+      const int e = v - 2 * NE;
+      if (corr[e]) pf = (vdt > 0. ? (y[2] / yb_m[e]) : (y[3] / yf_m[e])) * pf_m[e];
+    }
     const double pf_r = __shfl_down_sync(FULL, pf, 1);
     if (out) {
       const double fB = face_b ? ondB * un * L * dt * pf : 0.;
@@ -360,13 +642,15 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
 // node behind it, summed over the same cells in the same order, so each
 // lane sums its front cells once and hands the sum to lane l+1.
 // ---------------------------------------------------------------------------
-constexpr int NOUT = 28;  // nodes written per warp (lanes 2 .. 29)
+constexpr int NOUT = 28;    // nodes written per warp (lanes 2 .. 29)
+constexpr int NOUT_W = 26;  // generalised limiters (widths need 2 more nodes): lanes 3 .. 28
 
 struct DualArgs {
   const double* Uin;   // null on the first sweep (U built from m and v)
   double* Uout;
   int order;
   int limiter;
+  int simple_pente;    // projection-simple-pente (generalised limiters)
   int done_dirs;       // bit d: direction d already swept this cycle
 };
 
@@ -383,11 +667,13 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
   const long long NN = M.nnode, N = M.ncell;
   const int lane = threadIdx.x % SW_LANES, row = threadIdx.x / SW_LANES;
   const int nn = D == 0 ? M.nnx : (D == 1 ? M.nny : M.nnz);
-  if (sweep_warp_empty<D>(M.nnx, M.nny, M.nnz, NOUT, vbx, vby, row)) return;  // whole warp leaves together
+  constexpr int HL = LIM == LIM_GEN ? 3 : 2;
+  constexpr int NO = LIM == LIM_GEN ? NOUT_W : NOUT;
+  if (sweep_warp_empty<D>(M.nnx, M.nny, M.nnz, NO, HL, vbx, vby, row)) return;  // whole warp leaves together
   int i, j, k, id, ta, tb;
-  const bool ok = sweep_lane<D>(M.nnx, M.nny, M.nnz, NOUT, vbx, vby, lane, row, i, j, k, id, ta, tb);
+  const bool ok = sweep_lane<D>(M.nnx, M.nny, M.nnz, NO, HL, vbx, vby, lane, row, i, j, k, id, ta, tb);
   const bool inner = ok && id > 0 && id < nn - 1;
-  const bool out = ok && lane >= 2 && lane < 2 + NOUT;
+  const bool out = ok && lane >= HL && lane < HL + NO;
   long long n = 0;
   double U[5] = {0., 0., 0., 0., 0.};
   double ph[4] = {0., 0., 0., 0.};
@@ -451,6 +737,22 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
     ph_r[q] = __shfl_down_sync(FULL, ph[q], 1);
   }
   const double bfm = __shfl_up_sync(FULL, ffm, 1);
+  // dual cell widths for the generalised limiters (UtilesRemap.cc:51-63);
+  // a missing second neighbour gives a zero width
+  double h0 = 0., hm = 0., hp = 0.;
+  if constexpr (LIM == LIM_GEN) {
+    const double x_ll = __shfl_up_sync(FULL, x, 2), x_rr = __shfl_down_sync(FULL, x, 2);
+    const bool bb = id >= 2, ff = id + 2 < nn;
+    h0 = 0.5 * (x_r - x_l);
+    if (!bb) {
+      if (ff) hp = 0.5 * (x_rr - x);
+    } else if (!ff) {
+      hm = 0.5 * (x - x_ll);
+    } else {
+      hm = 0.5 * (x - x_ll);
+      hp = 0.5 * (x_rr - x);
+    }
+  }
   // limited gradients of the velocity components (inner nodes only)
   double g[3], g_l[3], g_r[3];
 #pragma unroll
@@ -459,7 +761,10 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
     if (LIM != LIM_ORDER1 && inner) {
       const double gfw = div_rn(ph_r[q] - ph[q], x_r - x);
       const double gbw = div_rn(ph[q] - ph_l[q], x - x_l);
-      g[q] = limited_gradient_t<LIM>(gbw, gfw);
+      if constexpr (LIM == LIM_GEN)
+        g[q] = generalized_gradient(A.limiter, gfw, gbw, ph_r[q], ph_l[q], h0, hp, hm, A.simple_pente);
+      else
+        g[q] = limited_gradient_t<LIM>(gbw, gfw);
     }
     g_l[q] = __shfl_up_sync(FULL, g[q], 1);
     g_r[q] = __shfl_down_sync(FULL, g[q], 1);
@@ -471,7 +776,7 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
     return;
   }
   const double dt = F.s->dt;
-  const int order2 = LIM == LIM_ORDER1 ? 0 : 1;  // ordre-projection - 1
+  const int order2 = LIM == LIM_ORDER1 ? 0 : A.order - 1;  // ordre-projection - 1
   U[3] += bfm - ffm;
   double FV[3], BV[3], FE, BE;
   {

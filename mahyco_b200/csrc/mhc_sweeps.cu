@@ -1,38 +1,66 @@
 // mhc_sweeps.cu -- launches of the remap sweeps, one kernel per (dimension,
-// number of environments, direction, limiter); kept in their own
-// translation unit because they are the bulk of the template instances.
+// number of environments, direction, sweep instance).  They are the bulk of
+// the template instances, so this file is compiled once per number of
+// environments (MHC_SWEEP_PART = NE - 1) and the parts build in parallel;
+// part 0 also holds the dispatcher.
 #include "mhc_engine.cuh"
+
+#ifndef MHC_SWEEP_PART
+#error "compile with -DMHC_SWEEP_PART=0..3 (number of environments - 1)"
+#endif
 
 namespace {
 
 template <int DIM, int NE, int LIM>
-void sweep_step(Engine* e, Group& g, int D, int k) {
-  {
-    StageTimer tm(e, MHC_STAGE_SWEEP_CELLS);
-    if (D == 0) plaunch(e, kb_sweep_cells<DIM, NE, 0, LIM>, SW_THREADS, 0, g.sw_cells[0], k);
-    else if (D == 1) plaunch(e, kb_sweep_cells<DIM, NE, 1, LIM>, SW_THREADS, 0, g.sw_cells[1], k);
-    else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells<DIM, NE, 2, LIM>, SW_THREADS, 0, g.sw_cells[2], k);
-  }
-  {
-    StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
-    if (D == 0) plaunch(e, kb_sweep_nodes<DIM, NE, 0, LIM>, SW_THREADS, 0, g.sw_nodes[0], k);
-    else if (D == 1) plaunch(e, kb_sweep_nodes<DIM, NE, 1, LIM>, SW_THREADS, 0, g.sw_nodes[1], k);
-    else if constexpr (DIM == 3) plaunch(e, kb_sweep_nodes<DIM, NE, 2, LIM>, SW_THREADS, 0, g.sw_nodes[2], k);
-  }
+void cell_sweep(Engine* e, Group& g, int D, int k) {
+  StageTimer tm(e, MHC_STAGE_SWEEP_CELLS);
+  if (D == 0) plaunch(e, kb_sweep_cells<DIM, NE, 0, LIM>, SW_THREADS, 0, g.sw_cells[0], k);
+  else if (D == 1) plaunch(e, kb_sweep_cells<DIM, NE, 1, LIM>, SW_THREADS, 0, g.sw_cells[1], k);
+  else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells<DIM, NE, 2, LIM>, SW_THREADS, 0, g.sw_cells[2], k);
 }
 
-template <int DIM, int NE>
-void sweep_step_lim(Engine* e, Group& g, int D, int k) {
-  switch (g.LIM) {
-    case 0: sweep_step<DIM, NE, 0>(e, g, D, k); break;
-    case 1: sweep_step<DIM, NE, 1>(e, g, D, k); break;
-    case 2: sweep_step<DIM, NE, 2>(e, g, D, k); break;
-    default: sweep_step<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
-  }
+template <int DIM, int NE, int LIM>
+void node_sweep(Engine* e, Group& g, int D, int k) {
+  StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
+  if (D == 0) plaunch(e, kb_sweep_nodes<DIM, NE, 0, LIM>, SW_THREADS, 0, g.sw_nodes[0], k);
+  else if (D == 1) plaunch(e, kb_sweep_nodes<DIM, NE, 1, LIM>, SW_THREADS, 0, g.sw_nodes[1], k);
+  else if constexpr (DIM == 3) plaunch(e, kb_sweep_nodes<DIM, NE, 2, LIM>, SW_THREADS, 0, g.sw_nodes[2], k);
 }
 
 }  // namespace
 
-void sweep_step_any(Engine* e, Group& g, int D, int k) {
-  DISPATCH_GROUP(g, (sweep_step_lim<DIM_, NE_>(e, g, D, k)));
+// one direction of the remap for a group: cell sweep, then node sweep
+template <int DIM, int NE>
+void sweep_step_dn(Engine* e, Group& g, int D, int k) {
+  switch (g.CLIM) {
+    case 0: cell_sweep<DIM, NE, 0>(e, g, D, k); break;
+    case 1: cell_sweep<DIM, NE, 1>(e, g, D, k); break;
+    case 2: cell_sweep<DIM, NE, 2>(e, g, D, k); break;
+    case LIM_GEN: cell_sweep<DIM, NE, LIM_GEN>(e, g, D, k); break;
+    case LIM_O3: cell_sweep<DIM, NE, LIM_O3>(e, g, D, k); break;
+    default: cell_sweep<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
+  }
+  switch (g.LIM) {
+    case 0: node_sweep<DIM, NE, 0>(e, g, D, k); break;
+    case 1: node_sweep<DIM, NE, 1>(e, g, D, k); break;
+    case 2: node_sweep<DIM, NE, 2>(e, g, D, k); break;
+    case LIM_GEN: node_sweep<DIM, NE, LIM_GEN>(e, g, D, k); break;
+    default: node_sweep<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
+  }
 }
+
+template void sweep_step_dn<2, MHC_SWEEP_PART + 1>(Engine*, Group&, int, int);
+template void sweep_step_dn<3, MHC_SWEEP_PART + 1>(Engine*, Group&, int, int);
+
+#if MHC_SWEEP_PART == 0
+extern template void sweep_step_dn<2, 2>(Engine*, Group&, int, int);
+extern template void sweep_step_dn<3, 2>(Engine*, Group&, int, int);
+extern template void sweep_step_dn<2, 3>(Engine*, Group&, int, int);
+extern template void sweep_step_dn<3, 3>(Engine*, Group&, int, int);
+extern template void sweep_step_dn<2, 4>(Engine*, Group&, int, int);
+extern template void sweep_step_dn<3, 4>(Engine*, Group&, int, int);
+
+void sweep_step_any(Engine* e, Group& g, int D, int k) {
+  DISPATCH_GROUP(g, (sweep_step_dn<DIM_, NE_>(e, g, D, k)));
+}
+#endif

@@ -51,10 +51,10 @@ def test_rejects_options_outside_the_hot_path():
     lib = mb.load()
     h = ctypes.c_void_p()
     p = mb.default_params()
-    p.ordre_projection = 3                      # order-3 remap
+    p.ordre_projection = 4                      # no such remap order
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p = mb.default_params()
-    p.projection_limiteur_id = 5                # generalised limiters
+    p.projection_limiteur_id = 8                # no such limiter (TypesMahyco.h limiteur)
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p = mb.default_params()
     p.env[0].elasto_model = 1                   # elasto with the Euler remap
