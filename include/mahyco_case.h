@@ -138,7 +138,11 @@ typedef struct mhc_case_params {
   /* EnvSummation period */
   int time_history_period;
   double coef_antiderive;   /* coef-antiderive: anti-hourglass velocity correction (Lagrange only) */
-  int projection_simple_pente; /* projection-simple-pente: single-slope bound of the generalised limiters */
+  int projection_simple_pente; /* projection-simple-pente: single-slope bound of the generalised limiters (pente-borne only) */
+  int projection_pente_borne;  /* projection-pente-borne: fluxes integrated over the swept length */
+  int projection_pente_borne_debar_fix; /* projection-pente-borne-debar-fix: 0, 1 (mean values) or 2 (cell values) */
+  int projection_pente_borne_mixte;     /* projection-pente-borne-mixte: pure-neighbourhood fluxes */
+  int projection_limiteur_pure_id;      /* projection-limiteur-pure-id: limiter of pure neighbourhoods */
 } mhc_case_params;
 
 #ifdef __cplusplus

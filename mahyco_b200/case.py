@@ -69,6 +69,8 @@ class CaseParams(C.Structure):
         ("time_history_period", C.c_int),
         ("coef_antiderive", C.c_double),
         ("projection_simple_pente", C.c_int),
+        ("projection_pente_borne", C.c_int), ("projection_pente_borne_debar_fix", C.c_int),
+        ("projection_pente_borne_mixte", C.c_int), ("projection_limiteur_pure_id", C.c_int),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -248,10 +250,13 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         eul = _txt(rm, "is-euler-scheme", "Full", str)
         if eul != "Full":
             raise NotImplementedError("is-euler-scheme other than Full")
-        for flag in ("projection-pente-borne", "conservation-energie-totale"):
-            if _txt(rm, flag, False, _bool):
-                raise NotImplementedError(flag)
+        if _txt(rm, "conservation-energie-totale", False, _bool):
+            raise NotImplementedError("conservation-energie-totale")
         p.projection_simple_pente = int(_txt(rm, "projection-simple-pente", False, _bool))
+        p.projection_pente_borne = int(_txt(rm, "projection-pente-borne", False, _bool))
+        p.projection_pente_borne_debar_fix = _txt(rm, "projection-pente-borne-debar-fix", 0, int)
+        p.projection_pente_borne_mixte = int(_txt(rm, "projection-pente-borne-mixte", False, _bool))
+        p.projection_limiteur_pure_id = _txt(rm, "projection-limiteur-pure-id", 0, int)
         if p.ordre_projection not in (1, 2, 3) or not 0 <= p.projection_limiteur_id <= 7:
             raise NotImplementedError("ordre-projection / projection-limiteur-id out of range")
     if _txt(m, "schema-csts", False, _bool):

@@ -157,6 +157,7 @@ struct Case {
   std::vector<double> u_dual, phi_dual, dual_grad;
   std::vector<double> back_flux, front_flux;
   std::vector<double> h_cell;          /* m_h_cell_lagrange of the current direction */
+  std::vector<double> delta_ar, delta_av; /* pente-borne fluxes through the back / front faces */
   std::vector<int> est_mixte, est_pure; /* EstMixte / EstPure (Arcane default 0) */
   int sens_projection = 0;
   /* emulation of a protection/reprise restart (test pinning only): after
@@ -674,6 +675,8 @@ static void setup(Case& C, const mhc_case_params* p) {
   C.back_flux.assign(C.nnode, 0.);
   C.front_flux.assign(C.nnode, 0.);
   C.h_cell.assign(C.ncell, 0.);
+  C.delta_ar.assign(C.ncell * C.nvars, 0.);
+  C.delta_av.assign(C.ncell * C.nvars, 0.);
   C.est_mixte.assign(C.ncell, 0);
   C.est_pure.assign(C.ncell, 0);
 }
@@ -1199,6 +1202,126 @@ static double order3_face_value(const double* y, const double* h, double vdt) {
   return v;
 }
 
+/* ---------------------------------------------------------------------------
+ * pente-borne fluxes (UtilesRemap.cc:84-96, 190-312, 417-832)
+ * ------------------------------------------------------------------------- */
+/* INTY: integral from -inf to X of the linear piece through (x0, y0),
+ * (x1, y1) restricted to [x0, x1] */
+static double inty(double X, double x0, double y0, double x1, double y1, double thr) {
+  double flux = 0.;
+  if (std::fabs(x1 - x0) > thr) {
+    const double eta = amin(amax(0., (X - x0) / (x1 - x0)), 1.);
+    flux = (y0 + 0.5 * eta * (y1 - y0)) * (x1 - x0) * eta;
+  }
+  return flux;
+}
+
+/* computeY0: monotonicity thresholds y0plus / y0moins of the three-piece
+ * reconstruction for the limiter id */
+static void pb_y0(int id, double yp, double ym, double h0, double hp, double hm, bool simple_pente,
+                  double& y0p, double& y0m) {
+  y0p = 0.; y0m = 0.;
+  if (id == MHC_MINMOD_G || id == MHC_MINMOD) {
+    y0p = yp; y0m = ym;
+  } else if (id == MHC_SUPERBEE_G || id == MHC_SUPERBEE) {
+    y0p = ((h0 + hm) * yp + h0 * ym) / (2 * h0 + hm);
+    y0m = ((h0 + hp) * ym + h0 * yp) / (2 * h0 + hp);
+  } else if (id == MHC_VANLEER_G || id == MHC_VANLEER) {
+    const double a = amin(yp, ym), b = amax(yp, ym);
+    double xp = (h0 * h0 + 3 * h0 * hm + 2 * hm * hm) * yp;
+    double xm = (h0 * h0 + 3 * h0 * hp + 2 * hp * hp) * ym;
+    xp += (h0 * h0 - h0 * hp - 2 * hp * hp + 2 * h0 * hm) * ym;
+    xm += (h0 * h0 - h0 * hm - 2 * hm * hm + 2 * h0 * hp) * yp;
+    xp /= (2 * h0 * h0 + 5 * h0 * hm + 2 * hm * hm - h0 * hp - 2 * hp * hp);
+    xm /= (2 * h0 * h0 + 5 * h0 * hp + 2 * hp * hp - h0 * hm - 2 * hm * hm);
+    y0p = amin(amax(xp, a), b);
+    y0m = amin(amax(xm, a), b);
+  } else if (id == MHC_ULTRABEE_G) {
+    y0p = (yp + ym) / 2.;
+    y0m = (yp + ym) / 2.;
+  } else if (id == MHC_ARITHMETIC_G) {
+    y0p = ((h0 + hm + hp) * yp + h0 * ym) / (2 * h0 + hm + hp);
+    y0m = ((h0 + hm + hp) * ym + h0 * yp) / (2 * h0 + hm + hp);
+  }
+  if (simple_pente) { y0p = yp; y0m = ym; }
+}
+
+/* flux of one variable out of a cell through its back (type 0) or front
+ * (type 1) face: integral of the three-piece reconstruction (computexgxd,
+ * computeygyd) over the swept length, or the cell value times that length
+ * at an extremum (formule 16) */
+static double pb_flux(int type, double y0, double yp, double ym, double h0, double hp, double hm, double grad,
+                      double ppv, int lim, bool simple_pente, double thr) {
+  double y0p, y0m;
+  pb_y0(lim, yp, ym, h0, hp, hm, simple_pente, y0p, y0m);
+  double xplus = 1., xmoins = 1.;
+  if (std::fabs(y0p - yp) > thr) xplus = (y0 - yp) / (y0p - yp) - 1. / 2.;
+  if (std::fabs(y0m - ym) > thr) xmoins = (y0 - ym) / (y0m - ym) - 1. / 2.;
+  const double xd = +h0 * amin(amax(xplus, -1. / 2.), 1. / 2.);
+  const double xg = -h0 * amin(amax(xmoins, -1. / 2.), 1. / 2.);
+  const double xtd = y0 + h0 / 2 * grad, xtg = y0 - h0 / 2 * grad;
+  const double ad = amin(yp, 2. * y0m - ym), bd = amax(yp, 2. * y0m - ym);
+  const double ag = amin(ym, 2. * y0p - yp), bg = amax(ym, 2. * y0p - yp);
+  const double yd = amin(amax(xtd, ad), bd), yg = amin(amax(xtg, ag), bg);
+  double f1, f1m, f2, f2m, f3, f3m;
+  if (type == 0) {
+    const double X = -h0 / 2. + ppv, X0 = -h0 / 2.;
+    f1m = inty(X, -h0 / 2., ym, xg, yg, thr);
+    f1 = inty(X0, -h0 / 2., ym, xg, yg, thr);
+    f2m = inty(X, xg, yg, xd, yd, thr);
+    f2 = inty(X0, xg, yg, xd, yd, thr);
+    f3m = inty(X, xd, yd, h0 / 2., yp, thr);
+    f3 = inty(X0, xd, yd, h0 / 2., yp, thr);
+  } else {
+    const double X = h0 / 2. - ppv, X1 = h0 / 2.;
+    f1 = inty(X, -h0 / 2., ym, xg, yg, thr);
+    f1m = inty(X1, -h0 / 2., ym, xg, yg, thr);
+    f2 = inty(X, xg, yg, xd, yd, thr);
+    f2m = inty(X1, xg, yg, xd, yd, thr);
+    f3 = inty(X, xd, yd, h0 / 2., yp, thr);
+    f3m = inty(X1, xd, yd, h0 / 2., yp, thr);
+  }
+  double F = std::max(((f1m - f1) + (f2m - f2) + (f3m - f3)), 0.);
+  if (((yp - y0) * (ym - y0)) >= 0.) F = y0 * ppv;
+  return F;
+}
+
+/* computeFluxPP / computeFluxPPPure (UtilesRemap.cc:417-832) for cell c
+ * with neighbours cf / cb: fluxes of every variable through one face, then
+ * the de-barring fix that rebuilds mass and energy fluxes */
+static void pb_cell_fluxes(const Case& C, long c, long cf, long cb, double v, int type, bool pure, double* F) {
+  const int nv = C.nvars, ne = C.nenv;
+  const double thr = C.P.remap_threshold;
+  const double ppv = 0.5 * (v + std::fabs(v)) * C.dt;
+  const int lim = pure ? C.P.projection_limiteur_pure_id : C.P.projection_limiteur_id;
+  const bool sp = C.P.projection_simple_pente != 0;
+  const double* P = C.phi_lag.data();
+  for (int iv = 0; iv < nv; ++iv) F[iv] = 0.;
+  for (int iv = 0; iv < C.nproj(); ++iv)
+    F[iv] = pb_flux(type, P[c * nv + iv], P[cf * nv + iv], P[cb * nv + iv], C.h_cell[c], C.h_cell[cf],
+                    C.h_cell[cb], C.grad_phi[c * nv + iv], ppv, lim, sp, thr);
+  const int fix = C.P.projection_pente_borne_debar_fix;
+  if (fix == 1) {
+    double sfv = 0.;
+    for (int e = 0; e < ne; ++e) sfv += F[e];
+    if (std::fabs(sfv) > thr) {
+      for (int e = 0; e < ne; ++e) {
+        if (!pure) F[ne + e] = (F[ne + e] / sfv) * F[e];
+        F[2 * ne + e] = (F[2 * ne + e] / sfv) * F[ne + e];
+      }
+    } else {
+      for (int iv = 0; iv < nv; ++iv) F[iv] = 0.;
+    }
+  } else if (fix == 2) {
+    for (int e = 0; e < ne; ++e) {
+      if (!pure) F[ne + e] = P[c * nv + ne + e] * F[e];
+      F[2 * ne + e] = P[c * nv + 2 * ne + e] * F[ne + e];
+    }
+  }
+  if (ppv == 0.)
+    for (int iv = 0; iv < nv; ++iv) F[iv] = 0.;
+}
+
 /* MahycoModule::computeVariablesForRemap (PrepareRemap.cc:94-193) */
 static void compute_variables_for_remap(Case& C) {
   const int ne = C.nenv, nv = C.nvars;
@@ -1212,7 +1335,17 @@ static void compute_variables_for_remap(Case& C) {
       u[ne + e] = V * rho;
       u[2 * ne + e] = V * rho * C.EV(C.internal_energy, e, c);
       u[3 * ne] = C.cell_volume.g[c] * C.pseudo.g[c];
-      for (int iv = 0; iv < C.nproj(); ++iv) C.phi_lag[c * nv + iv] = u[iv] / C.cell_volume.g[c];
+      if (C.P.projection_pente_borne) {
+        /* the cell's own environment values; entries of absent
+         * environments keep their values of the previous remap */
+        double* ph = &C.phi_lag[c * nv];
+        ph[e] = C.EV(C.fracvol, e, c);
+        ph[ne + e] = rho;
+        ph[2 * ne + e] = C.EV(C.internal_energy, e, c);
+        ph[3 * ne] = C.pseudo.g[c];
+      } else {
+        for (int iv = 0; iv < C.nproj(); ++iv) C.phi_lag[c * nv + iv] = u[iv] / C.cell_volume.g[c];
+      }
     }
   }
   for (long n = 0; n < C.nnode; ++n) {
@@ -1318,13 +1451,34 @@ static void compute_grad_phi_cell(Case& C, int d) {
     long cb = cell_step(C, c, d, -1), cf = cell_step(C, c, d, +1);
     if (cb < 0) cb = c;
     if (cf < 0) cf = c;
+    /* pure neighbourhood (projection-pente-borne-mixte only) */
+    const bool pure = C.P.projection_pente_borne_mixte && C.est_mixte[c] == 0 && C.est_mixte[cf] == 0 &&
+                      C.est_mixte[cb] == 0 && C.est_pure[c] == C.est_pure[cf] && C.est_pure[c] == C.est_pure[cb];
+    int l = lim;
+    if (C.P.projection_limiteur_pure_id == 1 && pure) l = C.P.projection_limiteur_pure_id;
     for (int iv = 0; iv < C.nproj(); ++iv) {
       const double gb = C.grad_phi_face[fb * nv + iv], gf = C.grad_phi_face[ff * nv + iv];
-      C.grad_phi[c * nv + iv] = lim < MHC_MINMOD_G
-          ? limited_gradient(lim, gb, gf)
-          : generalized_gradient(lim, gf, gb, C.phi_lag[c * nv + iv], C.phi_lag[cf * nv + iv], C.phi_lag[cb * nv + iv],
+      C.grad_phi[c * nv + iv] = l < MHC_MINMOD_G
+          ? limited_gradient(l, gb, gf)
+          : generalized_gradient(l, gf, gb, C.phi_lag[c * nv + iv], C.phi_lag[cf * nv + iv], C.phi_lag[cb * nv + iv],
                                  C.h_cell[c], C.h_cell[cf], C.h_cell[cb], C.P.projection_simple_pente != 0);
     }
+    if (!C.P.projection_pente_borne) continue;
+    /* outgoing normal velocities of the back and front faces
+     * (RemapADIService.cc:212-216) */
+    int i, j, k;
+    C.cijk(c, i, j, k);
+    double vb = 0., vf = 0.;
+    for (int q = 0; q < 2 * C.dim; ++q) {
+      int fd; long f;
+      C.cell_face(i, j, k, q, fd, f);
+      if (fd != d) continue;
+      const double ond = comp(C.outer_normal[c * 2 * C.dim + q], d);
+      if (f == fb) vb = ond * C.face_un[d][fb];
+      if (f == ff) vf = ond * C.face_un[d][ff];
+    }
+    pb_cell_fluxes(C, c, cf, cb, vb, 0, pure, &C.delta_ar[c * nv]);
+    pb_cell_fluxes(C, c, cf, cb, vf, 1, pure, &C.delta_av[c * nv]);
   }
 }
 
@@ -1339,6 +1493,11 @@ static void compute_upwind_face_quantities(Case& C, int d) {
     long cb, cf;
     face_cells(C, d, f, cb, cf);
     if (cb < 0 || cf < 0) continue;
+    if (C.P.ordre_projection <= 2 && C.P.projection_pente_borne) {
+      for (int iv = 0; iv < C.nproj(); ++iv)
+        C.phi_face[f * nv + iv] = C.delta_av[cb * nv + iv] - C.delta_ar[cf * nv + iv];
+      continue;
+    }
     if (C.P.ordre_projection <= 2) {
       long cu = (C.face_un[d][f] * C.deltax[d][f] > 0.0) ? cb : cf;
       for (int iv = 0; iv < C.nproj(); ++iv)
@@ -1409,20 +1568,43 @@ static void compute_uremap(Case& C, int d) {
       R3 on = C.outer_normal[c * 2 * C.dim + l];
       double ond = comp(on, d);
       for (int iv = 0; iv < C.nproj(); ++iv) {
-        double flux = ond * un * L * dt * C.phi_face[f * nv + iv];
+        /* pente-borne face values are already integrated fluxes */
+        double flux = C.P.projection_pente_borne ? ond * L * C.phi_face[f * nv + iv]
+                                                 : ond * un * L * dt * C.phi_face[f * nv + iv];
         flux_face[iv] += flux;
         C.dual_phi_flux[c * nv + iv] += 0.5 * flux * comp(on, d);
       }
     }
     double* u = &C.u_lag[c * nv];
     for (int iv = 0; iv < C.nproj(); ++iv) u[iv] -= flux_face[iv];
+    const double thr = C.P.remap_threshold;
+    if (C.P.projection_pente_borne) {
+      /* truncation of tiny projected volumes, masses and energies
+       * (RemapADIService.cc:440-462, with the dual projection) */
+      for (int e = 0; e < ne; ++e) {
+        if (u[e] < 1. * thr) { u[e] = 0.; u[ne + e] = 0.; u[2 * ne + e] = 0.; }
+        if (u[ne + e] < 1. * thr) { u[e] = 0.; u[ne + e] = 0.; u[2 * ne + e] = 0.; }
+        if (u[2 * ne + e] < 1. * thr) { u[e] = 0.; u[ne + e] = 0.; u[2 * ne + e] = 0.; }
+      }
+    }
     for (int e = 0; e < ne; ++e) {
       if (u[ne + e] < 0.) u[ne + e] = 0.;
       if (u[2 * ne + e] < 0.) u[2 * ne + e] = 0.;
     }
     double sv = 0.;
     for (int e = 0; e < ne; ++e) sv += u[e];
-    for (int iv = 0; iv < C.nproj(); ++iv) C.phi_lag[c * nv + iv] = u[iv] / sv;
+    if (C.P.projection_pente_borne) {
+      /* volume fractions, densities and specific energies
+       * (RemapADIService.cc:493-530); the pseudo-viscosity keeps its value */
+      double* ph = &C.phi_lag[c * nv];
+      for (int e = 0; e < ne; ++e) {
+        ph[e] = u[e] / sv;
+        ph[ne + e] = u[e] != 0. ? u[ne + e] / u[e] : 0.;
+      }
+      for (int e = 0; e < ne; ++e) ph[2 * ne + e] = u[ne + e] != 0. ? u[2 * ne + e] / u[ne + e] : 0.;
+    } else {
+      for (int iv = 0; iv < C.nproj(); ++iv) C.phi_lag[c * nv + iv] = u[iv] / sv;
+    }
     bool all[MHC_MAX_ENV];
     for (int e = 0; e < ne; ++e) all[e] = true;
     set_cell_purity(C, c, &C.phi_lag[c * nv], all);

@@ -39,6 +39,13 @@ CASES = {
     "CAS_BiSodCaseX_ordre_3": {"mpi_ranks": 4},
     "CAS_BiSodCaseY_ordre_3": {"mpi_ranks": 4},
     "CAS_BiSodCaseZ_ordre_3": {"mpi_ranks": 4},
+    # pente-borne fluxes, 4 MPI ranks with 2 ghost layers (the Z case has
+    # no EnvSummation curves in the reference tree)
+    "CAS_BiSodCaseX_pente_borne_minmod_debar_1": {"mpi_ranks": 4},
+    "CAS_BiSodCaseX_pente_borne_minmod_debar_2": {"mpi_ranks": 4},
+    "CAS_BiSodCaseX_pente_borne_superbee_debar_2": {"mpi_ranks": 4},
+    "CAS_BiSodCaseY_pente_borne_minmod_debar_2": {"mpi_ranks": 4},
+    "CAS_BiSodCaseY_pente_borne_superbee_debar_2": {"mpi_ranks": 4},
 }
 VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
 

@@ -76,8 +76,9 @@ def test_anti_hourglass_and_elasto_options(tmp_path):
 
 
 def test_remap_order_and_generalised_limiter_options(tmp_path):
-    """ordre-projection 3, the generalised limiters (ids 3-7) and
-    projection-simple-pente are read; pente-borne is refused."""
+    """ordre-projection 3, the generalised limiters (ids 3-7), the
+    pente-borne options and projection-simple-pente are read;
+    conservation-energie-totale is refused."""
     text = open(ARC).read().replace("<ordre-projection>2</ordre-projection>",
                                     "<ordre-projection>3</ordre-projection>").replace(
         "<projection-limiteur-id>1</projection-limiteur-id>",
@@ -90,6 +91,15 @@ def test_remap_order_and_generalised_limiter_options(tmp_path):
     assert (p.ordre_projection, p.projection_limiteur_id, p.projection_simple_pente) == (3, 5, 1)
     g = tmp_path / "pb.arc"
     g.write_text(text.replace("<ordre-projection>3</ordre-projection>",
-                              "<projection-pente-borne>true</projection-pente-borne>"))
+                              "<projection-pente-borne>true</projection-pente-borne>"
+                              "<projection-pente-borne-debar-fix>1</projection-pente-borne-debar-fix>"
+                              "<projection-pente-borne-mixte>true</projection-pente-borne-mixte>"
+                              "<projection-limiteur-pure-id>1</projection-limiteur-pure-id>"))
+    q, _ = read_arc(str(g))
+    assert (q.projection_pente_borne, q.projection_pente_borne_debar_fix, q.projection_pente_borne_mixte,
+            q.projection_limiteur_pure_id, q.ordre_projection) == (1, 1, 1, 1, 2)
+    r = tmp_path / "cet.arc"
+    r.write_text(text.replace("<ordre-projection>3</ordre-projection>",
+                              "<conservation-energie-totale>true</conservation-energie-totale>"))
     with pytest.raises(NotImplementedError):
-        read_arc(str(g))
+        read_arc(str(r))
