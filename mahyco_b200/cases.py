@@ -262,8 +262,23 @@ PARITY_CASES = {
                                                   interface=0.41, limiter=MINMOD_G, deltat_init=1e-3), 80),
     "adi3d_bisod_superbeeG": (lambda: sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True,
                                           limiter=SUPERBEE_G, deltat_init=1e-3), 60),
-    "adi2d_sedov_vanleerG_simple_pente": (lambda: _simple_pente(sedov(dim=2, n=(24, 24), limiter=VANLEER_G,
-                                                                      deltat_init=1e-4)), 100),
+    # pente-borne fluxes (computeFluxPP / computeFluxPPPure) with the three
+    # de-barring fixes, the pure-neighbourhood option and simple-pente
+    "adi3d_bisod_pb_minmod_debar1": (lambda: _pb(sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True,
+                                                      deltat_init=1e-3), 1), 60),
+    "adi2d_bisod_y_pb_superbee_debar2": (lambda: _pb(sod(dim=2, n=(5, 40), L=(0.1, 1.0), bi=True, axis=1,
+                                                          limiter=SUPERBEE, deltat_init=1e-3), 2), 60),
+    "adi2d_sedov_pb_vanleerG_simple_pente": (lambda: _pb(sedov(dim=2, n=(24, 24), limiter=VANLEER_G,
+                                                               deltat_init=1e-4), 2, simple=1), 100),
+    "adi3d_bisod_z_pb_mixte_superbeeG": (lambda: _pb(sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
+                                                          limiter=SUPERBEE_G, deltat_init=1e-3), 1, mixte=1,
+                                                      pure_id=1), 60),
+    "adi2d_two_state_pb_arithmeticG": (lambda: _pb(two_state(dim=2, n=(40, 30), left=(1.7, 1.3),
+                                                             right=(0.2, 0.07), interface=0.41,
+                                                             limiter=ARITHMETIC_G, deltat_init=1e-3), 2), 80),
+    "adi2d_water_air_pb_vanleer": (lambda: _pb(water_air(limiter=VANLEER, deltat_init=1e-6), 2, mixte=1), 80),
+    "adi2d_sod_mono_pb_fix0": (lambda: _pb(sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=False, limiter=SUPERBEE,
+                                               deltat_init=1e-3), 0), 80),
     "adi2d_bisod_arithmeticG": (lambda: sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True, limiter=ARITHMETIC_G,
                                             deltat_init=1e-3), 80),
     "adi3d_bisod_z_ultrabeeG": (lambda: sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
@@ -276,8 +291,12 @@ def _order3(p: CaseParams) -> CaseParams:
     return p
 
 
-def _simple_pente(p: CaseParams) -> CaseParams:
-    p.projection_simple_pente = 1
+def _pb(p: CaseParams, fix: int, mixte: int = 0, pure_id: int = 0, simple: int = 0) -> CaseParams:
+    p.projection_pente_borne = 1
+    p.projection_pente_borne_debar_fix = fix
+    p.projection_pente_borne_mixte = mixte
+    p.projection_limiteur_pure_id = pure_id
+    p.projection_simple_pente = simple
     return p
 
 

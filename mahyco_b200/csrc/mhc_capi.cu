@@ -346,7 +346,8 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   ncell = (long long)p->nx * p->ny * (dim == 3 ? p->nz : 1);
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
   int ne = p->nb_env, nv = 3 * ne + 1;
-  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8);
+  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8) +
+                    (p->projection_pente_borne ? nv : 0);
   long long nodes = 4 + 6 + 10;
   return cells * ncell + nodes * nnode;
 }
@@ -363,6 +364,14 @@ int validate(const mhc_case_params* p) {
   if (p->projection_limiteur_id < 0 || p->projection_limiteur_id > 7)
     return set_err(MHC_ERR_UNSUPPORTED, "projection-limiteur-id must be 0..7 (TypesMahyco.h limiteur)");
   if (p->is_euler_scheme != MHC_EULER_FULL) return set_err(MHC_ERR_UNSUPPORTED, "is-euler-scheme must be Full");
+  if (p->projection_simple_pente && !p->projection_pente_borne)
+    return set_err(MHC_ERR_UNSUPPORTED, "projection-simple-pente needs projection-pente-borne (MahycoModule.cc:47-51)");
+  if (p->projection_pente_borne && p->ordre_projection != 2)
+    return set_err(MHC_ERR_UNSUPPORTED, "projection-pente-borne needs ordre-projection 2");
+  if (p->projection_pente_borne_debar_fix < 0 || p->projection_pente_borne_debar_fix > 2)
+    return set_err(MHC_ERR_UNSUPPORTED, "projection-pente-borne-debar-fix must be 0, 1 or 2");
+  if (p->projection_limiteur_pure_id < 0 || p->projection_limiteur_pure_id > 7)
+    return set_err(MHC_ERR_UNSUPPORTED, "projection-limiteur-pure-id must be 0..7");
   for (int e = 0; e < p->nb_env; ++e) {
     const mhc_env_params& o = p->env[e];
     if (o.elasto_model < 0 || o.elasto_model > 1) return set_err(MHC_ERR_UNSUPPORTED, "elasto-model must be NoModel or DefaultModel");
@@ -475,6 +484,7 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   F.mflux = (double*)alloc(h->NE * N * sizeof(double));
   if (h->P.env[0].elasto_model) F.S = (double*)alloc(6 * N * sizeof(double));
   F.cqs = (double*)alloc((h->DIM == 3 ? 24 : 8) * N * sizeof(double));
+  if (h->P.projection_pente_borne) F.phi_pb = (double*)alloc(h->NV * N * sizeof(double));
   h->d_scal = (Scalars*)alloc(sizeof(Scalars));
   h->d_params = (mhc_case_params*)alloc(sizeof(mhc_case_params));
   F.s = h->d_scal;
@@ -482,6 +492,10 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
     cudaGetLastError();
     case_free(h);
     return set_err(MHC_ERR_NOMEM, "device allocation failed");
+  }
+  if (F.phi_pb && cudaMemsetAsync(F.phi_pb, 0, h->NV * N * sizeof(double), h->stream) != cudaSuccess) {
+    case_free(h);
+    return set_err(MHC_ERR_CUDA, "memset");
   }
   if (F.S && cudaMemsetAsync(F.S, 0, 6 * N * sizeof(double), h->stream) != cudaSuccess) {
     case_free(h);

@@ -204,10 +204,12 @@ __device__ __forceinline__ double div_rn(double x, double y) {
 // limiter id as a template argument: 0-2 the classical limiters (one
 // instance each), LIM_ORDER1 a first-order remap (no slope), LIM_GEN the
 // generalised limiters 3-7 (id read at run time), LIM_O3 the third-order
-// face values of the cell sweep
+// face values of the cell sweep, LIM_PB the pente-borne fluxes of the cell
+// sweep (limiter id read at run time)
 constexpr int LIM_ORDER1 = 3;
 constexpr int LIM_GEN = 4;
 constexpr int LIM_O3 = 5;
+constexpr int LIM_PB = 6;
 
 // RemapADIService::fluxLimiterG (UtilesRemap.cc:130-190): limited slope from
 // the back / front gradients gm / gp, the values ym, yp of the neighbours

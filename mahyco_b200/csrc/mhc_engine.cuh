@@ -69,7 +69,7 @@ struct Group {
   int DIM, NE, EULER, skip;
   int EL = 0, HG = 0;          // elasto-plastic model; anti-hourglass correction
   int LIM = 0;                 // node-sweep instance: limiter 0-2, LIM_ORDER1 or LIM_GEN
-  int CLIM = 0;                // cell-sweep instance: the same, or LIM_O3 for a third-order remap
+  int CLIM = 0;                // cell-sweep instance: the same, LIM_O3 (third order) or LIM_PB (pente-borne)
   long long it0;               // iteration of the members when the lists were built
   std::vector<int> members;
   DevList init_cells, init_nodes, lag_nodes, lag_cells, fin_cells, fin_nodes, dt;
@@ -139,6 +139,7 @@ inline int node_sweep_mode(const mhc_case_params& P) {
   return P.projection_limiteur_id >= MHC_MINMOD_G ? LIM_GEN : P.projection_limiteur_id;
 }
 inline int cell_sweep_mode(const mhc_case_params& P) {
+  if (P.projection_pente_borne) return LIM_PB;
   return P.ordre_projection == 3 ? LIM_O3 : node_sweep_mode(P);
 }
 

@@ -51,6 +51,9 @@ struct Fields {
   double* Ud[2];
   double* S;               // elasto: stress deviator [6][ncell] (xx yy zz xy yz zx)
   double* cqs;             // corner normals of the last Lagrangian mesh [NBN][3][ncell]
+  double* phi_pb;          // pente-borne only: projected values (phi) of the next remap's first sweep
+                           // [3 nb_env + 1][ncell]; entries of absent environments keep the
+                           // values of the last sweep before
   Scalars* s;
 };
 
@@ -520,6 +523,8 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   F.m[c] = pure ? 1.0 * m : m;
   F.V[c] = V; F.l[c] = l; F.Veul[c] = V;
   F.mask[c] = mask;
+  if (F.phi_pb)  // volume fractions of the first pente-borne remap (MahycoModule.cc hydroStartInit: 1 per environment)
+    for (int q = 0; q < NE; ++q) F.phi_pb[q * N + c] = ((mask >> q) & 1) ? fe[q] : 0.;
   if (NE > 1 && !pure) {
     for (int q = 0; q < NE; ++q) {
       F.ef[q * N + c] = fe[q]; F.emf[q * N + c] = mfe[q]; F.em[q * N + c] = me[q];
@@ -1007,6 +1012,17 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       U[(2 * NE + q) * N + c] = in ? Vq * rq * ee_[q] : 0.;
     }
     U[(NV - 1) * N + c] = V * qg;
+    if (F.phi_pb) {
+      // pente-borne phi of the first sweep (PrepareRemap.cc:138-157): the
+      // environment's density and internal energy, the pseudo-viscosity;
+      // the volume fractions are those of the last remap
+      for (int q = 0; q < NE; ++q) {
+        if (!((mask >> q) & 1)) continue;
+        F.phi_pb[(NE + q) * N + c] = rhoe[q];
+        F.phi_pb[(2 * NE + q) * N + c] = ee_[q];
+      }
+      F.phi_pb[(NV - 1) * N + c] = qg;
+    }
     F.V[c] = V;
     F.l[c] = l;
     return;
@@ -1195,6 +1211,23 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
       pg += fe[q] * pe[q];
       cg = option * smax(ce[q], cg);
       cg += (1. - option) * fe[q] * ce[q];
+    }
+  }
+  if (F.phi_pb) {
+    // pente-borne phi of the next remap's first sweep: the volume fraction
+    // of a present environment (the pure-cell value included); an absent
+    // environment keeps the values of this remap's last sweep
+    // (RemapADIService.cc:493-530 on the final projected values)
+    double sv = 0.;
+    for (int q = 0; q < NE; ++q) sv += u[q];
+    for (int q = 0; q < NE; ++q) {
+      if ((nm >> q) & 1) {
+        F.phi_pb[q * N + c] = EVF(q);
+      } else {
+        F.phi_pb[q * N + c] = div_rn(u[q], sv);
+        F.phi_pb[(NE + q) * N + c] = u[q] != 0. ? div_rn(u[NE + q], u[q]) : 0.;
+        F.phi_pb[(2 * NE + q) * N + c] = u[NE + q] != 0. ? div_rn(u[2 * NE + q], u[NE + q]) : 0.;
+      }
     }
   }
 #undef EVF

@@ -205,6 +205,7 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     A.first_remap = k == 0 && F.s->iteration == 1;
     const Mesh M = C[wi.c].M;
     if constexpr (LIM == LIM_O3) body_sweep_cells_o3<DIM, NE, D>(M, F, A, wi.x, wi.y);
+    else if constexpr (LIM == LIM_PB) body_sweep_cells_pb<DIM, NE, D>(M, F, P, A, wi.x, wi.y);
     else body_sweep_cells_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
   }
 }

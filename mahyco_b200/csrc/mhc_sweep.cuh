@@ -441,6 +441,270 @@ __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fiel
 }
 
 // ---------------------------------------------------------------------------
+// Pente-borne fluxes (UtilesRemap.cc:84-96 INTY, 190-312 computeY0 /
+// computexgxd / computeygyd, 417-832 computeFluxPP / computeFluxPPPure):
+// the flux of one variable out of a cell through its back (type 0) or front
+// (type 1) face is the integral, over the length swept in deltat, of a
+// three-piece reconstruction bounded by the neighbours.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double pb_inty(double X, double x0, double y0, double x1, double y1, double thr) {
+  double flux = 0.;
+  if (fabs(x1 - x0) > thr) {
+    const double eta = amin(amax(0., (X - x0) / (x1 - x0)), 1.);
+    flux = (y0 + 0.5 * eta * (y1 - y0)) * (x1 - x0) * eta;
+  }
+  return flux;
+}
+
+__device__ __forceinline__ void pb_y0(int id, double yp, double ym, double h0, double hp, double hm, int simple_pente,
+                                      double& y0p, double& y0m) {
+  y0p = 0.; y0m = 0.;
+  if (id == 3 || id == 0) {
+    y0p = yp; y0m = ym;
+  } else if (id == 4 || id == 1) {
+    y0p = ((h0 + hm) * yp + h0 * ym) / (2 * h0 + hm);
+    y0m = ((h0 + hp) * ym + h0 * yp) / (2 * h0 + hp);
+  } else if (id == 5 || id == 2) {
+    const double a = amin(yp, ym), b = amax(yp, ym);
+    double xp = (h0 * h0 + 3 * h0 * hm + 2 * hm * hm) * yp;
+    double xm = (h0 * h0 + 3 * h0 * hp + 2 * hp * hp) * ym;
+    xp += (h0 * h0 - h0 * hp - 2 * hp * hp + 2 * h0 * hm) * ym;
+    xm += (h0 * h0 - h0 * hm - 2 * hm * hm + 2 * h0 * hp) * yp;
+    xp /= (2 * h0 * h0 + 5 * h0 * hm + 2 * hm * hm - h0 * hp - 2 * hp * hp);
+    xm /= (2 * h0 * h0 + 5 * h0 * hp + 2 * hp * hp - h0 * hm - 2 * hm * hm);
+    y0p = amin(amax(xp, a), b);
+    y0m = amin(amax(xm, a), b);
+  } else if (id == 7) {
+    y0p = (yp + ym) / 2.;
+    y0m = (yp + ym) / 2.;
+  } else if (id == 6) {
+    y0p = ((h0 + hm + hp) * yp + h0 * ym) / (2 * h0 + hm + hp);
+    y0m = ((h0 + hm + hp) * ym + h0 * yp) / (2 * h0 + hm + hp);
+  }
+  if (simple_pente) { y0p = yp; y0m = ym; }
+}
+
+__device__ __forceinline__ double pb_flux(int type, double y0, double yp, double ym, double h0, double hp, double hm,
+                                          double grad, double ppv, int lim, int simple_pente, double thr) {
+  double y0p, y0m;
+  pb_y0(lim, yp, ym, h0, hp, hm, simple_pente, y0p, y0m);
+  double xplus = 1., xmoins = 1.;
+  if (fabs(y0p - yp) > thr) xplus = (y0 - yp) / (y0p - yp) - 1. / 2.;
+  if (fabs(y0m - ym) > thr) xmoins = (y0 - ym) / (y0m - ym) - 1. / 2.;
+  const double xd = +h0 * amin(amax(xplus, -1. / 2.), 1. / 2.);
+  const double xg = -h0 * amin(amax(xmoins, -1. / 2.), 1. / 2.);
+  const double xtd = y0 + h0 / 2 * grad, xtg = y0 - h0 / 2 * grad;
+  const double ad = amin(yp, 2. * y0m - ym), bd = amax(yp, 2. * y0m - ym);
+  const double ag = amin(ym, 2. * y0p - yp), bg = amax(ym, 2. * y0p - yp);
+  const double yd = amin(amax(xtd, ad), bd), yg = amin(amax(xtg, ag), bg);
+  double f1, f1m, f2, f2m, f3, f3m;
+  if (type == 0) {
+    const double X = -h0 / 2. + ppv, X0 = -h0 / 2.;
+    f1m = pb_inty(X, -h0 / 2., ym, xg, yg, thr);
+    f1 = pb_inty(X0, -h0 / 2., ym, xg, yg, thr);
+    f2m = pb_inty(X, xg, yg, xd, yd, thr);
+    f2 = pb_inty(X0, xg, yg, xd, yd, thr);
+    f3m = pb_inty(X, xd, yd, h0 / 2., yp, thr);
+    f3 = pb_inty(X0, xd, yd, h0 / 2., yp, thr);
+  } else {
+    const double X = h0 / 2. - ppv, X1 = h0 / 2.;
+    f1 = pb_inty(X, -h0 / 2., ym, xg, yg, thr);
+    f1m = pb_inty(X1, -h0 / 2., ym, xg, yg, thr);
+    f2 = pb_inty(X, xg, yg, xd, yd, thr);
+    f2m = pb_inty(X1, xg, yg, xd, yd, thr);
+    f3 = pb_inty(X, xd, yd, h0 / 2., yp, thr);
+    f3m = pb_inty(X1, xd, yd, h0 / 2., yp, thr);
+  }
+  double F = smax(((f1m - f1) + (f2m - f2) + (f3m - f3)), 0.);
+  if (((yp - y0) * (ym - y0)) >= 0.) F = y0 * ppv;  // extremum: formule 16
+  return F;
+}
+
+// ---------------------------------------------------------------------------
+// Cell sweep along D with the pente-borne fluxes (computeGradPhiCell,
+// computeUpwindFaceQuantitiesForProjection, computeUremap with
+// projection-pente-borne, RemapADIService.cc:196-266, 314-318, 419-530).
+// The lane layout of the classical sweep (2 halo lanes).  Every lane computes
+// the fluxes out of its cell through both faces; the value of the face
+// between lanes l-1 and l is front(l-1) - back(l).  The projected values
+// (phi) are the volume fraction, density and specific internal energy per
+// environment and the pseudo-viscosity, read from phi_pb on the first sweep
+// of a remap and rebuilt from the projected quantities on the others.
+// ---------------------------------------------------------------------------
+template <int DIM, int NE, int D>
+__device__ __forceinline__ void body_sweep_cells_pb(const Mesh& M, const Fields& F, const mhc_case_params& P,
+                                                    const SweepArgs& A, int vbx, int vby) {
+  constexpr int NV = 3 * NE + 1;
+  constexpr int NQ = DIM == 3 ? 4 : 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  const long long N = M.ncell;
+  const int lane = threadIdx.x % SW_LANES, row = threadIdx.x / SW_LANES;
+  const int nd = D == 0 ? M.ncx : (D == 1 ? M.ncy : M.ncz);
+  if (sweep_warp_empty<D>(M.ncx, M.ncy, M.ncz, XOUT, 2, vbx, vby, row)) return;  // whole warp leaves together
+  int i, j, k, p, ta, tb;
+  const bool ok = sweep_lane<D>(M.ncx, M.ncy, M.ncz, XOUT, 2, vbx, vby, lane, row, i, j, k, p, ta, tb);
+  const bool out = ok && lane >= 2 && lane < 2 + XOUT;
+  const double dt = F.s->dt;
+  const double thr = P.remap_threshold;
+  const int fix = P.projection_pente_borne_debar_fix;
+  const double* __restrict__ Uin = A.Uin;
+  Plane<DIM> back;
+  if (ok) load_plane<DIM, D>(M, F, i, j, k, back);
+  else {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) back.xd[q] = 0.;
+    back.fc = back.un = back.L = 0.;
+  }
+  Plane<DIM> front;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) front.xd[q] = __shfl_down_sync(FULL, back.xd[q], 1);
+  if (ok && p == nd - 1)
+    load_plane_xd<DIM, D>(M, F, D == 0 ? i + 1 : i, D == 1 ? j + 1 : j, D == 2 ? k + 1 : k, front);
+  long long c = 0;
+  double u[NV], ph[NV], xc = 0., ondB = 0., ondF = 0.;
+  uint8_t mask = 0;
+  if (ok) {
+    c = cell_id(M, i, j, k);
+    mask = F.mask[c];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = __ldg(Uin + v * N + c);
+    if (A.first) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) ph[v] = __ldg(F.phi_pb + v * N + c);
+    } else {
+      double sv = 0.;
+#pragma unroll
+      for (int q = 0; q < NE; ++q) sv += u[q];
+#pragma unroll
+      for (int q = 0; q < NE; ++q) {
+        ph[q] = div_rn(u[q], sv);
+        ph[NE + q] = u[q] != 0. ? div_rn(u[NE + q], u[q]) : 0.;
+        ph[2 * NE + q] = u[NE + q] != 0. ? div_rn(u[2 * NE + q], u[NE + q]) : 0.;
+      }
+      ph[NV - 1] = __ldg(F.phi_pb + (NV - 1) * N + c);  // the pseudo-viscosity is not rebuilt
+    }
+    xc = centre_from_planes<DIM, D>(back, front);
+    constexpr int A0 = D == 0 ? 1 : 0, A1 = D == 2 ? 1 : 2;
+    const double t0 = fc0_comp<DIM, D, A0>(M, ta) - cc0_comp<DIM, A0>(M, ta);
+    const double t1 = fc0_comp<DIM, D, A1>(M, tb) - cc0_comp<DIM, A1>(M, tb);
+    const double cc0 = cc0_comp<DIM, D>(M, p);
+    ondB = unit_comp<D>(fc0_comp<DIM, D, D>(M, p) - cc0, t0, t1);
+    ondF = unit_comp<D>(fc0_comp<DIM, D, D>(M, p + 1) - cc0, t0, t1);
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = ph[v] = 0.;
+  }
+  // cell widths, the cell itself beyond the line ends
+  const double hw = lane_cell_width<DIM, D>(M, F, ok, i, j, k, p, nd);
+  double hw_l = __shfl_up_sync(FULL, hw, 1), hw_r = __shfl_down_sync(FULL, hw, 1);
+  if (p == 0) hw_l = hw;
+  if (p == nd - 1) hw_r = hw;
+  // pure neighbourhood (projection-pente-borne-mixte): purity codes -2 mixed,
+  // else the last environment with a positive volume fraction (-1: none)
+  int code = 0;
+  if (ok && !A.first_remap) {
+    int cnt = 0;
+    code = -1;
+#pragma unroll
+    for (int q = 0; q < NE; ++q)
+      if ((!A.first || ((mask >> q) & 1)) && ph[q] > 0.) { ++cnt; code = q; }
+    if (cnt > 1) code = -2;
+  }
+  int code_l = __shfl_up_sync(FULL, code, 1), code_r = __shfl_down_sync(FULL, code, 1);
+  if (p == 0) code_l = code;
+  if (p == nd - 1) code_r = code;
+  const bool pure = P.projection_pente_borne_mixte && code != -2 && code_l != -2 && code_r != -2 &&
+                    code == code_l && code == code_r;
+  const int lim_g = (P.projection_limiteur_pure_id == 1 && pure) ? P.projection_limiteur_pure_id : A.limiter;
+  const int lim_y = pure ? P.projection_limiteur_pure_id : A.limiter;
+  const double un = back.un, L = back.L;  // back face of the cell
+  const bool ok_l = __shfl_up_sync(FULL, ok, 1) && lane > 0 && p > 0;  // same line
+  const double xc_l = __shfl_up_sync(FULL, xc, 1);
+  const bool face_b = ok && ok_l;
+  const bool face_f = __shfl_down_sync(FULL, face_b, 1) && lane < 31;
+  const double un_r = __shfl_down_sync(FULL, un, 1), L_r = __shfl_down_sync(FULL, L, 1);
+  const double dxb = xc - xc_l;
+  // outgoing normal velocities and swept lengths of the back / front faces
+  const double vb = ondB * un, vf = ondF * un_r;
+  const double ppv_b = 0.5 * (vb + fabs(vb)) * dt, ppv_f = 0.5 * (vf + fabs(vf)) * dt;
+  // raw flux of variable v through both faces
+  auto raw = [&](int v, double& Fb, double& Ff) {
+    const double y0 = ph[v];
+    const double y_l = __shfl_up_sync(FULL, y0, 1), y_r = __shfl_down_sync(FULL, y0, 1);
+    const double gf = face_b ? div_rn(y0 - y_l, dxb) : 0.;
+    const double gf_r = __shfl_down_sync(FULL, gf, 1);
+    const double ym = p > 0 ? y_l : y0, yp = p < nd - 1 ? y_r : y0;
+    double gr = 0.;
+    if (ok)
+      gr = lim_g < 3 ? limited_gradient(lim_g, gf, gf_r)
+                     : generalized_gradient(lim_g, gf_r, gf, yp, ym, hw, hw_r, hw_l, A.simple_pente);
+    Fb = ok ? pb_flux(0, y0, yp, ym, hw, hw_r, hw_l, gr, ppv_b, lim_y, A.simple_pente, thr) : 0.;
+    Ff = ok ? pb_flux(1, y0, yp, ym, hw, hw_r, hw_l, gr, ppv_f, lim_y, A.simple_pente, thr) : 0.;
+  };
+  // volume fluxes first: the de-barring fix 1 divides by their sum
+  double vol_b[NE], vol_f[NE], mass_b[NE], mass_f[NE];
+  double sfb = 0., sff = 0.;
+#pragma unroll
+  for (int q = 0; q < NE; ++q) {
+    raw(q, vol_b[q], vol_f[q]);
+    sfb += vol_b[q];
+    sff += vol_f[q];
+  }
+  const bool zb = (fix == 1 && !(fabs(sfb) > thr)) || ppv_b == 0.;
+  const bool zf = (fix == 1 && !(fabs(sff) > thr)) || ppv_f == 0.;
+  constexpr bool FRONT_FIRST = DIM == 2 && D == 0;
+  double uo[NV], dual[NE];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double Fb, Ff;
+    if (v < NE) { Fb = vol_b[v]; Ff = vol_f[v]; }
+    else raw(v, Fb, Ff);
+    if (v >= NE && v < 2 * NE) {
+      const int q = v - NE;
+      if (fix == 1 && !pure) { Fb = (Fb / sfb) * vol_b[q]; Ff = (Ff / sff) * vol_f[q]; }
+      if (fix == 2 && !pure) { Fb = ph[v] * vol_b[q]; Ff = ph[v] * vol_f[q]; }
+      mass_b[q] = Fb; mass_f[q] = Ff;
+    } else if (v >= 2 * NE && v < 3 * NE) {
+      const int q = v - 2 * NE;
+      if (fix == 1) { Fb = (Fb / sfb) * mass_b[q]; Ff = (Ff / sff) * mass_f[q]; }
+      if (fix == 2) { Fb = ph[v] * mass_b[q]; Ff = ph[v] * mass_f[q]; }
+    }
+    if (zb) Fb = 0.;
+    if (zf) Ff = 0.;
+    const double Ff_l = __shfl_up_sync(FULL, Ff, 1);
+    const double pf = face_b ? Ff_l - Fb : 0.;  // face value: front flux of l-1 minus back flux of l
+    const double pf_r = __shfl_down_sync(FULL, pf, 1);
+    const double fB = face_b ? ondB * L * pf : 0.;
+    const double fF = face_f ? ondF * L_r * pf_r : 0.;
+    double sumf = 0., du = 0.;
+    if (FRONT_FIRST) {
+      if (face_f) { sumf += fF; du += 0.5 * fF * ondF; }
+      if (face_b) { sumf += fB; du += 0.5 * fB * ondB; }
+    } else {
+      if (face_b) { sumf += fB; du += 0.5 * fB * ondB; }
+      if (face_f) { sumf += fF; du += 0.5 * fF * ondF; }
+    }
+    uo[v] = u[v] - sumf;
+    if (v >= NE && v < 2 * NE) dual[v - NE] = du;
+  }
+  if (!out) return;
+  // truncation of tiny volumes, masses and energies, then the clip of
+  // negative masses and energies
+#pragma unroll
+  for (int q = 0; q < NE; ++q) {
+    if (uo[q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
+    if (uo[NE + q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
+    if (uo[2 * NE + q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
+    if (uo[NE + q] < 0.) uo[NE + q] = 0.;
+    if (uo[2 * NE + q] < 0.) uo[2 * NE + q] = 0.;
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) A.Uout[v * N + c] = uo[v];
+#pragma unroll
+  for (int q = 0; q < NE; ++q) F.mflux[q * N + c] = dual[q];
+}
+
+// ---------------------------------------------------------------------------
 // Third-order face value (Remap-ordre-3.cc:16-188: evaluate_grad,
 // evaluate_ystar, evaluate_fm / evaluate_fp, the TVD interval bound of
 // ComputeFluxOrdre3).  y[0..5], h[0..5]: values and widths of the cells

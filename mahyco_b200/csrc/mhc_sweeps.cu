@@ -38,6 +38,7 @@ void sweep_step_dn(Engine* e, Group& g, int D, int k) {
     case 2: cell_sweep<DIM, NE, 2>(e, g, D, k); break;
     case LIM_GEN: cell_sweep<DIM, NE, LIM_GEN>(e, g, D, k); break;
     case LIM_O3: cell_sweep<DIM, NE, LIM_O3>(e, g, D, k); break;
+    case LIM_PB: cell_sweep<DIM, NE, LIM_PB>(e, g, D, k); break;
     default: cell_sweep<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
   }
   switch (g.LIM) {

@@ -57,6 +57,11 @@ def test_rejects_options_outside_the_hot_path():
     p.projection_limiteur_id = 8                # no such limiter (TypesMahyco.h limiteur)
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p = mb.default_params()
+    p.projection_simple_pente = 1               # simple-pente without pente-borne: the reference stops
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.projection_pente_borne, p.ordre_projection = 1, 3   # pente-borne with the third-order remap
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p = mb.default_params()
     p.env[0].elasto_model = 1                   # elasto with the Euler remap
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p.with_projection, p.nb_env = 0, 2          # elasto with two environments
