@@ -143,6 +143,7 @@ typedef struct mhc_case_params {
   int projection_pente_borne_debar_fix; /* projection-pente-borne-debar-fix: 0, 1 (mean values) or 2 (cell values) */
   int projection_pente_borne_mixte;     /* projection-pente-borne-mixte: pure-neighbourhood fluxes */
   int projection_limiteur_pure_id;      /* projection-limiteur-pure-id: limiter of pure neighbourhoods */
+  int conservation_energie_totale;      /* conservation-energie-totale: kinetic energy lost by the remap back to internal energy */
 } mhc_case_params;
 
 #ifdef __cplusplus

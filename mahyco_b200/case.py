@@ -71,6 +71,7 @@ class CaseParams(C.Structure):
         ("projection_simple_pente", C.c_int),
         ("projection_pente_borne", C.c_int), ("projection_pente_borne_debar_fix", C.c_int),
         ("projection_pente_borne_mixte", C.c_int), ("projection_limiteur_pure_id", C.c_int),
+        ("conservation_energie_totale", C.c_int),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -250,8 +251,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         eul = _txt(rm, "is-euler-scheme", "Full", str)
         if eul != "Full":
             raise NotImplementedError("is-euler-scheme other than Full")
-        if _txt(rm, "conservation-energie-totale", False, _bool):
-            raise NotImplementedError("conservation-energie-totale")
+        p.conservation_energie_totale = int(_txt(rm, "conservation-energie-totale", False, _bool))
         p.projection_simple_pente = int(_txt(rm, "projection-simple-pente", False, _bool))
         p.projection_pente_borne = int(_txt(rm, "projection-pente-borne", False, _bool))
         p.projection_pente_borne_debar_fix = _txt(rm, "projection-pente-borne-debar-fix", 0, int)

@@ -279,6 +279,10 @@ PARITY_CASES = {
     "adi2d_water_air_pb_vanleer": (lambda: _pb(water_air(limiter=VANLEER, deltat_init=1e-6), 2, mixte=1), 80),
     "adi2d_sod_mono_pb_fix0": (lambda: _pb(sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=False, limiter=SUPERBEE,
                                                deltat_init=1e-3), 0), 80),
+    # conservation-energie-totale (RemapADIFinal.cc:320-344)
+    "adi2d_sedov_cet": (lambda: _cet(sedov(dim=2, n=(24, 24), deltat_init=1e-4)), 100),
+    "adi3d_bisod_superbee_cet": (lambda: _cet(sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True,
+                                                  limiter=SUPERBEE, deltat_init=1e-3)), 60),
     "adi2d_bisod_arithmeticG": (lambda: sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True, limiter=ARITHMETIC_G,
                                             deltat_init=1e-3), 80),
     "adi3d_bisod_z_ultrabeeG": (lambda: sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
@@ -288,6 +292,11 @@ PARITY_CASES = {
 
 def _order3(p: CaseParams) -> CaseParams:
     p.ordre_projection = 3
+    return p
+
+
+def _cet(p: CaseParams) -> CaseParams:
+    p.conservation_energie_totale = 1
     return p
 
 

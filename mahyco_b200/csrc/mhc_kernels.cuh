@@ -1073,7 +1073,7 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
 // ---------------------------------------------------------------------------
 template <int DIM, int NE>
 __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const mhc_case_params& P, const Fields& F,
-                                                          const double* Ufin, int bx) {
+                                                          const double* Ufin, const double* Udfin, int bx) {
   long long c = bx * (long long)CT + threadIdx.x;
   if (c >= M.ncell) return;
   const long long N = M.ncell;
@@ -1195,6 +1195,34 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
     if (r != r || ie != ie) st |= ST_NAN;
   }
   if (st) atomicOr(&F.s->status, st);
+  if (P.conservation_energie_totale) {
+    // kinetic energy lost by the dual projection back into the internal
+    // energy (RemapADIFinal.cc:320-344): 0.25 per node of the projected
+    // minus the reconstructed kinetic energy, in cell node order
+    int ci, cj, ck;
+    cell_ijk(M, c, ci, cj, ck);
+    const long long NN = M.nnode;
+    double delta = 0.;
+    for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+      int di, dj, dk;
+      local_node_offset(l, di, dj, dk);
+      const long long n = node_id(M, ci + di, cj + dj, DIM == 3 ? ck + dk : 0);
+      const double m = Udfin[3 * NN + n];
+      if (m != 0.) {
+        const double ec_proj = Udfin[4 * NN + n] / m;
+        const double vx = Udfin[n] / m, vy = Udfin[NN + n] / m, vz = Udfin[2 * NN + n] / m;
+        const double ec_rec = 0.5 * (vx * vx + vy * vy + vz * vz);
+        delta += 0.25 * (ec_proj - ec_rec);
+      }
+    }
+    delta = smax(0., delta);
+    for (int q = 0; q < NE; ++q) {
+      if (!((nm >> q) & 1)) continue;
+      if (pure) eg += mfg * delta;
+      else ee[q] += mfe[q] * delta;
+    }
+    if (!pure) eg += delta;
+  }
   // applyEOS per environment, then computePressionMoyenne
   double pg = 0., cg = 0., pe[NE], ce[NE];
   for (int q = 0; q < NE; ++q) { pe[q] = ce[q] = 0.; }

@@ -257,7 +257,8 @@ __global__ void __launch_bounds__(CT, MHC_FIN_MIN_BLOCKS) kb_remap_finalize_cell
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_remap_finalize_cells<DIM, NE>(M, *C[wi.c].P, F, (K & 1) ? F.U[1] : F.U[0], wi.x);
+    body_remap_finalize_cells<DIM, NE>(M, *C[wi.c].P, F, (K & 1) ? F.U[1] : F.U[0],
+                                       ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
   }
 }
 

@@ -1862,6 +1862,29 @@ static int remap_variables(Case& C) {
       for (int e = 0; e < ne; ++e)
         if (C.has(c, e)) C.EV(C.cell_volume, e, c) = C.EV(C.fracvol, e, c) * C.cell_volume.g[c];
   }
+  if (C.P.conservation_energie_totale) {
+    /* kinetic energy lost by the dual projection goes back into the
+     * internal energy (RemapADIFinal.cc:320-344): 0.25 per node of the
+     * difference between the projected and the reconstructed kinetic
+     * energy, in cell node order */
+    for (long c = 0; c < C.ncell; ++c) {
+      double delta = 0.;
+      for (int l = 0; l < C.nbn; ++l) {
+        const long n = C.cnode(c, l);
+        const double* U = &C.u_dual[n * 5];
+        if (U[3] != 0.) {
+          const double ec_proj = U[4] / U[3];
+          const R3 v = C.vel[n];
+          const double ec_rec = 0.5 * (v.x * v.x + v.y * v.y + v.z * v.z);
+          delta += 0.25 * (ec_proj - ec_rec);
+        }
+      }
+      delta = std::max(0., delta);
+      for (int e = 0; e < ne; ++e)
+        if (C.has(c, e)) C.EV(C.internal_energy, e, c) += C.EV(C.mass_fraction, e, c) * delta;
+      if (!C.pure(c)) C.internal_energy.g[c] += delta;
+    }
+  }
   return ST_OK;
 }
 

@@ -77,8 +77,8 @@ def test_anti_hourglass_and_elasto_options(tmp_path):
 
 def test_remap_order_and_generalised_limiter_options(tmp_path):
     """ordre-projection 3, the generalised limiters (ids 3-7), the
-    pente-borne options and projection-simple-pente are read;
-    conservation-energie-totale is refused."""
+    pente-borne options, projection-simple-pente and
+    conservation-energie-totale are read."""
     text = open(ARC).read().replace("<ordre-projection>2</ordre-projection>",
                                     "<ordre-projection>3</ordre-projection>").replace(
         "<projection-limiteur-id>1</projection-limiteur-id>",
@@ -101,5 +101,4 @@ def test_remap_order_and_generalised_limiter_options(tmp_path):
     r = tmp_path / "cet.arc"
     r.write_text(text.replace("<ordre-projection>3</ordre-projection>",
                               "<conservation-energie-totale>true</conservation-energie-totale>"))
-    with pytest.raises(NotImplementedError):
-        read_arc(str(r))
+    assert read_arc(str(r))[0].conservation_energie_totale == 1
