@@ -60,7 +60,7 @@ int engine_rebuild(Engine* e) {
   }
   if (nc) CK(cudaMemcpyAsync(e->d_desc, desc.data(), nc * sizeof(CaseDesc), cudaMemcpyHostToDevice, e->stream));
   // groups
-  std::map<std::tuple<int, int, int, int, int, int, int, int, int>, int> gidx;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
@@ -68,12 +68,13 @@ int engine_rebuild(Engine* e) {
     int sens = (int)((h->it_host - 1) % h->DIM);
     const int el = case_elasto(h) ? 1 : 0, hg = case_hourglass(h) ? 1 : 0;
     const int lim = node_sweep_mode(h->P), clim = cell_sweep_mode(h->P);
-    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim);
+    const int cols = cols_mask(h), ncols = node_cols_mask(h);
+    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols);
     auto it = gidx.find(key);
     if (it == gidx.end()) {
       Group g;
       g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
-      g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim;
+      g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim; g.COLS = cols; g.NCOLS = ncols;
       gidx[key] = (int)e->groups.size();
       e->groups.push_back(g);
       it = gidx.find(key);
@@ -105,8 +106,9 @@ int engine_rebuild(Engine* e) {
     bool ok = phase(g.init_cells, PH_CELLS) && phase(g.init_nodes, PH_NODES) && phase(g.lag_cells, PH_CELLS) &&
               phase(g.fin_cells, PH_CELLS) && phase(g.fin_nodes, PH_NODES) && phase(g.dt, PH_CELLS) &&
               phase(g.lag_nodes, PH_NODES);
-    const int phc = g.CLIM == LIM_O3 ? PH_SWCW0 : PH_SWC0, phn = g.LIM == LIM_GEN ? PH_SWNW0 : PH_SWN0;
-    for (int D = 0; D < g.DIM; ++D) ok = ok && phase(g.sw_cells[D], phc + D) && phase(g.sw_nodes[D], phn + D);
+    for (int D = 0; D < g.DIM; ++D)
+      ok = ok && phase(g.sw_cells[D], cell_sweep_phase(((g.COLS >> D) & 1) ? LIM_COLS + g.CLIM : g.CLIM, D)) &&
+           phase(g.sw_nodes[D], node_sweep_phase(((g.NCOLS >> D) & 1) ? LIM_COLS + g.LIM : g.LIM, D));
     if (!ok) return set_err(MHC_ERR_ARG, "more than 2^31 blocks in one phase of a batch");
   }
   if (ints.size() > e->ints_cap) {

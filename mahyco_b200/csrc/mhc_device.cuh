@@ -210,6 +210,9 @@ constexpr int LIM_ORDER1 = 3;
 constexpr int LIM_GEN = 4;
 constexpr int LIM_O3 = 5;
 constexpr int LIM_PB = 6;
+// LIM_COLS + (0-2 or LIM_ORDER1): the same cell sweep along y / z with one
+// thread per line chunk (body_sweep_cells_cols), for large meshes
+constexpr int LIM_COLS = 8;
 
 // RemapADIService::fluxLimiterG (UtilesRemap.cc:130-190): limited slope from
 // the back / front gradients gm / gp, the values ym, yp of the neighbours

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <string>
 #include <vector>
@@ -70,6 +71,8 @@ struct Group {
   int EL = 0, HG = 0;          // elasto-plastic model; anti-hourglass correction
   int LIM = 0;                 // node-sweep instance: limiter 0-2, LIM_ORDER1 or LIM_GEN
   int CLIM = 0;                // cell-sweep instance: the same, LIM_O3 (third order) or LIM_PB (pente-borne)
+  int COLS = 0;                // bit D: the classical cell sweep along D uses one thread per line chunk
+  int NCOLS = 0;               // bit D: the same for the node sweep
   long long it0;               // iteration of the members when the lists were built
   std::vector<int> members;
   DevList init_cells, init_nodes, lag_nodes, lag_cells, fin_cells, fin_nodes, dt;
@@ -141,6 +144,39 @@ inline int node_sweep_mode(const mhc_case_params& P) {
 inline int cell_sweep_mode(const mhc_case_params& P) {
   if (P.projection_pente_borne) return LIM_PB;
   return P.ordre_projection == 3 ? LIM_O3 : node_sweep_mode(P);
+}
+
+// Directions whose classical cell sweep runs one thread per line chunk
+// (body_sweep_cells_cols): coalesced but with one line chunk per thread, it
+// pays when the sweep has enough line chunks to fill the device many times
+// over (large meshes); smaller meshes keep the warp-per-line layout.  The
+// threshold (line chunks of the sweep) can be changed with the environment
+// variable MHC_SWEEP_COLS_MIN_THREADS, read when the launch lists are built
+// (0: every y / z sweep in this layout).
+inline long long cols_min_threads() {
+  const char* s = getenv("MHC_SWEEP_COLS_MIN_THREADS");
+  if (s && *s) return atoll(s);
+  return 1LL << 18;
+}
+inline int cols_mask(const mhc_case* h) {
+  if (cell_sweep_mode(h->P) > LIM_ORDER1) return 0;
+  const long long lim = cols_min_threads();
+  int m = 0;
+  for (int D = 1; D < h->DIM; ++D) {
+    const int nd = D == 1 ? h->M.ncy : h->M.ncz, nb = D == 1 ? h->M.ncz : h->M.ncy;
+    if ((long long)h->M.ncx * nb * col_chunks(nd) >= lim) m |= 1 << D;
+  }
+  return m;
+}
+inline int node_cols_mask(const mhc_case* h) {
+  if (node_sweep_mode(h->P) > LIM_ORDER1) return 0;
+  const long long lim = cols_min_threads();
+  int m = 0;
+  for (int D = 1; D < h->DIM; ++D) {
+    const int nd = D == 1 ? h->M.nny : h->M.nnz, nb = D == 1 ? h->M.nnz : h->M.nny;
+    if ((long long)h->M.nnx * nb * col_chunks(nd) >= lim) m |= 1 << D;
+  }
+  return m;
 }
 
 inline int skip_mask(const mhc_case* h) {

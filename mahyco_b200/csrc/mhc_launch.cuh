@@ -32,8 +32,18 @@ enum PhaseKind {
   PH_SWC0 = 3,       // cell sweep along D = PH - PH_SWC0
   PH_SWN0 = 6,       // node sweep along D = PH - PH_SWN0
   PH_SWCW0 = 9,      // cell sweep with the wide (third-order) stencil
-  PH_SWNW0 = 12      // node sweep with the wide (generalised limiter) stencil
+  PH_SWNW0 = 12,     // node sweep with the wide (generalised limiter) stencil
+  PH_SWCC0 = 15,     // cell sweep along D = 1, 2, one thread per line chunk
+  PH_SWNC0 = 18      // node sweep along D = 1, 2, one thread per line chunk
 };
+
+// phase of the cell sweep along D for a cell-sweep instance
+__host__ __device__ constexpr int cell_sweep_phase(int lim, int D) {
+  return (D > 0 && lim >= LIM_COLS) ? PH_SWCC0 + D : (lim == LIM_O3 ? PH_SWCW0 : PH_SWC0) + D;
+}
+__host__ __device__ constexpr int node_sweep_phase(int lim, int D) {
+  return (D > 0 && lim >= LIM_COLS) ? PH_SWNC0 + D : (lim == LIM_GEN ? PH_SWNW0 : PH_SWN0) + D;
+}
 
 __host__ __device__ inline int cdiv_i(long long a, int b) { return (int)((a + b - 1) / b); }
 
@@ -43,6 +53,20 @@ __host__ __device__ inline void phase_grid(int ph, const Mesh& M, int& gx, int& 
   gy = gz = 1;
   if (ph == PH_CELLS) { gx = cdiv_i(M.ncell, CT); return; }
   if (ph == PH_NODES) { gx = cdiv_i(M.nnode, CT); return; }
+  if (ph >= PH_SWNC0) {  // body_sweep_nodes_cols
+    const int D = ph - PH_SWNC0;
+    const int nb = D == 1 ? M.nnz : M.nny, nd = D == 1 ? M.nny : M.nnz;
+    gx = cdiv_i((long long)M.nnx * nb, SW_THREADS);
+    gy = col_chunks(nd);
+    return;
+  }
+  if (ph >= PH_SWCC0) {  // body_sweep_cells_cols
+    const int D = ph - PH_SWCC0;
+    const int nb = D == 1 ? M.ncz : M.ncy, nd = D == 1 ? M.ncy : M.ncz;
+    gx = cdiv_i((long long)M.ncx * nb, SW_THREADS);
+    gy = col_chunks(nd);
+    return;
+  }
   // lane layout of mhc_sweep.cuh (sweep_lane)
   const bool wide = ph >= PH_SWCW0;
   const int base = wide ? (ph >= PH_SWNW0 ? PH_SWNW0 : PH_SWCW0) : (ph >= PH_SWN0 ? PH_SWN0 : PH_SWC0);
@@ -185,11 +209,15 @@ __global__ void __launch_bounds__(CT) kb_hourglass(const CaseDesc* __restrict__ 
 
 // the generalised-limiter and third-order instances hold more state per
 // lane and are asked for fewer resident blocks
+#ifndef MHC_SW_MIN_BLOCKS_COLS
+#define MHC_SW_MIN_BLOCKS_COLS 2
+#endif
 template <int DIM, int NE, int D, int LIM>
-__global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_GEN ? 2 : MHC_SW_MIN_BLOCKS_CELLS)
+__global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_COLS ? MHC_SW_MIN_BLOCKS_COLS
+                                              : (LIM >= LIM_GEN ? 2 : MHC_SW_MIN_BLOCKS_CELLS))
 kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
-    const WorkItem wi = item_at<(LIM == LIM_O3 ? PH_SWCW0 : PH_SWC0) + D>(C, L, w_);
+    const WorkItem wi = item_at<cell_sweep_phase(LIM, D)>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -204,17 +232,23 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     // EstMixte / EstPure are zero before the first remap of the run
     A.first_remap = k == 0 && F.s->iteration == 1;
     const Mesh M = C[wi.c].M;
-    if constexpr (LIM == LIM_O3) body_sweep_cells_o3<DIM, NE, D>(M, F, A, wi.x, wi.y);
+    if constexpr (LIM >= LIM_COLS && D > 0) body_sweep_cells_cols<DIM, NE, D, LIM - LIM_COLS>(M, F, A, wi.x, wi.y);
+    else if constexpr (LIM >= LIM_COLS) body_sweep_cells_lanes<DIM, NE, D, LIM - LIM_COLS>(M, F, A, wi.x, wi.y);
+    else if constexpr (LIM == LIM_O3) body_sweep_cells_o3<DIM, NE, D>(M, F, A, wi.x, wi.y);
     else if constexpr (LIM == LIM_PB) body_sweep_cells_pb<DIM, NE, D>(M, F, P, A, wi.x, wi.y);
     else body_sweep_cells_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
   }
 }
 
+#ifndef MHC_SW_MIN_BLOCKS_NODECOLS
+#define MHC_SW_MIN_BLOCKS_NODECOLS 2
+#endif
 template <int DIM, int NE, int D, int LIM>
-__global__ void __launch_bounds__(SW_THREADS, LIM == LIM_GEN ? 4 : MHC_SW_MIN_BLOCKS_NODES)
+__global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_COLS ? MHC_SW_MIN_BLOCKS_NODECOLS
+                                              : (LIM == LIM_GEN ? 4 : MHC_SW_MIN_BLOCKS_NODES))
 kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   MHC_FOR_ITEMS(L) {
-    const WorkItem wi = item_at<(LIM == LIM_GEN ? PH_SWNW0 : PH_SWN0) + D>(C, L, w_);
+    const WorkItem wi = item_at<node_sweep_phase(LIM, D)>(C, L, w_);
     Fields F = C[wi.c].F;
     if (!case_active(F)) continue;
     resolve_positions(F);
@@ -240,7 +274,9 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     A.limiter = P.projection_limiteur_id;
     A.simple_pente = P.projection_simple_pente;
     A.done_dirs = done;
-    body_sweep_nodes_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
+    if constexpr (LIM >= LIM_COLS && D > 0) body_sweep_nodes_cols<DIM, NE, D, LIM - LIM_COLS>(M, F, A, wi.x, wi.y);
+    else if constexpr (LIM >= LIM_COLS) body_sweep_nodes_lanes<DIM, NE, D, LIM - LIM_COLS>(M, F, A, wi.x, wi.y);
+    else body_sweep_nodes_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
   }
 }
 

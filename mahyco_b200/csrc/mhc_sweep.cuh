@@ -899,6 +899,139 @@ __device__ __forceinline__ void body_sweep_cells_o3(const Mesh& M, const Fields&
 }
 
 // ---------------------------------------------------------------------------
+// Cell sweep along D = 1, 2, classical limiters and first order, with one
+// thread per line: the threads of a warp hold consecutive x columns, so
+// every load and store is coalesced, and each thread walks a chunk of its
+// line in order with the stencil carried in registers.  Iteration q loads
+// cell q and the node plane in front of it; it completes the face gradient
+// of face q, the limited gradient of cell q-1, the value of face q-1 and the
+// update of cell q-2.  A chunk writes cells [o0, o1) and starts two cells
+// before o0.  Same arithmetic, in the same order, as
+// body_sweep_cells_lanes.
+// ---------------------------------------------------------------------------
+constexpr int SWC_CHUNK = 16;   // cells written per thread at most
+
+// chunks of a line of nd cells, and the cells [o0, o1) of chunk ch
+__host__ __device__ inline int col_chunks(int nd) { return (nd + SWC_CHUNK - 1) / SWC_CHUNK; }
+__host__ __device__ inline void col_chunk_range(int nd, int ch, int& o0, int& o1) {
+  const int n = col_chunks(nd);
+  const int len = (nd + n - 1) / n;
+  o0 = ch * len;
+  o1 = o0 + len < nd ? o0 + len : nd;
+}
+
+template <int DIM, int NE, int D, int LIM>
+__device__ __forceinline__ void body_sweep_cells_cols(const Mesh& M, const Fields& F, const SweepArgs& A, int vbx,
+                                                      int vby) {
+  static_assert(D >= 1, "x sweeps use the lane layout");
+  constexpr int NV = 3 * NE + 1;
+  constexpr int NQ = DIM == 3 ? 4 : 2;
+  const long long N = M.ncell;
+  const int nd = D == 1 ? M.ncy : M.ncz;
+  const int nb = D == 1 ? M.ncz : M.ncy;           // slow transverse extent
+  const long long col = (long long)vbx * SW_THREADS + threadIdx.x;
+  if (col >= (long long)M.ncx * nb) return;
+  const int i = (int)(col % M.ncx), tb = (int)(col / M.ncx);
+  int o0, o1;
+  col_chunk_range(nd, vby, o0, o1);
+  if (o0 >= o1) return;
+  const double dt = F.s->dt;
+  const int order2 = LIM == LIM_ORDER1 ? 0 : 1;  // ordre-projection - 1
+  const double* __restrict__ Uin = A.Uin;
+  // transverse parts of the initial outer normals (grid formula)
+  constexpr int A0 = 0, A1 = D == 2 ? 1 : 2;
+  const double t0 = fc0_comp<DIM, D, A0>(M, i) - cc0_comp<DIM, A0>(M, i);
+  const double t1 = fc0_comp<DIM, D, A1>(M, tb) - cc0_comp<DIM, A1>(M, tb);
+  auto cell_at = [&](int p) -> long long { return D == 1 ? cell_id(M, i, p, tb) : cell_id(M, i, tb, p); };
+  auto plane_at = [&](int p, Plane<DIM>& P) {
+    if (D == 1) load_plane<DIM, D>(M, F, i, p, tb, P);
+    else load_plane<DIM, D>(M, F, i, tb, p, P);
+  };
+  // carried state: 1 = previous cell / face, 2 = the one before
+  double phi1[NV], phi2[NV], gf1[NV], gr2[NV], pf2[NV];
+  double xc1 = 0., xc2 = 0., fc1 = 0., un1 = 0., un2 = 0., L1 = 0., L2 = 0.;
+  const int qs = o0 - 2 > 0 ? o0 - 2 : 0;
+  Plane<DIM> cur;       // back plane of cell q
+  plane_at(qs, cur);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) phi1[v] = phi2[v] = gf1[v] = gr2[v] = pf2[v] = 0.;
+  for (int q = qs; q <= o1 + 1; ++q) {
+    const bool cell = q < nd;                 // a cell is loaded at q
+    double phi[NV], xc = 0.;
+    Plane<DIM> nxt;
+    if (cell) {
+      plane_at(q + 1, nxt);
+      xc = centre_from_planes<DIM, D>(cur, nxt);
+      const long long c = cell_at(q);
+      double u[NV], den;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = __ldg(Uin + v * N + c);
+      if (A.first) {
+        den = __ldg(F.V + c);
+      } else {
+        den = 0.;
+#pragma unroll
+        for (int e = 0; e < NE; ++e) den += u[e];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) phi[v] = div_rn(u[v], den);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) phi[v] = 0.;
+    }
+    const bool face_q = cell && q > 0;        // face q (between q-1 and q) is inner
+    const double dx = xc - xc1;
+    const bool face_q1 = q - 1 > 0 && q - 1 < nd;  // face q-1 is inner
+    // face q-1 upwind test (its normal velocity and the centres of q-2, q-1)
+    const bool up_left = un1 * (xc1 - xc2) > 0.0;
+    double pf1[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double gf = face_q ? div_rn(phi[v] - phi1[v], dx) : 0.;
+      // limited gradient of cell q-1 from its back (gf1) and front (gf) faces
+      const double gr1 = (LIM != LIM_ORDER1 && q - 1 >= 0 && q - 1 < nd) ? limited_gradient_t<LIM>(gf1[v], gf) : 0.;
+      pf1[v] = 0.;
+      if (face_q1)
+        pf1[v] = up_left ? phi2[v] + order2 * (fc1 - xc2) * gr2[v] : phi1[v] + order2 * (fc1 - xc1) * gr1;
+      gf1[v] = gf;
+      gr2[v] = gr1;
+    }
+    // update of cell o = q - 2 from faces o (pf2) and o + 1 (pf1)
+    const int o = q - 2;
+    if (o >= o0 && o < o1) {
+      const long long c = cell_at(o);
+      const double cc0 = cc0_comp<DIM, D>(M, o);
+      const double ondB = unit_comp<D>(fc0_comp<DIM, D, D>(M, o) - cc0, t0, t1);
+      const double ondF = unit_comp<D>(fc0_comp<DIM, D, D>(M, o + 1) - cc0, t0, t1);
+      const bool fb = o > 0, ff = o + 1 < nd;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double fB = fb ? ondB * un2 * L2 * dt * pf2[v] : 0.;
+        const double fF = ff ? ondF * un1 * L1 * dt * pf1[v] : 0.;
+        double sumf = 0., dual = 0.;
+        if (fb) { sumf += fB; dual += 0.5 * fB * ondB; }
+        if (ff) { sumf += fF; dual += 0.5 * fF * ondF; }
+        double uo = __ldg(Uin + v * N + c) - sumf;
+        if (v >= NE && v < 3 * NE && uo < 0.) uo = 0.;  // masses and energies stay >= 0
+        A.Uout[v * N + c] = uo;
+        if (v >= NE && v < 2 * NE) F.mflux[(v - NE) * N + c] = dual;
+      }
+    }
+    // shift
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      phi2[v] = phi1[v];
+      phi1[v] = phi[v];
+      pf2[v] = pf1[v];
+    }
+    xc2 = xc1; xc1 = xc;
+    un2 = un1; L2 = L1;
+    un1 = cur.un; L1 = cur.L; fc1 = cur.fc;
+    if (cell) cur = nxt;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Node part: RemapADIService::computeDualUremap (DualPhaseRemap.cc:38-258,
 // classical limiter) with the same lane layout.  Lane l holds node
 // x0 - 2 + l along D; lanes 2 .. NOUT+1 write.  The mass flux through the
@@ -1069,6 +1202,159 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
     if (fabs(U[q]) < 1.e-300) U[q] = 0.;
 #pragma unroll
   for (int q = 0; q < 5; ++q) A.Uout[q * NN + n] = U[q];
+}
+
+// ---------------------------------------------------------------------------
+// Node sweep along D = 1, 2, classical limiters and first order, one thread
+// per line chunk (the layout of body_sweep_cells_cols).  Iteration q loads
+// node q; it completes the limited gradient of node q-1 and the update of
+// node q-2.  A chunk writes nodes [o0, o1) and starts two nodes before o0.
+// Same arithmetic, in the same order, as body_sweep_nodes_lanes.
+// ---------------------------------------------------------------------------
+// projected and phi values, position along D and front mass flux of node
+// (i, j, k) with index id along D
+template <int DIM, int NE, int D>
+__device__ __forceinline__ void node_state(const Mesh& M, const Fields& F, const DualArgs& A, int i, int j, int k,
+                                           int id, double (&U)[5], double (&ph)[4], double& x, double& ffm) {
+  const long long NN = M.nnode, N = M.ncell;
+  const long long n = node_id(M, i, j, k);
+  x = __ldg(F.Xn[D] + n);
+  bool was_inner = false;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+    if (((A.done_dirs >> d) & 1) && node_inner_dir(M, i, j, k, d)) was_inner = true;
+  if (A.Uin) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) U[q] = __ldg(A.Uin + q * NN + n);
+  } else {
+    const double mn = __ldg(F.mn + n), vx = __ldg(F.vx + n), vy = __ldg(F.vy + n), vz = __ldg(F.vz + n);
+    U[0] = mn * vx; U[1] = mn * vy; U[2] = mn * vz; U[3] = mn;
+    U[4] = 0.5 * mn * (vx * vx + vy * vy + vz * vz);
+  }
+  if (was_inner) {
+    ph[0] = div_rn(U[0], U[3]); ph[1] = div_rn(U[1], U[3]); ph[2] = div_rn(U[2], U[3]);
+    ph[3] = div_rn(U[4], U[3]);
+  } else {
+    const double vx = __ldg(F.vx + n), vy = __ldg(F.vy + n), vz = __ldg(F.vz + n);
+    ph[0] = vx; ph[1] = vy; ph[2] = vz;
+    ph[3] = 0.5 * (vx * vx + vy * vy + vz * vz);
+  }
+  ffm = 0.;
+  const int ndc = D == 1 ? M.ncy : M.ncz;
+  if (id < ndc) {
+    const double w = DIM == 2 ? .5 : .25;
+#pragma unroll
+    for (int b2 = 0; b2 < (DIM == 3 ? 2 : 1); ++b2) {
+#pragma unroll
+      for (int b1 = 0; b1 < 2; ++b1) {
+        int ci = i, cj = j, ck = k;
+        const int t1 = b1 - 1, t2 = b2 - 1;
+        if (D == 1) { ci += t1; ck += (DIM == 3 ? t2 : 0); }
+        else { ci += t1; cj += t2; }
+        if (ci < 0 || cj < 0 || ck < 0) continue;
+        if (ci >= M.ncx) continue;
+        if (D != 1 && cj >= M.ncy) continue;
+        if (DIM == 3 && D != 2 && ck >= M.ncz) continue;
+        const long long cf = cell_id(M, ci, cj, DIM == 3 ? ck : 0);
+#pragma unroll
+        for (int q = 0; q < NE; ++q) ffm += w * __ldg(F.mflux + q * N + cf);
+      }
+    }
+  }
+}
+
+template <int DIM, int NE, int D, int LIM>
+__device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Fields& F, const DualArgs& A, int vbx,
+                                                      int vby) {
+  static_assert(D >= 1, "x sweeps use the lane layout");
+  const long long NN = M.nnode;
+  const int nn = D == 1 ? M.nny : M.nnz;
+  const int nb = D == 1 ? M.nnz : M.nny;
+  const long long col = (long long)vbx * SW_THREADS + threadIdx.x;
+  if (col >= (long long)M.nnx * nb) return;
+  const int i = (int)(col % M.nnx), tb = (int)(col / M.nnx);
+  int o0, o1;
+  col_chunk_range(nn, vby, o0, o1);
+  if (o0 >= o1) return;
+  const double dt = F.s->dt;
+  const int order2 = LIM == LIM_ORDER1 ? 0 : A.order - 1;  // ordre-projection - 1
+  // carried state: 1 = node q-1, 2 = node q-2, 3 = node q-3
+  double U1[5], U2[5], ph1[4], ph2[4], ph3[4], g1[3], g2[3], g3[3];
+  double x1 = 0., x2 = 0., x3 = 0., ffm1 = 0., ffm2 = 0., ffm3 = 0.;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) U1[q] = U2[q] = 0.;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) ph1[q] = ph2[q] = ph3[q] = 0.;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) g1[q] = g2[q] = g3[q] = 0.;
+  const int qs = o0 - 2 > 0 ? o0 - 2 : 0;
+  for (int q = qs; q <= o1 + 1; ++q) {
+    double U[5] = {0., 0., 0., 0., 0.}, ph[4] = {0., 0., 0., 0.}, x = 0., ffm = 0.;
+    if (q < nn) {
+      if (D == 1) node_state<DIM, NE, D>(M, F, A, i, q, tb, q, U, ph, x, ffm);
+      else node_state<DIM, NE, D>(M, F, A, i, tb, q, q, U, ph, x, ffm);
+    }
+    // limited gradients of node q-1 (inner nodes only)
+    const int m = q - 1;
+    double gm[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      gm[c] = 0.;
+      if (LIM != LIM_ORDER1 && m > 0 && m < nn - 1) {
+        const double gfw = div_rn(ph[c] - ph1[c], x - x1);
+        const double gbw = div_rn(ph1[c] - ph2[c], x1 - x2);
+        gm[c] = limited_gradient_t<LIM>(gbw, gfw);
+      }
+    }
+    // update of node o = q - 2: neighbours o-1 (3), o (2), o+1 (1)
+    const int o = q - 2;
+    if (o >= o0 && o < o1) {
+      const long long n = D == 1 ? node_id(M, i, o, tb) : node_id(M, i, tb, o);
+      double V[5];
+#pragma unroll
+      for (int c = 0; c < 5; ++c) V[c] = U2[c];
+      if (o > 0 && o < nn - 1) {
+        const double bfm = ffm3, ffm_o = ffm2;
+        V[3] += bfm - ffm_o;
+        double FV[3], BV[3], FE, BE;
+        {
+          const double ufront = 0.5 * (ph2[D] + ph1[D]);
+          const int signfront = (ufront > 0) ? 1 : -1;
+          const bool fr = ffm_o < 0.;
+          const double geo = (signfront * (x1 - x2) - dt * ufront);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) FV[c] = (fr ? ph1[c] : ph2[c]) + order2 * (0.5 * (fr ? gm[c] : g1[c]) * geo);
+          FE = (fr ? ph1[3] : ph2[3]) + order2 * (0.5 * 0. * geo);
+        }
+        {
+          const double uback = 0.5 * (ph3[D] + ph2[D]);
+          const int signback = (uback > 0) ? 1 : -1;
+          const bool bk = bfm > 0.;
+          const double geo = (signback * (x2 - x3) - dt * uback);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) BV[c] = (bk ? ph3[c] : ph2[c]) + order2 * (0.5 * (bk ? g2[c] : g1[c]) * geo);
+          BE = (bk ? ph3[3] : ph2[3]) + order2 * (0.5 * 0. * geo);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) V[c] += bfm * BV[c] - ffm_o * FV[c];
+        V[4] += bfm * BE - ffm_o * FE;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          if (fabs(V[c]) < 1.e-300) V[c] = 0.;
+      }
+#pragma unroll
+      for (int c = 0; c < 5; ++c) A.Uout[c * NN + n] = V[c];
+    }
+    // shift
+#pragma unroll
+    for (int c = 0; c < 5; ++c) { U2[c] = U1[c]; U1[c] = U[c]; }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) { ph3[c] = ph2[c]; ph2[c] = ph1[c]; ph1[c] = ph[c]; }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { g3[c] = g2[c]; g2[c] = g1[c]; g1[c] = gm[c]; }
+    x3 = x2; x2 = x1; x1 = x;
+    ffm3 = ffm2; ffm2 = ffm1; ffm1 = ffm;
+  }
 }
 
 }  // namespace mhc

@@ -32,7 +32,12 @@ void node_sweep(Engine* e, Group& g, int D, int k) {
 // one direction of the remap for a group: cell sweep, then node sweep
 template <int DIM, int NE>
 void sweep_step_dn(Engine* e, Group& g, int D, int k) {
-  switch (g.CLIM) {
+  const int cl = ((g.COLS >> D) & 1) ? LIM_COLS + g.CLIM : g.CLIM;
+  switch (cl) {
+    case LIM_COLS + 0: cell_sweep<DIM, NE, LIM_COLS + 0>(e, g, D, k); break;
+    case LIM_COLS + 1: cell_sweep<DIM, NE, LIM_COLS + 1>(e, g, D, k); break;
+    case LIM_COLS + 2: cell_sweep<DIM, NE, LIM_COLS + 2>(e, g, D, k); break;
+    case LIM_COLS + LIM_ORDER1: cell_sweep<DIM, NE, LIM_COLS + LIM_ORDER1>(e, g, D, k); break;
     case 0: cell_sweep<DIM, NE, 0>(e, g, D, k); break;
     case 1: cell_sweep<DIM, NE, 1>(e, g, D, k); break;
     case 2: cell_sweep<DIM, NE, 2>(e, g, D, k); break;
@@ -41,7 +46,12 @@ void sweep_step_dn(Engine* e, Group& g, int D, int k) {
     case LIM_PB: cell_sweep<DIM, NE, LIM_PB>(e, g, D, k); break;
     default: cell_sweep<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
   }
-  switch (g.LIM) {
+  const int nl = ((g.NCOLS >> D) & 1) ? LIM_COLS + g.LIM : g.LIM;
+  switch (nl) {
+    case LIM_COLS + 0: node_sweep<DIM, NE, LIM_COLS + 0>(e, g, D, k); break;
+    case LIM_COLS + 1: node_sweep<DIM, NE, LIM_COLS + 1>(e, g, D, k); break;
+    case LIM_COLS + 2: node_sweep<DIM, NE, LIM_COLS + 2>(e, g, D, k); break;
+    case LIM_COLS + LIM_ORDER1: node_sweep<DIM, NE, LIM_COLS + LIM_ORDER1>(e, g, D, k); break;
     case 0: node_sweep<DIM, NE, 0>(e, g, D, k); break;
     case 1: node_sweep<DIM, NE, 1>(e, g, D, k); break;
     case 2: node_sweep<DIM, NE, 2>(e, g, D, k); break;

@@ -80,6 +80,22 @@ def test_parity_exact(name):
     assert not bad, (name, bad)
 
 
+# y / z cell sweeps in the one-thread-per-line-chunk layout (chosen by the
+# library for large meshes; forced here on the parity sizes)
+LINE_CHUNK_CASES = ["adi3d_bisod_superbee", "adi3d_sod_mono_y", "adi3d_bisod_z_vanleer", "adi2d_sedov",
+                    "adi3d_sedov", "adi2d_bisod_order1", "adi2d_water_air", "adi3d_bisod_newton"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", LINE_CHUNK_CASES)
+def test_parity_exact_line_chunk_layout(name, monkeypatch):
+    monkeypatch.setenv("MHC_SWEEP_COLS_MIN_THREADS", "0")
+    init_errs, errs = run_pair(name, cr_pow=True)
+    assert max(init_errs.values()) == 0.0, init_errs
+    bad = {k: v for k, v in errs.items() if v != 0.0}
+    assert not bad, (name, bad)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(PARITY_CASES))
 def test_parity_reference_libm(name):
