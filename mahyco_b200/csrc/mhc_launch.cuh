@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(CT) kb_hourglass(const CaseDesc* __restrict__ 
 // the generalised-limiter and third-order instances hold more state per
 // lane and are asked for fewer resident blocks
 #ifndef MHC_SW_MIN_BLOCKS_COLS
-#define MHC_SW_MIN_BLOCKS_COLS 2
+#define MHC_SW_MIN_BLOCKS_COLS 3
 #endif
 template <int DIM, int NE, int D, int LIM>
 __global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_COLS ? MHC_SW_MIN_BLOCKS_COLS
@@ -241,7 +241,7 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
 }
 
 #ifndef MHC_SW_MIN_BLOCKS_NODECOLS
-#define MHC_SW_MIN_BLOCKS_NODECOLS 2
+#define MHC_SW_MIN_BLOCKS_NODECOLS 3
 #endif
 template <int DIM, int NE, int D, int LIM>
 __global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_COLS ? MHC_SW_MIN_BLOCKS_NODECOLS
