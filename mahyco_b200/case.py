@@ -169,15 +169,20 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     """Parse a MaHyCo ``Donnees.arc`` into CaseParams.
 
     Returns ``(params, info)`` where ``info`` holds environment names, the
-    time loop and anything the hot path ignores.  Unsupported options that
-    change the cycle (CSTS scheme, pente-borne remap, elasto models, energy
-    deposits, non-velocity boundary conditions) raise ``NotImplementedError``.
+    time loop, the post-processed and EnvSummation variable lists and
+    anything the hot path ignores.  Unsupported options that change the cycle
+    (CSTS scheme, sans-lagrange, elasto models other than DefaultModel,
+    energy deposits, non-velocity boundary conditions) raise
+    ``NotImplementedError``.
     """
     root = ET.parse(path).getroot()
     p = default_params()
     info: dict = {"env_names": [], "timeloop": None}
     tl = root.find("arcane/timeloop")
     info["timeloop"] = tl.text.strip() if tl is not None else "MahycoLoop"
+    # post-processed variables (Ensight) and EnvSummation variables
+    info["output_vars"] = [v.text.strip() for v in root.findall("arcane-post-processing/output/variable")]
+    info["history_vars"] = [v.text.strip() for v in root.findall("time-history/bilan/variable")]
     cart = root.find("mesh/meshgenerator/cartesian")
     if cart is None:
         raise NotImplementedError("only the cartesian mesh generator is supported")

@@ -18,12 +18,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from mahyco_b200.case import read_arc, params_to_dict  # noqa: E402
+sys.path.insert(0, os.path.dirname(HERE))
+import ensight_digest  # noqa: E402
 
 # case -> extra oracle switches needed to reproduce how the reference ran it
 CASES = {
     "CAS_2D_Lag_SodCaseX": {},
     "CAS_2D_Lag_SodCaseX_newton": {},
-    "CAS_2D_Lag_BiSodCaseX": {},
+    "CAS_2D_Lag_BiSodCaseX": {"mpi_ranks": 4},
     "CAS_Lag_BiSodCaseX": {},
     "CAS_BiSodCaseX": {},
     # seq_pr test: 10 iterations, then a restart (launch_test.sh:25-38)
@@ -62,8 +64,20 @@ def main(ref_root="/root/reference"):
                     continue
                 rows = [[float(x) for x in line.split()] for line in open(fn) if line.strip()]
                 hist[f"{v}_{env}"] = rows
+        # digests of the reference's final Ensight files (6 significant
+        # digits, round-off noise removed: tests/ensight_digest.py), compared
+        # with the files mahyco_b200.output writes; a multi-rank reference
+        # run writes only its first sub-domain, so none are kept for those
+        dep = os.path.join(d, "output", "depouillement")
+        digests = {}
+        if extra.get("mpi_ranks", 1) == 1:
+            for root, _, files in os.walk(dep):
+                for fn in sorted(files):
+                    full = os.path.join(root, fn)
+                    digests[os.path.relpath(full, dep)] = ensight_digest.digest(full)
         out = {"case": case, "params": params_to_dict(p), "env_names": info["env_names"],
-               "timeloop": info["timeloop"], "extra": extra, "time_history": hist}
+               "timeloop": info["timeloop"], "extra": extra, "time_history": hist,
+               "output_vars": info["output_vars"], "ensight_sha256": digests}
         with open(os.path.join(HERE, case + ".json"), "w") as f:
             json.dump(out, f, indent=0)
         print(case, {k: len(v) for k, v in hist.items()})

@@ -102,3 +102,16 @@ def test_remap_order_and_generalised_limiter_options(tmp_path):
     r.write_text(text.replace("<ordre-projection>3</ordre-projection>",
                               "<conservation-energie-totale>true</conservation-energie-totale>"))
     assert read_arc(str(r))[0].conservation_energie_totale == 1
+
+
+def test_gnuplot_writer_format(tmp_path):
+    """EnvSummation curves in the reference's layout: <Var>_<Env>, one
+    'time value' line, 17 significant digits; absent environments skipped."""
+    import numpy as np
+    from mahyco_b200.output import write_gnuplot
+    rows = np.array([[1.2577892535548833e-04, 2.5, 1.0, 0.9999974710589157, 3.0, 1.0, 0., 0., 0., 0., 0.]])
+    files = write_gnuplot(str(tmp_path), ["ZG", "ZD"], rows)
+    assert sorted(os.path.basename(f) for f in files) == ["CellMass_ZG", "Density_ZG", "InternalEnergy_ZG",
+                                                          "Pressure_ZG"]
+    assert open(tmp_path / "courbes" / "gnuplot" / "Density_ZG").read() == \
+        "1.2577892535548833E-04 9.9999747105891568E-01\n"
