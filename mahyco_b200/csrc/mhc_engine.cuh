@@ -150,13 +150,20 @@ inline int cell_sweep_mode(const mhc_case_params& P) {
 // (body_sweep_cells_cols): coalesced but with one line chunk per thread, it
 // pays when the sweep has enough line chunks to fill the device many times
 // over (large meshes); smaller meshes keep the warp-per-line layout.  The
-// threshold (line chunks of the sweep) can be changed with the environment
-// variable MHC_SWEEP_COLS_MIN_THREADS, read when the launch lists are built
-// (0: every y / z sweep in this layout).
+// node sweep, with fewer registers per line, pays from a quarter of that.
+// The thresholds (line chunks of the sweep) can be changed with the
+// environment variables MHC_SWEEP_COLS_MIN_THREADS (cells) and
+// MHC_SWEEP_NODE_COLS_MIN_THREADS (nodes; default: the cell threshold / 4),
+// read when the launch lists are built (0: every y / z sweep in this layout).
 inline long long cols_min_threads() {
   const char* s = getenv("MHC_SWEEP_COLS_MIN_THREADS");
   if (s && *s) return atoll(s);
   return 1LL << 18;
+}
+inline long long node_cols_min_threads() {
+  const char* s = getenv("MHC_SWEEP_NODE_COLS_MIN_THREADS");
+  if (s && *s) return atoll(s);
+  return cols_min_threads() / 4;
 }
 inline int cols_mask(const mhc_case* h) {
   if (cell_sweep_mode(h->P) > LIM_ORDER1) return 0;
@@ -170,7 +177,7 @@ inline int cols_mask(const mhc_case* h) {
 }
 inline int node_cols_mask(const mhc_case* h) {
   if (node_sweep_mode(h->P) > LIM_ORDER1) return 0;
-  const long long lim = cols_min_threads();
+  const long long lim = node_cols_min_threads();
   int m = 0;
   for (int D = 1; D < h->DIM; ++D) {
     const int nd = D == 1 ? h->M.nny : h->M.nnz, nb = D == 1 ? h->M.nnz : h->M.nny;
