@@ -38,6 +38,10 @@ enum mhc_bc_kind {
   MHC_BC_VX = 0, MHC_BC_VY = 1, MHC_BC_VZ = 2
 };
 
+/* energy deposits (TypesMahyco.h eEnergyDepot): constant or linear in
+ * position and time; the super-Gaussian deposit is not supported */
+enum mhc_depot { MHC_DEPOT_NONE = 0, MHC_DEPOT_CONSTANT = 1, MHC_DEPOT_LINEAIRE = 2 };
+
 /* boundary surfaces built by MahycoModule::PrepareFaceGroup (MahycoAnnexe.cc:149-235) */
 enum mhc_surface {
   MHC_XMIN = 0, MHC_YMIN = 1, MHC_ZMIN = 2, MHC_XMAX = 3, MHC_YMAX = 4, MHC_ZMAX = 5
@@ -94,6 +98,15 @@ typedef struct mhc_env_params {
   int rotation_order;
   double shear_modulus;
   double yield_strength;
+  /* energy-depot (MahycoModule.cc:1364-1417), added to the environment's
+   * internal energy before the energy update: mhc_depot kind, value,
+   * origine, dependanceX/Y/Z/T, cutoffX/Y, Tdebut, Tfin */
+  int depot_type;
+  double depot_value;
+  double depot_origin[3];
+  double depot_dependance[4];
+  double depot_cutoff[2];
+  double depot_tdebut, depot_tfin;
 } mhc_env_params;
 
 typedef struct mhc_bc {

@@ -25,6 +25,7 @@ LENGTHS = {"racine-cubique-volume": 0, "faces-opposees": 1, "monodimX": 2,
            "monodimY": 3, "monodimZ": 4}
 MINMOD, SUPERBEE, VANLEER = 0, 1, 2
 MINMOD_G, SUPERBEE_G, VANLEER_G, ARITHMETIC_G, ULTRABEE_G = 3, 4, 5, 6, 7
+DEPOT_NONE, DEPOT_CONSTANT, DEPOT_LINEAIRE = 0, 1, 2
 
 
 class EnvParams(C.Structure):
@@ -42,6 +43,9 @@ class EnvParams(C.Structure):
         ("vitesse_initiale", C.c_double * 3),
         ("elasto_model", C.c_int), ("rotation_order", C.c_int),
         ("shear_modulus", C.c_double), ("yield_strength", C.c_double),
+        ("depot_type", C.c_int), ("depot_value", C.c_double), ("depot_origin", C.c_double * 3),
+        ("depot_dependance", C.c_double * 4), ("depot_cutoff", C.c_double * 2),
+        ("depot_tdebut", C.c_double), ("depot_tfin", C.c_double),
     ]
 
 
@@ -101,6 +105,11 @@ def env_defaults(e: EnvParams, eos: int = EOS_PERFECT_GAS) -> None:
     e.vitesse_initiale[:] = (0.0, 0.0, 0.0)
     e.elasto_model, e.rotation_order = 0, 1
     e.shear_modulus, e.yield_strength = 2.94e10, 3.0e8
+    e.depot_type, e.depot_value = DEPOT_NONE, 0.0
+    e.depot_origin[:] = (0.0, 0.0, 0.0)
+    e.depot_dependance[:] = (0.0, 0.0, 0.0, 0.0)
+    e.depot_cutoff[:] = (1000.0, 1000.0)
+    e.depot_tdebut, e.depot_tfin = 0.0, 1000.0
 
 
 def default_params() -> CaseParams:
@@ -172,7 +181,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     time loop, the post-processed and EnvSummation variable lists and
     anything the hot path ignores.  Unsupported options that change the cycle
     (CSTS scheme, sans-lagrange, elasto models other than DefaultModel,
-    energy deposits, non-velocity boundary conditions) raise
+    super-Gaussian energy deposits, non-velocity boundary conditions) raise
     ``NotImplementedError``.
     """
     root = ET.parse(path).getroot()
@@ -241,8 +250,19 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
                 e.shear_modulus = _txt(mu_el, "elastic-cst", 2.94e10)
             if y_el is not None:
                 e.yield_strength = _txt(y_el, "limit-elastic", 3.0e8)
-        if ev.find("energy-depot") is not None:
-            raise NotImplementedError("energy deposit")
+        dep = ev.find("energy-depot")
+        if dep is not None:
+            kind = _txt(dep, "type", "DepotConstant", str)
+            if kind not in ("DepotConstant", "DepotLineaire"):
+                raise NotImplementedError(f"energy deposit {kind}")
+            e.depot_type = DEPOT_CONSTANT if kind == "DepotConstant" else DEPOT_LINEAIRE
+            e.depot_value = _txt(dep, "valeur-source-energie", 0.0)
+            org = _txt(dep, "origine", "0. 0. 0.", str).split()
+            e.depot_origin[:] = [float(v) for v in org]
+            e.depot_dependance[:] = [_txt(dep, t, 0.0) for t in ("dependanceX", "dependanceY", "dependanceZ",
+                                                                  "dependanceT")]
+            e.depot_cutoff[:] = (_txt(dep, "cutoffX", 1000.0), _txt(dep, "cutoffY", 1000.0))
+            e.depot_tdebut, e.depot_tfin = _txt(dep, "Tdebut", 0.0), _txt(dep, "Tfin", 1000.0)
     cm = m.find("cas-model")
     p.cas_model = CASE_BY_NAME[cm.get("name")]
     p.cas_test = _txt(cm, "cas-test", 0, int)

@@ -279,6 +279,14 @@ PARITY_CASES = {
     "adi2d_water_air_pb_vanleer": (lambda: _pb(water_air(limiter=VANLEER, deltat_init=1e-6), 2, mixte=1), 80),
     "adi2d_sod_mono_pb_fix0": (lambda: _pb(sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=False, limiter=SUPERBEE,
                                                deltat_init=1e-3), 0), 80),
+    # energy deposits (MahycoModule.cc:1364-1417) with the explicit energy
+    # update that keeps them
+    "lag2d_sod_depot_constant": (lambda: _depot(sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=False, remap=False,
+                                                    deltat_max=1e-3, deltat_init=1e-4), 1), 120),
+    "lag3d_bisod_depot_lineaire": (lambda: _depot(sod(dim=3, n=(30, 4, 4), L=(1.0, 0.1, 0.1), bi=True, remap=False,
+                                                      deltat_max=1e-3, deltat_init=1e-4), 2), 100),
+    "adi2d_bisod_depot_constant": (lambda: _depot(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True,
+                                                      deltat_init=1e-3), 1), 60),
     # conservation-energie-totale (RemapADIFinal.cc:320-344)
     "adi2d_sedov_cet": (lambda: _cet(sedov(dim=2, n=(24, 24), deltat_init=1e-4)), 100),
     "adi3d_bisod_superbee_cet": (lambda: _cet(sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True,
@@ -292,6 +300,20 @@ PARITY_CASES = {
 
 def _order3(p: CaseParams) -> CaseParams:
     p.ordre_projection = 3
+    return p
+
+
+def _depot(p: CaseParams, kind: int) -> CaseParams:
+    """Deposit in environment 0 on a box around x = 0.3, from t = 2e-3."""
+    p.pression_explicite = 1
+    o = p.env[0]
+    o.depot_type = kind
+    o.depot_value = 40.0
+    o.depot_origin[:] = (0.3, 0.05, 0.0)
+    o.depot_cutoff[:] = (0.12, 0.04)
+    o.depot_tdebut, o.depot_tfin = 2e-3, 0.05
+    if kind == 2:
+        o.depot_dependance[:] = (15.0, -20.0, 5.0, 300.0)
     return p
 
 

@@ -962,6 +962,37 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
     ecur[0] = ecur[0] + w1;
     ecur[0] = ecur[0] + w2;
   }
+  // energy deposits (MahycoModule.cc:1364-1417): value x deltat at the
+  // Lagrangian cell centre of this iteration, before the energy update
+  bool depot = false;
+  for (int q = 0; q < NE; ++q) depot = depot || P.env[q].depot_type != MHC_DEPOT_NONE;
+  if (depot) {
+    R3 s = {0., 0., 0.};
+    for (int q = 0; q < NBN; ++q) {
+      int a, b, d;
+      local_node_offset(q, a, b, d);
+      const long long nn = node_id(M, i + a, j + b, DIM == 3 ? k + d : 0);
+      s = s + R3{F.Xn[0][nn], F.Xn[1][nn], DIM == 3 ? F.Xn[2][nn] : 0.};
+    }
+    const R3 cc = (DIM == 2 ? .25 : .125) * s;
+    const double t = F.s->t;
+    for (int q = 0; q < NE; ++q) {
+      const mhc_env_params& o = P.env[q];
+      if (o.depot_type == MHC_DEPOT_NONE || !((mask >> q) & 1)) continue;
+      double value = o.depot_value;
+      if (t < o.depot_tdebut) value = 0.;
+      if (t > o.depot_tfin) value = 0.;
+      if (o.depot_type == MHC_DEPOT_LINEAIRE) {
+        value += o.depot_dependance[0] * cc.x;
+        value += o.depot_dependance[1] * cc.y;
+        value += o.depot_dependance[2] * cc.z;
+        value += o.depot_dependance[3] * t;
+      }
+      if (fabs(cc.x - o.depot_origin[0]) > o.depot_cutoff[0]) value = 0.;
+      if (fabs(cc.y - o.depot_origin[1]) > o.depot_cutoff[1]) value = 0.;
+      ecur[q] = ecur[q] + value * dt;
+    }
+  }
   // updateEnergyAndPressure
   double ee_[NE], pe[NE], ce[NE];
   for (int q = 0; q < NE; ++q) {

@@ -1024,7 +1024,35 @@ static void compute_pression_moyenne(Case& C) {
  * updateEnergyAndPressureforGP (1623-1698, non-CSTS branch),
  * updateEnergyAndPressurebyNewton (1506-1571) or
  * updateEnergyAndPressureExplicite (1484-1502) */
+/* MahycoModule::DepotEnergy (MahycoModule.cc:1364-1417), constant and
+ * linear deposits: value x deltat added to the environment's internal
+ * energy, zero outside [Tdebut, Tfin] and beyond the x / y cutoffs around
+ * the origin (the Lagrangian cell centre of this iteration) */
+static void depot_energy(Case& C) {
+  for (int e = 0; e < C.nenv; ++e) {
+    const mhc_env_params& o = C.P.env[e];
+    if (o.depot_type == MHC_DEPOT_NONE) continue;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (!C.has(c, e)) continue;
+      const R3 cc = C.cell_coord[c];
+      double value = o.depot_value;
+      if (C.t < o.depot_tdebut) value = 0.;
+      if (C.t > o.depot_tfin) value = 0.;
+      if (o.depot_type == MHC_DEPOT_LINEAIRE) {
+        value += o.depot_dependance[0] * cc.x;
+        value += o.depot_dependance[1] * cc.y;
+        value += o.depot_dependance[2] * cc.z;
+        value += o.depot_dependance[3] * C.t;
+      }
+      if (std::fabs(cc.x - o.depot_origin[0]) > o.depot_cutoff[0]) value = 0.;
+      if (std::fabs(cc.y - o.depot_origin[1]) > o.depot_cutoff[1]) value = 0.;
+      C.EV(C.internal_energy, e, c) += value * C.dt;
+    }
+  }
+}
+
 static void update_energy_and_pressure(Case& C) {
+  depot_energy(C);
   if (C.P.pression_explicite) {
     for (int e = 0; e < C.nenv; ++e) {
       for (long c = 0; c < C.ncell; ++c) {

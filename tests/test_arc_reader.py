@@ -115,3 +115,23 @@ def test_gnuplot_writer_format(tmp_path):
                                                           "Pressure_ZG"]
     assert open(tmp_path / "courbes" / "gnuplot" / "Density_ZG").read() == \
         "1.2577892535548833E-04 9.9999747105891568E-01\n"
+
+
+def test_energy_deposit_options(tmp_path):
+    """<energy-depot> of an environment (Mahyco.axl:335-380): constant and
+    linear deposits are read, the super-Gaussian one is refused."""
+    dep = ("<energy-depot><type>DepotLineaire</type><valeur-source-energie>3.5e3</valeur-source-energie>"
+           "<origine>0.1 0.2 0.</origine><dependanceX>2.</dependanceX><dependanceT>5.</dependanceT>"
+           "<cutoffY>0.5</cutoffY><Tdebut>1e-3</Tdebut><Tfin>2e-3</Tfin></energy-depot>")
+    text = open(ARC).read().replace("</environment>", dep + "</environment>", 1)
+    f = tmp_path / "d.arc"
+    f.write_text(text)
+    p, _ = read_arc(str(f))
+    e = p.env[0]
+    assert (e.depot_type, e.depot_value, list(e.depot_origin)) == (2, 3.5e3, [0.1, 0.2, 0.0])
+    assert list(e.depot_dependance) == [2.0, 0.0, 0.0, 5.0] and list(e.depot_cutoff) == [1000.0, 0.5]
+    assert (e.depot_tdebut, e.depot_tfin, p.env[1].depot_type) == (1e-3, 2e-3, 0)
+    g = tmp_path / "g.arc"
+    g.write_text(text.replace("DepotLineaire", "DepotSuperGaussian"))
+    with pytest.raises(NotImplementedError):
+        read_arc(str(g))
