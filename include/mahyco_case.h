@@ -35,7 +35,9 @@ enum mhc_eos_kind {
 
 /* boundary-condition kinds, same numbering as TypesMahyco::eBoundaryCondition */
 enum mhc_bc_kind {
-  MHC_BC_VX = 0, MHC_BC_VY = 1, MHC_BC_VZ = 2
+  MHC_BC_VX = 0, MHC_BC_VY = 1, MHC_BC_VZ = 2,
+  /* pressure applied as a node force on the surface (MahycoModule.cc:909-986) */
+  MHC_BC_GEOMETRIC_PRESSURE = 3, MHC_BC_LINEAR_PRESSURE = 4
 };
 
 /* energy deposits (TypesMahyco.h eEnergyDepot): constant or linear in
@@ -58,7 +60,8 @@ enum mhc_limiter {
 enum mhc_case_model {
   MHC_CASE_SOD = 1,       /* casTest/SOD/SODService.cc */
   MHC_CASE_SEDOV = 2,     /* casTest/SEDOV/SEDOVService.cc */
-  MHC_CASE_TWO_STATE = 3  /* explicit left/right states (seeded batch cases) */
+  MHC_CASE_TWO_STATE = 3, /* explicit left/right states (seeded batch cases) */
+  MHC_CASE_ONECELL = 4    /* casTest/ONECELL/ONECELLService.cc: one uniform environment */
 };
 
 /* cas-test ids used by SOD and SEDOV (TypesMahyco.h:44-94) */
@@ -114,6 +117,7 @@ typedef struct mhc_bc {
   int surface;  /* mhc_surface */
   double value;
   double tdebut, tfin;
+  double dependance[4];  /* LinearPressure: dependanceX, Y, Z, T */
 } mhc_bc;
 
 typedef struct mhc_case_params {

@@ -9,6 +9,7 @@ Option names and defaults follow the reference descriptors:
 from __future__ import annotations
 
 import ctypes as C
+import math
 import xml.etree.ElementTree as ET
 
 MAX_ENV = 4
@@ -17,10 +18,10 @@ MAX_BC = 12
 EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN = 0, 1, 2
 EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
                "MieGruneisen": EOS_MIE_GRUNEISEN}
-BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2}
+BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
-CASE_SOD, CASE_SEDOV, CASE_TWO_STATE = 1, 2, 3
-CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV}
+CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL = 1, 2, 3, 4
+CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL}
 LENGTHS = {"racine-cubique-volume": 0, "faces-opposees": 1, "monodimX": 2,
            "monodimY": 3, "monodimZ": 4}
 MINMOD, SUPERBEE, VANLEER = 0, 1, 2
@@ -51,7 +52,7 @@ class EnvParams(C.Structure):
 
 class BC(C.Structure):
     _fields_ = [("kind", C.c_int), ("surface", C.c_int), ("value", C.c_double),
-                ("tdebut", C.c_double), ("tfin", C.c_double)]
+                ("tdebut", C.c_double), ("tfin", C.c_double), ("dependance", C.c_double * 4)]
 
 
 class CaseParams(C.Structure):
@@ -146,11 +147,12 @@ def default_params() -> CaseParams:
 
 
 def add_bc(p: CaseParams, surface: str, kind: str, value: float = 0.0,
-           tdebut: float = 0.0, tfin: float = 1000.0) -> None:
+           tdebut: float = 0.0, tfin: float = 1000.0, dependance=(0.0, 0.0, 0.0, 0.0)) -> None:
     if p.nb_bc >= MAX_BC:
         raise ValueError("too many boundary conditions")
     b = p.bc[p.nb_bc]
     b.kind, b.surface, b.value, b.tdebut, b.tfin = BC_BY_NAME[kind], SURFACES[surface], value, tdebut, tfin
+    b.dependance[:] = dependance
     p.nb_bc += 1
 
 
@@ -312,10 +314,17 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         if kind not in BC_BY_NAME:
             raise NotImplementedError(f"boundary condition {kind}")
         add_bc(p, b.find("surface").text.strip(), kind, _txt(b, "value", 0.0),
-               _txt(b, "Tdebut", 0.0), _txt(b, "Tfin", 1000.0))
+               _txt(b, "Tdebut", 0.0), _txt(b, "Tfin", 1000.0),
+               tuple(_txt(b, t, 0.0) for t in ("dependanceX", "dependanceY", "dependanceZ", "dependanceT")))
     th = root.find("time-history/bilan")
     if th is not None:
         p.time_history_period = _txt(th, "periode", 10, int)
+    # Arcane records history values only every output-history-period
+    # iterations: EnvSummation lines come out at multiples of both periods
+    ohp = _txt(root.find("arcane-post-processing"), "output-history-period", 1, int) \
+        if root.find("arcane-post-processing") is not None else 1
+    if ohp > 1:
+        p.time_history_period = math.lcm(p.time_history_period if p.time_history_period > 0 else 10, ohp)
     return p, info
 
 

@@ -15,9 +15,9 @@ from __future__ import annotations
 import math
 import random
 
-from .case import (ARITHMETIC_G, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, EOS_MIE_GRUNEISEN,
+from .case import (ARITHMETIC_G, CASE_ONECELL, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, EOS_MIE_GRUNEISEN,
                    EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
-                   ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, default_params, env_defaults,
+                   ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults,
                    symmetry_bcs)
 
 
@@ -198,6 +198,39 @@ def bar_impact(n=(80, 400), L=(0.01, 0.05), velocity=200.0, deltat_init=1e-9, el
     return p
 
 
+def compression(dim=2, n=(40, 4), L=(10e-6, 1e-6), coef_antiderive=0.0, ramp=3e17, plateau=3e10,
+                t_switch=2e-10) -> CaseParams:
+    """CAS_Compression_isotherme_ALU_monodimX at any size: an aluminium
+    block (ONECELL init, Mie-Gruneisen, elasto-plastic DefaultModel,
+    explicit pressure) squeezed from both x ends by a pressure rising
+    linearly in time (LinearPressure) then held (GeometricPressure)."""
+    p = default_params()
+    _mesh(p, dim, n, L)
+    p.nb_env = 1
+    env_defaults(p.env[0], EOS_MIE_GRUNEISEN)
+    o = p.env[0]
+    o.adiabatic_cst, o.rho0, o.s1, o.gamma0, o.a, o.c0 = 2.0, 2785.0, 1.339, 1.6, 0.48, 5328.0
+    o.densite_initiale, o.pression_initiale = 2785.0, 0.0
+    o.elasto_model, o.rotation_order = 1, 1
+    o.shear_modulus, o.yield_strength = 2.69e10, 2.9e8
+    p.coef_antiderive = coef_antiderive
+    p.cas_model = CASE_ONECELL
+    p.pression_explicite = 1
+    p.with_projection = 0
+    p.longueur_caracteristique = 2  # monodimX
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.1, 1e-12, 1e-14, 1e-12
+    for s in ("XMIN", "XMAX"):
+        add_bc(p, s, "LinearPressure", 0.0, 0.0, t_switch, (0.0, 0.0, 0.0, ramp))
+        add_bc(p, s, "GeometricPressure", plateau, t_switch, 2 * t_switch)
+        add_bc(p, s, "Vy", 0.0)
+    add_bc(p, "YMIN", "Vy", 0.0)
+    add_bc(p, "YMAX", "Vy", 0.0)
+    if dim == 3:
+        add_bc(p, "ZMIN", "Vz", 0.0)
+        add_bc(p, "ZMAX", "LinearPressure", 1e9, 0.0, 2 * t_switch, (1e14, 0.0, 0.0, 0.0))
+    return p
+
+
 def serving_request(kind: str, cells: int) -> CaseParams:
     """One request of the served mix, scaled to about `cells` cells."""
     if kind == "sedov2d":
@@ -287,6 +320,11 @@ PARITY_CASES = {
                                                       deltat_max=1e-3, deltat_init=1e-4), 2), 100),
     "adi2d_bisod_depot_constant": (lambda: _depot(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True,
                                                       deltat_init=1e-3), 1), 60),
+    # ONECELL init and pressure surfaces (LinearPressure, GeometricPressure)
+    # with the elasto-plastic model, as CAS_Compression_isotherme_ALU_monodimX
+    "lag2d_compression_pressure_bcs": (lambda: compression(), 400),
+    "lag3d_compression_pressure_bcs": (lambda: compression(dim=3, n=(16, 3, 3), L=(4e-6, 1e-6, 1e-6),
+                                                           coef_antiderive=0.01), 400),
     # conservation-energie-totale (RemapADIFinal.cc:320-344)
     "adi2d_sedov_cet": (lambda: _cet(sedov(dim=2, n=(24, 24), deltat_init=1e-4)), 100),
     "adi3d_bisod_superbee_cet": (lambda: _cet(sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True,

@@ -361,6 +361,13 @@ int validate(const mhc_case_params* p) {
   if ((long long)(p->nx + 1) * (p->ny + 1) * (p->dim == 3 ? p->nz + 1 : 1) > INT_MAX)
     return set_err(MHC_ERR_ARG, "a case holds at most 2^31 - 1 nodes");
   if (p->nb_bc < 0 || p->nb_bc > MHC_MAX_BC) return set_err(MHC_ERR_ARG, "nb_bc");
+  for (int b = 0; b < p->nb_bc; ++b) {
+    const int kind = p->bc[b].kind;
+    if (kind < MHC_BC_VX || kind > MHC_BC_LINEAR_PRESSURE) return set_err(MHC_ERR_UNSUPPORTED, "boundary condition kind");
+    if (kind >= MHC_BC_GEOMETRIC_PRESSURE && p->with_projection)
+      return set_err(MHC_ERR_UNSUPPORTED, "pressure boundary conditions need a Lagrangian loop");
+  }
+  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_ONECELL) return set_err(MHC_ERR_ARG, "cas-model");
   if (p->ordre_projection < 1 || p->ordre_projection > 3)
     return set_err(MHC_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
   if (p->projection_limiteur_id < 0 || p->projection_limiteur_id > 7)

@@ -435,6 +435,8 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
       mat = (comp(cc, P.cas_test - MHC_TEST_BISOD_X) < 0.5) ? 0. : 1.;
   } else if (P.cas_model == MHC_CASE_TWO_STATE) {
     if (NE > 1) mat = (comp(cc, P.interface_dir) < P.interface_pos) ? 0. : 1.;
+  } else if (P.cas_model == MHC_CASE_ONECELL) {
+    mat = 0.;  // ONECELLService::initMat
   } else if (P.cas_model == MHC_CASE_SEDOV && P.cas_test != MHC_TEST_SEDOV) {
     bool center = false;
     for (int l = 0; l < NBN; ++l) {
@@ -482,6 +484,11 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
     int st = (comp(cc, P.interface_dir) < P.interface_pos) ? 0 : 1;
     rho = P.env[st].densite_initiale;
     p = P.env[st].pression_initiale;
+  } else if (P.cas_model == MHC_CASE_ONECELL) {
+    // ONECELLService::initVarMono: the first environment's state everywhere
+    rho = P.env[0].densite_initiale;
+    p = P.env[0].pression_initiale;
+    e = P.env[0].energie_initiale;
   } else if (P.cas_model == MHC_CASE_SEDOV) {
     double rhoInit = P.env[0].densite_initiale, pInit = P.env[0].pression_initiale;
     if (P.cas_test == MHC_TEST_SEDOV) e = 0.244816e-5;
@@ -573,6 +580,105 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
 }
 
 // ---------------------------------------------------------------------------
+// Pressure surfaces of applyBoundaryConditionForCellVariables
+// (MahycoModule.cc:909-986), Lagrangian runs: for each pressure condition in
+// order and each face of its surface holding the node, in face order,
+// v -= dt_mid / nb_face_nodes * n * p * S / m_node, with n the unit vector
+// from the boundary cell's centre (positions at n) to the face centre of the
+// initial grid, S the length of the face edge that starts at the node (2D)
+// or the z-projected face area (3D), p the value plus its linear terms in
+// the node position and time, zero outside [Tdebut, Tfin).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void face_node_rt(int dim, int d, int q, int& a, int& b, int& c) {
+  a = b = c = 0;
+  if (dim == 2) {
+    if (d == 0) b = q; else a = q;
+    return;
+  }
+  const int s1 = (q == 1 || q == 2), s2 = (q == 2 || q == 3);
+  if (d == 0) { b = s1; c = s2; }
+  else if (d == 1) { a = s1; c = s2; }
+  else { a = s1; b = s2; }
+}
+
+template <int DIM>
+__device__ __forceinline__ void pressure_bcs(const Mesh& M, const mhc_case_params& P, const Fields& F, int i, int j,
+                                             int k, long long n, double dth, double t, double& vx, double& vy,
+                                             double& vz) {
+  constexpr int NQ = DIM == 3 ? 4 : 2;
+  const double w = DIM == 2 ? .5 : .25, wc = DIM == 2 ? .25 : .125;
+  for (int b = 0; b < P.nb_bc; ++b) {
+    const mhc_bc& bc = P.bc[b];
+    if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE) continue;
+    const int s = bc.surface;
+    const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
+    if (d >= DIM) continue;
+    const bool maxside = s >= MHC_XMAX;
+    const int nid = d == 0 ? i : (d == 1 ? j : k);
+    const int nnd = d == 0 ? M.nnx : (d == 1 ? M.nny : M.nnz);
+    if (nid != (maxside ? nnd - 1 : 0)) continue;
+    // transverse axes a1 < a2 of the surface, node and cell counts along them
+    const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+    const int idx[3] = {i, j, k};
+    const int nc[3] = {M.ncx, M.ncy, M.ncz};
+    for (int o2 = (DIM == 3 ? -1 : 0); o2 <= 0; ++o2) {
+      for (int o1 = -1; o1 <= 0; ++o1) {
+        const int t1 = idx[a1] + o1, t2 = DIM == 3 ? idx[a2] + o2 : 0;
+        if (t1 < 0 || t1 >= nc[a1]) continue;
+        if (DIM == 3 && (t2 < 0 || t2 >= nc[a2])) continue;
+        int f[3];
+        f[d] = nid; f[a1] = t1;
+        if (DIM == 3) f[a2] = t2; else f[2] = 0;
+        // face nodes in face order, initial face centre, this node's slot
+        long long fn[NQ];
+        R3 fc = {0., 0., 0.};
+        int me = 0;
+        for (int q = 0; q < NQ; ++q) {
+          int a, bb, c;
+          face_node_rt(DIM, d, q, a, bb, c);
+          fn[q] = node_id(M, f[0] + a, f[1] + bb, DIM == 3 ? f[2] + c : 0);
+          fc = fc + w * node_x0(M, f[0] + a, f[1] + bb, DIM == 3 ? f[2] + c : 0);
+          if (fn[q] == n) me = q;
+        }
+        auto X = [&](long long m) { return R3{F.Xp[0][m], F.Xp[1][m], F.Xp[2][m]}; };
+        double surface;
+        if (DIM == 2) {
+          const long long n2 = me < NQ - 1 ? fn[me + 1] : fn[0];
+          surface = norm(X(n2) - X(n));
+        } else {
+          const R3 v1 = X(fn[2]) - X(fn[0]), v2 = X(fn[3]) - X(fn[1]);
+          surface = 0.5 * produit(v1.x, v2.y, v1.y, v2.x);
+        }
+        // the boundary cell: first or last along d
+        int ci[3] = {f[0], f[1], f[2]};
+        if (maxside) ci[d] -= 1;
+        R3 sc = {0., 0., 0.};
+        for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+          int a, bb, c;
+          local_node_offset(l, a, bb, c);
+          sc = sc + X(node_id(M, ci[0] + a, ci[1] + bb, DIM == 3 ? ci[2] + c : 0));
+        }
+        const R3 cc = wc * sc;
+        const R3 diff = fc - cc;
+        const R3 nrm = diff / norm(diff);
+        double value = bc.value;
+        if (bc.kind == MHC_BC_LINEAR_PRESSURE) {
+          const R3 x = X(n);
+          value += bc.dependance[0] * x.x;
+          value += bc.dependance[1] * x.y;
+          value += bc.dependance[2] * x.z;
+          value += bc.dependance[3] * t;
+        }
+        if (t < bc.tdebut) value = 0.;
+        if (t >= bc.tfin) value = 0.;
+        const R3 dv = (dth * w * nrm * value * surface) / F.mn[n];
+        vx = vx - dv.x; vy = vy - dv.y; vz = vz - dv.z;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Lagrange, node pass: updateVelocity + applyBoundaryCondition + updatePosition
 // (MahycoModule.cc:438-501, 756-807, 730-741).
 //
@@ -643,6 +749,7 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
     else if (bc.kind == MHC_BC_VY) vy = bc.value;
     else if (bc.kind == MHC_BC_VZ) vz = bc.value;
   }
+  pressure_bcs<DIM>(M, P, F, i, j, k, n, dth, t, vx, vy, vz);
   const R3 x = P.with_projection ? node_x0(M, i, j, k) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
@@ -719,6 +826,7 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
     else if (bc.kind == MHC_BC_VY) vy = bc.value;
     else if (bc.kind == MHC_BC_VZ) vz = bc.value;
   }
+  pressure_bcs<DIM>(M, P, F, i, j, k, n, 0.5 * (F.s->old_dt + dt), t, vx, vy, vz);
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   F.Xn[0][n] = F.Xp[0][n] + dt * vx; F.Xn[1][n] = F.Xp[1][n] + dt * vy; F.Xn[2][n] = F.Xp[2][n] + dt * vz;
 }
@@ -739,8 +847,9 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
 // spin, work with S_n, deviator update with rotation, radial return, work
 // with S_n+1.  Returns the two work increments in order.  Where the
 // reference relies on undefined or framework behaviour: the deviator
-// increment takes trace = tr(D) (an uninitialised `trace` there,
-// DefaultModelService.cc:82,96), doubleContraction sums row by row, each
+// increment takes trace = 0 (an uninitialised `trace` there,
+// DefaultModelService.cc:82,96, whose non-regression curves match 0 and not
+// tr(D)), doubleContraction sums row by row, each
 // row left to right, pow(x, 2.) is x*x, Real3x3 / Real divides each
 // component.
 // ---------------------------------------------------------------------------
@@ -791,7 +900,7 @@ __device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh&
   w1 = work();
   const double sxx = Sv[0], syy = Sv[1], szz = Sv[2], sxy = Sv[3], syz = Sv[4], szx = Sv[5];
   const double mu = o.shear_modulus, Y = o.yield_strength;
-  const double trace = D[0][0] + D[1][1] + D[2][2];
+  const double trace = 0.;
   double Pt[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a)

@@ -489,6 +489,8 @@ static void init_materials(Case& C) {
         double r = comp(C.cell_coord[c], P.cas_test - MHC_TEST_BISOD_X);
         m = (r < 0.5) ? 0. : 1.;
       }
+    } else if (P.cas_model == MHC_CASE_ONECELL) {
+      m = 0.;  /* ONECELLService::initMat */
     } else if (P.cas_model == MHC_CASE_TWO_STATE) {
       if (C.nenv > 1) {
         double r = comp(C.cell_coord[c], P.interface_dir);
@@ -552,6 +554,15 @@ static void init_variables(Case& C) {
     // every node starts at the velocity of the first environment (zero in
     // the shock tubes, the impact velocity of a projectile)
     for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
+  } else if (P.cas_model == MHC_CASE_ONECELL) {
+    /* ONECELLService::initVarMono: the first environment's state everywhere,
+     * nodes at rest */
+    for (long c = 0; c < C.ncell; ++c) {
+      C.density.g[c] = P.env[0].densite_initiale;
+      C.pressure.g[c] = P.env[0].pression_initiale;
+      C.internal_energy.g[c] = P.env[0].energie_initiale;
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {0., 0., 0.};
   } else if (P.cas_model == MHC_CASE_SEDOV) {
     double rhoInit = P.env[0].densite_initiale, pInit = P.env[0].pression_initiale;
     bool mono = P.cas_test == MHC_TEST_SEDOV;
@@ -837,6 +848,7 @@ static bool node_on_surface(const Case& C, long n, int surf) {
 /* MahycoModule::applyBoundaryCondition (MahycoModule.cc:756-807), velocity
  * kinds on the PrepareFaceGroup surfaces.  A node lies on a surface exactly
  * when it belongs to one of the surface's faces. */
+static void apply_pressure_bcs(Case& C);
 static void apply_boundary_condition(Case& C) {
   const double eps = 1.e-8;
   for (int b = 0; b < C.P.nb_bc; ++b) {
@@ -850,6 +862,60 @@ static void apply_boundary_condition(Case& C) {
       if (bc.kind == MHC_BC_VX) C.vel[n].x = bc.value;
       else if (bc.kind == MHC_BC_VY) C.vel[n].y = bc.value;
       else if (bc.kind == MHC_BC_VZ) C.vel[n].z = bc.value;
+    }
+  }
+  apply_pressure_bcs(C);
+}
+
+/* pressure surfaces of applyBoundaryConditionForCellVariables
+ * (MahycoModule.cc:909-986): for every face of the surface in face order and
+ * every node of the face, v -= dt_mid / nb_face_nodes * n * p * S / m_node,
+ * with n the unit vector from the cell centre to the (initial) face centre,
+ * S the length of the face edge from that node (2D) or the z-projected face
+ * area (3D), p the BC value (plus its linear terms) inside [Tdebut, Tfin) */
+static void apply_pressure_bcs(Case& C) {
+  const double w = C.dim == 2 ? .5 : .25;
+  const double dt = 0.5 * (C.old_dt + C.dt);
+  for (int b = 0; b < C.P.nb_bc; ++b) {
+    const mhc_bc& bc = C.P.bc[b];
+    if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE) continue;
+    const int s = bc.surface;
+    const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
+    if (d >= C.dim) continue;
+    const bool maxside = s >= MHC_XMAX;
+    for (long f = 0; f < C.nface[d]; ++f) {
+      int i, j, k;
+      C.fijk(d, f, i, j, k);
+      const int id = d == 0 ? i : (d == 1 ? j : k);
+      if (id != (maxside ? C.ncd(d) : 0)) continue;
+      /* the one cell of the boundary face */
+      const long c = maxside ? (d == 0 ? C.cid(i - 1, j, k) : (d == 1 ? C.cid(i, j - 1, k) : C.cid(i, j, k - 1)))
+                             : C.cid(i, j, k);
+      long n[4] = {0, 0, 0, 0};
+      const int nb = C.face_nodes(d, i, j, k, n);
+      for (int q = 0; q < nb; ++q) {
+        const long node = n[q];
+        double value = bc.value;
+        double surface;
+        if (C.dim == 2) {
+          const long node2 = q < nb - 1 ? n[q + 1] : n[0];
+          surface = norm(C.coord[node2] - C.coord[node]);
+        } else {
+          const R3 v1 = C.coord[n[2]] - C.coord[n[0]], v2 = C.coord[n[3]] - C.coord[n[1]];
+          surface = 0.5 * produit(v1.x, v2.y, v1.y, v2.x);
+        }
+        const R3 diff = C.face_coord[d][f] - C.cell_coord[c];
+        const R3 nrm = diff / norm(diff);
+        if (bc.kind == MHC_BC_LINEAR_PRESSURE) {
+          value += bc.dependance[0] * C.coord[node].x;
+          value += bc.dependance[1] * C.coord[node].y;
+          value += bc.dependance[2] * C.coord[node].z;
+          value += bc.dependance[3] * C.t;
+        }
+        if (C.t < bc.tdebut) value = 0.;
+        if (C.t >= bc.tfin) value = 0.;
+        C.vel[node] -= (dt * w * nrm * value * surface) / C.node_mass[node];
+      }
     }
   }
 }
@@ -908,8 +974,10 @@ static void compute_artificial_viscosity(Case& C) {
  * velocity gradient from the mean corner normals, deformation rate and
  * spin, elasto-plastic work with S_n, deviator update with rotation, radial
  * return, work with S_n+1.  Restated where the reference is undefined or
- * relies on Arcane: the deviator increment takes trace = tr(D) (the
- * reference reads an uninitialised `trace`, DefaultModelService.cc:82,96);
+ * relies on Arcane: the deviator increment takes trace = 0 (the reference
+ * reads an uninitialised `trace`, DefaultModelService.cc:82,96; its
+ * CAS_Compression_isotherme_ALU_monodimX curves are reproduced with 0 and
+ * miss by 7 % with tr(D));
  * doubleContraction sums row by row, each row left to right; pow(x, 2.) is
  * x*x; Real3x3 / Real divides every component. */
 static void update_elasticity_and_plasticity(Case& C) {
@@ -954,7 +1022,7 @@ static void update_elasticity_and_plasticity(Case& C) {
     work();
     /* ComputeElasticity (78-169) */
     const double sxx = S[0], syy = S[1], szz = S[2], sxy = S[3], syz = S[4], szx = S[5];
-    const double trace = D[0][0] + D[1][1] + D[2][2];
+    const double trace = 0.;  /* see above */
     double P[3][3];
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) P[a][b] = 2 * mu * (D[a][b] - (1. / 3.) * trace * (a == b ? 1.0 : 0.0)) * dt;

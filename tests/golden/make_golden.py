@@ -48,7 +48,15 @@ CASES = {
     "CAS_BiSodCaseX_pente_borne_superbee_debar_2": {"mpi_ranks": 4},
     "CAS_BiSodCaseY_pente_borne_minmod_debar_2": {"mpi_ranks": 4},
     "CAS_BiSodCaseY_pente_borne_superbee_debar_2": {"mpi_ranks": 4},
+    # ONECELL init, LinearPressure / GeometricPressure surfaces, elasto
+    # DefaultModel (EPP / YEPP), Mie-Gruneisen, explicit pressure; pressure
+    # and energy grow from zero, so their first lines carry relative
+    # differences up to 3e-10 that fall to 1e-13 as they grow
+    "CAS_Compression_isotherme_ALU_monodimX": {"tol": 5e-10},
 }
+# variables the Ensight writer of mahyco_b200.output produces
+ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy", "PseudoViscosity",
+                "Materiau", "SoundSpeed", "CellVolume"}
 VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
 
 
@@ -70,7 +78,7 @@ def main(ref_root="/root/reference"):
         # run writes only its first sub-domain, so none are kept for those
         dep = os.path.join(d, "output", "depouillement")
         digests = {}
-        if extra.get("mpi_ranks", 1) == 1:
+        if extra.get("mpi_ranks", 1) == 1 and set(info["output_vars"]) <= ENSIGHT_VARS:
             for root, _, files in os.walk(dep):
                 for fn in sorted(files):
                     full = os.path.join(root, fn)

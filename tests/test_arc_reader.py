@@ -135,3 +135,25 @@ def test_energy_deposit_options(tmp_path):
     g.write_text(text.replace("DepotLineaire", "DepotSuperGaussian"))
     with pytest.raises(NotImplementedError):
         read_arc(str(g))
+
+
+def test_pressure_surfaces_and_onecell(tmp_path):
+    """LinearPressure / GeometricPressure surfaces with their time window
+    and linear dependences, the ONECELL init and the output-history-period
+    that thins the EnvSummation lines (here lcm(10, 500) = 500)."""
+    text = open(ARC).read().replace('<cas-model name="SOD">', '<cas-model name="ONECELL">').replace(
+        "<cas-test>13</cas-test>", "<cas-test>0</cas-test>").replace(
+        "<final-time>", "<boundary-condition><surface>XMAX</surface><type>LinearPressure</type><value>1.</value>"
+        "<dependanceT>3e17</dependanceT><Tfin>1e-7</Tfin></boundary-condition>"
+        "<boundary-condition><surface>XMIN</surface><type>GeometricPressure</type><value>30e9</value>"
+        "<Tdebut>1e-7</Tdebut></boundary-condition><final-time>", 1).replace(
+        "<mesh", "<arcane-post-processing><output-history-period>500</output-history-period>"
+        "</arcane-post-processing><mesh", 1)
+    f = tmp_path / "p.arc"
+    f.write_text(text)
+    p, _ = read_arc(str(f))
+    assert p.cas_model == 4 and p.time_history_period == 500
+    kinds = [(p.bc[i].kind, p.bc[i].surface, p.bc[i].value, p.bc[i].tdebut, p.bc[i].tfin, list(p.bc[i].dependance))
+             for i in range(p.nb_bc)]
+    assert (4, 3, 1.0, 0.0, 1e-7, [0.0, 0.0, 0.0, 3e17]) in kinds
+    assert (3, 0, 30e9, 1e-7, 1000.0, [0.0, 0.0, 0.0, 0.0]) in kinds

@@ -30,7 +30,7 @@ def test_gpu_matches_reference_goldens(path):
     from mahyco_b200 import Hydro, ST_STOP
     g = json.load(open(path))
     multi = g["extra"].get("mpi_ranks", 1) > 1
-    tol = 5e-12 if multi else 1e-13
+    tol = g["extra"].get("tol", 5e-12 if multi else 1e-13)
     ttol = 1e-13 if multi else 1e-14  # the time: a sum of deltat, per-rank orders move it by ulps
     p = params_from_dict(g["params"])
     period = p.time_history_period if p.time_history_period > 0 else 10
