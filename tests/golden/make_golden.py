@@ -48,6 +48,20 @@ CASES = {
     "CAS_BiSodCaseX_pente_borne_superbee_debar_2": {"mpi_ranks": 4},
     "CAS_BiSodCaseY_pente_borne_minmod_debar_2": {"mpi_ranks": 4},
     "CAS_BiSodCaseY_pente_borne_superbee_debar_2": {"mpi_ranks": 4},
+    # the other SOD directions and Lagrangian variants (src/CMakeLists.txt
+    # TEST_NAMES and TEST_NAMES_PARA_4)
+    "CAS_2D_Lag_SodCaseY": {"mpi_ranks": 4},
+    "CAS_2D_Lag_SodCaseZ": {},
+    "CAS_2D_Lag_BiSodCaseY": {"mpi_ranks": 4},
+    "CAS_Lag_SodCaseX": {"mpi_ranks": 4},
+    "CAS_Lag_SodCaseY": {},
+    "CAS_Lag_SodCaseZ": {},
+    "CAS_Lag_BiSodCaseY": {},
+    "CAS_Lag_BiSodCaseZ": {"mpi_ranks": 4},
+    "CAS_SodCaseY": {"mpi_ranks": 4},
+    "CAS_SodCaseZ": {"mpi_ranks": 4},
+    "CAS_BiSodCaseY": {"mpi_ranks": 4},
+    "CAS_BiSodCaseZ": {"mpi_ranks": 4},
     # ONECELL init, LinearPressure / GeometricPressure surfaces, elasto
     # DefaultModel (EPP / YEPP), Mie-Gruneisen, explicit pressure; pressure
     # and energy grow from zero, so their first lines carry relative
