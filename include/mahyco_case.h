@@ -40,9 +40,11 @@ enum mhc_bc_kind {
   MHC_BC_GEOMETRIC_PRESSURE = 3, MHC_BC_LINEAR_PRESSURE = 4
 };
 
-/* energy deposits (TypesMahyco.h eEnergyDepot): constant or linear in
- * position and time; the super-Gaussian deposit is not supported */
-enum mhc_depot { MHC_DEPOT_NONE = 0, MHC_DEPOT_CONSTANT = 1, MHC_DEPOT_LINEAIRE = 2 };
+/* energy deposits (TypesMahyco.h eEnergyDepot): constant, linear in
+ * position and time, or super-Gaussian in x and y */
+enum mhc_depot {
+  MHC_DEPOT_NONE = 0, MHC_DEPOT_CONSTANT = 1, MHC_DEPOT_LINEAIRE = 2, MHC_DEPOT_SUPER_GAUSSIAN = 3
+};
 
 /* boundary surfaces built by MahycoModule::PrepareFaceGroup (MahycoAnnexe.cc:149-235) */
 enum mhc_surface {
@@ -77,8 +79,12 @@ enum mhc_char_length {
   MHC_LENGTH_MONODIM_X = 2, MHC_LENGTH_MONODIM_Y = 3, MHC_LENGTH_MONODIM_Z = 4
 };
 
-/* is-euler-scheme option of RemapADI */
-enum mhc_euler_scheme { MHC_EULER_FULL = 0, MHC_EULER_NONE = 1 };
+/* is-euler-scheme option of RemapADI: Full (every axis back on the initial
+ * grid), NON, or one axis X / Y / Z (only that axis is remapped and reset;
+ * the other coordinates stay Lagrangian) */
+enum mhc_euler_scheme {
+  MHC_EULER_FULL = 0, MHC_EULER_NONE = 1, MHC_EULER_X = 2, MHC_EULER_Y = 3, MHC_EULER_Z = 4
+};
 
 typedef struct mhc_env_params {
   int eos;                       /* mhc_eos_kind */
@@ -103,13 +109,15 @@ typedef struct mhc_env_params {
   double yield_strength;
   /* energy-depot (MahycoModule.cc:1364-1417), added to the environment's
    * internal energy before the energy update: mhc_depot kind, value,
-   * origine, dependanceX/Y/Z/T, cutoffX/Y, Tdebut, Tfin */
+   * origine, dependanceX/Y/Z/T, cutoffX/Y, Tdebut, Tfin, power (exponent
+   * of the super-Gaussian profile) */
   int depot_type;
   double depot_value;
   double depot_origin[3];
   double depot_dependance[4];
   double depot_cutoff[2];
   double depot_tdebut, depot_tfin;
+  double depot_power;
 } mhc_env_params;
 
 typedef struct mhc_bc {

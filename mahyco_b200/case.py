@@ -26,7 +26,11 @@ LENGTHS = {"racine-cubique-volume": 0, "faces-opposees": 1, "monodimX": 2,
            "monodimY": 3, "monodimZ": 4}
 MINMOD, SUPERBEE, VANLEER = 0, 1, 2
 MINMOD_G, SUPERBEE_G, VANLEER_G, ARITHMETIC_G, ULTRABEE_G = 3, 4, 5, 6, 7
-DEPOT_NONE, DEPOT_CONSTANT, DEPOT_LINEAIRE = 0, 1, 2
+DEPOT_NONE, DEPOT_CONSTANT, DEPOT_LINEAIRE, DEPOT_SUPER_GAUSSIAN = 0, 1, 2, 3
+DEPOT_BY_NAME = {"DepotConstant": DEPOT_CONSTANT, "DepotLineaire": DEPOT_LINEAIRE,
+                 "DepotSuperGaussian": DEPOT_SUPER_GAUSSIAN}
+EULER_FULL, EULER_NONE, EULER_X, EULER_Y, EULER_Z = 0, 1, 2, 3, 4
+EULER_BY_NAME = {"Full": EULER_FULL, "NON": EULER_NONE, "X": EULER_X, "Y": EULER_Y, "Z": EULER_Z}
 
 
 class EnvParams(C.Structure):
@@ -46,7 +50,7 @@ class EnvParams(C.Structure):
         ("shear_modulus", C.c_double), ("yield_strength", C.c_double),
         ("depot_type", C.c_int), ("depot_value", C.c_double), ("depot_origin", C.c_double * 3),
         ("depot_dependance", C.c_double * 4), ("depot_cutoff", C.c_double * 2),
-        ("depot_tdebut", C.c_double), ("depot_tfin", C.c_double),
+        ("depot_tdebut", C.c_double), ("depot_tfin", C.c_double), ("depot_power", C.c_double),
     ]
 
 
@@ -111,6 +115,7 @@ def env_defaults(e: EnvParams, eos: int = EOS_PERFECT_GAS) -> None:
     e.depot_dependance[:] = (0.0, 0.0, 0.0, 0.0)
     e.depot_cutoff[:] = (1000.0, 1000.0)
     e.depot_tdebut, e.depot_tfin = 0.0, 1000.0
+    e.depot_power = 4.0
 
 
 def default_params() -> CaseParams:
@@ -255,9 +260,10 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         dep = ev.find("energy-depot")
         if dep is not None:
             kind = _txt(dep, "type", "DepotConstant", str)
-            if kind not in ("DepotConstant", "DepotLineaire"):
+            if kind not in DEPOT_BY_NAME:
                 raise NotImplementedError(f"energy deposit {kind}")
-            e.depot_type = DEPOT_CONSTANT if kind == "DepotConstant" else DEPOT_LINEAIRE
+            e.depot_type = DEPOT_BY_NAME[kind]
+            e.depot_power = _txt(dep, "power", 4.0)
             e.depot_value = _txt(dep, "valeur-source-energie", 0.0)
             org = _txt(dep, "origine", "0. 0. 0.", str).split()
             e.depot_origin[:] = [float(v) for v in org]
@@ -276,8 +282,9 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         p.projection_limiteur_id = _txt(rm, "projection-limiteur-id", 0, int)
         p.remap_threshold = _txt(rm, "threshold", 1.0e-10)
         eul = _txt(rm, "is-euler-scheme", "Full", str)
-        if eul != "Full":
-            raise NotImplementedError("is-euler-scheme other than Full")
+        if eul not in EULER_BY_NAME or eul == "NON":
+            raise NotImplementedError(f"is-euler-scheme {eul}")
+        p.is_euler_scheme = EULER_BY_NAME[eul]
         p.conservation_energie_totale = int(_txt(rm, "conservation-energie-totale", False, _bool))
         p.projection_simple_pente = int(_txt(rm, "projection-simple-pente", False, _bool))
         p.projection_pente_borne = int(_txt(rm, "projection-pente-borne", False, _bool))

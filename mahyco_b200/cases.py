@@ -15,7 +15,8 @@ from __future__ import annotations
 import math
 import random
 
-from .case import (ARITHMETIC_G, CASE_ONECELL, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, EOS_MIE_GRUNEISEN,
+from .case import (ARITHMETIC_G, CASE_ONECELL, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, DEPOT_CONSTANT,
+                   DEPOT_SUPER_GAUSSIAN, EOS_MIE_GRUNEISEN, EULER_X, EULER_Y, EULER_Z,
                    EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
                    ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults,
                    symmetry_bcs)
@@ -231,6 +232,34 @@ def compression(dim=2, n=(40, 4), L=(10e-6, 1e-6), coef_antiderive=0.0, ramp=3e1
     return p
 
 
+def plaque(n=(20, 100), L=(100e-6, 0.5e-3), euler=EULER_Y, depot=DEPOT_SUPER_GAUSSIAN) -> CaseParams:
+    """CAS_plaque_demi_euler_Y_depot_Gaussian at any size: an aluminium plate
+    (ONECELL init, Mie-Gruneisen, explicit pressure) heated by a deposit
+    centred on y = 0 and remapped along y only (is-euler-scheme Y); x stays
+    Lagrangian and its ends are free."""
+    p = default_params()
+    _mesh(p, 2, n, L)
+    p.origin[:] = (0.0, -0.5 * L[1], 0.0)
+    p.nb_env = 1
+    env_defaults(p.env[0], EOS_MIE_GRUNEISEN)
+    o = p.env[0]
+    o.adiabatic_cst, o.rho0, o.s1, o.gamma0, o.a, o.c0 = 2.0, 2785.0, 1.339, 1.6, 0.48, 5328.0
+    o.specific_heat, o.temperature_ref = 897.0, 300.0
+    o.densite_initiale, o.pression_initiale = 2710.0, 1.0e5
+    o.depot_type, o.depot_value, o.depot_power = depot, 3.7e16, 8.0
+    o.depot_dependance[:] = (0.0, 0.8e4, 0.0, 0.0)
+    o.depot_cutoff[:] = (0.1 * L[0], 0.25 * L[1])
+    o.depot_tdebut, o.depot_tfin = 0.0, 10e-9
+    p.cas_model = CASE_ONECELL
+    p.is_euler_scheme = euler
+    p.pression_explicite = 1
+    p.longueur_caracteristique = 2  # monodimX
+    p.deltat_init, p.deltat_min, p.deltat_max = 1e-13, 1e-15, 1e-13
+    add_bc(p, "YMIN", "Vy", 0.0)
+    add_bc(p, "YMAX", "Vy", 0.0)
+    return p
+
+
 def serving_request(kind: str, cells: int) -> CaseParams:
     """One request of the served mix, scaled to about `cells` cells."""
     if kind == "sedov2d":
@@ -333,7 +362,24 @@ PARITY_CASES = {
                                             deltat_init=1e-3), 80),
     "adi3d_bisod_z_ultrabeeG": (lambda: sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
                                             limiter=ULTRABEE_G, deltat_init=1e-3), 60),
+    # per-axis Euler (is-euler-scheme X / Y / Z): one remapped axis, the
+    # others Lagrangian, the receiving volumes rebuilt every cycle
+    "adi2d_sedov_euler_x": (lambda: _euler(sedov(dim=2, n=(24, 24), deltat_init=1e-4), EULER_X), 100),
+    "adi3d_sedov_euler_z": (lambda: _euler(sedov(dim=3, n=(12, 12, 12), deltat_init=1e-4), EULER_Z), 40),
+    "adi2d_bisod_y_euler_y": (lambda: _euler(sod(dim=2, n=(5, 40), L=(0.1, 1.0), bi=True, axis=1,
+                                                 deltat_init=1e-3), EULER_Y), 60),
+    "adi2d_plaque_euler_y_depot_constant": (lambda: plaque(depot=DEPOT_CONSTANT), 80),
+    "adi2d_plaque_euler_y_depot_gaussian": (lambda: plaque(), 80),
 }
+
+# cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
+# calls exp and pow, which CUDA and the oracle's libm round differently
+PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13}
+
+
+def _euler(p: CaseParams, scheme: int) -> CaseParams:
+    p.is_euler_scheme = scheme
+    return p
 
 
 def _order3(p: CaseParams) -> CaseParams:

@@ -372,7 +372,9 @@ int validate(const mhc_case_params* p) {
     return set_err(MHC_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
   if (p->projection_limiteur_id < 0 || p->projection_limiteur_id > 7)
     return set_err(MHC_ERR_UNSUPPORTED, "projection-limiteur-id must be 0..7 (TypesMahyco.h limiteur)");
-  if (p->is_euler_scheme != MHC_EULER_FULL) return set_err(MHC_ERR_UNSUPPORTED, "is-euler-scheme must be Full");
+  if (p->is_euler_scheme != MHC_EULER_FULL && p->is_euler_scheme != MHC_EULER_X && p->is_euler_scheme != MHC_EULER_Y &&
+      !(p->is_euler_scheme == MHC_EULER_Z && p->dim == 3))
+    return set_err(MHC_ERR_UNSUPPORTED, "is-euler-scheme must be Full, X, Y or (3D) Z");
   if (p->projection_simple_pente && !p->projection_pente_borne)
     return set_err(MHC_ERR_UNSUPPORTED, "projection-simple-pente needs projection-pente-borne (MahycoModule.cc:47-51)");
   if (p->projection_pente_borne && p->ordre_projection != 2)
@@ -391,6 +393,8 @@ int validate(const mhc_case_params* p) {
     if (!(o.shear_modulus > 0.) || !(o.yield_strength > 0.)) return set_err(MHC_ERR_ARG, "shear modulus and yield strength must be > 0");
   }
   for (int e = 0; e < p->nb_env; ++e) {
+    if (p->env[e].depot_type < MHC_DEPOT_NONE || p->env[e].depot_type > MHC_DEPOT_SUPER_GAUSSIAN)
+      return set_err(MHC_ERR_ARG, "energy deposit kind");
     if (p->env[e].density_damage_thresold != 0.0 || p->env[e].tension_damage_thresold > -1.e12)
       return set_err(MHC_ERR_UNSUPPORTED, "damage thresholds other than the defaults");
     if (p->env[e].eos < 0 || p->env[e].eos > 2) return set_err(MHC_ERR_ARG, "eos kind");
@@ -653,6 +657,16 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
     if ((r = fetch(st, pa, a.data(), NN * 8)) || (r = fetch(st, pb, b.data(), NN * 8)) || (r = fetch(st, pc, c.data(), NN * 8)))
       return r;
     for (long long i = 0; i < NN; ++i) { host[3 * i] = a[i]; host[3 * i + 1] = b[i]; host[3 * i + 2] = c[i]; }
+    const int es = h->P.is_euler_scheme;
+    if (name[0] == 'N' && h->P.with_projection && es >= MHC_EULER_X && es <= MHC_EULER_Z) {
+      // per-axis Euler: the remapped axis is back on the initial grid
+      const int ax = es - MHC_EULER_X;
+      const Mesh& M = h->M;
+      for (long long n = 0; n < NN; ++n) {
+        const long long idx = ax == 0 ? n % M.nnx : (ax == 1 ? (n / M.nnx) % M.nny : n / ((long long)M.nnx * M.nny));
+        host[3 * n + ax] = M.o[ax] + (int)idx * M.h[ax];
+      }
+    }
     return 3 * NN;
   }
   return set_err(MHC_ERR_ARG, std::string("unknown field ") + name);

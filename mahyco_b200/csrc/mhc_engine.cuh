@@ -186,11 +186,15 @@ inline int node_cols_mask(const mhc_case* h) {
   return m;
 }
 
+// directions the remap does not sweep: one cell thick, or not the axis of a
+// per-axis Euler scheme (RemapADIService.cc:26-32)
 inline int skip_mask(const mhc_case* h) {
   int m = 0;
   if (h->M.ncx == 1) m |= 1;
   if (h->M.ncy == 1) m |= 2;
   if (h->DIM == 3 && h->M.ncz == 1) m |= 4;
+  const int s = h->P.is_euler_scheme;
+  if (s >= MHC_EULER_X && s <= MHC_EULER_Z) m |= 7 & ~(1 << (s - MHC_EULER_X));
   return m;
 }
 

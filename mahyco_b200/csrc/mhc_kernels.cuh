@@ -690,6 +690,23 @@ __device__ __forceinline__ void pressure_bcs(const Mesh& M, const mhc_case_param
 // (kb_hourglass), so this pass only writes the uncorrected velocity into
 // the dual-remap scratch Ud[0] (unused by a Lagrangian run).
 // ---------------------------------------------------------------------------
+// node positions at the start of a cycle (RemapADIService.cc:62-83): the
+// initial grid after a Full Euler remap; after a per-axis one, the remapped
+// axis on the initial grid and the others where the last Lagrangian step
+// left them; a Lagrangian run's last positions
+__device__ __forceinline__ R3 cycle_start_position(const Mesh& M, const mhc_case_params& P, const Fields& F,
+                                                   int i, int j, int k, long long n) {
+  if (!P.with_projection) return R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+  const R3 x0 = node_x0(M, i, j, k);
+  const int s = P.is_euler_scheme;
+  if (s < MHC_EULER_X || s > MHC_EULER_Z) return x0;
+  R3 x = {F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+  if (s == MHC_EULER_X) x.x = x0.x;
+  else if (s == MHC_EULER_Y) x.y = x0.y;
+  else x.z = x0.z;
+  return x;
+}
+
 template <int DIM, bool EL, bool HG>
 __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   const long long n = bx * (long long)CT + threadIdx.x;
@@ -750,7 +767,7 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
     else if (bc.kind == MHC_BC_VZ) vz = bc.value;
   }
   pressure_bcs<DIM>(M, P, F, i, j, k, n, dth, t, vx, vy, vz);
-  const R3 x = P.with_projection ? node_x0(M, i, j, k) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+  const R3 x = cycle_start_position(M, P, F, i, j, k, n);
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
 }
@@ -1096,6 +1113,13 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
         value += o.depot_dependance[1] * cc.y;
         value += o.depot_dependance[2] * cc.z;
         value += o.depot_dependance[3] * t;
+      } else if (o.depot_type == MHC_DEPOT_SUPER_GAUSSIAN) {
+        // exp(-(y dY)^power) then exp(-(x dX)^power); CUDA's exp and pow,
+        // within a few ulps of the reference's libm
+        const double ay = cc.y * o.depot_dependance[1];
+        value *= exp(-pow(ay, o.depot_power));
+        const double ax = cc.x * o.depot_dependance[0];
+        value *= exp(-pow(ax, o.depot_power));
       }
       if (fabs(cc.x - o.depot_origin[0]) > o.depot_cutoff[0]) value = 0.;
       if (fabs(cc.y - o.depot_origin[1]) > o.depot_cutoff[1]) value = 0.;
@@ -1221,7 +1245,30 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   const double thr = P.remap_threshold;
   double u[NV];
   for (int v = 0; v < NV; ++v) u[v] = Ufin[v * N + c];
-  const double Veul = F.Veul[c];
+  double Veul;
+  if (P.is_euler_scheme >= MHC_EULER_X && P.is_euler_scheme <= MHC_EULER_Z) {
+    // RemapADIService::computeVolumeEuler (RemapADIService.cc:579-645): the
+    // receiving cell has the remapped axis on the initial grid and the other
+    // coordinates of this iteration's Lagrangian step; its corner normals
+    // replace the Lagrangian ones for the next node pass
+    const int ax = P.is_euler_scheme - MHC_EULER_X;
+    int i, j, k;
+    cell_ijk(M, c, i, j, k);
+    R3 coord[8], cqs[8];
+    for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+      int a, b, d;
+      local_node_offset(l, a, b, d);
+      const long long nn = node_id(M, i + a, j + b, DIM == 3 ? k + d : 0);
+      const R3 x0 = node_x0(M, i + a, j + b, DIM == 3 ? k + d : 0);
+      coord[l] = R3{ax == 0 ? x0.x : F.Xn[0][nn], ax == 1 ? x0.y : F.Xn[1][nn],
+                    DIM == 3 ? (ax == 2 ? x0.z : F.Xn[2][nn]) : 0.};
+    }
+    Veul = cell_volume<DIM>(coord, cqs);
+    store_cqs<DIM>(F, N, c, cqs);
+    F.Veul[c] = Veul;
+  } else {
+    Veul = F.Veul[c];
+  }
   const uint8_t old = F.mask[c];
   uint8_t nm = old;
   for (int q = 0; q < NE; ++q) {

@@ -263,6 +263,8 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
         const int d = (i + sens) % M.dim;
         const int ncd = d == 0 ? M.ncx : (d == 1 ? M.ncy : M.ncz);
         if (ncd == 1) continue;
+        if (P.is_euler_scheme >= MHC_EULER_X && P.is_euler_scheme <= MHC_EULER_Z && d != P.is_euler_scheme - MHC_EULER_X)
+          continue;
         if (cnt < k) done |= 1 << d;
         ++cnt;
       }

@@ -75,14 +75,16 @@ def write_ensight(h, out_dir: str, variables: list[str], time: float) -> list[st
     nx, ny, nz = p.nx, p.ny, (p.nz if dim == 3 else 1)
     nnx, nny, nnz = nx + 1, ny + 1, (nz + 1 if dim == 3 else 1)
     nn = h.nnode
-    if p.with_projection:
-        # Euler scheme: the mesh is back on the initial grid
+    if p.with_projection and p.is_euler_scheme == 0:
+        # Full Euler scheme: the mesh is back on the initial grid
         a, b, c = np.meshgrid(np.arange(nnx), np.arange(nny), np.arange(nnz), indexing="ij")
         a, b, c = (t.transpose(2, 1, 0).ravel() for t in (a, b, c))
         xs = p.origin[0] + a * (p.lx / p.nx)
         ys = p.origin[1] + b * (p.ly / p.ny)
         zs = p.origin[2] + c * (p.lz / p.nz) if dim == 3 else np.zeros(nn)
     else:
+        # Lagrangian run, or per-axis Euler (the remapped axis is on the
+        # initial grid, the others Lagrangian)
         xyz = h.field("NodeCoord").reshape(-1, 3)
         xs, ys, zs = xyz[:, 0], xyz[:, 1], xyz[:, 2] if dim == 3 else np.zeros(nn)
     written = []

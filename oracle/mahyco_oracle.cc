@@ -1092,10 +1092,12 @@ static void compute_pression_moyenne(Case& C) {
  * updateEnergyAndPressureforGP (1623-1698, non-CSTS branch),
  * updateEnergyAndPressurebyNewton (1506-1571) or
  * updateEnergyAndPressureExplicite (1484-1502) */
-/* MahycoModule::DepotEnergy (MahycoModule.cc:1364-1417), constant and
- * linear deposits: value x deltat added to the environment's internal
- * energy, zero outside [Tdebut, Tfin] and beyond the x / y cutoffs around
- * the origin (the Lagrangian cell centre of this iteration) */
+/* MahycoModule::DepotEnergy (MahycoModule.cc:1364-1417), constant, linear
+ * and super-Gaussian deposits: value x deltat added to the environment's
+ * internal energy, zero outside [Tdebut, Tfin] and beyond the x / y cutoffs
+ * around the origin (the Lagrangian cell centre of this iteration).  The
+ * super-Gaussian profile multiplies by exp(-(y dY)^power), then by
+ * exp(-(x dX)^power), with std::exp and std::pow as the reference does. */
 static void depot_energy(Case& C) {
   for (int e = 0; e < C.nenv; ++e) {
     const mhc_env_params& o = C.P.env[e];
@@ -1111,6 +1113,11 @@ static void depot_energy(Case& C) {
         value += o.depot_dependance[1] * cc.y;
         value += o.depot_dependance[2] * cc.z;
         value += o.depot_dependance[3] * C.t;
+      } else if (o.depot_type == MHC_DEPOT_SUPER_GAUSSIAN) {
+        const double ay = cc.y * o.depot_dependance[1];
+        value *= std::exp(-std::pow(ay, o.depot_power));
+        const double ax = cc.x * o.depot_dependance[0];
+        value *= std::exp(-std::pow(ax, o.depot_power));
       }
       if (std::fabs(cc.x - o.depot_origin[0]) > o.depot_cutoff[0]) value = 0.;
       if (std::fabs(cc.y - o.depot_origin[1]) > o.depot_cutoff[1]) value = 0.;
@@ -1984,11 +1991,42 @@ static int remap_variables(Case& C) {
   return ST_OK;
 }
 
+/* RemapADIService::computeVolumeEuler (RemapADIService.cc:579-645): the
+ * corner normals and volumes of the receiving grid, once the Euler axis of
+ * the node positions is back on the initial grid.  The corner normals
+ * replace those of the Lagrangian step (the next node pass uses them). */
+static void compute_volume_euler(Case& C) {
+  for (long c = 0; c < C.ncell; ++c) {
+    R3 coord[8];
+    gather_cell_coords(C, c, coord);
+    if (C.dim == 3) {
+      R3 fc[6];
+      hex_face_centres(coord, fc);
+      compute_cqs3(coord, fc, &C.cqs[c * 8]);
+    } else {
+      compute_cqs2(coord, &C.cqs[c * 4]);
+    }
+  }
+  for (long c = 0; c < C.ncell; ++c) {
+    double volume = 0.;
+    for (int n = 0; n < C.nbn; ++n) volume += dot(C.coord[C.cnode(c, n)], C.cqs[c * C.nbn + n]);
+    C.euler_volume[c] = volume / C.dim;
+  }
+}
+
+/* is-euler-scheme X / Y / Z: the only remapped axis (-1 for Full / NON) */
+static int euler_axis(const Case& C) {
+  const int s = C.P.is_euler_scheme;
+  return (s >= MHC_EULER_X && s <= MHC_EULER_Z) ? s - MHC_EULER_X : -1;
+}
+
 /* RemapADIService::appliRemap (RemapADIService.cc:15-90) */
 static int appli_remap(Case& C) {
+  const int axis = euler_axis(C);
   for (int i = 0; i < C.dim; ++i) {
     int d = (i + C.sens_projection) % C.dim;
     if (C.ncd(d) == 1) continue;
+    if (axis >= 0 && d != axis) continue;
     compute_grad_phi_face(C, d);
     compute_grad_phi_cell(C, d);
     compute_upwind_face_quantities(C, d);
@@ -1996,7 +2034,18 @@ static int appli_remap(Case& C) {
     compute_dual_uremap(C, d);
   }
   C.sens_projection = (C.sens_projection + 1) % C.dim;
-  if (C.P.is_euler_scheme == MHC_EULER_FULL) C.coord = C.coord0;
+  if (C.P.is_euler_scheme == MHC_EULER_FULL) {
+    C.coord = C.coord0;
+  } else if (axis >= 0) {
+    for (long n = 0; n < C.nnode; ++n) {
+      R3& x = C.coord[n];
+      const R3& x0 = C.coord0[n];
+      if (axis == 0) x.x = x0.x;
+      else if (axis == 1) x.y = x0.y;
+      else x.z = x0.z;
+    }
+    compute_volume_euler(C);
+  }
   return remap_variables(C);
 }
 

@@ -67,6 +67,11 @@ CASES = {
     # and energy grow from zero, so their first lines carry relative
     # differences up to 3e-10 that fall to 1e-13 as they grow
     "CAS_Compression_isotherme_ALU_monodimX": {"tol": 5e-10},
+    # per-axis Euler (is-euler-scheme Y), super-Gaussian energy deposit,
+    # ONECELL init, Mie-Gruneisen; 200 000 equal cell masses averaged in one
+    # running sum carry 3.7e-12 of rounding (the reference's four per-rank
+    # sums 2.5e-13), hence the bound
+    "CAS_plaque_demi_euler_Y_depot_Gaussian": {"mpi_ranks": 4, "tol": 1e-11},
 }
 # variables the Ensight writer of mahyco_b200.output produces
 ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy", "PseudoViscosity",

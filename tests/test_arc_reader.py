@@ -118,8 +118,8 @@ def test_gnuplot_writer_format(tmp_path):
 
 
 def test_energy_deposit_options(tmp_path):
-    """<energy-depot> of an environment (Mahyco.axl:335-380): constant and
-    linear deposits are read, the super-Gaussian one is refused."""
+    """<energy-depot> of an environment (Mahyco.axl:335-380): constant,
+    linear and super-Gaussian deposits with their power (default 4)."""
     dep = ("<energy-depot><type>DepotLineaire</type><valeur-source-energie>3.5e3</valeur-source-energie>"
            "<origine>0.1 0.2 0.</origine><dependanceX>2.</dependanceX><dependanceT>5.</dependanceT>"
            "<cutoffY>0.5</cutoffY><Tdebut>1e-3</Tdebut><Tfin>2e-3</Tfin></energy-depot>")
@@ -131,10 +131,27 @@ def test_energy_deposit_options(tmp_path):
     assert (e.depot_type, e.depot_value, list(e.depot_origin)) == (2, 3.5e3, [0.1, 0.2, 0.0])
     assert list(e.depot_dependance) == [2.0, 0.0, 0.0, 5.0] and list(e.depot_cutoff) == [1000.0, 0.5]
     assert (e.depot_tdebut, e.depot_tfin, p.env[1].depot_type) == (1e-3, 2e-3, 0)
+    assert e.depot_power == 4.0
     g = tmp_path / "g.arc"
-    g.write_text(text.replace("DepotLineaire", "DepotSuperGaussian"))
+    g.write_text(text.replace("DepotLineaire", "DepotSuperGaussian").replace("<Tfin>", "<power>8.</power><Tfin>"))
+    e = read_arc(str(g))[0].env[0]
+    assert (e.depot_type, e.depot_power) == (3, 8.0)
+
+
+def test_per_axis_euler_scheme(tmp_path):
+    """<is-euler-scheme> of RemapADI (RemapADI.axl:169): Full, X, Y, Z; NON
+    (a remap that never returns to the grid) is refused."""
+    text = open(ARC).read()
+    assert read_arc(ARC)[0].is_euler_scheme == 0
+    for name, v in (("X", 2), ("Y", 3), ("Z", 4), ("Full", 0)):
+        f = tmp_path / f"e{name}.arc"
+        f.write_text(text.replace("</ordre-projection>",
+                                  f"</ordre-projection><is-euler-scheme>{name}</is-euler-scheme>", 1))
+        assert read_arc(str(f))[0].is_euler_scheme == v
+    f = tmp_path / "non.arc"
+    f.write_text(text.replace("</ordre-projection>", "</ordre-projection><is-euler-scheme>NON</is-euler-scheme>", 1))
     with pytest.raises(NotImplementedError):
-        read_arc(str(g))
+        read_arc(str(f))
 
 
 def test_pressure_surfaces_and_onecell(tmp_path):

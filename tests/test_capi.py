@@ -66,6 +66,11 @@ def test_rejects_options_outside_the_hot_path():
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p.with_projection, p.nb_env = 0, 2          # elasto with two environments
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p = mb.default_params()
+    p.is_euler_scheme = 1                       # is-euler-scheme NON
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.dim, p.is_euler_scheme = 2, 4             # per-axis Euler along z on a 2D mesh
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
 
 
 @pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", "x") != "" and os.path.exists("/dev/nvidia0"),
