@@ -64,7 +64,9 @@ int engine_rebuild(Engine* e) {
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
-    int euler = h->P.with_projection ? 1 : 0;
+    // 0 Lagrangian, 1 Full Euler remap, 2 per-axis Euler remap
+    const int es = h->P.is_euler_scheme;
+    int euler = h->P.with_projection ? ((es >= MHC_EULER_X && es <= MHC_EULER_Z) ? 2 : 1) : 0;
     int sens = (int)((h->it_host - 1) % h->DIM);
     const int el = case_elasto(h) ? 1 : 0, hg = case_hourglass(h) ? 1 : 0;
     const int lim = node_sweep_mode(h->P), clim = cell_sweep_mode(h->P);
@@ -137,20 +139,24 @@ void launch_init(Engine* e) {
   }
 }
 
-template <int DIM, bool EL, bool HG>
+template <int DIM, bool EL, bool HG, bool LAG>
 void lag_nodes_launch(Engine* e, Group& g) {
-  plaunch(e, kb_lagrange_nodes<DIM, EL, HG>, CT, 0, g.lag_nodes);
+  plaunch(e, kb_lagrange_nodes<DIM, EL, HG, LAG>, CT, 0, g.lag_nodes);
   if (HG) plaunch(e, kb_hourglass<DIM>, CT, 0, g.lag_nodes);
 }
 
+// elasto-plasticity and the anti-hourglass correction come with Lagrangian
+// runs only (validated at creation)
 template <int DIM>
 void lag_nodes_dispatch(Engine* e, Group& g) {
-  if (g.EL) {
-    if (g.HG) lag_nodes_launch<DIM, true, true>(e, g);
-    else lag_nodes_launch<DIM, true, false>(e, g);
+  if (g.EULER) {
+    lag_nodes_launch<DIM, false, false, false>(e, g);
+  } else if (g.EL) {
+    if (g.HG) lag_nodes_launch<DIM, true, true, true>(e, g);
+    else lag_nodes_launch<DIM, true, false, true>(e, g);
   } else {
-    if (g.HG) lag_nodes_launch<DIM, false, true>(e, g);
-    else lag_nodes_launch<DIM, false, false>(e, g);
+    if (g.HG) lag_nodes_launch<DIM, false, true, true>(e, g);
+    else lag_nodes_launch<DIM, false, false, true>(e, g);
   }
 }
 
@@ -210,11 +216,16 @@ void launch_remap(Engine* e) {
     int K = group_dirs(e, g, dirs);
     {
       StageTimer tm(e, MHC_STAGE_FINALIZE_CELLS);
+      if (g.EULER == 2) {
+        if (g.DIM == 2) plaunch(e, kb_euler_volume<2>, CT, 0, g.fin_cells);
+        else plaunch(e, kb_euler_volume<3>, CT, 0, g.fin_cells);
+      }
       DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_cells<DIM_, NE_>, CT, 0, g.fin_cells, K)));
     }
-    if (K > 0) {
+    {
       StageTimer tm(e, MHC_STAGE_FINALIZE_NODES);
-      DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_nodes<DIM_>, CT, 0, g.fin_nodes, K)));
+      if (K > 0) DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_nodes<DIM_>, CT, 0, g.fin_nodes, K)));
+      if (g.EULER == 2) plaunch(e, kb_euler_axis_reset, CT, 0, g.fin_nodes);
     }
   }
 }
@@ -657,16 +668,6 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
     if ((r = fetch(st, pa, a.data(), NN * 8)) || (r = fetch(st, pb, b.data(), NN * 8)) || (r = fetch(st, pc, c.data(), NN * 8)))
       return r;
     for (long long i = 0; i < NN; ++i) { host[3 * i] = a[i]; host[3 * i + 1] = b[i]; host[3 * i + 2] = c[i]; }
-    const int es = h->P.is_euler_scheme;
-    if (name[0] == 'N' && h->P.with_projection && es >= MHC_EULER_X && es <= MHC_EULER_Z) {
-      // per-axis Euler: the remapped axis is back on the initial grid
-      const int ax = es - MHC_EULER_X;
-      const Mesh& M = h->M;
-      for (long long n = 0; n < NN; ++n) {
-        const long long idx = ax == 0 ? n % M.nnx : (ax == 1 ? (n / M.nnx) % M.nny : n / ((long long)M.nnx * M.nny));
-        host[3 * n + ax] = M.o[ax] + (int)idx * M.h[ax];
-      }
-    }
     return 3 * NN;
   }
   return set_err(MHC_ERR_ARG, std::string("unknown field ") + name);

@@ -601,10 +601,13 @@ __device__ __forceinline__ void face_node_rt(int dim, int d, int q, int& a, int&
   else { a = s1; b = s2; }
 }
 
+// Compiled into the Lagrangian instances of the node pass only (the only
+// runs allowed pressure surfaces): its local arrays and loops stay off the
+// register budget of the node pass of the remapped runs.
 template <int DIM>
-__device__ __forceinline__ void pressure_bcs(const Mesh& M, const mhc_case_params& P, const Fields& F, int i, int j,
-                                             int k, long long n, double dth, double t, double& vx, double& vy,
-                                             double& vz) {
+__device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params& P, const Fields& F, int i, int j,
+                                        int k, long long n, double dth, double t, R3 v) {
+  double vx = v.x, vy = v.y, vz = v.z;
   constexpr int NQ = DIM == 3 ? 4 : 2;
   const double w = DIM == 2 ? .5 : .25, wc = DIM == 2 ? .25 : .125;
   for (int b = 0; b < P.nb_bc; ++b) {
@@ -676,6 +679,7 @@ __device__ __forceinline__ void pressure_bcs(const Mesh& M, const mhc_case_param
       }
     }
   }
+  return R3{vx, vy, vz};
 }
 
 // ---------------------------------------------------------------------------
@@ -690,24 +694,7 @@ __device__ __forceinline__ void pressure_bcs(const Mesh& M, const mhc_case_param
 // (kb_hourglass), so this pass only writes the uncorrected velocity into
 // the dual-remap scratch Ud[0] (unused by a Lagrangian run).
 // ---------------------------------------------------------------------------
-// node positions at the start of a cycle (RemapADIService.cc:62-83): the
-// initial grid after a Full Euler remap; after a per-axis one, the remapped
-// axis on the initial grid and the others where the last Lagrangian step
-// left them; a Lagrangian run's last positions
-__device__ __forceinline__ R3 cycle_start_position(const Mesh& M, const mhc_case_params& P, const Fields& F,
-                                                   int i, int j, int k, long long n) {
-  if (!P.with_projection) return R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
-  const R3 x0 = node_x0(M, i, j, k);
-  const int s = P.is_euler_scheme;
-  if (s < MHC_EULER_X || s > MHC_EULER_Z) return x0;
-  R3 x = {F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
-  if (s == MHC_EULER_X) x.x = x0.x;
-  else if (s == MHC_EULER_Y) x.y = x0.y;
-  else x.z = x0.z;
-  return x;
-}
-
-template <int DIM, bool EL, bool HG>
+template <int DIM, bool EL, bool HG, bool LAG>
 __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   const long long n = bx * (long long)CT + threadIdx.x;
   if (n >= M.nnode) return;
@@ -766,8 +753,15 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
     else if (bc.kind == MHC_BC_VY) vy = bc.value;
     else if (bc.kind == MHC_BC_VZ) vz = bc.value;
   }
-  pressure_bcs<DIM>(M, P, F, i, j, k, n, dth, t, vx, vy, vz);
-  const R3 x = cycle_start_position(M, P, F, i, j, k, n);
+  if constexpr (LAG) {
+    const R3 v = pressure_bcs<DIM>(M, P, F, i, j, k, n, dth, t, R3{vx, vy, vz});
+    vx = v.x; vy = v.y; vz = v.z;
+  }
+  // positions at the start of the cycle: the initial grid after a Full
+  // Euler remap (RemapADIService.cc:62-64); otherwise the last ones (a
+  // per-axis remap has put its axis back on the grid, kb_euler_axis_reset)
+  const R3 x = (!LAG && P.is_euler_scheme == MHC_EULER_FULL) ? node_x0(M, i, j, k)
+                                                             : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
 }
@@ -843,7 +837,10 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
     else if (bc.kind == MHC_BC_VY) vy = bc.value;
     else if (bc.kind == MHC_BC_VZ) vz = bc.value;
   }
-  pressure_bcs<DIM>(M, P, F, i, j, k, n, 0.5 * (F.s->old_dt + dt), t, vx, vy, vz);
+  {
+    const R3 v = pressure_bcs<DIM>(M, P, F, i, j, k, n, 0.5 * (F.s->old_dt + dt), t, R3{vx, vy, vz});
+    vx = v.x; vy = v.y; vz = v.z;
+  }
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   F.Xn[0][n] = F.Xp[0][n] + dt * vx; F.Xn[1][n] = F.Xp[1][n] + dt * vy; F.Xn[2][n] = F.Xp[2][n] + dt * vz;
 }
@@ -1245,30 +1242,7 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   const double thr = P.remap_threshold;
   double u[NV];
   for (int v = 0; v < NV; ++v) u[v] = Ufin[v * N + c];
-  double Veul;
-  if (P.is_euler_scheme >= MHC_EULER_X && P.is_euler_scheme <= MHC_EULER_Z) {
-    // RemapADIService::computeVolumeEuler (RemapADIService.cc:579-645): the
-    // receiving cell has the remapped axis on the initial grid and the other
-    // coordinates of this iteration's Lagrangian step; its corner normals
-    // replace the Lagrangian ones for the next node pass
-    const int ax = P.is_euler_scheme - MHC_EULER_X;
-    int i, j, k;
-    cell_ijk(M, c, i, j, k);
-    R3 coord[8], cqs[8];
-    for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
-      int a, b, d;
-      local_node_offset(l, a, b, d);
-      const long long nn = node_id(M, i + a, j + b, DIM == 3 ? k + d : 0);
-      const R3 x0 = node_x0(M, i + a, j + b, DIM == 3 ? k + d : 0);
-      coord[l] = R3{ax == 0 ? x0.x : F.Xn[0][nn], ax == 1 ? x0.y : F.Xn[1][nn],
-                    DIM == 3 ? (ax == 2 ? x0.z : F.Xn[2][nn]) : 0.};
-    }
-    Veul = cell_volume<DIM>(coord, cqs);
-    store_cqs<DIM>(F, N, c, cqs);
-    F.Veul[c] = Veul;
-  } else {
-    Veul = F.Veul[c];
-  }
+  const double Veul = F.Veul[c];
   const uint8_t old = F.mask[c];
   uint8_t nm = old;
   for (int q = 0; q < NE; ++q) {
@@ -1457,6 +1431,44 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
       F.ec[q * N + c] = ce[q]; F.eq[q * N + c] = qe[q];
     }
   }
+}
+
+// per-axis Euler remap (is-euler-scheme X / Y / Z), after the sweeps:
+// RemapADIService::computeVolumeEuler (RemapADIService.cc:579-645) gives
+// the receiving cell the remapped axis on the initial grid and the other
+// coordinates of this iteration's Lagrangian step; its corner normals
+// replace the Lagrangian ones for the next node pass
+template <int DIM>
+__device__ __forceinline__ void body_euler_volume(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  long long c = bx * (long long)CT + threadIdx.x;
+  if (c >= M.ncell) return;
+  const long long N = M.ncell;
+  const int ax = P.is_euler_scheme - MHC_EULER_X;
+  int i, j, k;
+  cell_ijk(M, c, i, j, k);
+  R3 coord[8], cqs[8];
+  for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+    int a, b, d;
+    local_node_offset(l, a, b, d);
+    const long long nn = node_id(M, i + a, j + b, DIM == 3 ? k + d : 0);
+    const R3 x0 = node_x0(M, i + a, j + b, DIM == 3 ? k + d : 0);
+    coord[l] = R3{ax == 0 ? x0.x : F.Xn[0][nn], ax == 1 ? x0.y : F.Xn[1][nn],
+                  DIM == 3 ? (ax == 2 ? x0.z : F.Xn[2][nn]) : 0.};
+  }
+  F.Veul[c] = cell_volume<DIM>(coord, cqs);
+  store_cqs<DIM>(F, N, c, cqs);
+}
+
+// ... and the remapped axis of the node positions back on the initial grid
+// (RemapADIService.cc:65-82); the next Lagrangian step starts from them
+__device__ __forceinline__ void body_euler_axis_reset(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  long long n = bx * (long long)CT + threadIdx.x;
+  if (n >= M.nnode) return;
+  const int ax = P.is_euler_scheme - MHC_EULER_X;
+  int i, j, k;
+  node_ijk(M, n, i, j, k);
+  const R3 x0 = node_x0(M, i, j, k);
+  F.Xn[ax][n] = ax == 0 ? x0.x : (ax == 1 ? x0.y : x0.z);
 }
 
 // remap finalize, nodes: velocity from projected momentum and node mass

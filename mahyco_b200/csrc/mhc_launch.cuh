@@ -143,7 +143,8 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
 #define MHC_NODES_MIN_BLOCKS 4
 #endif
 
-template <int DIM, bool EL, bool HG>
+// LAG: a Lagrangian run (no remap): last positions, pressure surfaces
+template <int DIM, bool EL, bool HG, bool LAG>
 __global__ void __launch_bounds__(CT, MHC_NODES_MIN_BLOCKS) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_NODES>(C, L, w_);
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(CT, MHC_NODES_MIN_BLOCKS) kb_lagrange_nodes(co
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_lagrange_nodes<DIM, EL, HG>(M, *C[wi.c].P, F, wi.x);
+    body_lagrange_nodes<DIM, EL, HG, LAG>(M, *C[wi.c].P, F, wi.x);
   }
 }
 
@@ -309,6 +310,27 @@ __global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
     body_remap_finalize_nodes<DIM>(M, F, ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_euler_volume(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    body_euler_volume<DIM>(C[wi.c].M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+static __global__ void __launch_bounds__(CT) kb_euler_axis_reset(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    body_euler_axis_reset(C[wi.c].M, *C[wi.c].P, F, wi.x);
   }
 }
 

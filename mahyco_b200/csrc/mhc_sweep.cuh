@@ -1150,14 +1150,17 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
       hp = 0.5 * (x_rr - x);
     }
   }
-  // limited gradients of the velocity components (inner nodes only)
+  // limited gradients of the velocity components (inner nodes only).  The
+  // backward difference of a node is the forward difference of the node
+  // before it (same operands), taken from the previous lane: an inner node
+  // (id > 0) sits one lane after its back neighbour on the same line
   double g[3], g_l[3], g_r[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     g[q] = 0.;
+    const double gfw = LIM != LIM_ORDER1 ? div_rn(ph_r[q] - ph[q], x_r - x) : 0.;
+    const double gbw = __shfl_up_sync(FULL, gfw, 1);
     if (LIM != LIM_ORDER1 && inner) {
-      const double gfw = div_rn(ph_r[q] - ph[q], x_r - x);
-      const double gbw = div_rn(ph[q] - ph_l[q], x - x_l);
       if constexpr (LIM == LIM_GEN)
         g[q] = generalized_gradient(A.limiter, gfw, gbw, ph_r[q], ph_l[q], h0, hp, hm, A.simple_pente);
       else
@@ -1279,14 +1282,15 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
   const double dt = F.s->dt;
   const int order2 = LIM == LIM_ORDER1 ? 0 : A.order - 1;  // ordre-projection - 1
   // carried state: 1 = node q-1, 2 = node q-2, 3 = node q-3
-  double U1[5], U2[5], ph1[4], ph2[4], ph3[4], g1[3], g2[3], g3[3];
+  // fd1: forward difference of node q-2 (= backward difference of q-1)
+  double U1[5], U2[5], ph1[4], ph2[4], ph3[4], g1[3], g2[3], g3[3], fd1[3];
   double x1 = 0., x2 = 0., x3 = 0., ffm1 = 0., ffm2 = 0., ffm3 = 0.;
 #pragma unroll
   for (int q = 0; q < 5; ++q) U1[q] = U2[q] = 0.;
 #pragma unroll
   for (int q = 0; q < 4; ++q) ph1[q] = ph2[q] = ph3[q] = 0.;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) g1[q] = g2[q] = g3[q] = 0.;
+  for (int q = 0; q < 3; ++q) g1[q] = g2[q] = g3[q] = fd1[q] = 0.;
   const int qs = o0 - 2 > 0 ? o0 - 2 : 0;
   for (int q = qs; q <= o1 + 1; ++q) {
     double U[5] = {0., 0., 0., 0., 0.}, ph[4] = {0., 0., 0., 0.}, x = 0., ffm = 0.;
@@ -1294,17 +1298,17 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
       if (D == 1) node_state<DIM, NE, D>(M, F, A, i, q, tb, q, U, ph, x, ffm);
       else node_state<DIM, NE, D>(M, F, A, i, tb, q, q, U, ph, x, ffm);
     }
-    // limited gradients of node q-1 (inner nodes only)
+    // limited gradients of node q-1 (inner nodes only); its backward
+    // difference is the forward difference of node q-2, carried from the
+    // previous iteration (valid from the second iteration on, the first
+    // node whose gradient an update needs)
     const int m = q - 1;
-    double gm[3];
+    double gm[3], fd[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       gm[c] = 0.;
-      if (LIM != LIM_ORDER1 && m > 0 && m < nn - 1) {
-        const double gfw = div_rn(ph[c] - ph1[c], x - x1);
-        const double gbw = div_rn(ph1[c] - ph2[c], x1 - x2);
-        gm[c] = limited_gradient_t<LIM>(gbw, gfw);
-      }
+      fd[c] = LIM != LIM_ORDER1 ? div_rn(ph[c] - ph1[c], x - x1) : 0.;
+      if (LIM != LIM_ORDER1 && m > 0 && m < nn - 1) gm[c] = limited_gradient_t<LIM>(fd1[c], fd[c]);
     }
     // update of node o = q - 2: neighbours o-1 (3), o (2), o+1 (1)
     const int o = q - 2;
@@ -1351,7 +1355,7 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
 #pragma unroll
     for (int c = 0; c < 4; ++c) { ph3[c] = ph2[c]; ph2[c] = ph1[c]; ph1[c] = ph[c]; }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) { g3[c] = g2[c]; g2[c] = g1[c]; g1[c] = gm[c]; }
+    for (int c = 0; c < 3; ++c) { g3[c] = g2[c]; g2[c] = g1[c]; g1[c] = gm[c]; fd1[c] = fd[c]; }
     x3 = x2; x2 = x1; x1 = x;
     ffm3 = ffm2; ffm2 = ffm1; ffm1 = ffm;
   }
