@@ -108,7 +108,10 @@ def replica_value(units_per_rank: float, world: int, ms_max: float) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms.  Entering
+    waits for nvidia-smi's first sample (its start-up takes driver locks and
+    must not overlap the timed region); the summary keeps the samples taken
+    after that, and leaving waits for at least one of them."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -117,17 +120,25 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.samples = []
+        self.first = 0
         self.proc = None
+
+    def _wait(self, n: int, limit: float):
+        t0 = time.perf_counter()
+        while len(self.samples) <= n and time.perf_counter() - t0 < limit and self.proc.poll() is None:
+            time.sleep(0.005)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            self._wait(0, 10.0)
         except OSError:
             self.proc = None
+        self.first = len(self.samples)
         return self
 
     def _read(self):
@@ -138,6 +149,7 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            self._wait(self.first, 1.0)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -145,14 +157,15 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
-        if not self.samples:
+        samples = self.samples[self.first:]
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].lower() == "active"})
+        reasons = sorted({names[i] for s in samples for i in range(4) if s[4 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(samples)}
 
 
 def peaks() -> dict:

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -299,6 +300,34 @@ int engine_cycle_graph(Engine* e, int n) {
   return MHC_OK;
 }
 
+// page-locked host blocks are slow to allocate and to free (the driver maps
+// and unmaps them, and a free waits for the device): the small per-case and
+// per-engine blocks are kept in a process-wide free list and reused
+namespace {
+std::mutex g_pinned_mu;
+std::multimap<size_t, void*> g_pinned_free;
+}  // namespace
+
+int pinned_get(size_t bytes, void** out) {
+  {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    auto it = g_pinned_free.lower_bound(bytes);
+    if (it != g_pinned_free.end() && it->first <= 2 * bytes) {
+      *out = it->second;
+      g_pinned_free.erase(it);
+      return MHC_OK;
+    }
+  }
+  CK(cudaMallocHost(out, bytes));
+  return MHC_OK;
+}
+
+void pinned_put(void* p, size_t bytes) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  g_pinned_free.emplace(bytes, p);
+}
+
 int engine_create(cudaStream_t stream, Engine** out) {
   Engine* e = new Engine();
   if (stream) {
@@ -322,7 +351,7 @@ void engine_release(Engine* e) {
   for (int i = 0; i < 2; ++i)
     if (e->ev[i]) cudaEventDestroy(e->ev[i]);
   if (e->d_gather) cudaFreeAsync(e->d_gather, e->stream);
-  if (e->h_gather) { cudaStreamSynchronize(e->stream); cudaFreeHost(e->h_gather); }
+  if (e->h_gather) { cudaStreamSynchronize(e->stream); pinned_put(e->h_gather, e->gather_cap * sizeof(Scalars)); }
   e->d_gather = nullptr; e->h_gather = nullptr; e->gather_cap = 0;
   e->graph = nullptr; e->d_desc = nullptr; e->desc_cap = 0; e->d_ints = nullptr; e->ints_cap = 0;
   e->ev[0] = e->ev[1] = nullptr;
@@ -417,7 +446,7 @@ int validate(const mhc_case_params* p) {
 
 void case_free(mhc_case* h) {
   if (!h) return;
-  if (h->h_scal) { cudaStreamSynchronize(h->stream); cudaFreeHost(h->h_scal); h->h_scal = nullptr; }
+  if (h->h_scal) { cudaStreamSynchronize(h->stream); pinned_put(h->h_scal, 2 * sizeof(Scalars)); h->h_scal = nullptr; }
   for (int i = 0; i < 2; ++i)
     if (h->scal_ev[i]) { cudaEventDestroy(h->scal_ev[i]); h->scal_ev[i] = nullptr; }
   if (h->solo) { engine_destroy(h->solo); h->solo = nullptr; }
@@ -568,9 +597,53 @@ int solo_engine(mhc_case* h) {
   return MHC_OK;
 }
 
+// device -> host copy of `bytes` after the work queued on `s`: through two
+// page-locked staging chunks, so that the device copy of chunk i+1 runs
+// while the host copies chunk i out (a pageable cudaMemcpy stages through
+// the driver at a fraction of the link's bandwidth)
+namespace {
+constexpr size_t kStageChunk = 4u << 20;
+struct Staging {
+  std::mutex mu;
+  char* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // events belong to one device
+};
+Staging g_stage[64];  // per device
+}  // namespace
+
 int fetch(cudaStream_t s, const void* dev, void* host, size_t bytes) {
-  CK(cudaStreamSynchronize(s));
-  CK(cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost));
+  if (bytes == 0) return MHC_OK;
+  if (bytes <= 64 * 1024) {
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost));
+    return MHC_OK;
+  }
+  int device = 0;
+  CK(cudaGetDevice(&device));
+  if (device < 0 || device >= 64) return set_err(MHC_ERR_ARG, "device index");
+  Staging& g = g_stage[device];
+  std::lock_guard<std::mutex> lk(g.mu);
+  for (int b = 0; b < 2; ++b) {
+    if (!g.buf[b]) CK(cudaMallocHost((void**)&g.buf[b], kStageChunk));
+    if (!g.ev[b]) CK(cudaEventCreateWithFlags(&g.ev[b], cudaEventDisableTiming));
+  }
+  const char* src = static_cast<const char*>(dev);
+  char* dst = static_cast<char*>(host);
+  const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+  auto issue = [&](size_t i) -> int {
+    const size_t off = i * kStageChunk, len = std::min(kStageChunk, bytes - off);
+    CK(cudaMemcpyAsync(g.buf[i & 1], src + off, len, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(g.ev[i & 1], s));
+    return MHC_OK;
+  };
+  int r = issue(0);
+  if (r) return r;
+  for (size_t i = 0; i < nch; ++i) {
+    if (i + 1 < nch && (r = issue(i + 1))) return r;
+    CK(cudaEventSynchronize(g.ev[i & 1]));
+    const size_t off = i * kStageChunk, len = std::min(kStageChunk, bytes - off);
+    memcpy(dst + off, g.buf[i & 1], len);
+  }
   return MHC_OK;
 }
 
@@ -592,16 +665,16 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
   for (auto& c : cells) {
     if (strcmp(name, c.n)) continue;
     if (cap < N) return set_err(MHC_ERR_ARG, "capacity too small");
-    std::vector<double> g(N, 0.), e;
-    std::vector<uint8_t> mask(N);
     int r;
-    if ((r = fetch(st, F.mask, mask.data(), N))) return r;
-    if (c.g) { if ((r = fetch(st, c.g, g.data(), N * 8))) return r; }
-    if (env < 0) {
+    if (env < 0) {  // the cell (global) values straight into the caller's buffer
       if (!c.g) for (long long i = 0; i < N; ++i) host[i] = 1.;
-      else memcpy(host, g.data(), N * 8);
+      else if ((r = fetch(st, c.g, host, N * 8))) return r;
       return N;
     }
+    std::vector<double> g(N, 0.), e;
+    std::vector<uint8_t> mask(N);
+    if ((r = fetch(st, F.mask, mask.data(), N))) return r;
+    if (c.g) { if ((r = fetch(st, c.g, g.data(), N * 8))) return r; }
     if (h->NE > 1 && c.e) {
       e.resize(N);
       if ((r = fetch(st, c.e + env * N, e.data(), N * 8))) return r;
@@ -919,7 +992,7 @@ int mhc_case_restore(mhc_case* h, const void* host, long long size) {
 int mhc_scalars_request(mhc_case* h) {
   if (!h) return set_err(MHC_ERR_ARG, "null case");
   if (!h->h_scal) {
-    CK(cudaMallocHost((void**)&h->h_scal, 2 * sizeof(Scalars)));
+    if (int r = pinned_get(2 * sizeof(Scalars), (void**)&h->h_scal)) return r;
     for (int i = 0; i < 2; ++i) CK(cudaEventCreateWithFlags(&h->scal_ev[i], cudaEventDisableTiming));
   }
   const int slot = h->scal_next;
@@ -1106,10 +1179,11 @@ int mhc_batch_poll(mhc_batch* b, int capacity, long long* iteration, int* status
   const int n = (int)e->cases.size();
   if (n > e->gather_cap) {
     if (e->d_gather) CK(cudaFreeAsync(e->d_gather, e->stream));
-    if (e->h_gather) { CK(cudaStreamSynchronize(e->stream)); CK(cudaFreeHost(e->h_gather)); }
+    if (e->h_gather) { CK(cudaStreamSynchronize(e->stream)); pinned_put(e->h_gather, e->gather_cap * sizeof(Scalars)); }
+    e->h_gather = nullptr;
     e->gather_cap = std::max(n, 2 * e->gather_cap);
     CK(cudaMallocAsync((void**)&e->d_gather, e->gather_cap * sizeof(Scalars), e->stream));
-    CK(cudaMallocHost((void**)&e->h_gather, e->gather_cap * sizeof(Scalars)));
+    if (int r = pinned_get(e->gather_cap * sizeof(Scalars), (void**)&e->h_gather)) return r;
   }
   if (n > 0) {
     kb_gather_scalars<<<cdiv(n, 128), 128, 0, e->stream>>>(e->d_desc, n, e->d_gather);
