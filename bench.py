@@ -57,20 +57,8 @@ WORKLOADS = {
 
 
 def build_params(name: str, scale: float = 1.0):
-    from mahyco_b200.cases import sod, sedov, SUPERBEE, MINMOD
-    if name == "bisod3d":
-        ny = max(1, int(round(64 * scale)))
-        return sod(dim=3, n=(256, ny, ny), L=(1.0, 0.25 * ny / 64, 0.25 * ny / 64), bi=True,
-                   limiter=SUPERBEE, deltat_init=1e-5)
-    if name == "sedov3d":
-        n = max(2, int(round(384 * scale)))
-        p = sedov(dim=3, n=(n, n, n), L=1.2 * n / 384, limiter=MINMOD, energy=0.2468, p0=1e-6,
-                  deltat_init=None)
-        p.nb_env = 1  # a single perfect gas (the reference dataset's second environment stays empty)
-        return p
-    if name == "sod2d_lagrange":
-        return sod(dim=2, n=(200, 10), L=(1.0, 0.05), bi=False, remap=False, deltat_max=1e-4)
-    raise ValueError(name)
+    from mahyco_b200.cases import workload
+    return workload(name, scale)
 
 
 # algorithmic bytes per launch of each kernel group: compulsory traffic of

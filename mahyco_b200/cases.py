@@ -282,6 +282,26 @@ def serving_request(kind: str, cells: int) -> CaseParams:
 SERVING_KINDS = ("sedov2d", "sedov3d", "bisod3d", "water_air", "bar")
 
 
+def workload(name: str, scale: float = 1.0) -> CaseParams:
+    """The measured workloads at a linear scale of their mesh (same cell
+    size): "bisod3d" 3D BiSod 256x64x64, 2 materials, superbee;
+    "sedov3d" 3D Sedov 384^3, 1 material, minmod; "sod2d_lagrange" a
+    Lagrangian 2D Sod 200x10."""
+    if name == "bisod3d":
+        ny = max(1, int(round(64 * scale)))
+        return sod(dim=3, n=(256, ny, ny), L=(1.0, 0.25 * ny / 64, 0.25 * ny / 64), bi=True,
+                   limiter=SUPERBEE, deltat_init=1e-5)
+    if name == "sedov3d":
+        n = max(2, int(round(384 * scale)))
+        p = sedov(dim=3, n=(n, n, n), L=1.2 * n / 384, limiter=MINMOD, energy=0.2468, p0=1e-6,
+                  deltat_init=None)
+        p.nb_env = 1  # a single perfect gas (the reference dataset's second environment stays empty)
+        return p
+    if name == "sod2d_lagrange":
+        return sod(dim=2, n=(200, 10), L=(1.0, 0.05), bi=False, remap=False, deltat_max=1e-4)
+    raise ValueError(name)
+
+
 # small parity cases: name -> (builder, cycles).  Initial time steps are
 # large enough that the CFL bound, shocks and mixed cells are exercised.
 PARITY_CASES = {
