@@ -242,7 +242,7 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
 }
 
 #ifndef MHC_SW_MIN_BLOCKS_NODECOLS
-#define MHC_SW_MIN_BLOCKS_NODECOLS 3
+#define MHC_SW_MIN_BLOCKS_NODECOLS 4
 #endif
 template <int DIM, int NE, int D, int LIM>
 __global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_COLS ? MHC_SW_MIN_BLOCKS_NODECOLS

@@ -947,14 +947,17 @@ __device__ __forceinline__ void body_sweep_cells_cols(const Mesh& M, const Field
     if (D == 1) load_plane<DIM, D>(M, F, i, p, tb, P);
     else load_plane<DIM, D>(M, F, i, tb, p, P);
   };
-  // carried state: 1 = previous cell / face, 2 = the one before
-  double phi1[NV], phi2[NV], gf1[NV], gr2[NV], pf2[NV];
+  // carried state: 1 = previous cell / face, 2 = the one before; lc = the
+  // upwind value of face q-1 taken from its back cell q-2 (made one
+  // iteration early, when that cell's limited gradient is known, so that
+  // neither the gradient nor phi of cell q-2 has to be carried)
+  double phi1[NV], gf1[NV], lc[NV], pf2[NV];
   double xc1 = 0., xc2 = 0., fc1 = 0., un1 = 0., un2 = 0., L1 = 0., L2 = 0.;
   const int qs = o0 - 2 > 0 ? o0 - 2 : 0;
   Plane<DIM> cur;       // back plane of cell q
   plane_at(qs, cur);
 #pragma unroll
-  for (int v = 0; v < NV; ++v) phi1[v] = phi2[v] = gf1[v] = gr2[v] = pf2[v] = 0.;
+  for (int v = 0; v < NV; ++v) phi1[v] = gf1[v] = lc[v] = pf2[v] = 0.;
   for (int q = qs; q <= o1 + 1; ++q) {
     const bool cell = q < nd;                 // a cell is loaded at q
     double phi[NV], xc = 0.;
@@ -991,10 +994,10 @@ __device__ __forceinline__ void body_sweep_cells_cols(const Mesh& M, const Field
       // limited gradient of cell q-1 from its back (gf1) and front (gf) faces
       const double gr1 = (LIM != LIM_ORDER1 && q - 1 >= 0 && q - 1 < nd) ? limited_gradient_t<LIM>(gf1[v], gf) : 0.;
       pf1[v] = 0.;
-      if (face_q1)
-        pf1[v] = up_left ? phi2[v] + order2 * (fc1 - xc2) * gr2[v] : phi1[v] + order2 * (fc1 - xc1) * gr1;
+      if (face_q1) pf1[v] = up_left ? lc[v] : phi1[v] + order2 * (fc1 - xc1) * gr1;
+      // face q seen from its back cell q-1 (fc of face q = cur.fc)
+      lc[v] = phi1[v] + order2 * (cur.fc - xc1) * gr1;
       gf1[v] = gf;
-      gr2[v] = gr1;
     }
     // update of cell o = q - 2 from faces o (pf2) and o + 1 (pf1)
     const int o = q - 2;
@@ -1020,7 +1023,6 @@ __device__ __forceinline__ void body_sweep_cells_cols(const Mesh& M, const Field
     // shift
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      phi2[v] = phi1[v];
       phi1[v] = phi[v];
       pf2[v] = pf1[v];
     }
@@ -1216,16 +1218,9 @@ __device__ __forceinline__ void body_sweep_nodes_lanes(const Mesh& M, const Fiel
 // ---------------------------------------------------------------------------
 // projected and phi values, position along D and front mass flux of node
 // (i, j, k) with index id along D
-template <int DIM, int NE, int D>
-__device__ __forceinline__ void node_state(const Mesh& M, const Fields& F, const DualArgs& A, int i, int j, int k,
-                                           int id, double (&U)[5], double (&ph)[4], double& x, double& ffm) {
-  const long long NN = M.nnode, N = M.ncell;
-  const long long n = node_id(M, i, j, k);
-  x = __ldg(F.Xn[D] + n);
-  bool was_inner = false;
-#pragma unroll
-  for (int d = 0; d < DIM; ++d)
-    if (((A.done_dirs >> d) & 1) && node_inner_dir(M, i, j, k, d)) was_inner = true;
+// projected dual variables of node n before this sweep: the previous
+// sweep's output, or momentum, mass and kinetic energy from the node state
+__device__ __forceinline__ void node_u(const Fields& F, const DualArgs& A, long long NN, long long n, double (&U)[5]) {
   if (A.Uin) {
 #pragma unroll
     for (int q = 0; q < 5; ++q) U[q] = __ldg(A.Uin + q * NN + n);
@@ -1234,6 +1229,20 @@ __device__ __forceinline__ void node_state(const Mesh& M, const Fields& F, const
     U[0] = mn * vx; U[1] = mn * vy; U[2] = mn * vz; U[3] = mn;
     U[4] = 0.5 * mn * (vx * vx + vy * vy + vz * vz);
   }
+}
+
+template <int DIM, int NE, int D>
+__device__ __forceinline__ void node_state(const Mesh& M, const Fields& F, const DualArgs& A, int i, int j, int k,
+                                           int id, double (&ph)[4], double& x, double& ffm) {
+  const long long NN = M.nnode, N = M.ncell;
+  const long long n = node_id(M, i, j, k);
+  x = __ldg(F.Xn[D] + n);
+  bool was_inner = false;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d)
+    if (((A.done_dirs >> d) & 1) && node_inner_dir(M, i, j, k, d)) was_inner = true;
+  double U[5];
+  node_u(F, A, NN, n, U);
   if (was_inner) {
     ph[0] = div_rn(U[0], U[3]); ph[1] = div_rn(U[1], U[3]); ph[2] = div_rn(U[2], U[3]);
     ph[3] = div_rn(U[4], U[3]);
@@ -1282,21 +1291,21 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
   const double dt = F.s->dt;
   const int order2 = LIM == LIM_ORDER1 ? 0 : A.order - 1;  // ordre-projection - 1
   // carried state: 1 = node q-1, 2 = node q-2, 3 = node q-3
-  // fd1: forward difference of node q-2 (= backward difference of q-1)
-  double U1[5], U2[5], ph1[4], ph2[4], ph3[4], g1[3], g2[3], g3[3], fd1[3];
+  // fd1: forward difference of node q-2 (= backward difference of q-1);
+  // the projected variables of the node being updated are read again
+  // (cached) rather than carried, to keep registers for resident warps
+  double ph1[4], ph2[4], ph3[4], g1[3], g2[3], g3[3], fd1[3];
   double x1 = 0., x2 = 0., x3 = 0., ffm1 = 0., ffm2 = 0., ffm3 = 0.;
-#pragma unroll
-  for (int q = 0; q < 5; ++q) U1[q] = U2[q] = 0.;
 #pragma unroll
   for (int q = 0; q < 4; ++q) ph1[q] = ph2[q] = ph3[q] = 0.;
 #pragma unroll
   for (int q = 0; q < 3; ++q) g1[q] = g2[q] = g3[q] = fd1[q] = 0.;
   const int qs = o0 - 2 > 0 ? o0 - 2 : 0;
   for (int q = qs; q <= o1 + 1; ++q) {
-    double U[5] = {0., 0., 0., 0., 0.}, ph[4] = {0., 0., 0., 0.}, x = 0., ffm = 0.;
+    double ph[4] = {0., 0., 0., 0.}, x = 0., ffm = 0.;
     if (q < nn) {
-      if (D == 1) node_state<DIM, NE, D>(M, F, A, i, q, tb, q, U, ph, x, ffm);
-      else node_state<DIM, NE, D>(M, F, A, i, tb, q, q, U, ph, x, ffm);
+      if (D == 1) node_state<DIM, NE, D>(M, F, A, i, q, tb, q, ph, x, ffm);
+      else node_state<DIM, NE, D>(M, F, A, i, tb, q, q, ph, x, ffm);
     }
     // limited gradients of node q-1 (inner nodes only); its backward
     // difference is the forward difference of node q-2, carried from the
@@ -1315,8 +1324,7 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
     if (o >= o0 && o < o1) {
       const long long n = D == 1 ? node_id(M, i, o, tb) : node_id(M, i, tb, o);
       double V[5];
-#pragma unroll
-      for (int c = 0; c < 5; ++c) V[c] = U2[c];
+      node_u(F, A, NN, n, V);
       if (o > 0 && o < nn - 1) {
         const double bfm = ffm3, ffm_o = ffm2;
         V[3] += bfm - ffm_o;
@@ -1350,8 +1358,6 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
       for (int c = 0; c < 5; ++c) A.Uout[c * NN + n] = V[c];
     }
     // shift
-#pragma unroll
-    for (int c = 0; c < 5; ++c) { U2[c] = U1[c]; U1[c] = U[c]; }
 #pragma unroll
     for (int c = 0; c < 4; ++c) { ph3[c] = ph2[c]; ph2[c] = ph1[c]; ph1[c] = ph[c]; }
 #pragma unroll
