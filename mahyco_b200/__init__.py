@@ -264,10 +264,16 @@ class Hydro:
         _check(self.lib, self.lib.mhc_get_scalars(self.h, C.byref(t), C.byref(dt), C.byref(it), C.byref(st)), "scalars")
         return {"time": t.value, "deltat": dt.value, "iteration": it.value, "status": st.value}
 
-    def field(self, name: str, env: int = -1) -> np.ndarray:
+    def field(self, name: str, env: int = -1, out: np.ndarray | None = None) -> np.ndarray:
+        """Copy a field to the host: a new array, or `out` (float64,
+        contiguous, at least the field's size; page-locked memory is
+        written by one direct copy)."""
         n = 3 * self.nnode if name in ("Velocity", "NodeCoord") else (
             self.nnode if name == "NodeMass" else self.ncell)
-        out = np.empty(n, dtype=np.float64)
+        if out is None:
+            out = np.empty(n, dtype=np.float64)
+        elif out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"] or out.size < n:
+            raise MahycoError(f"field {name}: out must be a contiguous float64 array of >= {n} values")
         got = self.lib.mhc_get_field(self.h, name.encode(), int(env),
                                      out.ctypes.data_as(C.POINTER(C.c_double)), n)
         _check(self.lib, int(got), f"field {name}")

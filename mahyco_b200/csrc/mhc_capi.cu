@@ -613,6 +613,14 @@ Staging g_stage[64];  // per device
 
 int fetch(cudaStream_t s, const void* dev, void* host, size_t bytes) {
   if (bytes == 0) return MHC_OK;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, host) == cudaSuccess && at.type == cudaMemoryTypeHost) {
+    // a page-locked destination: one copy straight into it
+    CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return MHC_OK;
+  }
+  cudaGetLastError();
   if (bytes <= 64 * 1024) {
     CK(cudaStreamSynchronize(s));
     CK(cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost));
