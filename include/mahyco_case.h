@@ -37,7 +37,12 @@ enum mhc_eos_kind {
 enum mhc_bc_kind {
   MHC_BC_VX = 0, MHC_BC_VY = 1, MHC_BC_VZ = 2,
   /* pressure applied as a node force on the surface (MahycoModule.cc:909-986) */
-  MHC_BC_GEOMETRIC_PRESSURE = 3, MHC_BC_LINEAR_PRESSURE = 4
+  MHC_BC_GEOMETRIC_PRESSURE = 3, MHC_BC_LINEAR_PRESSURE = 4,
+  /* cell variables of the surface's cells (MahycoModule.cc:838-907): the
+   * density (and cell mass, added to the node masses), an added internal
+   * energy (flat or super-Gaussian in y, inside the x / y cutoffs), the
+   * pressure */
+  MHC_BC_DENSITY = 5, MHC_BC_ENERGY = 6, MHC_BC_SUPER_GAUSSIAN_ENERGY = 7, MHC_BC_PRESSURE = 8
 };
 
 /* energy deposits (TypesMahyco.h eEnergyDepot): constant, linear in
@@ -125,7 +130,8 @@ typedef struct mhc_bc {
   int surface;  /* mhc_surface */
   double value;
   double tdebut, tfin;
-  double dependance[4];  /* LinearPressure: dependanceX, Y, Z, T */
+  double dependance[4];  /* LinearPressure: dependanceX, Y, Z, T; SuperGaussianEnergy: dependanceY */
+  double cutoff[2];      /* Energy, SuperGaussianEnergy: cutoffX, cutoffY */
 } mhc_bc;
 
 typedef struct mhc_case_params {

@@ -18,7 +18,8 @@ MAX_BC = 12
 EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN = 0, 1, 2
 EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
                "MieGruneisen": EOS_MIE_GRUNEISEN}
-BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4}
+BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4, "Density": 5,
+              "Energy": 6, "SuperGaussianEnergy": 7, "Pressure": 8}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
 CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL = 1, 2, 3, 4
 CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL}
@@ -56,7 +57,8 @@ class EnvParams(C.Structure):
 
 class BC(C.Structure):
     _fields_ = [("kind", C.c_int), ("surface", C.c_int), ("value", C.c_double),
-                ("tdebut", C.c_double), ("tfin", C.c_double), ("dependance", C.c_double * 4)]
+                ("tdebut", C.c_double), ("tfin", C.c_double), ("dependance", C.c_double * 4),
+                ("cutoff", C.c_double * 2)]
 
 
 class CaseParams(C.Structure):
@@ -142,6 +144,8 @@ def default_params() -> CaseParams:
     p.threshold = 1.0e-10
     p.gravity[:] = (0.0, 0.0, 0.0)
     p.nb_bc = 0
+    for b in p.bc:
+        b.cutoff[:] = (1000.0, 1000.0)
     p.ordre_projection = 2
     p.projection_limiteur_id = MINMOD
     p.is_euler_scheme = 0
@@ -152,12 +156,14 @@ def default_params() -> CaseParams:
 
 
 def add_bc(p: CaseParams, surface: str, kind: str, value: float = 0.0,
-           tdebut: float = 0.0, tfin: float = 1000.0, dependance=(0.0, 0.0, 0.0, 0.0)) -> None:
+           tdebut: float = 0.0, tfin: float = 1000.0, dependance=(0.0, 0.0, 0.0, 0.0),
+           cutoff=(1000.0, 1000.0)) -> None:
     if p.nb_bc >= MAX_BC:
         raise ValueError("too many boundary conditions")
     b = p.bc[p.nb_bc]
     b.kind, b.surface, b.value, b.tdebut, b.tfin = BC_BY_NAME[kind], SURFACES[surface], value, tdebut, tfin
     b.dependance[:] = dependance
+    b.cutoff[:] = cutoff
     p.nb_bc += 1
 
 
@@ -322,7 +328,8 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
             raise NotImplementedError(f"boundary condition {kind}")
         add_bc(p, b.find("surface").text.strip(), kind, _txt(b, "value", 0.0),
                _txt(b, "Tdebut", 0.0), _txt(b, "Tfin", 1000.0),
-               tuple(_txt(b, t, 0.0) for t in ("dependanceX", "dependanceY", "dependanceZ", "dependanceT")))
+               tuple(_txt(b, t, 0.0) for t in ("dependanceX", "dependanceY", "dependanceZ", "dependanceT")),
+               (_txt(b, "cutoffX", 1000.0), _txt(b, "cutoffY", 1000.0)))
     th = root.find("time-history/bilan")
     if th is not None:
         p.time_history_period = _txt(th, "periode", 10, int)

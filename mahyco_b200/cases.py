@@ -390,11 +390,33 @@ PARITY_CASES = {
                                                  deltat_init=1e-3), EULER_Y), 60),
     "adi2d_plaque_euler_y_depot_constant": (lambda: plaque(depot=DEPOT_CONSTANT), 80),
     "adi2d_plaque_euler_y_depot_gaussian": (lambda: plaque(), 80),
+    # cell-variable boundary conditions (MahycoModule.cc:838-907): Density
+    # (cell mass and node masses), Energy with cutoffs, Pressure in a time
+    # window, SuperGaussianEnergy
+    "lag2d_sod_cell_bcs_explicit": (lambda: _cell_bcs(sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=False, remap=False,
+                                                          deltat_max=1e-3, deltat_init=1e-4), explicit=1), 100),
+    "lag3d_bisod_cell_bcs_gp": (lambda: _cell_bcs(sod(dim=3, n=(30, 4, 4), L=(1.0, 0.1, 0.1), bi=True, remap=False,
+                                                      deltat_max=1e-3, deltat_init=1e-4)), 80),
+    "adi2d_bisod_cell_bcs": (lambda: _cell_bcs(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True,
+                                                   deltat_init=1e-3)), 60),
+    "adi2d_bisod_cell_bcs_gaussian": (lambda: _cell_bcs(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True,
+                                                            deltat_init=1e-3), explicit=1, gaussian=True), 60),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
 # calls exp and pow, which CUDA and the oracle's libm round differently
-PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13}
+PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13}
+
+
+def _cell_bcs(p: CaseParams, explicit: int = 0, gaussian: bool = False) -> CaseParams:
+    """Density on XMIN, an energy source on XMAX inside a y cutoff, the
+    pressure on YMAX during a time window."""
+    p.pression_explicite = explicit
+    add_bc(p, "XMIN", "Density", 1.3)
+    add_bc(p, "XMAX", "SuperGaussianEnergy" if gaussian else "Energy", 0.02, dependance=(0.0, 12.0, 0.0, 0.0),
+           cutoff=(1000.0, 0.06))
+    add_bc(p, "YMAX", "Pressure", 0.4, 2e-3, 0.02)
+    return p
 
 
 def _euler(p: CaseParams, scheme: int) -> CaseParams:

@@ -35,6 +35,11 @@ namespace {
 
 bool case_elasto(const mhc_case* h) { return h->P.env[0].elasto_model != 0; }
 bool case_hourglass(const mhc_case* h) { return !h->P.with_projection && h->P.coef_antiderive != 0.; }
+bool case_cell_bcs(const mhc_case* h) {
+  for (int b = 0; b < h->P.nb_bc; ++b)
+    if (h->P.bc[b].kind >= MHC_BC_DENSITY && h->P.bc[b].kind <= MHC_BC_PRESSURE) return true;
+  return false;
+}
 
 // -- list building -----------------------------------------------------------
 int engine_rebuild(Engine* e) {
@@ -61,7 +66,7 @@ int engine_rebuild(Engine* e) {
   }
   if (nc) CK(cudaMemcpyAsync(e->d_desc, desc.data(), nc * sizeof(CaseDesc), cudaMemcpyHostToDevice, e->stream));
   // groups
-  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
@@ -72,12 +77,13 @@ int engine_rebuild(Engine* e) {
     const int el = case_elasto(h) ? 1 : 0, hg = case_hourglass(h) ? 1 : 0;
     const int lim = node_sweep_mode(h->P), clim = cell_sweep_mode(h->P);
     const int cols = cols_mask(h), ncols = node_cols_mask(h);
-    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols);
+    const int cbc = case_cell_bcs(h) ? 1 : 0;
+    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols, cbc);
     auto it = gidx.find(key);
     if (it == gidx.end()) {
       Group g;
       g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
-      g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim; g.COLS = cols; g.NCOLS = ncols;
+      g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim; g.COLS = cols; g.NCOLS = ncols; g.CBC = cbc;
       gidx[key] = (int)e->groups.size();
       e->groups.push_back(g);
       it = gidx.find(key);
@@ -166,6 +172,16 @@ void launch_lagrange_nodes(Engine* e) {
   for (Group& g : e->groups) {
     if (g.DIM == 2) lag_nodes_dispatch<2>(e, g);
     else lag_nodes_dispatch<3>(e, g);
+    if (g.CBC) {
+      // cell variables of the boundary conditions, after the node pass
+      if (g.DIM == 2) {
+        plaunch(e, kb_node_bcs<2>, CT, 0, g.lag_nodes);
+        plaunch(e, kb_cell_bcs<2>, CT, 0, g.lag_cells);
+      } else {
+        plaunch(e, kb_node_bcs<3>, CT, 0, g.lag_nodes);
+        plaunch(e, kb_cell_bcs<3>, CT, 0, g.lag_cells);
+      }
+    }
   }
 }
 
@@ -389,7 +405,7 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
   int ne = p->nb_env, nv = 3 * ne + 1;
   long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8) +
-                    (p->projection_pente_borne ? nv : 0);
+                    (p->projection_pente_borne ? nv : 0) + 2;  // (+2: boundary-condition energy, pressure)
   long long nodes = 4 + 6 + 10;
   return cells * ncell + nodes * nnode;
 }
@@ -401,12 +417,22 @@ int validate(const mhc_case_params* p) {
   if ((long long)(p->nx + 1) * (p->ny + 1) * (p->dim == 3 ? p->nz + 1 : 1) > INT_MAX)
     return set_err(MHC_ERR_ARG, "a case holds at most 2^31 - 1 nodes");
   if (p->nb_bc < 0 || p->nb_bc > MHC_MAX_BC) return set_err(MHC_ERR_ARG, "nb_bc");
+  bool surfaces = false, cellvars = false;
   for (int b = 0; b < p->nb_bc; ++b) {
     const int kind = p->bc[b].kind;
-    if (kind < MHC_BC_VX || kind > MHC_BC_LINEAR_PRESSURE) return set_err(MHC_ERR_UNSUPPORTED, "boundary condition kind");
-    if (kind >= MHC_BC_GEOMETRIC_PRESSURE && p->with_projection)
+    if (kind < MHC_BC_VX || kind > MHC_BC_PRESSURE) return set_err(MHC_ERR_UNSUPPORTED, "boundary condition kind");
+    if ((kind == MHC_BC_GEOMETRIC_PRESSURE || kind == MHC_BC_LINEAR_PRESSURE) && p->with_projection)
       return set_err(MHC_ERR_UNSUPPORTED, "pressure boundary conditions need a Lagrangian loop");
+    surfaces = surfaces || kind == MHC_BC_GEOMETRIC_PRESSURE || kind == MHC_BC_LINEAR_PRESSURE;
+    cellvars = cellvars || kind >= MHC_BC_DENSITY;
   }
+  // the reference interleaves both kinds condition by condition on shared node masses
+  if (surfaces && cellvars)
+    return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions together with pressure surfaces");
+  if (cellvars && p->with_projection && p->is_euler_scheme != MHC_EULER_FULL)
+    return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with a per-axis Euler remap");
+  if (cellvars && p->with_newton)
+    return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with the Newton energy update");
   if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_ONECELL) return set_err(MHC_ERR_ARG, "cas-model");
   if (p->ordre_projection < 1 || p->ordre_projection > 3)
     return set_err(MHC_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
@@ -538,6 +564,10 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   if (h->P.env[0].elasto_model) F.S = (double*)alloc(6 * N * sizeof(double));
   F.cqs = (double*)alloc((h->DIM == 3 ? 24 : 8) * N * sizeof(double));
   if (h->P.projection_pente_borne) F.phi_pb = (double*)alloc(h->NV * N * sizeof(double));
+  if (case_cell_bcs(h)) {
+    F.ebc = (double*)alloc(N * sizeof(double));
+    F.pbc = (double*)alloc(N * sizeof(double));
+  }
   h->d_scal = (Scalars*)alloc(sizeof(Scalars));
   h->d_params = (mhc_case_params*)alloc(sizeof(mhc_case_params));
   F.s = h->d_scal;

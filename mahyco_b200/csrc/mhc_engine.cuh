@@ -69,6 +69,7 @@ struct DevList {
 struct Group {
   int DIM, NE, EULER, skip;
   int EL = 0, HG = 0;          // elasto-plastic model; anti-hourglass correction
+  int CBC = 0;                 // cell-variable boundary conditions (Density, Energy, Pressure)
   int LIM = 0;                 // node-sweep instance: limiter 0-2, LIM_ORDER1 or LIM_GEN
   int CLIM = 0;                // cell-sweep instance: the same, LIM_O3 (third order) or LIM_PB (pente-borne)
   int COLS = 0;                // bit D: the classical cell sweep along D uses one thread per line chunk

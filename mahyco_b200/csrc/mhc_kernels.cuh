@@ -51,6 +51,9 @@ struct Fields {
   double* Ud[2];
   double* S;               // elasto: stress deviator [6][ncell] (xx yy zz xy yz zx)
   double* cqs;             // corner normals of the last Lagrangian mesh [NBN][3][ncell]
+  double *ebc, *pbc;       // cell-variable boundary conditions only: the cells' current internal
+                           // energy and pressure once the conditions applied (the values at n stay
+                           // in e, p)
   double* phi_pb;          // pente-borne only: projected values (phi) of the next remap's first sweep
                            // [3 nb_env + 1][ncell]; entries of absent environments keep the
                            // values of the last sweep before
@@ -1079,6 +1082,10 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   // explicit and Newton updates start from (the GP update restarts from e_n)
   double ecur[NE];
   for (int q = 0; q < NE; ++q) ecur[q] = ene[q];
+  if (F.ebc && pure) {
+    // a boundary condition changed the (pure) cell's current energy
+    for (int q = 0; q < NE; ++q) ecur[q] = F.ebc[c];
+  }
   if (EL) {
     double w1, w2;
     elasto_cell<DIM>(P.env[0], M, F, c, i, j, k, cqn, cqs, V, F.V[c], me[0], dt, w1, w2);
@@ -1158,7 +1165,9 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       if (!P.pseudo_centree && (qq * (1.0 / r - 1.0 / rn) < 0.)) pseudo = qq;
       double g = P.env[q].adiabatic_cst;
       double den = 1 + 0.5 * (g - 1.0) * r * (1.0 / r - 1.0 / rn);
-      double num = ene[q] - (0.5 * pne[q] + pseudo) * (1.0 / r - 1.0 / rn);
+      // the current pressure: the value at n unless a boundary condition set it
+      const double pcur = (F.pbc && pure) ? F.pbc[c] : pne[q];
+      double num = ene[q] - (0.5 * pcur + pseudo) * (1.0 / r - 1.0 / rn);
       ee_[q] = num / den;
     }
   }
@@ -1431,6 +1440,125 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
       F.ec[q * N + c] = ce[q]; F.eq[q * N + c] = qe[q];
     }
   }
+}
+
+// Cell variables of the boundary conditions (applyBoundaryConditionForCellVariables,
+// MahycoModule.cc:838-907), after the node pass and before the position
+// update has any effect on the cell pass: the conditions in order, each on
+// the cell of every face of its surface.  Global cell values (a pure cell's
+// environment value is the same).  Density and Pressure take the value
+// inside [Tdebut, Tfin), 0 outside; the energies always add theirs inside
+// the x / y cutoffs of the cell centre (the centre of the positions the
+// cycle started from), SuperGaussianEnergy times exp(-(y dY)^4).
+__device__ __forceinline__ bool cell_on_surface(const Mesh& M, int i, int j, int k, int surf) {
+  switch (surf) {
+    case MHC_XMIN: return i == 0;
+    case MHC_XMAX: return i == M.ncx - 1;
+    case MHC_YMIN: return j == 0;
+    case MHC_YMAX: return j == M.ncy - 1;
+    case MHC_ZMIN: return M.dim == 3 && k == 0;
+    default: return M.dim == 3 && k == M.ncz - 1;
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ void body_cell_bcs(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long c = bx * (long long)CT + threadIdx.x;
+  if (c >= M.ncell) return;
+  int i, j, k;
+  cell_ijk(M, c, i, j, k);
+  const double t = F.s->t;
+  bool centre = false;
+  R3 cc = {0., 0., 0.};
+  double ec = F.e[c], pc = F.p[c];
+  for (int b = 0; b < P.nb_bc; ++b) {
+    const mhc_bc& bc = P.bc[b];
+    if (bc.kind < MHC_BC_DENSITY || bc.kind > MHC_BC_PRESSURE) continue;
+    if (!cell_on_surface(M, i, j, k, bc.surface)) continue;
+    double value = bc.value;
+    if (t < bc.tdebut) value = 0.;
+    if (t >= bc.tfin) value = 0.;
+    if (bc.kind == MHC_BC_DENSITY) {
+      // the density itself is recomputed from this mass by updateDensity
+      F.m[c] = value * F.V[c];
+    } else if (bc.kind == MHC_BC_PRESSURE) {
+      pc = value;
+    } else {
+      if (!centre) {
+        R3 sum = {0., 0., 0.};
+        for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+          int a, bb, d;
+          local_node_offset(l, a, bb, d);
+          const long long nn = node_id(M, i + a, j + bb, DIM == 3 ? k + d : 0);
+          sum = sum + R3{F.Xp[0][nn], F.Xp[1][nn], DIM == 3 ? F.Xp[2][nn] : 0.};
+        }
+        cc = (DIM == 2 ? .25 : .125) * sum;
+        centre = true;
+      }
+      value = bc.value;
+      if (bc.kind == MHC_BC_SUPER_GAUSSIAN_ENERGY) {
+        // CUDA's exp and pow, within a few ulps of the reference's libm
+        const double ay = cc.y * bc.dependance[1];
+        value *= exp(-pow(ay, 4.));
+      }
+      if (fabs(cc.x) > bc.cutoff[0]) value = 0.;
+      if (fabs(cc.y) > bc.cutoff[1]) value = 0.;
+      ec = ec + value;
+    }
+  }
+  F.ebc[c] = ec;
+  F.pbc[c] = pc;
+}
+
+// ... and the Density conditions' cell masses added to the node masses: each
+// node gathers, condition by condition, the cells of its surface faces in
+// face order (the reference adds value * V / nb_nodes to every node of each
+// such cell as it walks the faces)
+template <int DIM>
+__device__ __forceinline__ void body_node_bcs(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long n = bx * (long long)CT + threadIdx.x;
+  if (n >= M.nnode) return;
+  int i, j, k;
+  node_ijk(M, n, i, j, k);
+  const double t = F.s->t;
+  const double w8 = DIM == 2 ? .25 : .125;
+  double mn = F.mn[n];
+  bool touched = false;
+  for (int b = 0; b < P.nb_bc; ++b) {
+    const mhc_bc& bc = P.bc[b];
+    if (bc.kind != MHC_BC_DENSITY) continue;
+    const int s = bc.surface;
+    const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
+    if (d >= DIM) continue;
+    const bool maxside = s >= MHC_XMAX;
+    const int nid = d == 0 ? i : (d == 1 ? j : k);
+    const int nnd = d == 0 ? M.nnx : (d == 1 ? M.nny : M.nnz);
+    // the two node layers of the surface's cells (every node of those cells)
+    if (maxside ? nid < nnd - 2 : nid > 1) continue;
+    double value = bc.value;
+    if (t < bc.tdebut) value = 0.;
+    if (t >= bc.tfin) value = 0.;
+    // the surface's faces around the node, in face id order (the slower
+    // transverse axis outermost), and the cell of each
+    const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+    const int idx[3] = {i, j, k};
+    const int nc[3] = {M.ncx, M.ncy, M.ncz};
+    for (int o2 = (DIM == 3 ? -1 : 0); o2 <= 0; ++o2) {
+      for (int o1 = -1; o1 <= 0; ++o1) {
+        const int t1 = idx[a1] + o1, t2 = DIM == 3 ? idx[a2] + o2 : 0;
+        if (t1 < 0 || t1 >= nc[a1]) continue;
+        if (DIM == 3 && (t2 < 0 || t2 >= nc[a2])) continue;
+        int ci[3];
+        ci[d] = maxside ? nc[d] - 1 : 0;
+        ci[a1] = t1;
+        ci[a2] = DIM == 3 ? t2 : 0;
+        const long long cf = cell_id(M, ci[0], ci[1], DIM == 3 ? ci[2] : 0);
+        mn = mn + w8 * (value * F.V[cf]);
+        touched = true;
+      }
+    }
+  }
+  if (touched) F.mn[n] = mn;
 }
 
 // per-axis Euler remap (is-euler-scheme X / Y / Z), after the sweeps:

@@ -314,6 +314,28 @@ __global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __
 }
 
 template <int DIM>
+__global__ void __launch_bounds__(CT) kb_cell_bcs(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    body_cell_bcs<DIM>(C[wi.c].M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_node_bcs(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    body_node_bcs<DIM>(C[wi.c].M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+template <int DIM>
 __global__ void __launch_bounds__(CT) kb_euler_volume(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_CELLS>(C, L, w_);

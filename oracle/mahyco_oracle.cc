@@ -867,18 +867,22 @@ static void apply_boundary_condition(Case& C) {
   apply_pressure_bcs(C);
 }
 
-/* pressure surfaces of applyBoundaryConditionForCellVariables
- * (MahycoModule.cc:909-986): for every face of the surface in face order and
+/* applyBoundaryConditionForCellVariables (MahycoModule.cc:811-1037), its
+ * conditions in order.  Cell variables (Density, Energy,
+ * SuperGaussianEnergy, Pressure) of the cell of every face of the surface;
+ * pressure surfaces (MahycoModule.cc:909-986): for every face of the surface in face order and
  * every node of the face, v -= dt_mid / nb_face_nodes * n * p * S / m_node,
  * with n the unit vector from the cell centre to the (initial) face centre,
  * S the length of the face edge from that node (2D) or the z-projected face
  * area (3D), p the BC value (plus its linear terms) inside [Tdebut, Tfin) */
 static void apply_pressure_bcs(Case& C) {
   const double w = C.dim == 2 ? .5 : .25;
+  const double w8 = C.dim == 2 ? .25 : .125;
   const double dt = 0.5 * (C.old_dt + C.dt);
   for (int b = 0; b < C.P.nb_bc; ++b) {
     const mhc_bc& bc = C.P.bc[b];
-    if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE) continue;
+    const bool cellvar = bc.kind >= MHC_BC_DENSITY && bc.kind <= MHC_BC_PRESSURE;
+    if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE && !cellvar) continue;
     const int s = bc.surface;
     const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
     if (d >= C.dim) continue;
@@ -891,6 +895,34 @@ static void apply_pressure_bcs(Case& C) {
       /* the one cell of the boundary face */
       const long c = maxside ? (d == 0 ? C.cid(i - 1, j, k) : (d == 1 ? C.cid(i, j - 1, k) : C.cid(i, j, k - 1)))
                              : C.cid(i, j, k);
+      if (cellvar) {
+        /* MahycoModule.cc:838-907, global cell values (a pure cell's
+         * environment value is the same): value 0 outside [Tdebut, Tfin)
+         * except for the energies, which re-read it and apply the x / y
+         * cutoffs to the cell centre */
+        double value = bc.value;
+        if (C.t < bc.tdebut) value = 0.;
+        if (C.t >= bc.tfin) value = 0.;
+        const R3 cc = C.cell_coord[c];
+        if (bc.kind == MHC_BC_DENSITY) {
+          C.density.g[c] = value;
+          C.cell_mass.g[c] = C.density.g[c] * C.cell_volume.g[c];
+          const double contrib = w8 * C.cell_mass.g[c];
+          for (int l = 0; l < C.nbn; ++l) C.node_mass[C.cnode(c, l)] += contrib;
+        } else if (bc.kind == MHC_BC_ENERGY || bc.kind == MHC_BC_SUPER_GAUSSIAN_ENERGY) {
+          value = bc.value;
+          if (bc.kind == MHC_BC_SUPER_GAUSSIAN_ENERGY) {
+            const double ay = cc.y * bc.dependance[1];
+            value *= std::exp(-std::pow(ay, 4.));
+          }
+          if (std::fabs(cc.x) > bc.cutoff[0]) value = 0.;
+          if (std::fabs(cc.y) > bc.cutoff[1]) value = 0.;
+          C.internal_energy.g[c] += value;
+        } else {
+          C.pressure.g[c] = value;
+        }
+        continue;
+      }
       long n[4] = {0, 0, 0, 0};
       const int nb = C.face_nodes(d, i, j, k, n);
       for (int q = 0; q < nb; ++q) {

@@ -174,3 +174,22 @@ def test_pressure_surfaces_and_onecell(tmp_path):
              for i in range(p.nb_bc)]
     assert (4, 3, 1.0, 0.0, 1e-7, [0.0, 0.0, 0.0, 3e17]) in kinds
     assert (3, 0, 30e9, 1e-7, 1000.0, [0.0, 0.0, 0.0, 0.0]) in kinds
+
+
+def test_cell_variable_boundary_conditions(tmp_path):
+    """Density / Energy / SuperGaussianEnergy / Pressure conditions
+    (Mahyco.axl:490-535) with their cutoffs (default 1000)."""
+    bcs = ("<boundary-condition><surface>XMIN</surface><type>Density</type><value>2.</value></boundary-condition>"
+           "<boundary-condition><surface>YMAX</surface><type>SuperGaussianEnergy</type><value>3.</value>"
+           "<dependanceY>5.</dependanceY><cutoffY>0.25</cutoffY></boundary-condition>"
+           "<boundary-condition><surface>XMAX</surface><type>Pressure</type><value>4.</value>"
+           "<Tdebut>1e-3</Tdebut></boundary-condition>")
+    text = open(ARC).read().replace("<final-time>", bcs + "<final-time>", 1)
+    f = tmp_path / "c.arc"
+    f.write_text(text)
+    p, _ = read_arc(str(f))
+    got = [(p.bc[i].kind, p.bc[i].surface, p.bc[i].value, p.bc[i].tdebut, list(p.bc[i].cutoff))
+           for i in range(p.nb_bc) if p.bc[i].kind >= 5]
+    assert got == [(5, 0, 2.0, 0.0, [1000.0, 1000.0]), (7, 4, 3.0, 0.0, [1000.0, 0.25]),
+                   (8, 3, 4.0, 1e-3, [1000.0, 1000.0])]
+    assert [p.bc[i].dependance[1] for i in range(p.nb_bc) if p.bc[i].kind == 7] == [5.0]

@@ -71,6 +71,15 @@ def test_rejects_options_outside_the_hot_path():
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p.dim, p.is_euler_scheme = 2, 4             # per-axis Euler along z on a 2D mesh
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p = mb.default_params()
+    p.with_projection = 0
+    mb.add_bc(p, "XMIN", "Density", 1.0)
+    mb.add_bc(p, "XMAX", "GeometricPressure", 1.0)  # interleaved with a pressure surface
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p = mb.default_params()
+    p.is_euler_scheme = 3
+    mb.add_bc(p, "XMIN", "Energy", 1.0)         # with a per-axis Euler remap
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
 
 
 @pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", "x") != "" and os.path.exists("/dev/nvidia0"),
