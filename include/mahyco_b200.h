@@ -103,8 +103,10 @@ int mhc_compute_delta_t(mhc_case* h);
  * error flag are skipped on the device. */
 int mhc_cycle(mhc_case* h, int n);
 
-/* same as mhc_cycle, but the n iterations are captured once in a CUDA
- * graph and replayed (launch-bound small cases) */
+/* same as mhc_cycle, but the iterations are captured once in a CUDA graph
+ * (one 6-iteration period, which brings every sweep order back) and
+ * replayed; n = 0 right after HydroStartInit captures the graph without
+ * running an iteration */
 int mhc_cycle_graph(mhc_case* h, int n);
 
 /* kernel groups of one iteration, for mhc_cycle_timed */

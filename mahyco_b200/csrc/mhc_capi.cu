@@ -288,7 +288,8 @@ int engine_cycle_graph(Engine* e, int n) {
     launch_cycle(e);
     --n;
   }
-  if (n >= period && !e->graph) {
+  // n = 0 on an aligned engine only captures (setup outside a timed loop)
+  if ((n >= period || n == 0) && !e->graph && e->cycles_since_build % period == 0) {
     long long saved = e->cycles_since_build;
     std::vector<long long> its;
     for (mhc_case* h : e->cases) its.push_back(h->it_host);
