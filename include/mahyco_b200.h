@@ -257,23 +257,35 @@ int mhc_server_stats(mhc_server* s, long long* queued, long long* running, long 
  * velocity components vx, vy, vz [nnode] (cartesian numbering, x fastest),
  * and writes the new deltat to deltat_out[0] (device memory): cfl * min
  * l/(c + vmax), bounded by 1.05*old_deltat and deltat_max; -2 when below
- * deltat_min, -1 when a cell gives NaN.  Work is enqueued on `stream`
+ * deltat_min.  vmax, the largest speed of a cell's nodes, enters only when
+ * euler_full is non-zero, as computeDeltaT adds it only when the remap's
+ * is-euler-scheme is "Full" (MahycoModule.cc:1771; "Full" is the option's
+ * default, Lagrangian runs included); with euler_full = 0 the velocity
+ * buffers are not read and may be NULL.  deltat-constant runs need no
+ * reduction and are not served here.  Work is enqueued on `stream`
  * (a cudaStream_t, or NULL).
+ *
+ * Bad cells: when any cell gives NaN or a negative l/(c + vmax), the result
+ * is -1 and no deltat is produced.  This differs from mhc_compute_delta_t,
+ * which sets MHC_ST_NAN on the case, leaves that cell out of the minimum and
+ * still produces a deltat from the others.
  *
  * It calls no allocator: the per-block minima live in a fixed array inside
  * the library (MHC_NOALLOC_SCRATCH_BYTES on every GPU that loads it, until
  * the process exits), so meshes above MHC_NOALLOC_MAX_CELLS cells are
  * rejected with MHC_ERR_ARG.  The first call on a device looks the array's
  * address up (cudaGetSymbolAddress); make that first call outside any
- * stream capture.  All calls on a device share the array: calls that
- * overlap on the GPU race and must be serialised by the caller.
+ * stream capture.  The address is kept for the life of the process and
+ * does not survive a cudaDeviceReset of that device.  All calls on a device
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.
  * Errors: mhc_noalloc_last_error(). */
 #define MHC_NOALLOC_MAX_CELLS (1 << 22)
 #define MHC_NOALLOC_SCRATCH_BYTES (MHC_NOALLOC_MAX_CELLS / 256 * 8)
 int mhc_cfl_delta_t_noalloc(int dim, int nx, int ny, int nz, const double* char_length,
                             const double* sound_speed, const double* vx, const double* vy,
-                            const double* vz, double cfl, double old_deltat, double deltat_max,
-                            double deltat_min, double* deltat_out, void* stream);
+                            const double* vz, int euler_full, double cfl, double old_deltat,
+                            double deltat_max, double deltat_min, double* deltat_out, void* stream);
 const char* mhc_noalloc_last_error(void);
 
 #ifdef __cplusplus

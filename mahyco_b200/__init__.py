@@ -78,8 +78,8 @@ _SIGS = {
     "mhc_batch_get_field": (C.c_longlong, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_double),
                                            C.c_longlong]),
     "mhc_cfl_delta_t_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
-                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
-                                          C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "mhc_noalloc_last_error": (C.c_char_p, []),
     "mhc_batch_detach": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_scalars_request": (C.c_int, [C.c_void_p]),

@@ -293,18 +293,24 @@ int engine_cycle_graph(Engine* e, int n) {
     long long saved = e->cycles_since_build;
     std::vector<long long> its;
     for (mhc_case* h : e->cases) its.push_back(h->it_host);
-    cudaGraph_t g;
+    cudaGraph_t g = nullptr;
     const long long before = e->launches;
     CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < period; ++it) launch_cycle(e);
     e->graph_launches = e->launches - before;
+    // the captured iterations did not run: the loop state goes back to
+    // where it was, whether or not the capture succeeded
     e->launches = before;
-    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
-    if (ce != cudaSuccess) return set_err(MHC_ERR_CUDA, cudaGetErrorString(ce));
-    CK(cudaGraphInstantiate(&e->graph, g, 0));
-    cudaGraphDestroy(g);
     e->cycles_since_build = saved;
     for (size_t i = 0; i < e->cases.size(); ++i) e->cases[i]->it_host = its[i];
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      e->graph = nullptr;
+      e->dirty = true;  // rebuild the launch lists before the next cycle
+      return set_err(MHC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    }
   }
   while (n >= period && e->graph) {
     CK(cudaGraphLaunch(e->graph, e->stream));

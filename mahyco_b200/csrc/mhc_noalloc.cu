@@ -30,7 +30,10 @@ static_assert(kMaxBlocks * 8 == MHC_NOALLOC_SCRATCH_BYTES, "scratch size");
 // per-block partial minima of l / (c + vmax); fully rewritten by every call
 __device__ __align__(256) double g_noalloc_scratch[kMaxBlocks];
 
-// host-side device addresses of g_noalloc_scratch, one per device
+// host-side device addresses of g_noalloc_scratch, one per device, looked
+// up once; they do not survive a cudaDeviceReset (the module is loaded
+// again at another address), so a process that resets a device must not
+// call this entry point on it afterwards
 constexpr int kMaxDevices = 64;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 std::mutex g_scratch_mutex;
@@ -39,17 +42,19 @@ thread_local std::string g_noalloc_err;
 using mhc::Mesh;
 
 // block minimum of l / (c + vmax) over the cells of one block
-// (MahycoModule::computeDeltaT, MahycoModule.cc:1766-1790)
+// (MahycoModule::computeDeltaT, MahycoModule.cc:1766-1790); the node speed
+// vmax enters only when the remap's is-euler-scheme is Full
+// (MahycoModule.cc:1771), otherwise it is 0
 __global__ void __launch_bounds__(kThreads)
 k_cfl_partial(Mesh M, const double* l, const double* c, const double* vx, const double* vy,
-              const double* vz, double* partial) {
+              const double* vz, int euler_full, double* partial) {
   long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double dx = 1.7976931348623157e308;
   if (cell < M.ncell) {
     int i, j, k;
     mhc::cell_ijk(M, cell, i, j, k);
     double vmax = 0.;
-    for (int n = 0; n < (M.dim == 3 ? 8 : 4); ++n) {
+    for (int n = 0; euler_full && n < (M.dim == 3 ? 8 : 4); ++n) {
       int a, b, d;
       mhc::local_node_offset(n, a, b, d);
       long long nn = mhc::node_id(M, i + a, j + b, k + d);
@@ -123,13 +128,13 @@ const char* mhc_noalloc_last_error(void) { return g_noalloc_err.c_str(); }
 
 int mhc_cfl_delta_t_noalloc(int dim, int nx, int ny, int nz, const double* char_length,
                             const double* sound_speed, const double* vx, const double* vy,
-                            const double* vz, double cfl, double old_deltat, double deltat_max,
-                            double deltat_min, double* deltat_out, void* stream) {
+                            const double* vz, int euler_full, double cfl, double old_deltat,
+                            double deltat_max, double deltat_min, double* deltat_out, void* stream) {
   if ((dim != 2 && dim != 3) || nx < 1 || ny < 1 || (dim == 3 && nz < 1)) {
     g_noalloc_err = "bad mesh dimensions";
     return MHC_ERR_ARG;
   }
-  if (!char_length || !sound_speed || !vx || !vy || !vz || !deltat_out) {
+  if (!char_length || !sound_speed || !deltat_out || (euler_full && (!vx || !vy || !vz))) {
     g_noalloc_err = "null buffer";
     return MHC_ERR_ARG;
   }
@@ -151,7 +156,8 @@ int mhc_cfl_delta_t_noalloc(int dim, int nx, int ny, int nz, const double* char_
   if (r != MHC_OK) return r;
   const int nblocks = (int)((M.ncell + kThreads - 1) / kThreads);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  k_cfl_partial<<<nblocks, kThreads, 0, s>>>(M, char_length, sound_speed, vx, vy, vz, scratch);
+  k_cfl_partial<<<nblocks, kThreads, 0, s>>>(M, char_length, sound_speed, vx, vy, vz, euler_full ? 1 : 0,
+                                             scratch);
   k_cfl_final<<<1, kThreads, 0, s>>>(scratch, nblocks, cfl, old_deltat, deltat_max, deltat_min, deltat_out);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -1,8 +1,9 @@
 """Extract golden fixtures from the reference's non-regression data.
 
-Run in a checkout that has the reference tree (default: /root/reference):
+Run with the root of a cea-hpc/MaHyCo checkout (the directory holding
+NONREGRESSION/ and src/) as its one required argument:
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 For each case below it parses NONREGRESSION/<case>/Donnees.arc with
 mahyco_b200.case.read_arc and stores the resulting parameters plus the
@@ -79,7 +80,7 @@ ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "Inte
 VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     for case, extra in CASES.items():
         d = os.path.join(ref_root, "NONREGRESSION", case)
         p, info = read_arc(os.path.join(d, "Donnees.arc"))
@@ -111,4 +112,6 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+    main(sys.argv[1])
