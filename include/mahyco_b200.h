@@ -39,6 +39,7 @@ extern "C" {
 #define MHC_ST_STOP 8             /* final time reached: stopComputeLoop (MahycoModule.cc:1851-1857) */
 #define MHC_ST_OOM_ADMISSION 16   /* serving: the case does not fit the HBM budget */
 #define MHC_ST_TIMEOUT 32         /* serving: the request outlived its deadline */
+#define MHC_ST_DAMAGE 64          /* Endommagement: a cell met a damage threshold (damaged cells are not modelled) */
 
 typedef struct mhc_case mhc_case;
 
@@ -67,6 +68,12 @@ void* mhc_case_stream(mhc_case* h);
 long long mhc_case_checkpoint_bytes(mhc_case* h);
 int mhc_case_checkpoint(mhc_case* h, void* host, long long capacity);
 int mhc_case_restore(mhc_case* h, const void* host, long long size);
+
+/* Fills *p with the reference option defaults (src/Mahyco.axl:263-557,
+ * Remap/RemapADI.axl:162-210, the EOS .axl files; a PerfectGas environment,
+ * SOD case model, one environment, a 1x1x1 3D mesh on the unit cube) for a
+ * host that then sets the options of its .arc dataset.  Host only. */
+void mhc_case_params_default(mhc_case_params* p);
 
 /* HBM bytes one case with these parameters needs (serving admission). */
 long long mhc_case_device_bytes(const mhc_case_params* params);
@@ -150,15 +157,81 @@ int mhc_scalars_wait(mhc_case* h, int slot, double* time, double* deltat, long l
  * Returns the number of doubles written, or an error. */
 long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, long long capacity);
 
-/* --- IEquationOfState (IEquationOfState.h:38-65) ------------------------
- * applyEOS(env) on the current density and internal energy of the env
- * cells; mixed cells holding env then get computePressionMoyenne. */
-int mhc_eos_apply(mhc_case* h, int env);
+/* Upload of a named field, the inverse of mhc_get_field, so that a host can
+ * push its own state onto the device (a restart from its own dumps, an
+ * initialisation this library lacks, a hand-off from its CPU code).  Same
+ * names, env semantics and layout as mhc_get_field: env < 0 writes the
+ * global cell value; env >= 0 writes the environment value of the cells
+ * that hold env (the global slot for the cells where env is alone, as the
+ * reference's environment manager stores them) and ignores the others.
+ * EnvMask (bit e = environment e present) is written as given: set it
+ * before the environment values.  CellVolume takes env < 0 only;
+ * NodeCoord is derived geometry (the corner normals of the last Lagrangian
+ * mesh are kept with it) and is read-only.  Only between iterations (after
+ * HydroStartInit, MHC_ERR_ORDER otherwise).  Reads n doubles of host;
+ * returns the number read, or an error.  Replaces the writes a host makes
+ * through Arcane's variables (src/Mahyco.axl:6-241). */
+long long mhc_set_field(mhc_case* h, const char* name, int env, const double* host, long long n);
 
-/* --- IRemap::appliRemap + remapVariables (IRemap.h:44-63) ---------------
- * The remap stage of the current iteration, for a caller that has run the
- * Lagrange entry points. */
+/* --- IEquationOfState (IEquationOfState.h:38-65) ------------------------
+ * One call per method of the service interface, on environment env of the
+ * case (its .axl options are the mhc_env_params of that environment).
+ * mhc_eos_apply: applyEOS(env) on the current density and internal energy
+ * of the env cells; mixed cells holding env then get computePressionMoyenne. */
+int mhc_eos_apply(mhc_case* h, int env);
+/* initEOS(env): internal energy and sound speed of the env cells from their
+ * pressure and density (PerfectGasEOSService.cc:12-35,
+ * StiffenedGasEOSService.cc:14-33, MieGruneisenEOSService.cc:12-34) */
+int mhc_eos_init(mhc_case* h, int env);
+/* ReinitEOS(env): the three services restore nothing on a restart (their
+ * ReinitEOS bodies are empty); checks its arguments and returns */
+int mhc_eos_reinit(mhc_case* h, int env);
+/* applyOneCellEOS(env, EnvCell): pressure and sound speed of one cell of
+ * env written in place, dp/de returned in *dpde (may be NULL); the cell
+ * must hold env.  Synchronous (reads dp/de back). */
+int mhc_eos_apply_one_cell(mhc_case* h, int env, long long cell, double* dpde);
+/* Endommagement(env): the damage test of the services on every env cell
+ * (pressure below tension-damage-thresold, or density / initial density
+ * below density-damage-thresold).  The library accepts only the default
+ * thresholds, under which no cell of positive density and pressure above
+ * the threshold is damaged, and does not model damaged cells: a cell that
+ * meets the test sets MHC_ST_DAMAGE on the case (which then stops). */
+int mhc_eos_endommagement(mhc_case* h, int env);
+/* getAdiabaticCst(env), getdensityDamageThresold(env) */
+int mhc_eos_get_adiabatic_cst(mhc_case* h, int env, double* out);
+int mhc_eos_get_density_damage_thresold(mhc_case* h, int env, double* out);
+
+/* --- IRemap (IRemap.h:44-63) ---------------------------------------------
+ * mhc_remap_apply: the remap stage of the current iteration
+ * (appliRemap, which ends with remapVariables), for a caller that has run
+ * the Lagrange entry points. */
 int mhc_remap_apply(mhc_case* h);
+/* appliRemap(dimension, withDualProjection, nb_vars_to_project, nb_env)
+ * with the reference's arguments, checked against the case: dimension and
+ * nb_env those of the case, withDualProjection 1 (the only form the
+ * reference's module uses), nb_vars_to_project 18 nb_env
+ * (MahycoAnnexe.cc:65) or 3 nb_env + 5 after a restart (MahycoModule.cc:288).
+ * The library projects its own packed set (3 nb_env + 1 cell and 5 node
+ * quantities), whatever the count. */
+int mhc_remap_appli_remap(mhc_case* h, int dimension, int with_dual_projection, int nb_vars_to_project, int nb_env);
+/* the two halves of appliRemap: the direction sweeps
+ * (RemapADIService.cc:23-56), then the Euler reset and remapVariables
+ * (RemapADIService.cc:58-87, RemapADIFinal.cc:21-346); same arguments */
+int mhc_remap_sweeps(mhc_case* h);
+int mhc_remap_variables(mhc_case* h, int dimension, int with_dual_projection, int nb_vars_to_project, int nb_env);
+/* resizeRemapVariables(nb_vars_to_project, nb_env): the remap arrays are
+ * sized when the case is created; checks the counts as appliRemap does */
+int mhc_remap_resize_remap_variables(mhc_case* h, int nb_vars_to_project, int nb_env);
+/* synchronizeUremap(): ghost-layer exchange between sub-domains; one case
+ * lives on one device here, so there is nothing to exchange */
+int mhc_remap_synchronize_uremap(mhc_case* h);
+/* option getters: the value (>= 0), or an error (< 0) */
+int mhc_remap_get_ordre_projection(mhc_case* h);
+int mhc_remap_has_projection_pente_borne(mhc_case* h);
+int mhc_remap_has_projection_simple_pente(mhc_case* h);
+int mhc_remap_has_conservation_energie_totale(mhc_case* h);
+/* isEuler(): "Full", "X", "Y" or "Z" copied into out (capacity bytes) */
+int mhc_remap_is_euler(mhc_case* h, char* out, int capacity);
 
 /* --- EnvSummation (EnvSummationService.cc:77-169) -----------------------
  * out[0] = time, then per environment: CellMass (plain average), Pressure

@@ -14,7 +14,7 @@
  * The struct is shared by the CUDA library (include/mahyco_b200.h) and by the
  * CPU oracle used by the tests; it contains no pointers, so it can be filled
  * from C, C++, Fortran or Python (ctypes) alike.  mhc_case_params_default()
- * writes the reference defaults.
+ * (include/mahyco_b200.h) writes the reference defaults.
  */
 #ifndef MAHYCO_CASE_H
 #define MAHYCO_CASE_H

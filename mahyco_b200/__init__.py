@@ -24,7 +24,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmahyco_b200.so")
 
 ST_NEG_VOLUME, ST_DT_UNDERFLOW, ST_NAN, ST_STOP = 1, 2, 4, 8
-ST_OOM_ADMISSION, ST_TIMEOUT = 16, 32
+ST_OOM_ADMISSION, ST_TIMEOUT, ST_DAMAGE = 16, 32, 64
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 _lib = None
@@ -108,6 +108,25 @@ _SIGS = {
     "mhc_server_release": (C.c_int, [C.c_void_p, C.c_longlong]),
     "mhc_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                    C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    # field upload and the per-method service surface (IEquationOfState, IRemap)
+    "mhc_case_params_default": (None, [C.POINTER(CaseParams)]),
+    "mhc_set_field": (C.c_longlong, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_longlong]),
+    "mhc_eos_init": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_eos_reinit": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_eos_apply_one_cell": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.POINTER(C.c_double)]),
+    "mhc_eos_endommagement": (C.c_int, [C.c_void_p, C.c_int]),
+    "mhc_eos_get_adiabatic_cst": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    "mhc_eos_get_density_damage_thresold": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    "mhc_remap_appli_remap": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "mhc_remap_sweeps": (C.c_int, [C.c_void_p]),
+    "mhc_remap_variables": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "mhc_remap_resize_remap_variables": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "mhc_remap_synchronize_uremap": (C.c_int, [C.c_void_p]),
+    "mhc_remap_get_ordre_projection": (C.c_int, [C.c_void_p]),
+    "mhc_remap_has_projection_pente_borne": (C.c_int, [C.c_void_p]),
+    "mhc_remap_has_projection_simple_pente": (C.c_int, [C.c_void_p]),
+    "mhc_remap_has_conservation_energie_totale": (C.c_int, [C.c_void_p]),
+    "mhc_remap_is_euler": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
 }
 
 
@@ -279,8 +298,77 @@ class Hydro:
         _check(self.lib, int(got), f"field {name}")
         return out
 
+    def set_field(self, name: str, values: np.ndarray, env: int = -1) -> None:
+        """Upload a field (mhc_set_field): same names, env semantics and
+        layout as field()."""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        got = self.lib.mhc_set_field(self.h, name.encode(), int(env), a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
+        _check(self.lib, int(got), f"set_field {name}")
+
+    # IEquationOfState (src/eos/IEquationOfState.h:38-65), per environment
     def eos_apply(self, env: int) -> None:
         _check(self.lib, self.lib.mhc_eos_apply(self.h, int(env)), "applyEOS")
+
+    def initEOS(self, env: int) -> None:
+        _check(self.lib, self.lib.mhc_eos_init(self.h, int(env)), "initEOS")
+
+    def ReinitEOS(self, env: int) -> None:
+        _check(self.lib, self.lib.mhc_eos_reinit(self.h, int(env)), "ReinitEOS")
+
+    def applyOneCellEOS(self, env: int, cell: int) -> float:
+        """Pressure and sound speed of one cell of env in place; returns dp/de."""
+        d = C.c_double()
+        _check(self.lib, self.lib.mhc_eos_apply_one_cell(self.h, int(env), int(cell), C.byref(d)), "applyOneCellEOS")
+        return d.value
+
+    def Endommagement(self, env: int) -> None:
+        _check(self.lib, self.lib.mhc_eos_endommagement(self.h, int(env)), "Endommagement")
+
+    def getAdiabaticCst(self, env: int) -> float:
+        d = C.c_double()
+        _check(self.lib, self.lib.mhc_eos_get_adiabatic_cst(self.h, int(env), C.byref(d)), "getAdiabaticCst")
+        return d.value
+
+    def getdensityDamageThresold(self, env: int) -> float:
+        d = C.c_double()
+        _check(self.lib, self.lib.mhc_eos_get_density_damage_thresold(self.h, int(env), C.byref(d)),
+               "getdensityDamageThresold")
+        return d.value
+
+    # IRemap (src/Remap/IRemap.h:44-63)
+    def appliRemap(self, dimension: int, with_dual: int, nb_vars: int, nb_env: int) -> None:
+        _check(self.lib, self.lib.mhc_remap_appli_remap(self.h, dimension, with_dual, nb_vars, nb_env), "appliRemap")
+
+    def remapSweeps(self) -> None:
+        _check(self.lib, self.lib.mhc_remap_sweeps(self.h), "remap sweeps")
+
+    def remapVariables(self, dimension: int, with_dual: int, nb_vars: int, nb_env: int) -> None:
+        _check(self.lib, self.lib.mhc_remap_variables(self.h, dimension, with_dual, nb_vars, nb_env),
+               "remapVariables")
+
+    def resizeRemapVariables(self, nb_vars: int, nb_env: int) -> None:
+        _check(self.lib, self.lib.mhc_remap_resize_remap_variables(self.h, nb_vars, nb_env), "resizeRemapVariables")
+
+    def synchronizeUremap(self) -> None:
+        _check(self.lib, self.lib.mhc_remap_synchronize_uremap(self.h), "synchronizeUremap")
+
+    def getOrdreProjection(self) -> int:
+        return _check(self.lib, self.lib.mhc_remap_get_ordre_projection(self.h), "getOrdreProjection")
+
+    def hasProjectionPenteBorne(self) -> bool:
+        return bool(_check(self.lib, self.lib.mhc_remap_has_projection_pente_borne(self.h), "hasProjectionPenteBorne"))
+
+    def hasProjectionSimplePente(self) -> bool:
+        return bool(_check(self.lib, self.lib.mhc_remap_has_projection_simple_pente(self.h), "hasProjectionSimplePente"))
+
+    def hasConservationEnergieTotale(self) -> bool:
+        return bool(_check(self.lib, self.lib.mhc_remap_has_conservation_energie_totale(self.h),
+                           "hasConservationEnergieTotale"))
+
+    def isEuler(self) -> str:
+        buf = C.create_string_buffer(8)
+        _check(self.lib, self.lib.mhc_remap_is_euler(self.h, buf, 8), "isEuler")
+        return buf.value.decode()
 
     def time_history(self) -> np.ndarray:
         out = np.empty(1 + 5 * self.params.nb_env, dtype=np.float64)

@@ -327,6 +327,11 @@ PARITY_CASES = {
     "lag2d_bar_impact_rot2": (lambda: _rot2(bar_impact(n=(10, 30), L=(0.01, 0.03), velocity=400.0)), 80),
     "lag3d_bar_impact": (lambda: _bar3d(), 40),
     "lag2d_bar_no_elasto": (lambda: bar_impact(n=(8, 40), L=(0.01, 0.05), elasto=False, coef_antiderive=0.0), 80),
+    # the measured configurations at their stated sizes: the Lagrangian 2D
+    # Sod tube of 200 x 10 cells (200 cycles) and the elasto-plastic bar
+    # impact of the serving mix, 80 x 400 cells
+    "lag2d_sod_200x10": (lambda: workload("sod2d_lagrange"), 200),
+    "lag2d_bar_impact_80x400": (lambda: bar_impact(), 60),
     "lag2d_sod_newton": (lambda: _newton(sod(dim=2, n=(60, 5), L=(1.0, 0.1), bi=True, remap=False,
                                              deltat_max=1e-3, deltat_init=1e-4)), 120),
     "adi3d_bisod_newton": (lambda: _newton(sod(dim=3, n=(24, 4, 4), L=(1.0, 0.2, 0.2), bi=True,

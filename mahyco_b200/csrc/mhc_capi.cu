@@ -216,8 +216,10 @@ int group_dirs(Engine* e, const Group& g, int* dirs) {
   return n;
 }
 
-// RemapADIService::appliRemap (RemapADIService.cc:15-90) for every group
-void launch_remap(Engine* e) {
+// RemapADIService::appliRemap (RemapADIService.cc:15-90) for every group:
+// the direction sweeps (:23-56), then the Euler reset and remapVariables
+// (:58-87)
+void launch_remap_sweeps(Engine* e) {
   for (int k = 0; k < 3; ++k) {
     for (Group& g : e->groups) {
       if (!g.EULER) continue;
@@ -227,6 +229,12 @@ void launch_remap(Engine* e) {
       sweep_step_any(e, g, dirs[k], k);
     }
   }
+}
+
+// the end of appliRemap: per-axis Euler volumes (computeVolumeEuler) and
+// RemapADIService::remapVariables (RemapADIFinal.cc:21-346), then the
+// per-axis coordinate reset
+void launch_remap_variables(Engine* e) {
   for (Group& g : e->groups) {
     if (!g.EULER) continue;
     int dirs[3];
@@ -247,13 +255,19 @@ void launch_remap(Engine* e) {
   }
 }
 
+void launch_remap(Engine* e) {
+  launch_remap_sweeps(e);
+  launch_remap_variables(e);
+}
+
 void launch_dt(Engine* e) {
   StageTimer tm(e, MHC_STAGE_DELTA_T);
   for (Group& g : e->groups) {
     DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_>, CT, 0, g.dt)));
-    if (g.cases.n > 0)
+    if (g.cases.n > 0) {
       kb_delta_t_finalize<<<cdiv(g.cases.n, 128), 128, 0, e->stream>>>(e->d_desc, e->d_ints + g.cases.off_cases, g.cases.n);
       ++e->launches;
+    }
   }
 }
 
@@ -829,6 +843,12 @@ int case_time_history(mhc_case* h, cudaStream_t st, double* out) {
 }
 
 }  // namespace
+
+int mhc::engine_rebuild_shared(Engine* e) { return engine_rebuild(e); }
+int mhc::solo_engine_shared(mhc_case* h) { return solo_engine(h); }
+void mhc::launch_remap_sweeps_shared(Engine* e) { launch_remap_sweeps(e); }
+void mhc::launch_remap_variables_shared(Engine* e) { launch_remap_variables(e); }
+int mhc::fetch_shared(cudaStream_t s, const void* dev, void* host, size_t bytes) { return fetch(s, dev, host, bytes); }
 
 // ===========================================================================
 // C ABI (linkage from the declarations in mahyco_b200.h)

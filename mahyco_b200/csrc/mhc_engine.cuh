@@ -24,7 +24,8 @@ int set_err(int code, const std::string& msg);
     if (e_ != cudaSuccess) return ::mhc::set_err(MHC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-enum Stage { S_IDLE = 0, S_SAVED, S_VELOCITY, S_BC, S_POSITION, S_GEOM, S_DENSITY, S_VISCO, S_ELASTO, S_ENERGY, S_REMAP };
+enum Stage { S_IDLE = 0, S_SAVED, S_VELOCITY, S_BC, S_POSITION, S_GEOM, S_DENSITY, S_VISCO, S_ELASTO, S_ENERGY, S_REMAP,
+             S_SWEPT /* remap sweeps done, remapVariables pending */ };
 
 inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
 
@@ -248,3 +249,13 @@ inline void plaunch(Engine* e, K kernel, int threads, size_t smem, const DevList
 // one performed sweep (cells, then nodes) of direction D as the k-th of the
 // cycle, for the members of a group (mhc_sweeps.cu)
 void sweep_step_any(Engine* e, Group& g, int D, int k);
+
+// engine operations defined in mhc_capi.cu and shared with the other C ABI
+// translation units (mhc_services.cu)
+namespace mhc {
+int engine_rebuild_shared(Engine* e);
+int solo_engine_shared(mhc_case* h);
+void launch_remap_sweeps_shared(Engine* e);
+void launch_remap_variables_shared(Engine* e);
+int fetch_shared(cudaStream_t s, const void* dev, void* host, size_t bytes);
+}  // namespace mhc

@@ -2287,10 +2287,60 @@ long oracle_get_field(void* h, const char* name, int env, double* out, long cap)
   return -2;
 }
 
+/* the inverse of oracle_get_field for the state a host can upload: env < 0
+ * writes the global cell value, env >= 0 the environment value of the cells
+ * that hold env (EV: the global slot where env is alone); node Real3 fields
+ * interleaved.  Returns the number of values read, < 0 for an unknown or
+ * read-only name. */
+long oracle_set_field(void* h, const char* name, int env, const double* in, long n) {
+  ora::Case& C = *(ora::Case*)h;
+  if (ora::MatField* f = mat_field(C, name)) {
+    if (n < C.ncell) return -1;
+    for (long c = 0; c < C.ncell; ++c) {
+      if (env < 0) f->g[c] = in[c];
+      else if (C.has(c, env)) C.EV(*f, env, c) = in[c];
+    }
+    return C.ncell;
+  }
+  if (!strcmp(name, "NodeMass")) {
+    if (n < C.nnode) return -1;
+    for (long i = 0; i < C.nnode; ++i) C.node_mass[i] = in[i];
+    return C.nnode;
+  }
+  if (!strcmp(name, "Velocity")) {
+    if (n < 3 * C.nnode) return -1;
+    for (long i = 0; i < C.nnode; ++i) C.vel[i] = ora::R3{in[3 * i], in[3 * i + 1], in[3 * i + 2]};
+    return 3 * C.nnode;
+  }
+  return -2;
+}
+
+/* IEquationOfState::applyEOS(env) on the current state, then
+ * computePressionMoyenne on the mixed cells that hold env (the sequence the
+ * library's mhc_eos_apply entry point runs) */
+int oracle_eos_apply(void* h, int env) {
+  ora::Case& C = *(ora::Case*)h;
+  if (env < 0 || env >= C.nenv) return -1;
+  ora::eos_apply(C, env);
+  double option = C.P.calcul_vitson_max ? 1. : 0.;
+  for (long c = 0; c < C.ncell; ++c) {
+    if (C.pure(c) || !C.has(c, env)) continue;
+    C.pressure.g[c] = 0.;
+    C.sound_speed.g[c] = 0.;
+    for (int e = 0; e < C.nenv; ++e) {
+      if (!C.has(c, e)) continue;
+      C.pressure.g[c] += C.EV(C.fracvol, e, c) * C.EV(C.pressure, e, c);
+      C.sound_speed.g[c] = option * std::max(C.EV(C.sound_speed, e, c), C.sound_speed.g[c]);
+      C.sound_speed.g[c] += (1. - option) * C.EV(C.fracvol, e, c) * C.EV(C.sound_speed, e, c);
+    }
+  }
+  return 0;
+}
+
 /* known-answer hooks for the oracle's own unit tests */
 double oracle_flux_limiter(int id, double r) { return ora::flux_limiter(id, r); }
 double oracle_limited_gradient(int id, double gb, double gf) { return ora::limited_gradient(id, gb, gf); }
-void oracle_eos_point(const mhc_env_params* o, double rho, double e, double* p, double* c) {
+void oracle_eos_point(const mhc_env_params* o, double rho, double e, double* p, double* c, double* dpde) {
   mhc_case_params P;
   memset(&P, 0, sizeof(P));
   P.dim = 2; P.nx = 1; P.ny = 1; P.lx = P.ly = 1.; P.nb_env = 1; P.env[0] = *o;
@@ -2301,6 +2351,7 @@ void oracle_eos_point(const mhc_env_params* o, double rho, double e, double* p, 
   ora::eos_apply(C, 0);
   *p = C.pressure.g[0];
   *c = C.sound_speed.g[0];
+  *dpde = C.dpde.g[0];
 }
 
 /* the oracle's correctly rounded x^(1./3.), for its own unit test */

@@ -37,6 +37,9 @@ def lib() -> C.CDLL:
     L.oracle_scalar.argtypes = [C.c_void_p, C.c_char_p]
     L.oracle_get_field.restype = C.c_long
     L.oracle_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_long]
+    L.oracle_eos_apply.argtypes = [C.c_void_p, C.c_int]
+    L.oracle_set_field.restype = C.c_long
+    L.oracle_set_field.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_long]
     L.oracle_th_count.restype = C.c_long
     L.oracle_th_count.argtypes = [C.c_void_p]
     L.oracle_th_line.argtypes = [C.c_void_p, C.c_long, C.POINTER(C.c_double)]
@@ -89,6 +92,14 @@ class Oracle:
         assert got == n, (name, got)
         return out
 
+    def set_field(self, name: str, values: np.ndarray, env: int = -1) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        got = self.L.oracle_set_field(self.h, name.encode(), env, a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
+        assert got > 0, (name, got)
+
+    def eos_apply(self, env: int) -> None:
+        assert self.L.oracle_eos_apply(self.h, env) == 0
+
     def time_history(self) -> np.ndarray:
         n = self.L.oracle_th_count(self.h)
         w = 1 + 5 * self.params.nb_env
@@ -107,12 +118,14 @@ def setup_kat(L):
     L.oracle_limited_gradient.argtypes = [C.c_int, C.c_double, C.c_double]
     from mahyco_b200.case import EnvParams
     L.oracle_eos_point.argtypes = [C.POINTER(EnvParams), C.c_double, C.c_double,
-                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     return L
 
 
-def eos_point(env, rho, e):
+def eos_point(env, rho, e, with_dpde=False):
+    """(p, c) of the oracle's applyEOS at one state; (p, c, dp/de) with
+    with_dpde."""
     L = setup_kat(lib())
-    p, c = C.c_double(), C.c_double()
-    L.oracle_eos_point(C.byref(env), rho, e, C.byref(p), C.byref(c))
-    return p.value, c.value
+    p, c, d = C.c_double(), C.c_double(), C.c_double()
+    L.oracle_eos_point(C.byref(env), rho, e, C.byref(p), C.byref(c), C.byref(d))
+    return (p.value, c.value, d.value) if with_dpde else (p.value, c.value)

@@ -89,3 +89,14 @@ def test_no_gpu_fails_loudly():
     p.nx = p.ny = p.nz = 4
     with pytest.raises(mb.MahycoError):
         mb.Hydro(p)
+
+
+def test_c_defaults_match_the_python_defaults():
+    """mhc_case_params_default (for C / C++ hosts) writes the same reference
+    defaults as mahyco_b200.case.default_params; host only, no GPU."""
+    lib = mb.load()
+    c = mb.CaseParams()
+    ctypes.memset(ctypes.byref(c), 0xAB, ctypes.sizeof(c))
+    lib.mhc_case_params_default(ctypes.byref(c))
+    py = mb.default_params()
+    assert bytes(c) == bytes(py)
