@@ -9,7 +9,14 @@ Two bars, on every case of mahyco_b200.cases.PARITY_CASES:
 * reference libm: against the oracle that calls glibc's std::pow like the
   reference (glibc's pow is not correctly rounded), every field must agree
   to a relative L-infinity |gpu - oracle|_inf / |oracle|_inf <= 1e-12 after
-  min(N, 40) iterations.
+  min(N, 40) iterations.  One exception, for Mie-Gruneisen environments:
+  the services' sound speed is sqrt((p(rho + 1e-7) - p(rho - 1e-7)) / 2e-7)
+  (MieGruneisenEOSService.cc:66-96), a difference of two pressures of
+  ~1e9 that differ by ~10, so the ~1e-16 relative disagreement of glibc's
+  pow(mu, 2), pow(mu, 3) with correctly rounded powers comes out amplified
+  by p / (p2 - p1) ~ 1e8-1e9; the sound speed and the pseudo-viscosity
+  built from it are held to 1e-5 there (LIBM_MG_TOL), every other field to
+  1e-12.
 """
 import numpy as np
 import pytest
@@ -18,6 +25,7 @@ from mahyco_b200.cases import PARITY_CASES, PARITY_EXACT_TOL
 
 TOL = 1e-12
 LIBM_CYCLES = 40
+LIBM_MG_TOL = {"SoundSpeed": 1e-5, "PseudoViscosity": 1e-5}
 CELL_FIELDS = ["Density", "Pressure", "InternalEnergy", "SoundSpeed", "PseudoViscosity",
                "CellMass", "CellVolume", "CaracteristicLength"]
 ENV_FIELDS = ["Density", "Pressure", "InternalEnergy", "FracVol", "CellMass"]
@@ -101,7 +109,11 @@ def test_parity_exact_line_chunk_layout(name, monkeypatch):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(PARITY_CASES))
 def test_parity_reference_libm(name):
+    from mahyco_b200.case import EOS_MIE_GRUNEISEN
     init_errs, errs = run_pair(name, cr_pow=False, ncycles=LIBM_CYCLES)
     assert max(init_errs.values()) <= TOL, init_errs
-    bad = {k: v for k, v in errs.items() if v > TOL}
+    p = PARITY_CASES[name][0]()
+    mg = any(p.env[e].eos == EOS_MIE_GRUNEISEN for e in range(p.nb_env))
+    tol = {k: (LIBM_MG_TOL.get(k.split("[")[0], TOL) if mg else TOL) for k in errs}
+    bad = {k: v for k, v in errs.items() if v > tol[k]}
     assert not bad, (name, bad, errs)
