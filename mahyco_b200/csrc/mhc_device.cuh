@@ -94,17 +94,22 @@ __device__ __forceinline__ long long cell_id(const Mesh& M, int i, int j, int k)
 __device__ __forceinline__ long long node_id(const Mesh& M, int i, int j, int k) {
   return (long long)(unsigned)(i + M.nnx * (j + M.nny * k));
 }
+// (i, j, k) of a linear id, in unsigned 32-bit arithmetic (ids < 2^31):
+// a 64-bit division is a long emulated sequence, a 32-bit one a few
+// instructions
 __device__ __forceinline__ void cell_ijk(const Mesh& M, long long c, int& i, int& j, int& k) {
-  i = (int)(c % M.ncx);
-  long long r = c / M.ncx;
-  j = (int)(r % M.ncy);
-  k = (int)(r / M.ncy);
+  const unsigned u = (unsigned)c, nx = (unsigned)M.ncx, ny = (unsigned)M.ncy;
+  const unsigned r = u / nx;
+  i = (int)(u - r * nx);
+  k = (int)(r / ny);
+  j = (int)(r - (unsigned)k * ny);
 }
 __device__ __forceinline__ void node_ijk(const Mesh& M, long long n, int& i, int& j, int& k) {
-  i = (int)(n % M.nnx);
-  long long r = n / M.nnx;
-  j = (int)(r % M.nny);
-  k = (int)(r / M.nny);
+  const unsigned u = (unsigned)n, nx = (unsigned)M.nnx, ny = (unsigned)M.nny;
+  const unsigned r = u / nx;
+  i = (int)(u - r * nx);
+  k = (int)(r / ny);
+  j = (int)(r - (unsigned)k * ny);
 }
 // initial (Euler) node position: origin + i*(L/n)
 __device__ __forceinline__ R3 node_x0(const Mesh& M, int i, int j, int k) {

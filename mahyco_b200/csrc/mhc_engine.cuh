@@ -74,6 +74,7 @@ struct Group {
   int LIM = 0;                 // node-sweep instance: limiter 0-2, LIM_ORDER1 or LIM_GEN
   int CLIM = 0;                // cell-sweep instance: the same, LIM_O3 (third order) or LIM_PB (pente-borne)
   int COLS = 0;                // bit D: the classical cell sweep along D uses one thread per line chunk
+  int TILE = 0;                // bit D: ... or a shared-memory tile (when not COLS)
   int NCOLS = 0;               // bit D: the same for the node sweep
   long long it0;               // iteration of the members when the lists were built
   std::vector<int> members;
@@ -186,6 +187,26 @@ inline int node_cols_mask(const mhc_case* h) {
     if ((long long)h->M.nnx * nb * col_chunks(nd) >= lim) m |= 1 << D;
   }
   return m;
+}
+
+// Directions whose classical cell sweep goes through a shared-memory tile
+// (body_sweep_cells_tile: coalesced loads and stores, the warp-per-line
+// arithmetic): every y / z sweep that does not take the line-chunk layout.
+// MHC_SWEEP_TILE=0 in the environment keeps the warp-per-line layout.
+inline int tile_mask(const mhc_case* h) {
+  if (cell_sweep_mode(h->P) > LIM_ORDER1) return 0;
+  const char* s = getenv("MHC_SWEEP_TILE");
+  if (s && *s == '0') return 0;
+  int m = 0;
+  for (int D = 1; D < h->DIM; ++D) m |= 1 << D;
+  return m & ~cols_mask(h);
+}
+
+// phase of the cell sweep of a group along D
+inline int group_cell_phase(int CLIM, int COLS, int TILE, int D) {
+  if ((COLS >> D) & 1) return cell_sweep_phase(LIM_COLS + CLIM, D);
+  if ((TILE >> D) & 1) return PH_SWCT0 + D;
+  return cell_sweep_phase(CLIM, D);
 }
 
 // directions the remap does not sweep: one cell thick, or not the axis of a

@@ -34,7 +34,8 @@ enum PhaseKind {
   PH_SWCW0 = 9,      // cell sweep with the wide (third-order) stencil
   PH_SWNW0 = 12,     // node sweep with the wide (generalised limiter) stencil
   PH_SWCC0 = 15,     // cell sweep along D = 1, 2, one thread per line chunk
-  PH_SWNC0 = 18      // node sweep along D = 1, 2, one thread per line chunk
+  PH_SWNC0 = 18,     // node sweep along D = 1, 2, one thread per line chunk
+  PH_SWCT0 = 21      // cell sweep along D = 1, 2 through a shared-memory tile
 };
 
 // phase of the cell sweep along D for a cell-sweep instance
@@ -45,7 +46,11 @@ __host__ __device__ constexpr int node_sweep_phase(int lim, int D) {
   return (D > 0 && lim >= LIM_COLS) ? PH_SWNC0 + D : (lim == LIM_GEN ? PH_SWNW0 : PH_SWN0) + D;
 }
 
-__host__ __device__ inline int cdiv_i(long long a, int b) { return (int)((a + b - 1) / b); }
+// ceil(a / b) for 0 <= a < 2^31 (every count of a case: it has fewer than
+// 2^31 nodes), in unsigned 32-bit arithmetic
+__host__ __device__ inline int cdiv_i(long long a, int b) {
+  return (int)(((unsigned)a + (unsigned)b - 1u) / (unsigned)b);
+}
 
 // virtual-block grid (gx, gy, gz) of one case in a phase; blocks are
 // numbered with x fastest
@@ -53,6 +58,13 @@ __host__ __device__ inline void phase_grid(int ph, const Mesh& M, int& gx, int& 
   gy = gz = 1;
   if (ph == PH_CELLS) { gx = cdiv_i(M.ncell, CT); return; }
   if (ph == PH_NODES) { gx = cdiv_i(M.nnode, CT); return; }
+  if (ph >= PH_SWCT0) {  // body_sweep_cells_tile
+    const int D = ph - PH_SWCT0;
+    const int nb = D == 1 ? M.ncz : M.ncy, nd = D == 1 ? M.ncy : M.ncz;
+    gx = cdiv_i(M.ncx, SWT_COLS);
+    gy = cdiv_i((long long)nb * nd, XOUT);
+    return;
+  }
   if (ph >= PH_SWNC0) {  // body_sweep_nodes_cols
     const int D = ph - PH_SWNC0;
     const int nb = D == 1 ? M.nnz : M.nny, nd = D == 1 ? M.nny : M.nnz;
@@ -101,10 +113,12 @@ __device__ __forceinline__ WorkItem item_at(const CaseDesc* __restrict__ C, cons
     else hi = mid - 1;
   }
   const int c = __ldg(L.cases + lo);
-  const int b = w - __ldg(L.start + lo);
+  const unsigned b = (unsigned)(w - __ldg(L.start + lo));
   int gx, gy, gz;
   phase_grid(PH, C[c].M, gx, gy, gz);
-  return WorkItem{c, b % gx, (b / gx) % gy, b / (gx * gy)};
+  if (gy == 1) return WorkItem{c, (int)b, 0, 0};  // every phase but the sweeps
+  const unsigned r = b / (unsigned)gx, z = r / (unsigned)gy;
+  return WorkItem{c, (int)(b - r * (unsigned)gx), (int)(r - z * (unsigned)gy), (int)z};
 }
 
 #define MHC_FOR_ITEMS(L) for (int w_ = blockIdx.x; w_ < (L).total; w_ += gridDim.x)
@@ -241,6 +255,35 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   }
 }
 
+// cell sweep along D = 1, 2 through a shared-memory tile (classical
+// limiters, first order): SWT_THREADS threads, swt_smem_bytes(NE) of
+// dynamic shared memory
+#ifndef MHC_SWT_MIN_BLOCKS
+#define MHC_SWT_MIN_BLOCKS 3
+#endif
+template <int DIM, int NE, int D, int LIM>
+__global__ void __launch_bounds__(SWT_THREADS, MHC_SWT_MIN_BLOCKS)
+kb_sweep_cells_tile(const CaseDesc* __restrict__ C, PhaseList L, int k) {
+  extern __shared__ double swt_tile[];
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_SWCT0 + D>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;  // uniform over the block (one case per item)
+    resolve_positions(F);
+    const mhc_case_params& P = *C[wi.c].P;
+    SweepArgs A;
+    A.Uin = (k & 1) ? F.U[1] : F.U[0];
+    A.Uout = (k & 1) ? F.U[0] : F.U[1];
+    A.first = k == 0;
+    A.order = P.ordre_projection;
+    A.limiter = P.projection_limiteur_id;
+    A.simple_pente = P.projection_simple_pente;
+    A.first_remap = k == 0 && F.s->iteration == 1;
+    const Mesh M = C[wi.c].M;
+    body_sweep_cells_tile<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y, swt_tile);
+  }
+}
+
 #ifndef MHC_SW_MIN_BLOCKS_NODECOLS
 #define MHC_SW_MIN_BLOCKS_NODECOLS 4
 #endif
@@ -258,7 +301,7 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     // directions swept before step k this cycle (RemapADIService.cc:23-33)
     int done = 0;
     {
-      const int sens = (int)((F.s->iteration - 1) % M.dim);
+      const int sens = (int)((F.s->iteration - 1) % DIM);
       int cnt = 0;
       for (int i = 0; i < M.dim; ++i) {
         const int d = (i + sens) % M.dim;

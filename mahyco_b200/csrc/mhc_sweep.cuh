@@ -207,22 +207,23 @@ template <int D>
 __device__ __forceinline__ bool sweep_lane(int nx, int ny, int nz, int out, int hl, int vbx, int vby, int lane,
                                            int row, int& i, int& j, int& k, int& p, int& ta, int& tb) {
   i = j = k = p = ta = tb = 0;
+  // positions in unsigned 32-bit arithmetic (a case has < 2^31 cells)
   if (D == 0) {
-    const long long g = ((long long)vbx * SW_ROWS + row) * out - hl + lane;
-    if (g < 0 || g >= (long long)nx * ny * nz) return false;
-    i = (int)(g % nx);
-    const long long r = g / nx;
-    j = (int)(r % ny);
-    k = (int)(r / ny);
+    const int g = (vbx * SW_ROWS + row) * out - hl + lane;
+    if (g < 0 || g >= nx * ny * nz) return false;
+    const unsigned r = (unsigned)g / (unsigned)nx;
+    i = (int)((unsigned)g - r * (unsigned)nx);
+    k = (int)(r / (unsigned)ny);
+    j = (int)(r - (unsigned)k * (unsigned)ny);
     p = i; ta = j; tb = k;
     return true;
   }
   const int nd = D == 1 ? ny : nz, nb = D == 1 ? nz : ny;
   ta = vbx * SW_ROWS + row;
-  const long long g = (long long)vby * out - hl + lane;
-  if (ta >= nx || g < 0 || g >= (long long)nb * nd) return false;
-  tb = (int)(g / nd);
-  p = (int)(g % nd);
+  const int g = vby * out - hl + lane;
+  if (ta >= nx || g < 0 || g >= nb * nd) return false;
+  tb = (int)((unsigned)g / (unsigned)nd);
+  p = g - tb * nd;
   i = ta;
   if (D == 1) { j = p; k = tb; }
   else { j = tb; k = p; }
@@ -232,9 +233,9 @@ __device__ __forceinline__ bool sweep_lane(int nx, int ny, int nz, int out, int 
 // the whole warp holds nothing (warp-uniform test, before any shuffle)
 template <int D>
 __device__ __forceinline__ bool sweep_warp_empty(int nx, int ny, int nz, int out, int hl, int vbx, int vby, int row) {
-  if (D == 0) return ((long long)vbx * SW_ROWS + row) * out - hl >= (long long)nx * ny * nz;
+  if (D == 0) return (vbx * SW_ROWS + row) * out - hl >= nx * ny * nz;
   const int nd = D == 1 ? ny : nz, nb = D == 1 ? nz : ny;
-  return vbx * SW_ROWS + row >= nx || (long long)vby * out - hl >= (long long)nb * nd;
+  return vbx * SW_ROWS + row >= nx || vby * out - hl >= nb * nd;
 }
 
 // D coordinates of the face nodes of the node plane whose lowest node is
@@ -931,7 +932,7 @@ __device__ __forceinline__ void body_sweep_cells_cols(const Mesh& M, const Field
   const int nb = D == 1 ? M.ncz : M.ncy;           // slow transverse extent
   const long long col = (long long)vbx * SW_THREADS + threadIdx.x;
   if (col >= (long long)M.ncx * nb) return;
-  const int i = (int)(col % M.ncx), tb = (int)(col / M.ncx);
+  const int tb = (int)((unsigned)col / (unsigned)M.ncx), i = (int)col - tb * M.ncx;
   int o0, o1;
   col_chunk_range(nd, vby, o0, o1);
   if (o0 >= o1) return;
@@ -1031,6 +1032,160 @@ __device__ __forceinline__ void body_sweep_cells_cols(const Mesh& M, const Field
     un1 = cur.un; L1 = cur.L; fc1 = cur.fc;
     if (cell) cur = nxt;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Cell sweep along D = 1, 2 through a shared-memory tile, classical limiters
+// and first order.  A block holds SWT_COLS neighbouring x columns and one
+// window of 32 positions along D (the concatenated lines of the lane layout:
+// 2 halo cells, XOUT written, the rest after them).
+//  1. Load: thread t takes column t % SWT_COLS and position t / SWT_COLS, so
+//     the SWT_COLS threads of one position read consecutive x cells (every
+//     global load and store is a contiguous 64-byte run); each thread
+//     stages its cell's projected quantities, divisor, Lagrangian centre
+//     along D and back-face centre, normal velocity and length.
+//  2. Sweep: warp w takes column w, lane = position along D, and runs the
+//     arithmetic of body_sweep_cells_lanes, in the same order, from the
+//     staged values (neighbours by shuffles); results go back to the tile.
+//  3. Store: the load layout again, written cells only.
+// The staged front-plane coordinates of a cell are loaded, not shuffled, so
+// the cell centre is the same sum of the same node coordinates.
+// ---------------------------------------------------------------------------
+constexpr int SWT_COLS = 8;                     // x columns (warps) per block
+constexpr int SWT_THREADS = SWT_COLS * SW_LANES;
+constexpr int SWT_PITCH = SWT_COLS + 1;         // padded row: two wavefronts per warp access
+constexpr int SWT_FIELD = SW_LANES * SWT_PITCH;  // doubles per staged quantity
+
+// staged quantities: NV projected values, divisor, centre, face centre,
+// normal velocity, face length (outputs reuse the first NV + NE slots)
+__host__ __device__ constexpr int swt_slots(int ne) { return 3 * ne + 1 + 5; }
+__host__ __device__ constexpr int swt_smem_bytes(int ne) { return swt_slots(ne) * SWT_FIELD * 8; }
+
+template <int DIM, int NE, int D, int LIM>
+__device__ __forceinline__ void body_sweep_cells_tile(const Mesh& M, const Fields& F, const SweepArgs& A, int vbx,
+                                                      int vby, double* __restrict__ sm) {
+  static_assert(D >= 1, "x sweeps use the lane layout");
+  constexpr int NV = 3 * NE + 1;
+  constexpr int S_DEN = NV, S_XC = NV + 1, S_FC = NV + 2, S_UN = NV + 3, S_L = NV + 4;
+  constexpr unsigned FULL = 0xffffffffu;
+  const long long N = M.ncell;
+  const int nd = D == 1 ? M.ncy : M.ncz, nb = D == 1 ? M.ncz : M.ncy;
+  const int x0 = vbx * SWT_COLS;
+  const int g0 = vby * XOUT - 2;  // first position of the window (2 halo cells)
+  const double* __restrict__ Uin = A.Uin;
+  // -- 1. load (row layout)
+  {
+    const int col = threadIdx.x % SWT_COLS, pos = threadIdx.x / SWT_COLS;
+    const int i = x0 + col, g = g0 + pos;
+    if (i < M.ncx && g >= 0 && g < nb * nd) {
+      const int tb = (int)((unsigned)g / (unsigned)nd), p = g - tb * nd;
+      const int j = D == 1 ? p : tb, k = D == 1 ? tb : p;
+      Plane<DIM> back, front;
+      load_plane<DIM, D>(M, F, i, j, k, back);
+      load_plane_xd<DIM, D>(M, F, i, D == 1 ? j + 1 : j, D == 2 ? k + 1 : k, front);
+      const long long c = cell_id(M, i, j, k);
+      double* s = sm + pos * SWT_PITCH + col;
+      double den = 0.;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double u = __ldg(Uin + v * N + c);
+        s[v * SWT_FIELD] = u;
+        if (v < NE) den += u;
+      }
+      if (A.first) den = __ldg(F.V + c);
+      s[S_DEN * SWT_FIELD] = den;
+      s[S_XC * SWT_FIELD] = centre_from_planes<DIM, D>(back, front);
+      s[S_FC * SWT_FIELD] = back.fc;
+      s[S_UN * SWT_FIELD] = back.un;
+      s[S_L * SWT_FIELD] = back.L;
+    }
+  }
+  __syncthreads();
+  // -- 2. sweep (warp w: column x0 + w, lane: position along D)
+  const int lane = threadIdx.x % SW_LANES, w = threadIdx.x / SW_LANES;
+  const int ta = x0 + w;
+  if (ta < M.ncx && g0 < nb * nd) {  // warp-uniform
+    const int g = g0 + lane;
+    const bool ok = g >= 0 && g < nb * nd;
+    int tb = 0, p = 0;
+    if (ok) {
+      tb = (int)((unsigned)g / (unsigned)nd);
+      p = g - tb * nd;
+    }
+    const bool out = ok && lane >= 2 && lane < 2 + XOUT;
+    const double dt = F.s->dt;
+    const int order2 = LIM == LIM_ORDER1 ? 0 : 1;  // ordre-projection - 1
+    double* s = sm + lane * SWT_PITCH + w;
+    double u[NV], den = 1., xc = 0., fc = 0., un = 0., L = 0., ondB = 0., ondF = 0.;
+    if (ok) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = s[v * SWT_FIELD];
+      den = s[S_DEN * SWT_FIELD];
+      xc = s[S_XC * SWT_FIELD];
+      fc = s[S_FC * SWT_FIELD];
+      un = s[S_UN * SWT_FIELD];
+      L = s[S_L * SWT_FIELD];
+      if (out) {
+        // outer normals of the back and front faces (initial grid)
+        constexpr int A0 = 0, A1 = D == 2 ? 1 : 2;
+        const double t0 = fc0_comp<DIM, D, A0>(M, ta) - cc0_comp<DIM, A0>(M, ta);
+        const double t1 = fc0_comp<DIM, D, A1>(M, tb) - cc0_comp<DIM, A1>(M, tb);
+        const double cc0 = cc0_comp<DIM, D>(M, p);
+        ondB = unit_comp<D>(fc0_comp<DIM, D, D>(M, p) - cc0, t0, t1);
+        ondF = unit_comp<D>(fc0_comp<DIM, D, D>(M, p + 1) - cc0, t0, t1);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = 0.;
+    }
+    const bool ok_l = __shfl_up_sync(FULL, ok, 1) && lane > 0 && p > 0;  // same line
+    const double xc_l = __shfl_up_sync(FULL, xc, 1);
+    const bool face_b = ok && ok_l;                       // face between p-1 and p
+    const bool face_f = __shfl_down_sync(FULL, face_b, 1) && lane < 31;
+    const double un_r = __shfl_down_sync(FULL, un, 1), L_r = __shfl_down_sync(FULL, L, 1);
+    const double dxb = xc - xc_l;
+    const bool up_left = un * dxb > 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double phi = ok ? div_rn(u[v], den) : 0.;
+      const double phi_l = __shfl_up_sync(FULL, phi, 1);
+      const double gf = face_b ? div_rn(phi - phi_l, dxb) : 0.;
+      const double gf_r = __shfl_down_sync(FULL, gf, 1);
+      const double gr = (LIM != LIM_ORDER1 && ok) ? limited_gradient_t<LIM>(gf, gf_r) : 0.;
+      const double gr_l = __shfl_up_sync(FULL, gr, 1);
+      double pf = 0.;
+      if (face_b) pf = up_left ? phi_l + order2 * (fc - xc_l) * gr_l : phi + order2 * (fc - xc) * gr;
+      const double pf_r = __shfl_down_sync(FULL, pf, 1);
+      if (out) {
+        // cell local face order along y and z: back then front
+        const double fB = face_b ? ondB * un * L * dt * pf : 0.;
+        const double fF = face_f ? ondF * un_r * L_r * dt * pf_r : 0.;
+        double sumf = 0., dual = 0.;
+        if (face_b) { sumf += fB; dual += 0.5 * fB * ondB; }
+        if (face_f) { sumf += fF; dual += 0.5 * fF * ondF; }
+        double uo = u[v] - sumf;
+        if (v >= NE && v < 3 * NE && uo < 0.) uo = 0.;  // masses and energies stay >= 0
+        s[v * SWT_FIELD] = uo;                          // the lane's own slots: read above
+        if (v >= NE && v < 2 * NE) s[(S_XC + v - NE) * SWT_FIELD] = dual;
+      }
+    }
+  }
+  __syncthreads();
+  // -- 3. store (row layout), written positions only
+  {
+    const int col = threadIdx.x % SWT_COLS, pos = threadIdx.x / SWT_COLS;
+    const int i = x0 + col, g = g0 + pos;
+    if (pos >= 2 && pos < 2 + XOUT && i < M.ncx && g < nb * nd) {
+      const int tb = (int)((unsigned)g / (unsigned)nd), p = g - tb * nd;
+      const long long c = cell_id(M, i, D == 1 ? p : tb, D == 1 ? tb : p);
+      const double* s = sm + pos * SWT_PITCH + col;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) A.Uout[v * N + c] = s[v * SWT_FIELD];
+#pragma unroll
+      for (int e = 0; e < NE; ++e) F.mflux[e * N + c] = s[(S_XC + e) * SWT_FIELD];
+    }
+  }
+  __syncthreads();  // the tile is reused by the block's next work item
 }
 
 // ---------------------------------------------------------------------------
@@ -1284,7 +1439,7 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
   const int nb = D == 1 ? M.nnz : M.nny;
   const long long col = (long long)vbx * SW_THREADS + threadIdx.x;
   if (col >= (long long)M.nnx * nb) return;
-  const int i = (int)(col % M.nnx), tb = (int)(col / M.nnx);
+  const int tb = (int)((unsigned)col / (unsigned)M.nnx), i = (int)col - tb * M.nnx;
   int o0, o1;
   col_chunk_range(nn, vby, o0, o1);
   if (o0 >= o1) return;

@@ -19,6 +19,14 @@ void cell_sweep(Engine* e, Group& g, int D, int k) {
   else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells<DIM, NE, 2, LIM>, SW_THREADS, 0, g.sw_cells[2], k);
 }
 
+// y / z cell sweeps through the shared-memory tile
+template <int DIM, int NE, int LIM>
+void cell_sweep_tile(Engine* e, Group& g, int D, int k) {
+  StageTimer tm(e, MHC_STAGE_SWEEP_CELLS);
+  if (D == 1) plaunch(e, kb_sweep_cells_tile<DIM, NE, 1, LIM>, SWT_THREADS, swt_smem_bytes(NE), g.sw_cells[1], k);
+  else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells_tile<DIM, NE, 2, LIM>, SWT_THREADS, swt_smem_bytes(NE), g.sw_cells[2], k);
+}
+
 template <int DIM, int NE, int LIM>
 void node_sweep(Engine* e, Group& g, int D, int k) {
   StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
@@ -33,7 +41,14 @@ void node_sweep(Engine* e, Group& g, int D, int k) {
 template <int DIM, int NE>
 void sweep_step_dn(Engine* e, Group& g, int D, int k) {
   const int cl = ((g.COLS >> D) & 1) ? LIM_COLS + g.CLIM : g.CLIM;
-  switch (cl) {
+  if (D > 0 && !((g.COLS >> D) & 1) && ((g.TILE >> D) & 1)) {
+    switch (g.CLIM) {
+      case 0: cell_sweep_tile<DIM, NE, 0>(e, g, D, k); break;
+      case 1: cell_sweep_tile<DIM, NE, 1>(e, g, D, k); break;
+      case 2: cell_sweep_tile<DIM, NE, 2>(e, g, D, k); break;
+      default: cell_sweep_tile<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
+    }
+  } else switch (cl) {
     case LIM_COLS + 0: cell_sweep<DIM, NE, LIM_COLS + 0>(e, g, D, k); break;
     case LIM_COLS + 1: cell_sweep<DIM, NE, LIM_COLS + 1>(e, g, D, k); break;
     case LIM_COLS + 2: cell_sweep<DIM, NE, LIM_COLS + 2>(e, g, D, k); break;

@@ -106,6 +106,18 @@ def test_parity_exact_line_chunk_layout(name, monkeypatch):
     assert not bad, (name, bad)
 
 
+# y / z cell sweeps in the warp-per-line layout that the shared-memory tile
+# replaced (MHC_SWEEP_TILE=0)
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["adi3d_bisod_superbee", "adi3d_bisod_z_vanleer", "adi2d_sedov", "adi2d_bisod_order1"])
+def test_parity_exact_warp_per_line_layout(name, monkeypatch):
+    monkeypatch.setenv("MHC_SWEEP_TILE", "0")
+    init_errs, errs = run_pair(name, cr_pow=True)
+    assert max(init_errs.values()) == 0.0, init_errs
+    bad = {k: v for k, v in errs.items() if v != 0.0}
+    assert not bad, (name, bad)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", sorted(PARITY_CASES))
 def test_parity_reference_libm(name):
