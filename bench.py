@@ -252,25 +252,17 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def run_ours(args):
+def measure_plain(lib, p, steps: int, warmup: int, local: int = 0, world: int = 1) -> dict:
+    """The plain form on one case, device-resident: W warm-up iterations,
+    then K iterations replayed from the case's CUDA graph (captured before
+    the warm-up) between CUDA events on the case stream; then per-kernel
+    device times (events around every kernel group) for the roofline."""
     import torch
     import mahyco_b200 as mb
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    lib = mb.load()
-    p = build_params(args.workload)
-    ncell, nnode = p.ncell, p.nnode
-    # -- device-resident throughput
     h = mb.Hydro(p, lib)
     h.hydroStartInit()
     h.cycle(0, graph=True)  # capture the CUDA graph of one sweep-order period (no iteration)
-    h.cycle(args.warmup, graph=True)
+    h.cycle(warmup, graph=True)
     st = h.synchronize()
     stream = torch.cuda.ExternalStream(h.stream_handle)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -285,7 +277,7 @@ def run_ours(args):
     l0 = h.launches
     with ClockSampler(local) as clocks:
         e0.record(stream)
-        h.cycle(args.steps, graph=True)
+        h.cycle(steps, graph=True)
         e1.record(stream)
         e1.synchronize()
     barrier()
@@ -293,12 +285,50 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     st |= h.synchronize()
     ms = max_over_ranks(ms)
-    value = replica_value(ncell * args.steps, world, ms)
-    # -- per-kernel device times (events on the case stream around each group)
-    nprof = max(2 * p.dim, min(args.steps, 4 * p.dim))
+    nprof = max(2 * p.dim, min(steps, 4 * p.dim))
     stages = h.cycle_timed(nprof)
-    s_after = h.scalars()
     h.close()
+    ncell, nnode = p.ncell, p.nnode
+    pk = peaks()
+    dom = max(stages, key=lambda s: stages[s][0])
+    dom_ms, dom_n = stages[dom]
+    dom_bytes = stage_bytes(dom, p.dim, p.nb_env, ncell, nnode)
+    achieved = dom_bytes / (dom_ms * 1e-3 / dom_n) / 1e9
+    cycle_bytes = sum(stage_bytes(s, p.dim, p.nb_env, ncell, nnode) * (stages[s][1] / nprof) for s in stages)
+    return {
+        "value": replica_value(ncell * steps, world, ms), "ms_per_step": ms / steps, "status": st,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk.get("hbm_gbs"),
+                     "unit": "GB/s", "frac": achieved / pk.get("hbm_gbs"),
+                     "peak_source": "measured" if "how" in pk else "fallback",
+                     "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms / dom_n},
+        "cycle_roofline": {"bytes_per_cell_cycle": cycle_bytes / ncell,
+                           "achieved_gbs": cycle_bytes * steps / (ms * 1e-3) / 1e9 * world},
+        "stages_ms_per_cycle": {s: stages[s][0] / nprof for s in stages},
+        "clocks": clocks.summary(),
+    }
+
+
+def run_ours(args):
+    import torch
+    import mahyco_b200 as mb
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    lib = mb.load()
+    p = build_params(args.workload)
+    ncell, nnode = p.ncell, p.nnode
+    parts = {}
+    w0 = time.perf_counter()
+    # -- device-resident throughput of the plain form
+    m = measure_plain(lib, p, args.steps, args.warmup, local, world)
+    m["roofline"]["traffic"] = profile_traffic(args.workload).get(m["roofline"]["kernel"])
+    parts["plain"] = time.perf_counter() - w0
     # -- end to end through the C ABI: host parameters in, host results out
     # (into page-locked result buffers the job allocates once, up front)
     import ctypes
@@ -326,59 +356,72 @@ def run_ours(args):
     g.close()
     e2e_s = time.perf_counter() - t0
     e2e_value = world * ncell * args.steps / e2e_s
+    parts["e2e"] = e2e_s
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    pk = peaks()
-    dom = max(stages, key=lambda s: stages[s][0])
-    dom_ms, dom_n = stages[dom]
-    dom_bytes = stage_bytes(dom, p.dim, p.nb_env, ncell, nnode)
-    achieved = dom_bytes / (dom_ms * 1e-3 / dom_n) / 1e9
-    traffic = profile_traffic(args.workload).get(dom)
-    cycle_bytes = sum(stage_bytes(s, p.dim, p.nb_env, ncell, nnode) * (stages[s][1] / nprof) for s in stages)
     out = {
-        "metric": METRIC, "value": value, "unit": "cell-cycles/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "metric": METRIC, "value": m["value"], "unit": "cell-cycles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload][0], "cells": ncell, "nodes": nnode,
                    "materials": p.nb_env, "remap": bool(p.with_projection),
-                   "l2": "working set > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
-        "status": st,
-        "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk.get("hbm_gbs"),
-                     "unit": "GB/s", "frac": achieved / pk.get("hbm_gbs"),
-                     "peak_source": "measured" if "how" in pk else "fallback",
-                     "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
-                     "ms_per_launch": dom_ms / dom_n},
-        "cycle_roofline": {"bytes_per_cell_cycle": cycle_bytes / ncell,
-                           "achieved_gbs": cycle_bytes * args.steps / (ms * 1e-3) / 1e9 * world},
-        "stages_ms_per_cycle": {s: stages[s][0] / nprof for s in stages},
-        "clocks": clocks.summary(),
+                   "l2": "working set > 126 MB L2, no flush", "parallelism": f"replicas x{world}",
+                   "timing": "K iterations replayed from the case's CUDA graph of one 6-iteration period"},
+        "status": m["status"],
+        "gpu_launches": m["gpu_launches"],
+        "roofline": m["roofline"],
+        "cycle_roofline": m["cycle_roofline"],
+        "stages_ms_per_cycle": m["stages_ms_per_cycle"],
+        "clocks": m["clocks"],
         "e2e": {"value": e2e_value, "unit": "cell-cycles/s",
                 "h2d_bytes_per_step": ctypes.sizeof(p) / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "timer": "host wall clock; includes case allocation, device init, every iteration's status read-back (overlapping the next iteration) and the final field download into page-locked result buffers allocated before the timed region"},
     }
     if world == 1 and not args.no_extras:
-        # the batched and served forms against the plain form, on bounded
-        # samples of their workloads (full runs: --workload batch2d / serve)
+        # the other stated configurations, each at its stated size:
+        # 3D Sedov 384^3 (the plain form's roofline target), the batched
+        # form on 4096 2D cases x 100 cycles and the served form on the
+        # mixed request stream, both against the plain form
+        w0 = time.perf_counter()
+        sp = build_params("sedov3d")
+        sm = measure_plain(lib, sp, steps=10, warmup=3, local=local)
+        out["sedov3d"] = dict(sm, workload=WORKLOADS["sedov3d"][0], cells=sp.ncell, steps=10, warmup=3,
+                              unit="cell-cycles/s")
+        parts["sedov3d"] = time.perf_counter() - w0
+        w0 = time.perf_counter()
         sub = argparse.Namespace(**vars(args))
-        sub.workload, sub.cases, sub.steps, sub.warmup, sub.plain_sample = "bisod3d", 1024, 12, 0, 128
+        sub.workload, sub.cases, sub.steps, sub.warmup, sub.plain_sample = "bisod3d", 4096, 100, 0, 512
         bo = run_batch(sub)
         out["batched"] = {"value": bo["value"], "plain_value": bo["plain"]["value"],
                           "batched_vs_plain": bo["batched_vs_plain"], "same_results": bo["plain"]["same_results"],
-                          "config": f"{sub.cases} cases of the batch2d workload, {sub.steps} timed cycles, plain form "
-                                    f"on {bo['plain']['sample_cases']} of them", "gpu_launches": bo["gpu_launches"]}
+                          "ms_per_step": bo["ms_per_step"], "latency_s": bo["latency_s"],
+                          "plain_latency_s": bo["plain"]["latency_s"],
+                          "config": f"{sub.cases} cases of the batch2d workload ({bo['config']['cells']} cells), "
+                                    f"{sub.steps} timed cycles each; plain form through each case's own CUDA "
+                                    f"graph on every {sub.cases // sub.plain_sample}-th case "
+                                    f"({bo['plain']['sample_cases']} cases)",
+                          "autotune": bo["autotune"], "gpu_launches": bo["gpu_launches"], "clocks": bo["clocks"]}
+        parts["batched"] = time.perf_counter() - w0
+        w0 = time.perf_counter()
         sub = argparse.Namespace(**vars(args))
-        sub.workload, sub.requests, sub.rate, sub.steps, sub.cycles_per_step = "bisod3d", 60, 40.0, 30, 4
+        sub.workload, sub.requests, sub.rate, sub.steps, sub.cycles_per_step = "bisod3d", 120, 16.0, 30, 4
         so = run_serve(sub)
         out["served"] = {"value": so["value"], "plain_value": so["plain"]["value"],
                          "served_vs_plain": so["served_vs_plain"], "latency_s": so["latency_s"],
                          "plain_latency_s": so["plain"]["latency_s"], "failed": len(so["failed"]),
-                         "config": f"{sub.requests} requests of the serve mix at {sub.rate}/s, {sub.steps} iterations each"}
+                         "offered_cell_cycles_per_s": so["config"]["offered_cell_cycles_per_s"],
+                         "config": f"{sub.requests} requests of the serve mix (1e3..1e7 cells) at a Poisson "
+                                   f"rate of {sub.rate}/s, {sub.steps} iterations each",
+                         "gpu_launches": so["gpu_launches"], "clocks": so["clocks"]}
+        parts["served"] = time.perf_counter() - w0
     if world == 1 and not args.no_cpu_baseline:
+        w0 = time.perf_counter()
         out["cpu_baseline"] = cpu_baseline(args.workload)
+        parts["cpu_baseline"] = time.perf_counter() - w0
+    out["parts_wall_s"] = parts
     print(json.dumps(out), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -452,12 +495,13 @@ def run_batch(args):
         w0 = time.perf_counter()
         h = mb.Hydro(p, lib)
         h.hydroStartInit()
-        h.cycle(warm)
+        h.cycle(0, graph=True)  # the plain form at its best: its own CUDA graph
+        h.cycle(warm, graph=True)
         st = torch.cuda.ExternalStream(h.stream_handle)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(st)
         pl0 = h.launches
-        h.cycle(args.steps)
+        h.cycle(args.steps, graph=True)
         plain_launches += h.launches - pl0
         a1.record(st)
         a1.synchronize()
@@ -488,7 +532,11 @@ def run_batch(args):
         "plain": {"value": plain, "unit": "cell-cycles/s", "sample_cases": len(sample),
                   "sample_cells": plain_cells, "same_results": same, "gpu_launches": plain_launches,
                   "latency_s": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-                  "how": "each sampled case alone through its own handle: create, init, warm-up, K timed cycles"},
+                  "how": "each sampled case alone through its own handle: create, init, capture of its CUDA "
+                         "graph, warm-up, K timed cycles replayed from the graph"},
+        "latency_s": {"p50": t_wall, "p99": t_wall,
+                      "how": "every case of the batch completes with the batch: host wall clock from the first "
+                             "case creation to the last status read-back"},
         "autotune": tuned["best"],
         "stages_ms_per_cycle": stages,
         "cases_not_at_limit": bad,
@@ -583,13 +631,20 @@ def run_serve(args):
     # sequential plain solves, each alone: create, init, cycles, read-back
     service = []
     for kind, p in reqs:
-        w0 = time.perf_counter()
-        h = mb.Hydro(p, lib)
-        h.hydroStartInit()
-        h.cycle(its)
-        h.scalars()
-        h.close()
-        service.append(time.perf_counter() - w0)
+        # the plain form at its best: each request solved both with plain
+        # launches and with its own CUDA graph of one sweep-order period
+        # (capture included), the faster kept
+        best = None
+        for graph in (False, True):
+            w0 = time.perf_counter()
+            h = mb.Hydro(p, lib)
+            h.hydroStartInit()
+            h.cycle(its, graph=graph)
+            h.scalars()
+            h.close()
+            dt_s = time.perf_counter() - w0
+            best = dt_s if best is None else min(best, dt_s)
+        service.append(best)
     fin, plat = 0.0, []
     for a, sv in zip(arrivals, service):  # FIFO queue under the same arrivals
         fin = max(fin, a) + sv
@@ -617,8 +672,9 @@ def run_serve(args):
                   "latency_s": {"p50": pct(plat, 0.5), "p99": pct(plat, 0.99), "max": plat[-1]},
                   "busy_value": work / sum(service),
                   "how": "the same requests solved one after another through their own handles (create, init, "
-                         "iterations, status read-back); value and latency from a FIFO queue of the measured "
-                         "service times under the same arrivals; busy_value = work / sum of service times"},
+                         "iterations, status read-back), each timed with plain launches and with its own CUDA "
+                         "graph and the faster kept; value and latency from a FIFO queue of those service times "
+                         "under the same arrivals; busy_value = work / sum of service times"},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "e2e": {"value": served, "unit": "cell-cycles/s",

@@ -66,7 +66,7 @@ int engine_rebuild(Engine* e) {
   }
   if (nc) CK(cudaMemcpyAsync(e->d_desc, desc.data(), nc * sizeof(CaseDesc), cudaMemcpyHostToDevice, e->stream));
   // groups
-  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
@@ -76,14 +76,14 @@ int engine_rebuild(Engine* e) {
     int sens = (int)((h->it_host - 1) % h->DIM);
     const int el = case_elasto(h) ? 1 : 0, hg = case_hourglass(h) ? 1 : 0;
     const int lim = node_sweep_mode(h->P), clim = cell_sweep_mode(h->P);
-    const int cols = cols_mask(h), ncols = node_cols_mask(h), tile = tile_mask(h);
+    const int cols = cols_mask(h), ncols = node_cols_mask(h), tile = tile_mask(h), ntile = node_tile_mask(h);
     const int cbc = case_cell_bcs(h) ? 1 : 0;
-    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols, cbc, tile);
+    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols, cbc, tile, ntile);
     auto it = gidx.find(key);
     if (it == gidx.end()) {
       Group g;
       g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
-      g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim; g.COLS = cols; g.NCOLS = ncols; g.CBC = cbc; g.TILE = tile;
+      g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim; g.COLS = cols; g.NCOLS = ncols; g.CBC = cbc; g.TILE = tile; g.NTILE = ntile;
       gidx[key] = (int)e->groups.size();
       e->groups.push_back(g);
       it = gidx.find(key);
@@ -117,7 +117,7 @@ int engine_rebuild(Engine* e) {
               phase(g.lag_nodes, PH_NODES);
     for (int D = 0; D < g.DIM; ++D)
       ok = ok && phase(g.sw_cells[D], group_cell_phase(g.CLIM, g.COLS, g.TILE, D)) &&
-           phase(g.sw_nodes[D], node_sweep_phase(((g.NCOLS >> D) & 1) ? LIM_COLS + g.LIM : g.LIM, D));
+           phase(g.sw_nodes[D], group_node_phase(g.LIM, g.NCOLS, g.NTILE, D));
     if (!ok) return set_err(MHC_ERR_ARG, "more than 2^31 blocks in one phase of a batch");
   }
   if (ints.size() > e->ints_cap) {

@@ -75,6 +75,7 @@ struct Group {
   int CLIM = 0;                // cell-sweep instance: the same, LIM_O3 (third order) or LIM_PB (pente-borne)
   int COLS = 0;                // bit D: the classical cell sweep along D uses one thread per line chunk
   int TILE = 0;                // bit D: ... or a shared-memory tile (when not COLS)
+  int NTILE = 0;               // bit D: the node sweep along D uses a shared-memory tile (when not NCOLS)
   int NCOLS = 0;               // bit D: the same for the node sweep
   long long it0;               // iteration of the members when the lists were built
   std::vector<int> members;
@@ -200,6 +201,23 @@ inline int tile_mask(const mhc_case* h) {
   int m = 0;
   for (int D = 1; D < h->DIM; ++D) m |= 1 << D;
   return m & ~cols_mask(h);
+}
+
+// the same for the node sweeps (MHC_SWEEP_TILE=0 also keeps their
+// warp-per-line layout)
+inline int node_tile_mask(const mhc_case* h) {
+  if (node_sweep_mode(h->P) > LIM_ORDER1) return 0;
+  const char* s = getenv("MHC_SWEEP_TILE");
+  if (s && *s == '0') return 0;
+  int m = 0;
+  for (int D = 1; D < h->DIM; ++D) m |= 1 << D;
+  return m & ~node_cols_mask(h);
+}
+
+inline int group_node_phase(int LIM, int NCOLS, int NTILE, int D) {
+  if ((NCOLS >> D) & 1) return node_sweep_phase(LIM_COLS + LIM, D);
+  if ((NTILE >> D) & 1) return PH_SWNT0 + D;
+  return node_sweep_phase(LIM, D);
 }
 
 // phase of the cell sweep of a group along D

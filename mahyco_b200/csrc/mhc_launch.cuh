@@ -35,7 +35,8 @@ enum PhaseKind {
   PH_SWNW0 = 12,     // node sweep with the wide (generalised limiter) stencil
   PH_SWCC0 = 15,     // cell sweep along D = 1, 2, one thread per line chunk
   PH_SWNC0 = 18,     // node sweep along D = 1, 2, one thread per line chunk
-  PH_SWCT0 = 21      // cell sweep along D = 1, 2 through a shared-memory tile
+  PH_SWCT0 = 21,     // cell sweep along D = 1, 2 through a shared-memory tile
+  PH_SWNT0 = 24      // node sweep along D = 1, 2 through a shared-memory tile
 };
 
 // phase of the cell sweep along D for a cell-sweep instance
@@ -58,6 +59,13 @@ __host__ __device__ inline void phase_grid(int ph, const Mesh& M, int& gx, int& 
   gy = gz = 1;
   if (ph == PH_CELLS) { gx = cdiv_i(M.ncell, CT); return; }
   if (ph == PH_NODES) { gx = cdiv_i(M.nnode, CT); return; }
+  if (ph >= PH_SWNT0) {  // body_sweep_nodes_tile
+    const int D = ph - PH_SWNT0;
+    const int nb = D == 1 ? M.nnz : M.nny, nd = D == 1 ? M.nny : M.nnz;
+    gx = cdiv_i(M.nnx, SWT_COLS);
+    gy = cdiv_i((long long)nb * nd, NOUT);
+    return;
+  }
   if (ph >= PH_SWCT0) {  // body_sweep_cells_tile
     const int D = ph - PH_SWCT0;
     const int nb = D == 1 ? M.ncz : M.ncy, nd = D == 1 ? M.ncy : M.ncz;
@@ -122,6 +130,25 @@ __device__ __forceinline__ WorkItem item_at(const CaseDesc* __restrict__ C, cons
 }
 
 #define MHC_FOR_ITEMS(L) for (int w_ = blockIdx.x; w_ < (L).total; w_ += gridDim.x)
+
+// directions swept before the k-th sweep of the iteration
+// (RemapADIService.cc:23-33)
+template <int DIM>
+__device__ __forceinline__ int sweep_done_dirs(const Mesh& M, const mhc_case_params& P, long long iteration, int k) {
+  int done = 0;
+  const int sens = (int)((iteration - 1) % DIM);
+  int cnt = 0;
+  for (int i = 0; i < M.dim; ++i) {
+    const int d = (i + sens) % M.dim;
+    const int ncd = d == 0 ? M.ncx : (d == 1 ? M.ncy : M.ncz);
+    if (ncd == 1) continue;
+    if (P.is_euler_scheme >= MHC_EULER_X && P.is_euler_scheme <= MHC_EULER_Z && d != P.is_euler_scheme - MHC_EULER_X)
+      continue;
+    if (cnt < k) done |= 1 << d;
+    ++cnt;
+  }
+  return done;
+}
 
 template <int DIM, int NE>
 __global__ void __launch_bounds__(CT) kb_init_cells(const CaseDesc* __restrict__ C, PhaseList L) {
@@ -284,6 +311,32 @@ kb_sweep_cells_tile(const CaseDesc* __restrict__ C, PhaseList L, int k) {
   }
 }
 
+// node sweep along D = 1, 2 through a shared-memory tile
+#ifndef MHC_SWTN_MIN_BLOCKS
+#define MHC_SWTN_MIN_BLOCKS 3
+#endif
+template <int DIM, int NE, int D, int LIM>
+__global__ void __launch_bounds__(SWT_THREADS, MHC_SWTN_MIN_BLOCKS)
+kb_sweep_nodes_tile(const CaseDesc* __restrict__ C, PhaseList L, int k) {
+  extern __shared__ double swtn_tile[];
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_SWNT0 + D>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;  // uniform over the block (one case per item)
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    const mhc_case_params& P = *C[wi.c].P;
+    DualArgs A;
+    A.Uin = k == 0 ? nullptr : (((k - 1) & 1) ? F.Ud[1] : F.Ud[0]);
+    A.Uout = (k & 1) ? F.Ud[1] : F.Ud[0];
+    A.order = P.ordre_projection;
+    A.limiter = P.projection_limiteur_id;
+    A.simple_pente = P.projection_simple_pente;
+    A.done_dirs = sweep_done_dirs<DIM>(M, P, F.s->iteration, k);
+    body_sweep_nodes_tile<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y, swtn_tile);
+  }
+}
+
 #ifndef MHC_SW_MIN_BLOCKS_NODECOLS
 #define MHC_SW_MIN_BLOCKS_NODECOLS 4
 #endif
@@ -298,21 +351,7 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
     const mhc_case_params& P = *C[wi.c].P;
-    // directions swept before step k this cycle (RemapADIService.cc:23-33)
-    int done = 0;
-    {
-      const int sens = (int)((F.s->iteration - 1) % DIM);
-      int cnt = 0;
-      for (int i = 0; i < M.dim; ++i) {
-        const int d = (i + sens) % M.dim;
-        const int ncd = d == 0 ? M.ncx : (d == 1 ? M.ncy : M.ncz);
-        if (ncd == 1) continue;
-        if (P.is_euler_scheme >= MHC_EULER_X && P.is_euler_scheme <= MHC_EULER_Z && d != P.is_euler_scheme - MHC_EULER_X)
-          continue;
-        if (cnt < k) done |= 1 << d;
-        ++cnt;
-      }
-    }
+    const int done = sweep_done_dirs<DIM>(M, P, F.s->iteration, k);
     DualArgs A;
     A.Uin = k == 0 ? nullptr : (((k - 1) & 1) ? F.Ud[1] : F.Ud[0]);
     A.Uout = (k & 1) ? F.Ud[1] : F.Ud[0];

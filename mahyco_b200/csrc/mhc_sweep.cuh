@@ -1522,4 +1522,133 @@ __device__ __forceinline__ void body_sweep_nodes_cols(const Mesh& M, const Field
   }
 }
 
+// ---------------------------------------------------------------------------
+// Node sweep along D = 1, 2 through a shared-memory tile, classical limiters
+// and first order (the layout of body_sweep_cells_tile): the load layout
+// stages, per node, its position along D, its projected dual variables, the
+// values phi of the limited reconstruction and the mass flux through its
+// front half-plane; warp w then runs the arithmetic of
+// body_sweep_nodes_lanes on column w, in the same order, and the store
+// layout writes the updated variables of the written nodes (NOUT per
+// window).
+// ---------------------------------------------------------------------------
+constexpr int SWTN_SLOTS = 11;  // x, U[5], phi[4], front mass flux
+constexpr int SWTN_SMEM_BYTES = SWTN_SLOTS * SWT_FIELD * 8;
+
+template <int DIM, int NE, int D, int LIM>
+__device__ __forceinline__ void body_sweep_nodes_tile(const Mesh& M, const Fields& F, const DualArgs& A, int vbx,
+                                                      int vby, double* __restrict__ sm) {
+  static_assert(D >= 1, "x sweeps use the lane layout");
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int S_X = 0, S_U = 1, S_PH = 6, S_FFM = 10;
+  const long long NN = M.nnode;
+  const int nn = D == 1 ? M.nny : M.nnz, nb = D == 1 ? M.nnz : M.nny;
+  const int x0 = vbx * SWT_COLS;
+  const int g0 = vby * NOUT - 2;  // first position of the window (2 halo nodes)
+  // -- 1. load (row layout)
+  {
+    const int col = threadIdx.x % SWT_COLS, pos = threadIdx.x / SWT_COLS;
+    const int i = x0 + col, g = g0 + pos;
+    if (i < M.nnx && g >= 0 && g < nb * nn) {
+      const int tb = (int)((unsigned)g / (unsigned)nn), id = g - tb * nn;
+      const int j = D == 1 ? id : tb, k = D == 1 ? tb : id;
+      double ph[4], x, ffm, U[5];
+      node_state<DIM, NE, D>(M, F, A, i, j, k, id, ph, x, ffm);
+      node_u(F, A, NN, node_id(M, i, j, k), U);
+      double* s = sm + pos * SWT_PITCH + col;
+      s[S_X * SWT_FIELD] = x;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) s[(S_U + q) * SWT_FIELD] = U[q];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) s[(S_PH + q) * SWT_FIELD] = ph[q];
+      s[S_FFM * SWT_FIELD] = ffm;
+    }
+  }
+  __syncthreads();
+  // -- 2. sweep (warp w: column x0 + w, lane: position along D)
+  const int lane = threadIdx.x % SW_LANES, w = threadIdx.x / SW_LANES;
+  if (x0 + w < M.nnx && g0 < nb * nn) {  // warp-uniform
+    const int g = g0 + lane;
+    const bool ok = g >= 0 && g < nb * nn;
+    const int id = ok ? g - (int)((unsigned)g / (unsigned)nn) * nn : 0;
+    const bool inner = ok && id > 0 && id < nn - 1;
+    const bool out = ok && lane >= 2 && lane < 2 + NOUT;
+    double* s = sm + lane * SWT_PITCH + w;
+    double U[5] = {0., 0., 0., 0., 0.}, ph[4] = {0., 0., 0., 0.}, x = 0., ffm = 0.;
+    if (ok) {
+      x = s[S_X * SWT_FIELD];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) U[q] = s[(S_U + q) * SWT_FIELD];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) ph[q] = s[(S_PH + q) * SWT_FIELD];
+      ffm = s[S_FFM * SWT_FIELD];
+    }
+    const double x_l = __shfl_up_sync(FULL, x, 1), x_r = __shfl_down_sync(FULL, x, 1);
+    double ph_l[4], ph_r[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ph_l[q] = __shfl_up_sync(FULL, ph[q], 1);
+      ph_r[q] = __shfl_down_sync(FULL, ph[q], 1);
+    }
+    const double bfm = __shfl_up_sync(FULL, ffm, 1);
+    double gr[3], g_l[3], g_r[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      gr[q] = 0.;
+      const double gfw = LIM != LIM_ORDER1 ? div_rn(ph_r[q] - ph[q], x_r - x) : 0.;
+      const double gbw = __shfl_up_sync(FULL, gfw, 1);
+      if (LIM != LIM_ORDER1 && inner) gr[q] = limited_gradient_t<LIM>(gbw, gfw);
+      g_l[q] = __shfl_up_sync(FULL, gr[q], 1);
+      g_r[q] = __shfl_down_sync(FULL, gr[q], 1);
+    }
+    if (out && inner) {
+      const double dt = F.s->dt;
+      const int order2 = LIM == LIM_ORDER1 ? 0 : A.order - 1;  // ordre-projection - 1
+      U[3] += bfm - ffm;
+      double FV[3], BV[3], FE, BE;
+      {
+        const double ufront = 0.5 * (ph[D] + ph_r[D]);
+        const int signfront = (ufront > 0) ? 1 : -1;
+        const bool fr = ffm < 0.;
+        const double geo = (signfront * (x_r - x) - dt * ufront);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) FV[q] = (fr ? ph_r[q] : ph[q]) + order2 * (0.5 * (fr ? g_r[q] : gr[q]) * geo);
+        FE = (fr ? ph_r[3] : ph[3]) + order2 * (0.5 * 0. * geo);
+      }
+      {
+        const double uback = 0.5 * (ph_l[D] + ph[D]);
+        const int signback = (uback > 0) ? 1 : -1;
+        const bool bk = bfm > 0.;
+        const double geo = (signback * (x - x_l) - dt * uback);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) BV[q] = (bk ? ph_l[q] : ph[q]) + order2 * (0.5 * (bk ? g_l[q] : gr[q]) * geo);
+        BE = (bk ? ph_l[3] : ph[3]) + order2 * (0.5 * 0. * geo);
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) U[q] += bfm * BV[q] - ffm * FV[q];
+      U[4] += bfm * BE - ffm * FE;
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        if (fabs(U[q]) < 1.e-300) U[q] = 0.;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) s[(S_U + q) * SWT_FIELD] = U[q];  // the lane's own slots
+    }
+    // outer nodes (not inner) keep their staged U
+  }
+  __syncthreads();
+  // -- 3. store (row layout), written positions only
+  {
+    const int col = threadIdx.x % SWT_COLS, pos = threadIdx.x / SWT_COLS;
+    const int i = x0 + col, g = g0 + pos;
+    if (pos >= 2 && pos < 2 + NOUT && i < M.nnx && g < nb * nn) {
+      const int tb = (int)((unsigned)g / (unsigned)nn), id = g - tb * nn;
+      const long long n = node_id(M, i, D == 1 ? id : tb, D == 1 ? tb : id);
+      const double* s = sm + pos * SWT_PITCH + col;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) A.Uout[q * NN + n] = s[(S_U + q) * SWT_FIELD];
+    }
+  }
+  __syncthreads();  // the tile is reused by the block's next work item
+}
+
 }  // namespace mhc

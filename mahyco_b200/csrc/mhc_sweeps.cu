@@ -27,6 +27,14 @@ void cell_sweep_tile(Engine* e, Group& g, int D, int k) {
   else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells_tile<DIM, NE, 2, LIM>, SWT_THREADS, swt_smem_bytes(NE), g.sw_cells[2], k);
 }
 
+// y / z node sweeps through the shared-memory tile
+template <int DIM, int NE, int LIM>
+void node_sweep_tile(Engine* e, Group& g, int D, int k) {
+  StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
+  if (D == 1) plaunch(e, kb_sweep_nodes_tile<DIM, NE, 1, LIM>, SWT_THREADS, SWTN_SMEM_BYTES, g.sw_nodes[1], k);
+  else if constexpr (DIM == 3) plaunch(e, kb_sweep_nodes_tile<DIM, NE, 2, LIM>, SWT_THREADS, SWTN_SMEM_BYTES, g.sw_nodes[2], k);
+}
+
 template <int DIM, int NE, int LIM>
 void node_sweep(Engine* e, Group& g, int D, int k) {
   StageTimer tm(e, MHC_STAGE_SWEEP_NODES);
@@ -62,7 +70,14 @@ void sweep_step_dn(Engine* e, Group& g, int D, int k) {
     default: cell_sweep<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
   }
   const int nl = ((g.NCOLS >> D) & 1) ? LIM_COLS + g.LIM : g.LIM;
-  switch (nl) {
+  if (D > 0 && !((g.NCOLS >> D) & 1) && ((g.NTILE >> D) & 1)) {
+    switch (g.LIM) {
+      case 0: node_sweep_tile<DIM, NE, 0>(e, g, D, k); break;
+      case 1: node_sweep_tile<DIM, NE, 1>(e, g, D, k); break;
+      case 2: node_sweep_tile<DIM, NE, 2>(e, g, D, k); break;
+      default: node_sweep_tile<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
+    }
+  } else switch (nl) {
     case LIM_COLS + 0: node_sweep<DIM, NE, LIM_COLS + 0>(e, g, D, k); break;
     case LIM_COLS + 1: node_sweep<DIM, NE, LIM_COLS + 1>(e, g, D, k); break;
     case LIM_COLS + 2: node_sweep<DIM, NE, LIM_COLS + 2>(e, g, D, k); break;
