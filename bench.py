@@ -405,18 +405,24 @@ def run_ours(args):
                                     f"({bo['plain']['sample_cases']} cases)",
                           "autotune": bo["autotune"], "gpu_launches": bo["gpu_launches"], "clocks": bo["clocks"]}
         parts["batched"] = time.perf_counter() - w0
-        w0 = time.perf_counter()
-        sub = argparse.Namespace(**vars(args))
-        sub.workload, sub.requests, sub.rate, sub.steps, sub.cycles_per_step = "bisod3d", 120, 16.0, 30, 4
-        so = run_serve(sub)
-        out["served"] = {"value": so["value"], "plain_value": so["plain"]["value"],
-                         "served_vs_plain": so["served_vs_plain"], "latency_s": so["latency_s"],
-                         "plain_latency_s": so["plain"]["latency_s"], "failed": len(so["failed"]),
-                         "offered_cell_cycles_per_s": so["config"]["offered_cell_cycles_per_s"],
-                         "config": f"{sub.requests} requests of the serve mix (1e3..1e7 cells) at a Poisson "
-                                   f"rate of {sub.rate}/s, {sub.steps} iterations each",
-                         "gpu_launches": so["gpu_launches"], "clocks": so["clocks"]}
-        parts["served"] = time.perf_counter() - w0
+        # the served form at two stated Poisson rates: 16/s (about half of
+        # the plain form's capacity: the latency regime) and 64/s (above
+        # it: both forms run flat out, the throughput regime)
+        for key, rate in (("served", 16.0), ("served_overload", 64.0)):
+            w0 = time.perf_counter()
+            sub = argparse.Namespace(**vars(args))
+            sub.workload, sub.requests, sub.rate, sub.steps, sub.cycles_per_step = "bisod3d", 120, rate, 30, 4
+            so = run_serve(sub)
+            out[key] = {"value": so["value"], "plain_value": so["plain"]["value"],
+                        "served_vs_plain": so["served_vs_plain"], "latency_s": so["latency_s"],
+                        "plain_latency_s": so["plain"]["latency_s"], "latency_by_class_s": so["latency_by_class_s"],
+                        "plain_busy_value": so["plain"]["busy_value"], "failed": len(so["failed"]),
+                        "offered_cell_cycles_per_s": so["config"]["offered_cell_cycles_per_s"],
+                        "work_share_requests_ge_1e6_cells": so["work_share_requests_ge_1e6_cells"],
+                        "config": f"{sub.requests} requests of the serve mix (1e3..1e7 cells) at a Poisson "
+                                  f"rate of {sub.rate}/s, {sub.steps} iterations each",
+                        "gpu_launches": so["gpu_launches"], "clocks": so["clocks"]}
+            parts[key] = time.perf_counter() - w0
     if world == 1 and not args.no_cpu_baseline:
         w0 = time.perf_counter()
         out["cpu_baseline"] = cpu_baseline(args.workload)
@@ -655,6 +661,23 @@ def run_serve(args):
 
     def pct(v, q):
         return v[min(len(v) - 1, int(q * len(v)))]
+
+    # latency by size class (the server's classes: < 3e4, < 1e6, larger)
+    def cls_of(n):
+        return "small" if n < 30000 else ("medium" if n < 1000000 else "large")
+    by_cls = {}
+    for i, (_, p) in enumerate(reqs):
+        c = cls_of(p.ncell)
+        by_cls.setdefault(c, ([], []))
+        by_cls[c][0].append(done_at[i][0] - arrivals[i])
+    fin2 = 0.0
+    for i, (a, sv) in enumerate(zip(arrivals, service)):
+        fin2 = max(fin2, a) + sv
+        by_cls[cls_of(reqs[i][1].ncell)][1].append(fin2 - a)
+    cls_lat = {c: {"requests": len(v[0]), "served_p50": pct(sorted(v[0]), 0.5), "served_p99": pct(sorted(v[0]), 0.99),
+                   "plain_p50": pct(sorted(v[1]), 0.5), "plain_p99": pct(sorted(v[1]), 0.99)}
+               for c, v in sorted(by_cls.items())}
+    big = sum(p.ncell for _, p in reqs if p.ncell >= 1000000) * its
     out = {
         "metric": METRIC, "value": served, "unit": "cell-cycles/s", "n_gpus": 1,
         "steps": its, "warmup": 3, "ms_per_step": None,
@@ -666,6 +689,8 @@ def run_serve(args):
                    "offered_cell_cycles_per_s": work / (arrivals[-1] - arrivals[0]),
                    "l2": "mixed sizes; large requests exceed L2"},
         "latency_s": {"p50": pct(lat, 0.5), "p99": pct(lat, 0.99), "max": lat[-1]},
+        "latency_by_class_s": cls_lat,
+        "work_share_requests_ge_1e6_cells": big / work,
         "failed": failed,
         "served_vs_plain": served / plain,
         "plain": {"value": plain, "unit": "cell-cycles/s",

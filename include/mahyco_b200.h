@@ -249,6 +249,9 @@ int mhc_time_history(mhc_case* h, double* out);
  * bit-identical to the same case run alone. */
 typedef struct mhc_batch mhc_batch;
 int mhc_batch_create(mhc_batch** out);
+/* the same on a stream the caller owns (a cudaStream_t, e.g. created with a
+ * priority); it must outlive the batch */
+int mhc_batch_create_on_stream(void* stream, mhc_batch** out);
 int mhc_batch_destroy(mhc_batch* b);
 void* mhc_batch_stream(mhc_batch* b);
 /* add a case (device state allocated, not yet initialised); iteration_limit
@@ -304,7 +307,9 @@ enum { MHC_REQ_QUEUED = 0, MHC_REQ_RUNNING = 1, MHC_REQ_DONE = 2, MHC_REQ_FAILED
 int mhc_server_create(long long hbm_budget_bytes, mhc_server** out);
 int mhc_server_destroy(mhc_server* s);
 /* requests are served by size class (cells < 3e4, < 1e6, larger), each a
- * batch on its own stream; stream of class cls (0..2) */
+ * batch on its own stream; the larger the class, the higher its stream's
+ * priority, so a large request is not slowed by small ones sharing the
+ * GPU; stream of class cls (0..2) */
 void* mhc_server_stream(mhc_server* s, int cls);
 /* kernels the server has put on the GPU so far */
 long long mhc_server_launches(mhc_server* s);

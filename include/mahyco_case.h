@@ -68,7 +68,9 @@ enum mhc_case_model {
   MHC_CASE_SOD = 1,       /* casTest/SOD/SODService.cc */
   MHC_CASE_SEDOV = 2,     /* casTest/SEDOV/SEDOVService.cc */
   MHC_CASE_TWO_STATE = 3, /* explicit left/right states (seeded batch cases) */
-  MHC_CASE_ONECELL = 4    /* casTest/ONECELL/ONECELLService.cc: one uniform environment */
+  MHC_CASE_ONECELL = 4,   /* casTest/ONECELL/ONECELLService.cc: one uniform environment */
+  MHC_CASE_BUBBLES = 5    /* casTest/CHOCBULLE/CHOCBULLEService.cc: a lattice of bubbles of
+                             environment 1 in environment 0 (mixed boundary cells) */
 };
 
 /* cas-test ids used by SOD and SEDOV (TypesMahyco.h:44-94) */
@@ -175,6 +177,18 @@ typedef struct mhc_case_params {
   int projection_pente_borne_mixte;     /* projection-pente-borne-mixte: pure-neighbourhood fluxes */
   int projection_limiteur_pure_id;      /* projection-limiteur-pure-id: limiter of pure neighbourhoods */
   int conservation_energie_totale;      /* conservation-energie-totale: kinetic energy lost by the remap back to internal energy */
+  /* BUBBLES case model (the bubble lattice of CHOCBULLE's cas-model
+   * options): nombre-bulles-x/-y/-z, position-premiere-bulle,
+   * deltax/deltay/deltaz-bulle, rayon-bulle.  A cell whose centre lies within
+   * the radius of a bubble centre in the (x, y) plane belongs to the bubble
+   * (environment 1; cylinders along z in 3D); it is mixed, with the bubble's
+   * volume fraction (radius - dmin) / (dmax - dmin), when its nodes' (x, y)
+   * distances to that centre range over [dmin, dmax] around the radius.
+   * Environment 0 elsewhere. */
+  int bubbles_n[3];
+  double bubbles_first[3];
+  double bubbles_delta[3];
+  double bubbles_radius;
 } mhc_case_params;
 
 #ifdef __cplusplus

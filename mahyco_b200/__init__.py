@@ -110,6 +110,7 @@ _SIGS = {
                                    C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     # field upload and the per-method service surface (IEquationOfState, IRemap)
     "mhc_case_params_default": (None, [C.POINTER(CaseParams)]),
+    "mhc_batch_create_on_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "mhc_set_field": (C.c_longlong, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_longlong]),
     "mhc_eos_init": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_eos_reinit": (C.c_int, [C.c_void_p, C.c_int]),

@@ -21,8 +21,8 @@ EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
 BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4, "Density": 5,
               "Energy": 6, "SuperGaussianEnergy": 7, "Pressure": 8}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
-CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL = 1, 2, 3, 4
-CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL}
+CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES = 1, 2, 3, 4, 5
+CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL, "CHOCBULLE": CASE_BUBBLES}
 LENGTHS = {"racine-cubique-volume": 0, "faces-opposees": 1, "monodimX": 2,
            "monodimY": 3, "monodimZ": 4}
 MINMOD, SUPERBEE, VANLEER = 0, 1, 2
@@ -83,6 +83,8 @@ class CaseParams(C.Structure):
         ("projection_pente_borne", C.c_int), ("projection_pente_borne_debar_fix", C.c_int),
         ("projection_pente_borne_mixte", C.c_int), ("projection_limiteur_pure_id", C.c_int),
         ("conservation_energie_totale", C.c_int),
+        ("bubbles_n", C.c_int * 3), ("bubbles_first", C.c_double * 3), ("bubbles_delta", C.c_double * 3),
+        ("bubbles_radius", C.c_double),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -280,6 +282,15 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     cm = m.find("cas-model")
     p.cas_model = CASE_BY_NAME[cm.get("name")]
     p.cas_test = _txt(cm, "cas-test", 0, int)
+    if p.cas_model == CASE_BUBBLES:
+        # the lattice of CHOCBULLE (src/casTest/CHOCBULLE/CHOCBULLE.axl:180-202);
+        # its random and file-read bubbles and fictitious regions are not read
+        if _txt(cm, "nombre-bulles-aleatoires", 0, int) or cm.find("fichier-bulles") is not None:
+            raise NotImplementedError("CHOCBULLE: random or file-read bubbles")
+        p.bubbles_n[:] = [_txt(cm, f"nombre-bulles-{a}", 1 if a == "z" else 0, int) for a in "xyz"]
+        p.bubbles_first[:] = [float(v) for v in _txt(cm, "position-premiere-bulle", "0. 0. 0.", str).split()]
+        p.bubbles_delta[:] = [_txt(cm, f"delta{a}-bulle", 0.0) for a in "xyz"]
+        p.bubbles_radius = _txt(cm, "rayon-bulle", 0.0)
     rm = m.find("remap")
     if rm is not None:
         if rm.get("name", "RemapADI") != "RemapADI":

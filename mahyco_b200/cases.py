@@ -9,13 +9,15 @@ reference datasets (``NONREGRESSION/CAS_*``) at any size:
   states and interface position (the batched workload)
 * ``water_air``  -- stiffened-gas / perfect-gas two-material shock tube
 * ``mie_gruneisen_plate`` -- two Mie-Gruneisen states, explicit pressure
+* ``water_bubbles`` -- CHOCBULLE-like lattice of air bubbles in stiffened-gas
+  water hit by the shock reflected from a wall
 """
 from __future__ import annotations
 
 import math
 import random
 
-from .case import (ARITHMETIC_G, CASE_ONECELL, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, DEPOT_CONSTANT,
+from .case import (ARITHMETIC_G, CASE_BUBBLES, CASE_ONECELL, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, DEPOT_CONSTANT,
                    DEPOT_SUPER_GAUSSIAN, EOS_MIE_GRUNEISEN, EULER_X, EULER_Y, EULER_Z,
                    EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
                    ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults,
@@ -150,6 +152,36 @@ def water_air(dim=2, n=(80, 8), L=(1.0, 0.1), limiter=SUPERBEE, remap=True, delt
     return p
 
 
+def water_bubbles(dim=2, n=(80, 40), L=(1.0, 0.5), bubbles=(3, 2), first=(0.55, 0.15), delta=(0.12, 0.2),
+                  radius=0.04, velocity=50.0, limiter=SUPERBEE, remap=True, deltat_init=1e-7) -> CaseParams:
+    """CHOCBULLE-like (src/casTest/CHOCBULLE/CHOCBULLEService.cc): a lattice
+    of perfect-gas air bubbles (gamma 1.4, rho 1, environment 1) in
+    stiffened-gas water (gamma 4.4, p_inf 6e8, rho 1000, environment 0):
+    density ratio 1000:1.  The water moves at `velocity` towards the wall
+    x = L_x, from which a shock runs back over the bubbles; cylinders along z
+    in 3D."""
+    p = default_params()
+    _mesh(p, dim, n, L)
+    p.nb_env = 2
+    env_defaults(p.env[0], EOS_STIFFENED_GAS)
+    env_defaults(p.env[1], EOS_PERFECT_GAS)
+    p.env[0].adiabatic_cst, p.env[0].limit_tension = 4.4, 6.0e8
+    p.env[0].densite_initiale, p.env[0].pression_initiale = 1000.0, 1.0e5
+    p.env[0].vitesse_initiale[:] = (velocity, 0.0, 0.0)
+    p.env[1].adiabatic_cst = 1.4
+    p.env[1].densite_initiale, p.env[1].pression_initiale = 1.0, 1.0e5
+    p.cas_model = CASE_BUBBLES
+    p.bubbles_n[:] = (bubbles[0], bubbles[1], 1)
+    p.bubbles_first[:] = (first[0], first[1], 0.0)
+    p.bubbles_delta[:] = (delta[0], delta[1], 0.0)
+    p.bubbles_radius = radius
+    p.with_projection = 1 if remap else 0
+    p.projection_limiteur_id = limiter
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.3, deltat_init, 1e-14, 1e-4
+    symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
+    return p
+
+
 def mie_gruneisen_plate(dim=2, n=(80, 8), L=(0.01, 0.001), remap=False, deltat_init=1e-10) -> CaseParams:
     """Aluminium-like Mie-Gruneisen material (rho0 2710, c0 5328, s1 1.338,
     Gamma0 2.0) compressed on one side; explicit pressure update as in
@@ -271,15 +303,15 @@ def serving_request(kind: str, cells: int) -> CaseParams:
     if kind == "bisod3d":
         m = max(2, int(round((cells / 4) ** (1 / 3))))
         return sod(dim=3, n=(4 * m, m, m), L=(1.0, 0.25, 0.25), bi=True, limiter=SUPERBEE)
-    if kind == "water_air":
-        m = max(2, int(round((cells / 10) ** 0.5)))
-        return water_air(dim=2, n=(10 * m, m), L=(1.0, 0.1))
+    if kind == "water_bubbles":
+        m = max(4, int(round((cells / 2) ** 0.5)))
+        return water_bubbles(dim=2, n=(2 * m, m), L=(1.0, 0.5))
     if kind == "bar":
         return bar_impact()
     raise ValueError(kind)
 
 
-SERVING_KINDS = ("sedov2d", "sedov3d", "bisod3d", "water_air", "bar")
+SERVING_KINDS = ("sedov2d", "sedov3d", "bisod3d", "water_bubbles", "bar")
 
 
 def workload(name: str, scale: float = 1.0) -> CaseParams:
@@ -322,6 +354,10 @@ PARITY_CASES = {
     "adi2d_bisod_order1": (lambda: _order1(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True,
                                                deltat_init=1e-3)), 80),
     "adi2d_water_air": (lambda: water_air(deltat_init=1e-6), 80),
+    # CHOCBULLE-like bubble lattice: mixed boundary cells with fractional
+    # volume and mass fractions from the initialisation on
+    "adi2d_water_bubbles": (lambda: water_bubbles(n=(40, 20)), 80),
+    "adi3d_water_bubbles_z": (lambda: water_bubbles(dim=3, n=(24, 12, 4), L=(1.0, 0.5, 0.1)), 40),
     "lag2d_mie_gruneisen": (lambda: mie_gruneisen_plate(deltat_init=1e-8), 100),
     "lag2d_bar_impact": (lambda: bar_impact(n=(8, 40), L=(0.01, 0.05)), 80),
     "lag2d_bar_impact_rot2": (lambda: _rot2(bar_impact(n=(10, 30), L=(0.01, 0.03), velocity=400.0)), 80),

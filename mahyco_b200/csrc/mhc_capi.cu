@@ -454,7 +454,10 @@ int validate(const mhc_case_params* p) {
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with a per-axis Euler remap");
   if (cellvars && p->with_newton)
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with the Newton energy update");
-  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_ONECELL) return set_err(MHC_ERR_ARG, "cas-model");
+  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_BUBBLES) return set_err(MHC_ERR_ARG, "cas-model");
+  if (p->cas_model == MHC_CASE_BUBBLES && (p->nb_env != 2 || p->bubbles_n[0] < 0 || p->bubbles_n[1] < 0 ||
+                                           p->bubbles_n[2] < 0 || !(p->bubbles_radius >= 0.)))
+    return set_err(MHC_ERR_ARG, "bubble lattice: two environments, counts >= 0, radius >= 0");
   if (p->ordre_projection < 1 || p->ordre_projection > 3)
     return set_err(MHC_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
   if (p->projection_limiteur_id < 0 || p->projection_limiteur_id > 7)
@@ -1140,6 +1143,15 @@ int mhc_batch_create(mhc_batch** out) {
   if (!out) return set_err(MHC_ERR_ARG, "null argument");
   mhc_batch* b = new mhc_batch();
   int r = engine_create(nullptr, &b->e);
+  if (r) { delete b; return r; }
+  *out = b;
+  return MHC_OK;
+}
+
+int mhc_batch_create_on_stream(void* stream, mhc_batch** out) {
+  if (!out || !stream) return set_err(MHC_ERR_ARG, "null argument");
+  mhc_batch* b = new mhc_batch();
+  int r = engine_create(static_cast<cudaStream_t>(stream), &b->e);
   if (r) { delete b; return r; }
   *out = b;
   return MHC_OK;

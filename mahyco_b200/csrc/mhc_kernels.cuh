@@ -414,6 +414,42 @@ __device__ __forceinline__ bool node_on_surface(const Mesh& M, int i, int j, int
 // ---------------------------------------------------------------------------
 constexpr int CT = 256;  // threads of the one-dimensional cell / node kernels
 
+// BUBBLES (CHOCBULLEService::initMat / initVar, the bubble lattice): the
+// material of a cell from its centre cc and node coordinates -- 0 the
+// medium, 1 a bubble, 0.5 a mixed cell whose bubble volume fraction is
+// returned in fbub.  Bubbles are visited x, then y, then z, later ones
+// overriding earlier ones; distances are taken in the (x, y) plane.
+template <int DIM>
+__device__ __forceinline__ double bubble_material(const mhc_case_params& P, const R3& cc, const R3* coord,
+                                                  double& fbub) {
+  double mat = 0.;
+  fbub = 0.;
+  const int nz = DIM == 3 ? P.bubbles_n[2] : 1;
+  for (int bx = 0; bx < P.bubbles_n[0]; ++bx)
+    for (int by = 0; by < P.bubbles_n[1]; ++by)
+      for (int bz = 0; bz < nz; ++bz) {
+        const double xb = P.bubbles_first[0] + bx * P.bubbles_delta[0];
+        const double yb = P.bubbles_first[1] + by * P.bubbles_delta[1];
+        const double rb = P.bubbles_radius;
+        const double x = cc.x - xb, y = cc.y - yb;
+        if (!(sqrt(x * x + y * y) <= rb)) continue;
+        mat = 1.;
+        fbub = 0.;
+        double rmin = 1.e300, rmax = 0.;
+        for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+          const double xn = coord[l].x - xb, yn = coord[l].y - yb;
+          const double rn = sqrt(xn * xn + yn * yn);
+          rmin = smin(rn, rmin);
+          rmax = smax(rn, rmax);
+        }
+        if (rmin < rb && rmax > rb) {
+          mat = 0.5;
+          fbub = (rb - rmin) / (rmax - rmin);
+        }
+      }
+  return mat;
+}
+
 template <int DIM, int NE>
 __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   long long c = bx * (long long)CT + threadIdx.x;
@@ -448,6 +484,8 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
     }
     mat = center ? 1. : 0.;
   }
+  double fbub = 0.;  // BUBBLES: the bubble's volume fraction of a mixed cell
+  if (P.cas_model == MHC_CASE_BUBBLES && NE > 1) mat = bubble_material<DIM>(P, cc, coord, fbub);
   uint8_t mask;
   if (mat == 0.) mask = 1;
   else if (mat > 0. && mat < 1.) mask = 3;
@@ -487,6 +525,16 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
     int st = (comp(cc, P.interface_dir) < P.interface_pos) ? 0 : 1;
     rho = P.env[st].densite_initiale;
     p = P.env[st].pression_initiale;
+  } else if (P.cas_model == MHC_CASE_BUBBLES) {
+    // pure cells: their environment's initial state; mixed cells: both
+    // environments' initial states, the cell values are their mixture
+    const int st = mat == 1. ? 1 : 0;
+    rho = P.env[st].densite_initiale;
+    p = P.env[st].pression_initiale;
+    if (!pure) {
+      rho = p = 0.;
+      for (int q = 0; q < 2; ++q) { rhoe[q] = P.env[q].densite_initiale; pe[q] = P.env[q].pression_initiale; }
+    }
   } else if (P.cas_model == MHC_CASE_ONECELL) {
     // ONECELLService::initVarMono: the first environment's state everywhere
     rho = P.env[0].densite_initiale;
@@ -516,6 +564,15 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   }
   double fe[NE], mfe[NE];
   for (int q = 0; q < NE; ++q) { fe[q] = 1.0; mfe[q] = 1.0; }
+  if (P.cas_model == MHC_CASE_BUBBLES && !pure) {
+    // volume fractions of the bubble (environment 1) and the medium, mass
+    // fractions f rho / sum of f rho
+    fe[0] = 1. - fbub;
+    fe[1] = fbub;
+    double rm = 0.;
+    for (int q = 0; q < 2; ++q) rm += rhoe[q] * fe[q];
+    for (int q = 0; q < 2; ++q) mfe[q] = (rhoe[q] * fe[q]) / rm;
+  }
   if (!pure) {
     e = 0.;
     for (int q = 0; q < NE; ++q) {
@@ -575,7 +632,7 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
   R3 x = node_x0(M, i, j, k);
   F.Xp[0][n] = x.x; F.Xp[1][n] = x.y; F.Xp[2][n] = x.z;
   double vx = 0., vy = 0., vz = 0.;
-  if (P.cas_model == MHC_CASE_SOD || P.cas_model == MHC_CASE_TWO_STATE) {
+  if (P.cas_model == MHC_CASE_SOD || P.cas_model == MHC_CASE_TWO_STATE || P.cas_model == MHC_CASE_BUBBLES) {
     vx = P.env[0].vitesse_initiale[0]; vy = P.env[0].vitesse_initiale[1]; vz = P.env[0].vitesse_initiale[2];
   }
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;

@@ -16,7 +16,7 @@
 // large one's pace.  Each step gives every class the number of cycles that
 // takes about as long as the slowest class's `cycles` (estimated from the
 // launches and cells per cycle), and the classes' streams overlap on the
-// GPU.  A class advances a bounded number of cells at once (one large case,
+// GPU, the larger class at the higher stream priority.  A class advances a bounded number of cells at once (one large case,
 // about two large cases' worth of medium ones, any number of small ones):
 // cases that already fill the GPU gain nothing from sharing it.  Requests never change each other's arithmetic: each case's results
 // are the same alone and in any mix.
@@ -70,6 +70,7 @@ double now_s(std::chrono::steady_clock::time_point t0) {
 
 struct mhc_server {
   mhc_batch* batch[kClasses] = {nullptr, nullptr, nullptr};
+  cudaStream_t stream[kClasses] = {nullptr, nullptr, nullptr};
   long long budget = 0;
   long long in_use = 0;
   int max_bypass = 64;        // admissions allowed past a blocked queue head
@@ -89,8 +90,18 @@ struct mhc_server {
 int mhc_server_create(long long hbm_budget_bytes, mhc_server** out) {
   if (!out) return MHC_ERR_ARG;
   mhc_server* s = new mhc_server();
+  // stream priorities: the large class first (its requests are the tail of
+  // the latency distribution and already fill the GPU), the small class last
+  // (its blocks fill whatever the others leave)
+  int lo = 0, hi = 0;
+  if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) { delete s; return MHC_ERR_CUDA; }
   for (int c = 0; c < kClasses; ++c) {
-    int r = mhc_batch_create(&s->batch[c]);
+    const int prio = c == kClasses - 1 ? hi : (c == 0 ? lo : (lo + hi) / 2);
+    if (cudaStreamCreateWithPriority(&s->stream[c], cudaStreamNonBlocking, prio) != cudaSuccess) {
+      mhc_server_destroy(s);
+      return MHC_ERR_CUDA;
+    }
+    int r = mhc_batch_create_on_stream(s->stream[c], &s->batch[c]);
     if (r) { mhc_server_destroy(s); return r; }
   }
   if (hbm_budget_bytes <= 0) {
@@ -106,7 +117,10 @@ int mhc_server_create(long long hbm_budget_bytes, mhc_server** out) {
 
 int mhc_server_destroy(mhc_server* s) {
   if (!s) return MHC_OK;
-  for (int c = 0; c < kClasses; ++c) mhc_batch_destroy(s->batch[c]);
+  for (int c = 0; c < kClasses; ++c) {
+    mhc_batch_destroy(s->batch[c]);
+    if (s->stream[c]) cudaStreamDestroy(s->stream[c]);
+  }
   delete s;
   return MHC_OK;
 }

@@ -478,6 +478,45 @@ static void cell_centres(Case& C) {
   }
 }
 
+/* CHOCBULLEService::initMat / initVar, the bubble lattice
+ * (src/casTest/CHOCBULLE/CHOCBULLEService.cc:22-95, 200-290): material of
+ * cell c (0 medium, 1 bubble, 0.5 mixed) and the bubble's volume fraction of
+ * a mixed cell.  Bubbles in x, y, z order, later ones overriding; distances
+ * in the (x, y) plane.  The node distances that decide a mixed cell are
+ * taken from the bubble's centre and per cell (the reference measures them
+ * from the origin and keeps the extremes across cells, which only agrees
+ * for a bubble at the origin). */
+static double bubble_material(const Case& C, long c, double& fbub) {
+  const mhc_case_params& P = C.P;
+  double mat = 0.;
+  fbub = 0.;
+  const int nz = C.dim == 3 ? P.bubbles_n[2] : 1;
+  for (int bx = 0; bx < P.bubbles_n[0]; ++bx)
+    for (int by = 0; by < P.bubbles_n[1]; ++by)
+      for (int bz = 0; bz < nz; ++bz) {
+        const double xb = P.bubbles_first[0] + bx * P.bubbles_delta[0];
+        const double yb = P.bubbles_first[1] + by * P.bubbles_delta[1];
+        const double rb = P.bubbles_radius;
+        const double x = C.cell_coord[c].x - xb, y = C.cell_coord[c].y - yb;
+        if (!(std::sqrt(x * x + y * y) <= rb)) continue;
+        mat = 1.;
+        fbub = 0.;
+        double rmin = 1.e300, rmax = 0.;
+        for (int l = 0; l < C.nbn; ++l) {
+          const R3& xn = C.coord[C.cnode(c, l)];
+          const double dx = xn.x - xb, dy = xn.y - yb;
+          const double rn = std::sqrt(dx * dx + dy * dy);
+          rmin = (rn < rmin) ? rn : rmin;
+          rmax = (rmax < rn) ? rn : rmax;
+        }
+        if (rmin < rb && rmax > rb) {
+          mat = 0.5;
+          fbub = (rb - rmin) / (rmax - rmin);
+        }
+      }
+  return mat;
+}
+
 /* SODService::initMat / SEDOVService::initMat and the environment sort of
  * MahycoModule::hydroStartInitEnvAndMat (MahycoAnnexe.cc:86-139) */
 static void init_materials(Case& C) {
@@ -503,6 +542,9 @@ static void init_materials(Case& C) {
         if (std::sqrt(x.x * x.x + x.y * x.y + x.z * x.z) < 1.e-10) center = true;
       }
       m = center ? 1. : 0.;
+    } else if (P.cas_model == MHC_CASE_BUBBLES && C.nenv > 1) {
+      double f;
+      m = bubble_material(C, c, f);
     }
     C.materiau[c] = m;
     uint8_t mask = 0;
@@ -553,6 +595,32 @@ static void init_variables(Case& C) {
     }
     // every node starts at the velocity of the first environment (zero in
     // the shock tubes, the impact velocity of a projectile)
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
+  } else if (P.cas_model == MHC_CASE_BUBBLES) {
+    /* pure cells: their environment's initial state; mixed cells: both
+     * environments' states, volume fractions (1 - f, f), mass fractions
+     * f rho / sum of f rho; the cell values are summed from them at the end
+     * of the initialisation */
+    for (long c = 0; c < C.ncell; ++c) {
+      double f;
+      const double m = bubble_material(C, c, f);
+      const int s = m == 1. ? 1 : 0;
+      C.density.g[c] = P.env[s].densite_initiale;
+      C.pressure.g[c] = P.env[s].pression_initiale;
+      if (!C.pure(c)) {
+        C.density.g[c] = C.pressure.g[c] = 0.;
+        C.EV(C.fracvol, 0, c) = 1. - f;
+        C.EV(C.fracvol, 1, c) = f;
+        double rm = 0.;
+        for (int e = 0; e < 2; ++e) {
+          C.EV(C.density, e, c) = P.env[e].densite_initiale;
+          C.EV(C.pressure, e, c) = P.env[e].pression_initiale;
+          rm += C.EV(C.density, e, c) * C.EV(C.fracvol, e, c);
+        }
+        for (int e = 0; e < 2; ++e)
+          C.EV(C.mass_fraction, e, c) = (C.EV(C.density, e, c) * C.EV(C.fracvol, e, c)) / rm;
+      }
+    }
     for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
   } else if (P.cas_model == MHC_CASE_ONECELL) {
     /* ONECELLService::initVarMono: the first environment's state everywhere,

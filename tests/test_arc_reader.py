@@ -193,3 +193,25 @@ def test_cell_variable_boundary_conditions(tmp_path):
     assert got == [(5, 0, 2.0, 0.0, [1000.0, 1000.0]), (7, 4, 3.0, 0.0, [1000.0, 0.25]),
                    (8, 3, 4.0, 1e-3, [1000.0, 1000.0])]
     assert [p.bc[i].dependance[1] for i in range(p.nb_bc) if p.bc[i].kind == 7] == [5.0]
+
+
+def test_read_chocbulle_lattice(tmp_path):
+    """The bubble lattice options of CHOCBULLE's cas-model
+    (src/casTest/CHOCBULLE/CHOCBULLE.axl:180-202) fill the BUBBLES case."""
+    from mahyco_b200.case import CASE_BUBBLES
+    text = open(ARC).read()
+    start, end = text.index("<cas-model"), text.index("</cas-model>") + len("</cas-model>")
+    block = ("<cas-model name=\"CHOCBULLE\"><cas-test>47</cas-test>"
+             "<nombre-bulles-x>2</nombre-bulles-x><nombre-bulles-y>3</nombre-bulles-y>"
+             "<position-premiere-bulle>0.3 0.1 0.0</position-premiere-bulle>"
+             "<deltax-bulle>0.1</deltax-bulle><deltay-bulle>0.05</deltay-bulle>"
+             "<rayon-bulle>0.02</rayon-bulle><nombre-bulles-aleatoires>0</nombre-bulles-aleatoires></cas-model>")
+    f = tmp_path / "bulles.arc"
+    f.write_text(text[:start] + block + text[end:])
+    p, _ = read_arc(str(f))
+    assert p.cas_model == CASE_BUBBLES and p.cas_test == 47
+    assert list(p.bubbles_n) == [2, 3, 1] and list(p.bubbles_first) == [0.3, 0.1, 0.0]
+    assert list(p.bubbles_delta) == [0.1, 0.05, 0.0] and p.bubbles_radius == 0.02
+    f.write_text(text[:start] + block.replace("<nombre-bulles-aleatoires>0", "<nombre-bulles-aleatoires>4") + text[end:])
+    with pytest.raises(NotImplementedError):
+        read_arc(str(f))
