@@ -620,13 +620,11 @@ def run_serve(args):
                 continue
             srv.step(args.cycles_per_step)
             now = time.perf_counter() - t0
-            for tk, i in list(tickets.items()):
-                if i in done_at:
-                    continue
+            for tk in srv.take_completed():
+                i = tickets[tk]
                 st = srv.poll(tk)
-                if st["state"] in (mb.REQ_DONE, mb.REQ_FAILED):
-                    done_at[i] = (now, st["state"], st["status"])
-                    srv.release(tk)
+                done_at[i] = (now, st["state"], st["status"])
+                srv.release(tk)
     launches = srv.launches - l0
     srv.close()
     makespan = max(d[0] for d in done_at.values()) - arrivals[0]

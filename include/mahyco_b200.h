@@ -288,6 +288,14 @@ int mhc_batch_restore(mhc_batch* b, int index, const void* host, long long size)
 /* iteration done, status flags and time of every case index (removed: -1),
  * read with one gather kernel and one copy; returns the number of indices */
 int mhc_batch_poll(mhc_batch* b, int capacity, long long* iteration, int* status, double* time);
+/* the same without waiting: mhc_batch_poll_request enqueues the gather and
+ * the copy after the work already on the batch stream and returns a request
+ * id (0 or 1, alternating; two may be outstanding); mhc_batch_poll_wait
+ * waits for that copy and fills the arrays as mhc_batch_poll does (cases
+ * added after the request: iteration 0, status 0).  A host can enqueue the
+ * next cycles, then read the previous status while they run. */
+int mhc_batch_poll_request(mhc_batch* b);
+int mhc_batch_poll_wait(mhc_batch* b, int request, int capacity, long long* iteration, int* status, double* time);
 
 /* --- serving: continuous batching under an HBM budget --------------------
  * No counterpart in the reference (one case per process there).  Requests
@@ -315,8 +323,16 @@ void* mhc_server_stream(mhc_server* s, int cls);
 long long mhc_server_launches(mhc_server* s);
 /* timeout_s <= 0: no deadline */
 int mhc_server_submit(mhc_server* s, const mhc_case_params* p, long long iterations, double timeout_s, long long* ticket);
-/* returns the number of requests that completed (done or failed) in this step */
+/* admits what fits, enqueues `cycles` iterations (per class, see above)
+ * and a status read of every class, then waits for the previous step's
+ * status read -- the GPU runs this step while the host retires the
+ * requests that finished in the previous one; returns the number of
+ * requests that completed (done or failed), whose tickets
+ * mhc_server_take_completed hands out */
 int mhc_server_step(mhc_server* s, int cycles);
+/* tickets of the requests completed since the last call (at most capacity;
+ * returns how many were written) */
+int mhc_server_take_completed(mhc_server* s, long long* tickets, int capacity);
 int mhc_server_poll(mhc_server* s, long long ticket, int* state, int* status, long long* iteration, double* time);
 /* host clock (seconds since server creation) of submission, admission, completion (-1: not yet) */
 int mhc_server_times(mhc_server* s, long long ticket, double* submit, double* admit, double* done);

@@ -111,6 +111,10 @@ _SIGS = {
     # field upload and the per-method service surface (IEquationOfState, IRemap)
     "mhc_case_params_default": (None, [C.POINTER(CaseParams)]),
     "mhc_batch_create_on_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mhc_batch_poll_request": (C.c_int, [C.c_void_p]),
+    "mhc_batch_poll_wait": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_double)]),
+    "mhc_server_take_completed": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]),
     "mhc_set_field": (C.c_longlong, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_longlong]),
     "mhc_eos_init": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_eos_reinit": (C.c_int, [C.c_void_p, C.c_int]),
@@ -522,6 +526,12 @@ class Server:
 
     def step(self, cycles: int = 1) -> int:
         return _check(self.lib, self.lib.mhc_server_step(self.s, int(cycles)), "mhc_server_step")
+
+    def take_completed(self, capacity: int = 4096) -> list[int]:
+        """Tickets completed since the last call."""
+        buf = (C.c_longlong * capacity)()
+        n = _check(self.lib, self.lib.mhc_server_take_completed(self.s, buf, capacity), "mhc_server_take_completed")
+        return list(buf[:n])
 
     def poll(self, ticket: int) -> dict:
         state, status, it, tm = C.c_int(), C.c_int(), C.c_longlong(), C.c_double()

@@ -33,6 +33,9 @@ int mhc::set_err(int code, const std::string& msg) {
 
 namespace {
 
+int pinned_get(size_t bytes, void** out);
+void pinned_put(void* p, size_t bytes);
+
 bool case_elasto(const mhc_case* h) { return h->P.env[0].elasto_model != 0; }
 bool case_hourglass(const mhc_case* h) { return !h->P.with_projection && h->P.coef_antiderive != 0.; }
 bool case_cell_bcs(const mhc_case* h) {
@@ -64,7 +67,6 @@ int engine_rebuild(Engine* e) {
     desc[i].F = h->F;
     desc[i].P = h->d_params;
   }
-  if (nc) CK(cudaMemcpyAsync(e->d_desc, desc.data(), nc * sizeof(CaseDesc), cudaMemcpyHostToDevice, e->stream));
   // groups
   std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
@@ -125,13 +127,31 @@ int engine_rebuild(Engine* e) {
     e->ints_cap = std::max(ints.size(), 2 * e->ints_cap);
     CK(cudaMallocAsync((void**)&e->d_ints, e->ints_cap * sizeof(int), e->stream));
   }
-  if (!ints.empty())
-    CK(cudaMemcpyAsync(e->d_ints, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, e->stream));
-  // the host vectors must outlive the async copies
-  CK(cudaStreamSynchronize(e->stream));
+  // upload through the page-locked staging block: the copies are truly
+  // asynchronous, so the host does not wait for the work in flight; the
+  // block is reused once the previous upload has landed
+  const size_t db = nc * sizeof(CaseDesc), ib = ints.size() * sizeof(int);
+  if (!e->stage_ev) CK(cudaEventCreateWithFlags(&e->stage_ev, cudaEventDisableTiming));
+  else CK(cudaEventSynchronize(e->stage_ev));
+  if (db + ib > e->stage_cap) {
+    if (e->h_stage) pinned_put(e->h_stage, e->stage_cap);
+    e->h_stage = nullptr;
+    e->stage_cap = std::max(db + ib, 2 * e->stage_cap);
+    if (int pr = pinned_get(e->stage_cap, (void**)&e->h_stage)) return pr;
+  }
+  if (db) {
+    memcpy(e->h_stage, desc.data(), db);
+    CK(cudaMemcpyAsync(e->d_desc, e->h_stage, db, cudaMemcpyHostToDevice, e->stream));
+  }
+  if (ib) {
+    memcpy(e->h_stage + db, ints.data(), ib);
+    CK(cudaMemcpyAsync(e->d_ints, e->h_stage + db, ib, cudaMemcpyHostToDevice, e->stream));
+  }
+  CK(cudaEventRecord(e->stage_ev, e->stream));
   e->dirty = false;
   e->cycles_since_build = 0;
   if (e->graph) {
+    CK(cudaStreamSynchronize(e->stream));  // no replay of the old graph in flight
     cudaGraphExecDestroy(e->graph);
     e->graph = nullptr;
   }
@@ -390,6 +410,9 @@ void engine_release(Engine* e) {
   if (e->d_gather) cudaFreeAsync(e->d_gather, e->stream);
   if (e->h_gather) { cudaStreamSynchronize(e->stream); pinned_put(e->h_gather, e->gather_cap * sizeof(Scalars)); }
   e->d_gather = nullptr; e->h_gather = nullptr; e->gather_cap = 0;
+  if (e->stage_ev) { cudaEventSynchronize(e->stage_ev); cudaEventDestroy(e->stage_ev); }
+  if (e->h_stage) pinned_put(e->h_stage, e->stage_cap);
+  e->stage_ev = nullptr; e->h_stage = nullptr; e->stage_cap = 0;
   e->graph = nullptr; e->d_desc = nullptr; e->desc_cap = 0; e->d_ints = nullptr; e->ints_cap = 0;
   e->ev[0] = e->ev[1] = nullptr;
 }
@@ -501,9 +524,13 @@ void case_free(mhc_case* h) {
     if (h->scal_ev[i]) { cudaEventDestroy(h->scal_ev[i]); h->scal_ev[i] = nullptr; }
   if (h->solo) { engine_destroy(h->solo); h->solo = nullptr; }
   if (h->stream) {
+    // stream-ordered frees: the work already queued that reads the case
+    // runs first; only a private stream is waited for, before it goes
     for (void* p : h->allocs) cudaFreeAsync(p, h->stream);
-    cudaStreamSynchronize(h->stream);
-    if (h->own_stream) cudaStreamDestroy(h->stream);
+    if (h->own_stream) {
+      cudaStreamSynchronize(h->stream);
+      cudaStreamDestroy(h->stream);
+    }
   }
   delete h;
 }
@@ -635,9 +662,9 @@ int case_reset_scalars(mhc_case* h, long long iteration_limit) {
   s.iteration = 1;
   s.dt_min_bits = 0x7fefffffffffffffull;
   s.iteration_limit = iteration_limit;
+  // a copy from pageable host memory is staged before the call returns, so
+  // the stack source may go at once (no wait for the work in flight)
   CK(cudaMemcpyAsync(h->d_scal, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
-  // the host copies (scalars, params) must stay valid until the copies ran
-  CK(cudaStreamSynchronize(h->stream));
   h->it_host = 1;
   return MHC_OK;
 }
@@ -1137,7 +1164,37 @@ struct mhc_batch {
   std::vector<mhc_case*> slots;   // case index -> case (nullptr once removed)
   std::vector<char> detached;     // slot kept resident but no longer advanced
   std::vector<Scalars> last;      // scalars read when the slot was detached
+  // asynchronous polls, double-buffered: the gathered scalars of every case,
+  // their page-locked copy, the event after the copy, and the engine index
+  // of every slot when the poll was enqueued (-1: not in that poll)
+  struct Poll {
+    Scalars* d = nullptr;
+    Scalars* h = nullptr;
+    int cap = 0;
+    cudaEvent_t ev = nullptr;
+    bool pending = false;
+    std::vector<int> index;
+  } poll[2];
+  int poll_next = 0;
+  std::vector<Scalars> polled;    // each slot's scalars from the last completed poll
+  std::vector<char> polled_ok;
+  // start-init engines of earlier mhc_batch_init calls, released once their
+  // list upload has landed (their frees are stream-ordered)
+  std::vector<Engine*> init_engines;
 };
+
+// releases the start-init engines whose uploads have landed (all of them,
+// waiting, with wait = true); no stream-wide synchronisation
+void reap_init_engines(mhc_batch* b, bool wait) {
+  std::vector<Engine*> keep;
+  for (Engine* e : b->init_engines) {
+    const bool done = !e->stage_ev || wait || cudaEventQuery(e->stage_ev) == cudaSuccess;
+    if (!done) { keep.push_back(e); continue; }
+    engine_release(e);  // waits on its own upload event only
+    delete e;
+  }
+  b->init_engines.swap(keep);
+}
 
 int mhc_batch_create(mhc_batch** out) {
   if (!out) return set_err(MHC_ERR_ARG, "null argument");
@@ -1160,6 +1217,13 @@ int mhc_batch_create_on_stream(void* stream, mhc_batch** out) {
 int mhc_batch_destroy(mhc_batch* b) {
   if (!b) return MHC_OK;
   cudaStreamSynchronize(b->e->stream);
+  reap_init_engines(b, true);
+  for (mhc_batch::Poll& P : b->poll) {
+    if (P.d) cudaFreeAsync(P.d, b->e->stream);
+    if (P.h) pinned_put(P.h, P.cap * sizeof(Scalars));
+    if (P.ev) cudaEventDestroy(P.ev);
+  }
+  cudaStreamSynchronize(b->e->stream);
   for (mhc_case* h : b->slots) case_free(h);
   engine_destroy(b->e);
   delete b;
@@ -1179,6 +1243,8 @@ int mhc_batch_add(mhc_batch* b, const mhc_case_params* params, long long iterati
   b->slots.push_back(h);
   b->detached.push_back(0);
   b->last.push_back(Scalars{});
+  b->polled.push_back(Scalars{});
+  b->polled_ok.push_back(0);
   b->e->cases.push_back(h);
   b->e->dirty = true;
   return MHC_OK;
@@ -1186,7 +1252,10 @@ int mhc_batch_add(mhc_batch* b, const mhc_case_params* params, long long iterati
 
 int mhc_batch_init(mhc_batch* b) {
   if (!b) return set_err(MHC_ERR_ARG, "null batch");
-  // start-init of the cases that have not run yet, through a temporary engine
+  // start-init of the cases that have not run yet, through a temporary
+  // engine on the batch stream, released later without waiting for the
+  // work in flight
+  reap_init_engines(b, false);
   Engine* tmp = nullptr;
   int r = engine_create(b->e->stream, &tmp);
   if (r) return r;
@@ -1198,7 +1267,7 @@ int mhc_batch_init(mhc_batch* b) {
     for (mhc_case* h : tmp->cases) h->initialised = true;
   }
   cudaError_t ce = cudaGetLastError();
-  engine_destroy(tmp);
+  b->init_engines.push_back(tmp);
   if (ce != cudaSuccess) return set_err(MHC_ERR_CUDA, cudaGetErrorString(ce));
   b->e->dirty = true;
   return MHC_OK;
@@ -1207,11 +1276,10 @@ int mhc_batch_init(mhc_batch* b) {
 int mhc_batch_remove(mhc_batch* b, int index) {
   if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
   mhc_case* h = b->slots[index];
-  cudaStreamSynchronize(b->e->stream);
   auto& v = b->e->cases;
   v.erase(std::remove(v.begin(), v.end(), h), v.end());
   b->e->dirty = true;
-  case_free(h);
+  case_free(h);  // stream-ordered: after the batch's work already queued
   b->slots[index] = nullptr;
   b->detached[index] = 0;
   return MHC_OK;
@@ -1239,8 +1307,16 @@ int mhc_batch_detach(mhc_batch* b, int index) {
   if (!b || index < 0 || index >= (int)b->slots.size() || !b->slots[index]) return set_err(MHC_ERR_ARG, "bad case index");
   if (b->detached[index]) return MHC_OK;
   mhc_case* h = b->slots[index];
-  int r = read_scalars(h, b->e->stream, &b->last[index]);
-  if (r) return r;
+  // a case that a completed poll saw finished (stopped, failed or at its
+  // iteration limit) no longer changes: keep those scalars without waiting
+  // for the work in flight; otherwise read them after it
+  const Scalars& ps = b->polled[index];
+  if (b->polled_ok[index] && (ps.status != 0 || ps.iteration_done >= ps.iteration_limit)) {
+    b->last[index] = ps;
+  } else {
+    int r = read_scalars(h, b->e->stream, &b->last[index]);
+    if (r) return r;
+  }
   auto& v = b->e->cases;
   v.erase(std::remove(v.begin(), v.end(), h), v.end());
   b->e->dirty = true;
@@ -1277,6 +1353,67 @@ int mhc_batch_poll(mhc_batch* b, int capacity, long long* iteration, int* status
     if (iteration) iteration[i] = sc->iteration_done;
     if (status) status[i] = sc->status;
     if (time) time[i] = sc->t_done;
+  }
+  return ns;
+}
+
+int mhc_batch_poll_request(mhc_batch* b) {
+  if (!b) return set_err(MHC_ERR_ARG, "null batch");
+  Engine* e = b->e;
+  int r = engine_rebuild(e);
+  if (r) return r;
+  const int k = b->poll_next;
+  mhc_batch::Poll& P = b->poll[k];
+  if (P.pending) CK(cudaEventSynchronize(P.ev));  // its buffers are about to be reused
+  P.pending = false;
+  const int n = (int)e->cases.size();
+  if (!P.ev) CK(cudaEventCreateWithFlags(&P.ev, cudaEventDisableTiming));
+  if (n > P.cap) {
+    if (P.d) CK(cudaFreeAsync(P.d, e->stream));
+    if (P.h) pinned_put(P.h, P.cap * sizeof(Scalars));
+    P.h = nullptr;
+    P.cap = std::max(n, 2 * P.cap);
+    CK(cudaMallocAsync((void**)&P.d, P.cap * sizeof(Scalars), e->stream));
+    if ((r = pinned_get(P.cap * sizeof(Scalars), (void**)&P.h))) return r;
+  }
+  P.index.assign(b->slots.size(), -1);
+  for (size_t i = 0; i < b->slots.size(); ++i)
+    if (b->slots[i] && !b->detached[i]) P.index[i] = b->slots[i]->slot;
+  if (n > 0) {
+    kb_gather_scalars<<<cdiv(n, 128), 128, 0, e->stream>>>(e->d_desc, n, P.d);
+    ++e->launches;
+    CK(cudaMemcpyAsync(P.h, P.d, n * sizeof(Scalars), cudaMemcpyDeviceToHost, e->stream));
+  }
+  CK(cudaEventRecord(P.ev, e->stream));
+  P.pending = true;
+  b->poll_next ^= 1;
+  return k;
+}
+
+int mhc_batch_poll_wait(mhc_batch* b, int request, int capacity, long long* iteration, int* status, double* time) {
+  if (!b || request < 0 || request > 1 || capacity < 0) return set_err(MHC_ERR_ARG, "bad argument");
+  mhc_batch::Poll& P = b->poll[request];
+  if (!P.pending) return set_err(MHC_ERR_ORDER, "no poll pending under this request");
+  CK(cudaEventSynchronize(P.ev));
+  P.pending = false;
+  const int ns = (int)b->slots.size();
+  for (int i = 0; i < ns; ++i) {
+    const int idx = i < (int)P.index.size() ? P.index[i] : -1;
+    const Scalars* sc = nullptr;
+    if (b->slots[i] && b->detached[i]) sc = &b->last[i];
+    else if (b->slots[i] && idx >= 0) {
+      sc = &P.h[idx];
+      b->polled[i] = *sc;
+      b->polled_ok[i] = 1;
+    }
+    if (i >= capacity) continue;
+    if (!b->slots[i]) { if (iteration) iteration[i] = -1; if (status) status[i] = -1; if (time) time[i] = 0.; }
+    else if (!sc) { if (iteration) iteration[i] = 0; if (status) status[i] = 0; if (time) time[i] = 0.; }  // added after the poll
+    else {
+      if (iteration) iteration[i] = sc->iteration_done;
+      if (status) status[i] = sc->status;
+      if (time) time[i] = sc->t_done;
+    }
   }
   return ns;
 }

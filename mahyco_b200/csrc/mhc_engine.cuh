@@ -113,6 +113,12 @@ struct Engine {
   // kernels this engine put on the GPU (graph replays count their nodes)
   long long launches = 0;
   long long graph_launches = 0;  // kernel nodes of the captured graph
+  // page-locked staging of the launch lists (case descriptors, then the
+  // int arena) and the event after their last upload, so that a rebuild
+  // does not wait for the work in flight
+  char* h_stage = nullptr;
+  size_t stage_cap = 0;
+  cudaEvent_t stage_ev = nullptr;
   // status gather of every case (one kernel + one copy)
   Scalars* d_gather = nullptr;
   Scalars* h_gather = nullptr;   // pinned

@@ -81,9 +81,8 @@ struct mhc_server {
   std::vector<long long> running;                  // tickets on the GPU
   std::unordered_map<long long, Request> reqs;
 
-  std::vector<long long> poll_it;
-  std::vector<int> poll_st;
-  std::vector<double> poll_t;
+  int pending_poll[kClasses] = {-1, -1, -1};       // status read enqueued by the last step, per class
+  std::vector<long long> completed_tickets;        // not yet handed out (mhc_server_take_completed)
   long long completed = 0;
 };
 
@@ -171,6 +170,7 @@ void finish(mhc_server* s, Request& q, int state, int status, double t) {
   q.status = status;
   q.t_done = t;
   ++s->completed;
+  s->completed_tickets.push_back(q.ticket);
 }
 
 int admit(mhc_server* s) {
@@ -247,10 +247,9 @@ int mhc_server_step(mhc_server* s, int cycles) {
   const long long done0 = s->completed;
   int r = admit(s);
   if (r < 0) return r;
-  if (s->running.empty()) return (int)(s->completed - done0);
   // estimated seconds per cycle of each class: launches + streamed cells
   long long cells[kClasses] = {0, 0, 0};
-  int cases[kClasses] = {0, 0, 0}, nslot[kClasses] = {0, 0, 0};
+  int cases[kClasses] = {0, 0, 0}, nslot[kClasses] = {1, 1, 1};
   for (long long tk : s->running) {
     const Request& q = s->reqs[tk];
     cells[q.cls] += q.cells;
@@ -262,30 +261,44 @@ int mhc_server_step(mhc_server* s, int cycles) {
     cost[c] = cases[c] ? 60e-6 + 1.0e-9 * (double)cells[c] : 0.;
     tmax = std::max(tmax, cost[c]);
   }
-  if (cycles > 0)
-    for (int c = 0; c < kClasses; ++c) {
-      if (!cases[c]) continue;
+  // this step's cycles, then a status read of every class behind them
+  int req[kClasses] = {-1, -1, -1};
+  for (int c = 0; c < kClasses; ++c) {
+    if (!cases[c]) continue;
+    if (cycles > 0) {
       const double k = (double)cycles * tmax / cost[c];
       const int kc = (int)std::min((double)(64 * cycles), std::max((double)cycles, k + 0.5));
       if ((r = mhc_batch_cycle(s->batch[c], kc))) return r;
     }
+    if ((req[c] = mhc_batch_poll_request(s->batch[c])) < 0) return req[c];
+  }
+  // while the GPU runs them, the previous step's status: retire what had
+  // finished by then (a case past its iteration limit does not advance, so
+  // its cycles of this step do nothing); with no previous read (first step
+  // after an idle server) this step's own is waited for
   std::vector<long long> pit[kClasses];
   std::vector<int> pst[kClasses];
   std::vector<double> ptm[kClasses];
+  bool have[kClasses] = {false, false, false};
   for (int c = 0; c < kClasses; ++c) {
-    if (!cases[c]) continue;
-    pit[c].resize(nslot[c]);
-    pst[c].resize(nslot[c]);
-    ptm[c].resize(nslot[c]);
-    r = mhc_batch_poll(s->batch[c], nslot[c], pit[c].data(), pst[c].data(), ptm[c].data());
-    if (r < 0) return r;
+    int rq = s->pending_poll[c] >= 0 ? s->pending_poll[c] : req[c];
+    if (rq < 0) continue;
+    const int n = nslot[c];  // the running requests' slots of the class
+    pit[c].resize(n); pst[c].resize(n); ptm[c].resize(n);
+    const int ns = mhc_batch_poll_wait(s->batch[c], rq, n, pit[c].data(), pst[c].data(), ptm[c].data());
+    if (ns < 0) return ns;
+    have[c] = true;
+    if (rq == req[c]) req[c] = -1;  // already consumed
   }
+  for (int c = 0; c < kClasses; ++c) s->pending_poll[c] = req[c];
   const double t = now_s(s->t0);
   std::vector<long long> still;
   for (long long tk : s->running) {
     Request& q = s->reqs[tk];
-    q.iteration = pit[q.cls][q.slot];
-    q.time = ptm[q.cls][q.slot];
+    if (!have[q.cls] || q.slot >= (int)pit[q.cls].size()) { still.push_back(tk); continue; }
+    const long long it = pit[q.cls][q.slot];
+    q.iteration = std::max(q.iteration, it);
+    if (it > 0) q.time = ptm[q.cls][q.slot];
     const int st = pst[q.cls][q.slot];
     const int err = st & ~MHC_ST_STOP;
     bool end = false;
@@ -303,6 +316,14 @@ int mhc_server_step(mhc_server* s, int cycles) {
   }
   s->running.swap(still);
   return (int)(s->completed - done0);
+}
+
+int mhc_server_take_completed(mhc_server* s, long long* tickets, int capacity) {
+  if (!s || (capacity > 0 && !tickets)) return MHC_ERR_ARG;
+  const int n = std::min(capacity, (int)s->completed_tickets.size());
+  for (int i = 0; i < n; ++i) tickets[i] = s->completed_tickets[i];
+  s->completed_tickets.erase(s->completed_tickets.begin(), s->completed_tickets.begin() + n);
+  return n;
 }
 
 int mhc_server_poll(mhc_server* s, long long ticket, int* state, int* status, long long* iteration,

@@ -15,8 +15,8 @@ pytestmark = pytest.mark.gpu
 
 FIELDS = ("Density", "Pressure", "InternalEnergy", "Velocity")
 
-MIX = [("sedov2d", 900, 30), ("bisod3d", 2000, 25), ("water_air", 1000, 40), ("sedov3d", 1000, 20),
-       ("bar", 0, 30), ("sedov2d", 3000, 15), ("bisod3d", 500, 35), ("water_air", 250, 20)]
+MIX = [("sedov2d", 900, 30), ("bisod3d", 2000, 25), ("water_bubbles", 1000, 40), ("sedov3d", 1000, 20),
+       ("bar", 0, 30), ("sedov2d", 3000, 15), ("bisod3d", 500, 35), ("water_bubbles", 250, 20)]
 
 
 def _params(kind, cells):
