@@ -13,7 +13,9 @@
 // Resident cases are split into size classes, each a batch on its own
 // stream: all cases of a batch advance in lockstep (one launch per phase),
 // so a small request sharing a batch with a large one would move at the
-// large one's pace.  Each step gives every class the number of cycles that
+// large one's pace.  A request stops counting against its class's share
+// once all its iterations are enqueued, so the next one is admitted behind
+// it without a gap.  Each step gives every class the number of cycles that
 // takes about as long as the slowest class's `cycles` (estimated from the
 // launches and cells per cycle), and the classes' streams overlap on the
 // GPU, the larger class at the higher stream priority.  A class advances a bounded number of cells at once (one large case,
@@ -52,6 +54,7 @@ struct Request {
   long long cells = 0;
   mhc_case_params P;
   long long iterations = 0;
+  long long enqueued = 0;     // iterations enqueued on the GPU so far
   double timeout_s = 0.;      // 0 = none
   long long bytes = 0;
   int state = MHC_REQ_QUEUED;
@@ -178,9 +181,14 @@ int admit(mhc_server* s) {
   bool touched[kClasses] = {false, false, false};
   long long run_cells[kClasses] = {0, 0, 0};
   int run_cases[kClasses] = {0, 0, 0};
+  // a request holds its class's share until all its iterations are
+  // enqueued: its successor's cycles then queue right behind its last ones
+  // instead of waiting for its completion to be read back
   for (long long tk : s->running) {
-    run_cells[s->reqs[tk].cls] += s->reqs[tk].cells;
-    run_cases[s->reqs[tk].cls] += 1;
+    const Request& q = s->reqs[tk];
+    if (q.enqueued >= q.iterations) continue;
+    run_cells[q.cls] += q.cells;
+    run_cases[q.cls] += 1;
   }
   bool head_blocked = false;
   for (auto it = s->queue.begin(); it != s->queue.end();) {
@@ -248,13 +256,14 @@ int mhc_server_step(mhc_server* s, int cycles) {
   int r = admit(s);
   if (r < 0) return r;
   // estimated seconds per cycle of each class: launches + streamed cells
-  long long cells[kClasses] = {0, 0, 0};
+  long long cells[kClasses] = {0, 0, 0}, remain[kClasses] = {0, 0, 0};
   int cases[kClasses] = {0, 0, 0}, nslot[kClasses] = {1, 1, 1};
   for (long long tk : s->running) {
     const Request& q = s->reqs[tk];
     cells[q.cls] += q.cells;
     cases[q.cls] += 1;
     nslot[q.cls] = std::max(nslot[q.cls], q.slot + 1);
+    remain[q.cls] = std::max(remain[q.cls], q.iterations - q.enqueued);
   }
   double cost[kClasses], tmax = 0.;
   for (int c = 0; c < kClasses; ++c) {
@@ -265,10 +274,17 @@ int mhc_server_step(mhc_server* s, int cycles) {
   int req[kClasses] = {-1, -1, -1};
   for (int c = 0; c < kClasses; ++c) {
     if (!cases[c]) continue;
-    if (cycles > 0) {
+    if (cycles > 0 && remain[c] > 0) {
+      // no more cycles than the class's longest remaining request needs:
+      // cycles past every member's limit would only launch empty kernels
       const double k = (double)cycles * tmax / cost[c];
-      const int kc = (int)std::min((double)(64 * cycles), std::max((double)cycles, k + 0.5));
+      const int kc = (int)std::min((double)remain[c],
+                                   std::min((double)(64 * cycles), std::max((double)cycles, k + 0.5)));
       if ((r = mhc_batch_cycle(s->batch[c], kc))) return r;
+      for (long long tk : s->running) {
+        Request& q = s->reqs[tk];
+        if (q.cls == c) q.enqueued += kc;
+      }
     }
     if ((req[c] = mhc_batch_poll_request(s->batch[c])) < 0) return req[c];
   }
