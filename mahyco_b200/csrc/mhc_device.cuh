@@ -32,8 +32,8 @@ __device__ __forceinline__ double produit(double A, double B, double C, double D
 __device__ __forceinline__ double amin(double a, double b) { return (a < b) ? a : b; }
 __device__ __forceinline__ double amax(double a, double b) { return (a < b) ? b : a; }
 // std::min / std::max
-__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
-__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__host__ __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__host__ __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
 
 // ---------------------------------------------------------------------------
 // correctly rounded powers
@@ -200,9 +200,13 @@ __device__ __forceinline__ double flux_limiter(int id, double r) {
 // the division: 0 / y is exactly +-0 (sign of x xor sign of y) for every y
 // other than 0 and NaN, and such quotients (absent materials, flat fields)
 // would otherwise leave the division's fast path.
-__device__ __forceinline__ double div_rn(double x, double y) {
+__host__ __device__ __forceinline__ double div_rn(double x, double y) {
+#ifdef __CUDA_ARCH__
   if (x == 0.0 && y == y && y != 0.0)
     return ((__double_as_longlong(x) ^ __double_as_longlong(y)) < 0) ? -0.0 : 0.0;
+#else
+  if (x == 0.0 && y == y && y != 0.0) return std::signbit(x) != std::signbit(y) ? -0.0 : 0.0;
+#endif
   return x / y;
 }
 
@@ -254,17 +258,61 @@ __device__ __forceinline__ double generalized_gradient(int id, double gp, double
   return g;
 }
 template <int LIM>
-__device__ __forceinline__ double flux_limiter_t(double r) {
+__host__ __device__ __forceinline__ double flux_limiter_t(double r) {
   if (LIM == 0) return smax(0.0, smin(1.0, r));
   if (LIM == 1) return smax(0.0, smax(smin(2.0 * r, 1.0), smin(r, 2.0)));
   if (LIM == 2) return (r <= 0.0) ? 0.0 : 2.0 * r / (1.0 + r);
   return 0.0;
 }
+// computeAndLimitGradPhi (UtilesRemap.cc:325-357):
+// g = 0.5 phi(gf / gb) gb + 0.5 phi(gb / gf) gf, each term present when its
+// divisor is not zero, phi the flux limiter
 template <int LIM>
-__device__ __forceinline__ double limited_gradient_t(double gb, double gf) {
+__host__ __device__ __forceinline__ double limited_gradient_ref(double gb, double gf) {
   double g = 0.;
   if (gb != 0.) g += 0.5 * (flux_limiter_t<LIM>(div_rn(gf, gb)) * gb);
   if (gf != 0.) g += 0.5 * (flux_limiter_t<LIM>(div_rn(gb, gf)) * gf);
+  return g;
+}
+
+// The same value with one division for minmod and superbee.  With slopes of
+// opposite signs, or a zero one, both limiter values are +0 and each term
+// is a signed zero, so g = +0.  With same-sign slopes, let n be the slope of
+// larger magnitude and d the other: the ratio n / d is >= 1, and comparing
+// |n| with |d| and 2 |d| exactly (doubling is exact) tells which branch of
+// the limiter the correctly rounded ratios fall in (the bounds 1/2, 1 and 2
+// are representable, so rounding never crosses them): minmod gives 1 for
+// n / d and d / n itself for the other; superbee gives n / d (<= 2) and 1,
+// or 2 and 2 d / n (the ratio < 1/2).  Only the ratio the result depends on
+// is divided; the constant term is formed as the reference forms it
+// (0.5 (phi x)), so the sum is bit-identical.  Non-finite slopes take the
+// reference path.
+template <int LIM>
+__host__ __device__ __forceinline__ double limited_gradient_t(double gb, double gf) {
+  if (LIM != 0 && LIM != 1) return limited_gradient_ref<LIM>(gb, gf);
+  const double ab = fabs(gb), af = fabs(gf);
+  if (!(ab <= 1.7976931348623157e308 && af <= 1.7976931348623157e308)) return limited_gradient_ref<LIM>(gb, gf);
+  if (!((gb > 0. && gf > 0.) || (gb < 0. && gf < 0.))) return 0.;
+  const bool fbig = af >= ab;             // the forward slope is n
+  const double n = fbig ? gf : gb, d = fbig ? gb : gf;
+  double tn, td;                          // terms whose limiter argument is n / d, d / n
+  if (LIM == 0) {
+    // minmod: phi(n / d) = 1, phi(d / n) = d / n
+    tn = 0.5 * (1.0 * d);
+    td = 0.5 * (flux_limiter_t<LIM>(div_rn(d, n)) * n);
+  } else if (fabs(n) <= 2.0 * fabs(d)) {
+    // superbee, n / d in [1, 2]: phi(n / d) = n / d, phi(d / n) = 1
+    tn = 0.5 * (flux_limiter_t<LIM>(div_rn(n, d)) * d);
+    td = 0.5 * (1.0 * n);
+  } else {
+    // superbee, n / d > 2: phi(n / d) = 2, phi(d / n) = 2 d / n
+    tn = 0.5 * (2.0 * d);
+    td = 0.5 * (flux_limiter_t<LIM>(div_rn(d, n)) * n);
+  }
+  // the reference adds the term of gf / gb (divisor gb) first
+  double g = 0.;
+  if (fbig) { g += tn; g += td; }
+  else { g += td; g += tn; }
   return g;
 }
 __device__ __forceinline__ double limited_gradient(int id, double gb, double gf) {
