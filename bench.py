@@ -457,11 +457,18 @@ def run_batch(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     lib = mb.load()
-    cases = batch_cases(args.cases)
+    all_cases = batch_cases(args.cases)
+    # N > 1: the cases are shared between the ranks by device bytes (every
+    # case on exactly one GPU; no exchange while they run)
+    from mahyco_b200.partition import partition_by_bytes, gather_results
+    sizes = [lib.mhc_case_device_bytes(ctypes.byref(p)) for p in all_cases]
+    mine = partition_by_bytes(sizes, world)[rank]
+    cases = [all_cases[i] for i in mine]
     tune_cycles = 2 * len(CANDIDATES)
     warm = max(args.warmup, tune_cycles + 4)
     limit = warm + args.steps
     cells = sum(p.ncell for p in cases)
+    total_cells = sum(p.ncell for p in all_cases)
     # -- batched arm
     t_wall0 = time.perf_counter()
     b = mb.Batch(lib)
@@ -486,10 +493,13 @@ def run_batch(args):
     ms = e0.elapsed_time(e1)
     launches = b.launches - l0
     done = [b.scalars(i) for i in idx]
-    t_wall = time.perf_counter() - t_wall0
+    t_wall = max_over_ranks((time.perf_counter() - t_wall0) * 1e3) * 1e-3
     bad = sum(1 for d in done if d["iteration"] != limit)
     ms = max_over_ranks(ms)
-    batched = replica_value(cells * args.steps, world, ms)
+    # whole job: every rank's cells over the slowest rank's device time
+    batched = total_cells * args.steps / (ms * 1e-3)
+    # every case's final (iteration, time) gathered on rank 0
+    gathered = gather_results({mine[j]: (done[j]["iteration"], done[j]["time"]) for j in range(len(mine))}, world)
     # -- plain arm on a seeded sample (every k-th case), device time of the
     # same K cycles per case, plus its per-solve wall latency
     k = max(1, len(cases) // args.plain_sample) if args.plain_sample > 0 else 1
@@ -521,6 +531,11 @@ def run_batch(args):
         h.close()
     b.close()
     plain = plain_cells * args.steps / (plain_ms * 1e-3)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([plain_cells * args.steps, plain_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)  # the sampled plain solves of all ranks (each rank's GPU runs its own)
+        plain = world * float(t[0]) / (float(t[1]) * 1e-3)
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -531,9 +546,11 @@ def run_batch(args):
         "steps": args.steps, "warmup": warm, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOADS["batch2d"][0], "cases": len(cases), "cells": cells,
+        "config": {"workload": WORKLOADS["batch2d"][0], "cases": len(all_cases), "cells": total_cells,
                    "step": "one cycle of every case", "graph": "CUDA graph of 6 cycles",
-                   "l2": "working set > 126 MB L2, no flush", "parallelism": f"replicas x{world}"},
+                   "l2": "working set > 126 MB L2, no flush",
+                   "parallelism": f"cases shared by device bytes over {world} GPU(s)" if world > 1 else "1 GPU",
+                   "cases_gathered": len(gathered) if gathered is not None else None},
         "batched_vs_plain": batched / plain,
         "plain": {"value": plain, "unit": "cell-cycles/s", "sample_cases": len(sample),
                   "sample_cells": plain_cells, "same_results": same, "gpu_launches": plain_launches,
@@ -548,7 +565,7 @@ def run_batch(args):
         "cases_not_at_limit": bad,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
-        "e2e": {"value": world * cells * args.steps / t_wall, "unit": "cell-cycles/s",
+        "e2e": {"value": total_cells * args.steps / t_wall, "unit": "cell-cycles/s",
                 "h2d_bytes_per_step": len(cases) * ctypes.sizeof(cases[0]) / args.steps,
                 "d2h_bytes_per_step": len(cases) * 40 / args.steps,
                 "timer": "host wall clock of the whole batched run: case creation, init, tuning, warm-up, K cycles, status read-back"},
@@ -582,19 +599,29 @@ def run_serve(args):
     import torch
     import mahyco_b200 as mb
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if rank != 0:
-        return  # the served form runs on one GPU; other ranks have nothing to do
+    if world > 1 and not torch.distributed.is_initialized():
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     lib = mb.load()
     its = args.steps
-    reqs = serve_requests(args.requests)
+    all_reqs = serve_requests(args.requests)
     rng = random.Random(11)
-    arrivals, t = [], 0.0
-    for _ in reqs:
+    all_arrivals, t = [], 0.0
+    for _ in all_reqs:
         t += rng.expovariate(args.rate)
-        arrivals.append(t)
+        all_arrivals.append(t)
+    # N > 1: the request stream is shared between the GPUs by device bytes
+    # (each rank serves its requests at their arrival times)
+    import ctypes
+    from mahyco_b200.partition import partition_by_bytes, gather_results
+    mine = partition_by_bytes([lib.mhc_case_device_bytes(ctypes.byref(p)) for _, p in all_reqs], world)[rank]
+    reqs = [all_reqs[i] for i in mine]
+    arrivals = [all_arrivals[i] for i in mine]
     work = sum(p.ncell for _, p in reqs) * its
+    total_work = sum(p.ncell for _, p in all_reqs) * its
     # warm-up: one small solve of every kind through the server (module load,
     # pools, first launches)
     srv = mb.Server()
@@ -605,6 +632,8 @@ def run_serve(args):
         srv.step(3)
     srv.close()
     srv = mb.Server()
+    if world > 1:
+        torch.distributed.barrier()
     t0 = time.perf_counter()
     nxt, tickets, done_at = 0, {}, {}
     l0 = srv.launches
@@ -627,11 +656,14 @@ def run_serve(args):
                 srv.release(tk)
     launches = srv.launches - l0
     srv.close()
-    makespan = max(d[0] for d in done_at.values()) - arrivals[0]
-    lat = sorted(done_at[i][0] - arrivals[i] for i in range(len(reqs)))
+    # whole job: every rank's work over the latest completion (from the
+    # stream's first arrival) of any rank
+    makespan = max(d[0] for d in done_at.values()) - all_arrivals[0]
+    makespan = max_over_ranks(makespan * 1e3) * 1e-3
+    lat_local = {mine[i]: done_at[i][0] - arrivals[i] for i in range(len(reqs))}
     failed = [{"kind": reqs[i][0], "cells": reqs[i][1].ncell, "status": d[2]}
               for i, d in sorted(done_at.items()) if d[1] != mb.REQ_DONE]
-    served = work / makespan
+    served = total_work / makespan
     # sequential plain solves, each alone: create, init, cycles, read-back
     service = []
     for kind, p in reqs:
@@ -649,13 +681,23 @@ def run_serve(args):
             dt_s = time.perf_counter() - w0
             best = dt_s if best is None else min(best, dt_s)
         service.append(best)
-    fin, plat = 0.0, []
-    for a, sv in zip(arrivals, service):  # FIFO queue under the same arrivals
+    fin, plat_local = 0.0, {}
+    for j, (a, sv) in enumerate(zip(arrivals, service)):  # FIFO queue under the same arrivals
         fin = max(fin, a) + sv
-        plat.append(fin - a)
-    plat.sort()
+        plat_local[mine[j]] = fin - a
     # both forms over the same arrivals: work / (last completion - first arrival)
-    plain = work / (fin - arrivals[0])
+    plain = total_work / (max_over_ranks((fin - all_arrivals[0]) * 1e3) * 1e-3)
+    busy = max_over_ranks(sum(service) * 1e3) * 1e-3
+    # every request's latency in both forms, gathered on rank 0
+    g_lat = gather_results(lat_local, world)
+    g_plat = gather_results(plat_local, world)
+    g_fail = gather_results({rank: failed}, world)
+    if rank != 0:
+        return None
+    lat = sorted(g_lat.values())
+    plat = sorted(g_plat.values())
+    failed = [f for r in sorted(g_fail) for f in g_fail[r]]
+    reqs, arrivals, work = all_reqs, all_arrivals, total_work
 
     def pct(v, q):
         return v[min(len(v) - 1, int(q * len(v)))]
@@ -667,21 +709,19 @@ def run_serve(args):
     for i, (_, p) in enumerate(reqs):
         c = cls_of(p.ncell)
         by_cls.setdefault(c, ([], []))
-        by_cls[c][0].append(done_at[i][0] - arrivals[i])
-    fin2 = 0.0
-    for i, (a, sv) in enumerate(zip(arrivals, service)):
-        fin2 = max(fin2, a) + sv
-        by_cls[cls_of(reqs[i][1].ncell)][1].append(fin2 - a)
+        by_cls[c][0].append(g_lat[i])
+        by_cls[c][1].append(g_plat[i])
     cls_lat = {c: {"requests": len(v[0]), "served_p50": pct(sorted(v[0]), 0.5), "served_p99": pct(sorted(v[0]), 0.99),
                    "plain_p50": pct(sorted(v[1]), 0.5), "plain_p99": pct(sorted(v[1]), 0.99)}
                for c, v in sorted(by_cls.items())}
     big = sum(p.ncell for _, p in reqs if p.ncell >= 1000000) * its
     out = {
-        "metric": METRIC, "value": served, "unit": "cell-cycles/s", "n_gpus": 1,
+        "metric": METRIC, "value": served, "unit": "cell-cycles/s", "n_gpus": world,
         "steps": its, "warmup": 3, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOADS["serve"][0], "requests": len(reqs), "rate_per_s": args.rate,
+                   "parallelism": f"requests shared by device bytes over {world} GPU(s)" if world > 1 else "1 GPU",
                    "iterations_per_request": its, "cells": sum(p.ncell for _, p in reqs),
                    "cycles_per_step": args.cycles_per_step,
                    "offered_cell_cycles_per_s": work / (arrivals[-1] - arrivals[0]),
@@ -693,7 +733,7 @@ def run_serve(args):
         "served_vs_plain": served / plain,
         "plain": {"value": plain, "unit": "cell-cycles/s",
                   "latency_s": {"p50": pct(plat, 0.5), "p99": pct(plat, 0.99), "max": plat[-1]},
-                  "busy_value": work / sum(service),
+                  "busy_value": total_work / busy,
                   "how": "the same requests solved one after another through their own handles (create, init, "
                          "iterations, status read-back), each timed with plain launches and with its own CUDA "
                          "graph and the faster kept; value and latency from a FIFO queue of those service times "
@@ -744,6 +784,9 @@ def main():
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
     else:
         run_ours(args)
 
