@@ -272,6 +272,15 @@ int mhc_batch_set_grid_scale(mhc_batch* b, int scale);
 /* per-phase override of the grid scale (stage = enum mhc_stage, scale -1 =
  * back to the batch-wide value); the autotuner sets these */
 int mhc_batch_set_stage_grid_scale(mhc_batch* b, int stage, int scale);
+/* layout of the y / z remap sweeps of classical-limiter cases, for cells
+ * and for nodes: 0 = by mesh size (default), 1 = one warp per line,
+ * 2 = shared-memory tile, 3 = one thread per line chunk.  Results are the
+ * same bit for bit whatever the layout; the autotuner picks the fastest.
+ * The _case_ variants set them, and the per-phase grid scale, for one case
+ * run alone. */
+int mhc_batch_set_sweep_layout(mhc_batch* b, int cell_layout, int node_layout);
+int mhc_case_set_sweep_layout(mhc_case* h, int cell_layout, int node_layout);
+int mhc_case_set_stage_grid_scale(mhc_case* h, int stage, int scale);
 /* number of kernels the batch (or a single case) has put on the GPU so far;
  * a CUDA graph replay counts every kernel node it runs */
 long long mhc_batch_launches(mhc_batch* b);

@@ -112,6 +112,9 @@ _SIGS = {
     "mhc_case_params_default": (None, [C.POINTER(CaseParams)]),
     "mhc_batch_create_on_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "mhc_batch_poll_request": (C.c_int, [C.c_void_p]),
+    "mhc_batch_set_sweep_layout": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "mhc_case_set_sweep_layout": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "mhc_case_set_stage_grid_scale": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "mhc_batch_poll_wait": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                                       C.POINTER(C.c_double)]),
     "mhc_server_take_completed": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]),
@@ -311,6 +314,19 @@ class Hydro:
         _check(self.lib, int(got), f"set_field {name}")
 
     # IEquationOfState (src/eos/IEquationOfState.h:38-65), per environment
+    def set_sweep_layout(self, cell_layout: int, node_layout: int):
+        """y / z sweep layouts: 0 by mesh size, 1 warp per line, 2 tile, 3 line chunks."""
+        _check(self.lib, self.lib.mhc_case_set_sweep_layout(self.h, int(cell_layout), int(node_layout)),
+               "sweep layout")
+
+    def set_stage_grid_scale(self, stage: int | str, scale: int):
+        st = Hydro.STAGES.index(stage) if isinstance(stage, str) else int(stage)
+        _check(self.lib, self.lib.mhc_case_set_stage_grid_scale(self.h, st, int(scale)), "stage grid scale")
+
+    def set_grid_scale(self, scale: int):
+        for st in range(len(Hydro.STAGES)):
+            self.set_stage_grid_scale(st, scale)
+
     def eos_apply(self, env: int) -> None:
         _check(self.lib, self.lib.mhc_eos_apply(self.h, int(env)), "applyEOS")
 
@@ -443,6 +459,11 @@ class Batch:
 
     def set_grid_scale(self, scale: int):
         _check(self.lib, self.lib.mhc_batch_set_grid_scale(self.b, int(scale)), "grid scale")
+
+    def set_sweep_layout(self, cell_layout: int, node_layout: int):
+        """y / z sweep layouts: 0 by mesh size, 1 warp per line, 2 tile, 3 line chunks."""
+        _check(self.lib, self.lib.mhc_batch_set_sweep_layout(self.b, int(cell_layout), int(node_layout)),
+               "sweep layout")
 
     @property
     def launches(self) -> int:

@@ -78,7 +78,9 @@ int engine_rebuild(Engine* e) {
     int sens = (int)((h->it_host - 1) % h->DIM);
     const int el = case_elasto(h) ? 1 : 0, hg = case_hourglass(h) ? 1 : 0;
     const int lim = node_sweep_mode(h->P), clim = cell_sweep_mode(h->P);
-    const int cols = cols_mask(h), ncols = node_cols_mask(h), tile = tile_mask(h), ntile = node_tile_mask(h);
+    int cols, tile, ncols, ntile;
+    sweep_masks(h, e->cell_layout, false, cols, tile);
+    sweep_masks(h, e->node_layout, true, ncols, ntile);
     const int cbc = case_cell_bcs(h) ? 1 : 0;
     auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols, cbc, tile, ntile);
     auto it = gidx.find(key);
@@ -1449,6 +1451,35 @@ int mhc_batch_set_grid_scale(mhc_batch* b, int scale) {
 long long mhc_batch_launches(mhc_batch* b) { return b ? b->e->launches : -1; }
 
 long long mhc_case_launches(mhc_case* h) { return (h && h->solo) ? h->solo->launches : (h ? 0 : -1); }
+
+int mhc_batch_set_sweep_layout(mhc_batch* b, int cell_layout, int node_layout) {
+  if (!b || cell_layout < 0 || cell_layout > 3 || node_layout < 0 || node_layout > 3)
+    return set_err(MHC_ERR_ARG, "layouts are 0..3");
+  b->e->cell_layout = cell_layout;
+  b->e->node_layout = node_layout;
+  b->e->dirty = true;
+  return MHC_OK;
+}
+
+int mhc_case_set_sweep_layout(mhc_case* h, int cell_layout, int node_layout) {
+  if (!h || cell_layout < 0 || cell_layout > 3 || node_layout < 0 || node_layout > 3)
+    return set_err(MHC_ERR_ARG, "layouts are 0..3");
+  int r = solo_engine(h);
+  if (r) return r;
+  h->solo->cell_layout = cell_layout;
+  h->solo->node_layout = node_layout;
+  h->solo->dirty = true;
+  return MHC_OK;
+}
+
+int mhc_case_set_stage_grid_scale(mhc_case* h, int stage, int scale) {
+  if (!h || stage < 0 || stage >= MHC_NUM_STAGES || scale < -1) return set_err(MHC_ERR_ARG, "bad stage or scale");
+  int r = solo_engine(h);
+  if (r) return r;
+  h->solo->stage_scale[stage] = scale;
+  if (h->solo->graph) h->solo->dirty = true;  // a captured graph holds the old grids
+  return MHC_OK;
+}
 
 int mhc_batch_set_stage_grid_scale(mhc_batch* b, int stage, int scale) {
   if (!b || stage < 0 || stage >= MHC_NUM_STAGES || scale < -1 || scale > 64)

@@ -110,6 +110,10 @@ struct Engine {
   // per-phase override of grid_scale (-1 = use grid_scale), set by a tuner
   int stage_scale[MHC_NUM_STAGES] = {-1, -1, -1, -1, -1, -1, -1};
   int cur_stage = -1;  // phase being launched (StageTimer scope)
+  // layout of the y / z sweeps of classical-limiter cases, set by a caller
+  // or the tuner (mhc_*_set_sweep_layout): 0 = by mesh size (the line-chunk
+  // thresholds), 1 = warp per line, 2 = shared-memory tile, 3 = line chunks
+  int cell_layout = 0, node_layout = 0;
   // kernels this engine put on the GPU (graph replays count their nodes)
   long long launches = 0;
   long long graph_launches = 0;  // kernel nodes of the captured graph
@@ -224,6 +228,19 @@ inline int group_node_phase(int LIM, int NCOLS, int NTILE, int D) {
   if ((NCOLS >> D) & 1) return node_sweep_phase(LIM_COLS + LIM, D);
   if ((NTILE >> D) & 1) return PH_SWNT0 + D;
   return node_sweep_phase(LIM, D);
+}
+
+// the (line-chunk, tile) direction masks of a case's cell or node sweeps
+// under an engine's layout choice
+inline void sweep_masks(const mhc_case* h, int layout, bool nodes, int& cols, int& tile) {
+  cols = nodes ? node_cols_mask(h) : cols_mask(h);
+  tile = nodes ? node_tile_mask(h) : tile_mask(h);
+  const int mode = nodes ? node_sweep_mode(h->P) : cell_sweep_mode(h->P);
+  if (layout == 0 || mode > LIM_ORDER1) return;
+  int all = 0;
+  for (int D = 1; D < h->DIM; ++D) all |= 1 << D;
+  cols = layout == 3 ? all : 0;
+  tile = layout == 2 ? all : 0;
 }
 
 // phase of the cell sweep of a group along D
