@@ -147,7 +147,7 @@ def load(path: str | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("MAHYCO_B200_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise MahycoError(f"{p} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
     lib = C.CDLL(p)
