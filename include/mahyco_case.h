@@ -30,7 +30,10 @@ extern "C" {
 enum mhc_eos_kind {
   MHC_EOS_PERFECT_GAS = 0,   /* PerfectGasEOSService.cc */
   MHC_EOS_STIFFENED_GAS = 1, /* StiffenedGasEOSService.cc */
-  MHC_EOS_MIE_GRUNEISEN = 2  /* MieGruneisenEOSService.cc */
+  MHC_EOS_MIE_GRUNEISEN = 2, /* MieGruneisenEOSService.cc */
+  MHC_EOS_FICTIF = 3         /* FictifEOSService.cc: the pressure a function of time only, sound
+                                speed 1, internal energy reset to 0 (advection without Lagrange
+                                phase, sans_lagrange) */
 };
 
 /* boundary-condition kinds, same numbering as TypesMahyco::eBoundaryCondition */
@@ -69,14 +72,25 @@ enum mhc_case_model {
   MHC_CASE_SEDOV = 2,     /* casTest/SEDOV/SEDOVService.cc */
   MHC_CASE_TWO_STATE = 3, /* explicit left/right states (seeded batch cases) */
   MHC_CASE_ONECELL = 4,   /* casTest/ONECELL/ONECELLService.cc: one uniform environment */
-  MHC_CASE_BUBBLES = 5    /* casTest/CHOCBULLE/CHOCBULLEService.cc: a lattice of bubbles of
+  MHC_CASE_BUBBLES = 5,   /* casTest/CHOCBULLE/CHOCBULLEService.cc: a lattice of bubbles of
                              environment 1 in environment 0 (mixed boundary cells) */
+  MHC_CASE_RIDER = 6      /* casTest/RIDER/RIDERService.cc: a disc advected by a prescribed
+                             velocity field (cas_test 23-38) */
 };
 
 /* cas-test ids used by SOD and SEDOV (TypesMahyco.h:44-94) */
 enum mhc_cas_test {
   MHC_TEST_SEDOV = 1, MHC_TEST_SOD_X = 3, MHC_TEST_SOD_Y = 4, MHC_TEST_SOD_Z = 5,
-  MHC_TEST_BISEDOV = 11, MHC_TEST_BISOD_X = 13, MHC_TEST_BISOD_Y = 14, MHC_TEST_BISOD_Z = 15
+  MHC_TEST_BISEDOV = 11, MHC_TEST_BISOD_X = 13, MHC_TEST_BISOD_Y = 14, MHC_TEST_BISOD_Z = 15,
+  /* RIDER: one environment (MonoRider*, 23-30) or a disc of environment 1 in
+   * environment 0 (Rider*, 31-38); velocity a translation along x, y or the
+   * diagonal, a rotation about (0.5, 0.5), a vortex or a deformation field */
+  MHC_TEST_MONO_RIDER_TX = 23, MHC_TEST_MONO_RIDER_TY = 24, MHC_TEST_MONO_RIDER_T45 = 25,
+  MHC_TEST_MONO_RIDER_ROTATION = 26, MHC_TEST_MONO_RIDER_VORTEX = 27, MHC_TEST_MONO_RIDER_DEFORMATION = 28,
+  MHC_TEST_MONO_RIDER_VORTEX_REVERSE = 29, MHC_TEST_MONO_RIDER_DEFORMATION_REVERSE = 30,
+  MHC_TEST_RIDER_TX = 31, MHC_TEST_RIDER_TY = 32, MHC_TEST_RIDER_T45 = 33, MHC_TEST_RIDER_ROTATION = 34,
+  MHC_TEST_RIDER_VORTEX = 35, MHC_TEST_RIDER_DEFORMATION = 36, MHC_TEST_RIDER_VORTEX_REVERSE = 37,
+  MHC_TEST_RIDER_DEFORMATION_REVERSE = 38
 };
 
 /* longueur-caracteristique option values */
@@ -125,6 +139,10 @@ typedef struct mhc_env_params {
   double depot_cutoff[2];
   double depot_tdebut, depot_tfin;
   double depot_power;
+  /* Fictif EOS (FictifEOS.axl): tdebut-pression, tfin-pression,
+   * valeur-debut-pression, valeur-dependance-temps; the pressure is
+   * p0 + dpdt t once t > tdebut, 0 once t > tfin */
+  double fictif_tdebut, fictif_tfin, fictif_p0, fictif_dpdt;
 } mhc_env_params;
 
 typedef struct mhc_bc {
@@ -189,6 +207,19 @@ typedef struct mhc_case_params {
   double bubbles_first[3];
   double bubbles_delta[3];
   double bubbles_radius;
+  /* sans-lagrange (Mahyco.axl): pure advection.  The node velocities are
+   * prescribed (those of the initialisation, times cos(Pi t parameter) with
+   * the RIDER reverse option), only nodes shared by exactly four cells move,
+   * the density, pseudo-viscosity and energy updates are skipped, the time
+   * step stays deltat_init, and the remap projects the cells only (no dual
+   * projection: the velocities are not remapped). */
+  int sans_lagrange;
+  /* RIDER case model options (RIDER.axl): reverse-option, parametre,
+   * rayon-bulle, densite-interieure-initiale-lineaire */
+  int rider_reverse;
+  double rider_parameter;
+  double rider_radius;
+  int rider_linear_density;
 } mhc_case_params;
 
 #ifdef __cplusplus

@@ -15,14 +15,21 @@ import xml.etree.ElementTree as ET
 MAX_ENV = 4
 MAX_BC = 12
 
-EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN = 0, 1, 2
+EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN, EOS_FICTIF = 0, 1, 2, 3
 EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
-               "MieGruneisen": EOS_MIE_GRUNEISEN}
+               "MieGruneisen": EOS_MIE_GRUNEISEN, "Fictif": EOS_FICTIF}
 BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4, "Density": 5,
               "Energy": 6, "SuperGaussianEnergy": 7, "Pressure": 8}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
-CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES = 1, 2, 3, 4, 5
-CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL, "CHOCBULLE": CASE_BUBBLES}
+CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES, CASE_RIDER = 1, 2, 3, 4, 5, 6
+CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL, "CHOCBULLE": CASE_BUBBLES,
+                "RIDER": CASE_RIDER}
+# RIDER cas-test ids (TypesMahyco.h:69-84): MonoRider* 23-30, Rider* 31-38
+RIDER_TESTS = {n: 23 + i for i, n in enumerate(
+    ("MonoRiderTx", "MonoRiderTy", "MonoRiderT45", "MonoRiderRotation", "MonoRiderVortex", "MonoRiderDeformation",
+     "MonoRiderVortexTimeReverse", "MonoRiderDeformationTimeReverse", "RiderTx", "RiderTy", "RiderT45",
+     "RiderRotation", "RiderVortex", "RiderDeformation", "RiderVortexTimeReverse",
+     "RiderDeformationTimeReverse"))}
 LENGTHS = {"racine-cubique-volume": 0, "faces-opposees": 1, "monodimX": 2,
            "monodimY": 3, "monodimZ": 4}
 MINMOD, SUPERBEE, VANLEER = 0, 1, 2
@@ -52,6 +59,8 @@ class EnvParams(C.Structure):
         ("depot_type", C.c_int), ("depot_value", C.c_double), ("depot_origin", C.c_double * 3),
         ("depot_dependance", C.c_double * 4), ("depot_cutoff", C.c_double * 2),
         ("depot_tdebut", C.c_double), ("depot_tfin", C.c_double), ("depot_power", C.c_double),
+        ("fictif_tdebut", C.c_double), ("fictif_tfin", C.c_double), ("fictif_p0", C.c_double),
+        ("fictif_dpdt", C.c_double),
     ]
 
 
@@ -85,6 +94,8 @@ class CaseParams(C.Structure):
         ("conservation_energie_totale", C.c_int),
         ("bubbles_n", C.c_int * 3), ("bubbles_first", C.c_double * 3), ("bubbles_delta", C.c_double * 3),
         ("bubbles_radius", C.c_double),
+        ("sans_lagrange", C.c_int), ("rider_reverse", C.c_int), ("rider_parameter", C.c_double),
+        ("rider_radius", C.c_double), ("rider_linear_density", C.c_int),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -154,6 +165,7 @@ def default_params() -> CaseParams:
     p.remap_threshold = 1.0e-10
     p.time_history_period = 10
     p.coef_antiderive = 0.0
+    p.rider_radius = 0.15
     return p
 
 
@@ -195,7 +207,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     Returns ``(params, info)`` where ``info`` holds environment names, the
     time loop, the post-processed and EnvSummation variable lists and
     anything the hot path ignores.  Unsupported options that change the cycle
-    (CSTS scheme, sans-lagrange, elasto models other than DefaultModel,
+    (CSTS scheme, elasto models other than DefaultModel,
     super-Gaussian energy deposits, non-velocity boundary conditions) raise
     ``NotImplementedError``.
     """
@@ -207,6 +219,8 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     # post-processed variables (Ensight) and EnvSummation variables
     info["output_vars"] = [v.text.strip() for v in root.findall("arcane-post-processing/output/variable")]
     info["history_vars"] = [v.text.strip() for v in root.findall("time-history/bilan/variable")]
+    # save-init: the post-processing also writes the initial state (step 0)
+    info["save_init"] = bool(_txt(root, "arcane-post-processing/save-init", False, _bool))
     cart = root.find("mesh/meshgenerator/cartesian")
     if cart is None:
         raise NotImplementedError("only the cartesian mesh generator is supported")
@@ -247,7 +261,10 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
                           ("s2", "s2"), ("s3", "s3"), ("gamma0", "gamma0"), ("a", "a"), ("c0", "c0"),
                           ("energie-ref", "energie_ref"), ("temperature-ref", "temperature_ref"),
                           ("tension-damage-thresold", "tension_damage_thresold"),
-                          ("density-damage-thresold", "density_damage_thresold")):
+                          ("density-damage-thresold", "density_damage_thresold"),
+                          ("tdebut-pression", "fictif_tdebut"), ("tfin-pression", "fictif_tfin"),
+                          ("valeur-debut-pression", "fictif_p0"),
+                          ("valeur-dependance-temps", "fictif_dpdt")):
             v = _txt(eosel, tag, None)
             if v is not None:
                 setattr(e, attr, v)
@@ -291,6 +308,12 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         p.bubbles_first[:] = [float(v) for v in _txt(cm, "position-premiere-bulle", "0. 0. 0.", str).split()]
         p.bubbles_delta[:] = [_txt(cm, f"delta{a}-bulle", 0.0) for a in "xyz"]
         p.bubbles_radius = _txt(cm, "rayon-bulle", 0.0)
+    if p.cas_model == CASE_RIDER:
+        # RIDER.axl:145-166
+        p.rider_reverse = int(_txt(cm, "reverse-option", False, _bool))
+        p.rider_parameter = _txt(cm, "parametre", 0.0)
+        p.rider_radius = _txt(cm, "rayon-bulle", 0.15)
+        p.rider_linear_density = int(_txt(cm, "densite-interieure-initiale-lineaire", False, _bool))
     rm = m.find("remap")
     if rm is not None:
         if rm.get("name", "RemapADI") != "RemapADI":
@@ -312,8 +335,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
             raise NotImplementedError("ordre-projection / projection-limiteur-id out of range")
     if _txt(m, "schema-csts", False, _bool):
         raise NotImplementedError("schema-csts")
-    if _txt(m, "sans-lagrange", False, _bool):
-        raise NotImplementedError("sans-lagrange")
+    p.sans_lagrange = int(_txt(m, "sans-lagrange", False, _bool))
     p.pseudo_centree = int(_txt(m, "pseudo-centree", False, _bool))
     p.with_projection = int(_txt(m, "with-projection", True, _bool))
     if info["timeloop"] == "MahycoLagrangeLoop":

@@ -11,14 +11,16 @@ reference datasets (``NONREGRESSION/CAS_*``) at any size:
 * ``mie_gruneisen_plate`` -- two Mie-Gruneisen states, explicit pressure
 * ``water_bubbles`` -- CHOCBULLE-like lattice of air bubbles in stiffened-gas
   water hit by the shock reflected from a wall
+* ``rider``      -- RIDER service: a disc advected by a prescribed velocity
+  field without Lagrange phase (sans-lagrange, Fictif equation of state)
 """
 from __future__ import annotations
 
 import math
 import random
 
-from .case import (ARITHMETIC_G, CASE_BUBBLES, CASE_ONECELL, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE, DEPOT_CONSTANT,
-                   DEPOT_SUPER_GAUSSIAN, EOS_MIE_GRUNEISEN, EULER_X, EULER_Y, EULER_Z,
+from .case import (ARITHMETIC_G, CASE_BUBBLES, CASE_ONECELL, CASE_RIDER, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE,
+                   DEPOT_CONSTANT, DEPOT_SUPER_GAUSSIAN, EOS_FICTIF, EOS_MIE_GRUNEISEN, EULER_X, EULER_Y, EULER_Z,
                    EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
                    ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults,
                    symmetry_bcs)
@@ -179,6 +181,29 @@ def water_bubbles(dim=2, n=(80, 40), L=(1.0, 0.5), bubbles=(3, 2), first=(0.55, 
     p.projection_limiteur_id = limiter
     p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.3, deltat_init, 1e-14, 1e-4
     symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
+    return p
+
+
+def rider(test=31, dim=3, n=(50, 50, 1), L=(1.0, 1.0, 0.1), limiter=MINMOD, reverse=False, parameter=0.0,
+          radius=0.15, deltat=1e-3, final_time=1e30) -> CaseParams:
+    """CAS_(Mono)Rider*: the RIDER service (cas-test 23-38) on the unit
+    square (one cell thick in z in 3D), environments "Vide" (density 0) and
+    "Bulle" (density 1) with the Fictif equation of state (pressure 0 until
+    t = 10), sans-lagrange, constant deltat."""
+    p = default_params()
+    _mesh(p, dim, n, L)
+    p.nb_env = 2
+    for e in range(2):
+        env_defaults(p.env[e], EOS_FICTIF)
+        p.env[e].specific_heat = 2.4
+        p.env[e].pression_initiale = 0.0
+        p.env[e].fictif_tfin = 10.0
+    p.env[0].densite_initiale, p.env[1].densite_initiale = 0.0, 1.0
+    p.cas_model, p.cas_test = CASE_RIDER, test
+    p.rider_reverse, p.rider_parameter, p.rider_radius = int(reverse), parameter, radius
+    p.sans_lagrange = 1
+    p.projection_limiteur_id = limiter
+    p.deltat_init, p.deltat_max, p.final_time = deltat, 1e-4, final_time
     return p
 
 
@@ -442,11 +467,36 @@ PARITY_CASES = {
                                                    deltat_init=1e-3)), 60),
     "adi2d_bisod_cell_bcs_gaussian": (lambda: _cell_bcs(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True,
                                                             deltat_init=1e-3), explicit=1, gaussian=True), 60),
+    # sans-lagrange advection of the RIDER discs (Fictif equation of state):
+    # translations, rotation, vortex and deformation fields, the reverse
+    # option, pente-borne fluxes, a 2D mesh and a 3D mesh of several layers
+    # (only nodes shared by four cells move), a Fictif pressure law that
+    # switches on and off inside the run
+    "adv3d_rider_tx": (lambda: rider(31), 120),
+    "adv3d_mono_rider_rotation": (lambda: rider(26), 100),
+    "adv3d_rider_vortex_superbee": (lambda: rider(35, limiter=SUPERBEE), 100),
+    "adv2d_rider_deformation_vanleer": (lambda: rider(36, dim=2, n=(40, 40), L=(1.0, 1.0), limiter=VANLEER), 100),
+    "adv3d_rider_deformation_reverse": (lambda: rider(38, reverse=True, parameter=1.0), 100),
+    "adv3d_rider_ty_pb_mixte_superbee": (lambda: _pb(rider(32, limiter=SUPERBEE), 2, mixte=1), 100),
+    "adv3d_rider_t45_layers": (lambda: rider(33, n=(24, 24, 4), L=(1.0, 1.0, 0.4)), 80),
+    "adv2d_rider_rotation_fictif_window": (lambda: _fictif_window(rider(34, dim=2, n=(40, 40), L=(1.0, 1.0))), 100),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
-# calls exp and pow, which CUDA and the oracle's libm round differently
-PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13}
+# calls exp and pow, and the reverse option of RIDER scales the velocities by
+# cos(Pi t), which CUDA and the oracle's libm round differently
+PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13,
+                    "adv3d_rider_deformation_reverse": 1e-12}
+
+
+def _fictif_window(p: CaseParams) -> CaseParams:
+    """Fictif pressures p0 + dpdt t between t = 0.02 and t = 0.07, the
+    initial pressures before (the disc at 2, the rest at 0.5)."""
+    for e, (p_init, p0, dpdt) in enumerate(((0.5, 1.0, 3.0), (2.0, 0.25, 10.0))):
+        o = p.env[e]
+        o.pression_initiale = p_init
+        o.fictif_tdebut, o.fictif_tfin, o.fictif_p0, o.fictif_dpdt = 0.02, 0.07, p0, dpdt
+    return p
 
 
 def _cell_bcs(p: CaseParams, explicit: int = 0, gaussian: bool = False) -> CaseParams:

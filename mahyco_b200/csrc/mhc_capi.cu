@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -68,7 +69,7 @@ int engine_rebuild(Engine* e) {
     desc[i].P = h->d_params;
   }
   // groups
-  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
@@ -82,12 +83,15 @@ int engine_rebuild(Engine* e) {
     sweep_masks(h, e->cell_layout, false, cols, tile);
     sweep_masks(h, e->node_layout, true, ncols, ntile);
     const int cbc = case_cell_bcs(h) ? 1 : 0;
-    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols, cbc, tile, ntile);
+    const int adv = h->P.sans_lagrange ? 1 : 0;
+    auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols, cbc, tile, ntile,
+                               adv);
     auto it = gidx.find(key);
     if (it == gidx.end()) {
       Group g;
       g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
       g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim; g.COLS = cols; g.NCOLS = ncols; g.CBC = cbc; g.TILE = tile; g.NTILE = ntile;
+      g.ADV = adv;
       gidx[key] = (int)e->groups.size();
       e->groups.push_back(g);
       it = gidx.find(key);
@@ -160,6 +164,56 @@ int engine_rebuild(Engine* e) {
   return MHC_OK;
 }
 
+// RIDER velocity fields (RIDERService.cc:141-172 and 255-285): evaluated on
+// the host with the C library's sin, cos and atan2, the functions the
+// reference's own initialisation calls (the device versions differ from
+// them by an ulp here and there), and written over the node velocities and
+// prescribed velocities kb_init_nodes left; stream-ordered after it.  Pi is
+// TypesMahyco.h:42's 3.14159265359.
+int rider_upload(mhc_case* h, cudaStream_t st) {
+  const mhc_case_params& P = h->P;
+  const Mesh& M = h->M;
+  const long long NN = M.nnode;
+  const double Pi = 3.14159265359;
+  const int kind = (P.cas_test - MHC_TEST_MONO_RIDER_TX) % 8;  // Tx Ty T45 Rotation Vortex Deformation (+2 reverse)
+  std::vector<double> v(3 * NN, 0.0);
+  for (long long n = 0; n < NN; ++n) {
+    const long long i = n % M.nnx, r = n / M.nnx, j = r % M.nny, k = r / M.nny;
+    const double x = M.o[0] + i * M.h[0], y = M.o[1] + j * M.h[1], z = M.dim == 3 ? M.o[2] + k * M.h[2] : 0.;
+    (void)z;
+    double vx = 0.0, vy = 0.0;
+    if (kind == 0) vx = 1.;
+    if (kind == 1) vy = 1.;
+    if (kind == 2) { vx = 1.0; vy = 1.0; }
+    if (kind == 3) {
+      const double ddx = x - 0.5, ddy = y - 0.5;
+      const double theta = std::atan2(ddy, ddx);
+      const double rr = std::sqrt(ddx * ddx + ddy * ddy);
+      const double omega = 4. * Pi;
+      vx = -rr * omega * std::sin(omega * 0. + theta);
+      vy = rr * omega * std::cos(omega * 0. + theta);
+    }
+    if (kind == 4 || kind == 6) {
+      vx = -2. * std::cos(Pi * y) * std::sin(Pi * y) * std::sin(Pi * x) * std::sin(Pi * x);
+      vy = 2. * std::cos(Pi * x) * std::sin(Pi * x) * std::sin(Pi * y) * std::sin(Pi * y);
+    }
+    if (kind == 5 || kind == 7) {
+      const double ddx = x + 0.5, ddy = y + 0.5;
+      vx = std::sin(4. * Pi * ddx) * std::sin(4. * Pi * ddy);
+      vy = std::cos(4. * Pi * ddx) * std::cos(4. * Pi * ddy);
+    }
+    v[n] = vx;
+    v[NN + n] = vy;
+  }
+  // pageable sources: each copy is staged before the call returns
+  const size_t b = NN * sizeof(double);
+  CK(cudaMemcpyAsync(h->F.vx, v.data(), b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->F.vy, v.data() + NN, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->F.vz, v.data() + 2 * NN, b, cudaMemcpyHostToDevice, st));
+  if (h->F.v0) CK(cudaMemcpyAsync(h->F.v0, v.data(), 3 * b, cudaMemcpyHostToDevice, st));
+  return MHC_OK;
+}
+
 // -- phase launches -------------------------------------------------------------
 void launch_init(Engine* e) {
   for (Group& g : e->groups) {
@@ -192,6 +246,13 @@ void lag_nodes_dispatch(Engine* e, Group& g) {
 void launch_lagrange_nodes(Engine* e) {
   StageTimer tm(e, MHC_STAGE_LAGRANGE_NODES);
   for (Group& g : e->groups) {
+    if (g.ADV) {
+      // sans-lagrange: prescribed velocities (validated without cell
+      // boundary conditions)
+      if (g.DIM == 2) plaunch(e, kb_advect_nodes<2>, CT, 0, g.lag_nodes);
+      else plaunch(e, kb_advect_nodes<3>, CT, 0, g.lag_nodes);
+      continue;
+    }
     if (g.DIM == 2) lag_nodes_dispatch<2>(e, g);
     else lag_nodes_dispatch<3>(e, g);
     if (g.CBC) {
@@ -217,7 +278,8 @@ void launch_lagrange_cells(Engine* e) {
     } else {
       if (g.DIM == 2) plaunch(e, kb_lagrange_geom<2>, CT, 0, g.lag_cells);
       else plaunch(e, kb_lagrange_geom<3>, CT, 0, g.lag_cells);
-      if (g.EULER) DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true, false>, CT, 0, g.lag_cells)));
+      if (g.ADV) DISPATCH_GROUP(g, (plaunch(e, kb_advect_cells<DIM_, NE_>, CT, 0, g.lag_cells)));
+      else if (g.EULER) DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true, false>, CT, 0, g.lag_cells)));
       else DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, false, false>, CT, 0, g.lag_cells)));
     }
   }
@@ -267,11 +329,13 @@ void launch_remap_variables(Engine* e) {
         if (g.DIM == 2) plaunch(e, kb_euler_volume<2>, CT, 0, g.fin_cells);
         else plaunch(e, kb_euler_volume<3>, CT, 0, g.fin_cells);
       }
-      DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_cells<DIM_, NE_>, CT, 0, g.fin_cells, K)));
+      if (g.ADV) DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_cells<DIM_, NE_, true>, CT, 0, g.fin_cells, K)));
+      else DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_cells<DIM_, NE_>, CT, 0, g.fin_cells, K)));
     }
     {
       StageTimer tm(e, MHC_STAGE_FINALIZE_NODES);
-      if (K > 0) DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_nodes<DIM_>, CT, 0, g.fin_nodes, K)));
+      if (K > 0 && g.ADV) DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_nodes<DIM_, false>, CT, 0, g.fin_nodes, K)));
+      else if (K > 0) DISPATCH_GROUP(g, (plaunch(e, kb_remap_finalize_nodes<DIM_>, CT, 0, g.fin_nodes, K)));
       if (g.EULER == 2) plaunch(e, kb_euler_axis_reset, CT, 0, g.fin_nodes);
     }
   }
@@ -285,7 +349,8 @@ void launch_remap(Engine* e) {
 void launch_dt(Engine* e) {
   StageTimer tm(e, MHC_STAGE_DELTA_T);
   for (Group& g : e->groups) {
-    DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_>, CT, 0, g.dt)));
+    // sans-lagrange keeps deltat_init: no CFL reduction
+    if (!g.ADV) DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_>, CT, 0, g.dt)));
     if (g.cases.n > 0) {
       kb_delta_t_finalize<<<cdiv(g.cases.n, 128), 128, 0, e->stream>>>(e->d_desc, e->d_ints + g.cases.off_cases, g.cases.n);
       ++e->launches;
@@ -452,7 +517,7 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   int ne = p->nb_env, nv = 3 * ne + 1;
   long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8) +
                     (p->projection_pente_borne ? nv : 0) + 2;  // (+2: boundary-condition energy, pressure)
-  long long nodes = 4 + 6 + 10;
+  long long nodes = 4 + 6 + 10 + (p->sans_lagrange ? 3 : 0);
   return cells * ncell + nodes * nnode;
 }
 
@@ -479,7 +544,22 @@ int validate(const mhc_case_params* p) {
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with a per-axis Euler remap");
   if (cellvars && p->with_newton)
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with the Newton energy update");
-  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_BUBBLES) return set_err(MHC_ERR_ARG, "cas-model");
+  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_RIDER) return set_err(MHC_ERR_ARG, "cas-model");
+  if (p->cas_model == MHC_CASE_RIDER &&
+      (p->cas_test < MHC_TEST_MONO_RIDER_TX || p->cas_test > MHC_TEST_RIDER_DEFORMATION_REVERSE || p->nb_env < 2 ||
+       !p->sans_lagrange || !(p->rider_radius > 0.)))
+    return set_err(MHC_ERR_ARG, "RIDER: cas-test 23..38, two environments or more, sans-lagrange, radius > 0");
+  if (p->sans_lagrange) {
+    // pure advection: the remap carries the cells; nothing of the
+    // Lagrange phase (elasto-plasticity, cell-variable or pressure
+    // boundary conditions) has a meaning without it
+    if (!p->with_projection) return set_err(MHC_ERR_UNSUPPORTED, "sans-lagrange needs the remap");
+    if (cellvars) return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with sans-lagrange");
+    // it returns the kinetic energy lost by the dual projection, which does
+    // not run here
+    if (p->conservation_energie_totale)
+      return set_err(MHC_ERR_UNSUPPORTED, "conservation-energie-totale with sans-lagrange");
+  }
   if (p->cas_model == MHC_CASE_BUBBLES && (p->nb_env != 2 || p->bubbles_n[0] < 0 || p->bubbles_n[1] < 0 ||
                                            p->bubbles_n[2] < 0 || !(p->bubbles_radius >= 0.)))
     return set_err(MHC_ERR_ARG, "bubble lattice: two environments, counts >= 0, radius >= 0");
@@ -512,7 +592,9 @@ int validate(const mhc_case_params* p) {
       return set_err(MHC_ERR_ARG, "energy deposit kind");
     if (p->env[e].density_damage_thresold != 0.0 || p->env[e].tension_damage_thresold > -1.e12)
       return set_err(MHC_ERR_UNSUPPORTED, "damage thresholds other than the defaults");
-    if (p->env[e].eos < 0 || p->env[e].eos > 2) return set_err(MHC_ERR_ARG, "eos kind");
+    if (p->env[e].eos < 0 || p->env[e].eos > MHC_EOS_FICTIF) return set_err(MHC_ERR_ARG, "eos kind");
+    if (p->env[e].eos == MHC_EOS_FICTIF && !p->sans_lagrange)
+      return set_err(MHC_ERR_UNSUPPORTED, "the Fictif equation of state with a Lagrange phase");
   }
   if (p->longueur_caracteristique == MHC_LENGTH_OPPOSITE_FACES && p->dim != 3)
     return set_err(MHC_ERR_UNSUPPORTED, "faces-opposees needs a 3D mesh");
@@ -617,6 +699,7 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   if (h->P.env[0].elasto_model) F.S = (double*)alloc(6 * N * sizeof(double));
   F.cqs = (double*)alloc((h->DIM == 3 ? 24 : 8) * N * sizeof(double));
   if (h->P.projection_pente_borne) F.phi_pb = (double*)alloc(h->NV * N * sizeof(double));
+  if (h->P.sans_lagrange) F.v0 = (double*)alloc(3 * NN * sizeof(double));
   if (case_cell_bcs(h)) {
     F.ebc = (double*)alloc(N * sizeof(double));
     F.pbc = (double*)alloc(N * sizeof(double));
@@ -776,10 +859,12 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
       fr.resize(N);
       if ((r = fetch(st, F.ef + env * N, fr.data(), N * 8))) return r;
     }
+    const bool fracvol = !strcmp(name, "FracVol");
     for (long long i = 0; i < N; ++i) {
       bool in = (mask[i] >> env) & 1;
       bool pure = __builtin_popcount(mask[i]) == 1;
       if (!in) host[i] = 0.;
+      else if (pure && fracvol && h->NE > 1) host[i] = e[i];  // the remap's normalised fraction
       else if (pure) host[i] = c.g ? g[i] : 1.;
       else if (volume) host[i] = fr[i] * g[i];
       else host[i] = c.e ? e[i] : 0.;
@@ -915,6 +1000,7 @@ int mhc_hydro_start_init(mhc_case* h) {
   h->solo->dirty = true;
   if ((r = engine_rebuild(h->solo))) return r;
   launch_init(h->solo);
+  if (h->P.cas_model == MHC_CASE_RIDER && (r = rider_upload(h, h->solo->stream))) return r;
   CK(cudaGetLastError());
   h->stage = S_IDLE;
   h->initialised = true;
@@ -1266,7 +1352,10 @@ int mhc_batch_init(mhc_batch* b) {
   if (!tmp->cases.empty()) {
     if ((r = engine_rebuild(tmp))) { engine_destroy(tmp); return r; }
     launch_init(tmp);
-    for (mhc_case* h : tmp->cases) h->initialised = true;
+    for (mhc_case* h : tmp->cases) {
+      if (h->P.cas_model == MHC_CASE_RIDER && (r = rider_upload(h, tmp->stream))) return r;
+      h->initialised = true;
+    }
   }
   cudaError_t ce = cudaGetLastError();
   b->init_engines.push_back(tmp);

@@ -5,6 +5,7 @@
 //   env slots       ef emf em erho ee ep ec eq      [NE][ncell]  (mixed cells only)
 //   env mask        mask                            [ncell] (bit e = cell holds env e)
 //   nodes           vx vy vz mn                     [nnode]
+//                   v0 [3][nnode] (sans-lagrange: the prescribed velocities)
 //   Lagrangian pos  Xp[3] (previous cycle), Xn[3] (this cycle)
 //   remap           U[2][NV][ncell] (NV = 3*NE+1: volumes, masses, energies, pseudo*V)
 //                   mflux[NE][ncell] (cell mass flux of the current sweep)
@@ -57,6 +58,7 @@ struct Fields {
   double* phi_pb;          // pente-borne only: projected values (phi) of the next remap's first sweep
                            // [3 nb_env + 1][ncell]; entries of absent environments keep the
                            // values of the last sweep before
+  double* v0;              // sans-lagrange only: the prescribed node velocities at n [3][nnode]
   Scalars* s;
 };
 
@@ -155,10 +157,26 @@ __device__ __forceinline__ void eos_init(const mhc_env_params& o, double p, doub
     double g = o.adiabatic_cst, pinf = o.limit_tension;
     e = (p + (g * pinf)) / ((g - 1.) * rho);
     c = sqrt((g / rho) * (p + pinf));
+  } else if (o.eos == MHC_EOS_FICTIF) {
+    // FictifEOSService::initEOS (lines 12-34)
+    double g = o.adiabatic_cst;
+    e = p / ((g - 1.) * rho);
+    c = sqrt(g * p / rho);
   } else {
     e = p / o.gamma0;
     c = o.c0;
   }
+}
+
+// FictifEOSService::applyEOS (lines 44-78) for one environment cell: the
+// pressure p_old kept until tdebut, then p0 + dpdt t, 0 after tfin; the
+// sound speed 1 (no influence on the time step); the caller resets the
+// internal energy to 0
+__device__ __forceinline__ void fictif_apply(const mhc_env_params& o, double t, double p_old, double& p, double& c) {
+  p = p_old;
+  if (t > o.fictif_tdebut) p = o.fictif_p0 + o.fictif_dpdt * t;
+  if (t > o.fictif_tfin) p = 0.;
+  c = 1.;
 }
 
 __device__ __forceinline__ double char_length(const mhc_case_params& P, int DIM, double V, const R3* coord) {
@@ -450,6 +468,25 @@ __device__ __forceinline__ double bubble_material(const mhc_case_params& P, cons
   return mat;
 }
 
+// RIDER (RIDERService.cc): the disc centre of the test (lines 27-30 and
+// 76-79) and the range of the cell's node distances to it in the (x, y)
+// plane (lines 36-45)
+__device__ __forceinline__ bool rider_mono(const mhc_case_params& P) { return P.cas_test <= MHC_TEST_MONO_RIDER_DEFORMATION_REVERSE; }
+__device__ __forceinline__ R3 rider_centre(const mhc_case_params& P) {
+  const int first_rotation = rider_mono(P) ? MHC_TEST_MONO_RIDER_ROTATION : MHC_TEST_RIDER_ROTATION;
+  return P.cas_test < first_rotation ? R3{0.20, 0.20, 0.} : R3{0.50, 0.75, 0.};
+}
+template <int DIM>
+__device__ __forceinline__ void rider_range(const R3& xb, const R3* coord, double& rmin, double& rmax) {
+  rmin = 10.;
+  rmax = 0.;
+  for (int l = 0; l < (DIM == 3 ? 8 : 4); ++l) {
+    const double rn = sqrt((coord[l].x - xb.x) * (coord[l].x - xb.x) + (coord[l].y - xb.y) * (coord[l].y - xb.y));
+    rmin = smin(rmin, rn);
+    rmax = smax(rmax, rn);
+  }
+}
+
 template <int DIM, int NE>
 __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   long long c = bx * (long long)CT + threadIdx.x;
@@ -486,6 +523,16 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   }
   double fbub = 0.;  // BUBBLES: the bubble's volume fraction of a mixed cell
   if (P.cas_model == MHC_CASE_BUBBLES && NE > 1) mat = bubble_material<DIM>(P, cc, coord, fbub);
+  double rmin = 0., rmax = 0.;  // RIDER: node distances to the disc centre
+  if (P.cas_model == MHC_CASE_RIDER) {
+    rider_range<DIM>(rider_centre(P), coord, rmin, rmax);
+    // RIDERService::initMat (lines 18-57); one environment for MonoRider*
+    const double rb = P.rider_radius;
+    if (!rider_mono(P) && NE > 1) {
+      if (rmax < rb) mat = 1;
+      else if ((rmax >= rb) && (rmin < rb)) mat = (rb - rmin) / (rmax - rmin);
+    }
+  }
   uint8_t mask;
   if (mat == 0.) mask = 1;
   else if (mat > 0. && mat < 1.) mask = 3;
@@ -507,6 +554,8 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   double rho = 0., p = 0., e = 0., cs = 0.;
   double rhoe[NE], pe[NE], ee[NE], ce[NE];
   for (int q = 0; q < NE; ++q) { rhoe[q] = pe[q] = ee[q] = ce[q] = 0.; }
+  double fe[NE], mfe[NE];
+  for (int q = 0; q < NE; ++q) { fe[q] = 1.0; mfe[q] = 1.0; }
   if (P.cas_model == MHC_CASE_SOD) {
     bool mono = P.cas_test == MHC_TEST_SOD_X || P.cas_test == MHC_TEST_SOD_Y || P.cas_test == MHC_TEST_SOD_Z;
     if (mono) {
@@ -535,6 +584,36 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
       rho = p = 0.;
       for (int q = 0; q < 2; ++q) { rhoe[q] = P.env[q].densite_initiale; pe[q] = P.env[q].pression_initiale; }
     }
+  } else if (P.cas_model == MHC_CASE_RIDER) {
+    // RIDERService::initVar / initVarMono (lines 62-173, 178-289): the disc
+    // state inside the radius, the surrounding state outside; a boundary
+    // cell takes the disc density times its covered fraction (Rider*: the
+    // first environment holds the disc's density and fraction)
+    const bool lin = P.rider_linear_density != 0;
+    const R3 xb = rider_centre(P);
+    const double rb = P.rider_radius;
+    const double croissance = lin ? 1. / rb : 1.;
+    const double d0 = P.env[0].densite_initiale, d1 = P.env[NE > 1 ? 1 : 0].densite_initiale;
+    const double p0 = P.env[0].pression_initiale, p1 = P.env[NE > 1 ? 1 : 0].pression_initiale;
+    rho = d0;
+    p = p0;
+    e = P.env[0].energie_initiale;
+    const double r = sqrt((cc.x - xb.x) * (cc.x - xb.x) + (cc.y - xb.y) * (cc.y - xb.y));
+    const double r_cell = lin ? r : rmax;
+    if (r_cell < rb) {
+      rho = d1;
+      if (lin) rho = d1 * smin(croissance * 2 * (rb - r), 1.);
+      p = p1;
+    } else if ((rmax >= rb) && (rmin < rb) && !lin) {
+      const double frac_b = (rb - rmin) / (rmax - rmin);
+      if (NE > 1 && !rider_mono(P) && !pure) {
+        constexpr int E1 = NE > 1 ? 1 : 0;
+        rhoe[0] = d1; fe[0] = frac_b; mfe[0] = frac_b;
+        rhoe[E1] = d0; fe[E1] = 1. - frac_b; mfe[E1] = 1. - frac_b;
+      }
+      rho = frac_b * d1;
+      p = p1;
+    }
   } else if (P.cas_model == MHC_CASE_ONECELL) {
     // ONECELLService::initVarMono: the first environment's state everywhere
     rho = P.env[0].densite_initiale;
@@ -556,14 +635,13 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
       p = 0.4 * rhoInit * e;
     }
   }
-  // EOS init per environment (aliased for pure cells)
-  for (int q = 0; q < NE; ++q) {
+  // EOS init per environment (aliased for pure cells); none at the start
+  // of a sans-lagrange run (MahycoModule.cc:143-171)
+  for (int q = 0; q < NE && !P.sans_lagrange; ++q) {
     if (!((mask >> q) & 1)) continue;
     if (pure) eos_init(P.env[q], p, rho, e, cs);
     else eos_init(P.env[q], pe[q], rhoe[q], ee[q], ce[q]);
   }
-  double fe[NE], mfe[NE];
-  for (int q = 0; q < NE; ++q) { fe[q] = 1.0; mfe[q] = 1.0; }
   if (P.cas_model == MHC_CASE_BUBBLES && !pure) {
     // volume fractions of the bubble (environment 1) and the medium, mass
     // fractions f rho / sum of f rho
@@ -573,7 +651,7 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
     for (int q = 0; q < 2; ++q) rm += rhoe[q] * fe[q];
     for (int q = 0; q < 2; ++q) mfe[q] = (rhoe[q] * fe[q]) / rm;
   }
-  if (!pure) {
+  if (!pure && !P.sans_lagrange) {
     e = 0.;
     for (int q = 0; q < NE; ++q) {
       if (!((mask >> q) & 1)) continue;
@@ -598,6 +676,9 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
       F.erho[q * N + c] = rhoe[q]; F.ee[q * N + c] = ee[q]; F.ep[q * N + c] = pe[q];
       F.ec[q * N + c] = ce[q]; F.eq[q * N + c] = 0.;
     }
+  } else if (NE > 1) {
+    for (int q = 0; q < NE; ++q)
+      if ((mask >> q) & 1) F.ef[q * N + c] = 1.0;  // a pure cell's volume fraction (read back only)
   }
 }
 
@@ -636,6 +717,11 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
     vx = P.env[0].vitesse_initiale[0]; vy = P.env[0].vitesse_initiale[1]; vz = P.env[0].vitesse_initiale[2];
   }
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
+  if (F.v0) {
+    // RIDER fields are written over these by the host after the launch
+    const long long NN = M.nnode;
+    F.v0[n] = vx; F.v0[NN + n] = vy; F.v0[2 * NN + n] = vz;
+  }
   F.mn[n] = node_mass_gather<DIM>(M, F.m, i, j, k);
 }
 
@@ -1291,6 +1377,90 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   }
 }
 
+// ---------------------------------------------------------------------------
+// sans-lagrange (pure advection), nodes: updateVelocityWithoutLagrange
+// (MahycoModule.cc:676-700), applyBoundaryCondition and updatePosition
+// (MahycoModule.cc:730-750), where only the nodes shared by exactly four
+// cells move.  The velocities at n are the prescribed ones (v0); with the
+// RIDER reverse option they are scaled by cos(Pi t parameter), Pi the
+// reference's 3.14159265359 (TypesMahyco.h:42).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ void body_advect_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long n = bx * (long long)CT + threadIdx.x;
+  if (n >= M.nnode) return;
+  const long long NN = M.nnode;
+  int i, j, k;
+  node_ijk(M, n, i, j, k);
+  const double dt = F.s->dt;
+  const double t = F.s->t;
+  const bool rider = P.cas_model == MHC_CASE_RIDER;
+  const double option_real = (rider && P.rider_reverse) ? 1. : 0.;
+  const double factor = rider ? P.rider_parameter : 0.;
+  const double cs = cos(3.14159265359 * t * factor);
+  const double ux = F.v0[n], uy = F.v0[NN + n], uz = F.v0[2 * NN + n];
+  double vx = ux * (1. - option_real) + option_real * ux * cs;
+  double vy = uy * (1. - option_real) + option_real * uy * cs;
+  double vz = uz * (1. - option_real) + option_real * uz * cs;
+  const double eps = 1.e-8;
+  for (int b = 0; b < P.nb_bc; ++b) {
+    const mhc_bc& bc = P.bc[b];
+    if ((t - dt * (1 - eps)) < bc.tdebut) continue;
+    if ((t - dt * (1 - eps)) > bc.tfin) continue;
+    if (!node_on_surface(M, i, j, k, bc.surface)) continue;
+    if (bc.kind == MHC_BC_VX) vx = bc.value;
+    else if (bc.kind == MHC_BC_VY) vy = bc.value;
+    else if (bc.kind == MHC_BC_VZ) vz = bc.value;
+  }
+  const R3 x = P.is_euler_scheme == MHC_EULER_FULL ? node_x0(M, i, j, k) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+  int nc = ((i > 0) + (i < M.ncx)) * ((j > 0) + (j < M.ncy));
+  if (DIM == 3) nc *= (k > 0) + (k < M.ncz);
+  F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
+  if (nc == 4) {
+    F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
+  } else {
+    F.Xn[0][n] = x.x; F.Xn[1][n] = x.y; F.Xn[2][n] = x.z;
+  }
+}
+
+// sans-lagrange, cells: after the geometry pass (body_lagrange_geom), only
+// computeVariablesForRemap (PrepareRemap.cc:94-193): the density, energy
+// and pseudo-viscosity keep their values (updateDensity,
+// computeArtificialViscosity and updateEnergyAndPressure return at once),
+// the volumes are the new ones (a mixed cell's environment volume its
+// fraction of the cell's, computeGeometricValues)
+template <int DIM, int NE>
+__device__ __forceinline__ void body_advect_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long c = bx * (long long)CT + threadIdx.x;
+  if (c >= M.ncell) return;
+  const long long N = M.ncell;
+  constexpr int NV = 3 * NE + 1;
+  const double V = F.V[c];
+  const uint8_t mask = F.mask[c];
+  const bool pure = __popc(mask) == 1;
+  double* U = F.U[0];
+  for (int q = 0; q < NE; ++q) {
+    const bool in = (mask >> q) & 1;
+    double Vq = 0., rq = 0., eq = 0.;
+    if (in) {
+      const bool slot = NE > 1 && !pure;
+      Vq = slot ? F.ef[q * N + c] * V : V;
+      rq = slot ? F.erho[q * N + c] : F.rho[c];
+      eq = slot ? F.ee[q * N + c] : F.e[c];
+      if (F.phi_pb) {
+        F.phi_pb[(NE + q) * N + c] = rq;
+        F.phi_pb[(2 * NE + q) * N + c] = eq;
+      }
+    }
+    U[q * N + c] = Vq;
+    U[(NE + q) * N + c] = in ? Vq * rq : 0.;
+    U[(2 * NE + q) * N + c] = in ? Vq * rq * eq : 0.;
+  }
+  const double qg = F.q[c];
+  U[(NV - 1) * N + c] = V * qg;
+  if (F.phi_pb) F.phi_pb[(NV - 1) * N + c] = qg;
+}
+
 // The remap sweeps (one direction, cells and nodes) live in mhc_sweep.cuh.
 
 // ---------------------------------------------------------------------------
@@ -1298,7 +1468,11 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
 // then applyEOS per environment and computePressionMoyenne
 // (PrepareRemap.cc:242-249, MahycoModule.cc:1708-1735)
 // ---------------------------------------------------------------------------
-template <int DIM, int NE>
+// ADV: sans-lagrange (no dual projection): a cell keeps an environment
+// whose projected mass is zero, the pressure and sound speed of a mixed
+// cell are not averaged (computePressionMoyenne returns at once), and the
+// Fictif equation of state applies
+template <int DIM, int NE, bool ADV>
 __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const mhc_case_params& P, const Fields& F,
                                                           const double* Ufin, const double* Udfin, int bx) {
   long long c = bx * (long long)CT + threadIdx.x;
@@ -1313,7 +1487,7 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   uint8_t nm = old;
   for (int q = 0; q < NE; ++q) {
     bool in = (old >> q) & 1;
-    if ((div_rn(u[q], Veul) < thr || (u[NE + q] == 0.)) && in) {
+    if ((div_rn(u[q], Veul) < thr || (u[NE + q] == 0. && !ADV)) && in) {
       nm &= (uint8_t)~(1 << q);
     } else if (div_rn(u[q], Veul) > thr && !in) {
       double volt = 0.;
@@ -1455,10 +1629,28 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   for (int q = 0; q < NE; ++q) { pe[q] = ce[q] = 0.; }
   for (int q = 0; q < NE; ++q) {
     if (!((nm >> q) & 1)) continue;
+    if (ADV && P.env[q].eos == MHC_EOS_FICTIF) {
+      // the environment's pressure before: its slot value carried through
+      // the membership change (a new environment of a mixed cell starts
+      // from 0, a pure cell's global slot keeps its value)
+      const bool was = (old >> q) & 1;
+      double p_old;
+      if (pure) p_old = (was && !oldpure && NE > 1) ? F.ep[q * N + c] : F.p[c];
+      else p_old = was ? (oldpure ? F.p[c] : F.ep[q * N + c]) : 0.;
+      const double t = F.s->t;
+      if (pure) { fictif_apply(P.env[q], t, p_old, pg, cg); eg = 0.; }
+      else { fictif_apply(P.env[q], t, p_old, pe[q], ce[q]); ee[q] = 0.; }
+      continue;
+    }
     if (pure) eos_apply(P.env[q], rhog, eg, pg, cg);
     else eos_apply(P.env[q], rhoe[q], ee[q], pe[q], ce[q]);
   }
-  if (!pure) {
+  if (!pure && ADV) {
+    // no pressure average without Lagrange phase (MahycoModule.cc:1711)
+    pg = F.p[c];
+    cg = F.c[c];
+  }
+  if (!pure && !ADV) {
     pg = 0.; cg = 0.;
     double option = P.calcul_vitson_max ? 1. : 0.;
     for (int q = 0; q < NE; ++q) {
@@ -1496,6 +1688,12 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
       F.erho[q * N + c] = rhoe[q]; F.ee[q * N + c] = ee[q]; F.ep[q * N + c] = pe[q];
       F.ec[q * N + c] = ce[q]; F.eq[q * N + c] = qe[q];
     }
+  } else if (NE > 1) {
+    // a pure cell's volume fraction, the normalised one of the reference
+    // (m_fracvol of the cell, which can end an ulp below 1); only read
+    // back, in the environment's slot
+    for (int q = 0; q < NE; ++q)
+      if ((nm >> q) & 1) F.ef[q * N + c] = fg;
   }
 }
 
@@ -1658,12 +1856,14 @@ __device__ __forceinline__ void body_euler_axis_reset(const Mesh& M, const mhc_c
 
 // remap finalize, nodes: velocity from projected momentum and node mass
 // rebuilt from the new cell masses (RemapADIFinal.cc:287-319)
-template <int DIM>
+// DUAL: the dual projection ran (not with sans-lagrange, whose velocities
+// stay prescribed)
+template <int DIM, bool DUAL>
 __device__ __forceinline__ void body_remap_finalize_nodes(const Mesh& M, const Fields& F, const double* Ud, int bx) {
   long long n = bx * (long long)CT + threadIdx.x;
   if (n >= M.nnode) return;
   const long long NN = M.nnode;
-  double m = Ud[3 * NN + n];
+  double m = DUAL ? Ud[3 * NN + n] : 0.;
   if (m != 0.) {
     F.vx[n] = div_rn(Ud[n], m);
     F.vy[n] = div_rn(Ud[NN + n], m);
@@ -1721,15 +1921,20 @@ __device__ __forceinline__ void body_eos_apply(const Mesh& M, const mhc_case_par
   const uint8_t mask = F.mask[c];
   if (!((mask >> env) & 1)) return;
   const bool pure = __popc(mask) == 1;
+  const mhc_env_params& o = P.env[env];
+  const bool fictif = o.eos == MHC_EOS_FICTIF;
   if (pure) {
     double p, cs;
-    eos_apply(P.env[env], F.rho[c], F.e[c], p, cs);
+    if (fictif) { fictif_apply(o, F.s->t, F.p[c], p, cs); F.e[c] = 0.; }
+    else eos_apply(o, F.rho[c], F.e[c], p, cs);
     F.p[c] = p; F.c[c] = cs;
     return;
   }
   double p, cs;
-  eos_apply(P.env[env], F.erho[env * N + c], F.ee[env * N + c], p, cs);
+  if (fictif) { fictif_apply(o, F.s->t, F.ep[env * N + c], p, cs); F.ee[env * N + c] = 0.; }
+  else eos_apply(o, F.erho[env * N + c], F.ee[env * N + c], p, cs);
   F.ep[env * N + c] = p; F.ec[env * N + c] = cs;
+  if (P.sans_lagrange) return;  // no pressure average (MahycoModule.cc:1711)
   double option = P.calcul_vitson_max ? 1. : 0.;
   double pg = 0., cg = 0.;
   for (int q = 0; q < NE; ++q) {
@@ -1747,7 +1952,7 @@ __device__ __forceinline__ void body_delta_t_finalize(const mhc_case_params& P, 
   Scalars* s = F.s;
   double old = s->dt;
   double new_dt;
-  if (P.deltat_constant) {
+  if (P.sans_lagrange || P.deltat_constant) {
     new_dt = P.deltat_init;
   } else {
     double minimum_aux = __longlong_as_double((long long)s->dt_min_bits);

@@ -370,7 +370,7 @@ kb_sweep_nodes(const CaseDesc* __restrict__ C, PhaseList L, int k) {
 #define MHC_FIN_MIN_BLOCKS 3
 #endif
 
-template <int DIM, int NE>
+template <int DIM, int NE, bool ADV = false>
 __global__ void __launch_bounds__(CT, MHC_FIN_MIN_BLOCKS) kb_remap_finalize_cells(const CaseDesc* __restrict__ C, PhaseList L, int K) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
@@ -378,12 +378,12 @@ __global__ void __launch_bounds__(CT, MHC_FIN_MIN_BLOCKS) kb_remap_finalize_cell
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_remap_finalize_cells<DIM, NE>(M, *C[wi.c].P, F, (K & 1) ? F.U[1] : F.U[0],
-                                       ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
+    body_remap_finalize_cells<DIM, NE, ADV>(M, *C[wi.c].P, F, (K & 1) ? F.U[1] : F.U[0],
+                                            ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
   }
 }
 
-template <int DIM>
+template <int DIM, bool DUAL = true>
 __global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __restrict__ C, PhaseList L, int K) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_NODES>(C, L, w_);
@@ -391,7 +391,33 @@ __global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_remap_finalize_nodes<DIM>(M, F, ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
+    body_remap_finalize_nodes<DIM, DUAL>(M, F, ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
+  }
+}
+
+// sans-lagrange (pure advection): prescribed node velocities and positions,
+// then the remap quantities of the cells (after kb_lagrange_geom)
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_advect_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_advect_nodes<DIM>(M, *C[wi.c].P, F, wi.x);
+  }
+}
+
+template <int DIM, int NE>
+__global__ void __launch_bounds__(CT) kb_advect_cells(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_advect_cells<DIM, NE>(M, *C[wi.c].P, F, wi.x);
   }
 }
 

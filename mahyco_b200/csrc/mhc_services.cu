@@ -47,14 +47,23 @@ __global__ void __launch_bounds__(CT) kb_eos_init_env(const CaseDesc* __restrict
 }
 
 // applyOneCellEOS on one cell: pressure and sound speed in place, dp/de out
+// (Fictif, FictifEOSService.cc:82-104: the pressure of the time, the
+// internal energy reset to 0)
 __global__ void kb_eos_one_cell(Fields F, mhc_env_params o, long long N, long long c, int env, int pure,
                                 double* dpde_out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const long long k = pure ? c : env * N + c;
   const double rho = pure ? F.rho[k] : F.erho[k], e = pure ? F.e[k] : F.ee[k];
   double p, cs, p2, dpde;
-  eos_apply(o, rho, e, p, cs);
-  eos_one_cell(o, rho, e, p2, dpde);
+  if (o.eos == MHC_EOS_FICTIF) {
+    fictif_apply(o, F.s->t, pure ? F.p[k] : F.ep[k], p, cs);
+    dpde = (o.adiabatic_cst - 1.) * rho;
+    if (pure) F.e[k] = 0.;
+    else F.ee[k] = 0.;
+  } else {
+    eos_apply(o, rho, e, p, cs);
+    eos_one_cell(o, rho, e, p2, dpde);
+  }
   if (pure) { F.p[k] = p; F.c[k] = cs; }
   else { F.ep[k] = p; F.ec[k] = cs; }
   *dpde_out = dpde;
@@ -74,6 +83,7 @@ __global__ void __launch_bounds__(CT) kb_eos_damage_test(const CaseDesc* __restr
     const long long c = wi.x * (long long)CT + threadIdx.x;
     if (c >= N || !((F.mask[c] >> env) & 1)) continue;
     const mhc_env_params& o = C[wi.c].P->env[env];
+    if (o.eos == MHC_EOS_FICTIF) continue;  // FictifEOSService::Endommagement does nothing
     const bool density_test = o.eos != MHC_EOS_MIE_GRUNEISEN && F.rho[c] < 0.;
     if (F.p[c] < o.tension_damage_thresold || density_test) atomicOr(&F.s->status, MHC_ST_DAMAGE);
   }
@@ -106,7 +116,9 @@ int check_remap_args(mhc_case* h, int dimension, int with_dual, int nvars, int n
   if (!h) return set_err(MHC_ERR_ARG, "null case");
   if (dimension != h->DIM) return set_err(MHC_ERR_ARG, "dimension differs from the case's");
   if (nenv != h->NE) return set_err(MHC_ERR_ARG, "nb_env differs from the case's");
-  if (with_dual != 1) return set_err(MHC_ERR_UNSUPPORTED, "withDualProjection must be 1");
+  // the module passes withDualProjection = 1, 0 without Lagrange phase (PrepareRemap.cc:211)
+  if (with_dual != (h->P.sans_lagrange ? 0 : 1))
+    return set_err(MHC_ERR_ARG, "withDualProjection must be 1 (0 with sans-lagrange)");
   if (nvars != 18 * nenv && nvars != 3 * nenv + 5)
     return set_err(MHC_ERR_ARG, "nb_vars_to_project must be 18 nb_env or 3 nb_env + 5");
   return MHC_OK;
@@ -155,6 +167,7 @@ void mhc_case_params_default(mhc_case_params* p) {
   p->is_euler_scheme = MHC_EULER_FULL;
   p->remap_threshold = 1.e-10;
   p->time_history_period = 10;
+  p->rider_radius = 0.15;
 }
 
 // ---------------------------------------------------------------------------
@@ -196,11 +209,13 @@ long long mhc_set_field(mhc_case* h, const char* name, int env, const double* ho
       e.resize(N);
       if ((r = fetch_shared(st, c.e + env * N, e.data(), N * 8))) return r;
     }
+    // a pure cell's volume fraction lives in its environment's slot
+    const bool fracvol = !strcmp(name, "FracVol");
     for (long long i = 0; i < N; ++i) {
       if (!((mask[i] >> env) & 1)) continue;
       const bool pure = __builtin_popcount(mask[i]) == 1;
       if (pure && c.g) g[i] = host[i];
-      else if (!pure && env_array) e[i] = host[i];
+      else if ((!pure || fracvol) && env_array) e[i] = host[i];
     }
     if (c.g && (r = upload(st, c.g, g.data(), N * 8))) return r;
     if (env_array && (r = upload(st, c.e + env * N, e.data(), N * 8))) return r;

@@ -689,13 +689,15 @@ __device__ __forceinline__ void body_sweep_cells_pb(const Mesh& M, const Fields&
     if (v >= NE && v < 2 * NE) dual[v - NE] = du;
   }
   if (!out) return;
-  // truncation of tiny volumes, masses and energies, then the clip of
+  // truncation of tiny volumes, masses and energies (with the dual
+  // projection only, not in a sans-lagrange advection), then the clip of
   // negative masses and energies
+  const bool trunc = !P.sans_lagrange;
 #pragma unroll
   for (int q = 0; q < NE; ++q) {
-    if (uo[q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
-    if (uo[NE + q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
-    if (uo[2 * NE + q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
+    if (trunc && uo[q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
+    if (trunc && uo[NE + q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
+    if (trunc && uo[2 * NE + q] < 1. * thr) { uo[q] = 0.; uo[NE + q] = 0.; uo[2 * NE + q] = 0.; }
     if (uo[NE + q] < 0.) uo[NE + q] = 0.;
     if (uo[2 * NE + q] < 0.) uo[2 * NE + q] = 0.;
   }

@@ -69,6 +69,7 @@ void sweep_step_dn(Engine* e, Group& g, int D, int k) {
     case LIM_PB: cell_sweep<DIM, NE, LIM_PB>(e, g, D, k); break;
     default: cell_sweep<DIM, NE, LIM_ORDER1>(e, g, D, k); break;
   }
+  if (g.ADV) return;  // sans-lagrange: no dual projection (PrepareRemap.cc:211)
   const int nl = ((g.NCOLS >> D) & 1) ? LIM_COLS + g.LIM : g.LIM;
   if (D > 0 && !((g.NCOLS >> D) & 1) && ((g.NTILE >> D) & 1)) {
     switch (g.LIM) {

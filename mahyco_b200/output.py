@@ -10,7 +10,9 @@ NONREGRESSION/launch_test.sh:74-96) applies unchanged:
   line per period-th iteration, 17 significant digits;
 * Ensight gold ASCII of the final state (Arcane's post-processing service):
   ``output/depouillement/ensight.case``, ``ensight.geo/ensight.geo000000``
-  and ``<Variable>/<Variable>000000``, values with 6 significant digits.
+  and ``<Variable>/<Variable>000000``, values with 6 significant digits;
+  with ``save-init`` the initial state is step 000000 and the final one
+  step 000001.
 """
 from __future__ import annotations
 
@@ -66,8 +68,13 @@ def materiau(h) -> np.ndarray:
     return out
 
 
-def write_ensight(h, out_dir: str, variables: list[str], time: float) -> list[str]:
-    """Ensight gold ASCII files of the current state of case ``h``."""
+def write_ensight(h, out_dir: str, variables: list[str], time: float, step: int = 0,
+                  times: list[float] | None = None) -> list[str]:
+    """Ensight gold ASCII files of the current state of case ``h`` as time
+    step ``step``; ``times`` (default ``[time]``) are the time values of
+    every step written so far, listed in ensight.case."""
+    times = [time] if times is None else times
+    sfx = f"{step:06d}"
     p: CaseParams = h.params
     d = os.path.join(out_dir, "depouillement")
     os.makedirs(os.path.join(d, "ensight.geo"), exist_ok=True)
@@ -101,7 +108,7 @@ def write_ensight(h, out_dir: str, variables: list[str], time: float) -> list[st
            "part\n", f"{1:10d}\n", "AllCells\n", "coordinates\n", f"{nn:10d}\n",
            _values(xs), _values(ys), _values(zs), f"{etype}\n", f"{h.ncell:10d}\n",
            "".join("".join(f"{v:10d}" for v in row) + "\n" for row in conn)]
-    fn = os.path.join(d, "ensight.geo", "ensight.geo000000")
+    fn = os.path.join(d, "ensight.geo", "ensight.geo" + sfx)
     with open(fn, "w") as f:
         f.writelines(geo)
     written.append(fn)
@@ -122,14 +129,14 @@ def write_ensight(h, out_dir: str, variables: list[str], time: float) -> list[st
             text = f"{var}\npart\n{1:10d}\n{etype}\n" + _values(a)
             entries.append(f"scalar per element:    1   {var} {var}/{var}******\n")
         os.makedirs(os.path.join(d, var), exist_ok=True)
-        fn = os.path.join(d, var, f"{var}000000")
+        fn = os.path.join(d, var, f"{var}{sfx}")
         with open(fn, "w") as f:
             f.write(text)
         written.append(fn)
     case = ["FORMAT\n", "type: ensight gold\n", "\n", "GEOMETRY\n", "model: 1 ensight.geo/ensight.geo******\n",
             "\n", "VARIABLE\n", *entries, "\n", "TIME\n", "time set:              1\n",
-            "number of steps:       1\n", "filename start number: 0\n", "filename increment:    1\n",
-            "time values:\n", f"{time:.15g}\n", "\n"]
+            f"number of steps:       {len(times)}\n", "filename start number: 0\n", "filename increment:    1\n",
+            "time values:\n", *(f"{t:.15g}\n" for t in times), "\n"]
     fn = os.path.join(d, "ensight.case")
     with open(fn, "w") as f:
         f.writelines(case)
@@ -147,12 +154,16 @@ def run_arc(arc_path: str, out_dir: str, max_iter: int = 10 ** 7) -> dict:
 
 def run_case(p: CaseParams, info: dict, out_dir: str, max_iter: int = 10 ** 7) -> dict:
     """run_arc on parameters already read (``info``: env_names and,
-    optionally, output_vars and history_vars as read_arc returns them)."""
+    optionally, output_vars, history_vars and save_init as read_arc returns
+    them)."""
     from . import Hydro, ST_STOP
     period = p.time_history_period if p.time_history_period > 0 else 10
     h = Hydro(p)
     try:
         h.hydroStartInit()
+        init_files = []
+        if info.get("save_init"):
+            init_files = write_ensight(h, out_dir, info.get("output_vars", []), 0.0)
         rows = []
         it = 0
         st = 0
@@ -168,7 +179,11 @@ def run_case(p: CaseParams, info: dict, out_dir: str, max_iter: int = 10 ** 7) -
                 break
         s = h.scalars()
         files = write_gnuplot(out_dir, info["env_names"], np.array(rows), info.get("history_vars", HISTORY_VARS))
-        files += write_ensight(h, out_dir, info.get("output_vars", []), s["time"])
+        if info.get("save_init"):
+            files += init_files + write_ensight(h, out_dir, info.get("output_vars", []), s["time"], 1,
+                                                [0.0, s["time"]])
+        else:
+            files += write_ensight(h, out_dir, info.get("output_vars", []), s["time"])
         return {"scalars": s, "files": files}
     finally:
         h.close()

@@ -346,6 +346,11 @@ static void eos_init(Case& C, int env) {
       double g = o.adiabatic_cst, pinf = o.limit_tension;
       C.EV(C.internal_energy, env, c) = (p + (g * pinf)) / ((g - 1.) * rho);
       C.EV(C.sound_speed, env, c) = std::sqrt((g / rho) * (p + pinf));
+    } else if (o.eos == MHC_EOS_FICTIF) {
+      /* FictifEOSService.cc:12-34 (the temperature is not carried) */
+      double g = o.adiabatic_cst;
+      C.EV(C.internal_energy, env, c) = p / ((g - 1.) * rho);
+      C.EV(C.sound_speed, env, c) = std::sqrt(g * p / rho);
     } else {
       /* MieGruneisenEOSService.cc:12-34 */
       C.EV(C.internal_energy, env, c) = C.EV(C.pressure, env, c) / o.gamma0;
@@ -376,6 +381,15 @@ static void eos_apply(Case& C, int env) {
       C.EV(C.pressure, env, c) = p;
       C.EV(C.sound_speed, env, c) = std::sqrt((g / rho) * (p + pinf));
       C.EV(C.dpde, env, c) = (g - 1.) * rho;
+    } else if (o.eos == MHC_EOS_FICTIF) {
+      /* FictifEOSService.cc:44-78: the pressure a function of the time
+       * only, the internal energy reset to zero */
+      double g = o.adiabatic_cst;
+      if (C.t > o.fictif_tdebut) C.EV(C.pressure, env, c) = o.fictif_p0 + o.fictif_dpdt * C.t;
+      if (C.t > o.fictif_tfin) C.EV(C.pressure, env, c) = 0.;
+      C.EV(C.sound_speed, env, c) = 1.;
+      C.EV(C.dpde, env, c) = (g - 1.) * rho;
+      C.EV(C.internal_energy, env, c) = 0.;
     } else {
       double J = o.rho0 / rho;
       double mu = 1. / J - 1.;
@@ -486,6 +500,54 @@ static void cell_centres(Case& C) {
  * taken from the bubble's centre and per cell (the reference measures them
  * from the origin and keeps the extremes across cells, which only agrees
  * for a bubble at the origin). */
+/* RIDERService (casTest/RIDER/RIDERService.cc): centre of the disc
+ * (Xb, lines 27-30 and 76-79), node-distance range of a cell to it
+ * (rmin / rmax, lines 36-45), and the velocity field of the test (lines
+ * 141-172 and 255-285).  Pi is TypesMahyco.h:42's 3.14159265359. */
+static const double kPi = 3.14159265359;
+static bool rider_mono(const mhc_case_params& P) { return P.cas_test >= 23 && P.cas_test <= 30; }
+static R3 rider_centre(const mhc_case_params& P) {
+  const int first_rotation = rider_mono(P) ? 26 : 34;
+  return P.cas_test < first_rotation ? R3{0.20, 0.20, 0.} : R3{0.50, 0.75, 0.};
+}
+static void rider_range(const Case& C, long c, R3 xb, double& rmin, double& rmax) {
+  rmin = 10.;
+  rmax = 0.;
+  for (int l = 0; l < C.nbn; ++l) {
+    const R3 x = C.coord[C.cnode(c, l)];
+    const double rn = std::sqrt((x.x - xb.x) * (x.x - xb.x) + (x.y - xb.y) * (x.y - xb.y));
+    rmin = std::min(rmin, rn);
+    rmax = std::max(rmax, rn);
+  }
+}
+static R3 rider_velocity(const mhc_case_params& P, R3 x) {
+  const int kind = (P.cas_test - 23) % 8;  /* Tx Ty T45 Rotation Vortex Deformation VortexR DeformationR */
+  const R3 cc = {0.5, 0.5, 0.};
+  R3 v = {0.0, 0.0, 0.0};
+  if (kind == 0) v.x = 1.;
+  if (kind == 1) v.y = 1.;
+  if (kind == 2) v = {1.0, 1.0, 0.0};
+  if (kind == 3) {
+    const R3 dd = x - cc;
+    const double theta = std::atan2(dd.y, dd.x);
+    const double r = std::sqrt(dd.x * dd.x + dd.y * dd.y);
+    const double omega = 4. * kPi;
+    v.x = -r * omega * std::sin(omega * 0. + theta);
+    v.y = r * omega * std::cos(omega * 0. + theta);
+  }
+  if (kind == 4 || kind == 6) {
+    const R3 dd = x;
+    v.x = -2. * std::cos(kPi * dd.y) * std::sin(kPi * dd.y) * std::sin(kPi * dd.x) * std::sin(kPi * dd.x);
+    v.y = 2. * std::cos(kPi * dd.x) * std::sin(kPi * dd.x) * std::sin(kPi * dd.y) * std::sin(kPi * dd.y);
+  }
+  if (kind == 5 || kind == 7) {
+    const R3 dd = x + cc;
+    v.x = std::sin(4. * kPi * dd.x) * std::sin(4. * kPi * dd.y);
+    v.y = std::cos(4. * kPi * dd.x) * std::cos(4. * kPi * dd.y);
+  }
+  return v;
+}
+
 static double bubble_material(const Case& C, long c, double& fbub) {
   const mhc_case_params& P = C.P;
   double mat = 0.;
@@ -545,6 +607,14 @@ static void init_materials(Case& C) {
     } else if (P.cas_model == MHC_CASE_BUBBLES && C.nenv > 1) {
       double f;
       m = bubble_material(C, c, f);
+    } else if (P.cas_model == MHC_CASE_RIDER && !rider_mono(P)) {
+      /* RIDERService::initMat (RIDERService.cc:18-57); MonoRider*: initMatMono */
+      double rmin, rmax;
+      rider_range(C, c, rider_centre(P), rmin, rmax);
+      const double rb = P.rider_radius;
+      m = 0;
+      if (rmax < rb) m = 1;
+      else if ((rmax >= rb) && (rmin < rb)) m = (rb - rmin) / (rmax - rmin);
     }
     C.materiau[c] = m;
     uint8_t mask = 0;
@@ -622,6 +692,52 @@ static void init_variables(Case& C) {
       }
     }
     for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
+  } else if (P.cas_model == MHC_CASE_RIDER) {
+    /* RIDERService::initVar / initVarMono (RIDERService.cc:62-173, 178-289) */
+    const bool mono = rider_mono(P), lin = P.rider_linear_density != 0;
+    const R3 xb = rider_centre(P);
+    const double rb = P.rider_radius;
+    const double croissance = lin ? 1. / rb : 1.;
+    const double d0 = P.env[0].densite_initiale, d1 = P.env[C.nenv > 1 ? 1 : 0].densite_initiale;
+    const double p0 = P.env[0].pression_initiale, p1 = P.env[C.nenv > 1 ? 1 : 0].pression_initiale;
+    for (long c = 0; c < C.ncell; ++c) {
+      double rmin, rmax;
+      rider_range(C, c, xb, rmin, rmax);
+      C.density.g[c] = d0;
+      C.pressure.g[c] = p0;
+      C.internal_energy.g[c] = P.env[0].energie_initiale;
+      const R3 cc = C.cell_coord[c];
+      const double r = std::sqrt((cc.x - xb.x) * (cc.x - xb.x) + (cc.y - xb.y) * (cc.y - xb.y));
+      const double r_cell = lin ? r : rmax;
+      if (r_cell < rb) {
+        C.density.g[c] = d1;
+        if (lin) C.density.g[c] = d1 * std::min(croissance * 2 * (rb - r), 1.);
+        C.pressure.g[c] = p1;
+      } else if ((rmax >= rb) && (rmin < rb) && !lin) {
+        const double frac_b = (rb - rmin) / (rmax - rmin);
+        if (!mono) {
+          /* the first environment takes the disc's density and fraction */
+          for (int e = 0; e < C.nenv; ++e) {
+            if (!C.has(c, e)) continue;
+            if (e == 0) {
+              C.EV(C.density, e, c) = d1;
+              C.EV(C.fracvol, e, c) = frac_b;
+              C.EV(C.mass_fraction, e, c) = frac_b;
+            }
+            if (e == 1) {
+              C.EV(C.density, e, c) = d0;
+              C.EV(C.fracvol, e, c) = 1. - frac_b;
+              C.EV(C.mass_fraction, e, c) = 1. - frac_b;
+            }
+            C.EV(C.pressure, e, c) = 0.;
+          }
+        }
+        C.density.g[c] = frac_b * d1;
+        C.pressure.g[c] = p1;
+      }
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = rider_velocity(P, C.coord[n]);
+    C.vel_n = C.vel;
   } else if (P.cas_model == MHC_CASE_ONECELL) {
     /* ONECELLService::initVarMono: the first environment's state everywhere,
      * nodes at rest */
@@ -773,9 +889,12 @@ static int hydro_start_init(Case& C) {
   C.pseudo.fill(0.0);
   C.internal_energy_n.fill(0.0);
   init_variables(C);
-  for (int e = 0; e < C.nenv; ++e) eos_init(C, e);
+  /* no equation of state and no mixed-cell averages at the start of a
+   * sans-lagrange run (MahycoModule.cc:143-171) */
+  if (!C.P.sans_lagrange)
+    for (int e = 0; e < C.nenv; ++e) eos_init(C, e);
   for (long c = 0; c < C.ncell; ++c) {
-    if (C.pure(c)) continue;
+    if (C.pure(c) || C.P.sans_lagrange) continue;
     C.internal_energy.g[c] = 0.;
     for (int e = 0; e < C.nenv; ++e) {
       if (!C.has(c, e)) continue;
@@ -831,8 +950,21 @@ static void save_values_at_n(Case& C) {
   cp(C.density_n, C.density);
   cp(C.internal_energy_n, C.internal_energy);
   C.cqs_n = C.cqs;
-  C.vel_n = C.vel;
+  /* sans-lagrange: the velocities at n stay those of the initialisation */
+  if (!C.P.sans_lagrange) C.vel_n = C.vel;
   C.sdev_n = C.sdev;
+}
+
+/* MahycoModule::updateVelocityWithoutLagrange (MahycoModule.cc:676-700):
+ * the velocities at n, times cos(Pi t parameter) with the reverse option */
+static void update_velocity_without_lagrange(Case& C) {
+  const double option_real = (double)(C.P.cas_model == MHC_CASE_RIDER && C.P.rider_reverse);
+  const double factor = C.P.cas_model == MHC_CASE_RIDER ? C.P.rider_parameter : 0.;
+  for (long n = 0; n < C.nnode; ++n) {
+    const R3 v = C.vel_n[n];
+    const double cs = std::cos(kPi * C.t * factor);
+    C.vel[n] = v * (1. - option_real) + option_real * v * cs;
+  }
 }
 
 /* MahycoModule::updateVelocity (MahycoModule.cc:438-562): pressure forces
@@ -1022,7 +1154,17 @@ static void apply_pressure_bcs(Case& C) {
 
 /* MahycoModule::updatePosition (MahycoModule.cc:730-751) */
 static void update_position(Case& C) {
-  for (long n = 0; n < C.nnode; ++n) C.coord[n] += C.dt * C.vel[n];
+  for (long n = 0; n < C.nnode; ++n) {
+    if (C.P.sans_lagrange) {
+      /* only the nodes shared by exactly four cells move (MahycoModule.cc:737) */
+      int i, j, k;
+      C.nijk(n, i, j, k);
+      int nc = ((i > 0) + (i < C.ncx)) * ((j > 0) + (j < C.ncy));
+      if (C.dim == 3) nc *= (k > 0) + (k < C.ncz);
+      if (nc != 4) continue;
+    }
+    C.coord[n] += C.dt * C.vel[n];
+  }
   cell_centres(C);
 }
 
@@ -1174,6 +1316,7 @@ static void update_elasticity_and_plasticity(Case& C) {
 
 /* MahycoModule::computePressionMoyenne (MahycoModule.cc:1708-1735) */
 static void compute_pression_moyenne(Case& C) {
+  if (C.P.sans_lagrange) return;  /* MahycoModule.cc:1711 */
   double option = C.P.calcul_vitson_max ? 1. : 0.;
   for (long c = 0; c < C.ncell; ++c) {
     if (C.pure(c)) continue;
@@ -1781,7 +1924,7 @@ static void compute_uremap(Case& C, int d) {
     double* u = &C.u_lag[c * nv];
     for (int iv = 0; iv < C.nproj(); ++iv) u[iv] -= flux_face[iv];
     const double thr = C.P.remap_threshold;
-    if (C.P.projection_pente_borne) {
+    if (C.P.projection_pente_borne && !C.P.sans_lagrange) {
       /* truncation of tiny projected volumes, masses and energies
        * (RemapADIService.cc:440-462, with the dual projection) */
       for (int e = 0; e < ne; ++e) {
@@ -1924,7 +2067,7 @@ static void compute_dual_uremap(Case& C, int d) {
 static int remap_variables(Case& C) {
   const int ne = C.nenv, nv = C.nvars;
   const double thr = C.P.remap_threshold;
-  const bool with_dual = true;
+  const bool with_dual = !C.P.sans_lagrange;  /* PrepareRemap.cc:211 */
   /* environment membership update: the add / remove criteria of one
    * environment only read that environment's membership, so the new masks
    * are computed first and the storage transfer is applied once per cell */
@@ -2051,7 +2194,7 @@ static int remap_variables(Case& C) {
       if (r != r || ie != ie) { C.status = ST_NAN; return C.status; }
     }
   }
-  for (long n = 0; n < C.nnode; ++n) {
+  for (long n = 0; n < C.nnode && with_dual; ++n) {
     const double* U = &C.u_dual[n * 5];
     double m = U[3];
     if (m != 0.) C.vel[n] = {U[0] / m, U[1] / m, U[2] / m};
@@ -2131,7 +2274,7 @@ static int appli_remap(Case& C) {
     compute_grad_phi_cell(C, d);
     compute_upwind_face_quantities(C, d);
     compute_uremap(C, d);
-    compute_dual_uremap(C, d);
+    if (!C.P.sans_lagrange) compute_dual_uremap(C, d);
   }
   C.sens_projection = (C.sens_projection + 1) % C.dim;
   if (C.P.is_euler_scheme == MHC_EULER_FULL) {
@@ -2165,7 +2308,7 @@ static int compute_delta_t(Case& C) {
   C.old_dt = C.dt;
   C.m_old_deltat = C.old_dt;
   double new_dt;
-  if (C.P.deltat_constant) {
+  if (C.P.sans_lagrange || C.P.deltat_constant) {
     new_dt = C.P.deltat_init;
   } else {
     double minimum_aux = 1.7976931348623157e308;
@@ -2228,14 +2371,20 @@ static int iterate(Case& C) {
   C.iteration += 1;
   C.t = C.t + C.dt;
   save_values_at_n(C);
-  update_velocity(C);
+  if (C.P.sans_lagrange) update_velocity_without_lagrange(C);
+  else update_velocity(C);
   apply_boundary_condition(C);
   update_position(C);
   if (compute_geometric_values(C) != ST_OK) return C.status;
-  update_density(C);
-  compute_artificial_viscosity(C);
-  update_elasticity_and_plasticity(C);
-  update_energy_and_pressure(C);
+  /* updateDensity, computeArtificialViscosity,
+   * updateElasticityAndPlasticity and updateEnergyAndPressure return at
+   * once without Lagrange phase */
+  if (!C.P.sans_lagrange) {
+    update_density(C);
+    compute_artificial_viscosity(C);
+    update_elasticity_and_plasticity(C);
+    update_energy_and_pressure(C);
+  }
   if (remap(C) != ST_OK) return C.status;
   if (compute_delta_t(C) != ST_OK) return C.status;
   time_history_write(C);

@@ -1,9 +1,10 @@
 """Extract golden fixtures from the reference's non-regression data.
 
 Run with the root of a cea-hpc/MaHyCo checkout (the directory holding
-NONREGRESSION/ and src/) as its one required argument:
+NONREGRESSION/ and src/) as its first, required argument, optionally
+followed by the cases to (re)make (all of CASES by default):
 
-    python tests/golden/make_golden.py REFERENCE_ROOT
+    python tests/golden/make_golden.py REFERENCE_ROOT [CASE ...]
 
 For each case below it parses NONREGRESSION/<case>/Donnees.arc with
 mahyco_b200.case.read_arc and stores the resulting parameters plus the
@@ -73,6 +74,26 @@ CASES = {
     # running sum carry 3.7e-12 of rounding (the reference's four per-rank
     # sums 2.5e-13), hence the bound
     "CAS_plaque_demi_euler_Y_depot_Gaussian": {"mpi_ranks": 4, "tol": 1e-11},
+    # sans-lagrange advection of the RIDER discs, Fictif equation of state
+    # (src/CMakeLists.txt: the nsd of each Donnees.arc gives its ranks)
+    "CAS_MonoRiderTx": {},
+    "CAS_MonoRiderTy": {},
+    "CAS_MonoRiderT45": {},
+    "CAS_MonoRiderRotation": {},
+    "CAS_MonoRiderDeformation": {},
+    "CAS_RiderT45": {},
+    "CAS_RiderTx": {"mpi_ranks": 8},
+    "CAS_RiderTy": {"mpi_ranks": 8},
+    "CAS_RiderRotation": {"mpi_ranks": 8},
+    "CAS_RiderDeformation": {"mpi_ranks": 8},
+    "CAS_RiderVortex": {"mpi_ranks": 8},
+    "CAS_MonoRiderVortex": {"mpi_ranks": 8},
+    "CAS_MonoRiderTy_pb_simple_superbee": {"mpi_ranks": 8},
+    "CAS_MonoRiderTy_pb_mixte_superbee_vanleer": {"mpi_ranks": 8},
+    "CAS_RiderVortexTimeReverse": {"mpi_ranks": 8},
+    "CAS_MonoRiderVortexTimeReverse": {"mpi_ranks": 8},
+    "CAS_RiderDeformationTimeReverse": {"mpi_ranks": 8},
+    "CAS_MonoRiderDeformationTimeReverse": {"mpi_ranks": 8},
 }
 # variables the Ensight writer of mahyco_b200.output produces
 ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy", "PseudoViscosity",
@@ -80,8 +101,10 @@ ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "Inte
 VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
 
 
-def main(ref_root):
+def main(ref_root, only=()):
     for case, extra in CASES.items():
+        if only and case not in only:
+            continue
         d = os.path.join(ref_root, "NONREGRESSION", case)
         p, info = read_arc(os.path.join(d, "Donnees.arc"))
         hist = {}
@@ -105,13 +128,13 @@ def main(ref_root):
                     digests[os.path.relpath(full, dep)] = ensight_digest.digest(full)
         out = {"case": case, "params": params_to_dict(p), "env_names": info["env_names"],
                "timeloop": info["timeloop"], "extra": extra, "time_history": hist,
-               "output_vars": info["output_vars"], "ensight_sha256": digests}
+               "output_vars": info["output_vars"], "save_init": info["save_init"], "ensight_sha256": digests}
         with open(os.path.join(HERE, case + ".json"), "w") as f:
             json.dump(out, f, indent=0)
         print(case, {k: len(v) for k, v in hist.items()})
 
 
 if __name__ == "__main__":
-    if len(sys.argv) != 2:
-        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
-    main(sys.argv[1])
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT [CASE ...]")
+    main(sys.argv[1], tuple(sys.argv[2:]))

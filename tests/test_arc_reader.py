@@ -34,8 +34,7 @@ def test_lagrange_loop_disables_remap(tmp_path):
     assert p.with_projection == 0
 
 
-@pytest.mark.parametrize("snippet", ["<schema-csts>1</schema-csts>",
-                                     "<sans-lagrange>true</sans-lagrange>"])
+@pytest.mark.parametrize("snippet", ["<schema-csts>1</schema-csts>"])
 def test_unsupported_options_raise(tmp_path, snippet):
     text = open(ARC).read().replace("<pseudo-centree>0</pseudo-centree>", "<pseudo-centree>0</pseudo-centree>" + snippet)
     f = tmp_path / "u.arc"
@@ -215,3 +214,33 @@ def test_read_chocbulle_lattice(tmp_path):
     f.write_text(text[:start] + block.replace("<nombre-bulles-aleatoires>0", "<nombre-bulles-aleatoires>4") + text[end:])
     with pytest.raises(NotImplementedError):
         read_arc(str(f))
+
+
+def test_rider_fictif_sans_lagrange_options(tmp_path):
+    """A RIDER cas-model (src/casTest/RIDER/RIDER.axl:145-166), Fictif
+    equations of state (src/eos/fictif/FictifEOS.axl:184-196),
+    sans-lagrange and save-init (CAS_*Rider* style)."""
+    from mahyco_b200.case import CASE_RIDER, EOS_FICTIF
+    text = open(ARC).read()
+    start, end = text.index("<cas-model"), text.index("</cas-model>") + len("</cas-model>")
+    block = ("<cas-model name=\"RIDER\"><cas-test>38</cas-test><reverse-option>true</reverse-option>"
+             "<parametre>1.</parametre><rayon-bulle>0.2</rayon-bulle></cas-model>")
+    text = text[:start] + block + text[end:]
+    text = text.replace("<pseudo-centree>0</pseudo-centree>",
+                        "<pseudo-centree>0</pseudo-centree><sans-lagrange>true</sans-lagrange>")
+    text = text.replace("</arcane>", "</arcane><arcane-post-processing><save-init>true</save-init>"
+                                      "</arcane-post-processing>", 1)
+    fictif = ("<eos-model name=\"Fictif\"><tdebut-pression>0.1</tdebut-pression><tfin-pression>10</tfin-pression>"
+              "<valeur-debut-pression>2.</valeur-debut-pression><valeur-dependance-temps>3.</valeur-dependance-temps>")
+    for name in ("PerfectGas", "StiffenedGas"):
+        text = text.replace(f"<eos-model name=\"{name}\">", fictif)
+    f = tmp_path / "rider.arc"
+    f.write_text(text)
+    p, info = read_arc(str(f))
+    assert p.cas_model == CASE_RIDER and p.cas_test == 38 and p.sans_lagrange == 1
+    assert p.rider_reverse == 1 and p.rider_parameter == 1.0 and p.rider_radius == 0.2 and p.rider_linear_density == 0
+    assert info["save_init"] is True
+    for e in range(p.nb_env):
+        o = p.env[e]
+        assert o.eos == EOS_FICTIF
+        assert (o.fictif_tdebut, o.fictif_tfin, o.fictif_p0, o.fictif_dpdt) == (0.1, 10.0, 2.0, 3.0)

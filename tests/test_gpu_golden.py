@@ -59,5 +59,7 @@ def test_gpu_matches_reference_goldens(path):
             ref = np.array(g["time_history"][key])
             ours = th[: len(ref)]
             np.testing.assert_allclose(ours[:, 0], ref[:, 0], rtol=ttol, atol=0)
-            rel = np.abs(ours[:, 1 + 5 * e + q] - ref[:, 1]) / np.abs(ref[:, 1])
+            # curves that stay 0 (the Fictif pressure and energy) must be 0
+            den = np.where(ref[:, 1] == 0.0, 1.0, np.abs(ref[:, 1]))
+            rel = np.abs(ours[:, 1 + 5 * e + q] - ref[:, 1]) / den
             assert rel.max() <= tol, (key, rel.max(), int(rel.argmax()))

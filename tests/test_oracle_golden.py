@@ -39,6 +39,10 @@ def run_oracle(g, cr_pow=False):
 @pytest.mark.parametrize("cr_pow", [False, True], ids=["glibc_pow", "cr_pow"])
 def test_oracle_matches_reference_goldens(path, cr_pow):
     g = json.load(open(path))
+    if cr_pow and g["params"].get("sans_lagrange"):
+        # an advection without Lagrange phase calls no power that reaches
+        # the state (the characteristic length is never read)
+        pytest.skip("no power on the path")
     multi = g["extra"].get("mpi_ranks", 1) > 1
     tol = g["extra"].get("tol", 5e-12 if multi else 1e-13)
     ttol = 1e-13 if multi else 1e-14  # the time: a sum of deltat, per-rank orders move it by ulps
@@ -52,5 +56,7 @@ def test_oracle_matches_reference_goldens(path, cr_pow):
             assert len(th) >= len(ref), (key, len(th), len(ref))
             ours = th[: len(ref)]
             np.testing.assert_allclose(ours[:, 0], ref[:, 0], rtol=ttol, atol=0)
-            rel = np.abs(ours[:, 1 + 5 * e + q] - ref[:, 1]) / np.abs(ref[:, 1])
+            # curves that stay 0 (the Fictif pressure and energy) must be 0
+            den = np.where(ref[:, 1] == 0.0, 1.0, np.abs(ref[:, 1]))
+            rel = np.abs(ours[:, 1 + 5 * e + q] - ref[:, 1]) / den
             assert rel.max() <= tol, (key, rel.max(), int(rel.argmax()))
