@@ -152,7 +152,8 @@ int mhc_scalars_wait(mhc_case* h, int slot, double* time, double* deltat, long l
 /* Named fields (names of src/Mahyco.axl: Density, Pressure, InternalEnergy,
  * SoundSpeed, PseudoViscosity, CellMass, CellVolume, FracVol, MassFraction,
  * CaracteristicLength, EnvMask; nodes: Velocity (x,y,z interleaved),
- * NodeMass, NodeCoord).  env < 0 selects the global cell value, env >= 0
+ * NodeMass, NodeCoord, and VelocityN for sans-lagrange cases: the prescribed
+ * velocities at n).  env < 0 selects the global cell value, env >= 0
  * the environment value (0 where the cell is not in the environment).
  * Returns the number of doubles written, or an error. */
 long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, long long capacity);

@@ -295,7 +295,7 @@ class Hydro:
         """Copy a field to the host: a new array, or `out` (float64,
         contiguous, at least the field's size; page-locked memory is
         written by one direct copy)."""
-        n = 3 * self.nnode if name in ("Velocity", "NodeCoord") else (
+        n = 3 * self.nnode if name in ("Velocity", "VelocityN", "NodeCoord") else (
             self.nnode if name == "NodeMass" else self.ncell)
         if out is None:
             out = np.empty(n, dtype=np.float64)
@@ -494,7 +494,7 @@ class Batch:
 
     def field(self, idx: int, name: str, env: int = -1) -> np.ndarray:
         p = self.params[idx]
-        n = 3 * p.nnode if name in ("Velocity", "NodeCoord") else (p.nnode if name == "NodeMass" else p.ncell)
+        n = 3 * p.nnode if name in ("Velocity", "VelocityN", "NodeCoord") else (p.nnode if name == "NodeMass" else p.ncell)
         out = np.empty(n, dtype=np.float64)
         got = self.lib.mhc_batch_get_field(self.b, int(idx), name.encode(), int(env),
                                            out.ctypes.data_as(C.POINTER(C.c_double)), n)
@@ -568,7 +568,7 @@ class Server:
 
     def fetch(self, ticket: int, name: str, env: int = -1) -> np.ndarray:
         p = self.params[ticket]
-        n = 3 * p.nnode if name in ("Velocity", "NodeCoord") else (p.nnode if name == "NodeMass" else p.ncell)
+        n = 3 * p.nnode if name in ("Velocity", "VelocityN", "NodeCoord") else (p.nnode if name == "NodeMass" else p.ncell)
         out = np.empty(n, dtype=np.float64)
         got = self.lib.mhc_server_fetch(self.s, int(ticket), name.encode(), int(env),
                                         out.ctypes.data_as(C.POINTER(C.c_double)), n)

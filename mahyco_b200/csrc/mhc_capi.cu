@@ -900,11 +900,14 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
     int r = fetch(st, F.mn, host, NN * 8);
     return r ? r : NN;
   }
-  if (!strcmp(name, "Velocity") || !strcmp(name, "NodeCoord")) {
+  const bool vn = !strcmp(name, "VelocityN");
+  if (vn && !F.v0) return set_err(MHC_ERR_ARG, "VelocityN is kept by sans-lagrange cases only");
+  if (!strcmp(name, "Velocity") || !strcmp(name, "NodeCoord") || vn) {
     if (cap < 3 * NN) return set_err(MHC_ERR_ARG, "capacity too small");
     std::vector<double> a(NN), b(NN), c(NN);
     const double *pa, *pb, *pc;
-    if (name[0] == 'V') { pa = F.vx; pb = F.vy; pc = F.vz; }
+    if (vn) { pa = F.v0; pb = F.v0 + NN; pc = F.v0 + 2 * NN; }
+    else if (name[0] == 'V') { pa = F.vx; pb = F.vy; pc = F.vz; }
     else {
       // last Lagrangian positions: X of the last completed iteration
       Scalars s;

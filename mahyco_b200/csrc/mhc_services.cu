@@ -246,12 +246,18 @@ long long mhc_set_field(mhc_case* h, const char* name, int env, const double* ho
     if (n < NN) return set_err(MHC_ERR_ARG, "too few values");
     return (r = upload(st, F.mn, host, NN * 8)) ? r : NN;
   }
-  if (!strcmp(name, "Velocity")) {
+  const bool vn = !strcmp(name, "VelocityN");
+  if (vn && !F.v0) return set_err(MHC_ERR_ARG, "VelocityN is kept by sans-lagrange cases only");
+  if (!strcmp(name, "Velocity") || vn) {
+    // VelocityN: the velocities at n of a sans-lagrange case, which the
+    // node pass prescribes every iteration (m_velocity_n)
     if (n < 3 * NN) return set_err(MHC_ERR_ARG, "too few values");
     std::vector<double> a(NN), b(NN), c(NN);
     for (long long i = 0; i < NN; ++i) { a[i] = host[3 * i]; b[i] = host[3 * i + 1]; c[i] = host[3 * i + 2]; }
-    if ((r = upload(st, F.vx, a.data(), NN * 8)) || (r = upload(st, F.vy, b.data(), NN * 8)) ||
-        (r = upload(st, F.vz, c.data(), NN * 8)))
+    double* d[3] = {F.vx, F.vy, F.vz};
+    if (vn) { d[0] = F.v0; d[1] = F.v0 + NN; d[2] = F.v0 + 2 * NN; }
+    if ((r = upload(st, d[0], a.data(), NN * 8)) || (r = upload(st, d[1], b.data(), NN * 8)) ||
+        (r = upload(st, d[2], c.data(), NN * 8)))
       return r;
     return 3 * NN;
   }

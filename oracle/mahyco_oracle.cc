@@ -2493,11 +2493,12 @@ long oracle_get_field(void* h, const char* name, int env, double* out, long cap)
     for (long n = 0; n < C.nnode; ++n) out[n] = C.node_mass[n];
     return C.nnode;
   }
-  if (!strcmp(name, "Velocity") || !strcmp(name, "NodeCoord") || !strcmp(name, "CellCoord")) {
+  const bool vn = !strcmp(name, "VelocityN");
+  if (!strcmp(name, "Velocity") || !strcmp(name, "NodeCoord") || !strcmp(name, "CellCoord") || vn) {
     bool cc = !strcmp(name, "CellCoord");
     long n_ = cc ? C.ncell : C.nnode;
     if (cap < 3 * n_) return -1;
-    const std::vector<ora::R3>& v = cc ? C.cell_coord : (name[0] == 'V' ? C.vel : C.coord);
+    const std::vector<ora::R3>& v = cc ? C.cell_coord : (vn ? C.vel_n : (name[0] == 'V' ? C.vel : C.coord));
     for (long n = 0; n < n_; ++n) { out[3 * n] = v[n].x; out[3 * n + 1] = v[n].y; out[3 * n + 2] = v[n].z; }
     return 3 * n_;
   }
@@ -2524,9 +2525,11 @@ long oracle_set_field(void* h, const char* name, int env, const double* in, long
     for (long i = 0; i < C.nnode; ++i) C.node_mass[i] = in[i];
     return C.nnode;
   }
-  if (!strcmp(name, "Velocity")) {
+  if (!strcmp(name, "Velocity") || !strcmp(name, "VelocityN")) {
+    /* VelocityN: m_velocity_n, the prescribed velocities of a sans-lagrange run */
     if (n < 3 * C.nnode) return -1;
-    for (long i = 0; i < C.nnode; ++i) C.vel[i] = ora::R3{in[3 * i], in[3 * i + 1], in[3 * i + 2]};
+    std::vector<ora::R3>& v = name[8] == 'N' ? C.vel_n : C.vel;
+    for (long i = 0; i < C.nnode; ++i) v[i] = ora::R3{in[3 * i], in[3 * i + 1], in[3 * i + 2]};
     return 3 * C.nnode;
   }
   return -2;

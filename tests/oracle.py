@@ -85,7 +85,7 @@ class Oracle:
         return self.L.oracle_scalar(self.h, name.encode())
 
     def field(self, name: str, env: int = -1) -> np.ndarray:
-        n = 3 * (self.ncell if name == "CellCoord" else self.nnode) if name in ("Velocity", "NodeCoord", "CellCoord") else (
+        n = 3 * (self.ncell if name == "CellCoord" else self.nnode) if name in ("Velocity", "VelocityN", "NodeCoord", "CellCoord") else (
             self.nnode if name == "NodeMass" else self.ncell)
         out = np.empty(n, dtype=np.float64)
         got = self.L.oracle_get_field(self.h, name.encode(), env, out.ctypes.data_as(C.POINTER(C.c_double)), n)

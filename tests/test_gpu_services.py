@@ -71,6 +71,36 @@ def test_uploaded_state_matches_oracle_bitwise():
 
 
 @pytest.mark.gpu
+def test_uploaded_prescribed_velocities_advect_like_the_oracle():
+    """sans-lagrange: the velocities at n (VelocityN, m_velocity_n) are the
+    ones the node pass prescribes; a host field uploaded over the RIDER
+    translation is advected bit for bit like the oracle's."""
+    from mahyco_b200 import Hydro
+    from mahyco_b200.cases import rider
+    from tests.oracle import Oracle
+    p = rider(31, n=(30, 30, 1))
+    ora = Oracle(p, cr_pow=True)
+    assert ora.init() == 0
+    gpu = Hydro(p)
+    gpu.hydroStartInit()
+    assert np.array_equal(gpu.field("VelocityN"), ora.field("VelocityN"))
+    xyz = ora.field("NodeCoord").reshape(-1, 3)
+    v = np.zeros_like(xyz)
+    v[:, 0], v[:, 1] = -(xyz[:, 1] - 0.5) * 3.0, (xyz[:, 0] - 0.5) * 3.0  # a solid rotation
+    gpu.set_field("VelocityN", v.ravel())
+    ora.set_field("VelocityN", v.ravel())
+    n = 40
+    gpu.cycle(n)
+    assert gpu.synchronize() == 0
+    assert ora.iterate(n) == 0
+    errs = compare(gpu, ora, p.nb_env)
+    errs["VelocityN"] = float(np.max(np.abs(gpu.field("VelocityN") - ora.field("VelocityN"))))
+    gpu.close()
+    bad = {k: v for k, v in errs.items() if v != 0.0}
+    assert not bad, bad
+
+
+@pytest.mark.gpu
 def test_set_field_rejects_read_only_and_mid_iteration():
     import mahyco_b200 as mb
     h = mb.Hydro(_bisod3d())
