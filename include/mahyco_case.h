@@ -220,6 +220,13 @@ typedef struct mhc_case_params {
   double rider_parameter;
   double rider_radius;
   int rider_linear_density;
+  /* schema-csts (Mahyco.axl:396-399), with the remap: the velocities go
+   * back to n-1/2 before the node pass (updateVelocityBackward) and forward
+   * to n+1 before the remap (updateVelocityForward), the ideal-gas energy
+   * update takes the work of the forces at n and n+1 through the corner
+   * normals, and the remap's face velocities are the mean of those at n and
+   * n+1 */
+  int schema_csts;
 } mhc_case_params;
 
 #ifdef __cplusplus

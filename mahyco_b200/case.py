@@ -96,6 +96,7 @@ class CaseParams(C.Structure):
         ("bubbles_radius", C.c_double),
         ("sans_lagrange", C.c_int), ("rider_reverse", C.c_int), ("rider_parameter", C.c_double),
         ("rider_radius", C.c_double), ("rider_linear_density", C.c_int),
+        ("schema_csts", C.c_int),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -207,7 +208,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     Returns ``(params, info)`` where ``info`` holds environment names, the
     time loop, the post-processed and EnvSummation variable lists and
     anything the hot path ignores.  Unsupported options that change the cycle
-    (CSTS scheme, elasto models other than DefaultModel,
+    (elasto models other than DefaultModel,
     super-Gaussian energy deposits, non-velocity boundary conditions) raise
     ``NotImplementedError``.
     """
@@ -333,8 +334,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         p.projection_limiteur_pure_id = _txt(rm, "projection-limiteur-pure-id", 0, int)
         if p.ordre_projection not in (1, 2, 3) or not 0 <= p.projection_limiteur_id <= 7:
             raise NotImplementedError("ordre-projection / projection-limiteur-id out of range")
-    if _txt(m, "schema-csts", False, _bool):
-        raise NotImplementedError("schema-csts")
+    p.schema_csts = int(_txt(m, "schema-csts", False, _bool))
     p.sans_lagrange = int(_txt(m, "sans-lagrange", False, _bool))
     p.pseudo_centree = int(_txt(m, "pseudo-centree", False, _bool))
     p.with_projection = int(_txt(m, "with-projection", True, _bool))

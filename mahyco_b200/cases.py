@@ -480,6 +480,19 @@ PARITY_CASES = {
     "adv3d_rider_ty_pb_mixte_superbee": (lambda: _pb(rider(32, limiter=SUPERBEE), 2, mixte=1), 100),
     "adv3d_rider_t45_layers": (lambda: rider(33, n=(24, 24, 4), L=(1.0, 1.0, 0.4)), 80),
     "adv2d_rider_rotation_fictif_window": (lambda: _fictif_window(rider(34, dim=2, n=(40, 40), L=(1.0, 1.0))), 100),
+    # schema-csts with the remap: velocities taken back to n-1/2 and forward
+    # to n+1, the CSTS ideal-gas energy update, averaged face velocities;
+    # with the explicit pressure, gravity, a stiffened gas, pente-borne
+    "adi2d_bisod_csts": (lambda: _csts(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True, deltat_init=1e-3)), 60),
+    "adi3d_bisod_csts_superbee": (lambda: _csts(sod(dim=3, n=(30, 5, 5), L=(1.0, 0.1, 0.1), bi=True,
+                                                    limiter=SUPERBEE, deltat_init=1e-3)), 50),
+    "adi2d_sedov_csts": (lambda: _csts(sedov(dim=2, n=(24, 24), deltat_init=1e-4)), 80),
+    "adi2d_two_state_csts_explicit_gravity": (lambda: _gravity(_csts(two_state(dim=2, n=(40, 30), left=(1.7, 1.3),
+                                                                               right=(0.2, 0.07), interface=0.41,
+                                                                               deltat_init=1e-3), explicit=1)), 60),
+    "adi2d_water_air_csts": (lambda: _csts(water_air(deltat_init=1e-6)), 60),
+    "adi3d_bisod_z_csts_pb_vanleer": (lambda: _pb(_csts(sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
+                                                            limiter=VANLEER, deltat_init=1e-3)), 2), 50),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
@@ -487,6 +500,17 @@ PARITY_CASES = {
 # cos(Pi t), which CUDA and the oracle's libm round differently
 PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13,
                     "adv3d_rider_deformation_reverse": 1e-12}
+
+
+def _csts(p: CaseParams, explicit: int = 0) -> CaseParams:
+    p.schema_csts = 1
+    p.pression_explicite = explicit
+    return p
+
+
+def _gravity(p: CaseParams) -> CaseParams:
+    p.gravity[:] = (0.0, -0.5, 0.0)
+    return p
 
 
 def _fictif_window(p: CaseParams) -> CaseParams:

@@ -69,7 +69,7 @@ int engine_rebuild(Engine* e) {
     desc[i].P = h->d_params;
   }
   // groups
-  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, int, int, int, int, int, int, int, int>, int> gidx;
   e->groups.clear();
   for (int i = 0; i < nc; ++i) {
     mhc_case* h = e->cases[i];
@@ -83,15 +83,16 @@ int engine_rebuild(Engine* e) {
     sweep_masks(h, e->cell_layout, false, cols, tile);
     sweep_masks(h, e->node_layout, true, ncols, ntile);
     const int cbc = case_cell_bcs(h) ? 1 : 0;
-    const int adv = h->P.sans_lagrange ? 1 : 0;
+    const int adv = h->P.sans_lagrange ? 1 : 0, csts = (h->P.schema_csts && h->P.with_projection) ? 1 : 0;
     auto key = std::make_tuple(h->DIM, h->NE, euler, skip_mask(h), sens, el, hg, lim, clim, cols, ncols, cbc, tile, ntile,
-                               adv);
+                               adv, csts);
     auto it = gidx.find(key);
     if (it == gidx.end()) {
       Group g;
       g.DIM = h->DIM; g.NE = h->NE; g.EULER = euler; g.skip = skip_mask(h); g.it0 = h->it_host;
       g.EL = el; g.HG = hg; g.LIM = lim; g.CLIM = clim; g.COLS = cols; g.NCOLS = ncols; g.CBC = cbc; g.TILE = tile; g.NTILE = ntile;
       g.ADV = adv;
+      g.CSTS = csts;
       gidx[key] = (int)e->groups.size();
       e->groups.push_back(g);
       it = gidx.find(key);
@@ -222,9 +223,9 @@ void launch_init(Engine* e) {
   }
 }
 
-template <int DIM, bool EL, bool HG, bool LAG>
+template <int DIM, bool EL, bool HG, bool LAG, bool CSTS = false>
 void lag_nodes_launch(Engine* e, Group& g) {
-  plaunch(e, kb_lagrange_nodes<DIM, EL, HG, LAG>, CT, 0, g.lag_nodes);
+  plaunch(e, kb_lagrange_nodes<DIM, EL, HG, LAG, CSTS>, CT, 0, g.lag_nodes);
   if (HG) plaunch(e, kb_hourglass<DIM>, CT, 0, g.lag_nodes);
 }
 
@@ -232,7 +233,9 @@ void lag_nodes_launch(Engine* e, Group& g) {
 // runs only (validated at creation)
 template <int DIM>
 void lag_nodes_dispatch(Engine* e, Group& g) {
-  if (g.EULER) {
+  if (g.EULER && g.CSTS) {
+    lag_nodes_launch<DIM, false, false, false, true>(e, g);
+  } else if (g.EULER) {
     lag_nodes_launch<DIM, false, false, false>(e, g);
   } else if (g.EL) {
     if (g.HG) lag_nodes_launch<DIM, true, true, true>(e, g);
@@ -275,6 +278,12 @@ void launch_lagrange_cells(Engine* e) {
       // elasto cases: one environment, Lagrangian (validated at creation)
       if (g.DIM == 2) plaunch(e, kb_lagrange_cells<2, 1, false, true>, CT, 0, g.lag_cells);
       else plaunch(e, kb_lagrange_cells<3, 1, false, true>, CT, 0, g.lag_cells);
+    } else if (g.CSTS) {
+      // CSTS: the cell pass computes the geometry itself (it reads the
+      // corner normals at n first), then the forward velocity update
+      DISPATCH_GROUP(g, (plaunch(e, kb_lagrange_cells<DIM_, NE_, true, false, true>, CT, 0, g.lag_cells)));
+      if (g.DIM == 2) plaunch(e, kb_csts_forward<2>, CT, 0, g.lag_nodes);
+      else plaunch(e, kb_csts_forward<3>, CT, 0, g.lag_nodes);
     } else {
       if (g.DIM == 2) plaunch(e, kb_lagrange_geom<2>, CT, 0, g.lag_cells);
       else plaunch(e, kb_lagrange_geom<3>, CT, 0, g.lag_cells);
@@ -517,7 +526,9 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   int ne = p->nb_env, nv = 3 * ne + 1;
   long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8) +
                     (p->projection_pente_borne ? nv : 0) + 2;  // (+2: boundary-condition energy, pressure)
-  long long nodes = 4 + 6 + 10 + (p->sans_lagrange ? 3 : 0);
+  const bool csts = p->schema_csts && p->with_projection;
+  long long nodes = 4 + 6 + 10 + ((p->sans_lagrange || csts) ? 3 : 0) + (csts ? 3 : 0);
+  if (csts) cells += 1;
   return cells * ncell + nodes * nnode;
 }
 
@@ -559,6 +570,17 @@ int validate(const mhc_case_params* p) {
     // not run here
     if (p->conservation_energie_totale)
       return set_err(MHC_ERR_UNSUPPORTED, "conservation-energie-totale with sans-lagrange");
+    if (p->schema_csts) return set_err(MHC_ERR_UNSUPPORTED, "schema-csts with sans-lagrange");
+  }
+  if (p->schema_csts) {
+    // the CSTS Newton update starts from a pressure the reference never
+    // sets (MahycoModule.cc:1596-1599); without the remap the scheme needs
+    // the pseudo-viscosity at n-1, kept only there; the forward update
+    // reads the cell pressure that the cell-variable conditions replace
+    if (!p->with_projection) return set_err(MHC_ERR_UNSUPPORTED, "schema-csts needs the remap");
+    if (p->with_newton) return set_err(MHC_ERR_UNSUPPORTED, "schema-csts with the Newton energy update");
+    if (cellvars) return set_err(MHC_ERR_UNSUPPORTED, "schema-csts with cell-variable boundary conditions");
+    if (p->is_euler_scheme != MHC_EULER_FULL) return set_err(MHC_ERR_UNSUPPORTED, "schema-csts with a per-axis Euler remap");
   }
   if (p->cas_model == MHC_CASE_BUBBLES && (p->nb_env != 2 || p->bubbles_n[0] < 0 || p->bubbles_n[1] < 0 ||
                                            p->bubbles_n[2] < 0 || !(p->bubbles_radius >= 0.)))
@@ -699,7 +721,14 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   if (h->P.env[0].elasto_model) F.S = (double*)alloc(6 * N * sizeof(double));
   F.cqs = (double*)alloc((h->DIM == 3 ? 24 : 8) * N * sizeof(double));
   if (h->P.projection_pente_borne) F.phi_pb = (double*)alloc(h->NV * N * sizeof(double));
-  if (h->P.sans_lagrange) F.v0 = (double*)alloc(3 * NN * sizeof(double));
+  const bool csts = h->P.schema_csts && h->P.with_projection;
+  if (h->P.sans_lagrange || csts) F.v0 = (double*)alloc(3 * NN * sizeof(double));
+  if (csts) {
+    F.pq = dcell();
+    for (int d = 0; d < 3; ++d) F.fv[d] = dnode();
+  } else {
+    F.fv[0] = F.vx; F.fv[1] = F.vy; F.fv[2] = F.vz;
+  }
   if (case_cell_bcs(h)) {
     F.ebc = (double*)alloc(N * sizeof(double));
     F.pbc = (double*)alloc(N * sizeof(double));

@@ -78,6 +78,7 @@ struct Group {
   int NTILE = 0;               // bit D: the node sweep along D uses a shared-memory tile (when not NCOLS)
   int NCOLS = 0;               // bit D: the same for the node sweep
   int ADV = 0;                 // sans-lagrange: prescribed velocities, no Lagrange phase, no dual projection
+  int CSTS = 0;                // schema-csts with the remap: half-step velocity updates around the step
   long long it0;               // iteration of the members when the lists were built
   std::vector<int> members;
   DevList init_cells, init_nodes, lag_nodes, lag_cells, fin_cells, fin_nodes, dt;

@@ -58,7 +58,11 @@ struct Fields {
   double* phi_pb;          // pente-borne only: projected values (phi) of the next remap's first sweep
                            // [3 nb_env + 1][ncell]; entries of absent environments keep the
                            // values of the last sweep before
-  double* v0;              // sans-lagrange only: the prescribed node velocities at n [3][nnode]
+  double* v0;              // sans-lagrange: the prescribed node velocities at n [3][nnode];
+                           // CSTS: the velocities at n (after the last remap)
+  double* fv[3];           // the node terms of the remap's face velocities: vx, vy, vz themselves,
+                           // or (CSTS) the means of the velocities at n and n+1
+  double* pq;              // CSTS: pressure + pseudo-viscosity of the forces at n+1 [ncell]
   Scalars* s;
 };
 
@@ -840,7 +844,10 @@ __device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params&
 // (kb_hourglass), so this pass only writes the uncorrected velocity into
 // the dual-remap scratch Ud[0] (unused by a Lagrangian run).
 // ---------------------------------------------------------------------------
-template <int DIM, bool EL, bool HG, bool LAG>
+// CSTS (with the remap): the velocities after the remap (at n) are kept
+// in v0, then taken back to n-1/2 with the same forces and -old_dt/2
+// (updateVelocityBackward, MahycoModule.cc:573-627) before the update
+template <int DIM, bool EL, bool HG, bool LAG, bool CSTS = false>
 __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   const long long n = bx * (long long)CT + threadIdx.x;
   if (n >= M.nnode) return;
@@ -882,6 +889,13 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
   const double dth = 0.5 * (F.s->old_dt + dt);
   const double t = F.s->t;
   double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
+  if constexpr (CSTS) {
+    F.v0[n] = vx; F.v0[NN + n] = vy; F.v0[2 * NN + n] = vz;
+    const double dtb = -0.5 * F.s->old_dt;
+    const double fb = dtb / F.mn[n];
+    vx = vx + fb * S.x; vy = vy + fb * S.y; vz = vz + fb * S.z;
+    vx = vx + dtb * P.gravity[0]; vy = vy + dtb * P.gravity[1]; vz = vz + dtb * P.gravity[2];
+  }
   const double f = dth / F.mn[n];
   vx = vx + f * S.x; vy = vy + f * S.y; vz = vz + f * S.z;
   vx = vx + dth * P.gravity[0]; vy = vy + dth * P.gravity[1]; vz = vz + dth * P.gravity[2];
@@ -1146,9 +1160,12 @@ __device__ __forceinline__ void body_lagrange_geom(const Mesh& M, const mhc_case
 
 // EL: the elasto-plastic model needs the corner normals at n and n+1, so
 // this pass computes the geometry itself; otherwise body_lagrange_geom ran
-// first and V, l are read back.
-template <int DIM, int NE, bool EULER, bool EL = false>
+// first and V, l are read back.  CSTS (with the remap) needs them too, for
+// the work of the forces in its energy update, and leaves pressure +
+// pseudo-viscosity of the forward velocity update in pq.
+template <int DIM, int NE, bool EULER, bool EL = false, bool CSTS = false>
 __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  constexpr bool GEO = EL || CSTS;
   long long c = bx * (long long)CT + threadIdx.x;
   if (c >= M.ncell) return;
   const long long N = M.ncell;
@@ -1156,10 +1173,10 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   int i, j, k;
   cell_ijk(M, c, i, j, k);
   const int NBN = DIM == 3 ? 8 : 4;
-  R3 cqs[EL ? 8 : 1];
-  R3 cqn[EL ? 8 : 1];  // EL: corner normals at n, read before they are replaced
+  R3 cqs[GEO ? 8 : 1];
+  R3 cqn[GEO ? 8 : 1];  // corner normals at n, read before they are replaced
   double V, l;
-  if (EL) {
+  if (GEO) {
     R3 coord[8];
     for (int q = 0; q < NBN; ++q) {
       int a, b, d;
@@ -1273,6 +1290,25 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       ecur[q] = ecur[q] + value * dt;
     }
   }
+  // CSTS: work of the forces through the corner normals at n+1 and n and
+  // the node velocities at n+1/2 and n (MahycoModule.cc:1664-1675), summed
+  // in local node order
+  double cn1 = 0., cn = 0., cdn = 0., cov = 0.;
+  if constexpr (CSTS) {
+    const long long NN = M.nnode;
+    const double odt = F.s->old_dt;
+    for (int q = 0; q < NBN; ++q) {
+      int a, b, d;
+      local_node_offset(q, a, b, d);
+      const long long nn = node_id(M, i + a, j + b, k + d);
+      const R3 v = {F.vx[nn], F.vy[nn], F.vz[nn]};
+      const R3 vn = {F.v0[nn], F.v0[NN + nn], F.v0[2 * NN + nn]};
+      cn1 = cn1 + dot(v, cqs[q]) * dt;
+      cn = cn + dot(v, cqn[q]) * dt;
+      cdn = cdn + dot(v - vn, cqn[q]) * (dt - odt);
+      cov = cov + dot(vn, cqn[q]) * odt;
+    }
+  }
   // updateEnergyAndPressure
   double ee_[NE], pe[NE], ce[NE];
   for (int q = 0; q < NE; ++q) {
@@ -1302,6 +1338,16 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
         ++it;
       }
       ee_[q] = en1;
+    } else if (CSTS) {
+      // updateEnergyAndPressureforGP, CSTS branch (MahycoModule.cc:1676-1694);
+      // the pseudo-viscosity at n-1 is 0 with the remap, which resets the
+      // values at n after every remap (PrepareRemap.cc:219)
+      const double g = P.env[q].adiabatic_cst;
+      const double m = me[q], pn = pne[q], qnm1 = 0.;
+      const double den = 1 + 0.5 * (g - 1.0) * r * cn1 / m;
+      const double num = ecur[q] - (0.5 * (pn + qn) * cn / m) - (0.5 * qq * cn1 / m) + (0.25 * (pn + qn) * cdn / m) -
+                         (0.5 * (qn - qnm1) * cov / m);
+      ee_[q] = num / den;
     } else {
       double pseudo = 0.;
       if (P.pseudo_centree && ((qn + qq) * (1.0 / r - 1.0 / rn) < 0.)) pseudo = 0.5 * (qq + qn);
@@ -1325,6 +1371,15 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       U[(2 * NE + q) * N + c] = in ? Vq * rq * ee_[q] : 0.;
     }
     U[(NV - 1) * N + c] = V * qg;
+    if constexpr (CSTS) {
+      // the cell pressure of the forward update: the new one of an explicit
+      // update in a pure cell, otherwise the one the cell holds (at n; a
+      // mixed cell's average of the last remap)
+      double pf = F.p[c];
+      if (P.pression_explicite && pure)
+        for (int q = 0; q < NE; ++q) if ((mask >> q) & 1) pf = pe[q];
+      F.pq[c] = pf + qg;
+    }
     if (F.phi_pb) {
       // pente-borne phi of the first sweep (PrepareRemap.cc:138-157): the
       // environment's density and internal energy, the pseudo-viscosity;
@@ -1459,6 +1514,43 @@ __device__ __forceinline__ void body_advect_cells(const Mesh& M, const mhc_case_
   const double qg = F.q[c];
   U[(NV - 1) * N + c] = V * qg;
   if (F.phi_pb) F.phi_pb[(NV - 1) * N + c] = qg;
+}
+
+// ---------------------------------------------------------------------------
+// CSTS, before the remap: updateVelocityForward (MahycoModule.cc:637-700),
+// the velocities from n+1/2 to n+1 with the forces of the new pressure,
+// pseudo-viscosity and corner normals (gathered in ascending cell id), and
+// the node terms of the remap's face velocities, the means of the
+// velocities at n and n+1 (PrepareRemap.cc:45-52)
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ void body_csts_forward(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
+  const long long n = bx * (long long)CT + threadIdx.x;
+  if (n >= M.nnode) return;
+  const long long N = M.ncell, NN = M.nnode;
+  int i, j, k;
+  node_ijk(M, n, i, j, k);
+  constexpr int NS = DIM == 3 ? 8 : 4;
+  R3 S = {0., 0., 0.};
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int di = (s & 1) - 1, dj = ((s >> 1) & 1) - 1, dk = DIM == 3 ? ((s >> 2) & 1) - 1 : 0;
+    const int ci = i + di, cj = j + dj, ck = k + dk;
+    if (ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy || (DIM == 3 && (ck < 0 || ck >= M.ncz))) continue;
+    const int l = (-dk) * 4 + ((-dj) ? ((-di) ? 2 : 3) : ((-di) ? 1 : 0));
+    const long long c = cell_id(M, ci, cj, ck);
+    const R3 fv = F.pq[c] * load_cqs<DIM>(F, N, c, l);
+    S.x = S.x + fv.x; S.y = S.y + fv.y; S.z = S.z + fv.z;
+  }
+  const double dt = 0.5 * F.s->dt;
+  const double f = dt / F.mn[n];
+  double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
+  vx = vx + f * S.x; vy = vy + f * S.y; vz = vz + f * S.z;
+  vx = vx + dt * P.gravity[0]; vy = vy + dt * P.gravity[1]; vz = vz + dt * P.gravity[2];
+  F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
+  F.fv[0][n] = 0.5 * (vx + F.v0[n]);
+  F.fv[1][n] = 0.5 * (vy + F.v0[NN + n]);
+  F.fv[2][n] = 0.5 * (vz + F.v0[2 * NN + n]);
 }
 
 // The remap sweeps (one direction, cells and nodes) live in mhc_sweep.cuh.

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
 #endif
 
 // LAG: a Lagrangian run (no remap): last positions, pressure surfaces
-template <int DIM, bool EL, bool HG, bool LAG>
+template <int DIM, bool EL, bool HG, bool LAG, bool CSTS = false>
 __global__ void __launch_bounds__(CT, MHC_NODES_MIN_BLOCKS) kb_lagrange_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_NODES>(C, L, w_);
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(CT, MHC_NODES_MIN_BLOCKS) kb_lagrange_nodes(co
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_lagrange_nodes<DIM, EL, HG, LAG>(M, *C[wi.c].P, F, wi.x);
+    body_lagrange_nodes<DIM, EL, HG, LAG, CSTS>(M, *C[wi.c].P, F, wi.x);
   }
 }
 
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(CT, MHC_GEOM_MIN_BLOCKS) kb_lagrange_geom(cons
   }
 }
 
-template <int DIM, int NE, bool EULER, bool EL>
+template <int DIM, int NE, bool EULER, bool EL, bool CSTS = false>
 __global__ void __launch_bounds__(CT, MHC_LAG_MIN_BLOCKS) kb_lagrange_cells(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(CT, MHC_LAG_MIN_BLOCKS) kb_lagrange_cells(cons
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_lagrange_cells<DIM, NE, EULER, EL>(M, *C[wi.c].P, F, wi.x);
+    body_lagrange_cells<DIM, NE, EULER, EL, CSTS>(M, *C[wi.c].P, F, wi.x);
   }
 }
 
@@ -392,6 +392,18 @@ __global__ void __launch_bounds__(CT) kb_remap_finalize_nodes(const CaseDesc* __
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
     body_remap_finalize_nodes<DIM, DUAL>(M, F, ((K - 1) & 1) ? F.Ud[1] : F.Ud[0], wi.x);
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(CT) kb_csts_forward(const CaseDesc* __restrict__ C, PhaseList L) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_NODES>(C, L, w_);
+    Fields F = C[wi.c].F;
+    if (!case_active(F)) continue;
+    resolve_positions(F);
+    const Mesh M = C[wi.c].M;
+    body_csts_forward<DIM>(M, *C[wi.c].P, F, wi.x);
   }
 }
 

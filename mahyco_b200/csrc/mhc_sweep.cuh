@@ -136,7 +136,7 @@ template <int DIM, int D>
 __device__ __forceinline__ void load_plane(const Mesh& M, const Fields& F, int i, int j, int k, Plane<DIM>& P) {
   constexpr int NQ = DIM == 3 ? 4 : 2;
   const double wf = DIM == 2 ? .5 : .25;
-  const double* vD = D == 0 ? F.vx : (D == 1 ? F.vy : F.vz);
+  const double* vD = F.fv[D];  // the node velocities, or (CSTS) their means at n and n+1
   long long fn[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {

@@ -988,9 +988,16 @@ static void update_velocity(Case& C) {
       }
     }
   }
+  R3 g = {C.P.gravity[0], C.P.gravity[1], C.P.gravity[2]};
+  if (C.P.schema_csts && C.P.with_projection) {
+    /* updateVelocityBackward (MahycoModule.cc:573-627): the velocities after
+     * the remap (at n) back to n-1/2 with the same forces, -old_dt/2 */
+    const double dtb = -0.5 * C.old_dt;
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] += (dtb / C.node_mass[n]) * C.force[n];
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] += dtb * g;
+  }
   const double dt = 0.5 * (C.old_dt + C.dt);
   for (long n = 0; n < C.nnode; ++n) C.vel[n] += (dt / C.node_mass[n]) * C.force[n];
-  R3 g = {C.P.gravity[0], C.P.gravity[1], C.P.gravity[2]};
   for (long n = 0; n < C.nnode; ++n) C.vel[n] += dt * g;
   if (!C.P.with_projection && C.P.coef_antiderive != 0.) {
     /* MahycoModule.cc:497-555 */
@@ -1409,6 +1416,31 @@ static void update_energy_and_pressure(Case& C) {
         C.EV(C.internal_energy, e, c) = en1;
       }
     }
+  } else if (C.P.schema_csts) {
+    /* updateEnergyAndPressureforGP, CSTS branch (MahycoModule.cc:1660-1697):
+     * the work of the forces at n and n+1 through the corner normals and
+     * node velocities at n and n+1/2 */
+    for (int e = 0; e < C.nenv; ++e) {
+      double g = C.P.env[e].adiabatic_cst;
+      for (long c = 0; c < C.ncell; ++c) {
+        if (!C.has(c, e)) continue;
+        double cn1 = 0., cn = 0., cdn = 0., cov = 0.;
+        for (int l = 0; l < C.nbn; ++l) {
+          const long n = C.cnode(c, l);
+          const R3 v = C.vel[n], vn = C.vel_n[n];
+          cn1 += dot(v, C.cqs[c * C.nbn + l]) * C.dt;
+          cn += dot(v, C.cqs_n[c * C.nbn + l]) * C.dt;
+          cdn += dot(v - vn, C.cqs_n[c * C.nbn + l]) * (C.dt - C.old_dt);
+          cov += dot(vn, C.cqs_n[c * C.nbn + l]) * C.old_dt;
+        }
+        const double m = C.EV(C.cell_mass, e, c), pn = C.EV(C.pressure_n, e, c);
+        const double qn = C.EV(C.pseudo_n, e, c), qn1 = C.EV(C.pseudo, e, c), qnm1 = C.EV(C.pseudo_nm1, e, c);
+        double den = 1 + 0.5 * (g - 1.0) * C.EV(C.density, e, c) * cn1 / m;
+        double num = C.EV(C.internal_energy, e, c) - (0.5 * (pn + qn) * cn / m) - (0.5 * qn1 * cn1 / m) +
+                     (0.25 * (pn + qn) * cdn / m) - (0.5 * (qn - qnm1) * cov / m);
+        C.EV(C.internal_energy, e, c) = num / den;
+      }
+    }
   } else {
     bool pc = C.P.pseudo_centree;
     for (int e = 0; e < C.nenv; ++e) {
@@ -1729,7 +1761,9 @@ static void compute_face_quantities_for_remap(Case& C) {
       R3 vm = {0., 0., 0.}, fc = {0., 0., 0.};
       for (int q = 0; q < nb; ++q) {
         fc += w * C.coord[n[q]];
-        vm += C.vel[n[q]];
+        /* CSTS: the mean of the velocities at n and n+1 */
+        if (C.P.schema_csts) vm += 0.5 * (C.vel[n[q]] + C.vel_n[n[q]]);
+        else vm += C.vel[n[q]];
       }
       C.face_coord[d][f] = fc;
       C.face_un[d][f] = dot((w * vm), C.face_normal[d][f]);
@@ -2295,9 +2329,29 @@ static int appli_remap(Case& C) {
 /* MahycoModule::remap (PrepareRemap.cc:203-251) */
 static int remap(Case& C) {
   if (!C.P.with_projection) return ST_OK;
+  if (C.P.schema_csts) {
+    /* updateVelocityForward (MahycoModule.cc:637-700): n+1/2 to n+1 with the
+     * forces of the new pressure, pseudo-viscosity and corner normals */
+    for (auto& f : C.force) f = {0., 0., 0.};
+    for (long c = 0; c < C.ncell; ++c) {
+      double pressure = C.pressure.g[c] + C.pseudo.g[c];
+      for (int l = 0; l < C.nbn; ++l) C.force[C.cnode(c, l)] += pressure * C.cqs[c * C.nbn + l];
+    }
+    const double dt = 0.5 * C.dt;
+    R3 g = {C.P.gravity[0], C.P.gravity[1], C.P.gravity[2]};
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] += (dt / C.node_mass[n]) * C.force[n];
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] += dt * g;
+  }
   compute_variables_for_remap(C);
   compute_face_quantities_for_remap(C);
   if (appli_remap(C) != ST_OK) return C.status;
+  /* values at n reset after the remap (PrepareRemap.cc:219-226); the
+   * pseudo-viscosity at n-1 of the next iteration is therefore 0 */
+  C.pseudo_n.fill(0.0);
+  C.cell_volume_n.fill(0.0);
+  C.pressure_n.fill(0.0);
+  C.density_n.fill(0.0);
+  C.tau_density.fill(0.0);
   for (int e = 0; e < C.nenv; ++e) eos_apply(C, e);
   compute_pression_moyenne(C);
   return ST_OK;

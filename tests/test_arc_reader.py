@@ -34,13 +34,13 @@ def test_lagrange_loop_disables_remap(tmp_path):
     assert p.with_projection == 0
 
 
-@pytest.mark.parametrize("snippet", ["<schema-csts>1</schema-csts>"])
-def test_unsupported_options_raise(tmp_path, snippet):
-    text = open(ARC).read().replace("<pseudo-centree>0</pseudo-centree>", "<pseudo-centree>0</pseudo-centree>" + snippet)
+def test_schema_csts_is_read(tmp_path):
+    text = open(ARC).read().replace("<pseudo-centree>0</pseudo-centree>",
+                                    "<pseudo-centree>0</pseudo-centree><schema-csts>1</schema-csts>")
     f = tmp_path / "u.arc"
     f.write_text(text)
-    with pytest.raises(NotImplementedError):
-        read_arc(str(f))
+    p, _ = read_arc(str(f))
+    assert p.schema_csts == 1
 
 
 def test_params_roundtrip():
