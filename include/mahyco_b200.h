@@ -158,6 +158,16 @@ int mhc_scalars_wait(mhc_case* h, int slot, double* time, double* deltat, long l
  * Returns the number of doubles written, or an error. */
 long long mhc_get_field(mhc_case* h, const char* name, int env, double* host, long long capacity);
 
+/* Initial fields, before mhc_hydro_start_init: what the reference reads
+ * from the dataset's mesh file and <initialisation> block.  NodeCoord (3
+ * per node, x y z interleaved, the library's node order): the initial
+ * positions of a Lagrangian case, a mesh file's grid (mahyco_b200/msh.py
+ * maps the logically structured Gmsh quadrangle grids of the datasets);
+ * Materiau, Density, Pressure (one per cell): the initial state of the
+ * EXTERNAL case model (the values not given: environment 0 and its
+ * initial state).  Returns the number of doubles read, or an error. */
+long long mhc_case_set_initial_field(mhc_case* h, const char* name, const double* host, long long n);
+
 /* Upload of a named field, the inverse of mhc_get_field, so that a host can
  * push its own state onto the device (a restart from its own dumps, an
  * initialisation this library lacks, a hand-off from its CPU code).  Same

@@ -74,8 +74,15 @@ enum mhc_case_model {
   MHC_CASE_ONECELL = 4,   /* casTest/ONECELL/ONECELLService.cc: one uniform environment */
   MHC_CASE_BUBBLES = 5,   /* casTest/CHOCBULLE/CHOCBULLEService.cc: a lattice of bubbles of
                              environment 1 in environment 0 (mixed boundary cells) */
-  MHC_CASE_RIDER = 6      /* casTest/RIDER/RIDERService.cc: a disc advected by a prescribed
+  MHC_CASE_RIDER = 6,     /* casTest/RIDER/RIDERService.cc: a disc advected by a prescribed
                              velocity field (cas_test 23-38) */
+  MHC_CASE_EXTERNAL = 7   /* casTest/EXTERNAL/EXTERNALService.cc (the default cas-model): the
+                             dataset's <initialisation> block sets Materiau, Density and
+                             Pressure per cell (mhc_case_set_initial_field; by default
+                             environment 0 and its initial state everywhere), then
+                             initUtilisateur sets the node velocities of every environment
+                             with initialisation_utilisateur: its vitesse_initiale, or
+                             -x/|x| when that is zero */
 };
 
 /* cas-test ids used by SOD and SEDOV (TypesMahyco.h:44-94) */
@@ -143,6 +150,9 @@ typedef struct mhc_env_params {
    * valeur-debut-pression, valeur-dependance-temps; the pressure is
    * p0 + dpdt t once t > tdebut, 0 once t > tfin */
   double fictif_tdebut, fictif_tfin, fictif_p0, fictif_dpdt;
+  /* initialisation-utilisateur (Mahyco.axl): the EXTERNAL case model's
+   * initUtilisateur runs for this environment */
+  int initialisation_utilisateur;
 } mhc_env_params;
 
 typedef struct mhc_bc {
@@ -227,6 +237,12 @@ typedef struct mhc_case_params {
    * normals, and the remap's face velocities are the mean of those at n and
    * n+1 */
   int schema_csts;
+  /* order of the cells in the reference's numbering, which fixes the order
+   * of its sums over cells (node forces and masses, the anti-hourglass
+   * correction, the time history): 0 x-fastest (the cartesian generator),
+   * 1 y-fastest (the 2D Gmsh quadrangle grids of the datasets, whose
+   * elements run column by column) */
+  int mesh_cell_order;
 } mhc_case_params;
 
 #ifdef __cplusplus

@@ -119,6 +119,7 @@ _SIGS = {
                                       C.POINTER(C.c_double)]),
     "mhc_server_take_completed": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]),
     "mhc_set_field": (C.c_longlong, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_longlong]),
+    "mhc_case_set_initial_field": (C.c_longlong, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.c_longlong]),
     "mhc_eos_init": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_eos_reinit": (C.c_int, [C.c_void_p, C.c_int]),
     "mhc_eos_apply_one_cell": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.POINTER(C.c_double)]),
@@ -229,6 +230,15 @@ class Hydro:
 
     def __exit__(self, *a):
         self.close()
+
+    def set_initial_field(self, name: str, values) -> None:
+        """Before hydroStartInit: NodeCoord of a mesh file (Lagrangian
+        cases), Materiau / Density / Pressure of the EXTERNAL case model
+        (mhc_case_set_initial_field)."""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        got = self.lib.mhc_case_set_initial_field(self.h, name.encode(), a.ctypes.data_as(C.POINTER(C.c_double)),
+                                                  a.size)
+        _check(self.lib, int(got), f"set_initial_field {name}")
 
     # -- init entry points (Mahyco.config:15-21)
     def hydroStartInit(self):

@@ -21,9 +21,9 @@ EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
 BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4, "Density": 5,
               "Energy": 6, "SuperGaussianEnergy": 7, "Pressure": 8}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
-CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES, CASE_RIDER = 1, 2, 3, 4, 5, 6
+CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES, CASE_RIDER, CASE_EXTERNAL = 1, 2, 3, 4, 5, 6, 7
 CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL, "CHOCBULLE": CASE_BUBBLES,
-                "RIDER": CASE_RIDER}
+                "RIDER": CASE_RIDER, "EXTERNAL": CASE_EXTERNAL}
 # RIDER cas-test ids (TypesMahyco.h:69-84): MonoRider* 23-30, Rider* 31-38
 RIDER_TESTS = {n: 23 + i for i, n in enumerate(
     ("MonoRiderTx", "MonoRiderTy", "MonoRiderT45", "MonoRiderRotation", "MonoRiderVortex", "MonoRiderDeformation",
@@ -60,7 +60,7 @@ class EnvParams(C.Structure):
         ("depot_dependance", C.c_double * 4), ("depot_cutoff", C.c_double * 2),
         ("depot_tdebut", C.c_double), ("depot_tfin", C.c_double), ("depot_power", C.c_double),
         ("fictif_tdebut", C.c_double), ("fictif_tfin", C.c_double), ("fictif_p0", C.c_double),
-        ("fictif_dpdt", C.c_double),
+        ("fictif_dpdt", C.c_double), ("initialisation_utilisateur", C.c_int),
     ]
 
 
@@ -96,7 +96,7 @@ class CaseParams(C.Structure):
         ("bubbles_radius", C.c_double),
         ("sans_lagrange", C.c_int), ("rider_reverse", C.c_int), ("rider_parameter", C.c_double),
         ("rider_radius", C.c_double), ("rider_linear_density", C.c_int),
-        ("schema_csts", C.c_int),
+        ("schema_csts", C.c_int), ("mesh_cell_order", C.c_int),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -223,20 +223,58 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
     # save-init: the post-processing also writes the initial state (step 0)
     info["save_init"] = bool(_txt(root, "arcane-post-processing/save-init", False, _bool))
     cart = root.find("mesh/meshgenerator/cartesian")
-    if cart is None:
-        raise NotImplementedError("only the cartesian mesh generator is supported")
-    org = [float(v) for v in cart.find("origine").text.split()]
-    p.origin[:] = (org + [0.0, 0.0, 0.0])[:3]
-    lx, ly, lz = cart.find("lx"), cart.find("ly"), cart.find("lz")
-    p.lx, p.nx = float(lx.text), int(lx.get("nx"))
-    p.ly, p.ny = float(ly.text), int(ly.get("ny"))
-    if lz is not None:
-        p.dim, p.lz, p.nz = 3, float(lz.text), int(lz.get("nz"))
+    mfile = root.find("mesh/file")
+    info["init_fields"] = {}
+    msh = None
+    if cart is None and mfile is not None and mfile.text.strip().endswith(".msh"):
+        # a Gmsh file of logically structured quadrangles, 2D: its node
+        # coordinates and the <initialisation> values of its cell groups
+        # are the case's initial fields (mahyco_b200.msh)
+        import os
+        from .msh import read_msh
+        msh = read_msh(os.path.join(os.path.dirname(os.path.abspath(path)), mfile.text.strip()))
+        xyz = msh["coords"]
+        p.dim, p.nx, p.ny, p.nz = 2, msh["nx"], msh["ny"], 1
+        p.origin[:] = (float(xyz[:, 0].min()), float(xyz[:, 1].min()), 0.0)
+        p.lx, p.ly, p.lz = float(xyz[:, 0].max() - xyz[:, 0].min()), float(xyz[:, 1].max() - xyz[:, 1].min()), 0.0
+        info["init_fields"]["NodeCoord"] = xyz.ravel().tolist()
+        info["msh_sides"] = msh["sides"]
+        # the file's elements run column by column: its sums over cells too
+        order = msh["cell_order"]
+        nx_, ny_ = msh["nx"], msh["ny"]
+        colmajor = all(order[a + nx_ * b] == a * ny_ + b for a in range(nx_) for b in range(ny_))
+        rowmajor = all(order[c] == c for c in range(nx_ * ny_))
+        if not (colmajor or rowmajor):
+            raise NotImplementedError("mesh file cells neither row by row nor column by column")
+        p.mesh_cell_order = 1 if colmajor and not rowmajor else 0
+        vals: dict[str, dict[str, float]] = {}
+        for v in root.findall("mesh/initialisation/variable"):
+            vals.setdefault(v.get("nom"), {})[v.get("groupe")] = float(v.get("valeur"))
+        for var in ("Materiau", "Density", "Pressure"):
+            if var in vals:
+                per_group = vals[var]
+                missing = {g for g in msh["cell_groups"] if g not in per_group}
+                if missing:
+                    raise NotImplementedError(f"{var} not initialised on cell groups {sorted(missing)}")
+                info["init_fields"][var] = [per_group[g] for g in msh["cell_groups"]]
+    elif cart is None:
+        raise NotImplementedError("only the cartesian mesh generator and Gmsh quadrangle files are supported")
+    if msh is not None:
+        org = None
     else:
-        p.dim, p.lz, p.nz = 2, 0.0, 1
-    for el, n in ((lx, "prx"), (ly, "pry"), (lz, "prz")):
-        if el is not None and float(el.get(n, "1.0")) != 1.0:
-            raise NotImplementedError("non-uniform cartesian progression")
+        org = [float(v) for v in cart.find("origine").text.split()]
+    if msh is None:
+        p.origin[:] = (org + [0.0, 0.0, 0.0])[:3]
+        lx, ly, lz = cart.find("lx"), cart.find("ly"), cart.find("lz")
+        p.lx, p.nx = float(lx.text), int(lx.get("nx"))
+        p.ly, p.ny = float(ly.text), int(ly.get("ny"))
+        if lz is not None:
+            p.dim, p.lz, p.nz = 3, float(lz.text), int(lz.get("nz"))
+        else:
+            p.dim, p.lz, p.nz = 2, 0.0, 1
+        for el, n in ((lx, "prx"), (ly, "pry"), (lz, "prz")):
+            if el is not None and float(el.get(n, "1.0")) != 1.0:
+                raise NotImplementedError("non-uniform cartesian progression")
     m = root.find("mahyco")
     envs = m.findall("environment")
     if not 1 <= len(envs) <= MAX_ENV:
@@ -255,6 +293,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         vi = ev.find("vitesse-initiale")
         if vi is not None:
             e.vitesse_initiale[:] = [float(v) for v in vi.text.split()]
+        e.initialisation_utilisateur = int(_txt(ev, "initialisation-utilisateur", False, _bool))
         e.linear_pseudo_coeff = _txt(ev, "linear-pseudo-coeff", 0.5)
         e.quadratic_pseudo_coeff = _txt(ev, "quadratic-pseudo-coeff", 1.2)
         for tag, attr in (("adiabatic-cst", "adiabatic_cst"), ("limit-tension", "limit_tension"),
@@ -298,6 +337,9 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
             e.depot_cutoff[:] = (_txt(dep, "cutoffX", 1000.0), _txt(dep, "cutoffY", 1000.0))
             e.depot_tdebut, e.depot_tfin = _txt(dep, "Tdebut", 0.0), _txt(dep, "Tfin", 1000.0)
     cm = m.find("cas-model")
+    if cm is None:
+        # the default cas-model (Mahyco.axl:386): EXTERNAL
+        cm = ET.Element("cas-model", {"name": "EXTERNAL"})
     p.cas_model = CASE_BY_NAME[cm.get("name")]
     p.cas_test = _txt(cm, "cas-test", 0, int)
     if p.cas_model == CASE_BUBBLES:
@@ -359,7 +401,13 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         kind = b.find("type").text.strip()
         if kind not in BC_BY_NAME:
             raise NotImplementedError(f"boundary condition {kind}")
-        add_bc(p, b.find("surface").text.strip(), kind, _txt(b, "value", 0.0),
+        surf = b.find("surface").text.strip()
+        if msh is not None:
+            # a mesh file's boundary group: the logical side it lies on
+            if surf not in msh["sides"]:
+                raise NotImplementedError(f"boundary group {surf} is not one side of the grid")
+            surf = {v: k for k, v in SURFACES.items()}[msh["sides"][surf]]
+        add_bc(p, surf, kind, _txt(b, "value", 0.0),
                _txt(b, "Tdebut", 0.0), _txt(b, "Tfin", 1000.0),
                tuple(_txt(b, t, 0.0) for t in ("dependanceX", "dependanceY", "dependanceZ", "dependanceT")),
                (_txt(b, "cutoffX", 1000.0), _txt(b, "cutoffY", 1000.0)))

@@ -19,7 +19,8 @@ from __future__ import annotations
 import math
 import random
 
-from .case import (ARITHMETIC_G, CASE_BUBBLES, CASE_ONECELL, CASE_RIDER, CASE_SEDOV, CASE_SOD, CASE_TWO_STATE,
+from .case import (ARITHMETIC_G, CASE_BUBBLES, CASE_EXTERNAL, CASE_ONECELL, CASE_RIDER, CASE_SEDOV, CASE_SOD,
+                   CASE_TWO_STATE,
                    DEPOT_CONSTANT, DEPOT_SUPER_GAUSSIAN, EOS_FICTIF, EOS_MIE_GRUNEISEN, EULER_X, EULER_Y, EULER_Z,
                    EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
                    ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults,
@@ -493,6 +494,11 @@ PARITY_CASES = {
     "adi2d_water_air_csts": (lambda: _csts(water_air(deltat_init=1e-6)), 60),
     "adi3d_bisod_z_csts_pb_vanleer": (lambda: _pb(_csts(sod(dim=3, n=(4, 5, 28), L=(0.1, 0.1, 1.0), bi=True, axis=2,
                                                             limiter=VANLEER, deltat_init=1e-3)), 2), 50),
+    # EXTERNAL case model: the user initialisation's -x/|x| velocity (a
+    # Noh-like implosion, anti-hourglass), and its constant velocity with
+    # the cells numbered column by column (mesh_cell_order 1)
+    "lag2d_external_implosion": (lambda: _external(deltat_init=1e-4), 150),
+    "lag2d_external_colmajor_bar": (lambda: _external(velocity=(0.0, -0.3, 0.0), colmajor=True, deltat_init=1e-4), 150),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
@@ -500,6 +506,27 @@ PARITY_CASES = {
 # cos(Pi t), which CUDA and the oracle's libm round differently
 PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13,
                     "adv3d_rider_deformation_reverse": 1e-12}
+
+
+def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> CaseParams:
+    """EXTERNAL case model on a 30 x 24 grid off the origin: one perfect
+    gas at rest state (1, 1e-3), the user initialisation's velocity,
+    anti-hourglass, symmetry planes x = 0.01 and y = 0.01."""
+    p = default_params()
+    _mesh(p, 2, (30, 24), (1.0, 0.8))
+    p.origin[:] = (0.01, 0.01, 0.0)
+    p.nb_env = 1
+    env_defaults(p.env[0], EOS_PERFECT_GAS)
+    p.env[0].densite_initiale, p.env[0].pression_initiale = 1.0, 1e-3
+    p.env[0].vitesse_initiale[:] = velocity
+    p.env[0].initialisation_utilisateur = 1
+    p.cas_model = CASE_EXTERNAL
+    p.with_projection = 0
+    p.coef_antiderive = 0.01
+    p.mesh_cell_order = 1 if colmajor else 0
+    p.deltat_init, p.deltat_max = deltat_init, 1e-3
+    symmetry_bcs(p, ("XMIN", "YMIN"))
+    return p
 
 
 def _csts(p: CaseParams, explicit: int = 0) -> CaseParams:

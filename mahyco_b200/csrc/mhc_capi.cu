@@ -555,7 +555,9 @@ int validate(const mhc_case_params* p) {
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with a per-axis Euler remap");
   if (cellvars && p->with_newton)
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with the Newton energy update");
-  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_RIDER) return set_err(MHC_ERR_ARG, "cas-model");
+  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_EXTERNAL) return set_err(MHC_ERR_ARG, "cas-model");
+  if (p->mesh_cell_order != 0 && !(p->mesh_cell_order == 1 && p->dim == 2))
+    return set_err(MHC_ERR_ARG, "mesh_cell_order: 0, or 1 in 2D");
   if (p->cas_model == MHC_CASE_RIDER &&
       (p->cas_test < MHC_TEST_MONO_RIDER_TX || p->cas_test > MHC_TEST_RIDER_DEFORMATION_REVERSE || p->nb_env < 2 ||
        !p->sans_lagrange || !(p->rider_radius > 0.)))
@@ -970,15 +972,22 @@ int case_time_history(mhc_case* h, cudaStream_t st, double* out) {
       return MHC_ERR_CUDA;
     long long cnt = 0;
     double sm = 0., sp = 0., rv = 0., vv = 0., em = 0., mm = 0.;
-    for (long long c = 0; c < N; ++c) {
+    // in the order of the reference's cell numbering (mesh_cell_order)
+    const bool cm = h->DIM == 2 && h->P.mesh_cell_order == 1;
+    const long long nx = h->M.ncx, ny = h->M.ncy;
+    auto cell = [&](long long k) { return cm ? (k / ny) + nx * (k % ny) : k; };
+    for (long long k = 0; k < N; ++k) {
+      const long long c = cell(k);
       if (!(((int)env[c] >> q) & 1)) continue;
       ++cnt; sm += m[c]; sp += p[c];
     }
-    for (long long c = 0; c < N; ++c) {
+    for (long long k = 0; k < N; ++k) {
+      const long long c = cell(k);
       if (!(((int)env[c] >> q) & 1)) continue;
       em += e[c] * m[c]; mm += m[c];
     }
-    for (long long c = 0; c < N; ++c) {
+    for (long long k = 0; k < N; ++k) {
+      const long long c = cell(k);
       if (!(((int)env[c] >> q) & 1)) continue;
       rv += rho[c] * V[c]; vv += V[c];
     }

@@ -63,8 +63,32 @@ struct Fields {
   double* fv[3];           // the node terms of the remap's face velocities: vx, vy, vz themselves,
                            // or (CSTS) the means of the velocities at n and n+1
   double* pq;              // CSTS: pressure + pseudo-viscosity of the forces at n+1 [ncell]
+  double* x0;              // initial node coordinates read from a mesh file [3][nnode] (else the
+                           // cartesian grid)
+  double* init;            // EXTERNAL initial state given per cell: Materiau, Density, Pressure
+                           // [3][ncell] (else environment 0 and its initial state everywhere)
   Scalars* s;
 };
+
+// the s-th cell around a node (bits of s: x, y, z offsets - 1) in the order
+// of the reference's cell numbering, which its node sums follow: x-fastest,
+// or y-fastest for the 2D mesh files numbered column by column
+// (mesh_cell_order 1)
+__device__ __forceinline__ void around_node(int s, bool colmajor, int& di, int& dj, int& dk) {
+  const int b0 = s & 1, b1 = (s >> 1) & 1;
+  di = (colmajor ? b1 : b0) - 1;
+  dj = (colmajor ? b0 : b1) - 1;
+  dk = ((s >> 2) & 1) - 1;
+}
+
+// initial position of node (i, j, k): the mesh file's, or the cartesian grid's
+__device__ __forceinline__ R3 node_initial(const Mesh& M, const Fields& F, int i, int j, int k) {
+  if (F.x0) {
+    const long long n = node_id(M, i, j, k), NN = M.nnode;
+    return {F.x0[n], F.x0[NN + n], F.x0[2 * NN + n]};
+  }
+  return node_x0(M, i, j, k);
+}
 
 // the previous cycle's Lagrangian positions are X[(iteration-1)&1], this
 // cycle's are X[iteration&1]
@@ -504,7 +528,7 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   for (int l = 0; l < NBN; ++l) {
     int a, b, d;
     local_node_offset(l, a, b, d);
-    coord[l] = node_x0(M, i + a, j + b, k + d);
+    coord[l] = node_initial(M, F, i + a, j + b, k + d);
     s = s + coord[l];
   }
   R3 cc = (DIM == 2 ? .25 : .125) * s;
@@ -517,6 +541,8 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
     if (NE > 1) mat = (comp(cc, P.interface_dir) < P.interface_pos) ? 0. : 1.;
   } else if (P.cas_model == MHC_CASE_ONECELL) {
     mat = 0.;  // ONECELLService::initMat
+  } else if (P.cas_model == MHC_CASE_EXTERNAL) {
+    mat = F.init ? F.init[c] : 0.;  // the dataset's <initialisation> Materiau
   } else if (P.cas_model == MHC_CASE_SEDOV && P.cas_test != MHC_TEST_SEDOV) {
     bool center = false;
     for (int l = 0; l < NBN; ++l) {
@@ -618,6 +644,11 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
       rho = frac_b * d1;
       p = p1;
     }
+  } else if (P.cas_model == MHC_CASE_EXTERNAL) {
+    // EXTERNALService (no initVar): the dataset's <initialisation> Density
+    // and Pressure of the cell
+    rho = F.init ? F.init[N + c] : P.env[0].densite_initiale;
+    p = F.init ? F.init[2 * N + c] : P.env[0].pression_initiale;
   } else if (P.cas_model == MHC_CASE_ONECELL) {
     // ONECELLService::initVarMono: the first environment's state everywhere
     rho = P.env[0].densite_initiale;
@@ -689,21 +720,16 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
 // computeNodeMass (MahycoModule.cc:247-262): gather of 1/8 (1/4) cell masses in
 // ascending cell id; also initial velocity and Lagrangian positions.
 template <int DIM>
-__device__ __forceinline__ double node_mass_gather(const Mesh& M, const double* cm, int i, int j, int k) {
+__device__ __forceinline__ double node_mass_gather(const Mesh& M, const double* cm, int i, int j, int k,
+                                                   bool colmajor = false) {
   const double w = DIM == 2 ? .25 : .125;
   double s = 0.;
-  for (int dk = (DIM == 3 ? -1 : 0); dk <= 0; ++dk) {
-    int ck = k + dk;
-    if (DIM == 3 && (ck < 0 || ck >= M.ncz)) continue;
-    for (int dj = -1; dj <= 0; ++dj) {
-      int cj = j + dj;
-      if (cj < 0 || cj >= M.ncy) continue;
-      for (int di = -1; di <= 0; ++di) {
-        int ci = i + di;
-        if (ci < 0 || ci >= M.ncx) continue;
-        s += w * cm[cell_id(M, ci, cj, DIM == 3 ? ck : 0)];
-      }
-    }
+  for (int q = 0; q < (DIM == 3 ? 8 : 4); ++q) {
+    int di, dj, dk;
+    around_node(q, DIM == 2 && colmajor, di, dj, dk);
+    const int ci = i + di, cj = j + dj, ck = DIM == 3 ? k + dk : 0;
+    if (ci < 0 || ci >= M.ncx || cj < 0 || cj >= M.ncy || (DIM == 3 && (ck < 0 || ck >= M.ncz))) continue;
+    s += w * cm[cell_id(M, ci, cj, ck)];
   }
   return s;
 }
@@ -714,11 +740,25 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
   if (n >= M.nnode) return;
   int i, j, k;
   node_ijk(M, n, i, j, k);
-  R3 x = node_x0(M, i, j, k);
+  R3 x = node_initial(M, F, i, j, k);
   F.Xp[0][n] = x.x; F.Xp[1][n] = x.y; F.Xp[2][n] = x.z;
   double vx = 0., vy = 0., vz = 0.;
   if (P.cas_model == MHC_CASE_SOD || P.cas_model == MHC_CASE_TWO_STATE || P.cas_model == MHC_CASE_BUBBLES) {
     vx = P.env[0].vitesse_initiale[0]; vy = P.env[0].vitesse_initiale[1]; vz = P.env[0].vitesse_initiale[2];
+  }
+  if (P.cas_model == MHC_CASE_EXTERNAL) {
+    // EXTERNALService::initUtilisateur (EXTERNALService.cc:25-40) for every
+    // environment that asks for it: its initial velocity, or -x/|x|
+    for (int e = 0; e < P.nb_env; ++e) {
+      if (!P.env[e].initialisation_utilisateur) continue;
+      const double* w = P.env[e].vitesse_initiale;
+      if (w[0] == 0. && w[1] == 0. && w[2] == 0.) {
+        const double r = sqrt(x.x * x.x + x.y * x.y + x.z * x.z);
+        vx = (-x.x) / r; vy = (-x.y) / r; vz = (-x.z) / r;
+      } else {
+        vx = w[0]; vy = w[1]; vz = w[2];
+      }
+    }
   }
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   if (F.v0) {
@@ -726,7 +766,7 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
     const long long NN = M.nnode;
     F.v0[n] = vx; F.v0[NN + n] = vy; F.v0[2 * NN + n] = vz;
   }
-  F.mn[n] = node_mass_gather<DIM>(M, F.m, i, j, k);
+  F.mn[n] = node_mass_gather<DIM>(M, F.m, i, j, k, P.mesh_cell_order == 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -857,10 +897,13 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
   // the <= 8 cells around the node in ascending id: slot s = (dk, dj, di)
   // bits, the node's local index in the cell is the complement
   constexpr int NS = DIM == 3 ? 8 : 4;
+  const bool cm = DIM == 2 && P.mesh_cell_order == 1;
   R3 S = {0., 0., 0.};
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
-    const int di = (s & 1) - 1, dj = ((s >> 1) & 1) - 1, dk = DIM == 3 ? ((s >> 2) & 1) - 1 : 0;
+    int di, dj, dk;
+    around_node(s, cm, di, dj, dk);
+    if (DIM == 2) dk = 0;
     const int ci = i + di, cj = j + dj, ck = k + dk;
     if (ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy || (DIM == 3 && (ck < 0 || ck >= M.ncz))) continue;
     const int l = (-dk) * 4 + ((-dj) ? ((-di) ? 2 : 3) : ((-di) ? 1 : 0));
@@ -872,7 +915,9 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
   if (EL) {
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      const int di = (s & 1) - 1, dj = ((s >> 1) & 1) - 1, dk = DIM == 3 ? ((s >> 2) & 1) - 1 : 0;
+      int di, dj, dk;
+      around_node(s, cm, di, dj, dk);
+      if (DIM == 2) dk = 0;
       const int ci = i + di, cj = j + dj, ck = k + dk;
       if (ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy || (DIM == 3 && (ck < 0 || ck >= M.ncz))) continue;
       const int l = (-dk) * 4 + ((-dj) ? ((-di) ? 2 : 3) : ((-di) ? 1 : 0));
@@ -946,9 +991,11 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
   const double nb = (double)(((i > 0 && i < M.nnx - 1) ? 2 : 1) * ((j > 0 && j < M.nny - 1) ? 2 : 1) *
                              (DIM == 3 ? ((k > 0 && k < M.nnz - 1) ? 2 : 1) : 1));
   R3 h = {0., 0., 0.};
-  for (int dk = (DIM == 3 ? -1 : 0); dk <= 0; ++dk)
-    for (int dj = -1; dj <= 0; ++dj)
-      for (int di = -1; di <= 0; ++di) {
+  const bool cm = DIM == 2 && P.mesh_cell_order == 1;
+  for (int s = 0; s < (DIM == 3 ? 8 : 4); ++s) {
+        int di, dj, dk;
+        around_node(s, cm, di, dj, dk);
+        if (DIM == 2) dk = 0;
         const int ci = i + di, cj = j + dj, ck = k + dk;
         if (ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy) continue;
         if (DIM == 3 && (ck < 0 || ck >= M.ncz)) continue;

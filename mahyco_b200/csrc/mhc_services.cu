@@ -171,6 +171,58 @@ void mhc_case_params_default(mhc_case_params* p) {
 }
 
 // ---------------------------------------------------------------------------
+// initial fields (before HydroStartInit)
+// ---------------------------------------------------------------------------
+long long mhc_case_set_initial_field(mhc_case* h, const char* name, const double* host, long long n) {
+  if (!h || !name || !host) return set_err(MHC_ERR_ARG, "null argument");
+  if (h->initialised) return set_err(MHC_ERR_ORDER, "initial fields go before HydroStartInit");
+  const long long N = h->M.ncell, NN = h->M.nnode;
+  Fields& F = h->F;
+  cudaStream_t st = h->stream;
+  auto grow = [&](double** p, size_t bytes) -> int {
+    if (*p) return MHC_OK;
+    void* d = nullptr;
+    CK(cudaMallocAsync(&d, bytes, st));
+    h->allocs.push_back(d);
+    h->alloc_bytes.push_back(bytes);
+    *p = (double*)d;
+    return MHC_OK;
+  };
+  int r;
+  if (!strcmp(name, "NodeCoord")) {
+    // a mesh file's grid: the initial positions of a Lagrangian case (the
+    // remap and the pressure surfaces go back to the cartesian grid)
+    if (h->P.with_projection) return set_err(MHC_ERR_UNSUPPORTED, "mesh-file coordinates with the remap");
+    for (int b = 0; b < h->P.nb_bc; ++b)
+      if (h->P.bc[b].kind == MHC_BC_GEOMETRIC_PRESSURE || h->P.bc[b].kind == MHC_BC_LINEAR_PRESSURE)
+        return set_err(MHC_ERR_UNSUPPORTED, "mesh-file coordinates with pressure surfaces");
+    if (n < 3 * NN) return set_err(MHC_ERR_ARG, "too few values");
+    std::vector<double> x(3 * NN);
+    for (long long i = 0; i < NN; ++i)
+      for (int d = 0; d < 3; ++d) x[d * NN + i] = host[3 * i + d];
+    if ((r = grow(&F.x0, 3 * NN * sizeof(double))) || (r = upload(st, F.x0, x.data(), 3 * NN * 8))) return r;
+    return 3 * NN;
+  }
+  const int slot = !strcmp(name, "Materiau") ? 0 : !strcmp(name, "Density") ? 1 : !strcmp(name, "Pressure") ? 2 : -1;
+  if (slot < 0) return set_err(MHC_ERR_ARG, std::string("unknown initial field ") + name);
+  if (h->P.cas_model != MHC_CASE_EXTERNAL)
+    return set_err(MHC_ERR_ARG, "Materiau / Density / Pressure initial fields are for the EXTERNAL case model");
+  if (n < N) return set_err(MHC_ERR_ARG, "too few values");
+  if (!F.init) {
+    // the ones not given: environment 0 and its initial state
+    std::vector<double> d(3 * N);
+    for (long long i = 0; i < N; ++i) {
+      d[i] = 0.;
+      d[N + i] = h->P.env[0].densite_initiale;
+      d[2 * N + i] = h->P.env[0].pression_initiale;
+    }
+    if ((r = grow(&F.init, 3 * N * sizeof(double))) || (r = upload(st, F.init, d.data(), 3 * N * 8))) return r;
+  }
+  if ((r = upload(st, F.init + slot * N, host, N * 8))) return r;
+  return N;
+}
+
+// ---------------------------------------------------------------------------
 // field upload
 // ---------------------------------------------------------------------------
 long long mhc_set_field(mhc_case* h, const char* name, int env, const double* host, long long n) {

@@ -160,6 +160,8 @@ def run_case(p: CaseParams, info: dict, out_dir: str, max_iter: int = 10 ** 7) -
     period = p.time_history_period if p.time_history_period > 0 else 10
     h = Hydro(p)
     try:
+        for name, values in info.get("init_fields", {}).items():
+            h.set_initial_field(name, values)
         h.hydroStartInit()
         init_files = []
         if info.get("save_init"):

@@ -172,6 +172,12 @@ struct Case {
   bool stop = false;
   std::vector<THLine> th;
 
+  /* EXTERNAL initial state given per cell (the dataset's <initialisation>
+   * block); empty: environment 0 and its initial state everywhere */
+  std::vector<double> init_mat, init_rho, init_p;
+  /* the k-th cell of the reference's numbering (mesh_cell_order) */
+  std::vector<long> order;
+  long ord(long k) const { return order.empty() ? k : order[k]; }
   long cid(int i, int j, int k) const { return i + (long)ncx * (j + (long)ncy * k); }
   long nid(int i, int j, int k) const { return i + (long)nnx * (j + (long)nny * k); }
   void cijk(long c, int& i, int& j, int& k) const {
@@ -607,6 +613,8 @@ static void init_materials(Case& C) {
     } else if (P.cas_model == MHC_CASE_BUBBLES && C.nenv > 1) {
       double f;
       m = bubble_material(C, c, f);
+    } else if (P.cas_model == MHC_CASE_EXTERNAL) {
+      m = C.init_mat.empty() ? 0. : C.init_mat[c];
     } else if (P.cas_model == MHC_CASE_RIDER && !rider_mono(P)) {
       /* RIDERService::initMat (RIDERService.cc:18-57); MonoRider*: initMatMono */
       double rmin, rmax;
@@ -692,6 +700,22 @@ static void init_variables(Case& C) {
       }
     }
     for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
+  } else if (P.cas_model == MHC_CASE_EXTERNAL) {
+    /* the dataset's <initialisation> values, then EXTERNALService::initUtilisateur
+     * (EXTERNALService.cc:25-40) for every environment that asks for it
+     * (MahycoModule.cc:132-139): its initial velocity, or -x/|x| when that
+     * is zero */
+    for (long c = 0; c < C.ncell; ++c) {
+      C.density.g[c] = C.init_rho.empty() ? P.env[0].densite_initiale : C.init_rho[c];
+      C.pressure.g[c] = C.init_p.empty() ? P.env[0].pression_initiale : C.init_p[c];
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {0., 0., 0.};
+    for (int e = 0; e < C.nenv; ++e) {
+      if (!P.env[e].initialisation_utilisateur) continue;
+      const R3 v0 = {P.env[e].vitesse_initiale[0], P.env[e].vitesse_initiale[1], P.env[e].vitesse_initiale[2]};
+      const bool zero = v0.x == 0. && v0.y == 0. && v0.z == 0.;
+      for (long n = 0; n < C.nnode; ++n) C.vel[n] = zero ? (-C.coord[n]) / norm(C.coord[n]) : v0;
+    }
   } else if (P.cas_model == MHC_CASE_RIDER) {
     /* RIDERService::initVar / initVarMono (RIDERService.cc:62-173, 178-289) */
     const bool mono = rider_mono(P), lin = P.rider_linear_density != 0;
@@ -873,6 +897,12 @@ static void setup(Case& C, const mhc_case_params* p) {
   C.delta_ar.assign(C.ncell * C.nvars, 0.);
   C.delta_av.assign(C.ncell * C.nvars, 0.);
   C.est_mixte.assign(C.ncell, 0);
+  if (p->mesh_cell_order == 1 && C.dim == 2) {
+    C.order.resize(C.ncell);
+    long k = 0;
+    for (int i = 0; i < C.ncx; ++i)
+      for (int j = 0; j < C.ncy; ++j) C.order[k++] = C.cid(i, j, 0);
+  }
   C.est_pure.assign(C.ncell, 0);
 }
 
@@ -920,7 +950,8 @@ static int hydro_start_init(Case& C) {
   /* computeNodeMass */
   std::fill(C.node_mass.begin(), C.node_mass.end(), 0.);
   const double w = C.dim == 2 ? .25 : .125;
-  for (long c = 0; c < C.ncell; ++c) {
+  for (long k = 0; k < C.ncell; ++k) {
+    const long c = C.ord(k);
     double contrib = w * C.cell_mass.g[c];
     for (int l = 0; l < C.nbn; ++l) C.node_mass[C.cnode(c, l)] += contrib;
   }
@@ -973,12 +1004,14 @@ static void update_velocity_without_lagrange(Case& C) {
  * the anti-hourglass correction of a Lagrangian run */
 static void update_velocity(Case& C) {
   for (auto& f : C.force) f = {0., 0., 0.};
-  for (long c = 0; c < C.ncell; ++c) {
+  for (long k = 0; k < C.ncell; ++k) {
+    const long c = C.ord(k);
     double pressure = C.pressure_n.g[c] + C.pseudo_n.g[c];
     for (int l = 0; l < C.nbn; ++l) C.force[C.cnode(c, l)] += pressure * C.cqs_n[c * C.nbn + l];
   }
   if (C.elasto) {
-    for (long c = 0; c < C.ncell; ++c) {
+    for (long k = 0; k < C.ncell; ++k) {
+      const long c = C.ord(k);
       const double* S = &C.sdev_n[c * 6];
       /* force_tensor = -S_n; prodTensVec(t, v) = (t.x.v, t.y.v, t.z.v) */
       const R3 tx = {-S[0], -S[3], -S[5]}, ty = {-S[3], -S[1], -S[4]}, tz = {-S[5], -S[4], -S[2]};
@@ -1010,7 +1043,8 @@ static void update_velocity(Case& C) {
       if (C.dim == 3) m *= (k > 0 && k < C.nnz - 1) ? 2 : 1;
       return (double)m;
     };
-    for (long c = 0; c < C.ncell; ++c) {
+    for (long k = 0; k < C.ncell; ++k) {
+      const long c = C.ord(k);
       long nd[8];
       R3 v[8];
       for (int l = 0; l < C.nbn; ++l) { nd[l] = C.cnode(c, l); v[l] = C.vel[nd[l]]; }
@@ -1304,16 +1338,19 @@ static void update_elasticity_and_plasticity(Case& C) {
     }
     S[0] = sxx + P[0][0]; S[1] = syy + P[1][1]; S[2] = szz + P[2][2];
     S[3] = sxy + P[0][1]; S[4] = syz + P[1][2]; S[5] = szx + P[2][0];
-    /* ComputePlasticity (173-226): radial return onto the yield surface */
-    double j2 = S[0] * S[0];
-    j2 += S[1] * S[1];
+    /* ComputePlasticity (173-226): radial return onto the yield surface;
+     * the squares are math::pow(x, 2.) there (glibc's pow, or the correctly
+     * rounded square x * x with cr_pow) */
+    auto sq = [](double x) { return g_cr_pow ? x * x : std::pow(x, 2.); };
+    double j2 = sq(S[0]);
+    j2 += sq(S[1]);
     j2 += S[0] * S[1];
-    j2 += S[3] * S[3];
+    j2 += sq(S[3]);
     if (C.dim == 3) {
-      j2 += S[4] * S[4];
-      j2 += S[5] * S[5];
+      j2 += sq(S[4]);
+      j2 += sq(S[5]);
     }
-    if (j2 > (Y * Y) / 3.) {
+    if (j2 > sq(Y) / 3.) {
       const double coeff = Y / std::sqrt(3. * j2);
       for (int q = 0; q < 6; ++q) S[q] *= coeff;
     }
@@ -2394,18 +2431,21 @@ static void time_history_write(Case& C) {
   for (int e = 0; e < C.nenv; ++e) {
     long cnt = 0;
     double m = 0., p = 0., rv = 0., vv = 0., em = 0., mm = 0.;
-    for (long c = 0; c < C.ncell; ++c) {
+    for (long k = 0; k < C.ncell; ++k) {
+      const long c = C.ord(k);
       if (!C.has(c, e)) continue;
       ++cnt;
       m += C.EV(C.cell_mass, e, c);
       p += C.EV(C.pressure, e, c);
     }
-    for (long c = 0; c < C.ncell; ++c) {
+    for (long k = 0; k < C.ncell; ++k) {
+      const long c = C.ord(k);
       if (!C.has(c, e)) continue;
       em += C.EV(C.internal_energy, e, c) * C.EV(C.cell_mass, e, c);
       mm += C.EV(C.cell_mass, e, c);
     }
-    for (long c = 0; c < C.ncell; ++c) {
+    for (long k = 0; k < C.ncell; ++k) {
+      const long c = C.ord(k);
       if (!C.has(c, e)) continue;
       rv += C.EV(C.density, e, c) * C.EV(C.cell_volume, e, c);
       vv += C.EV(C.cell_volume, e, c);
@@ -2587,6 +2627,25 @@ long oracle_set_field(void* h, const char* name, int env, const double* in, long
     return 3 * C.nnode;
   }
   return -2;
+}
+
+/* initial state of the EXTERNAL case model and node coordinates read from a
+ * mesh file, before oracle_init: NodeCoord (3 per node, interleaved),
+ * Materiau, Density, Pressure (one per cell) */
+int oracle_set_initial_field(void* h, const char* name, const double* in, long n) {
+  ora::Case& C = *(ora::Case*)h;
+  if (!strcmp(name, "NodeCoord")) {
+    if (n < 3 * C.nnode) return -1;
+    for (long i = 0; i < C.nnode; ++i) C.coord[i] = ora::R3{in[3 * i], in[3 * i + 1], in[3 * i + 2]};
+    return 3 * C.nnode;
+  }
+  std::vector<double>* v = !strcmp(name, "Materiau") ? &C.init_mat
+                           : !strcmp(name, "Density") ? &C.init_rho
+                           : !strcmp(name, "Pressure") ? &C.init_p : nullptr;
+  if (!v) return -2;
+  if (n < C.ncell) return -1;
+  v->assign(in, in + C.ncell);
+  return C.ncell;
 }
 
 /* IEquationOfState::applyEOS(env) on the current state, then

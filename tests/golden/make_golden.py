@@ -94,6 +94,16 @@ CASES = {
     "CAS_MonoRiderVortexTimeReverse": {"mpi_ranks": 8},
     "CAS_RiderDeformationTimeReverse": {"mpi_ranks": 8},
     "CAS_MonoRiderDeformationTimeReverse": {"mpi_ranks": 8},
+    # Gmsh grid (plaqueTaylor.msh, numbered column by column), EXTERNAL
+    # init with a user velocity, Mie-Gruneisen, elasto-plastic, explicit
+    # pressure, anti-hourglass.  The oracle's EnvSummation lines equal the
+    # reference's bit for bit for the first 32 lines (320 iterations); then
+    # the mean pressure drifts by at most 1.5e-5 relative (density 1.2e-9,
+    # energy 6.8e-9); the reference's elasticity update reads an
+    # uninitialised trace (elasto/DefaultModelService.cc:82, 96), which the
+    # restatement takes as 0
+    "CAS_2D_Lag_Taylor_elasto": {"exact_lines": 32, "time_tol": 3e-7,
+                                 "tol_var": {"Pressure": 3e-5, "Density": 3e-9, "InternalEnergy": 2e-8}},
 }
 # variables the Ensight writer of mahyco_b200.output produces
 ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy", "PseudoViscosity",
@@ -121,7 +131,9 @@ def main(ref_root, only=()):
         # run writes only its first sub-domain, so none are kept for those
         dep = os.path.join(d, "output", "depouillement")
         digests = {}
-        if extra.get("mpi_ranks", 1) == 1 and set(info["output_vars"]) <= ENSIGHT_VARS:
+        # (a mesh file's run numbers its nodes and cells like the file, the
+        # library like its grid: no digest for those)
+        if extra.get("mpi_ranks", 1) == 1 and set(info["output_vars"]) <= ENSIGHT_VARS and not info["init_fields"]:
             for root, _, files in os.walk(dep):
                 for fn in sorted(files):
                     full = os.path.join(root, fn)
@@ -129,6 +141,8 @@ def main(ref_root, only=()):
         out = {"case": case, "params": params_to_dict(p), "env_names": info["env_names"],
                "timeloop": info["timeloop"], "extra": extra, "time_history": hist,
                "output_vars": info["output_vars"], "save_init": info["save_init"], "ensight_sha256": digests}
+        if info["init_fields"]:
+            out["init_fields"] = info["init_fields"]
         with open(os.path.join(HERE, case + ".json"), "w") as f:
             json.dump(out, f, indent=0)
         print(case, {k: len(v) for k, v in hist.items()})

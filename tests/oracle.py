@@ -38,6 +38,8 @@ def lib() -> C.CDLL:
     L.oracle_get_field.restype = C.c_long
     L.oracle_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_long]
     L.oracle_eos_apply.argtypes = [C.c_void_p, C.c_int]
+    L.oracle_set_initial_field.restype = C.c_int
+    L.oracle_set_initial_field.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.c_long]
     L.oracle_set_field.restype = C.c_long
     L.oracle_set_field.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_double), C.c_long]
     L.oracle_th_count.restype = C.c_long
@@ -91,6 +93,12 @@ class Oracle:
         got = self.L.oracle_get_field(self.h, name.encode(), env, out.ctypes.data_as(C.POINTER(C.c_double)), n)
         assert got == n, (name, got)
         return out
+
+    def set_initial_field(self, name: str, values) -> None:
+        """EXTERNAL initial state / mesh-file node coordinates, before init()."""
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        got = self.L.oracle_set_initial_field(self.h, name.encode(), a.ctypes.data_as(C.POINTER(C.c_double)), a.size)
+        assert got > 0, (name, got)
 
     def set_field(self, name: str, values: np.ndarray, env: int = -1) -> None:
         a = np.ascontiguousarray(values, dtype=np.float64)

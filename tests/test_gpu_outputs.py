@@ -32,7 +32,8 @@ def test_gpu_outputs_match_reference_files(path, tmp_path):
     from mahyco_b200.output import run_case
     g = json.load(open(path))
     r = run_case(params_from_dict(g["params"]), {"env_names": g["env_names"], "output_vars": g["output_vars"],
-                                                 "save_init": g.get("save_init", False)}, str(tmp_path))
+                                                 "save_init": g.get("save_init", False),
+                                                 "init_fields": g.get("init_fields", {})}, str(tmp_path))
     assert r["scalars"]["status"] == 8, r["scalars"]  # stopped at the final time
     dep = tmp_path / "depouillement"
     bad = [k for k, v in g["ensight_sha256"].items() if ensight_digest.digest(str(dep / k)) != v]
