@@ -45,7 +45,12 @@ enum mhc_bc_kind {
    * density (and cell mass, added to the node masses), an added internal
    * energy (flat or super-Gaussian in y, inside the x / y cutoffs), the
    * pressure */
-  MHC_BC_DENSITY = 5, MHC_BC_ENERGY = 6, MHC_BC_SUPER_GAUSSIAN_ENERGY = 7, MHC_BC_PRESSURE = 8
+  MHC_BC_DENSITY = 5, MHC_BC_ENERGY = 6, MHC_BC_SUPER_GAUSSIAN_ENERGY = 7, MHC_BC_PRESSURE = 8,
+  /* pressure surfaces (MahycoModule.cc:952-970): the value times
+   * exp(-(y dY)^power) exp(-(x dX)^power) at the node, 0 beyond |y| >
+   * cutoffY; or times sqrt(1 - x^2/a2 - y^2/b2) at the boundary cell's
+   * centre (a2 = dependanceX, b2 = dependanceY), 0 outside that ellipse */
+  MHC_BC_SUPER_GAUSSIAN_PRESSURE = 9, MHC_BC_CONTACT_HERZ_PRESSURE = 10
 };
 
 /* energy deposits (TypesMahyco.h eEnergyDepot): constant, linear in
@@ -161,7 +166,8 @@ typedef struct mhc_bc {
   double value;
   double tdebut, tfin;
   double dependance[4];  /* LinearPressure: dependanceX, Y, Z, T; SuperGaussianEnergy: dependanceY */
-  double cutoff[2];      /* Energy, SuperGaussianEnergy: cutoffX, cutoffY */
+  double cutoff[2];      /* Energy, SuperGaussianEnergy: cutoffX, cutoffY; SuperGaussianPressure: cutoffY */
+  double power;          /* SuperGaussianPressure: the exponent (default 4) */
 } mhc_bc;
 
 typedef struct mhc_case_params {

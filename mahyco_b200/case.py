@@ -19,7 +19,8 @@ EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN, EOS_FICTIF = 0, 1, 2, 3
 EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
                "MieGruneisen": EOS_MIE_GRUNEISEN, "Fictif": EOS_FICTIF}
 BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4, "Density": 5,
-              "Energy": 6, "SuperGaussianEnergy": 7, "Pressure": 8}
+              "Energy": 6, "SuperGaussianEnergy": 7, "Pressure": 8, "SuperGaussianPressure": 9,
+              "ContactHerzPressure": 10}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
 CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES, CASE_RIDER, CASE_EXTERNAL = 1, 2, 3, 4, 5, 6, 7
 CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL, "CHOCBULLE": CASE_BUBBLES,
@@ -67,7 +68,7 @@ class EnvParams(C.Structure):
 class BC(C.Structure):
     _fields_ = [("kind", C.c_int), ("surface", C.c_int), ("value", C.c_double),
                 ("tdebut", C.c_double), ("tfin", C.c_double), ("dependance", C.c_double * 4),
-                ("cutoff", C.c_double * 2)]
+                ("cutoff", C.c_double * 2), ("power", C.c_double)]
 
 
 class CaseParams(C.Structure):
@@ -160,6 +161,7 @@ def default_params() -> CaseParams:
     p.nb_bc = 0
     for b in p.bc:
         b.cutoff[:] = (1000.0, 1000.0)
+        b.power = 4.0
     p.ordre_projection = 2
     p.projection_limiteur_id = MINMOD
     p.is_euler_scheme = 0
@@ -172,13 +174,14 @@ def default_params() -> CaseParams:
 
 def add_bc(p: CaseParams, surface: str, kind: str, value: float = 0.0,
            tdebut: float = 0.0, tfin: float = 1000.0, dependance=(0.0, 0.0, 0.0, 0.0),
-           cutoff=(1000.0, 1000.0)) -> None:
+           cutoff=(1000.0, 1000.0), power: float = 4.0) -> None:
     if p.nb_bc >= MAX_BC:
         raise ValueError("too many boundary conditions")
     b = p.bc[p.nb_bc]
     b.kind, b.surface, b.value, b.tdebut, b.tfin = BC_BY_NAME[kind], SURFACES[surface], value, tdebut, tfin
     b.dependance[:] = dependance
     b.cutoff[:] = cutoff
+    b.power = power
     p.nb_bc += 1
 
 
@@ -410,7 +413,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         add_bc(p, surf, kind, _txt(b, "value", 0.0),
                _txt(b, "Tdebut", 0.0), _txt(b, "Tfin", 1000.0),
                tuple(_txt(b, t, 0.0) for t in ("dependanceX", "dependanceY", "dependanceZ", "dependanceT")),
-               (_txt(b, "cutoffX", 1000.0), _txt(b, "cutoffY", 1000.0)))
+               (_txt(b, "cutoffX", 1000.0), _txt(b, "cutoffY", 1000.0)), _txt(b, "power", 4.0))
     th = root.find("time-history/bilan")
     if th is not None:
         p.time_history_period = _txt(th, "periode", 10, int)

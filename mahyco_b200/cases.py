@@ -499,13 +499,18 @@ PARITY_CASES = {
     # the cells numbered column by column (mesh_cell_order 1)
     "lag2d_external_implosion": (lambda: _external(deltat_init=1e-4), 150),
     "lag2d_external_colmajor_bar": (lambda: _external(velocity=(0.0, -0.3, 0.0), colmajor=True, deltat_init=1e-4), 150),
+    # pressure surfaces of a contact ellipse (ContactHerzPressure, at the
+    # boundary cell's centre) and of a super-Gaussian spot
+    # (SuperGaussianPressure, exp and pow at the node)
+    "lag3d_contact_herz_pressure": (lambda: _spot(_herz=True), 120),
+    "lag2d_super_gaussian_pressure": (lambda: _spot(_herz=False), 120),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
 # calls exp and pow, and the reverse option of RIDER scales the velocities by
 # cos(Pi t), which CUDA and the oracle's libm round differently
 PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13,
-                    "adv3d_rider_deformation_reverse": 1e-12}
+                    "adv3d_rider_deformation_reverse": 1e-12, "lag2d_super_gaussian_pressure": 1e-12}
 
 
 def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> CaseParams:
@@ -526,6 +531,25 @@ def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> Cas
     p.mesh_cell_order = 1 if colmajor else 0
     p.deltat_init, p.deltat_max = deltat_init, 1e-3
     symmetry_bcs(p, ("XMIN", "YMIN"))
+    return p
+
+
+def _spot(_herz: bool) -> CaseParams:
+    """An aluminium block (as ``compression``) loaded on its top side by a
+    contact ellipse of semi-axes^2 (4e-12, 9e-12) (3D, ZMAX) or a
+    super-Gaussian spot of power 2 (2D, YMAX), from t = 1e-12."""
+    if _herz:
+        p = compression(dim=3, n=(8, 8, 10), L=(4e-6, 4e-6, 5e-6), coef_antiderive=0.01)
+    else:
+        p = compression(dim=2, n=(24, 16), L=(6e-6, 4e-6))
+    p.nb_bc = 0
+    add_bc(p, "XMIN", "Vx", 0.0)
+    add_bc(p, "YMIN", "Vy", 0.0)
+    if _herz:
+        add_bc(p, "ZMIN", "Vz", 0.0)
+        add_bc(p, "ZMAX", "ContactHerzPressure", 2e9, 1e-12, 1e-9, (4e-12, 9e-12, 0.0, 0.0))
+    else:
+        add_bc(p, "YMAX", "SuperGaussianPressure", 2e9, 1e-12, 1e-9, (3e5, 0.0, 0.0, 0.0), (1000.0, 1000.0), 2.0)
     return p
 
 

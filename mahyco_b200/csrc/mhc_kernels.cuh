@@ -802,7 +802,9 @@ __device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params&
   const double w = DIM == 2 ? .5 : .25, wc = DIM == 2 ? .25 : .125;
   for (int b = 0; b < P.nb_bc; ++b) {
     const mhc_bc& bc = P.bc[b];
-    if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE) continue;
+    if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE &&
+        bc.kind != MHC_BC_SUPER_GAUSSIAN_PRESSURE && bc.kind != MHC_BC_CONTACT_HERZ_PRESSURE)
+      continue;
     const int s = bc.surface;
     const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
     if (d >= DIM) continue;
@@ -830,7 +832,7 @@ __device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params&
           int a, bb, c;
           face_node_rt(DIM, d, q, a, bb, c);
           fn[q] = node_id(M, f[0] + a, f[1] + bb, DIM == 3 ? f[2] + c : 0);
-          fc = fc + w * node_x0(M, f[0] + a, f[1] + bb, DIM == 3 ? f[2] + c : 0);
+          fc = fc + w * node_initial(M, F, f[0] + a, f[1] + bb, DIM == 3 ? f[2] + c : 0);
           if (fn[q] == n) me = q;
         }
         auto X = [&](long long m) { return R3{F.Xp[0][m], F.Xp[1][m], F.Xp[2][m]}; };
@@ -861,6 +863,19 @@ __device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params&
           value += bc.dependance[1] * x.y;
           value += bc.dependance[2] * x.z;
           value += bc.dependance[3] * t;
+        } else if (bc.kind == MHC_BC_SUPER_GAUSSIAN_PRESSURE) {
+          // CUDA's exp and pow, within a few ulps of the reference's libm
+          const R3 x = X(n);
+          const double ay = x.y * bc.dependance[1];
+          value *= exp(-pow(ay, bc.power));
+          const double ax = x.x * bc.dependance[0];
+          value *= exp(-pow(ax, bc.power));
+          if (fabs(x.y) > bc.cutoff[1]) value = 0.;
+        } else if (bc.kind == MHC_BC_CONTACT_HERZ_PRESSURE) {
+          const double a2 = bc.dependance[0], b2 = bc.dependance[1];
+          const double x2 = cc.x * cc.x, y2 = cc.y * cc.y;
+          if (x2 / a2 + y2 / b2 < 1.) value *= sqrt(1 - x2 / a2 - y2 / b2);
+          else value = 0.;
         }
         if (t < bc.tdebut) value = 0.;
         if (t >= bc.tfin) value = 0.;

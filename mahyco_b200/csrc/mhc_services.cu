@@ -161,7 +161,10 @@ void mhc_case_params_default(mhc_case_params* p) {
   p->final_time = 1.e30;
   p->threshold = 1.e-10;
   p->with_projection = 1;
-  for (int b = 0; b < MHC_MAX_BC; ++b) p->bc[b].cutoff[0] = p->bc[b].cutoff[1] = 1000.;
+  for (int b = 0; b < MHC_MAX_BC; ++b) {
+    p->bc[b].cutoff[0] = p->bc[b].cutoff[1] = 1000.;
+    p->bc[b].power = 4.;
+  }
   p->ordre_projection = 2;
   p->projection_limiteur_id = MHC_MINMOD;
   p->is_euler_scheme = MHC_EULER_FULL;
@@ -193,9 +196,6 @@ long long mhc_case_set_initial_field(mhc_case* h, const char* name, const double
     // a mesh file's grid: the initial positions of a Lagrangian case (the
     // remap and the pressure surfaces go back to the cartesian grid)
     if (h->P.with_projection) return set_err(MHC_ERR_UNSUPPORTED, "mesh-file coordinates with the remap");
-    for (int b = 0; b < h->P.nb_bc; ++b)
-      if (h->P.bc[b].kind == MHC_BC_GEOMETRIC_PRESSURE || h->P.bc[b].kind == MHC_BC_LINEAR_PRESSURE)
-        return set_err(MHC_ERR_UNSUPPORTED, "mesh-file coordinates with pressure surfaces");
     if (n < 3 * NN) return set_err(MHC_ERR_ARG, "too few values");
     std::vector<double> x(3 * NN);
     for (long long i = 0; i < NN; ++i)

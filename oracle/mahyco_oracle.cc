@@ -1123,7 +1123,9 @@ static void apply_pressure_bcs(Case& C) {
   for (int b = 0; b < C.P.nb_bc; ++b) {
     const mhc_bc& bc = C.P.bc[b];
     const bool cellvar = bc.kind >= MHC_BC_DENSITY && bc.kind <= MHC_BC_PRESSURE;
-    if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE && !cellvar) continue;
+    const bool surface = bc.kind == MHC_BC_GEOMETRIC_PRESSURE || bc.kind == MHC_BC_LINEAR_PRESSURE ||
+                         bc.kind == MHC_BC_SUPER_GAUSSIAN_PRESSURE || bc.kind == MHC_BC_CONTACT_HERZ_PRESSURE;
+    if (!surface && !cellvar) continue;
     const int s = bc.surface;
     const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
     if (d >= C.dim) continue;
@@ -1184,6 +1186,19 @@ static void apply_pressure_bcs(Case& C) {
           value += bc.dependance[1] * C.coord[node].y;
           value += bc.dependance[2] * C.coord[node].z;
           value += bc.dependance[3] * C.t;
+        } else if (bc.kind == MHC_BC_SUPER_GAUSSIAN_PRESSURE) {
+          /* MahycoModule.cc:952-959 */
+          const double ay = C.coord[node].y * bc.dependance[1];
+          value *= std::exp(-std::pow(ay, bc.power));
+          const double ax = C.coord[node].x * bc.dependance[0];
+          value *= std::exp(-std::pow(ax, bc.power));
+          if (std::fabs(C.coord[node].y) > bc.cutoff[1]) value = 0.;
+        } else if (bc.kind == MHC_BC_CONTACT_HERZ_PRESSURE) {
+          /* MahycoModule.cc:960-970, at the boundary cell's centre */
+          const double a2 = bc.dependance[0], b2 = bc.dependance[1];
+          const double x2 = C.cell_coord[c].x * C.cell_coord[c].x, y2 = C.cell_coord[c].y * C.cell_coord[c].y;
+          if (x2 / a2 + y2 / b2 < 1.) value *= std::sqrt(1 - x2 / a2 - y2 / b2);
+          else value = 0.;
         }
         if (C.t < bc.tdebut) value = 0.;
         if (C.t >= bc.tfin) value = 0.;
