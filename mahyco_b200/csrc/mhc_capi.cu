@@ -355,11 +355,25 @@ void launch_remap(Engine* e) {
   launch_remap_variables(e);
 }
 
+// node speeds stored by the node finalize pass for computeDeltaT;
+// MHC_NODE_SPEED=0 in the environment recomputes them per cell corner
+bool spd_enabled() {
+  static const bool v = [] {
+    const char* s = getenv("MHC_NODE_SPEED");
+    return !(s && *s == '0');
+  }();
+  return v;
+}
+
 void launch_dt(Engine* e) {
   StageTimer tm(e, MHC_STAGE_DELTA_T);
   for (Group& g : e->groups) {
-    // sans-lagrange keeps deltat_init: no CFL reduction
-    if (!g.ADV) DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_>, CT, 0, g.dt)));
+    // sans-lagrange keeps deltat_init: no CFL reduction; a Full Euler group
+    // whose remap ran reads the node speeds its node finalize pass stored
+    int dirs[3];
+    const bool spd = g.EULER == 1 && group_dirs(e, g, dirs) > 0 && spd_enabled();
+    if (!g.ADV && spd) DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_, true>, CT, 0, g.dt)));
+    else if (!g.ADV) DISPATCH_GROUP(g, (plaunch(e, kb_delta_t<DIM_>, CT, 0, g.dt)));
     if (g.cases.n > 0) {
       kb_delta_t_finalize<<<cdiv(g.cases.n, 128), 128, 0, e->stream>>>(e->d_desc, e->d_ints + g.cases.off_cases, g.cases.n);
       ++e->launches;
@@ -527,7 +541,7 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8) +
                     (p->projection_pente_borne ? nv : 0) + 2;  // (+2: boundary-condition energy, pressure)
   const bool csts = p->schema_csts && p->with_projection;
-  long long nodes = 4 + 6 + 10 + ((p->sans_lagrange || csts) ? 3 : 0) + (csts ? 3 : 0);
+  long long nodes = 4 + 6 + 10 + ((p->sans_lagrange || csts) ? 3 : 0) + (csts ? 3 : 0) + ((p->with_projection && p->is_euler_scheme == MHC_EULER_FULL && !p->sans_lagrange) ? 1 : 0);
   if (csts) cells += 1;
   return cells * ncell + nodes * nnode;
 }
@@ -728,6 +742,7 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   if (h->P.projection_pente_borne) F.phi_pb = (double*)alloc(h->NV * N * sizeof(double));
   const bool csts = h->P.schema_csts && h->P.with_projection;
   if (h->P.sans_lagrange || csts) F.v0 = (double*)alloc(3 * NN * sizeof(double));
+  if (h->P.with_projection && h->P.is_euler_scheme == MHC_EULER_FULL && !h->P.sans_lagrange) F.spd = dnode();
   if (csts) {
     F.pq = dcell();
     for (int d = 0; d < 3; ++d) F.fv[d] = dnode();

@@ -63,6 +63,7 @@ struct Fields {
   double* fv[3];           // the node terms of the remap's face velocities: vx, vy, vz themselves,
                            // or (CSTS) the means of the velocities at n and n+1
   double* pq;              // CSTS: pressure + pseudo-viscosity of the forces at n+1 [ncell]
+  double* spd;             // Full Euler remap: |v| of every node after the remap, for computeDeltaT [nnode]
   double* x0;              // initial node coordinates read from a mesh file [3][nnode] (else the
                            // cartesian grid)
   double* init;            // EXTERNAL initial state given per cell: Materiau, Density, Pressure
@@ -2018,11 +2019,15 @@ __device__ __forceinline__ void body_remap_finalize_nodes(const Mesh& M, const F
   if (n >= M.nnode) return;
   const long long NN = M.nnode;
   double m = DUAL ? Ud[3 * NN + n] : 0.;
+  double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
   if (m != 0.) {
-    F.vx[n] = div_rn(Ud[n], m);
-    F.vy[n] = div_rn(Ud[NN + n], m);
-    F.vz[n] = div_rn(Ud[2 * NN + n], m);
+    vx = div_rn(Ud[n], m);
+    vy = div_rn(Ud[NN + n], m);
+    vz = div_rn(Ud[2 * NN + n], m);
+    F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   }
+  // the node speed of computeDeltaT (Vector normL2), once per node
+  if (F.spd) F.spd[n] = sqrt(vx * vx + vy * vy + vz * vz);
   int i, j, k;
   node_ijk(M, n, i, j, k);
   F.mn[n] = node_mass_gather<DIM>(M, F.m, i, j, k);
@@ -2033,7 +2038,7 @@ __device__ __forceinline__ void body_remap_finalize_nodes(const Mesh& M, const F
 // minimum, then one ordered-bits atomicMin per block.  The minimum of
 // non-NaN values does not depend on the reduction order.
 // ---------------------------------------------------------------------------
-template <int DIM>
+template <int DIM, bool SPD = false>
 __device__ __forceinline__ void body_delta_t(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   long long c = bx * (long long)CT + threadIdx.x;
   double dx = 1.7976931348623157e308;
@@ -2046,8 +2051,12 @@ __device__ __forceinline__ void body_delta_t(const Mesh& M, const mhc_case_param
         int a, b, d;
         local_node_offset(l, a, b, d);
         long long n = node_id(M, i + a, j + b, k + d);
-        double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
-        vmax = amax(sqrt(vx * vx + vy * vy + vz * vz), vmax);
+        if (SPD) {
+          vmax = amax(__ldg(F.spd + n), vmax);  // stored by the node finalize pass of this iteration
+        } else {
+          double vx = F.vx[n], vy = F.vy[n], vz = F.vz[n];
+          vmax = amax(sqrt(vx * vx + vy * vy + vz * vz), vmax);
+        }
       }
     }
     dx = F.l[c] / (F.c[c] + vmax);

@@ -476,7 +476,8 @@ static __global__ void __launch_bounds__(CT) kb_euler_axis_reset(const CaseDesc*
   }
 }
 
-template <int DIM>
+// SPD: the node speeds stored by the node finalize pass (remap cases)
+template <int DIM, bool SPD = false>
 __global__ void __launch_bounds__(CT) kb_delta_t(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {
     const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
@@ -484,7 +485,7 @@ __global__ void __launch_bounds__(CT) kb_delta_t(const CaseDesc* __restrict__ C,
     if (!case_active(F)) continue;
     resolve_positions(F);
     const Mesh M = C[wi.c].M;
-    body_delta_t<DIM>(M, *C[wi.c].P, F, wi.x);
+    body_delta_t<DIM, SPD>(M, *C[wi.c].P, F, wi.x);
     __syncthreads();
   }
 }
