@@ -74,6 +74,9 @@ int mhc_case_restore(mhc_case* h, const void* host, long long size);
  * SOD case model, one environment, a 1x1x1 3D mesh on the unit cube) for a
  * host that then sets the options of its .arc dataset.  Host only. */
 void mhc_case_params_default(mhc_case_params* p);
+/* sizeof(mhc_case_params) as this library was built, for bindings that
+ * mirror the structure (no device work) */
+long long mhc_case_params_size(void);
 
 /* HBM bytes one case with these parameters needs (serving admission). */
 long long mhc_case_device_bytes(const mhc_case_params* params);

@@ -25,6 +25,7 @@ extern "C" {
 
 #define MHC_MAX_ENV 4
 #define MHC_MAX_BC 12
+#define MHC_MAX_PTABLE 32
 
 /* equation-of-state service kinds (<eos-model name="...">) */
 enum mhc_eos_kind {
@@ -36,7 +37,8 @@ enum mhc_eos_kind {
                                 phase, sans_lagrange) */
 };
 
-/* boundary-condition kinds, same numbering as TypesMahyco::eBoundaryCondition */
+/* boundary-condition kinds, named after TypesMahyco::eBoundaryCondition
+ * (TypesMahyco.h:16-32) and numbered in the order this library added them */
 enum mhc_bc_kind {
   MHC_BC_VX = 0, MHC_BC_VY = 1, MHC_BC_VZ = 2,
   /* pressure applied as a node force on the surface (MahycoModule.cc:909-986) */
@@ -50,7 +52,19 @@ enum mhc_bc_kind {
    * exp(-(y dY)^power) exp(-(x dX)^power) at the node, 0 beyond |y| >
    * cutoffY; or times sqrt(1 - x^2/a2 - y^2/b2) at the boundary cell's
    * centre (a2 = dependanceX, b2 = dependanceY), 0 outside that ellipse */
-  MHC_BC_SUPER_GAUSSIAN_PRESSURE = 9, MHC_BC_CONTACT_HERZ_PRESSURE = 10
+  MHC_BC_SUPER_GAUSSIAN_PRESSURE = 9, MHC_BC_CONTACT_HERZ_PRESSURE = 10,
+  /* OnFileVelocity ("OFV", MahycoModule.cc:796-798): the node's x and y
+   * velocities set to -x / |X| and -y / |X| from its position X at the
+   * start of the cycle (a unit velocity towards the origin); the value is
+   * not used */
+  MHC_BC_ON_FILE_VELOCITY = 11,
+  /* OnFilePressure (MahycoModule.cc:987-1030): a pressure surface whose
+   * value is the case's (time, pressure) table interpolated linearly at the
+   * current time (0 before the first time and from the last time on), the
+   * surface of every face node the length of the face
+   * edge that starts at it (in 3D too), no time window; the value and
+   * dependances are not used */
+  MHC_BC_ON_FILE_PRESSURE = 12
 };
 
 /* energy deposits (TypesMahyco.h eEnergyDepot): constant, linear in
@@ -249,6 +263,12 @@ typedef struct mhc_case_params {
    * 1 y-fastest (the 2D Gmsh quadrangle grids of the datasets, whose
    * elements run column by column) */
   int mesh_cell_order;
+  /* the (time, pressure) table of OnFilePressure, which the reference reads
+   * from Pression.data at init (lireFichierCDL, MahycoAnnexe.cc:242-269):
+   * pressure_table_n pairs in the file's order */
+  int pressure_table_n;
+  double pressure_table_t[MHC_MAX_PTABLE];
+  double pressure_table_p[MHC_MAX_PTABLE];
 } mhc_case_params;
 
 #ifdef __cplusplus

@@ -110,6 +110,7 @@ _SIGS = {
                                    C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     # field upload and the per-method service surface (IEquationOfState, IRemap)
     "mhc_case_params_default": (None, [C.POINTER(CaseParams)]),
+    "mhc_case_params_size": (C.c_longlong, []),
     "mhc_batch_create_on_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "mhc_batch_poll_request": (C.c_int, [C.c_void_p]),
     "mhc_batch_set_sweep_layout": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),

@@ -10,17 +10,19 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import xml.etree.ElementTree as ET
 
 MAX_ENV = 4
 MAX_BC = 12
+MAX_PTABLE = 32
 
 EOS_PERFECT_GAS, EOS_STIFFENED_GAS, EOS_MIE_GRUNEISEN, EOS_FICTIF = 0, 1, 2, 3
 EOS_BY_NAME = {"PerfectGas": EOS_PERFECT_GAS, "StiffenedGas": EOS_STIFFENED_GAS,
                "MieGruneisen": EOS_MIE_GRUNEISEN, "Fictif": EOS_FICTIF}
 BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure": 4, "Density": 5,
               "Energy": 6, "SuperGaussianEnergy": 7, "Pressure": 8, "SuperGaussianPressure": 9,
-              "ContactHerzPressure": 10}
+              "ContactHerzPressure": 10, "OFV": 11, "OnFilePressure": 12}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
 CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES, CASE_RIDER, CASE_EXTERNAL = 1, 2, 3, 4, 5, 6, 7
 CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL, "CHOCBULLE": CASE_BUBBLES,
@@ -98,6 +100,8 @@ class CaseParams(C.Structure):
         ("sans_lagrange", C.c_int), ("rider_reverse", C.c_int), ("rider_parameter", C.c_double),
         ("rider_radius", C.c_double), ("rider_linear_density", C.c_int),
         ("schema_csts", C.c_int), ("mesh_cell_order", C.c_int),
+        ("pressure_table_n", C.c_int), ("pressure_table_t", C.c_double * MAX_PTABLE),
+        ("pressure_table_p", C.c_double * MAX_PTABLE),
     ]
 
     # -- convenience -------------------------------------------------------
@@ -172,6 +176,29 @@ def default_params() -> CaseParams:
     return p
 
 
+def read_pressure_table(path: str) -> list[tuple[float, float]]:
+    """(time, pressure) pairs of an OnFilePressure table: whitespace
+    separated reals read two by two until the first that does not parse, as
+    lireFichierCDL's stream loop does (MahycoAnnexe.cc:242-269)."""
+    pairs, vals = [], []
+    for tok in open(path).read().split():
+        try:
+            vals.append(float(tok))
+        except ValueError:
+            break
+    for i in range(0, len(vals) - 1, 2):
+        pairs.append((vals[i], vals[i + 1]))
+    return pairs
+
+
+def set_pressure_table(p: CaseParams, pairs) -> None:
+    if len(pairs) > MAX_PTABLE:
+        raise ValueError(f"at most {MAX_PTABLE} (time, pressure) pairs")
+    p.pressure_table_n = len(pairs)
+    for i, (t, v) in enumerate(pairs):
+        p.pressure_table_t[i], p.pressure_table_p[i] = t, v
+
+
 def add_bc(p: CaseParams, surface: str, kind: str, value: float = 0.0,
            tdebut: float = 0.0, tfin: float = 1000.0, dependance=(0.0, 0.0, 0.0, 0.0),
            cutoff=(1000.0, 1000.0), power: float = 4.0) -> None:
@@ -233,7 +260,6 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         # a Gmsh file of logically structured quadrangles, 2D: its node
         # coordinates and the <initialisation> values of its cell groups
         # are the case's initial fields (mahyco_b200.msh)
-        import os
         from .msh import read_msh
         msh = read_msh(os.path.join(os.path.dirname(os.path.abspath(path)), mfile.text.strip()))
         xyz = msh["coords"]
@@ -414,6 +440,12 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
                _txt(b, "Tdebut", 0.0), _txt(b, "Tfin", 1000.0),
                tuple(_txt(b, t, 0.0) for t in ("dependanceX", "dependanceY", "dependanceZ", "dependanceT")),
                (_txt(b, "cutoffX", 1000.0), _txt(b, "cutoffY", 1000.0)), _txt(b, "power", 4.0))
+        if kind == "OnFilePressure" and p.pressure_table_n == 0:
+            # the reference reads Pression.data from the run directory
+            # whatever the fichier option says (MahycoModule.cc:77-82)
+            fn = os.path.join(os.path.dirname(os.path.abspath(path)), "Pression.data")
+            if os.path.exists(fn):
+                set_pressure_table(p, read_pressure_table(fn))
     th = root.find("time-history/bilan")
     if th is not None:
         p.time_history_period = _txt(th, "periode", 10, int)

@@ -23,7 +23,7 @@ from .case import (ARITHMETIC_G, CASE_BUBBLES, CASE_EXTERNAL, CASE_ONECELL, CASE
                    CASE_TWO_STATE,
                    DEPOT_CONSTANT, DEPOT_SUPER_GAUSSIAN, EOS_FICTIF, EOS_MIE_GRUNEISEN, EULER_X, EULER_Y, EULER_Z,
                    EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
-                   ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults,
+                   ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults, set_pressure_table,
                    symmetry_bcs)
 
 
@@ -504,6 +504,18 @@ PARITY_CASES = {
     # (SuperGaussianPressure, exp and pow at the node)
     "lag3d_contact_herz_pressure": (lambda: _spot(_herz=True), 120),
     "lag2d_super_gaussian_pressure": (lambda: _spot(_herz=False), 120),
+    # OnFileVelocity (a unit velocity towards the origin from the node's
+    # position) on the outer sides: the implosion with anti-hourglass, a 3D
+    # Lagrangian tube, a Full Euler tube (positions back on the grid)
+    "lag2d_external_implosion_ofv": (lambda: _ofv(_external(deltat_init=1e-4), ("XMAX", "YMAX")), 150),
+    "lag3d_bisod_ofv": (lambda: _ofv(sod(dim=3, n=(30, 4, 4), L=(1.0, 0.1, 0.1), bi=True, remap=False,
+                                         deltat_max=1e-3, deltat_init=1e-4), ("XMAX",)), 100),
+    "adi2d_bisod_ofv": (lambda: _ofv(sod(dim=2, n=(40, 6), L=(1.0, 0.15), bi=True, deltat_init=1e-4), ("XMAX",)), 60),
+    # OnFilePressure: an aluminium plate pushed on its x = 0 side by a
+    # tabulated pressure (CAS_lag_ChocPlaque1D_3phases' ramp and plateau; in
+    # 3D a table that also ends inside the run)
+    "lag2d_plate_onfile_pressure": (lambda: _onfile(2), 150),
+    "lag3d_plate_onfile_pressure": (lambda: _onfile(3), 150),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
@@ -531,6 +543,37 @@ def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> Cas
     p.mesh_cell_order = 1 if colmajor else 0
     p.deltat_init, p.deltat_max = deltat_init, 1e-3
     symmetry_bcs(p, ("XMIN", "YMIN"))
+    return p
+
+
+def _ofv(p: CaseParams, surfaces) -> CaseParams:
+    for s in surfaces:
+        add_bc(p, s, "OFV", 1.0)
+    return p
+
+
+def _onfile(dim: int) -> CaseParams:
+    """An aluminium plate (as ``compression``) held at x = L and on its
+    lateral sides, loaded on x = 0 by OnFilePressure: in 2D the table of
+    CAS_lag_ChocPlaque1D_3phases (a 1e-11 s ramp to 1e10 Pa, held), in 3D a
+    ramp, a plateau and a release to 0 inside 1e-10 s.  In 3D the reference
+    still weighs the pressure by a face edge's length, not the face's area,
+    so the table's pressures are scaled down by about that length."""
+    if dim == 2:
+        p = compression(dim=2, n=(60, 2), L=(15e-6, 0.5e-6))
+        table = [(0.0, 0.0), (1.0e-11, 10.0e9), (9.0e-9, 10.0e9), (9.01e-9, 0.0)]
+    else:
+        p = compression(dim=3, n=(16, 3, 3), L=(4e-6, 1e-6, 1e-6), coef_antiderive=0.01)
+        table = [(0.0, 0.0), (2e-11, 2e3), (6e-11, 2e3), (8e-11, 0.0)]
+    p.nb_bc = 0
+    add_bc(p, "XMIN", "OnFilePressure", -1.0)
+    add_bc(p, "XMAX", "Vx", 0.0)
+    add_bc(p, "YMIN", "Vy", 0.0)
+    add_bc(p, "YMAX", "Vy", 0.0)
+    if dim == 3:
+        add_bc(p, "ZMIN", "Vz", 0.0)
+        add_bc(p, "ZMAX", "Vz", 0.0)
+    set_pressure_table(p, table)
     return p
 
 

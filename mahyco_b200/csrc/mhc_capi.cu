@@ -556,15 +556,18 @@ int validate(const mhc_case_params* p) {
   bool surfaces = false, cellvars = false;
   for (int b = 0; b < p->nb_bc; ++b) {
     const int kind = p->bc[b].kind;
-    if (kind < MHC_BC_VX || kind > MHC_BC_CONTACT_HERZ_PRESSURE)
+    if (kind < MHC_BC_VX || kind > MHC_BC_ON_FILE_PRESSURE)
       return set_err(MHC_ERR_UNSUPPORTED, "boundary condition kind");
     const bool surface = kind == MHC_BC_GEOMETRIC_PRESSURE || kind == MHC_BC_LINEAR_PRESSURE ||
-                         kind == MHC_BC_SUPER_GAUSSIAN_PRESSURE || kind == MHC_BC_CONTACT_HERZ_PRESSURE;
+                         kind == MHC_BC_SUPER_GAUSSIAN_PRESSURE || kind == MHC_BC_CONTACT_HERZ_PRESSURE ||
+                         kind == MHC_BC_ON_FILE_PRESSURE;
     if (surface && p->with_projection)
       return set_err(MHC_ERR_UNSUPPORTED, "pressure boundary conditions need a Lagrangian loop");
     surfaces = surfaces || surface;
     cellvars = cellvars || (kind >= MHC_BC_DENSITY && kind <= MHC_BC_PRESSURE);
   }
+  if (p->pressure_table_n < 0 || p->pressure_table_n > MHC_MAX_PTABLE)
+    return set_err(MHC_ERR_ARG, "pressure_table_n: 0..MHC_MAX_PTABLE");
   // the reference interleaves both kinds condition by condition on shared node masses
   if (surfaces && cellvars)
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions together with pressure surfaces");

@@ -456,6 +456,28 @@ __device__ __forceinline__ bool node_on_surface(const Mesh& M, int i, int j, int
   }
 }
 
+// applyBoundaryCondition's velocity kinds (MahycoModule.cc:756-807) at one
+// node, condition by condition in the dataset's order; X is the node's
+// position at the start of the cycle (OnFileVelocity: -x / |X|, -y / |X|)
+__device__ __forceinline__ void velocity_bcs(const Mesh& M, const mhc_case_params& P, int i, int j, int k, double t,
+                                             double dt, const R3& X, double& vx, double& vy, double& vz) {
+  const double eps = 1.e-8;
+  for (int b = 0; b < P.nb_bc; ++b) {
+    const mhc_bc& bc = P.bc[b];
+    if ((t - dt * (1 - eps)) < bc.tdebut) continue;
+    if ((t - dt * (1 - eps)) > bc.tfin) continue;
+    if (!node_on_surface(M, i, j, k, bc.surface)) continue;
+    if (bc.kind == MHC_BC_VX) vx = bc.value;
+    else if (bc.kind == MHC_BC_VY) vy = bc.value;
+    else if (bc.kind == MHC_BC_VZ) vz = bc.value;
+    else if (bc.kind == MHC_BC_ON_FILE_VELOCITY) {
+      const double r = sqrt(X.x * X.x + X.y * X.y + X.z * X.z);
+      vx = -X.x / r;
+      vy = -X.y / r;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // init: MahycoModule::hydroStartInit + computeCellMass (MahycoModule.cc:21-237)
 // ---------------------------------------------------------------------------
@@ -792,6 +814,25 @@ __device__ __forceinline__ void face_node_rt(int dim, int d, int q, int& a, int&
   else { a = s1; b = s2; }
 }
 
+// OnFilePressure's value (MahycoModule.cc:987-1008): the first table time
+// above t ends the interval, the value is interpolated linearly with the
+// weight clamped to [0, 1] (Arcane's math::min / math::max); 0 before the
+// first time and from the last time on
+__device__ __forceinline__ double onfile_pressure(const mhc_case_params& P, double t) {
+  int it = -1;
+  for (int i = 0; i < P.pressure_table_n; ++i) {
+    if (t < P.pressure_table_t[i]) {
+      it = i;
+      break;
+    }
+  }
+  if (it <= 0) return 0.;
+  double alpha = (t - P.pressure_table_t[it - 1]) / (P.pressure_table_t[it] - P.pressure_table_t[it - 1]);
+  alpha = alpha < 1. ? alpha : 1.;
+  alpha = alpha < 0. ? 0. : alpha;
+  return P.pressure_table_p[it - 1] + alpha * (P.pressure_table_p[it] - P.pressure_table_p[it - 1]);
+}
+
 // Compiled into the Lagrangian instances of the node pass only (the only
 // runs allowed pressure surfaces): its local arrays and loops stay off the
 // register budget of the node pass of the remapped runs.
@@ -804,8 +845,10 @@ __device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params&
   for (int b = 0; b < P.nb_bc; ++b) {
     const mhc_bc& bc = P.bc[b];
     if (bc.kind != MHC_BC_GEOMETRIC_PRESSURE && bc.kind != MHC_BC_LINEAR_PRESSURE &&
-        bc.kind != MHC_BC_SUPER_GAUSSIAN_PRESSURE && bc.kind != MHC_BC_CONTACT_HERZ_PRESSURE)
+        bc.kind != MHC_BC_SUPER_GAUSSIAN_PRESSURE && bc.kind != MHC_BC_CONTACT_HERZ_PRESSURE &&
+        bc.kind != MHC_BC_ON_FILE_PRESSURE)
       continue;
+    const bool onfile = bc.kind == MHC_BC_ON_FILE_PRESSURE;
     const int s = bc.surface;
     const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
     if (d >= DIM) continue;
@@ -838,7 +881,7 @@ __device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params&
         }
         auto X = [&](long long m) { return R3{F.Xp[0][m], F.Xp[1][m], F.Xp[2][m]}; };
         double surface;
-        if (DIM == 2) {
+        if (DIM == 2 || onfile) {
           const long long n2 = me < NQ - 1 ? fn[me + 1] : fn[0];
           surface = norm(X(n2) - X(n));
         } else {
@@ -878,8 +921,12 @@ __device__ __forceinline__ R3 pressure_bcs(const Mesh& M, const mhc_case_params&
           if (x2 / a2 + y2 / b2 < 1.) value *= sqrt(1 - x2 / a2 - y2 / b2);
           else value = 0.;
         }
-        if (t < bc.tdebut) value = 0.;
-        if (t >= bc.tfin) value = 0.;
+        if (onfile) {
+          value = onfile_pressure(P, t);
+        } else {
+          if (t < bc.tdebut) value = 0.;
+          if (t >= bc.tfin) value = 0.;
+        }
         const R3 dv = (dth * w * nrm * value * surface) / F.mn[n];
         vx = vx - dv.x; vy = vy - dv.y; vz = vz - dv.z;
       }
@@ -974,25 +1021,16 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
     F.Ud[0][n] = vx; F.Ud[0][NN + n] = vy; F.Ud[0][2 * NN + n] = vz;
     return;
   }
-  const double eps = 1.e-8;
-  for (int b = 0; b < P.nb_bc; ++b) {
-    const mhc_bc& bc = P.bc[b];
-    if ((t - dt * (1 - eps)) < bc.tdebut) continue;
-    if ((t - dt * (1 - eps)) > bc.tfin) continue;
-    if (!node_on_surface(M, i, j, k, bc.surface)) continue;
-    if (bc.kind == MHC_BC_VX) vx = bc.value;
-    else if (bc.kind == MHC_BC_VY) vy = bc.value;
-    else if (bc.kind == MHC_BC_VZ) vz = bc.value;
-  }
-  if constexpr (LAG) {
-    const R3 v = pressure_bcs<DIM>(M, P, F, i, j, k, n, dth, t, R3{vx, vy, vz});
-    vx = v.x; vy = v.y; vz = v.z;
-  }
   // positions at the start of the cycle: the initial grid after a Full
   // Euler remap (RemapADIService.cc:62-64); otherwise the last ones (a
   // per-axis remap has put its axis back on the grid, kb_euler_axis_reset)
   const R3 x = (!LAG && P.is_euler_scheme == MHC_EULER_FULL) ? node_x0(M, i, j, k)
                                                              : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+  velocity_bcs(M, P, i, j, k, t, dt, x, vx, vy, vz);
+  if constexpr (LAG) {
+    const R3 v = pressure_bcs<DIM>(M, P, F, i, j, k, n, dth, t, R3{vx, vy, vz});
+    vx = v.x; vy = v.y; vz = v.z;
+  }
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;
   F.Xn[0][n] = x.x + dt * vx; F.Xn[1][n] = x.y + dt * vy; F.Xn[2][n] = x.z + dt * vz;
 }
@@ -1060,16 +1098,7 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
       }
   double vx = ux[n] - h.x, vy = uy[n] - h.y, vz = uz[n] - h.z;
   const double dt = F.s->dt, t = F.s->t;
-  const double eps = 1.e-8;
-  for (int b = 0; b < P.nb_bc; ++b) {
-    const mhc_bc& bc = P.bc[b];
-    if ((t - dt * (1 - eps)) < bc.tdebut) continue;
-    if ((t - dt * (1 - eps)) > bc.tfin) continue;
-    if (!node_on_surface(M, i, j, k, bc.surface)) continue;
-    if (bc.kind == MHC_BC_VX) vx = bc.value;
-    else if (bc.kind == MHC_BC_VY) vy = bc.value;
-    else if (bc.kind == MHC_BC_VZ) vz = bc.value;
-  }
+  velocity_bcs(M, P, i, j, k, t, dt, R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]}, vx, vy, vz);
   {
     const R3 v = pressure_bcs<DIM>(M, P, F, i, j, k, n, 0.5 * (F.s->old_dt + dt), t, R3{vx, vy, vz});
     vx = v.x; vy = v.y; vz = v.z;
@@ -1530,17 +1559,8 @@ __device__ __forceinline__ void body_advect_nodes(const Mesh& M, const mhc_case_
   double vx = ux * (1. - option_real) + option_real * ux * cs;
   double vy = uy * (1. - option_real) + option_real * uy * cs;
   double vz = uz * (1. - option_real) + option_real * uz * cs;
-  const double eps = 1.e-8;
-  for (int b = 0; b < P.nb_bc; ++b) {
-    const mhc_bc& bc = P.bc[b];
-    if ((t - dt * (1 - eps)) < bc.tdebut) continue;
-    if ((t - dt * (1 - eps)) > bc.tfin) continue;
-    if (!node_on_surface(M, i, j, k, bc.surface)) continue;
-    if (bc.kind == MHC_BC_VX) vx = bc.value;
-    else if (bc.kind == MHC_BC_VY) vy = bc.value;
-    else if (bc.kind == MHC_BC_VZ) vz = bc.value;
-  }
   const R3 x = P.is_euler_scheme == MHC_EULER_FULL ? node_x0(M, i, j, k) : R3{F.Xp[0][n], F.Xp[1][n], F.Xp[2][n]};
+  velocity_bcs(M, P, i, j, k, t, dt, x, vx, vy, vz);
   int nc = ((i > 0) + (i < M.ncx)) * ((j > 0) + (j < M.ncy));
   if (DIM == 3) nc *= (k > 0) + (k < M.ncz);
   F.vx[n] = vx; F.vy[n] = vy; F.vz[n] = vz;

@@ -129,6 +129,8 @@ int check_remap_args(mhc_case* h, int dimension, int with_dual, int nvars, int n
 // ---------------------------------------------------------------------------
 // option defaults
 // ---------------------------------------------------------------------------
+long long mhc_case_params_size(void) { return (long long)sizeof(mhc_case_params); }
+
 void mhc_case_params_default(mhc_case_params* p) {
   if (!p) return;
   memset(p, 0, sizeof(*p));

@@ -1103,6 +1103,13 @@ static void apply_boundary_condition(Case& C) {
       if (bc.kind == MHC_BC_VX) C.vel[n].x = bc.value;
       else if (bc.kind == MHC_BC_VY) C.vel[n].y = bc.value;
       else if (bc.kind == MHC_BC_VZ) C.vel[n].z = bc.value;
+      else if (bc.kind == MHC_BC_ON_FILE_VELOCITY) {
+        /* OnFileVelocity (MahycoModule.cc:796-798): Real3::normL2 of the
+         * position before updatePosition */
+        const R3& X = C.coord[n];
+        C.vel[n].x = -X.x / std::sqrt(X.x * X.x + X.y * X.y + X.z * X.z);
+        C.vel[n].y = -X.y / std::sqrt(X.x * X.x + X.y * X.y + X.z * X.z);
+      }
     }
   }
   apply_pressure_bcs(C);
@@ -1116,6 +1123,29 @@ static void apply_boundary_condition(Case& C) {
  * with n the unit vector from the cell centre to the (initial) face centre,
  * S the length of the face edge from that node (2D) or the z-projected face
  * area (3D), p the BC value (plus its linear terms) inside [Tdebut, Tfin) */
+/* OnFilePressure (MahycoModule.cc:987-1008): the table read by
+ * lireFichierCDL (MahycoAnnexe.cc:242-269) interpolated at the current time:
+ * the interval ends at the first time above it, value 0 when that is the
+ * first entry or no entry is above it */
+static double onfile_pressure(const Case& C) {
+  const mhc_case_params& P = C.P;
+  double value = 0.;
+  int it = -1;
+  for (int i = 0; i < P.pressure_table_n; ++i) {
+    if (C.t < P.pressure_table_t[i]) {
+      it = i;
+      break;
+    }
+  }
+  if (it > 0) {
+    double alpha = (C.t - P.pressure_table_t[it - 1]) / (P.pressure_table_t[it] - P.pressure_table_t[it - 1]);
+    alpha = alpha < 1. ? alpha : 1.;  /* math::min(alpha, 1.) */
+    alpha = alpha < 0. ? 0. : alpha;  /* math::max(alpha, 0.) */
+    value = P.pressure_table_p[it - 1] + alpha * (P.pressure_table_p[it] - P.pressure_table_p[it - 1]);
+  }
+  return value;
+}
+
 static void apply_pressure_bcs(Case& C) {
   const double w = C.dim == 2 ? .5 : .25;
   const double w8 = C.dim == 2 ? .25 : .125;
@@ -1123,8 +1153,9 @@ static void apply_pressure_bcs(Case& C) {
   for (int b = 0; b < C.P.nb_bc; ++b) {
     const mhc_bc& bc = C.P.bc[b];
     const bool cellvar = bc.kind >= MHC_BC_DENSITY && bc.kind <= MHC_BC_PRESSURE;
+    const bool onfile = bc.kind == MHC_BC_ON_FILE_PRESSURE;
     const bool surface = bc.kind == MHC_BC_GEOMETRIC_PRESSURE || bc.kind == MHC_BC_LINEAR_PRESSURE ||
-                         bc.kind == MHC_BC_SUPER_GAUSSIAN_PRESSURE || bc.kind == MHC_BC_CONTACT_HERZ_PRESSURE;
+                         bc.kind == MHC_BC_SUPER_GAUSSIAN_PRESSURE || bc.kind == MHC_BC_CONTACT_HERZ_PRESSURE || onfile;
     if (!surface && !cellvar) continue;
     const int s = bc.surface;
     const int d = (s == MHC_XMIN || s == MHC_XMAX) ? 0 : ((s == MHC_YMIN || s == MHC_YMAX) ? 1 : 2);
@@ -1172,7 +1203,7 @@ static void apply_pressure_bcs(Case& C) {
         const long node = n[q];
         double value = bc.value;
         double surface;
-        if (C.dim == 2) {
+        if (C.dim == 2 || onfile) {
           const long node2 = q < nb - 1 ? n[q + 1] : n[0];
           surface = norm(C.coord[node2] - C.coord[node]);
         } else {
@@ -1200,8 +1231,12 @@ static void apply_pressure_bcs(Case& C) {
           if (x2 / a2 + y2 / b2 < 1.) value *= std::sqrt(1 - x2 / a2 - y2 / b2);
           else value = 0.;
         }
-        if (C.t < bc.tdebut) value = 0.;
-        if (C.t >= bc.tfin) value = 0.;
+        if (onfile) {
+          value = onfile_pressure(C);
+        } else {
+          if (C.t < bc.tdebut) value = 0.;
+          if (C.t >= bc.tfin) value = 0.;
+        }
         C.vel[node] -= (dt * w * nrm * value * surface) / C.node_mass[node];
       }
     }

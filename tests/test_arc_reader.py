@@ -175,6 +175,28 @@ def test_pressure_surfaces_and_onecell(tmp_path):
     assert (3, 0, 30e9, 1e-7, 1000.0, [0.0, 0.0, 0.0, 0.0]) in kinds
 
 
+def test_on_file_boundary_conditions(tmp_path):
+    """OFV (OnFileVelocity) and OnFilePressure (Mahyco.axl:498, 505); the
+    pressure table comes from Pression.data beside the dataset, whatever
+    the fichier option names, read two reals at a time (MahycoAnnexe.cc:
+    242-269); without that file the table stays empty."""
+    bcs = ("<boundary-condition><surface>XMAX</surface><type>OFV</type><value>1.</value></boundary-condition>"
+           "<boundary-condition><surface>XMIN</surface><type>OnFilePressure</type><value>-1.</value>"
+           "<fichier>other.data</fichier></boundary-condition>")
+    text = open(ARC).read().replace("<final-time>", bcs + "<final-time>", 1)
+    f = tmp_path / "o.arc"
+    f.write_text(text)
+    p, _ = read_arc(str(f))
+    got = [(p.bc[i].kind, p.bc[i].surface) for i in range(p.nb_bc) if p.bc[i].kind >= 11]
+    assert got == [(11, 3), (12, 0)]
+    assert p.pressure_table_n == 0
+    (tmp_path / "Pression.data").write_text("0. 0.\n1.00e-11 10.0e9\n9.00e-9  10.0e9\n9.01e-9  0.\n")
+    p, _ = read_arc(str(f))
+    assert p.pressure_table_n == 4
+    assert list(p.pressure_table_t[:4]) == [0.0, 1e-11, 9e-9, 9.01e-9]
+    assert list(p.pressure_table_p[:4]) == [0.0, 1e10, 1e10, 0.0]
+
+
 def test_cell_variable_boundary_conditions(tmp_path):
     """Density / Energy / SuperGaussianEnergy / Pressure conditions
     (Mahyco.axl:490-535) with their cutoffs (default 1000)."""

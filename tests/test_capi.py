@@ -100,3 +100,10 @@ def test_c_defaults_match_the_python_defaults():
     lib.mhc_case_params_default(ctypes.byref(c))
     py = mb.default_params()
     assert bytes(c) == bytes(py)
+
+
+def test_params_size_matches_the_binding():
+    """The ctypes mirror of mhc_case_params has the library's layout size
+    (host only, no GPU)."""
+    lib = mb.load()
+    assert lib.mhc_case_params_size() == ctypes.sizeof(mb.CaseParams)

@@ -67,3 +67,7 @@ def test_gpu_matches_reference_goldens(path):
             den = np.where(ref[:, 1] == 0.0, 1.0, np.abs(ref[:, 1]))
             rel = np.abs(ours[:, 1 + 5 * e + q] - ref[:, 1]) / den
             assert rel.max() <= tol_var.get(var, tol), (key, rel.max(), int(rel.argmax()))
+            # the GPU rounds like the correctly rounded oracle: the lines that
+            # oracle reproduces bit for bit, it reproduces too
+            exact = g["extra"].get("exact_lines_cr_pow", 0)
+            assert np.array_equal(ours[:exact, 1 + 5 * e + q], ref[:exact, 1]), key

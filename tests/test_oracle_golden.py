@@ -50,7 +50,7 @@ def test_oracle_matches_reference_goldens(path, cr_pow):
     ttol = 1e-13 if multi else 1e-14  # the time: a sum of deltat, per-rank orders move it by ulps
     ttol = g["extra"].get("time_tol", ttol)
     tol_var = g["extra"].get("tol_var", {})
-    exact = 0 if cr_pow else g["extra"].get("exact_lines", 0)
+    exact = g["extra"].get("exact_lines_cr_pow" if cr_pow else "exact_lines", 0)
     p, th = run_oracle(g, cr_pow)
     for e, env in enumerate(g["env_names"]):
         for q, var in enumerate(VARS):
