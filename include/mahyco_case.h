@@ -95,19 +95,25 @@ enum mhc_case_model {
                              environment 1 in environment 0 (mixed boundary cells) */
   MHC_CASE_RIDER = 6,     /* casTest/RIDER/RIDERService.cc: a disc advected by a prescribed
                              velocity field (cas_test 23-38) */
-  MHC_CASE_EXTERNAL = 7   /* casTest/EXTERNAL/EXTERNALService.cc (the default cas-model): the
+  MHC_CASE_EXTERNAL = 7,  /* casTest/EXTERNAL/EXTERNALService.cc (the default cas-model): the
                              dataset's <initialisation> block sets Materiau, Density and
                              Pressure per cell (mhc_case_set_initial_field; by default
                              environment 0 and its initial state everywhere), then
                              initUtilisateur sets the node velocities of every environment
                              with initialisation_utilisateur: its vitesse_initiale, or
                              -x/|x| when that is zero */
+  MHC_CASE_TRIPLE_POINT = 8 /* casTest/POINTTRIPLE/POINTTRIPLEService.cc: three regions, x <= 0.01,
+                               then y <= 0.015 or above, each holding environment 0, 1, 2
+                               (BiTriplePoint, cas_test 12) or all environment 0 (MonoTriplePoint,
+                               cas_test 2) with that environment's initial state; every node at
+                               environment 0's initial velocity */
 };
 
-/* cas-test ids used by SOD and SEDOV (TypesMahyco.h:44-94) */
+/* cas-test ids used by SOD, SEDOV, POINTTRIPLE and RIDER (TypesMahyco.h:44-94) */
 enum mhc_cas_test {
-  MHC_TEST_SEDOV = 1, MHC_TEST_SOD_X = 3, MHC_TEST_SOD_Y = 4, MHC_TEST_SOD_Z = 5,
-  MHC_TEST_BISEDOV = 11, MHC_TEST_BISOD_X = 13, MHC_TEST_BISOD_Y = 14, MHC_TEST_BISOD_Z = 15,
+  MHC_TEST_SEDOV = 1, MHC_TEST_MONO_TRIPLE_POINT = 2, MHC_TEST_SOD_X = 3, MHC_TEST_SOD_Y = 4, MHC_TEST_SOD_Z = 5,
+  MHC_TEST_BISEDOV = 11, MHC_TEST_BI_TRIPLE_POINT = 12, MHC_TEST_BISOD_X = 13, MHC_TEST_BISOD_Y = 14,
+  MHC_TEST_BISOD_Z = 15,
   /* RIDER: one environment (MonoRider*, 23-30) or a disc of environment 1 in
    * environment 0 (Rider*, 31-38); velocity a translation along x, y or the
    * diagonal, a rotation about (0.5, 0.5), a vortex or a deformation field */

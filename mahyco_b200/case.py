@@ -25,8 +25,9 @@ BC_BY_NAME = {"Vx": 0, "Vy": 1, "Vz": 2, "GeometricPressure": 3, "LinearPressure
               "ContactHerzPressure": 10, "OFV": 11, "OnFilePressure": 12}
 SURFACES = {"XMIN": 0, "YMIN": 1, "ZMIN": 2, "XMAX": 3, "YMAX": 4, "ZMAX": 5}
 CASE_SOD, CASE_SEDOV, CASE_TWO_STATE, CASE_ONECELL, CASE_BUBBLES, CASE_RIDER, CASE_EXTERNAL = 1, 2, 3, 4, 5, 6, 7
+CASE_TRIPLE_POINT = 8
 CASE_BY_NAME = {"SOD": CASE_SOD, "SEDOV": CASE_SEDOV, "ONECELL": CASE_ONECELL, "CHOCBULLE": CASE_BUBBLES,
-                "RIDER": CASE_RIDER, "EXTERNAL": CASE_EXTERNAL}
+                "RIDER": CASE_RIDER, "EXTERNAL": CASE_EXTERNAL, "POINTTRIPLE": CASE_TRIPLE_POINT}
 # RIDER cas-test ids (TypesMahyco.h:69-84): MonoRider* 23-30, Rider* 31-38
 RIDER_TESTS = {n: 23 + i for i, n in enumerate(
     ("MonoRiderTx", "MonoRiderTy", "MonoRiderT45", "MonoRiderRotation", "MonoRiderVortex", "MonoRiderDeformation",

@@ -20,7 +20,7 @@ import math
 import random
 
 from .case import (ARITHMETIC_G, CASE_BUBBLES, CASE_EXTERNAL, CASE_ONECELL, CASE_RIDER, CASE_SEDOV, CASE_SOD,
-                   CASE_TWO_STATE,
+                   CASE_TRIPLE_POINT, CASE_TWO_STATE,
                    DEPOT_CONSTANT, DEPOT_SUPER_GAUSSIAN, EOS_FICTIF, EOS_MIE_GRUNEISEN, EULER_X, EULER_Y, EULER_Z,
                    EOS_PERFECT_GAS, EOS_STIFFENED_GAS, MINMOD, MINMOD_G, SUPERBEE, SUPERBEE_G,
                    ULTRABEE_G, VANLEER, VANLEER_G, CaseParams, add_bc, default_params, env_defaults, set_pressure_table,
@@ -55,6 +55,28 @@ def sod(dim=3, n=(100, 5, 5), L=(1.0, 0.1, 0.1), bi=True, axis=0, remap=True,
     p.projection_limiteur_id, p.ordre_projection = limiter, order
     p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = cfl, deltat_init, 1e-8, deltat_max
     p.final_time = final_time
+    symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
+    return p
+
+
+def triple_point(dim=2, n=(35, 15, 3), mono=False, limiter=VANLEER, deltat_init=1e-5) -> CaseParams:
+    """CAS_bitriplepoint_minmod / CAS_MonoPointtriple_* at any resolution of
+    their 0.07 x 0.03 box: (rho, p) = (1, 1) at x <= 0.01, (1, 0.1) below
+    y = 0.015 and (0.125, 0.1) above, gamma 1.4, in three environments
+    (POINTTRIPLE, cas-test 12) or all in environment 0 (cas-test 2); walls
+    all around."""
+    p = default_params()
+    _mesh(p, dim, n, (0.07, 0.03, 0.03 * n[2] / n[1] if dim == 3 else 0.0))
+    p.nb_env = 3
+    for e, (rho, pr) in enumerate(((1.0, 1.0), (1.0, 0.1), (0.125, 0.1))):
+        env_defaults(p.env[e], EOS_PERFECT_GAS)
+        p.env[e].specific_heat = 2.4
+        p.env[e].densite_initiale, p.env[e].pression_initiale = rho, pr
+    p.cas_model = CASE_TRIPLE_POINT
+    p.cas_test = 2 if mono else 12
+    p.with_projection = 1
+    p.projection_limiteur_id = limiter
+    p.cfl, p.deltat_init, p.deltat_min, p.deltat_max = 0.3, deltat_init, 1e-10, 1e-5
     symmetry_bcs(p, ("XMIN", "XMAX", "YMIN", "YMAX") + (("ZMIN", "ZMAX") if dim == 3 else ()))
     return p
 
@@ -516,6 +538,14 @@ PARITY_CASES = {
     # 3D a table that also ends inside the run)
     "lag2d_plate_onfile_pressure": (lambda: _onfile(2), 150),
     "lag3d_plate_onfile_pressure": (lambda: _onfile(3), 150),
+    # POINTTRIPLE: three environments meeting at (0.01, 0.015), the
+    # pente-borne variant of its datasets, one environment with three states,
+    # a 3D slab
+    "adi2d_triple_point": (lambda: triple_point(), 120),
+    "adi2d_triple_point_pb_superbeeG": (lambda: _pb(triple_point(limiter=SUPERBEE_G), 1, mixte=1, pure_id=SUPERBEE_G),
+                                        120),
+    "adi2d_triple_point_mono": (lambda: triple_point(mono=True, limiter=SUPERBEE), 120),
+    "adi3d_triple_point": (lambda: triple_point(dim=3, n=(28, 12, 3)), 60),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit

@@ -575,7 +575,11 @@ int validate(const mhc_case_params* p) {
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with a per-axis Euler remap");
   if (cellvars && p->with_newton)
     return set_err(MHC_ERR_UNSUPPORTED, "cell-variable boundary conditions with the Newton energy update");
-  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_EXTERNAL) return set_err(MHC_ERR_ARG, "cas-model");
+  if (p->cas_model < MHC_CASE_SOD || p->cas_model > MHC_CASE_TRIPLE_POINT) return set_err(MHC_ERR_ARG, "cas-model");
+  // the three regions read the initial states of three environments
+  if (p->cas_model == MHC_CASE_TRIPLE_POINT &&
+      (p->nb_env != 3 || (p->cas_test != MHC_TEST_MONO_TRIPLE_POINT && p->cas_test != MHC_TEST_BI_TRIPLE_POINT)))
+    return set_err(MHC_ERR_ARG, "POINTTRIPLE needs three environments and cas_test 2 or 12");
   if (p->mesh_cell_order != 0 && !(p->mesh_cell_order == 1 && p->dim == 2))
     return set_err(MHC_ERR_ARG, "mesh_cell_order: 0, or 1 in 2D");
   if (p->cas_model == MHC_CASE_RIDER &&

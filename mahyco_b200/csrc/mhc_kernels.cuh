@@ -456,6 +456,13 @@ __device__ __forceinline__ bool node_on_surface(const Mesh& M, int i, int j, int
   }
 }
 
+// POINTTRIPLE's regions (POINTTRIPLEService.cc:26-36, 49-58): 0 for a cell
+// centre at x <= 0.01, else 1 at y <= 0.015, else 2
+__device__ __forceinline__ int triple_point_region(const R3& cc) {
+  if (cc.x <= 0.01) return 0;
+  return cc.y <= 0.015 ? 1 : 2;
+}
+
 // applyBoundaryCondition's velocity kinds (MahycoModule.cc:756-807) at one
 // node, condition by condition in the dataset's order; X is the node's
 // position at the start of the cycle (OnFileVelocity: -x / |X|, -y / |X|)
@@ -564,6 +571,9 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
     if (NE > 1) mat = (comp(cc, P.interface_dir) < P.interface_pos) ? 0. : 1.;
   } else if (P.cas_model == MHC_CASE_ONECELL) {
     mat = 0.;  // ONECELLService::initMat
+  } else if (P.cas_model == MHC_CASE_TRIPLE_POINT) {
+    // POINTTRIPLEService::initMat (lines 42-60); initMatMono for MonoTriplePoint
+    if (P.cas_test != MHC_TEST_MONO_TRIPLE_POINT && NE > 1) mat = (double)triple_point_region(cc);
   } else if (P.cas_model == MHC_CASE_EXTERNAL) {
     mat = F.init ? F.init[c] : 0.;  // the dataset's <initialisation> Materiau
   } else if (P.cas_model == MHC_CASE_SEDOV && P.cas_test != MHC_TEST_SEDOV) {
@@ -625,6 +635,12 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
     }
   } else if (P.cas_model == MHC_CASE_TWO_STATE) {
     int st = (comp(cc, P.interface_dir) < P.interface_pos) ? 0 : 1;
+    rho = P.env[st].densite_initiale;
+    p = P.env[st].pression_initiale;
+  } else if (P.cas_model == MHC_CASE_TRIPLE_POINT) {
+    // POINTTRIPLEService::initVar / initVarMono (lines 14-41, 62-141): the
+    // region's environment state (every cell is pure)
+    const int st = triple_point_region(cc);
     rho = P.env[st].densite_initiale;
     p = P.env[st].pression_initiale;
   } else if (P.cas_model == MHC_CASE_BUBBLES) {
@@ -766,7 +782,8 @@ __device__ __forceinline__ void body_init_nodes(const Mesh& M, const mhc_case_pa
   R3 x = node_initial(M, F, i, j, k);
   F.Xp[0][n] = x.x; F.Xp[1][n] = x.y; F.Xp[2][n] = x.z;
   double vx = 0., vy = 0., vz = 0.;
-  if (P.cas_model == MHC_CASE_SOD || P.cas_model == MHC_CASE_TWO_STATE || P.cas_model == MHC_CASE_BUBBLES) {
+  if (P.cas_model == MHC_CASE_SOD || P.cas_model == MHC_CASE_TWO_STATE || P.cas_model == MHC_CASE_BUBBLES ||
+      P.cas_model == MHC_CASE_TRIPLE_POINT) {
     vx = P.env[0].vitesse_initiale[0]; vy = P.env[0].vitesse_initiale[1]; vz = P.env[0].vitesse_initiale[2];
   }
   if (P.cas_model == MHC_CASE_EXTERNAL) {

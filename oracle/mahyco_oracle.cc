@@ -585,6 +585,13 @@ static double bubble_material(const Case& C, long c, double& fbub) {
   return mat;
 }
 
+/* the regions of POINTTRIPLEService (POINTTRIPLEService.cc:26-36, 49-58) */
+static int triple_point_region(const R3& cc) {
+  if (cc.x <= 0.01) return 0;
+  if (cc.y <= 0.015) return 1;
+  return 2;
+}
+
 /* SODService::initMat / SEDOVService::initMat and the environment sort of
  * MahycoModule::hydroStartInitEnvAndMat (MahycoAnnexe.cc:86-139) */
 static void init_materials(Case& C) {
@@ -598,6 +605,10 @@ static void init_materials(Case& C) {
       }
     } else if (P.cas_model == MHC_CASE_ONECELL) {
       m = 0.;  /* ONECELLService::initMat */
+    } else if (P.cas_model == MHC_CASE_TRIPLE_POINT) {
+      /* POINTTRIPLEService::initMat (POINTTRIPLEService.cc:42-60); initMatMono
+       * puts every cell in environment 0 */
+      if (P.cas_test != MHC_TEST_MONO_TRIPLE_POINT) m = triple_point_region(C.cell_coord[c]);
     } else if (P.cas_model == MHC_CASE_TWO_STATE) {
       if (C.nenv > 1) {
         double r = comp(C.cell_coord[c], P.interface_dir);
@@ -662,6 +673,17 @@ static void init_variables(Case& C) {
           for (int e = 0; e < C.nenv; ++e)
             if (C.has(c, e)) { C.EV(C.density, e, c) = P.env[s].densite_initiale; C.EV(C.pressure, e, c) = P.env[s].pression_initiale; }
       }
+    }
+    for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
+  } else if (P.cas_model == MHC_CASE_TRIPLE_POINT) {
+    /* POINTTRIPLEService::initVar / initVarMono (POINTTRIPLEService.cc:14-41,
+     * 62-141): the region's initial state, every node at environment 0's
+     * velocity; the cells are pure, so the per-environment branch of initVar
+     * never runs */
+    for (long c = 0; c < C.ncell; ++c) {
+      const int s = triple_point_region(C.cell_coord[c]);
+      C.density.g[c] = P.env[s].densite_initiale;
+      C.pressure.g[c] = P.env[s].pression_initiale;
     }
     for (long n = 0; n < C.nnode; ++n) C.vel[n] = {P.env[0].vitesse_initiale[0], P.env[0].vitesse_initiale[1], P.env[0].vitesse_initiale[2]};
   } else if (P.cas_model == MHC_CASE_TWO_STATE) {

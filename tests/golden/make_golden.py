@@ -110,6 +110,20 @@ CASES = {
     # the reference's curves is reproduced bit for bit (glibc's pow moves
     # them by ulps from line 117 on)
     "CAS_2D_Lag_NOH": {"exact_lines_cr_pow": 602},
+    # POINTTRIPLE init, three environments, 4 MPI ranks; the means of the
+    # volumes, masses and energies stay within 7e-14 of the reference's, but
+    # an environment's mean pressure can hang on a cell where it is nearly
+    # absent, and one line of each run misses by 4e-11 (vanleer) or 6e-10
+    # (pente-borne simple pente); the errors do not grow after it
+    "CAS_bitriplepoint_minmod": {"mpi_ranks": 4, "tol_var": {"Pressure": 1e-10}},
+    "CAS_MonoPointtriple_pb_sp_mixte_superbeeG_superbeeG": {"mpi_ranks": 4, "tol_var": {"Pressure": 2e-9}},
+    # the same with the two-slope pente-borne fluxes is chaotic: two oracle
+    # runs whose powers differ by an ulp part by 1e-2 after 2400 iterations,
+    # so only the first 140 lines (1400 iterations) are kept, where the
+    # 4-rank reference is still within 2e-13 (masses), 1e-11 (densities,
+    # energies), 1e-8 (pressures)
+    "CAS_MonoPointtriple_pb_mixte_superbeeG_superbeeG": {"mpi_ranks": 4, "lines": 140, "tol": 1e-10,
+                                                          "tol_var": {"Pressure": 5e-8}},
 }
 # variables the Ensight writer of mahyco_b200.output produces
 ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy", "PseudoViscosity",
@@ -130,7 +144,7 @@ def main(ref_root, only=()):
                 if not os.path.exists(fn):
                     continue
                 rows = [[float(x) for x in line.split()] for line in open(fn) if line.strip()]
-                hist[f"{v}_{env}"] = rows
+                hist[f"{v}_{env}"] = rows[:extra["lines"]] if "lines" in extra else rows
         # digests of the reference's final Ensight files (6 significant
         # digits, round-off noise removed: tests/ensight_digest.py), compared
         # with the files mahyco_b200.output writes; a multi-rank reference
