@@ -122,7 +122,10 @@ enum mhc_cas_test {
   MHC_TEST_MONO_RIDER_VORTEX_REVERSE = 29, MHC_TEST_MONO_RIDER_DEFORMATION_REVERSE = 30,
   MHC_TEST_RIDER_TX = 31, MHC_TEST_RIDER_TY = 32, MHC_TEST_RIDER_T45 = 33, MHC_TEST_RIDER_ROTATION = 34,
   MHC_TEST_RIDER_VORTEX = 35, MHC_TEST_RIDER_DEFORMATION = 36, MHC_TEST_RIDER_VORTEX_REVERSE = 37,
-  MHC_TEST_RIDER_DEFORMATION_REVERSE = 38
+  MHC_TEST_RIDER_DEFORMATION_REVERSE = 38,
+  /* BiSodSph: the BiSod states inside and outside the sphere of radius 0.5
+   * about the origin (SODService.cc:56-62) */
+  MHC_TEST_BISOD_SPH = 39
 };
 
 /* longueur-caracteristique option values */

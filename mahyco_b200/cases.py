@@ -546,6 +546,11 @@ PARITY_CASES = {
                                         120),
     "adi2d_triple_point_mono": (lambda: triple_point(mono=True, limiter=SUPERBEE), 120),
     "adi3d_triple_point": (lambda: triple_point(dim=3, n=(28, 12, 3)), 60),
+    # BiSodSph (cas-test 39): the BiSod states inside and outside the sphere
+    # of radius 0.5 about the origin (CAS_BiSodSph at 16^3 and in 2D)
+    "adi3d_bisod_sph": (lambda: _sph(sod(dim=3, n=(16, 16, 16), L=(1.0, 1.0, 1.0), deltat_init=1e-3)), 40),
+    "adi2d_bisod_sph_superbee": (lambda: _sph(sod(dim=2, n=(40, 40), L=(1.0, 1.0), limiter=SUPERBEE,
+                                                  deltat_init=1e-3)), 60),
 }
 
 # cases whose exact bar is a bound instead of 0: the super-Gaussian deposit
@@ -573,6 +578,11 @@ def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> Cas
     p.mesh_cell_order = 1 if colmajor else 0
     p.deltat_init, p.deltat_max = deltat_init, 1e-3
     symmetry_bcs(p, ("XMIN", "YMIN"))
+    return p
+
+
+def _sph(p: CaseParams) -> CaseParams:
+    p.cas_test = 39
     return p
 
 

@@ -567,6 +567,8 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   if (P.cas_model == MHC_CASE_SOD) {
     if (P.cas_test == MHC_TEST_BISOD_X || P.cas_test == MHC_TEST_BISOD_Y || P.cas_test == MHC_TEST_BISOD_Z)
       mat = (comp(cc, P.cas_test - MHC_TEST_BISOD_X) < 0.5) ? 0. : 1.;
+    else if (P.cas_test == MHC_TEST_BISOD_SPH)
+      mat = (sqrt(cc.x * cc.x + cc.y * cc.y + cc.z * cc.z) < 0.5) ? 0. : 1.;
   } else if (P.cas_model == MHC_CASE_TWO_STATE) {
     if (NE > 1) mat = (comp(cc, P.interface_dir) < P.interface_pos) ? 0. : 1.;
   } else if (P.cas_model == MHC_CASE_ONECELL) {

@@ -602,6 +602,10 @@ static void init_materials(Case& C) {
       if (P.cas_test == MHC_TEST_BISOD_X || P.cas_test == MHC_TEST_BISOD_Y || P.cas_test == MHC_TEST_BISOD_Z) {
         double r = comp(C.cell_coord[c], P.cas_test - MHC_TEST_BISOD_X);
         m = (r < 0.5) ? 0. : 1.;
+      } else if (P.cas_test == MHC_TEST_BISOD_SPH) {
+        /* SODService.cc:56-62 */
+        const R3& x = C.cell_coord[c];
+        m = (std::sqrt(x.x * x.x + x.y * x.y + x.z * x.z) < 0.5) ? 0. : 1.;
       }
     } else if (P.cas_model == MHC_CASE_ONECELL) {
       m = 0.;  /* ONECELLService::initMat */
