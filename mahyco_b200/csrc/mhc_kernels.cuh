@@ -1702,9 +1702,10 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   }
   const bool oldpure = __popc(old) == 1;
   const bool pure = __popc(nm) == 1;
-  // mass fractions survive a cell whose total mass is below threshold^2
-  double mfe[NE], mfg;
-  mfg = 1.;
+  // mass fractions survive a cell whose total mass is below threshold^2.
+  // A pure cell's volume and mass fractions (the global slots of the
+  // reference) live in the entries of its one environment.
+  double mfe[NE];
   for (int q = 0; q < NE; ++q) mfe[q] = 0.;
   {
     // previous values with the pure-cell storage transfer of the env manager
@@ -1713,78 +1714,77 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
       if (!was) continue;
       mfe[q] = (NE > 1 && !oldpure) ? F.emf[q * N + c] : 1.;
     }
-    if (pure) for (int q = 0; q < NE; ++q) if ((nm >> q) & 1) mfg = ((old >> q) & 1) ? mfe[q] : 1.;
+    if (pure)
+      for (int q = 0; q < NE; ++q)
+        if (((nm >> q) & 1) && !((old >> q) & 1)) mfe[q] = 1.;
   }
-  double vol[NE], dens[NE], ener[NE];
+  double vol[NE];
   double volt = 0., masset = 0.;
   for (int q = 0; q < NE; ++q) { vol[q] = u[q]; volt += vol[q]; masset += u[NE + q]; }
   double unsurvolt = 1. / volt;
   for (int q = 0; q < NE; ++q) vol[q] *= Veul * unsurvolt;
   double unsurvol = 1. / Veul;
-  double fe[NE], fg = 0.;
+  double fe[NE];
   for (int q = 0; q < NE; ++q) fe[q] = 0.;
-#define EVF(q) (*(pure ? &fg : &fe[q]))
-#define EVMF(q) (*(pure ? &mfg : &mfe[q]))
   double somme_frac = 0.;
   for (int q = 0; q < NE; ++q) {
     if (!((nm >> q) & 1)) continue;
-    EVF(q) = vol[q] * unsurvol;
-    if (EVF(q) < thr) EVF(q) = 0.;
-    somme_frac += EVF(q);
+    fe[q] = vol[q] * unsurvol;
+    if (fe[q] < thr) fe[q] = 0.;
+    somme_frac += fe[q];
   }
   double unsursf = 0.;
   if (somme_frac != 0.) unsursf = 1. / somme_frac;
   for (int q = 0; q < NE; ++q)
-    if ((nm >> q) & 1) EVF(q) *= unsursf;
+    if ((nm >> q) & 1) fe[q] *= unsursf;
   if (masset > thr * thr) {
     double unsurm = 1. / masset, fm = 0.;
     for (int q = 0; q < NE; ++q) {
       if (!((nm >> q) & 1)) continue;
-      EVMF(q) = u[NE + q] * unsurm;
-      if (EVF(q) < thr) EVMF(q) = 0.;
-      fm += EVMF(q);
+      mfe[q] = u[NE + q] * unsurm;
+      if (fe[q] < thr) mfe[q] = 0.;
+      fm += mfe[q];
     }
     if (fm != 0.) {
       double unsurfm = 1. / fm;
       for (int q = 0; q < NE; ++q)
-        if ((nm >> q) & 1) EVMF(q) *= unsurfm;
+        if ((nm >> q) & 1) mfe[q] *= unsurfm;
     }
   }
+  // environment densities and energies (0 for an absent environment)
+  double rhoe[NE], ee[NE];
   double dn = 0.;
   for (int q = 0; q < NE; ++q) {
-    dens[q] = 0.;
+    rhoe[q] = 0.;
     if (!((nm >> q) & 1)) continue;
-    if (EVF(q) > thr && vol[q] != 0.) dens[q] = div_rn(u[NE + q], vol[q]);
-    dn += EVF(q) * dens[q];
+    if (fe[q] > thr && vol[q] != 0.) rhoe[q] = div_rn(u[NE + q], vol[q]);
+    dn += fe[q] * rhoe[q];
   }
   for (int q = 0; q < NE; ++q) {
-    ener[q] = 0.;
+    ee[q] = 0.;
     if (!((nm >> q) & 1)) continue;
-    if (EVF(q) > thr && u[NE + q] != 0.) ener[q] = div_rn(u[2 * NE + q], u[NE + q]);
+    if (fe[q] > thr && u[NE + q] != 0.) ee[q] = div_rn(u[2 * NE + q], u[NE + q]);
   }
-  // aliased stores: g* are the global slots, e*[] the env slots
+  // aliased stores: g* are the global slots, e*[] the env slots (a mixed
+  // cell's environment masses mfe * mg and pseudo-viscosities qv are
+  // formed at the store)
   double rhog = dn;
   double mg = Veul * dn;
   double eg = 0., qg = 0.;
-  double me[NE], rhoe[NE], ee[NE], qe[NE];
-  for (int q = 0; q < NE; ++q) { me[q] = rhoe[q] = ee[q] = qe[q] = 0.; }
+  const double qv = u[NV - 1] * unsurvol;
   double en = 0., ps = 0.;
   for (int q = 0; q < NE; ++q) {
     if (!((nm >> q) & 1)) continue;
     if (pure) {
-      mg = mfg * mg;
-      qg = u[NV - 1] * unsurvol;
-      rhog = dens[q];
-      eg = ener[q];
-      en += mfg * eg;
-      ps += fg * qg;
+      mg = mfe[q] * mg;
+      qg = qv;
+      rhog = rhoe[q];
+      eg = ee[q];
+      en += mfe[q] * eg;
+      ps += fe[q] * qg;
     } else {
-      me[q] = mfe[q] * mg;
-      qe[q] = u[NV - 1] * unsurvol;
-      rhoe[q] = dens[q];
-      ee[q] = ener[q];
       en += mfe[q] * ee[q];
-      ps += fe[q] * qe[q];
+      ps += fe[q] * qv;
     }
   }
   eg = en;
@@ -1792,12 +1792,13 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
   int st = 0;
   for (int q = 0; q < NE; ++q) {
     if (!((nm >> q) & 1)) continue;
-    double& r = pure ? rhog : rhoe[q];
-    double& ie = pure ? eg : ee[q];
-    if (r < 0. || ie < 0.) {
-      ie = 0.; r = 0.; EVF(q) = 0.; EVMF(q) = 0.;
+    if (pure) {
+      if (rhog < 0. || eg < 0.) { eg = 0.; rhog = 0.; fe[q] = 0.; mfe[q] = 0.; }
+      if (rhog != rhog || eg != eg) st |= ST_NAN;
+    } else {
+      if (rhoe[q] < 0. || ee[q] < 0.) { ee[q] = 0.; rhoe[q] = 0.; fe[q] = 0.; mfe[q] = 0.; }
+      if (rhoe[q] != rhoe[q] || ee[q] != ee[q]) st |= ST_NAN;
     }
-    if (r != r || ie != ie) st |= ST_NAN;
   }
   if (st) atomicOr(&F.s->status, st);
   if (P.conservation_energie_totale) {
@@ -1823,7 +1824,7 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
     delta = smax(0., delta);
     for (int q = 0; q < NE; ++q) {
       if (!((nm >> q) & 1)) continue;
-      if (pure) eg += mfg * delta;
+      if (pure) eg += mfe[q] * delta;
       else ee[q] += mfe[q] * delta;
     }
     if (!pure) eg += delta;
@@ -1869,35 +1870,37 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
     // of a present environment (the pure-cell value included); an absent
     // environment keeps the values of this remap's last sweep
     // (RemapADIService.cc:493-530 on the final projected values)
+    // (the projected values read again: they are cached, and not keeping
+    // them live through the EOS saves registers)
     double sv = 0.;
-    for (int q = 0; q < NE; ++q) sv += u[q];
+    for (int q = 0; q < NE; ++q) sv += Ufin[q * N + c];
     for (int q = 0; q < NE; ++q) {
       if ((nm >> q) & 1) {
-        F.phi_pb[q * N + c] = EVF(q);
+        F.phi_pb[q * N + c] = fe[q];
       } else {
-        F.phi_pb[q * N + c] = div_rn(u[q], sv);
-        F.phi_pb[(NE + q) * N + c] = u[q] != 0. ? div_rn(u[NE + q], u[q]) : 0.;
-        F.phi_pb[(2 * NE + q) * N + c] = u[NE + q] != 0. ? div_rn(u[2 * NE + q], u[NE + q]) : 0.;
+        const double v = Ufin[q * N + c], m = Ufin[(NE + q) * N + c], ie = Ufin[(2 * NE + q) * N + c];
+        F.phi_pb[q * N + c] = div_rn(v, sv);
+        F.phi_pb[(NE + q) * N + c] = v != 0. ? div_rn(m, v) : 0.;
+        F.phi_pb[(2 * NE + q) * N + c] = m != 0. ? div_rn(ie, m) : 0.;
       }
     }
   }
-#undef EVF
-#undef EVMF
   F.rho[c] = rhog; F.e[c] = eg; F.p[c] = pg; F.c[c] = cg; F.q[c] = qg; F.m[c] = mg;
   F.V[c] = Veul;
   F.mask[c] = nm;
   if (NE > 1 && !pure) {
     for (int q = 0; q < NE; ++q) {
-      F.ef[q * N + c] = fe[q]; F.emf[q * N + c] = mfe[q]; F.em[q * N + c] = me[q];
+      const bool in = (nm >> q) & 1;
+      F.ef[q * N + c] = fe[q]; F.emf[q * N + c] = mfe[q]; F.em[q * N + c] = in ? mfe[q] * mg : 0.;
       F.erho[q * N + c] = rhoe[q]; F.ee[q * N + c] = ee[q]; F.ep[q * N + c] = pe[q];
-      F.ec[q * N + c] = ce[q]; F.eq[q * N + c] = qe[q];
+      F.ec[q * N + c] = ce[q]; F.eq[q * N + c] = in ? qv : 0.;
     }
   } else if (NE > 1) {
     // a pure cell's volume fraction, the normalised one of the reference
     // (m_fracvol of the cell, which can end an ulp below 1); only read
     // back, in the environment's slot
     for (int q = 0; q < NE; ++q)
-      if ((nm >> q) & 1) F.ef[q * N + c] = fg;
+      if ((nm >> q) & 1) F.ef[q * N + c] = fe[q];
   }
 }
 
