@@ -982,9 +982,9 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
   const bool cm = DIM == 2 && P.mesh_cell_order == 1;
   R3 S = {0., 0., 0.};
   // every load of the node's cells first (a cell outside the mesh reads
-  // cell 0 and is skipped), then the sums in the reference's order
-  double pq[NS];
-  R3 cq[NS];
+  // cell 0 and is skipped), each cell's force (p + q) CQS formed as its
+  // loads arrive, then the sums in the reference's order
+  R3 fv[NS];
   bool in[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -995,14 +995,12 @@ __device__ __forceinline__ void body_lagrange_nodes(const Mesh& M, const mhc_cas
     in[s] = !(ci < 0 || cj < 0 || ci >= M.ncx || cj >= M.ncy || (DIM == 3 && (ck < 0 || ck >= M.ncz)));
     const int l = (-dk) * 4 + ((-dj) ? ((-di) ? 2 : 3) : ((-di) ? 1 : 0));
     const long long c = in[s] ? cell_id(M, ci, cj, ck) : 0;
-    pq[s] = __ldg(F.p + c) + __ldg(F.q + c);
-    cq[s] = load_cqs<DIM>(F, N, c, l);
+    fv[s] = (__ldg(F.p + c) + __ldg(F.q + c)) * load_cqs<DIM>(F, N, c, l);
   }
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     if (!in[s]) continue;
-    const R3 fv = pq[s] * cq[s];
-    S.x = S.x + fv.x; S.y = S.y + fv.y; S.z = S.z + fv.z;
+    S.x = S.x + fv[s].x; S.y = S.y + fv[s].y; S.z = S.z + fv[s].z;
   }
   if (EL) {
 #pragma unroll

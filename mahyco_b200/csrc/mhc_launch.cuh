@@ -172,10 +172,11 @@ __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__
   }
 }
 
-// resident blocks per SM asked of the compiler for the two Lagrange kernels
-// (their corner normals hold ~100 doubles live per thread)
+// resident blocks per SM asked of the compiler for the Lagrange cell pass:
+// 3 (80 registers) spills a little but hides more of its loads than 2
+// (124 registers, no spills)
 #ifndef MHC_LAG_MIN_BLOCKS
-#define MHC_LAG_MIN_BLOCKS 1
+#define MHC_LAG_MIN_BLOCKS 3
 #endif
 
 // resident blocks per SM asked of the compiler for the node pass (a latency
