@@ -269,6 +269,7 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
         p.lx, p.ly, p.lz = float(xyz[:, 0].max() - xyz[:, 0].min()), float(xyz[:, 1].max() - xyz[:, 1].min()), 0.0
         info["init_fields"]["NodeCoord"] = xyz.ravel().tolist()
         info["msh_sides"] = msh["sides"]
+        info["mesh_file"] = msh["file_order"]
         # the file's elements run column by column: its sums over cells too
         order = msh["cell_order"]
         nx_, ny_ = msh["nx"], msh["ny"]

@@ -50,9 +50,14 @@ def read_msh(path: str) -> dict:
     ``cell_groups`` (the 2D physical group name of every cell, library
     cell order), ``sides`` (1D physical group name -> logical side, an
     mhc_surface number), ``cell_order`` (the file's element index of every
-    library cell) and ``node_tags`` (the file's node tag of every library
-    node).  Raises NotImplementedError when the mesh is not a logically
-    structured grid of quadrangles."""
+    library cell), ``node_tags`` (the file's node tag of every library
+    node) and ``file_order``, the numbering the reference's outputs use
+    (its mesh reader numbers the quadrangles and the nodes they use in
+    file order): ``cells`` (the library cell of every quadrangle),
+    ``nodes`` (the library node of every used node) and ``conn`` (every
+    quadrangle's nodes as 1-based positions in ``nodes``).  Raises
+    NotImplementedError when the mesh is not a logically structured grid of
+    quadrangles."""
     sec = _sections(open(path).read())
     fmt = sec["MeshFormat"][0].split()
     if not fmt[0].startswith("4") or fmt[1] != "0":
@@ -84,11 +89,13 @@ def read_msh(path: str) -> dict:
     nl = [l for l in sec["Nodes"] if l.strip()]
     nblocks = int(nl[0].split()[0])
     coords: dict[int, tuple[float, float, float]] = {}
+    file_nodes: list[int] = []
     r = 1
     for _ in range(nblocks):
         d, tag, param, n = map(int, nl[r].split())
         r += 1
         tags = [int(nl[r + k]) for k in range(n)]
+        file_nodes += tags
         r += n
         for k in range(n):
             x, y, z = (float(t) for t in nl[r + k].split()[:3])
@@ -185,5 +192,12 @@ def read_msh(path: str) -> dict:
             sides[name] = SIDES["j=0"]
         elif ijs and all(b == ny for _, b in ijs):
             sides[name] = SIDES["j=ny"]
+    lib_node = {int(t): q for q, t in enumerate(node_tags)}
+    used = [t for t in file_nodes if t in lib_node]
+    pos = {t: q + 1 for q, t in enumerate(used)}
+    cells = np.zeros(nx * ny, dtype=np.int64)
+    cells[order] = np.arange(nx * ny)
+    file_order = {"cells": cells.tolist(), "nodes": [lib_node[t] for t in used],
+                  "conn": [[pos[t] for t in v] for _, _, v in quads]}
     return {"nx": nx, "ny": ny, "coords": xyz, "cell_groups": groups, "sides": sides,
-            "cell_order": order, "node_tags": node_tags}
+            "cell_order": order, "node_tags": node_tags, "file_order": file_order}

@@ -24,6 +24,11 @@ from .case import CaseParams, read_arc
 
 HISTORY_VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
 NODE_VARS = {"Velocity": "vector", "NodeMass": "scalar", "NodeCoord": "vector"}
+# post-processed variables the Ensight writer produces; the others of a
+# dataset's <output> list are left out
+ENSIGHT_VARS = frozenset({"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy",
+                          "PseudoViscosity", "Materiau", "SoundSpeed", "CellVolume", "StrainTensorXX",
+                          "StrainTensorYY", "StrainTensorXY", "StrainTensorXZ", "StrainTensorYZ"})
 
 
 def write_gnuplot(out_dir: str, env_names: list[str], rows: np.ndarray, variables=HISTORY_VARS) -> list[str]:
@@ -69,11 +74,15 @@ def materiau(h) -> np.ndarray:
 
 
 def write_ensight(h, out_dir: str, variables: list[str], time: float, step: int = 0,
-                  times: list[float] | None = None) -> list[str]:
+                  times: list[float] | None = None, mesh_file: dict | None = None) -> list[str]:
     """Ensight gold ASCII files of the current state of case ``h`` as time
     step ``step``; ``times`` (default ``[time]``) are the time values of
-    every step written so far, listed in ensight.case."""
+    every step written so far, listed in ensight.case.  Variables outside
+    ENSIGHT_VARS are skipped.  ``mesh_file`` (``read_msh``'s ``file_order``)
+    writes a Gmsh grid's nodes, quadrangles and values in the file's
+    numbering, as the reference does."""
     times = [time] if times is None else times
+    variables = [v for v in variables if v in ENSIGHT_VARS]
     sfx = f"{step:06d}"
     p: CaseParams = h.params
     d = os.path.join(out_dir, "depouillement")
@@ -104,6 +113,13 @@ def write_ensight(h, out_dir: str, variables: list[str], time: float, step: int 
     if dim == 3:
         offs += [(0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
     conn = np.stack([nid(i + a, j + b, k + c) for a, b, c in offs], axis=1)
+    cell_perm = node_perm = None
+    if mesh_file is not None:
+        cell_perm = np.asarray(mesh_file["cells"])
+        node_perm = np.asarray(mesh_file["nodes"])
+        xs, ys, zs = xs[node_perm], ys[node_perm], zs[node_perm]
+        conn = np.asarray(mesh_file["conn"])
+        nn = len(node_perm)
     geo = ["Output ensight test\n", "File description\n", "node id assign\n", "element id assign\n",
            "part\n", f"{1:10d}\n", "AllCells\n", "coordinates\n", f"{nn:10d}\n",
            _values(xs), _values(ys), _values(zs), f"{etype}\n", f"{h.ncell:10d}\n",
@@ -118,14 +134,18 @@ def write_ensight(h, out_dir: str, variables: list[str], time: float, step: int 
             kind = NODE_VARS[var]
             a = h.field(var)
             if kind == "scalar":
-                body = _values(a)
+                body = _values(a if node_perm is None else a[node_perm])
             else:
                 v = a.reshape(-1, 3)
+                if node_perm is not None:
+                    v = v[node_perm]
                 body = _values(v[:, 0]) + _values(v[:, 1]) + _values(v[:, 2])
             text = f"{var}\npart\n{1:10d}\ncoordinates\n" + body
             entries.append(f"{kind} per node:       1   {var} {var}/{var}******\n")
         else:
             a = materiau(h) if var == "Materiau" else h.field(var)
+            if cell_perm is not None:
+                a = a[cell_perm]
             text = f"{var}\npart\n{1:10d}\n{etype}\n" + _values(a)
             entries.append(f"scalar per element:    1   {var} {var}/{var}******\n")
         os.makedirs(os.path.join(d, var), exist_ok=True)
@@ -164,8 +184,9 @@ def run_case(p: CaseParams, info: dict, out_dir: str, max_iter: int = 10 ** 7) -
             h.set_initial_field(name, values)
         h.hydroStartInit()
         init_files = []
+        mf = info.get("mesh_file")
         if info.get("save_init"):
-            init_files = write_ensight(h, out_dir, info.get("output_vars", []), 0.0)
+            init_files = write_ensight(h, out_dir, info.get("output_vars", []), 0.0, mesh_file=mf)
         rows = []
         it = 0
         st = 0
@@ -183,9 +204,9 @@ def run_case(p: CaseParams, info: dict, out_dir: str, max_iter: int = 10 ** 7) -
         files = write_gnuplot(out_dir, info["env_names"], np.array(rows), info.get("history_vars", HISTORY_VARS))
         if info.get("save_init"):
             files += init_files + write_ensight(h, out_dir, info.get("output_vars", []), s["time"], 1,
-                                                [0.0, s["time"]])
+                                                [0.0, s["time"]], mesh_file=mf)
         else:
-            files += write_ensight(h, out_dir, info.get("output_vars", []), s["time"])
+            files += write_ensight(h, out_dir, info.get("output_vars", []), s["time"], mesh_file=mf)
         return {"scalars": s, "files": files}
     finally:
         h.close()

@@ -68,7 +68,10 @@ CASES = {
     # DefaultModel (EPP / YEPP), Mie-Gruneisen, explicit pressure; pressure
     # and energy grow from zero, so their first lines carry relative
     # differences up to 3e-10 that fall to 1e-13 as they grow
-    "CAS_Compression_isotherme_ALU_monodimX": {"tol": 5e-10},
+    "CAS_Compression_isotherme_ALU_monodimX": {"tol": 5e-10,
+                                               # round-off residues (|value| <= 0.2 where XX reaches 1.7e8)
+                                               "ensight_skip": ["StrainTensorYY/StrainTensorYY000001",
+                                                                "StrainTensorXY/StrainTensorXY000001"]},
     # per-axis Euler (is-euler-scheme Y), super-Gaussian energy deposit,
     # ONECELL init, Mie-Gruneisen; 200 000 equal cell masses averaged in one
     # running sum carry 3.7e-12 of rounding (the reference's four per-rank
@@ -103,7 +106,11 @@ CASES = {
     # uninitialised trace (elasto/DefaultModelService.cc:82, 96), which the
     # restatement takes as 0
     "CAS_2D_Lag_Taylor_elasto": {"exact_lines": 32, "time_tol": 3e-7,
-                                 "tol_var": {"Pressure": 3e-5, "Density": 3e-9, "InternalEnergy": 2e-8}},
+                                 "tol_var": {"Pressure": 3e-5, "Density": 3e-9, "InternalEnergy": 2e-8},
+                                 # the final state of the variables that the drift moves beyond 6 digits
+                                 "ensight_skip": [f"{v}/{v}000001" for v in (
+                                     "Pressure", "SoundSpeed", "Velocity", "StrainTensorXX", "StrainTensorYY",
+                                     "StrainTensorXY")] + ["ensight.geo/ensight.geo000001"]},
     # Gmsh quarter annulus (noh.msh: 100 radial x 10 angular cells), EXTERNAL
     # init with the user velocity -x/|x|, OnFileVelocity on the outer radius,
     # 6020 Lagrangian iterations; with correctly rounded powers every line of
@@ -126,8 +133,7 @@ CASES = {
                                                           "tol_var": {"Pressure": 5e-8}},
 }
 # variables the Ensight writer of mahyco_b200.output produces
-ENSIGHT_VARS = {"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy", "PseudoViscosity",
-                "Materiau", "SoundSpeed", "CellVolume"}
+from mahyco_b200.output import ENSIGHT_VARS  # noqa: E402
 VARS = ("CellMass", "Pressure", "Density", "InternalEnergy")
 
 
@@ -151,18 +157,28 @@ def main(ref_root, only=()):
         # run writes only its first sub-domain, so none are kept for those
         dep = os.path.join(d, "output", "depouillement")
         digests = {}
-        # (a mesh file's run numbers its nodes and cells like the file, the
-        # library like its grid: no digest for those)
-        if extra.get("mpi_ranks", 1) == 1 and set(info["output_vars"]) <= ENSIGHT_VARS and not info["init_fields"]:
+        # (a mesh file's run is written in the file's numbering; a dataset
+        # that post-processes variables the writer does not produce keeps the
+        # digests of the geometry and of the variables it does)
+        partial = not set(info["output_vars"]) <= ENSIGHT_VARS
+        if extra.get("mpi_ranks", 1) == 1 and (not info["init_fields"] or "mesh_file" in info):
             for root, _, files in os.walk(dep):
                 for fn in sorted(files):
                     full = os.path.join(root, fn)
-                    digests[os.path.relpath(full, dep)] = ensight_digest.digest(full)
+                    rel = os.path.relpath(full, dep)
+                    top = rel.split(os.sep)[0]
+                    if partial and top not in ENSIGHT_VARS and top != "ensight.geo":
+                        continue
+                    if rel in extra.get("ensight_skip", ()):
+                        continue
+                    digests[rel] = ensight_digest.digest(full)
         out = {"case": case, "params": params_to_dict(p), "env_names": info["env_names"],
                "timeloop": info["timeloop"], "extra": extra, "time_history": hist,
                "output_vars": info["output_vars"], "save_init": info["save_init"], "ensight_sha256": digests}
         if info["init_fields"]:
             out["init_fields"] = info["init_fields"]
+        if "mesh_file" in info:
+            out["mesh_file"] = info["mesh_file"]
         with open(os.path.join(HERE, case + ".json"), "w") as f:
             json.dump(out, f, indent=0)
         print(case, {k: len(v) for k, v in hist.items()})
