@@ -154,7 +154,11 @@ int mhc_scalars_wait(mhc_case* h, int slot, double* time, double* deltat, long l
 
 /* Named fields (names of src/Mahyco.axl: Density, Pressure, InternalEnergy,
  * SoundSpeed, PseudoViscosity, CellMass, CellVolume, FracVol, MassFraction,
- * CaracteristicLength, EnvMask; nodes: Velocity (x,y,z interleaved),
+ * CaracteristicLength, EnvMask, Temperature (Lagrangian runs; the cell value
+ * of a mixed cell is 0, as the services write environment values only),
+ * StrainTensorXX/YY/ZZ/XY/YZ/XZ, PlasticDeformation,
+ * PlasticDeformationVelocity, StrainNorm (elasto-plastic runs); nodes:
+ * Velocity (x,y,z interleaved),
  * NodeMass, NodeCoord, and VelocityN for sans-lagrange cases: the prescribed
  * velocities at n).  env < 0 selects the global cell value, env >= 0
  * the environment value (0 where the cell is not in the environment).
@@ -191,7 +195,11 @@ long long mhc_set_field(mhc_case* h, const char* name, int env, const double* ho
  * One call per method of the service interface, on environment env of the
  * case (its .axl options are the mhc_env_params of that environment).
  * mhc_eos_apply: applyEOS(env) on the current density and internal energy
- * of the env cells; mixed cells holding env then get computePressionMoyenne. */
+ * of the env cells; mixed cells holding env then get computePressionMoyenne.
+ * The temperature (field "Temperature", carried by Lagrangian runs) is set by
+ * mhc_eos_init and advanced by the iterations; mhc_eos_apply and
+ * mhc_eos_apply_one_cell leave it (its update needs the energy at the start
+ * of the iteration, which is not kept between iterations). */
 int mhc_eos_apply(mhc_case* h, int env);
 /* initEOS(env): internal energy and sound speed of the env cells from their
  * pressure and density (PerfectGasEOSService.cc:12-35,

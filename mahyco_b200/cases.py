@@ -546,6 +546,16 @@ PARITY_CASES = {
                                         120),
     "adi2d_triple_point_mono": (lambda: triple_point(mono=True, limiter=SUPERBEE), 120),
     "adi3d_triple_point": (lambda: triple_point(dim=3, n=(28, 12, 3)), 60),
+    # the temperature of Lagrangian runs through the other schemes and
+    # services: a stiffened gas (its zero default cv gives infinite
+    # temperatures, as the reference's), Mie-Gruneisen with Newton steps
+    # (its applyOneCellEOS adds to the value kept by the last applyEOS), with
+    # an energie-ref, and with an energie-ref of 0 taken from the first cell
+    # of nonzero energy
+    "lag2d_water_air": (lambda: water_air(remap=False, deltat_init=1e-8), 100),
+    "lag2d_mie_gruneisen_newton": (lambda: _mg_newton(mie_gruneisen_plate(deltat_init=1e-8)), 100),
+    "lag2d_mie_gruneisen_eref": (lambda: _mg_eref(mie_gruneisen_plate(deltat_init=1e-8)), 80),
+    "lag2d_mie_gruneisen_first_eref": (lambda: _mg_first_eref(mie_gruneisen_plate(deltat_init=1e-8)), 80),
     # BiSodSph (cas-test 39): the BiSod states inside and outside the sphere
     # of radius 0.5 about the origin (CAS_BiSodSph at 16^3 and in 2D)
     "adi3d_bisod_sph": (lambda: _sph(sod(dim=3, n=(16, 16, 16), L=(1.0, 1.0, 1.0), deltat_init=1e-3)), 40),
@@ -578,6 +588,29 @@ def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> Cas
     p.mesh_cell_order = 1 if colmajor else 0
     p.deltat_init, p.deltat_max = deltat_init, 1e-3
     symmetry_bcs(p, ("XMIN", "YMIN"))
+    return p
+
+
+def _mg_newton(p: CaseParams) -> CaseParams:
+    p.pression_explicite = 0
+    p.with_newton = 1
+    for e in range(p.nb_env):
+        p.env[e].specific_heat = 897.0
+    return p
+
+
+def _mg_eref(p: CaseParams) -> CaseParams:
+    p.pression_explicite = 0
+    for e in range(p.nb_env):
+        p.env[e].energie_ref, p.env[e].temperature_ref = 2.0e5, 290.0
+    return p
+
+
+def _mg_first_eref(p: CaseParams) -> CaseParams:
+    # one environment, no initial pressure left of the interface (zero
+    # energy, so the reference energy is the first cell to its right)
+    p.nb_env = 1
+    p.env[0].pression_initiale = 0.0
     return p
 
 

@@ -219,6 +219,11 @@ int rider_upload(mhc_case* h, cudaStream_t st) {
 void launch_init(Engine* e) {
   for (Group& g : e->groups) {
     DISPATCH_GROUP(g, (plaunch(e, kb_init_cells<DIM_, NE_>, CT, 0, g.init_cells)));
+    if (!g.EULER && !g.ADV) {
+      // the temperature of a Lagrangian run (initEOS)
+      DISPATCH_GROUP(g, (plaunch(e, kb_eref_candidates<DIM_, NE_>, CT, 0, g.init_cells, -1)));
+      DISPATCH_GROUP(g, (plaunch(e, kb_init_temperature<DIM_, NE_>, CT, 0, g.init_cells, -1)));
+    }
     DISPATCH_GROUP(g, (plaunch(e, kb_init_nodes<DIM_>, CT, 0, g.init_nodes)));
   }
 }
@@ -538,11 +543,12 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   ncell = (long long)p->nx * p->ny * (dim == 3 ? p->nz : 1);
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
   int ne = p->nb_env, nv = 3 * ne + 1;
-  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 6 : 0) + (dim == 3 ? 24 : 8) +
+  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 9 : 0) + (dim == 3 ? 24 : 8) +
                     (p->projection_pente_borne ? nv : 0) + 2;  // (+2: boundary-condition energy, pressure)
   const bool csts = p->schema_csts && p->with_projection;
   long long nodes = 4 + 6 + 10 + ((p->sans_lagrange || csts) ? 3 : 0) + (csts ? 3 : 0) + ((p->with_projection && p->is_euler_scheme == MHC_EULER_FULL && !p->sans_lagrange) ? 1 : 0);
   if (csts) cells += 1;
+  if (!p->with_projection && !p->sans_lagrange) cells += 2 * ne;  // temperature
   return cells * ncell + nodes * nnode;
 }
 
@@ -744,7 +750,10 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
     F.Ud[b] = (double*)alloc(5 * NN * sizeof(double));
   }
   F.mflux = (double*)alloc(h->NE * N * sizeof(double));
-  if (h->P.env[0].elasto_model) F.S = (double*)alloc(6 * N * sizeof(double));
+  if (h->P.env[0].elasto_model) {
+    F.S = (double*)alloc(6 * N * sizeof(double));
+    F.pl = (double*)alloc(3 * N * sizeof(double));
+  }
   F.cqs = (double*)alloc((h->DIM == 3 ? 24 : 8) * N * sizeof(double));
   if (h->P.projection_pente_borne) F.phi_pb = (double*)alloc(h->NV * N * sizeof(double));
   const bool csts = h->P.schema_csts && h->P.with_projection;
@@ -760,6 +769,11 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
     F.ebc = (double*)alloc(N * sizeof(double));
     F.pbc = (double*)alloc(N * sizeof(double));
   }
+  if (!h->P.with_projection && !h->P.sans_lagrange) {
+    // the temperature the EOS services advance, carried by Lagrangian runs
+    F.T = (double*)alloc(h->NE * N * sizeof(double));
+    F.Tn = (double*)alloc(h->NE * N * sizeof(double));
+  }
   h->d_scal = (Scalars*)alloc(sizeof(Scalars));
   h->d_params = (mhc_case_params*)alloc(sizeof(mhc_case_params));
   F.s = h->d_scal;
@@ -772,7 +786,8 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
     case_free(h);
     return set_err(MHC_ERR_CUDA, "memset");
   }
-  if (F.S && cudaMemsetAsync(F.S, 0, 6 * N * sizeof(double), h->stream) != cudaSuccess) {
+  if ((F.S && cudaMemsetAsync(F.S, 0, 6 * N * sizeof(double), h->stream) != cudaSuccess) ||
+      (F.pl && cudaMemsetAsync(F.pl, 0, 3 * N * sizeof(double), h->stream) != cudaSuccess)) {
     case_free(h);
     return set_err(MHC_ERR_CUDA, "memset");
   }
@@ -803,6 +818,7 @@ int case_reset_scalars(mhc_case* h, long long iteration_limit) {
   s.iteration = 1;
   s.dt_min_bits = 0x7fefffffffffffffull;
   s.iteration_limit = iteration_limit;
+  for (int q = 0; q < 4; ++q) s.eref_first[q] = 0xffffffffu;
   // a copy from pageable host memory is staged before the call returns, so
   // the stack source may go at once (no wait for the work in flight)
   CK(cudaMemcpyAsync(h->d_scal, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
@@ -927,6 +943,23 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
     }
     return N;
   }
+  if (!strcmp(name, "Temperature")) {
+    // env >= 0: the environment's temperature (0 where it is absent); env <
+    // 0: the cell value, which is a pure cell's and 0 in a mixed cell (the
+    // services write environment values only)
+    if (!F.T) return set_err(MHC_ERR_UNSUPPORTED, "the temperature is carried by Lagrangian runs only");
+    if (cap < N) return set_err(MHC_ERR_ARG, "capacity too small");
+    std::vector<uint8_t> mask(N);
+    std::vector<double> t((size_t)h->NE * N);
+    int r;
+    if ((r = fetch(st, F.mask, mask.data(), N)) || (r = fetch(st, F.T, t.data(), h->NE * N * 8))) return r;
+    for (long long i = 0; i < N; ++i) {
+      const bool pure = __builtin_popcount(mask[i]) == 1;
+      if (env >= 0) host[i] = ((mask[i] >> env) & 1) ? t[env * N + i] : 0.;
+      else host[i] = pure ? t[(__builtin_ffs(mask[i]) - 1) * N + i] : 0.;
+    }
+    return N;
+  }
   if (!strcmp(name, "EnvMask")) {
     if (cap < N) return set_err(MHC_ERR_ARG, "capacity too small");
     std::vector<uint8_t> mask(N);
@@ -934,6 +967,19 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
     if (r) return r;
     for (long long i = 0; i < N; ++i) host[i] = mask[i];
     return N;
+  }
+  // elasto output variables: plastic strain, its rate, the deviator's norm
+  // (DefaultModelService.cc:211-224)
+  static const char* kPlastic[] = {"PlasticDeformation", "PlasticDeformationVelocity", "StrainNorm"};
+  for (int q = 0; q < 3; ++q) {
+    if (strcmp(name, kPlastic[q])) continue;
+    if (cap < N) return set_err(MHC_ERR_ARG, "capacity too small");
+    if (!F.pl) {
+      for (long long i = 0; i < N; ++i) host[i] = 0.;
+      return N;
+    }
+    int r = fetch(st, F.pl + q * N, host, N * 8);
+    return r ? r : N;
   }
   // elasto output variables: minus the deviator components
   // (DefaultModelService.cc:217-221)

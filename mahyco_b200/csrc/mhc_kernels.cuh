@@ -38,6 +38,8 @@ struct Scalars {
   long long iteration_limit;  // last iteration this case may run
   int status;        // ST_* flags
   int pad;
+  unsigned int eref_first[4];  // Mie-Gruneisen, energie-ref 0: the first cell (reference order) of
+                               // each environment with a nonzero initial energy
 };
 
 struct Fields {
@@ -68,6 +70,9 @@ struct Fields {
                            // cartesian grid)
   double* init;            // EXTERNAL initial state given per cell: Materiau, Density, Pressure
                            // [3][ncell] (else environment 0 and its initial state everywhere)
+  double *T, *Tn;          // Lagrangian runs: the temperature the EOS services advance and its
+                           // previous value [nb_env][ncell] (a pure cell's in its environment's row)
+  double* pl;              // elasto: plastic strain, its rate, the deviator's norm [3][ncell]
   Scalars* s;
 };
 
@@ -758,6 +763,80 @@ __device__ __forceinline__ void body_init_cells(const Mesh& M, const mhc_case_pa
   }
 }
 
+// ---------------------------------------------------------------------------
+// the temperature of initEOS, Lagrangian runs (PerfectGasEOSService.cc:30,
+// StiffenedGasEOSService.cc:30: p / (287 rho); MieGruneisenEOSService.cc:
+// 17, 29-30: (e - eref) / cv + tref, an energie-ref of 0 taking the first
+// nonzero energy of the environment in the reference's cell order).  Two
+// passes: the first cell with a nonzero energy of each such environment
+// (atomicMin on its reference index), then the temperatures.  env < 0: every
+// environment.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ unsigned ref_cell_index(const Mesh& M, const mhc_case_params& P, long long c) {
+  if (DIM == 2 && P.mesh_cell_order == 1) {
+    int i, j, k;
+    cell_ijk(M, c, i, j, k);
+    return (unsigned)i * (unsigned)M.ncy + (unsigned)j;
+  }
+  return (unsigned)c;
+}
+
+__device__ __forceinline__ double env_value(const double* g, const double* e, bool pure, int q, long long N,
+                                            long long c) {
+  return pure ? g[c] : e[q * N + c];
+}
+
+template <int DIM, int NE>
+__device__ __forceinline__ void body_eref_candidates(const Mesh& M, const mhc_case_params& P, const Fields& F,
+                                                     int env, int bx) {
+  const long long c = bx * (long long)CT + threadIdx.x;
+  if (c >= M.ncell || !F.T) return;
+  const long long N = M.ncell;
+  const uint8_t mask = F.mask[c];
+  const bool pure = __popc(mask) == 1;
+  for (int q = 0; q < NE; ++q) {
+    if ((env >= 0 && q != env) || !((mask >> q) & 1)) continue;
+    const mhc_env_params& o = P.env[q];
+    if (o.eos != MHC_EOS_MIE_GRUNEISEN || o.energie_ref != 0.) continue;
+    if (env_value(F.e, F.ee, pure, q, N, c) != 0.) atomicMin(&F.s->eref_first[q], ref_cell_index<DIM>(M, P, c));
+  }
+}
+
+template <int DIM, int NE>
+__device__ __forceinline__ void body_init_temperature(const Mesh& M, const mhc_case_params& P, const Fields& F,
+                                                      int env, int bx) {
+  const long long c = bx * (long long)CT + threadIdx.x;
+  if (c >= M.ncell || !F.T) return;
+  const long long N = M.ncell;
+  const uint8_t mask = F.mask[c];
+  const bool pure = __popc(mask) == 1;
+  for (int q = 0; q < NE; ++q) {
+    if (env >= 0 && q != env) continue;
+    double T = 0.;
+    if ((mask >> q) & 1) {
+      const mhc_env_params& o = P.env[q];
+      const double p = env_value(F.p, F.ep, pure, q, N, c), rho = env_value(F.rho, F.erho, pure, q, N, c);
+      const double e = env_value(F.e, F.ee, pure, q, N, c);
+      if (o.eos == MHC_EOS_PERFECT_GAS || o.eos == MHC_EOS_STIFFENED_GAS) {
+        T = p / (287. * rho);
+      } else if (o.eos == MHC_EOS_MIE_GRUNEISEN) {
+        double eref = o.energie_ref;
+        const unsigned first = F.s->eref_first[q];
+        if (eref == 0. && first != 0xffffffffu && ref_cell_index<DIM>(M, P, c) >= first) {
+          // the energy of that first cell: the reference index back to the cell
+          long long cf = first;
+          if (DIM == 2 && P.mesh_cell_order == 1) cf = (long long)(first % M.ncy) * M.ncx + first / M.ncy;
+          eref = env_value(F.e, F.ee, __popc(F.mask[cf]) == 1, q, N, cf);
+        }
+        T = (e - eref) / o.specific_heat + o.temperature_ref;
+      }
+    }
+    F.T[q * N + c] = T;
+    F.Tn[q * N + c] = 0.;
+  }
+}
+
 // computeNodeMass (MahycoModule.cc:247-262): gather of 1/8 (1/4) cell masses in
 // ascending cell id; also initial velocity and Lagrangian positions.
 template <int DIM>
@@ -1239,7 +1318,14 @@ __device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh&
     const double coeff = Y / sqrt(3. * j2);
 #pragma unroll
     for (int q = 0; q < 6; ++q) Sv[q] *= coeff;
+    // the plastic strain rate and strain (DefaultModelService.cc:211-214),
+    // then the deviator's norm on the yield surface (215)
+    const double rate = (1. - coeff) * Y / (3. * mu * coeff * dt);
+    F.pl[N + c] = rate;
+    F.pl[c] = F.pl[c] + rate;
+    j2 = (Y * Y) / 3.;
   }
+  F.pl[2 * N + c] = sqrt(j2);  // StrainNorm (224)
   w2 = work();
 #pragma unroll
   for (int q = 0; q < 6; ++q) F.S[q * N + c] = Sv[q];
@@ -1282,6 +1368,18 @@ __device__ __forceinline__ void body_lagrange_geom(const Mesh& M, const mhc_case
 // first and V, l are read back.  CSTS (with the remap) needs them too, for
 // the work of the forces in its energy update, and leaves pressure +
 // pseudo-viscosity of the forward velocity update in pq.
+// the temperature update of applyEOS (PerfectGasEOSService.cc:62-64,
+// StiffenedGasEOSService.cc:58-60, MieGruneisenEOSService.cc:67-69) and of
+// the PerfectGas / StiffenedGas applyOneCellEOS: the previous value kept
+// (keep), the energy gained since the start of the iteration over cv added
+// to it; Mie-Gruneisen's applyOneCellEOS (121-122) adds it to the value
+// kept before
+__device__ __forceinline__ void advance_temperature(const mhc_env_params& o, double e, double e_n, bool keep,
+                                                    double& T, double& Tn) {
+  if (keep) Tn = T;
+  T = (e - e_n) / o.specific_heat + Tn;
+}
+
 template <int DIM, int NE, bool EULER, bool EL = false, bool CSTS = false>
 __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_case_params& P, const Fields& F, int bx) {
   constexpr bool GEO = EL || CSTS;
@@ -1428,6 +1526,14 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       cov = cov + dot(vn, cqn[q]) * odt;
     }
   }
+  // the temperature of a Lagrangian run, advanced by every EOS call below
+  // (advance_temperature)
+  const bool temp = !EULER && F.T != nullptr;
+  double Te[NE], Tne[NE];
+  for (int q = 0; q < NE; ++q) {
+    Te[q] = temp ? F.T[q * N + c] : 0.;
+    Tne[q] = temp ? F.Tn[q * N + c] : 0.;
+  }
   // updateEnergyAndPressure
   double ee_[NE], pe[NE], ce[NE];
   for (int q = 0; q < NE; ++q) {
@@ -1439,6 +1545,7 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
     if (P.pression_explicite) {
       ee_[q] = ecur[q] - (pne[q] + qq) * (1.0 / r - 1.0 / rn);
       eos_apply(P.env[q], r, ee_[q], pe[q], ce[q]);
+      if (temp) advance_temperature(P.env[q], ee_[q], ene[q], true, Te[q], Tne[q]);
     } else if (P.with_newton) {
       // updateEnergyAndPressurebyNewton, non-CSTS branch (MahycoModule.cc:1506-1571):
       // at most 50 Newton steps from the energy at n; the pressure and sound
@@ -1452,6 +1559,7 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       int it = 0;
       while (it < 50 && fabs(fvnr(en1, pp, en, pseudo, pn, r, rn)) >= P.threshold) {
         eos_one_cell(P.env[q], r, en1, pp, dpde);
+        if (temp) advance_temperature(P.env[q], en1, en, P.env[q].eos != MHC_EOS_MIE_GRUNEISEN, Te[q], Tne[q]);
         const double enew = en1 - fvnr(en1, pp, en, pseudo, pn, r, rn) / fvnrderiv(dpde, r, rn);
         en1 = enew;
         ++it;
@@ -1528,6 +1636,14 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       double r = pure ? rho : rhoe[q];
       double ev = pure ? eg : ee_[q];
       eos_apply(P.env[q], r, ev, pe[q], ce[q]);
+      if (temp) advance_temperature(P.env[q], ev, ene[q], true, Te[q], Tne[q]);
+    }
+  }
+  if (temp) {
+    for (int q = 0; q < NE; ++q) {
+      if (!((mask >> q) & 1)) continue;
+      F.T[q * N + c] = Te[q];
+      F.Tn[q * N + c] = Tne[q];
     }
   }
   if (pure) {

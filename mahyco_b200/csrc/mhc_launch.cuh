@@ -161,6 +161,27 @@ __global__ void __launch_bounds__(CT) kb_init_cells(const CaseDesc* __restrict__
   }
 }
 
+// the temperature of initEOS (Lagrangian runs; env < 0: every environment)
+template <int DIM, int NE>
+__global__ void __launch_bounds__(CT) kb_eref_candidates(const CaseDesc* __restrict__ C, PhaseList L, int env) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
+    const Fields F = C[wi.c].F;
+    const Mesh M = C[wi.c].M;
+    body_eref_candidates<DIM, NE>(M, *C[wi.c].P, F, env, wi.x);
+  }
+}
+
+template <int DIM, int NE>
+__global__ void __launch_bounds__(CT) kb_init_temperature(const CaseDesc* __restrict__ C, PhaseList L, int env) {
+  MHC_FOR_ITEMS(L) {
+    const WorkItem wi = item_at<PH_CELLS>(C, L, w_);
+    const Fields F = C[wi.c].F;
+    const Mesh M = C[wi.c].M;
+    body_init_temperature<DIM, NE>(M, *C[wi.c].P, F, env, wi.x);
+  }
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(CT) kb_init_nodes(const CaseDesc* __restrict__ C, PhaseList L) {
   MHC_FOR_ITEMS(L) {

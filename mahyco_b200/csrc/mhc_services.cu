@@ -275,6 +275,24 @@ long long mhc_set_field(mhc_case* h, const char* name, int env, const double* ho
     if (env_array && (r = upload(st, c.e + env * N, e.data(), N * 8))) return r;
     return N;
   }
+  if (!strcmp(name, "Temperature")) {
+    // the environment's temperature where it is present (env >= 0), or
+    // every present environment's of a pure cell (env < 0)
+    if (!F.T) return set_err(MHC_ERR_UNSUPPORTED, "the temperature is carried by Lagrangian runs only");
+    if (n < N) return set_err(MHC_ERR_ARG, "too few values");
+    std::vector<uint8_t> mask(N);
+    std::vector<double> t((size_t)h->NE * N);
+    if ((r = fetch_shared(st, F.mask, mask.data(), N)) || (r = fetch_shared(st, F.T, t.data(), h->NE * N * 8)))
+      return r;
+    for (long long i = 0; i < N; ++i) {
+      if (env >= 0) {
+        if ((mask[i] >> env) & 1) t[env * N + i] = host[i];
+      } else if (__builtin_popcount(mask[i]) == 1) {
+        t[(__builtin_ffs(mask[i]) - 1) * N + i] = host[i];
+      }
+    }
+    return (r = upload(st, F.T, t.data(), h->NE * N * 8)) ? r : N;
+  }
   if (!strcmp(name, "EnvMask")) {
     if (n < N) return set_err(MHC_ERR_ARG, "too few values");
     std::vector<uint8_t> mask(N);
@@ -334,6 +352,14 @@ int mhc_eos_init(mhc_case* h, int env) {
       case 2: plaunch(e, kb_eos_init_env<2>, CT, 0, g.init_cells, env); break;
       case 3: plaunch(e, kb_eos_init_env<3>, CT, 0, g.init_cells, env); break;
       default: plaunch(e, kb_eos_init_env<4>, CT, 0, g.init_cells, env); break;
+    }
+  }
+  if (h->F.T) {
+    // initEOS also sets the environment's temperature (Lagrangian runs)
+    CK(cudaMemsetAsync(&h->d_scal->eref_first[env], 0xff, sizeof(unsigned int), h->stream));
+    for (Group& g : e->groups) {
+      DISPATCH_GROUP(g, (plaunch(e, kb_eref_candidates<DIM_, NE_>, CT, 0, g.init_cells, env)));
+      DISPATCH_GROUP(g, (plaunch(e, kb_init_temperature<DIM_, NE_>, CT, 0, g.init_cells, env)));
     }
   }
   CK(cudaGetLastError());

@@ -28,7 +28,18 @@ NODE_VARS = {"Velocity": "vector", "NodeMass": "scalar", "NodeCoord": "vector"}
 # dataset's <output> list are left out
 ENSIGHT_VARS = frozenset({"CellMass", "Pressure", "Density", "Velocity", "NodeMass", "InternalEnergy",
                           "PseudoViscosity", "Materiau", "SoundSpeed", "CellVolume", "StrainTensorXX",
-                          "StrainTensorYY", "StrainTensorXY", "StrainTensorXZ", "StrainTensorYZ"})
+                          "StrainTensorYY", "StrainTensorXY", "StrainTensorXZ", "StrainTensorYZ",
+                          "Temperature", "PlasticDeformation", "PlasticDeformationVelocity", "StrainNorm",
+                          "FracPhase1", "FracPhase2", "FracPhase3"})
+
+
+def frac_phase(h, var: str) -> np.ndarray:
+    """The phase fractions of the cells: only the tabulated EOS (not built)
+    changes them; ONECELL sets the first to 1 (ONECELLService.cc:29-31),
+    the other initialisations leave the 0 of hydroStartInit."""
+    from .case import CASE_ONECELL
+    one = var == "FracPhase1" and h.params.cas_model == CASE_ONECELL
+    return np.full(h.ncell, 1.0 if one else 0.0)
 
 
 def write_gnuplot(out_dir: str, env_names: list[str], rows: np.ndarray, variables=HISTORY_VARS) -> list[str]:
@@ -143,7 +154,12 @@ def write_ensight(h, out_dir: str, variables: list[str], time: float, step: int 
             text = f"{var}\npart\n{1:10d}\ncoordinates\n" + body
             entries.append(f"{kind} per node:       1   {var} {var}/{var}******\n")
         else:
-            a = materiau(h) if var == "Materiau" else h.field(var)
+            if var == "Materiau":
+                a = materiau(h)
+            elif var.startswith("FracPhase"):
+                a = frac_phase(h, var)
+            else:
+                a = h.field(var)
             if cell_perm is not None:
                 a = a[cell_perm]
             text = f"{var}\npart\n{1:10d}\n{etype}\n" + _values(a)

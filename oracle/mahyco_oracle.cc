@@ -138,6 +138,8 @@ struct Case {
    * symmetric, components xx yy zz xy yz zx per cell */
   bool elasto = false;
   std::vector<double> sdev, sdev_n;
+  /* elasto outputs: plastic strain, its rate, the deviator's norm */
+  std::vector<double> plastic, plastic_rate, strain_norm;
   std::vector<R3> hourglass;          /* anti-hourglass velocity correction */
   std::vector<R3> outer_normal;       /* ncell * 2*dim */
   /* faces, per direction */
@@ -150,6 +152,10 @@ struct Case {
   MatField density, density_n, density_0, pressure, pressure_n, pseudo, pseudo_n, pseudo_nm1,
       mass_fraction, cell_mass, internal_energy, internal_energy_n, dpde, fracvol,
       cell_volume, cell_volume_n, tau_density, sound_speed;
+  /* the temperature the EOS services advance and its previous value
+   * (m_temperature, m_temperature_n), carried in Lagrangian runs */
+  MatField temperature, temperature_n;
+  bool carries_temperature() const { return !P.with_projection && !P.sans_lagrange; }
   std::vector<uint8_t> envmask, nenvc;
   /* remap */
   int nvars = 4;
@@ -363,13 +369,41 @@ static void eos_init(Case& C, int env) {
       C.EV(C.sound_speed, env, c) = o.c0;
     }
     C.EV(C.density_0, env, c) = C.EV(C.density, env, c);
+    /* the temperature of PerfectGas and StiffenedGas (line 30 of both):
+     * the air constant 287 */
+    if (C.carries_temperature() && (o.eos == MHC_EOS_PERFECT_GAS || o.eos == MHC_EOS_STIFFENED_GAS))
+      C.EV(C.temperature, env, c) = p / (287. * rho);
   }
+  if (C.carries_temperature() && o.eos == MHC_EOS_MIE_GRUNEISEN) {
+    /* MieGruneisenEOSService.cc:17, 29-30: an energie-ref of 0 takes the
+     * first nonzero energy of the environment's cells, in cell order */
+    double eref = o.energie_ref;
+    for (long k = 0; k < C.ncell; ++k) {
+      const long c = C.ord(k);
+      if (!C.has(c, env)) continue;
+      const double e = C.EV(C.internal_energy, env, c);
+      if (eref == 0) eref = e;
+      C.EV(C.temperature, env, c) = (e - eref) / o.specific_heat + o.temperature_ref;
+    }
+  }
+}
+
+/* the temperature update of applyEOS (PerfectGas 62-64, StiffenedGas
+ * 58-60, MieGruneisen 67-69) and of the PerfectGas / StiffenedGas
+ * applyOneCellEOS: the previous value kept, the energy gained since the
+ * start of the iteration over cv added to it; Mie-Gruneisen's
+ * applyOneCellEOS (121-122) adds it to the kept value instead */
+static void advance_temperature(Case& C, const mhc_env_params& o, int env, long c, double e, bool keep) {
+  double& T = C.EV(C.temperature, env, c);
+  double& Tn = C.EV(C.temperature_n, env, c);
+  if (keep) Tn = T;
+  T = (e - C.EV(C.internal_energy_n, env, c)) / o.specific_heat + Tn;
 }
 
 /* IEquationOfState::applyEOS for one environment (PG 45-67, SG 43-63, MG 44-97).
  * Damage (m_maille_endo) never triggers with the threshold defaults, and the
  * temperature update has no hydro feedback; neither is carried. */
-static void eos_apply(Case& C, int env) {
+static void eos_apply(Case& C, int env, bool temperature = true) {
   const mhc_env_params& o = C.P.env[env];
   for (long c = 0; c < C.ncell; ++c) {
     if (!C.has(c, env)) continue;
@@ -407,6 +441,8 @@ static void eos_apply(Case& C, int env) {
       if ((p2 - p1) > 0.) C.EV(C.sound_speed, env, c) = std::sqrt((p2 - p1) / 2.e-7);
       else C.EV(C.sound_speed, env, c) = 1.e4;
     }
+    if (temperature && C.carries_temperature() && o.eos != MHC_EOS_FICTIF)
+      advance_temperature(C, o, env, c, C.EV(C.internal_energy, env, c), true);
   }
 }
 
@@ -889,6 +925,9 @@ static void setup(Case& C, const mhc_case_params* p) {
   C.cqs_n = C.cqs;
   C.elasto = p->env[0].elasto_model != 0;
   C.sdev.assign(C.elasto ? C.ncell * 6 : 0, 0.);
+  C.plastic.assign(C.elasto ? C.ncell : 0, 0.);
+  C.plastic_rate.assign(C.elasto ? C.ncell : 0, 0.);
+  C.strain_norm.assign(C.elasto ? C.ncell : 0, 0.);
   C.sdev_n = C.sdev;
   C.hourglass.assign(C.nnode, {0, 0, 0});
   C.outer_normal.assign(C.ncell * 2 * C.dim, {0, 0, 0});
@@ -905,7 +944,7 @@ static void setup(Case& C, const mhc_case_params* p) {
   MatField* mf[] = {&C.density, &C.density_n, &C.density_0, &C.pressure, &C.pressure_n, &C.pseudo,
                     &C.pseudo_n, &C.pseudo_nm1, &C.mass_fraction, &C.cell_mass, &C.internal_energy,
                     &C.internal_energy_n, &C.dpde, &C.fracvol, &C.cell_volume, &C.cell_volume_n,
-                    &C.tau_density, &C.sound_speed};
+                    &C.tau_density, &C.sound_speed, &C.temperature, &C.temperature_n};
   for (MatField* f : mf) f->init(C.ncell, C.nenv, 0.);
   C.envmask.assign(C.ncell, 1);
   C.nenvc.assign(C.ncell, 1);
@@ -1429,7 +1468,13 @@ static void update_elasticity_and_plasticity(Case& C) {
     if (j2 > sq(Y) / 3.) {
       const double coeff = Y / std::sqrt(3. * j2);
       for (int q = 0; q < 6; ++q) S[q] *= coeff;
+      /* the plastic strain rate and strain (DefaultModelService.cc:211-214),
+       * then the deviator's norm on the yield surface (215, 224) */
+      C.plastic_rate[c] = (1. - coeff) * Y / (3. * mu * coeff * dt);
+      C.plastic[c] += C.plastic_rate[c];
+      j2 = sq(Y) / 3.;
     }
+    C.strain_norm[c] = std::sqrt(j2);
     work();
   }
 }
@@ -1522,6 +1567,7 @@ static void update_energy_and_pressure(Case& C) {
         int i = 0;
         while (i < 50 && std::fabs(fvnr(en1, p, en, pseudo, pn, rn1, rn)) >= eps) {
           eos_one_cell(o, rn1, en1, p, dpde);
+          if (C.carries_temperature()) advance_temperature(C, o, e, c, en1, o.eos != MHC_EOS_MIE_GRUNEISEN);
           double enew = en1 - fvnr(en1, p, en, pseudo, pn, rn1, rn) / fvnrderiv(dpde, rn1, rn);
           en1 = enew;
           i++;
@@ -2626,7 +2672,7 @@ static ora::MatField* mat_field(ora::Case& C, const char* name) {
       {"Density", &C.density}, {"Pressure", &C.pressure}, {"InternalEnergy", &C.internal_energy},
       {"SoundSpeed", &C.sound_speed}, {"PseudoViscosity", &C.pseudo}, {"CellMass", &C.cell_mass},
       {"CellVolume", &C.cell_volume}, {"FracVol", &C.fracvol}, {"MassFraction", &C.mass_fraction},
-      {"DpDe", &C.dpde}, {"TauxDensity", &C.tau_density}};
+      {"DpDe", &C.dpde}, {"TauxDensity", &C.tau_density}, {"Temperature", &C.temperature}};
   for (auto& t : tab)
     if (!strcmp(name, t.n)) return t.f;
   return nullptr;
@@ -2656,6 +2702,13 @@ long oracle_get_field(void* h, const char* name, int env, double* out, long cap)
     if (strcmp(name, kStrain[q])) continue;
     if (cap < C.ncell) return -1;
     for (long c = 0; c < C.ncell; ++c) out[c] = C.elasto ? -C.sdev[c * 6 + q] : 0.;
+    return C.ncell;
+  }
+  if (!strcmp(name, "PlasticDeformation") || !strcmp(name, "PlasticDeformationVelocity") ||
+      !strcmp(name, "StrainNorm")) {
+    if (cap < C.ncell) return -1;
+    const std::vector<double>& v = name[0] == 'S' ? C.strain_norm : (name[18] == 'V' ? C.plastic_rate : C.plastic);
+    for (long c = 0; c < C.ncell; ++c) out[c] = v.empty() ? 0. : v[c];
     return C.ncell;
   }
   if (!strcmp(name, "NodeMass")) {
@@ -2730,7 +2783,9 @@ int oracle_set_initial_field(void* h, const char* name, const double* in, long n
 int oracle_eos_apply(void* h, int env) {
   ora::Case& C = *(ora::Case*)h;
   if (env < 0 || env >= C.nenv) return -1;
-  ora::eos_apply(C, env);
+  /* the library's entry point leaves the temperature (it does not keep the
+   * energy at the start of the iteration that the update needs) */
+  ora::eos_apply(C, env, false);
   double option = C.P.calcul_vitson_max ? 1. : 0.;
   for (long c = 0; c < C.ncell; ++c) {
     if (C.pure(c) || !C.has(c, env)) continue;
@@ -2757,7 +2812,7 @@ void oracle_eos_point(const mhc_env_params* o, double rho, double e, double* p, 
   ora::setup(C, &P);
   C.density.g[0] = rho;
   C.internal_energy.g[0] = e;
-  ora::eos_apply(C, 0);
+  ora::eos_apply(C, 0, false);
   *p = C.pressure.g[0];
   *c = C.sound_speed.g[0];
   *dpde = C.dpde.g[0];

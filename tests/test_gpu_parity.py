@@ -32,6 +32,12 @@ ENV_FIELDS = ["Density", "Pressure", "InternalEnergy", "FracVol", "CellMass"]
 
 
 def rel_inf(a, b):
+    # non-finite values (a temperature over a zero specific heat) must sit at
+    # the same places with the same values; the rest is compared relatively
+    fa, fb = np.isfinite(a), np.isfinite(b)
+    if not np.array_equal(fa, fb) or not np.array_equal(a[~fa], b[~fb], equal_nan=True):
+        return np.inf
+    a, b = a[fa], b[fb]
     d = np.max(np.abs(a - b)) if a.size else 0.0
     s = np.max(np.abs(b)) if b.size else 0.0
     return d / s if s > 0 else d
@@ -43,8 +49,15 @@ def compare(gpu, ora, nenv):
         errs[f] = rel_inf(gpu.field(f), ora.field(f))
     for f in ("Velocity", "NodeMass"):
         errs[f] = rel_inf(gpu.field(f), ora.field(f))
-    for f in ("StrainTensorXX", "StrainTensorYY", "StrainTensorXY"):
+    for f in ("StrainTensorXX", "StrainTensorYY", "StrainTensorXY", "PlasticDeformation",
+              "PlasticDeformationVelocity", "StrainNorm"):
         errs[f] = rel_inf(gpu.field(f), ora.field(f))
+    p = gpu.params
+    if not p.with_projection and not p.sans_lagrange:
+        # the temperature the EOS services advance (Lagrangian runs)
+        errs["Temperature"] = rel_inf(gpu.field("Temperature"), ora.field("Temperature"))
+        for e in range(nenv):
+            errs[f"Temperature[{e}]"] = rel_inf(gpu.field("Temperature", e), ora.field("Temperature", e))
     if nenv > 1:
         errs["EnvMask"] = float(np.any(gpu.field("EnvMask") != ora.field("EnvMask")))
         for e in range(nenv):
