@@ -37,6 +37,17 @@ namespace {
 int pinned_get(size_t bytes, void** out);
 void pinned_put(void* p, size_t bytes);
 
+// a node vector field's three component arrays interleaved (x, y, z per
+// node) on the device, so that it comes back in one copy
+__global__ void kb_interleave3(const double* __restrict__ a, const double* __restrict__ b,
+                               const double* __restrict__ c, double* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    out[3 * i] = a[i];
+    out[3 * i + 1] = b[i];
+    out[3 * i + 2] = c[i];
+  }
+}
+
 bool case_elasto(const mhc_case* h) { return h->P.env[0].elasto_model != 0; }
 bool case_hourglass(const mhc_case* h) { return !h->P.with_projection && h->P.coef_antiderive != 0.; }
 bool case_cell_bcs(const mhc_case* h) {
@@ -1006,7 +1017,7 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
   if (vn && !F.v0) return set_err(MHC_ERR_ARG, "VelocityN is kept by sans-lagrange cases only");
   if (!strcmp(name, "Velocity") || !strcmp(name, "NodeCoord") || vn) {
     if (cap < 3 * NN) return set_err(MHC_ERR_ARG, "capacity too small");
-    std::vector<double> a(NN), b(NN), c(NN);
+    std::vector<double> a, b, c;
     const double *pa, *pb, *pc;
     if (vn) { pa = F.v0; pb = F.v0 + NN; pc = F.v0 + 2 * NN; }
     else if (name[0] == 'V') { pa = F.vx; pb = F.vy; pc = F.vz; }
@@ -1019,6 +1030,18 @@ long long case_get_field(mhc_case* h, cudaStream_t st, const char* name, int env
       pa = F.X[par][0]; pb = F.X[par][1]; pc = F.X[par][2];
     }
     int r;
+    double* d = nullptr;
+    if (cudaMallocAsync((void**)&d, 3 * NN * sizeof(double), st) == cudaSuccess) {
+      // interleaved on the device, then one copy (straight into a
+      // page-locked destination)
+      const int blocks = (int)std::min<long long>((NN + 255) / 256, 148LL * 8);
+      kb_interleave3<<<blocks, 256, 0, st>>>(pa, pb, pc, d, NN);
+      r = fetch(st, d, host, 3 * NN * 8);
+      cudaFreeAsync(d, st);
+      return r ? r : 3 * NN;
+    }
+    cudaGetLastError();  // no device memory left: the three arrays, interleaved here
+    a.resize(NN); b.resize(NN); c.resize(NN);
     if ((r = fetch(st, pa, a.data(), NN * 8)) || (r = fetch(st, pb, b.data(), NN * 8)) || (r = fetch(st, pc, c.data(), NN * 8)))
       return r;
     for (long long i = 0; i < NN; ++i) { host[3 * i] = a[i]; host[3 * i + 1] = b[i]; host[3 * i + 2] = c[i]; }
