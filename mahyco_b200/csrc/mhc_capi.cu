@@ -32,11 +32,7 @@ int mhc::set_err(int code, const std::string& msg) {
   return code;
 }
 
-namespace {
-
-int pinned_get(size_t bytes, void** out);
-void pinned_put(void* p, size_t bytes);
-
+namespace mhc {
 // a node vector field's three component arrays interleaved (x, y, z per
 // node) on the device, so that it comes back in one copy
 __global__ void kb_interleave3(const double* __restrict__ a, const double* __restrict__ b,
@@ -47,6 +43,13 @@ __global__ void kb_interleave3(const double* __restrict__ a, const double* __res
     out[3 * i + 2] = c[i];
   }
 }
+}  // namespace mhc
+
+namespace {
+
+int pinned_get(size_t bytes, void** out);
+void pinned_put(void* p, size_t bytes);
+
 
 bool case_elasto(const mhc_case* h) { return h->P.env[0].elasto_model != 0; }
 bool case_hourglass(const mhc_case* h) { return !h->P.with_projection && h->P.coef_antiderive != 0.; }
