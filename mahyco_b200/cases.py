@@ -556,6 +556,12 @@ PARITY_CASES = {
     "lag2d_mie_gruneisen_newton": (lambda: _mg_newton(mie_gruneisen_plate(deltat_init=1e-8)), 100),
     "lag2d_mie_gruneisen_eref": (lambda: _mg_eref(mie_gruneisen_plate(deltat_init=1e-8)), 80),
     "lag2d_mie_gruneisen_first_eref": (lambda: _mg_first_eref(mie_gruneisen_plate(deltat_init=1e-8)), 80),
+    # elasto-plasticity with the Full Euler remap: the deviator and plastic
+    # strains projected with the other variables
+    "adi2d_bar_impact_remap": (lambda: _remap_elasto(bar_impact(n=(8, 40), L=(0.01, 0.05)), MINMOD), 60),
+    "adi2d_bar_impact_remap_superbee": (lambda: _remap_elasto(
+        bar_impact(n=(10, 30), L=(0.01, 0.03), velocity=400.0), SUPERBEE), 60),
+    "adi3d_bar_impact_remap_vanleer": (lambda: _remap_elasto(_bar3d(), VANLEER), 30),
     # BiSodSph (cas-test 39): the BiSod states inside and outside the sphere
     # of radius 0.5 about the origin (CAS_BiSodSph at 16^3 and in 2D)
     "adi3d_bisod_sph": (lambda: _sph(sod(dim=3, n=(16, 16, 16), L=(1.0, 1.0, 1.0), deltat_init=1e-3)), 40),
@@ -611,6 +617,15 @@ def _mg_first_eref(p: CaseParams) -> CaseParams:
     # energy, so the reference energy is the first cell to its right)
     p.nb_env = 1
     p.env[0].pression_initiale = 0.0
+    return p
+
+
+def _remap_elasto(p: CaseParams, limiter: int) -> CaseParams:
+    p.with_projection = 1
+    p.is_euler_scheme = 0  # Full
+    p.ordre_projection = 2
+    p.projection_limiteur_id = limiter
+    p.coef_antiderive = 0.0  # the anti-hourglass correction is Lagrangian only
     return p
 
 

@@ -254,6 +254,8 @@ template <int DIM>
 void lag_nodes_dispatch(Engine* e, Group& g) {
   if (g.EULER && g.CSTS) {
     lag_nodes_launch<DIM, false, false, false, true>(e, g);
+  } else if (g.EULER && g.EL) {
+    lag_nodes_launch<DIM, true, false, false>(e, g);
   } else if (g.EULER) {
     lag_nodes_launch<DIM, false, false, false>(e, g);
   } else if (g.EL) {
@@ -293,8 +295,13 @@ void launch_lagrange_nodes(Engine* e) {
 void launch_lagrange_cells(Engine* e) {
   StageTimer tm(e, MHC_STAGE_LAGRANGE_CELLS);
   for (Group& g : e->groups) {
-    if (g.EL) {
-      // elasto cases: one environment, Lagrangian (validated at creation)
+    if (g.EL && g.EULER) {
+      // elasto cases with the remap: the deviator and plastic strains packed
+      // among the projected variables
+      if (g.DIM == 2) plaunch(e, kb_lagrange_cells<2, 1, true, true>, CT, 0, g.lag_cells);
+      else plaunch(e, kb_lagrange_cells<3, 1, true, true>, CT, 0, g.lag_cells);
+    } else if (g.EL) {
+      // elasto cases: one environment (validated at creation)
       if (g.DIM == 2) plaunch(e, kb_lagrange_cells<2, 1, false, true>, CT, 0, g.lag_cells);
       else plaunch(e, kb_lagrange_cells<3, 1, false, true>, CT, 0, g.lag_cells);
     } else if (g.CSTS) {
@@ -556,7 +563,7 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   int dim = p->dim;
   ncell = (long long)p->nx * p->ny * (dim == 3 ? p->nz : 1);
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
-  int ne = p->nb_env, nv = 3 * ne + 1;
+  int ne = p->nb_env, nv = 3 * ne + 1 + ((p->env[0].elasto_model && p->with_projection) ? MHC_ELASTO_XV : 0);
   long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 9 : 0) + (dim == 3 ? 24 : 8) +
                     (p->projection_pente_borne ? nv : 0) + 2;  // (+2: boundary-condition energy, pressure)
   const bool csts = p->schema_csts && p->with_projection;
@@ -650,8 +657,15 @@ int validate(const mhc_case_params* p) {
     const mhc_env_params& o = p->env[e];
     if (o.elasto_model < 0 || o.elasto_model > 1) return set_err(MHC_ERR_UNSUPPORTED, "elasto-model must be NoModel or DefaultModel");
     if (o.elasto_model == 0) continue;
-    if (p->nb_env != 1 || p->with_projection)
-      return set_err(MHC_ERR_UNSUPPORTED, "elasto-plasticity needs one environment and a Lagrangian loop");
+    if (p->nb_env != 1) return set_err(MHC_ERR_UNSUPPORTED, "elasto-plasticity needs one environment");
+    // with the remap: the deviator and plastic strains ride along as seven
+    // more projected variables, through the warp-per-line cell sweeps
+    if (p->with_projection &&
+        (p->is_euler_scheme != MHC_EULER_FULL || p->projection_pente_borne || p->ordre_projection > 2 ||
+         p->projection_limiteur_id > MHC_VANLEER || p->schema_csts || p->sans_lagrange))
+      return set_err(MHC_ERR_UNSUPPORTED,
+                     "elasto-plasticity with the remap needs the Full Euler scheme, order 1 or 2, a classical "
+                     "limiter, no pente-borne, no schema-csts");
     if (o.rotation_order != 1 && o.rotation_order != 2) return set_err(MHC_ERR_UNSUPPORTED, "ordre-rotation must be 1 or 2");
     if (!(o.shear_modulus > 0.) || !(o.yield_strength > 0.)) return set_err(MHC_ERR_ARG, "shear modulus and yield strength must be > 0");
   }
@@ -714,7 +728,11 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   h->P = *params;
   h->DIM = params->dim;
   h->NE = params->nb_env;
-  h->NV = 3 * h->NE + 1;
+  // projected variables: volume, mass, energy per environment, the
+  // pseudo-viscosity, then (elasto-plasticity with the remap) the deviator's
+  // xx, yy, xy, yz, zx times the volume and the plastic strain rate and
+  // strain times the mass (PrepareRemap.cc:121-128)
+  h->NV = 3 * h->NE + 1 + ((h->P.env[0].elasto_model && h->P.with_projection) ? MHC_ELASTO_XV : 0);
   Mesh& M = h->M;
   M.dim = h->DIM;
   M.ncx = params->nx; M.ncy = params->ny; M.ncz = h->DIM == 3 ? params->nz : 1;

@@ -235,6 +235,11 @@ inline int group_node_phase(int LIM, int NCOLS, int NTILE, int D) {
 // the (line-chunk, tile) direction masks of a case's cell or node sweeps
 // under an engine's layout choice
 inline void sweep_masks(const mhc_case* h, int layout, bool nodes, int& cols, int& tile) {
+  if (!nodes && h->P.env[0].elasto_model && h->P.with_projection) {
+    // the seven elasto variables ride through the warp-per-line cell sweeps only
+    cols = tile = 0;
+    return;
+  }
   cols = nodes ? node_cols_mask(h) : cols_mask(h);
   tile = nodes ? node_tile_mask(h) : tile_mask(h);
   const int mode = nodes ? node_sweep_mode(h->P) : cell_sweep_mode(h->P);

@@ -494,6 +494,10 @@ __device__ __forceinline__ void velocity_bcs(const Mesh& M, const mhc_case_param
 // init: MahycoModule::hydroStartInit + computeCellMass (MahycoModule.cc:21-237)
 // ---------------------------------------------------------------------------
 constexpr int CT = 256;  // threads of the one-dimensional cell / node kernels
+// projected variables an elasto-plastic case adds with the remap: the
+// deviator's xx, yy, xy, yz, zx (times the volume), the plastic strain rate
+// and strain (times the mass), after the pseudo-viscosity
+constexpr int MHC_ELASTO_XV = 7;
 
 // BUBBLES (CHOCBULLEService::initMat / initVar, the bubble lattice): the
 // material of a cell from its centre cc and node coordinates -- 0 the
@@ -1598,6 +1602,18 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
       U[(2 * NE + q) * N + c] = in ? Vq * rq * ee_[q] : 0.;
     }
     U[(NV - 1) * N + c] = V * qg;
+    if constexpr (EL) {
+      // the deviator times the volume and the plastic strain rate and
+      // strain times the mass (PrepareRemap.cc:121-128), one environment
+      const double Vq = Ve[0], mq = Ve[0] * rhoe[0];
+      U[(NV + 0) * N + c] = Vq * F.S[c];
+      U[(NV + 1) * N + c] = Vq * F.S[N + c];
+      U[(NV + 2) * N + c] = Vq * F.S[3 * N + c];
+      U[(NV + 3) * N + c] = Vq * F.S[4 * N + c];
+      U[(NV + 4) * N + c] = Vq * F.S[5 * N + c];
+      U[(NV + 5) * N + c] = mq * F.pl[N + c];
+      U[(NV + 6) * N + c] = mq * F.pl[c];
+    }
     if constexpr (CSTS) {
       // the cell pressure of the forward update: the new one of an explicit
       // update in a pure cell, otherwise the one the cell holds (at n; a
@@ -1878,6 +1894,20 @@ __device__ __forceinline__ void body_remap_finalize_cells(const Mesh& M, const m
     ee[q] = 0.;
     if (!((nm >> q) & 1)) continue;
     if (fe[q] > thr && u[NE + q] != 0.) ee[q] = div_rn(u[2 * NE + q], u[NE + q]);
+  }
+  if (NE == 1 && F.S && !ADV && fe[0] > thr && u[NE] != 0.) {
+    // an elasto-plastic case: the deviator over the projected volume, its
+    // zz from the zero trace, the plastic strain rate and strain over the
+    // projected mass (RemapADIFinal.cc:200-214)
+    const double xx = Ufin[NV * N + c] / u[0], yy = Ufin[(NV + 1) * N + c] / u[0];
+    F.S[c] = xx;
+    F.S[N + c] = yy;
+    F.S[2 * N + c] = -(xx + yy);
+    F.S[3 * N + c] = Ufin[(NV + 2) * N + c] / u[0];
+    F.S[4 * N + c] = Ufin[(NV + 3) * N + c] / u[0];
+    F.S[5 * N + c] = Ufin[(NV + 4) * N + c] / u[0];
+    F.pl[N + c] = Ufin[(NV + 5) * N + c] / u[NE];
+    F.pl[c] = Ufin[(NV + 6) * N + c] / u[NE];
   }
   // aliased stores: g* are the global slots, e*[] the env slots (a mixed
   // cell's environment masses mfe * mg and pseudo-viscosities qv are

@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(CT) kb_hourglass(const CaseDesc* __restrict__ 
 #ifndef MHC_SW_MIN_BLOCKS_COLS
 #define MHC_SW_MIN_BLOCKS_COLS 3
 #endif
-template <int DIM, int NE, int D, int LIM>
+template <int DIM, int NE, int D, int LIM, int XV = 0>
 __global__ void __launch_bounds__(SW_THREADS, LIM >= LIM_COLS ? MHC_SW_MIN_BLOCKS_COLS
                                               : (LIM >= LIM_GEN ? 2 : MHC_SW_MIN_BLOCKS_CELLS))
 kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
@@ -300,7 +300,7 @@ kb_sweep_cells(const CaseDesc* __restrict__ C, PhaseList L, int k) {
     else if constexpr (LIM >= LIM_COLS) body_sweep_cells_lanes<DIM, NE, D, LIM - LIM_COLS>(M, F, A, wi.x, wi.y);
     else if constexpr (LIM == LIM_O3) body_sweep_cells_o3<DIM, NE, D>(M, F, A, wi.x, wi.y);
     else if constexpr (LIM == LIM_PB) body_sweep_cells_pb<DIM, NE, D>(M, F, P, A, wi.x, wi.y);
-    else body_sweep_cells_lanes<DIM, NE, D, LIM>(M, F, A, wi.x, wi.y);
+    else body_sweep_cells_lanes<DIM, NE, D, LIM, XV>(M, F, A, wi.x, wi.y);
   }
 }
 

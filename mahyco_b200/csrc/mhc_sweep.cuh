@@ -326,10 +326,12 @@ __device__ __forceinline__ double lane_cell_width(const Mesh& M, const Fields& F
 // the lowest transverse axis fastest, so the warps of a block read
 // neighbouring columns and share L1 sectors.
 // ---------------------------------------------------------------------------
-template <int DIM, int NE, int D, int LIM>
+// XV: further projected variables after the pseudo-viscosity (the
+// deviator and plastic strains of an elasto-plastic case), remapped like it
+template <int DIM, int NE, int D, int LIM, int XV = 0>
 __device__ __forceinline__ void body_sweep_cells_lanes(const Mesh& M, const Fields& F, const SweepArgs& A,
                                                        int vbx, int vby) {
-  constexpr int NV = 3 * NE + 1;
+  constexpr int NV = 3 * NE + 1 + XV;
   constexpr int NQ = DIM == 3 ? 4 : 2;
   constexpr unsigned FULL = 0xffffffffu;
   const long long N = M.ncell;

@@ -11,6 +11,16 @@
 
 namespace {
 
+// elasto-plastic cases with the remap: one environment, the warp-per-line
+// sweep with the seven elasto variables
+template <int DIM, int LIM>
+void cell_sweep_elasto(Engine* e, Group& g, int D, int k) {
+  StageTimer tm(e, MHC_STAGE_SWEEP_CELLS);
+  if (D == 0) plaunch(e, kb_sweep_cells<DIM, 1, 0, LIM, MHC_ELASTO_XV>, SW_THREADS, 0, g.sw_cells[0], k);
+  else if (D == 1) plaunch(e, kb_sweep_cells<DIM, 1, 1, LIM, MHC_ELASTO_XV>, SW_THREADS, 0, g.sw_cells[1], k);
+  else if constexpr (DIM == 3) plaunch(e, kb_sweep_cells<DIM, 1, 2, LIM, MHC_ELASTO_XV>, SW_THREADS, 0, g.sw_cells[2], k);
+}
+
 template <int DIM, int NE, int LIM>
 void cell_sweep(Engine* e, Group& g, int D, int k) {
   StageTimer tm(e, MHC_STAGE_SWEEP_CELLS);
@@ -49,7 +59,16 @@ void node_sweep(Engine* e, Group& g, int D, int k) {
 template <int DIM, int NE>
 void sweep_step_dn(Engine* e, Group& g, int D, int k) {
   const int cl = ((g.COLS >> D) & 1) ? LIM_COLS + g.CLIM : g.CLIM;
-  if (D > 0 && !((g.COLS >> D) & 1) && ((g.TILE >> D) & 1)) {
+  if (NE == 1 && g.EL && g.EULER) {
+    if constexpr (NE == 1) {
+      switch (g.CLIM) {
+        case 0: cell_sweep_elasto<DIM, 0>(e, g, D, k); break;
+        case 1: cell_sweep_elasto<DIM, 1>(e, g, D, k); break;
+        case 2: cell_sweep_elasto<DIM, 2>(e, g, D, k); break;
+        default: cell_sweep_elasto<DIM, LIM_ORDER1>(e, g, D, k); break;
+      }
+    }
+  } else if (D > 0 && !((g.COLS >> D) & 1) && ((g.TILE >> D) & 1)) {
     switch (g.CLIM) {
       case 0: cell_sweep_tile<DIM, NE, 0>(e, g, D, k); break;
       case 1: cell_sweep_tile<DIM, NE, 1>(e, g, D, k); break;

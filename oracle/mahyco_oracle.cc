@@ -948,7 +948,9 @@ static void setup(Case& C, const mhc_case_params* p) {
   for (MatField* f : mf) f->init(C.ncell, C.nenv, 0.);
   C.envmask.assign(C.ncell, 1);
   C.nenvc.assign(C.ncell, 1);
-  C.nvars = 3 * C.nenv + 1;
+  /* elasto-plasticity with the remap: the deviator and plastic strains
+   * after the pseudo-viscosity (PrepareRemap.cc:121-128) */
+  C.nvars = 3 * C.nenv + 1 + ((C.P.env[0].elasto_model && C.P.with_projection) ? 7 : 0);
   C.u_lag.assign(C.ncell * C.nvars, 0.);
   C.phi_lag = C.u_lag;
   C.grad_phi = C.u_lag;
@@ -1872,6 +1874,15 @@ static void compute_variables_for_remap(Case& C) {
       u[ne + e] = V * rho;
       u[2 * ne + e] = V * rho * C.EV(C.internal_energy, e, c);
       u[3 * ne] = C.cell_volume.g[c] * C.pseudo.g[c];
+      if (nv > 3 * ne + 1) {
+        /* the deviator times the volume, the plastic strain rate and strain
+         * times the mass (PrepareRemap.cc:121-128) */
+        const double* S = &C.sdev[c * 6];  /* xx yy zz xy yz zx */
+        double* x = &u[3 * ne + 1];
+        x[0] = V * S[0]; x[1] = V * S[1]; x[2] = V * S[3]; x[3] = V * S[4]; x[4] = V * S[5];
+        x[5] = V * rho * C.plastic_rate[c];
+        x[6] = V * rho * C.plastic[c];
+      }
       if (C.P.projection_pente_borne) {
         /* the cell's own environment values; entries of absent
          * environments keep their values of the previous remap */
@@ -2360,6 +2371,20 @@ static int remap_variables(Case& C) {
       if (!C.has(c, e)) continue;
       ener[e] = 0.;
       if (C.EV(C.fracvol, e, c) > thr && u[ne + e] != 0.) ener[e] = u[2 * ne + e] / u[ne + e];
+      if (nv > 3 * ne + 1 && C.EV(C.fracvol, e, c) > thr && u[ne + e] != 0.) {
+        /* RemapADIFinal.cc:200-214: the deviator over the projected volume,
+         * zz from the zero trace, the plastic strains over the mass */
+        const double* x = &u[3 * ne + 1];
+        double* S = &C.sdev[c * 6];
+        S[0] = x[0] / u[e];
+        S[1] = x[1] / u[e];
+        S[3] = x[2] / u[e];
+        S[4] = x[3] / u[e];
+        S[5] = x[4] / u[e];
+        S[2] = -(S[0] + S[1]);
+        C.plastic_rate[c] = x[5] / u[ne + e];
+        C.plastic[c] = x[6] / u[ne + e];
+      }
     }
     C.density.g[c] = dn;
     C.cell_mass.g[c] = C.euler_volume[c] * dn;

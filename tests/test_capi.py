@@ -62,8 +62,14 @@ def test_rejects_options_outside_the_hot_path():
     p.projection_pente_borne, p.ordre_projection = 1, 3   # pente-borne with the third-order remap
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p = mb.default_params()
-    p.env[0].elasto_model = 1                   # elasto with the Euler remap
+    p.env[0].elasto_model = 1
+    p.is_euler_scheme = 2                       # elasto with a per-axis Euler remap
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.is_euler_scheme, p.projection_pente_borne = 0, 1   # elasto with pente-borne fluxes
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.projection_pente_borne, p.projection_limiteur_id = 0, 4   # ... or a generalised limiter
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.projection_limiteur_id = 0
     p.with_projection, p.nb_env = 0, 2          # elasto with two environments
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p = mb.default_params()
