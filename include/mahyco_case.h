@@ -156,9 +156,12 @@ typedef struct mhc_env_params {
   /* initial state */
   double densite_initiale, pression_initiale, energie_initiale, temperature_initiale;
   double vitesse_initiale[3];
-  /* elasto-model: 0 NoModel, 1 DefaultModel (src/elasto/DefaultModelService.cc)
-   * with the EPP shear modulus (elasto-mu-model elastic-cst) and the YEPP
-   * yield strength (elasto-y-model limit-elastic); ordre-rotation 1 or 2 */
+  /* elasto-model: 0 NoModel, 1 DefaultModel (src/elasto/DefaultModelService.cc),
+   * 2 NewHypoModel (src/elasto/NewHypoModelService.cc: the deviator's rate
+   * from the left Cauchy-Green tensor of the accumulated deformation
+   * gradient), each with the EPP shear modulus (elasto-mu-model elastic-cst)
+   * and the YEPP yield strength (elasto-y-model limit-elastic);
+   * ordre-rotation 1 or 2 */
   int elasto_model;
   int rotation_order;
   double shear_modulus;

@@ -341,13 +341,13 @@ def read_arc(path: str) -> tuple[CaseParams, dict]:
                 setattr(e, attr, v)
         el = ev.find("elasto-model")
         if el is not None and el.get("name") not in (None, "NoModel"):
-            if el.get("name") != "DefaultModel":
+            if el.get("name") not in ("DefaultModel", "NewHypoModel"):
                 raise NotImplementedError(f"elasto-model {el.get('name')}")
             mu_el, y_el = el.find("elasto-mu-model"), el.find("elasto-y-model")
             if (mu_el is not None and mu_el.get("name", "EPP") != "EPP") or \
                     (y_el is not None and y_el.get("name", "YEPP") != "YEPP"):
                 raise NotImplementedError("elasto mu/y models other than EPP/YEPP")
-            e.elasto_model = 1
+            e.elasto_model = 2 if el.get("name") == "NewHypoModel" else 1
             e.rotation_order = _txt(el, "ordre-rotation", 1, int)
             if mu_el is not None:
                 e.shear_modulus = _txt(mu_el, "elastic-cst", 2.94e10)

@@ -562,6 +562,13 @@ PARITY_CASES = {
     "adi2d_bar_impact_remap_superbee": (lambda: _remap_elasto(
         bar_impact(n=(10, 30), L=(0.01, 0.03), velocity=400.0), SUPERBEE), 60),
     "adi3d_bar_impact_remap_vanleer": (lambda: _remap_elasto(_bar3d(), VANLEER), 30),
+    # NewHypoModel: the deformation gradient and the left Cauchy-Green tensor
+    "lag2d_bar_impact_newhypo": (lambda: _newhypo(bar_impact(n=(8, 40), L=(0.01, 0.05))), 80),
+    "lag2d_bar_impact_newhypo_rot2": (lambda: _newhypo(_rot2(bar_impact(n=(10, 30), L=(0.01, 0.03),
+                                                                         velocity=400.0))), 80),
+    "lag3d_bar_impact_newhypo": (lambda: _newhypo(_bar3d()), 40),
+    "adi2d_bar_impact_remap_newhypo": (lambda: _newhypo(_remap_elasto(bar_impact(n=(8, 40), L=(0.01, 0.05)),
+                                                                      MINMOD)), 60),
     # BiSodSph (cas-test 39): the BiSod states inside and outside the sphere
     # of radius 0.5 about the origin (CAS_BiSodSph at 16^3 and in 2D)
     "adi3d_bisod_sph": (lambda: _sph(sod(dim=3, n=(16, 16, 16), L=(1.0, 1.0, 1.0), deltat_init=1e-3)), 40),
@@ -573,7 +580,10 @@ PARITY_CASES = {
 # calls exp and pow, and the reverse option of RIDER scales the velocities by
 # cos(Pi t), which CUDA and the oracle's libm round differently
 PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13,
-                    "adv3d_rider_deformation_reverse": 1e-12, "lag2d_super_gaussian_pressure": 1e-12}
+                    "adv3d_rider_deformation_reverse": 1e-12, "lag2d_super_gaussian_pressure": 1e-12,
+                    # NewHypoModel's J^(5/3): pow with a non-integer exponent
+                    "lag2d_bar_impact_newhypo": 1e-11, "lag2d_bar_impact_newhypo_rot2": 1e-11,
+                    "lag3d_bar_impact_newhypo": 1e-11, "adi2d_bar_impact_remap_newhypo": 1e-11}
 
 
 def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> CaseParams:
@@ -617,6 +627,11 @@ def _mg_first_eref(p: CaseParams) -> CaseParams:
     # energy, so the reference energy is the first cell to its right)
     p.nb_env = 1
     p.env[0].pression_initiale = 0.0
+    return p
+
+
+def _newhypo(p: CaseParams) -> CaseParams:
+    p.env[0].elasto_model = 2  # NewHypoModel
     return p
 
 

@@ -43,6 +43,16 @@ __global__ void kb_interleave3(const double* __restrict__ a, const double* __res
     out[3 * i + 2] = c[i];
   }
 }
+// NewHypoModel::initElasto (NewHypoModelService.cc:13-26) and the initial
+// density the equations of state keep (MieGruneisenEOSService.cc:31 and the
+// like): F = I, rho_0 = the density after the initialisation
+__global__ void kb_hyper_init(double* __restrict__ hf, const double* __restrict__ rho, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) hf[q * n + i] = (q % 4 == 0) ? 1. : 0.;
+    hf[9 * n + i] = rho[i];
+  }
+}
 }  // namespace mhc
 
 namespace {
@@ -240,6 +250,8 @@ void launch_init(Engine* e) {
     }
     DISPATCH_GROUP(g, (plaunch(e, kb_init_nodes<DIM_>, CT, 0, g.init_nodes)));
   }
+  for (mhc_case* h : e->cases)
+    if (h->F.hf) kb_hyper_init<<<(unsigned)((h->M.ncell + 255) / 256), 256, 0, e->stream>>>(h->F.hf, h->F.rho, h->M.ncell);
 }
 
 template <int DIM, bool EL, bool HG, bool LAG, bool CSTS = false>
@@ -564,7 +576,7 @@ long long count_doubles(const mhc_case_params* p, long long& ncell, long long& n
   ncell = (long long)p->nx * p->ny * (dim == 3 ? p->nz : 1);
   nnode = (long long)(p->nx + 1) * (p->ny + 1) * (dim == 3 ? p->nz + 1 : 1);
   int ne = p->nb_env, nv = 3 * ne + 1 + ((p->env[0].elasto_model && p->with_projection) ? MHC_ELASTO_XV : 0);
-  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 9 : 0) + (dim == 3 ? 24 : 8) +
+  long long cells = 9 + (ne > 1 ? 8 * ne : 0) + 2 * nv + ne + (p->env[0].elasto_model ? 9 : 0) + (p->env[0].elasto_model == 2 ? 10 : 0) + (dim == 3 ? 24 : 8) +
                     (p->projection_pente_borne ? nv : 0) + 2;  // (+2: boundary-condition energy, pressure)
   const bool csts = p->schema_csts && p->with_projection;
   long long nodes = 4 + 6 + 10 + ((p->sans_lagrange || csts) ? 3 : 0) + (csts ? 3 : 0) + ((p->with_projection && p->is_euler_scheme == MHC_EULER_FULL && !p->sans_lagrange) ? 1 : 0);
@@ -655,7 +667,8 @@ int validate(const mhc_case_params* p) {
     return set_err(MHC_ERR_UNSUPPORTED, "projection-limiteur-pure-id must be 0..7");
   for (int e = 0; e < p->nb_env; ++e) {
     const mhc_env_params& o = p->env[e];
-    if (o.elasto_model < 0 || o.elasto_model > 1) return set_err(MHC_ERR_UNSUPPORTED, "elasto-model must be NoModel or DefaultModel");
+    if (o.elasto_model < 0 || o.elasto_model > 2)
+      return set_err(MHC_ERR_UNSUPPORTED, "elasto-model must be NoModel, DefaultModel or NewHypoModel");
     if (o.elasto_model == 0) continue;
     if (p->nb_env != 1) return set_err(MHC_ERR_UNSUPPORTED, "elasto-plasticity needs one environment");
     // with the remap: the deviator and plastic strains ride along as seven
@@ -785,6 +798,7 @@ int case_alloc(const mhc_case_params* params, cudaStream_t stream, mhc_case** ou
   if (h->P.env[0].elasto_model) {
     F.S = (double*)alloc(6 * N * sizeof(double));
     F.pl = (double*)alloc(3 * N * sizeof(double));
+    if (h->P.env[0].elasto_model == 2) F.hf = (double*)alloc(10 * N * sizeof(double));
   }
   F.cqs = (double*)alloc((h->DIM == 3 ? 24 : 8) * N * sizeof(double));
   if (h->P.projection_pente_borne) F.phi_pb = (double*)alloc(h->NV * N * sizeof(double));

@@ -73,6 +73,8 @@ struct Fields {
   double *T, *Tn;          // Lagrangian runs: the temperature the EOS services advance and its
                            // previous value [nb_env][ncell] (a pure cell's in its environment's row)
   double* pl;              // elasto: plastic strain, its rate, the deviator's norm [3][ncell]
+  double* hf;              // NewHypoModel: deformation gradient F [9][ncell] (row by row), then
+                           // the density at the EOS initialisation rho_0 [ncell]
   Scalars* s;
 };
 
@@ -1232,7 +1234,7 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
 template <int DIM>
 __device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh& M, const Fields& F, long long c,
                                             int i, int j, int k, const R3* cqn, const R3* cqs, double V, double Vn,
-                                            double mass, double dt, double& w1, double& w2) {
+                                            double mass, double rho, double dt, double& w1, double& w2) {
   constexpr int NBN = DIM == 3 ? 8 : 4;
   const long long N = M.ncell;
   R3 vel[8];
@@ -1278,10 +1280,53 @@ __device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh&
   const double mu = o.shear_modulus, Y = o.yield_strength;
   const double trace = 0.;
   double Pt[3][3];
+  if (o.elasto_model == 2) {
+    // NewHypoModel: F <- (I + G dt) F, B = F F^T (NewHypoModelService.cc:
+    // 48-49, 76-79), J = rho_0 / rho and the deviator's rate
+    // mu / J^(5/3) (DB + BD - 2/3 (B:D) I - 5/3 tr(D) dev B) dt (102-128);
+    // the thermal term mu' (T - T_n) dev B vanishes for the constant EPP
+    // shear modulus (EPPService.cc:26-28)
+    double Fo[9], Fn[3][3], B[3][3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
+    for (int q = 0; q < 9; ++q) Fo[q] = F.hf[q * N + c];
 #pragma unroll
-    for (int b = 0; b < 3; ++b) Pt[a][b] = 2 * mu * (D[a][b] - (1. / 3.) * trace * (a == b ? 1.0 : 0.0)) * dt;
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const double g0 = (a == 0 ? 1. : 0.) + G[a][0] * dt, g1 = (a == 1 ? 1. : 0.) + G[a][1] * dt,
+                     g2 = (a == 2 ? 1. : 0.) + G[a][2] * dt;
+        Fn[a][b] = g0 * Fo[0 * 3 + b] + g1 * Fo[1 * 3 + b] + g2 * Fo[2 * 3 + b];
+      }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        F.hf[(a * 3 + b) * N + c] = Fn[a][b];
+        B[a][b] = Fn[a][0] * Fn[b][0] + Fn[a][1] * Fn[b][1] + Fn[a][2] * Fn[b][2];
+      }
+    const double J = F.hf[9 * N + c] / rho;
+    const double mu_over_J = mu / pow(J, 5. / 3.);
+    const double traceD = D[0][0] + D[1][1] + D[2][2];
+    const double traceB = B[0][0] + B[1][1] + B[2][2];
+    double dcb = B[0][0] * D[0][0] + B[0][1] * D[0][1] + B[0][2] * D[0][2];
+    dcb += B[1][0] * D[1][0] + B[1][1] * D[1][1] + B[1][2] * D[1][2];
+    dcb += B[2][0] * D[2][0] + B[2][1] * D[2][1] + B[2][2] * D[2][2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const double id = a == b ? 1. : 0.;
+        const double DB = D[a][0] * B[0][b] + D[a][1] * B[1][b] + D[a][2] * B[2][b];
+        const double BD = B[a][0] * D[0][b] + B[a][1] * D[1][b] + B[a][2] * D[2][b];
+        const double devB = B[a][b] - (1. / 3. * traceB) * id;
+        Pt[a][b] = (mu_over_J * (((DB + BD) - (2. / 3. * dcb) * id) - (5. / 3. * traceD) * devB)) * dt;
+      }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) Pt[a][b] = 2 * mu * (D[a][b] - (1. / 3.) * trace * (a == b ? 1.0 : 0.0)) * dt;
+  }
   if (DIM == 2) {
     if (o.rotation_order == 1) {
       Pt[0][0] += 2 * dt * sxy * wz;
@@ -1469,7 +1514,7 @@ __device__ __forceinline__ void body_lagrange_cells(const Mesh& M, const mhc_cas
   }
   if (EL) {
     double w1, w2;
-    elasto_cell<DIM>(P.env[0], M, F, c, i, j, k, cqn, cqs, V, F.V[c], me[0], dt, w1, w2);
+    elasto_cell<DIM>(P.env[0], M, F, c, i, j, k, cqn, cqs, V, F.V[c], me[0], rhoe[0], dt, w1, w2);
     ecur[0] = ecur[0] + w1;
     ecur[0] = ecur[0] + w2;
   }

@@ -362,6 +362,11 @@ int mhc_eos_init(mhc_case* h, int env) {
       DISPATCH_GROUP(g, (plaunch(e, kb_init_temperature<DIM_, NE_>, CT, 0, g.init_cells, env)));
     }
   }
+  if (h->F.hf && env == 0) {
+    // and the initial density NewHypoModel divides by (one environment)
+    const long long N = h->M.ncell;
+    CK(cudaMemcpyAsync(h->F.hf + 9 * N, h->F.rho, N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  }
   CK(cudaGetLastError());
   return MHC_OK;
 }

@@ -140,6 +140,7 @@ struct Case {
   std::vector<double> sdev, sdev_n;
   /* elasto outputs: plastic strain, its rate, the deviator's norm */
   std::vector<double> plastic, plastic_rate, strain_norm;
+  std::vector<double> tensF;  /* NewHypoModel: the deformation gradient [ncell][3][3] */
   std::vector<R3> hourglass;          /* anti-hourglass velocity correction */
   std::vector<R3> outer_normal;       /* ncell * 2*dim */
   /* faces, per direction */
@@ -928,6 +929,8 @@ static void setup(Case& C, const mhc_case_params* p) {
   C.plastic.assign(C.elasto ? C.ncell : 0, 0.);
   C.plastic_rate.assign(C.elasto ? C.ncell : 0, 0.);
   C.strain_norm.assign(C.elasto ? C.ncell : 0, 0.);
+  C.tensF.assign(p->env[0].elasto_model == 2 ? C.ncell * 9 : 0, 0.);
+  for (long c = 0; c < (long)C.tensF.size() / 9; ++c) C.tensF[c * 9] = C.tensF[c * 9 + 4] = C.tensF[c * 9 + 8] = 1.;
   C.sdev_n = C.sdev;
   C.hourglass.assign(C.nnode, {0, 0, 0});
   C.outer_normal.assign(C.ncell * 2 * C.dim, {0, 0, 0});
@@ -1423,9 +1426,48 @@ static void update_elasticity_and_plasticity(Case& C) {
     /* ComputeElasticity (78-169) */
     const double sxx = S[0], syy = S[1], szz = S[2], sxy = S[3], syz = S[4], szx = S[5];
     const double trace = 0.;  /* see above */
-    double P[3][3];
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) P[a][b] = 2 * mu * (D[a][b] - (1. / 3.) * trace * (a == b ? 1.0 : 0.0)) * dt;
+    double P[3][3], TH[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}};
+    if (o.elasto_model == 2) {
+      /* NewHypoModel: the deformation gradient F <- (I + G dt) F and
+       * B = F F^T (NewHypoModelService.cc:48-49, 76-79), then the
+       * deviator's rate mu / J^(5/3) (DB + BD - 2/3 (B:D) I - 5/3 tr(D)
+       * dev B) dt and the thermal term mu' (T - T_n) dev B, mu' = 0 for
+       * EPP (102-139); products and contractions in Arcane's order */
+      double* Ft = &C.tensF[c * 9];
+      double Dg[3][3], Fn[3][3], B[3][3], DB[3][3], BD[3][3], devB[3][3];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) Dg[a][b] = (a == b ? 1. : 0.) + G[a][b] * dt;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) Fn[a][b] = Dg[a][0] * Ft[0 * 3 + b] + Dg[a][1] * Ft[1 * 3 + b] + Dg[a][2] * Ft[2 * 3 + b];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) Ft[a * 3 + b] = Fn[a][b];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) B[a][b] = Fn[a][0] * Fn[b][0] + Fn[a][1] * Fn[b][1] + Fn[a][2] * Fn[b][2];
+      const double J = C.EV(C.density_0, 0, c) / C.EV(C.density, 0, c);
+      const double mu_over_J = mu / std::pow(J, 5. / 3.);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          DB[a][b] = D[a][0] * B[0][b] + D[a][1] * B[1][b] + D[a][2] * B[2][b];
+          BD[a][b] = B[a][0] * D[0][b] + B[a][1] * D[1][b] + B[a][2] * D[2][b];
+        }
+      const double traceD = D[0][0] + D[1][1] + D[2][2];
+      const double traceB = B[0][0] + B[1][1] + B[2][2];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) devB[a][b] = B[a][b] - (1. / 3. * traceB) * (a == b ? 1. : 0.);
+      double dcb = B[0][0] * D[0][0] + B[0][1] * D[0][1] + B[0][2] * D[0][2];
+      dcb += B[1][0] * D[1][0] + B[1][1] * D[1][1] + B[1][2] * D[1][2];
+      dcb += B[2][0] * D[2][0] + B[2][1] * D[2][1] + B[2][2] * D[2][2];
+      const double dT = C.carries_temperature() ? C.EV(C.temperature, 0, c) - C.EV(C.temperature_n, 0, c) : 0.;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          P[a][b] = (mu_over_J * (((DB[a][b] + BD[a][b]) - (2. / 3. * dcb) * (a == b ? 1. : 0.)) -
+                                  (5. / 3. * traceD) * devB[a][b])) * dt;
+          TH[a][b] = (0. * dT) * devB[a][b];
+        }
+    } else {
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) P[a][b] = 2 * mu * (D[a][b] - (1. / 3.) * trace * (a == b ? 1.0 : 0.0)) * dt;
+    }
     if (C.dim == 2) {
       if (o.rotation_order == 1) {
         P[0][0] += 2 * dt * sxy * wz;
@@ -1453,8 +1495,8 @@ static void update_elasticity_and_plasticity(Case& C) {
       P[2][0] -= dt * (szz - sxx) * wy - dt * sxy * wx - dt * syz * wz;
       P[1][0] = P[0][1]; P[2][1] = P[1][2]; P[0][2] = P[2][0];
     }
-    S[0] = sxx + P[0][0]; S[1] = syy + P[1][1]; S[2] = szz + P[2][2];
-    S[3] = sxy + P[0][1]; S[4] = syz + P[1][2]; S[5] = szx + P[2][0];
+    S[0] = (sxx + P[0][0]) + TH[0][0]; S[1] = (syy + P[1][1]) + TH[1][1]; S[2] = (szz + P[2][2]) + TH[2][2];
+    S[3] = (sxy + P[0][1]) + TH[0][1]; S[4] = (syz + P[1][2]) + TH[1][2]; S[5] = (szx + P[2][0]) + TH[2][0];
     /* ComputePlasticity (173-226): radial return onto the yield surface;
      * the squares are math::pow(x, 2.) there (glibc's pow, or the correctly
      * rounded square x * x with cr_pow) */

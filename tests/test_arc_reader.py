@@ -70,8 +70,12 @@ def test_anti_hourglass_and_elasto_options(tmp_path):
     assert (p2.env[0].shear_modulus, p2.env[0].yield_strength) == (2.6e10, 3.e8)
     f3 = tmp_path / "n.arc"
     f3.write_text(src[:i] + el.replace("DefaultModel", "NewHypoModel") + src[i:])
+    p3, _ = read_arc(str(f3))
+    assert (p3.env[0].elasto_model, p3.env[0].rotation_order) == (2, 2)
+    f4 = tmp_path / "m.arc"
+    f4.write_text(src[:i] + el.replace('"EPP"', '"SCG"') + src[i:])
     with pytest.raises(NotImplementedError):
-        read_arc(str(f3))
+        read_arc(str(f4))
 
 
 def test_remap_order_and_generalised_limiter_options(tmp_path):
