@@ -1219,7 +1219,8 @@ __device__ __forceinline__ void body_hourglass(const Mesh& M, const mhc_case_par
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
 // updateElasticityAndPlasticity (MahycoModule.cc:1327-1353) with
-// DefaultModelService (src/elasto/DefaultModelService.cc:27-242) and the
+// DefaultModelService (src/elasto/DefaultModelService.cc:27-242), or
+// NewHypoModelService (src/elasto/NewHypoModelService.cc:32-308), and the
 // constant EPP shear modulus / YEPP yield strength, for one environment:
 // velocity gradient from the mean corner normals, deformation rate and
 // spin, work with S_n, deviator update with rotation, radial return, work
