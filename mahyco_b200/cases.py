@@ -580,10 +580,7 @@ PARITY_CASES = {
 # calls exp and pow, and the reverse option of RIDER scales the velocities by
 # cos(Pi t), which CUDA and the oracle's libm round differently
 PARITY_EXACT_TOL = {"adi2d_plaque_euler_y_depot_gaussian": 1e-13, "adi2d_bisod_cell_bcs_gaussian": 1e-13,
-                    "adv3d_rider_deformation_reverse": 1e-12, "lag2d_super_gaussian_pressure": 1e-12,
-                    # NewHypoModel's J^(5/3): pow with a non-integer exponent
-                    "lag2d_bar_impact_newhypo": 1e-11, "lag2d_bar_impact_newhypo_rot2": 1e-11,
-                    "lag3d_bar_impact_newhypo": 1e-11, "adi2d_bar_impact_remap_newhypo": 1e-11}
+                    "adv3d_rider_deformation_reverse": 1e-12, "lag2d_super_gaussian_pressure": 1e-12}
 
 
 def _external(velocity=(0.0, 0.0, 0.0), colmajor=False, deltat_init=1e-4) -> CaseParams:

@@ -74,6 +74,26 @@ __device__ __forceinline__ double pow_one_third(double x) {
   return r + corr;
 }
 
+// x^y for y = the double nearest to 5/3 (NewHypoModelService.cc:123 writes
+// pow(J, 5./3.)).  y = 5/3 + d, d = 2^-52/3 exactly, so x^y = x c^2 x^d with
+// c = cbrt(x) refined to double-double as above; x c^2 is formed as a
+// double-double (TwoProduct), the factor x^d ~ 1 + d ln x applied to first
+// order, and the sum rounded once: the correctly rounded x^y except within
+// ~2^-90 relative of a rounding boundary.
+__device__ __forceinline__ double pow_five_thirds(double x) {
+  if (!(x > 0.0) || isinf(x)) return pow(x, 5. / 3.);
+  double r = cbrt(x);
+  double s, sl, t, tl;
+  two_prod(r, r, s, sl);
+  two_prod(s, r, t, tl);
+  const double c_lo = (((x - t) - tl) - sl * r) / (3.0 * s);  // cbrt(x) = r + c_lo
+  double q, ql;
+  two_prod(x, s, q, ql);                                        // x r^2 = q + ql
+  const double d = (1.0 / 3.0) * 0x1p-52;                       // double(5/3) - 5/3
+  const double corr = (ql + x * (sl + 2.0 * r * c_lo)) + q * (d * log(x));
+  return q + corr;
+}
+
 // ---------------------------------------------------------------------------
 // structured mesh indexing (Arcane cartesian generator numbering)
 // ---------------------------------------------------------------------------

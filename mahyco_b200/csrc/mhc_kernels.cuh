@@ -1306,7 +1306,7 @@ __device__ __forceinline__ void elasto_cell(const mhc_env_params& o, const Mesh&
         B[a][b] = Fn[a][0] * Fn[b][0] + Fn[a][1] * Fn[b][1] + Fn[a][2] * Fn[b][2];
       }
     const double J = F.hf[9 * N + c] / rho;
-    const double mu_over_J = mu / pow(J, 5. / 3.);
+    const double mu_over_J = mu / pow_five_thirds(J);
     const double traceD = D[0][0] + D[1][1] + D[2][2];
     const double traceB = B[0][0] + B[1][1] + B[2][2];
     double dcb = B[0][0] * D[0][0] + B[0][1] * D[0][1] + B[0][2] * D[0][2];

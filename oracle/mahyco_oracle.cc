@@ -96,6 +96,21 @@ static inline double pow_third_cr(double x) {
   double corr = c_lo - r * (d * std::log(x));
   return r + corr;
 }
+/* x^(5./3.): x times the double-double square of the refined cbrt, times
+ * exp(d ln x) with d = double(5/3) - 5/3 = 2^-52/3, rounded once */
+static inline double pow_five_thirds_cr(double x) {
+  if (!(x > 0.0) || std::isinf(x)) return std::pow(x, 5. / 3.);
+  double r = std::cbrt(x);
+  double s, sl, t, tl;
+  two_prod(r, r, s, sl);
+  two_prod(s, r, t, tl);
+  const double c_lo = (((x - t) - tl) - sl * r) / (3.0 * s);
+  double q, ql;
+  two_prod(x, s, q, ql);
+  const double d = (1.0 / 3.0) * 0x1p-52;
+  const double corr = (ql + x * (sl + 2.0 * r * c_lo)) + q * (d * std::log(x));
+  return q + corr;
+}
 
 /* MahycoModule::produit (MahycoModule.cc:1935) */
 static inline double produit(double A, double B, double C, double D) { return A * B - C * D; }
@@ -1444,7 +1459,7 @@ static void update_elasticity_and_plasticity(Case& C) {
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) B[a][b] = Fn[a][0] * Fn[b][0] + Fn[a][1] * Fn[b][1] + Fn[a][2] * Fn[b][2];
       const double J = C.EV(C.density_0, 0, c) / C.EV(C.density, 0, c);
-      const double mu_over_J = mu / std::pow(J, 5. / 3.);
+      const double mu_over_J = mu / (g_cr_pow ? pow_five_thirds_cr(J) : std::pow(J, 5. / 3.));
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) {
           DB[a][b] = D[a][0] * B[0][b] + D[a][1] * B[1][b] + D[a][2] * B[2][b];
@@ -2888,6 +2903,7 @@ void oracle_eos_point(const mhc_env_params* o, double rho, double e, double* p, 
 /* the oracle's correctly rounded x^(1./3.), for its own unit test */
 double oracle_pow_third_cr(double x) { return ora::pow_third_cr(x); }
 double oracle_cube_cr(double x) { return ora::cube_cr(x); }
+double oracle_pow_five_thirds_cr(double x) { return ora::pow_five_thirds_cr(x); }
 
 /* number of time-history lines recorded so far */
 long oracle_th_count(void* h) { return (long)((ora::Case*)h)->th.size(); }

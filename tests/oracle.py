@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
     L.oracle_pow_third_cr.argtypes = [C.c_double]
     L.oracle_cube_cr.restype = C.c_double
     L.oracle_cube_cr.argtypes = [C.c_double]
+    L.oracle_pow_five_thirds_cr.restype = C.c_double
+    L.oracle_pow_five_thirds_cr.argtypes = [C.c_double]
     _lib = L
     return L
 

@@ -59,6 +59,19 @@ def test_cube_root_power_correctly_rounded():
         assert abs(Decimal(r) - exact) <= Decimal(math.ulp(r)) / 2, x
 
 
+def test_five_thirds_power_correctly_rounded():
+    """NewHypoModel's J^(5./3.) (the double nearest to 5/3 as exponent)."""
+    getcontext().prec = 60
+    L = lib()
+    y = Decimal(5.0 / 3.0)
+    rng = random.Random(11)
+    for _ in range(3000):
+        x = rng.uniform(0.5, 2.0) if rng.random() < 0.5 else 10 ** rng.uniform(-6, 6)
+        r = L.oracle_pow_five_thirds_cr(x)
+        exact = Decimal(x) ** y
+        assert abs(Decimal(r) - exact) <= Decimal(math.ulp(r)) / 2, x
+
+
 def test_cube_correctly_rounded():
     getcontext().prec = 60
     L = lib()
