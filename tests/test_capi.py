@@ -72,6 +72,10 @@ def test_rejects_options_outside_the_hot_path():
     p.projection_limiteur_id = 0
     p.with_projection, p.nb_env = 0, 2          # elasto with two environments
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.env[0].elasto_model = 2                   # ... NewHypoModel too
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
+    p.nb_env, p.env[0].elasto_model = 1, 3      # no such elasto model
+    assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
     p = mb.default_params()
     p.is_euler_scheme = 1                       # is-euler-scheme NON
     assert lib.mhc_case_create(ctypes.byref(p), ctypes.byref(h)) == -3
